@@ -1,0 +1,181 @@
+/*
+ * kami_vbd.h -- C ABI of the B200 Stable Cosserat Rods vertex-block-descent solver.
+ *
+ * This library replaces, for KamiSimulator's StableCosseratRods solver, the C++ calls
+ * that StableCosseratRodsSolver makes into YarnBall::Sim and SDFBodyCollisionSolver.
+ * Every entry point is extern "C", takes plain pointers and sizes, never throws, and
+ * returns a kami_status.  kami_vbd_last_error_string() describes the last failure on
+ * the calling thread.  Citations are file:line in the KamiSimulator project.
+ *
+ * Vertex order at the boundary: strands are contiguous, described by CSR offsets
+ * strand_begin[0..S] (strand s owns vertices strand_begin[s] .. strand_begin[s+1]-1),
+ * positions/velocities are packed float xyz triples in that order.  This is the
+ * order of YarnBall::Sim::verts after createFromCurves (YarnBall/io/reader.cpp:16-50)
+ * and of the rootVertices/strandRefs scatter in StableCosseratRodsSolver.cpp:238-277.
+ * Internally the solver keeps its own tile-major layout on the device.
+ */
+#ifndef KAMI_VBD_H_
+#define KAMI_VBD_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum kami_status {
+    KAMI_OK = 0,
+    KAMI_ERR_INVALID_ARGUMENT = 1, /* bad pointer, size, enum or parameter value */
+    KAMI_ERR_CUDA = 2,             /* a CUDA runtime call failed (message has the CUDA error) */
+    KAMI_ERR_OUT_OF_MEMORY = 3,    /* device or pinned-host allocation failed */
+    KAMI_ERR_NONFINITE = 4,        /* the device status word saw a NaN/Inf position, velocity or orientation */
+    KAMI_ERR_GEOMETRY = 5,         /* zero-length or dangling segment (Sim::configure, YBSimulator.cu:185-197) */
+    KAMI_ERR_UNSUPPORTED = 6,      /* request outside what this build supports (e.g. strand longer than a tile) */
+    KAMI_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
+    KAMI_ERR_STATE = 8             /* call made in the wrong order (e.g. backward without a recorded forward) */
+} kami_status;
+
+/* Gauss-Seidel order of the position and orientation sweeps. */
+typedef enum kami_schedule {
+    KAMI_SCHEDULE_COLOUR2 = 0, /* even then odd vertices, even then odd segments (by index within the strand) */
+    KAMI_SCHEDULE_JACOBI = 1   /* all vertices from the previous sweep: the intent of cosseratItr /
+                                  quaternionLambdaItr (YarnBall/sim/cosserat.cu:25-337), without their races */
+} kami_schedule;
+
+/* Which device implementation steps the solver. */
+typedef enum kami_form {
+    KAMI_FORM_AUTO = 0,  /* fused when every strand fits one warp tile, else sweep */
+    KAMI_FORM_SWEEP = 1, /* one kernel per colour sweep, replayed from a CUDA graph (the plain per-groom form) */
+    KAMI_FORM_FUSED = 2  /* one kernel per step: each warp owns a strand tile for all iterations */
+} kami_form;
+
+typedef enum kami_stiffness_mode {
+    KAMI_STIFFNESS_YOUNG = 0, /* Sim::setYoung(E [GPa], deviation), YBSimulator.cu:300-320 */
+    KAMI_STIFFNESS_K = 1      /* Sim::setKStretch / setKBend, YBSimulator.cu:276-298 */
+} kami_stiffness_mode;
+
+typedef enum kami_memory {
+    KAMI_MEMORY_HOST = 0,  /* pointer is host memory (pageable or pinned) */
+    KAMI_MEMORY_DEVICE = 1 /* pointer is device memory of the solver's device */
+} kami_memory;
+
+/* Body signed-distance grid: SDFBodyCollisionSolver's grid (SDFBodyCollisionSolver.cpp:122-167,
+ * cudaSDFCollision.cuh:23-48).  Node (i, j, k) sits at grid_min + ds * (i, j, k) with
+ * ds = (grid_max - grid_min) / dims; arrays are x-fastest: index = i + nx * (j + ny * k). */
+typedef struct kami_vbd_sdf_desc {
+    int32_t dims[3];
+    float grid_min[3];
+    float grid_max[3];
+    float threshold;   /* SDFThreshold: surface offset subtracted from phi (ThreshSdf) */
+    const float* phi;  /* host, nx*ny*nz signed distances */
+    const float* grad; /* host, 3*nx*ny*nz gradient (unnormalised) */
+} kami_vbd_sdf_desc;
+
+/* Everything StableCosseratRodsSolver::BuildYarnBallHair and JsonParams
+ * (StableCosseratRodsSolver.h:41-112, .cpp:112-212) hand to YarnBall::Sim. */
+typedef struct kami_vbd_desc {
+    int32_t num_strands;
+    const int32_t* strand_begin; /* host, num_strands + 1 CSR offsets; every strand >= 2 vertices */
+    const float* positions;      /* host, 3 * V rest/initial positions [m] */
+    const float* velocities;     /* host, 3 * V initial velocities [m/s], or NULL for zero */
+
+    float radius;  /* MetaData::radius [m] */
+    float density; /* [kg/m^3], Sim::configure(density) */
+
+    int32_t stiffness_mode;        /* kami_stiffness_mode */
+    float young;                   /* YoungsModule [GPa], used when strand_young is NULL */
+    float deviation;               /* StiffnessDeviationCoeff, used when strand_deviation is NULL */
+    const float* strand_young;     /* host, optional per-strand E [GPa] */
+    const float* strand_deviation; /* host, optional per-strand bend/twist deviation (scales |qRest|) */
+    float k_stretch;               /* StretchK (KAMI_STIFFNESS_K) */
+    float k_bend;                  /* BendK (KAMI_STIFFNESS_K) */
+
+    float gravity[3];                /* MetaData::gravity [m/s^2] */
+    float damping;                   /* MetaData::damping (reference default 1e-6) */
+    float velocity_decay;            /* VelocityDecay */
+    float acceleration_ratio;        /* MetaData::accelerationRatio (1) */
+    float external_force_multiplier; /* ExternalForceMultiplier */
+    float wind_peak, wind_y_freq, wind_z_freq, wind_time_freq, wind_sharpness; /* Wind* (iteration.cu:19-29) */
+
+    int32_t num_itr;   /* NumItr: VBD iterations per substep */
+    float max_h;       /* Sim::maxH: substeps = ceil(dt / max_h) (step.cpp:42); reference fixes 4e-4 */
+    int32_t schedule;  /* kami_schedule */
+    int32_t form;      /* kami_form */
+    int32_t pin_roots; /* 1: invMass = 0 at each strand root (StableCosseratRodsSolver.cpp:203-205) */
+    int32_t device;    /* CUDA device ordinal; -1 = current device */
+
+    const kami_vbd_sdf_desc* sdf; /* NULL: no body collision (EnableSDF false) */
+} kami_vbd_desc;
+
+typedef struct kami_vbd_solver* kami_vbd_handle;
+
+/* Fills d with the reference's defaults (JsonParams(), StableCosseratRodsSolver.h:86-111, with
+ * WindPeak 0 and max_h 4e-4) and zero/NULL geometry.  Replaces: JsonParams::JsonParams. */
+kami_status kami_vbd_desc_init(kami_vbd_desc* d);
+
+/* Builds the solver: flags, rest lengths, masses, orientations, rest Darboux quaternions and
+ * stiffness, then uploads the state.
+ * Replaces: YarnBall::createFromCurves (reader.cpp:16-50) + Sim::Sim (YBSimulator.cu:81-127) +
+ * Sim::configure (YBSimulator.cu:161-274) + setYoung/setKStretch/setKBend (:276-320) + root
+ * pinning (StableCosseratRodsSolver.cpp:203-209) + SDFBodyCollisionSolver::Construct (:11-21). */
+kami_status kami_vbd_create(const kami_vbd_desc* desc, kami_vbd_handle* out);
+
+/* Releases every device and host resource of the handle.  Replaces: Sim::~Sim (YBSimulator.cu:129-157). */
+kami_status kami_vbd_destroy(kami_vbd_handle h);
+
+/* Number of vertices / strands at the boundary, and the device-side tile shape (slots per lane). */
+kami_status kami_vbd_get_sizes(kami_vbd_handle h, int64_t* num_vertices, int32_t* num_strands, int32_t* slots_per_lane);
+
+/* Positions and velocities (3*V floats each, either may be NULL to leave it unchanged).
+ * Replaces: StableCosseratRodsSolver::UploadHair -> Sim::uploadPosAndVel (.cpp:238-256,
+ * YBSimulator.cu:375-380).  Last velocities and orientations are left untouched, as there. */
+kami_status kami_vbd_set_positions_velocities(kami_vbd_handle h, const float* xyz, const float* vxyz, int32_t memory);
+
+/* Replaces: StableCosseratRodsSolver::DownloadHair -> Sim::downloadPosAndVel (.cpp:258-277,
+ * YBSimulator.cu:382-386).  Synchronises the solver's stream and reports KAMI_ERR_NONFINITE if the
+ * device status word was raised since the last check. */
+kami_status kami_vbd_get_positions_velocities(kami_vbd_handle h, float* xyz, float* vxyz, int32_t memory);
+
+/* Segment orientations (4*V floats, x y z w per vertex; the tip copies its previous segment).
+ * Replaces: the qs part of Sim::download (YBSimulator.cu:355-360). */
+kami_status kami_vbd_get_orientations(kami_vbd_handle h, float* xyzw, int32_t memory);
+kami_status kami_vbd_set_orientations(kami_vbd_handle h, const float* xyzw, int32_t memory);
+
+/* Rest Darboux quaternions scaled by the bend/twist stiffness (4*V floats), d_qRests of
+ * YBSimulator.cu:256 after setYoung.  set_ lets a caller change bend/twist stiffness per vertex. */
+kami_status kami_vbd_get_rest_darboux(kami_vbd_handle h, float* xyzw, int32_t memory);
+kami_status kami_vbd_set_rest_darboux(kami_vbd_handle h, const float* xyzw, int32_t memory);
+
+/* Body transform used by the SDF pass: rotation quaternion (x, y, z, w) and translation, as
+ * SDFSimulationParams.rotation / translate (cudaSDFCollision.cuh:43-44, set in
+ * SDFBodyCollisionSolver::SendSimParamsToCuda, .cpp:308-325). */
+kami_status kami_vbd_set_body_transform(kami_vbd_handle h, const float rotation_xyzw[4], const float translate[3]);
+
+/* One KamiSimulator internal step: Sim::advance(dt) (step.cpp:38-62) -- ceil(dt/max_h) substeps of
+ * predict, num_itr x (position sweep, orientation sweep), velocity update -- followed by the SDF
+ * body-collision pass that StableCosseratRodsSolver::SolveNextStep runs after it (.cpp:216-234),
+ * with no host round trip.  Asynchronous on `stream` (a cudaStream_t; NULL = the handle's stream). */
+kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream);
+
+/* Waits for the handle's work and checks the device status word.  Replaces: Sim::checkErrors
+ * (YBSimulator.cu:388-414). */
+kami_status kami_vbd_synchronize(kami_vbd_handle h);
+
+/* Full dynamic state snapshot (positions, velocities, last velocities, orientations and the
+ * h / lastH / time clock) for checkpoint/resume; the reference saves none of these. */
+kami_status kami_vbd_state_size(kami_vbd_handle h, size_t* bytes);
+kami_status kami_vbd_get_state(kami_vbd_handle h, void* dst, size_t bytes, int32_t memory);
+kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes, int32_t memory);
+
+/* Description of the last error on the calling thread ("" if none). */
+const char* kami_vbd_last_error_string(void);
+
+/* Library version string. */
+const char* kami_vbd_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* KAMI_VBD_H_ */

@@ -1,0 +1,600 @@
+// kami_vbd.cpp -- implementation of the C ABI in include/kami_vbd.h.
+#include "kami_vbd.h"
+
+#include <cuda_runtime.h>
+
+#include <cmath>
+#include <cstdarg>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "vbd_host.h"
+#include "vbd_kernels.h"
+
+using namespace kami;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+kami_status fail(kami_status st, const char* fmt, ...) {
+    char buf[1024];
+    va_list ap;
+    va_start(ap, fmt);
+    vsnprintf(buf, sizeof(buf), fmt, ap);
+    va_end(ap);
+    g_last_error = buf;
+    return st;
+}
+
+kami_status cuda_fail(cudaError_t e, const char* what) {
+    if (e == cudaErrorMemoryAllocation) return fail(KAMI_ERR_OUT_OF_MEMORY, "%s: %s", what, cudaGetErrorString(e));
+    return fail(KAMI_ERR_CUDA, "%s: %s", what, cudaGetErrorString(e));
+}
+
+#define KAMI_CUDA(call, what)                          \
+    do {                                               \
+        cudaError_t e_ = (call);                       \
+        if (e_ != cudaSuccess) return cuda_fail(e_, what); \
+    } while (0)
+
+}  // namespace
+
+struct kami_vbd_solver {
+    int device = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev_a = nullptr, ev_b = nullptr;
+
+    int64_t nv = 0;
+    int32_t ns = 0;
+    std::vector<int32_t> strand_begin;
+    TileLayout layout;
+    int64_t* d_slot_of = nullptr;
+
+    // device state (tile slots)
+    float4 *d_xm = nullptr, *d_vel = nullptr, *d_vlast = nullptr, *d_q = nullptr, *d_qr = nullptr, *d_prm = nullptr;
+    // sweep-form scratch
+    float4 *d_y = nullptr, *d_dx = nullptr, *d_dx2 = nullptr, *d_q2 = nullptr;
+    StepParams* d_step = nullptr;
+    StepParams h_step{};
+    // boundary staging (4 floats per boundary vertex)
+    float* d_stage = nullptr;
+    int* d_status = nullptr;
+    float4* d_sdf = nullptr;
+    SdfParams sdf{};
+
+    PhysParams pp{};
+    float h = 0.f, last_h = 0.f, time = 0.f, max_h = 4e-4f;
+    float rot[4] = {0.f, 0.f, 0.f, 1.f};
+    float tr[3] = {0.f, 0.f, 0.f};
+    int schedule = KAMI_SCHEDULE_COLOUR2;
+    int form = KAMI_FORM_FUSED;
+    int warps_per_block = 4;
+
+    cudaGraphExec_t graph = nullptr;
+    int graph_substeps = -1;
+
+    DeviceState dstate() const {
+        DeviceState s;
+        s.xm = d_xm;
+        s.vel = d_vel;
+        s.vlast = d_vlast;
+        s.q = d_q;
+        s.qr = d_qr;
+        s.prm = d_prm;
+        s.num_tiles = layout.num_tiles;
+        s.status = d_status;
+        return s;
+    }
+};
+
+namespace {
+
+void release(kami_vbd_solver* h) {
+    if (!h) return;
+    cudaSetDevice(h->device);
+    if (h->stream) cudaStreamSynchronize(h->stream);
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    void* ptrs[] = {h->d_slot_of, h->d_xm, h->d_vel, h->d_vlast, h->d_q,      h->d_qr,     h->d_prm,
+                    h->d_y,       h->d_dx, h->d_dx2, h->d_q2,    h->d_step,   h->d_stage,  h->d_status,
+                    h->d_sdf};
+    for (void* p : ptrs)
+        if (p) cudaFree(p);
+    if (h->ev_a) cudaEventDestroy(h->ev_a);
+    if (h->ev_b) cudaEventDestroy(h->ev_b);
+    if (h->stream) cudaStreamDestroy(h->stream);
+    delete h;
+}
+
+template <typename T>
+cudaError_t dalloc(T** p, size_t count) {
+    return cudaMalloc((void**)p, sizeof(T) * (count > 0 ? count : 1));
+}
+
+// Runs `body` on the caller's stream if one is given, ordered after and before the handle's own
+// stream so every other entry point (which uses the handle's stream) stays ordered with it.
+template <typename F>
+kami_status on_stream(kami_vbd_solver* h, void* user_stream, F body) {
+    cudaStream_t us = (cudaStream_t)user_stream;
+    if (!us || us == h->stream) return body(h->stream);
+    KAMI_CUDA(cudaEventRecord(h->ev_a, h->stream), "cudaEventRecord");
+    KAMI_CUDA(cudaStreamWaitEvent(us, h->ev_a, 0), "cudaStreamWaitEvent");
+    kami_status st = body(us);
+    if (st != KAMI_OK) return st;
+    KAMI_CUDA(cudaEventRecord(h->ev_b, us), "cudaEventRecord");
+    KAMI_CUDA(cudaStreamWaitEvent(h->stream, h->ev_b, 0), "cudaStreamWaitEvent");
+    return KAMI_OK;
+}
+
+kami_status check_status_word(kami_vbd_solver* h) {
+    int word = 0;
+    KAMI_CUDA(cudaMemcpyAsync(&word, h->d_status, sizeof(int), cudaMemcpyDeviceToHost, h->stream), "status read");
+    KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    if (word != 0) {
+        KAMI_CUDA(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream), "status reset");
+        if (word & STATUS_NONFINITE)
+            return fail(KAMI_ERR_NONFINITE, "non-finite position, velocity or orientation produced by a step");
+        return fail(KAMI_ERR_CUDA, "device status word 0x%x", word);
+    }
+    return KAMI_OK;
+}
+
+// Copies 3*nv (or 4*nv) boundary floats into the staging buffer, from host or device memory.
+kami_status stage_in(kami_vbd_solver* h, const float* src, int comps, int32_t memory) {
+    size_t bytes = sizeof(float) * comps * (size_t)h->nv;
+    cudaMemcpyKind kind = memory == KAMI_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    KAMI_CUDA(cudaMemcpyAsync(h->d_stage, src, bytes, kind, h->stream), "copy in");
+    return KAMI_OK;
+}
+kami_status stage_out(kami_vbd_solver* h, float* dst, int comps, int32_t memory) {
+    size_t bytes = sizeof(float) * comps * (size_t)h->nv;
+    cudaMemcpyKind kind = memory == KAMI_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    KAMI_CUDA(cudaMemcpyAsync(dst, h->d_stage, bytes, kind, h->stream), "copy out");
+    return KAMI_OK;
+}
+
+kami_status valid_handle(kami_vbd_solver* h) {
+    if (!h) return fail(KAMI_ERR_INVALID_ARGUMENT, "null handle");
+    KAMI_CUDA(cudaSetDevice(h->device), "cudaSetDevice");
+    return KAMI_OK;
+}
+
+#define KAMI_TRY(expr)                      \
+    do {                                    \
+        kami_status s_ = (expr);            \
+        if (s_ != KAMI_OK) return s_;       \
+    } while (0)
+
+kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
+    if (h->graph && h->graph_substeps == substeps) return KAMI_OK;
+    if (h->graph) {
+        cudaGraphExecDestroy(h->graph);
+        h->graph = nullptr;
+    }
+    const DeviceState st = h->dstate();
+    const bool jac = h->schedule == KAMI_SCHEDULE_JACOBI;
+    const int C = h->layout.C;
+    cudaStream_t s = h->stream;
+    KAMI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+    cudaError_t err = cudaSuccess;
+    for (int sub = 0; sub < substeps && err == cudaSuccess; sub++) {
+        err = launch_sweep_predict(st, h->d_y, h->d_dx, h->d_step, h->pp, h->layout.num_slots, s);
+        float4* dx_cur = h->d_dx;
+        float4* dx_alt = h->d_dx2;
+        float4* q_cur = h->d_q;
+        float4* q_alt = h->d_q2;
+        for (int it = 0; it < h->pp.num_itr && err == cudaSuccess; it++) {
+            if (jac) {
+                err = launch_sweep_position(st, h->d_y, q_cur, dx_cur, dx_alt, h->d_step, h->pp, C, 0, true, s);
+                std::swap(dx_cur, dx_alt);
+                if (err == cudaSuccess) err = launch_sweep_orientation(st, dx_cur, q_cur, q_alt, C, 0, true, s);
+                std::swap(q_cur, q_alt);
+            } else {
+                for (int c = 0; c < 2 && err == cudaSuccess; c++)
+                    err = launch_sweep_position(st, h->d_y, q_cur, dx_cur, dx_cur, h->d_step, h->pp, C, c, false, s);
+                for (int c = 0; c < 2 && err == cudaSuccess; c++)
+                    err = launch_sweep_orientation(st, dx_cur, q_cur, q_cur, C, c, false, s);
+            }
+        }
+        if (err == cudaSuccess && q_cur != h->d_q)
+            err = cudaMemcpyAsync(h->d_q, q_cur, sizeof(float4) * h->layout.num_slots, cudaMemcpyDeviceToDevice, s);
+        if (err == cudaSuccess)
+            err = launch_sweep_finish(st, dx_cur, h->d_step, h->pp, h->sdf, sub == substeps - 1, h->layout.num_slots, s);
+    }
+    cudaGraph_t g = nullptr;
+    cudaError_t e2 = cudaStreamEndCapture(s, &g);
+    if (err != cudaSuccess) {
+        if (g) cudaGraphDestroy(g);
+        return cuda_fail(err, "capturing the sweep graph");
+    }
+    if (e2 != cudaSuccess) return cuda_fail(e2, "cudaStreamEndCapture");
+    cudaError_t e3 = cudaGraphInstantiate(&h->graph, g, 0);
+    cudaGraphDestroy(g);
+    if (e3 != cudaSuccess) return cuda_fail(e3, "cudaGraphInstantiate");
+    h->graph_substeps = substeps;
+    return KAMI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+kami_status kami_vbd_desc_init(kami_vbd_desc* d) {
+    if (!d) return fail(KAMI_ERR_INVALID_ARGUMENT, "null descriptor");
+    std::memset(d, 0, sizeof(*d));
+    d->radius = 4e-5f;
+    d->density = 1300.f;
+    d->stiffness_mode = KAMI_STIFFNESS_YOUNG;
+    d->young = 5.f;
+    d->deviation = 1.f;
+    d->k_stretch = 3e3f;
+    d->k_bend = 6e-4f;
+    d->gravity[0] = 0.f;
+    d->gravity[1] = -9.8f;
+    d->gravity[2] = 0.f;
+    d->damping = 1e-6f;
+    d->velocity_decay = 0.05f;
+    d->acceleration_ratio = 1.f;
+    d->external_force_multiplier = 1.f;
+    d->wind_peak = 0.f;
+    d->wind_y_freq = 1.f;
+    d->wind_z_freq = 0.7f;
+    d->wind_time_freq = 0.4f;
+    d->wind_sharpness = 3.f;
+    d->num_itr = 8;
+    d->max_h = 4e-4f;
+    d->schedule = KAMI_SCHEDULE_COLOUR2;
+    d->form = KAMI_FORM_AUTO;
+    d->pin_roots = 1;
+    d->device = -1;
+    d->sdf = nullptr;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_create(const kami_vbd_desc* d, kami_vbd_handle* out) {
+    if (!d || !out) return fail(KAMI_ERR_INVALID_ARGUMENT, "null descriptor or output handle");
+    *out = nullptr;
+    if (d->num_strands <= 0 || !d->strand_begin || !d->positions)
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "need num_strands > 0, strand_begin and positions");
+    if (d->strand_begin[0] != 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "strand_begin[0] must be 0");
+    for (int32_t s = 0; s < d->num_strands; s++)
+        if (d->strand_begin[s + 1] - d->strand_begin[s] < 2)
+            return fail(KAMI_ERR_GEOMETRY, "strand %d has fewer than 2 vertices (dangling segment)", s);
+    if (d->num_itr < 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "num_itr must be >= 0");
+    if (!(d->max_h > 0.f)) return fail(KAMI_ERR_INVALID_ARGUMENT, "max_h must be > 0");
+    if (!(d->radius > 0.f) || !(d->density > 0.f)) return fail(KAMI_ERR_INVALID_ARGUMENT, "radius and density must be > 0");
+    if (d->schedule != KAMI_SCHEDULE_COLOUR2 && d->schedule != KAMI_SCHEDULE_JACOBI)
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "unknown schedule %d", d->schedule);
+    if (d->form < KAMI_FORM_AUTO || d->form > KAMI_FORM_FUSED) return fail(KAMI_ERR_INVALID_ARGUMENT, "unknown form %d", d->form);
+    if (d->stiffness_mode != KAMI_STIFFNESS_YOUNG && d->stiffness_mode != KAMI_STIFFNESS_K)
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "unknown stiffness mode %d", d->stiffness_mode);
+    if (d->sdf) {
+        const kami_vbd_sdf_desc* s = d->sdf;
+        if (s->dims[0] <= 0 || s->dims[1] <= 0 || s->dims[2] <= 0 || !s->phi || !s->grad)
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "SDF needs positive dims and phi/grad arrays");
+        for (int a = 0; a < 3; a++)
+            if (!(s->grid_max[a] > s->grid_min[a])) return fail(KAMI_ERR_INVALID_ARGUMENT, "SDF grid_max must exceed grid_min");
+    }
+
+    kami_vbd_solver* h = new (std::nothrow) kami_vbd_solver();
+    if (!h) return fail(KAMI_ERR_OUT_OF_MEMORY, "host allocation failed");
+    auto bail = [&](kami_status st) {
+        release(h);
+        return st;
+    };
+    h->ns = d->num_strands;
+    h->strand_begin.assign(d->strand_begin, d->strand_begin + d->num_strands + 1);
+    h->nv = h->strand_begin.back();
+
+    // per-vertex material in boundary order
+    MaterialDesc md;
+    md.radius = d->radius;
+    md.density = d->density;
+    md.stiffness_mode = d->stiffness_mode;
+    md.strand_young = d->strand_young;
+    md.strand_dev = d->strand_deviation;
+    md.young = d->young;
+    md.deviation = d->deviation;
+    md.k_stretch = d->k_stretch;
+    md.k_bend = d->k_bend;
+    md.pin_roots = d->pin_roots != 0;
+    Material m;
+    std::string err;
+    int rc = build_material(h->strand_begin.data(), h->ns, d->positions, md, m, err);
+    if (rc != 0) return bail(fail(rc == 1 ? KAMI_ERR_INVALID_ARGUMENT : KAMI_ERR_GEOMETRY, "%s", err.c_str()));
+
+    // tile layout and form
+    int C = slots_per_lane_for(h->strand_begin.data(), h->ns);
+    int form = d->form;
+    if (form == KAMI_FORM_AUTO) form = fused_supported(C) ? KAMI_FORM_FUSED : KAMI_FORM_SWEEP;
+    if (form == KAMI_FORM_FUSED && !fused_supported(C))
+        return bail(fail(KAMI_ERR_UNSUPPORTED, "fused form supports strands of up to 128 vertices"));
+    h->form = form;
+    if (!pack_tiles(h->strand_begin.data(), h->ns, C, h->layout, err))
+        return bail(fail(KAMI_ERR_UNSUPPORTED, "%s", err.c_str()));
+    const int64_t S = h->layout.num_slots;
+
+    // everything above is host-only validation; device work starts here
+    if (d->device >= 0) {
+        cudaError_t e = cudaSetDevice(d->device);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "cudaSetDevice"));
+        h->device = d->device;
+    } else {
+        cudaError_t e = cudaGetDevice(&h->device);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "cudaGetDevice"));
+    }
+
+    // host images of the device arrays (padding slots: lRest 1, no flags, zero mass)
+    std::vector<float4> xm(S, make_float4(0.f, 0.f, 0.f, 0.f)), vel(S, make_float4(0.f, 0.f, 0.f, 0.f)),
+        vlast(S, make_float4(0.f, 0.f, 0.f, 0.f)), q(S, make_float4(0.f, 0.f, 0.f, 1.f)),
+        qr(S, make_float4(0.f, 0.f, 0.f, 1.f)), prm(S, make_float4(1.f, 0.f, 0.f, 0.f));
+    for (int64_t i = 0; i < h->nv; i++) {
+        const int64_t g = h->layout.slot_of[i];
+        xm[g] = make_float4(d->positions[3 * i], d->positions[3 * i + 1], d->positions[3 * i + 2], m.inv_mass[i]);
+        if (d->velocities) vel[g] = make_float4(d->velocities[3 * i], d->velocities[3 * i + 1], d->velocities[3 * i + 2], 0.f);
+        q[g] = make_float4(m.q[4 * i], m.q[4 * i + 1], m.q[4 * i + 2], m.q[4 * i + 3]);
+        qr[g] = make_float4(m.q_rest[4 * i], m.q_rest[4 * i + 1], m.q_rest[4 * i + 2], m.q_rest[4 * i + 3]);
+        uint32_t fl = m.flags[i];
+        float flf;
+        std::memcpy(&flf, &fl, 4);
+        prm[g] = make_float4(m.l_rest[i], m.k_stretch[i], 0.f, flf);
+    }
+
+    // physical parameters and clock (meta.h starts at maxH, YBSimulator.cu:85)
+    h->pp.gx = d->gravity[0];
+    h->pp.gy = d->gravity[1];
+    h->pp.gz = d->gravity[2];
+    h->pp.damping = d->damping;
+    h->pp.velocity_decay = d->velocity_decay;
+    h->pp.accel_ratio = d->acceleration_ratio;
+    h->pp.ext_mult = d->external_force_multiplier;
+    h->pp.wind_peak = d->wind_peak;
+    h->pp.wind_yf = d->wind_y_freq;
+    h->pp.wind_zf = d->wind_z_freq;
+    h->pp.wind_tf = d->wind_time_freq;
+    h->pp.wind_sharp = d->wind_sharpness;
+    h->pp.num_itr = d->num_itr;
+    h->max_h = d->max_h;
+    h->h = d->max_h;
+    h->schedule = d->schedule;
+
+    // a blocking stream, so work on the legacy default stream (e.g. a torch producer) orders with ours
+    cudaError_t e = cudaStreamCreate(&h->stream);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_a, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = cudaEventCreateWithFlags(&h->ev_b, cudaEventDisableTiming);
+    if (e == cudaSuccess) e = dalloc(&h->d_slot_of, h->nv);
+    if (e == cudaSuccess) e = dalloc(&h->d_xm, S);
+    if (e == cudaSuccess) e = dalloc(&h->d_vel, S);
+    if (e == cudaSuccess) e = dalloc(&h->d_vlast, S);
+    if (e == cudaSuccess) e = dalloc(&h->d_q, S);
+    if (e == cudaSuccess) e = dalloc(&h->d_qr, S);
+    if (e == cudaSuccess) e = dalloc(&h->d_prm, S);
+    if (e == cudaSuccess) e = dalloc(&h->d_stage, 4 * h->nv);
+    if (e == cudaSuccess) e = dalloc(&h->d_status, 1);
+    if (e == cudaSuccess && form == KAMI_FORM_SWEEP) {
+        e = dalloc(&h->d_y, S);
+        if (e == cudaSuccess) e = dalloc(&h->d_dx, S);
+        if (e == cudaSuccess) e = dalloc(&h->d_step, 1);
+        if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_JACOBI) e = dalloc(&h->d_dx2, S);
+        if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_JACOBI) e = dalloc(&h->d_q2, S);
+    }
+    if (e != cudaSuccess) return bail(cuda_fail(e, "allocating solver state"));
+    const size_t b4 = sizeof(float4) * S;
+    e = cudaMemcpy(h->d_slot_of, h->layout.slot_of.data(), sizeof(int64_t) * h->nv, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_xm, xm.data(), b4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_vel, vel.data(), b4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_vlast, vlast.data(), b4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_q, q.data(), b4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_qr, qr.data(), b4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(h->d_prm, prm.data(), b4, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(h->d_status, 0, sizeof(int));
+    if (e != cudaSuccess) return bail(cuda_fail(e, "uploading solver state"));
+
+    if (d->sdf) {
+        const kami_vbd_sdf_desc* s = d->sdf;
+        const int64_t n = (int64_t)s->dims[0] * s->dims[1] * s->dims[2];
+        std::vector<float4> grid(n);
+        for (int64_t i = 0; i < n; i++) grid[i] = make_float4(s->grad[3 * i], s->grad[3 * i + 1], s->grad[3 * i + 2], s->phi[i]);
+        e = dalloc(&h->d_sdf, n);
+        if (e == cudaSuccess) e = cudaMemcpy(h->d_sdf, grid.data(), sizeof(float4) * n, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) return bail(cuda_fail(e, "uploading the SDF grid"));
+        // grid spacing as SDFBodyCollisionSolver::InitParams computes it (SDFBodyCollisionSolver.cpp:142-159)
+        SdfParams& sp = h->sdf;
+        sp.grid = h->d_sdf;
+        sp.nx = s->dims[0];
+        sp.ny = s->dims[1];
+        sp.nz = s->dims[2];
+        sp.min_x = s->grid_min[0];
+        sp.min_y = s->grid_min[1];
+        sp.min_z = s->grid_min[2];
+        sp.ds_x = (s->grid_max[0] - s->grid_min[0]) / (1.f * sp.nx);
+        sp.ds_y = (s->grid_max[1] - s->grid_min[1]) / (1.f * sp.ny);
+        sp.ds_z = (s->grid_max[2] - s->grid_min[2]) / (1.f * sp.nz);
+        sp.inv_x = 1.f / sp.ds_x;
+        sp.inv_y = 1.f / sp.ds_y;
+        sp.inv_z = 1.f / sp.ds_z;
+        sp.thresh = s->threshold;
+    }
+    *out = h;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_destroy(kami_vbd_handle h) {
+    if (!h) return KAMI_OK;
+    release(h);
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_get_sizes(kami_vbd_handle h, int64_t* num_vertices, int32_t* num_strands, int32_t* slots_per_lane) {
+    if (!h) return fail(KAMI_ERR_INVALID_ARGUMENT, "null handle");
+    if (num_vertices) *num_vertices = h->nv;
+    if (num_strands) *num_strands = h->ns;
+    if (slots_per_lane) *slots_per_lane = h->layout.C;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_set_positions_velocities(kami_vbd_handle h, const float* xyz, const float* vxyz, int32_t memory) {
+    KAMI_TRY(valid_handle(h));
+    if (memory != KAMI_MEMORY_HOST && memory != KAMI_MEMORY_DEVICE) return fail(KAMI_ERR_INVALID_ARGUMENT, "bad memory kind");
+    if (xyz) {
+        KAMI_TRY(stage_in(h, xyz, 3, memory));
+        KAMI_CUDA(launch_scatter3(h->d_stage, h->d_xm, h->d_slot_of, h->nv, h->stream), "scatter positions");
+    }
+    if (vxyz) {
+        KAMI_TRY(stage_in(h, vxyz, 3, memory));
+        KAMI_CUDA(launch_scatter3(h->d_stage, h->d_vel, h->d_slot_of, h->nv, h->stream), "scatter velocities");
+    }
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_get_positions_velocities(kami_vbd_handle h, float* xyz, float* vxyz, int32_t memory) {
+    KAMI_TRY(valid_handle(h));
+    if (memory != KAMI_MEMORY_HOST && memory != KAMI_MEMORY_DEVICE) return fail(KAMI_ERR_INVALID_ARGUMENT, "bad memory kind");
+    if (xyz) {
+        KAMI_CUDA(launch_gather3(h->d_xm, h->d_stage, h->d_slot_of, h->nv, h->stream), "gather positions");
+        KAMI_TRY(stage_out(h, xyz, 3, memory));
+    }
+    if (vxyz) {
+        KAMI_CUDA(launch_gather3(h->d_vel, h->d_stage, h->d_slot_of, h->nv, h->stream), "gather velocities");
+        KAMI_TRY(stage_out(h, vxyz, 3, memory));
+    }
+    return check_status_word(h);
+}
+
+static kami_status get4(kami_vbd_solver* h, const float4* src, float* dst, int32_t memory) {
+    KAMI_TRY(valid_handle(h));
+    if (!dst) return fail(KAMI_ERR_INVALID_ARGUMENT, "null output");
+    KAMI_CUDA(launch_gather4(src, (float4*)h->d_stage, h->d_slot_of, h->nv, h->stream), "gather");
+    KAMI_TRY(stage_out(h, dst, 4, memory));
+    KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    return KAMI_OK;
+}
+static kami_status set4(kami_vbd_solver* h, float4* dst, const float* src, int32_t memory) {
+    KAMI_TRY(valid_handle(h));
+    if (!src) return fail(KAMI_ERR_INVALID_ARGUMENT, "null input");
+    KAMI_TRY(stage_in(h, src, 4, memory));
+    KAMI_CUDA(launch_scatter4((const float4*)h->d_stage, dst, h->d_slot_of, h->nv, h->stream), "scatter");
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_get_orientations(kami_vbd_handle h, float* xyzw, int32_t memory) { return get4(h, h ? h->d_q : nullptr, xyzw, memory); }
+kami_status kami_vbd_set_orientations(kami_vbd_handle h, const float* xyzw, int32_t memory) { return set4(h, h ? h->d_q : nullptr, xyzw, memory); }
+kami_status kami_vbd_get_rest_darboux(kami_vbd_handle h, float* xyzw, int32_t memory) { return get4(h, h ? h->d_qr : nullptr, xyzw, memory); }
+kami_status kami_vbd_set_rest_darboux(kami_vbd_handle h, const float* xyzw, int32_t memory) { return set4(h, h ? h->d_qr : nullptr, xyzw, memory); }
+
+kami_status kami_vbd_set_body_transform(kami_vbd_handle h, const float rotation_xyzw[4], const float translate[3]) {
+    if (!h) return fail(KAMI_ERR_INVALID_ARGUMENT, "null handle");
+    if (rotation_xyzw)
+        for (int i = 0; i < 4; i++) h->rot[i] = rotation_xyzw[i];
+    if (translate)
+        for (int i = 0; i < 3; i++) h->tr[i] = translate[i];
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
+    KAMI_TRY(valid_handle(h));
+    if (!(dt > 0.f)) return KAMI_OK;  // Sim::advance returns for h <= 0 (step.cpp:113)
+    if (!std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
+    const int steps = std::max(1, (int)std::ceil(dt / h->max_h));
+    h->last_h = h->h;
+    h->h = dt / (float)steps;
+    StepParams sp;
+    sp.h = h->h;
+    sp.last_h = h->last_h;
+    sp.time = h->time;
+    sp.substeps = steps;
+    sp.rot_x = h->rot[0];
+    sp.rot_y = h->rot[1];
+    sp.rot_z = h->rot[2];
+    sp.rot_w = h->rot[3];
+    sp.tr_x = h->tr[0];
+    sp.tr_y = h->tr[1];
+    sp.tr_z = h->tr[2];
+    kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
+        if (h->form == KAMI_FORM_FUSED) {
+            KAMI_CUDA(launch_fused_step(h->dstate(), h->pp, sp, h->sdf, h->layout.C, h->schedule == KAMI_SCHEDULE_JACOBI,
+                                        h->warps_per_block, s),
+                      "fused step launch");
+        } else {
+            KAMI_TRY(build_sweep_graph(h, steps));
+            h->h_step = sp;
+            KAMI_CUDA(cudaMemcpyAsync(h->d_step, &h->h_step, sizeof(StepParams), cudaMemcpyHostToDevice, s), "step params");
+            KAMI_CUDA(cudaGraphLaunch(h->graph, s), "cudaGraphLaunch");
+        }
+        return KAMI_OK;
+    });
+    if (st != KAMI_OK) return st;
+    h->time += dt;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_synchronize(kami_vbd_handle h) {
+    KAMI_TRY(valid_handle(h));
+    return check_status_word(h);
+}
+
+kami_status kami_vbd_state_size(kami_vbd_handle h, size_t* bytes) {
+    if (!h || !bytes) return fail(KAMI_ERR_INVALID_ARGUMENT, "null argument");
+    *bytes = sizeof(float) * 13 * (size_t)h->nv + 4 * sizeof(float);
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_get_state(kami_vbd_handle h, void* dst, size_t bytes, int32_t memory) {
+    KAMI_TRY(valid_handle(h));
+    size_t need = 0;
+    kami_vbd_state_size(h, &need);
+    if (!dst || bytes < need) return fail(KAMI_ERR_INVALID_ARGUMENT, "state buffer must hold %zu bytes", need);
+    float* f = (float*)dst;
+    const int64_t nv = h->nv;
+    cudaMemcpyKind kind = memory == KAMI_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyDeviceToHost;
+    const float4* srcs[3] = {h->d_xm, h->d_vel, h->d_vlast};
+    for (int a = 0; a < 3; a++) {
+        KAMI_CUDA(launch_gather3(srcs[a], h->d_stage, h->d_slot_of, nv, h->stream), "gather state");
+        KAMI_CUDA(cudaMemcpyAsync(f + 3 * nv * a, h->d_stage, sizeof(float) * 3 * nv, kind, h->stream), "state copy");
+    }
+    KAMI_CUDA(launch_gather4(h->d_q, (float4*)h->d_stage, h->d_slot_of, nv, h->stream), "gather state");
+    KAMI_CUDA(cudaMemcpyAsync(f + 9 * nv, h->d_stage, sizeof(float) * 4 * nv, kind, h->stream), "state copy");
+    KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    const float clk[4] = {h->h, h->last_h, h->time, 0.f};
+    if (memory == KAMI_MEMORY_DEVICE)
+        KAMI_CUDA(cudaMemcpy(f + 13 * nv, clk, sizeof(clk), cudaMemcpyHostToDevice), "state clock");
+    else
+        std::memcpy(f + 13 * nv, clk, sizeof(clk));
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes, int32_t memory) {
+    KAMI_TRY(valid_handle(h));
+    size_t need = 0;
+    kami_vbd_state_size(h, &need);
+    if (!src || bytes < need) return fail(KAMI_ERR_INVALID_ARGUMENT, "state buffer must hold %zu bytes", need);
+    const float* f = (const float*)src;
+    const int64_t nv = h->nv;
+    cudaMemcpyKind kind = memory == KAMI_MEMORY_DEVICE ? cudaMemcpyDeviceToDevice : cudaMemcpyHostToDevice;
+    float4* dsts[3] = {h->d_xm, h->d_vel, h->d_vlast};
+    for (int a = 0; a < 3; a++) {
+        KAMI_CUDA(cudaMemcpyAsync(h->d_stage, f + 3 * nv * a, sizeof(float) * 3 * nv, kind, h->stream), "state copy");
+        KAMI_CUDA(launch_scatter3(h->d_stage, dsts[a], h->d_slot_of, nv, h->stream), "scatter state");
+    }
+    KAMI_CUDA(cudaMemcpyAsync(h->d_stage, f + 9 * nv, sizeof(float) * 4 * nv, kind, h->stream), "state copy");
+    KAMI_CUDA(launch_scatter4((const float4*)h->d_stage, h->d_q, h->d_slot_of, nv, h->stream), "scatter state");
+    KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    float clk[4];
+    if (memory == KAMI_MEMORY_DEVICE)
+        KAMI_CUDA(cudaMemcpy(clk, f + 13 * nv, sizeof(clk), cudaMemcpyDeviceToHost), "state clock");
+    else
+        std::memcpy(clk, f + 13 * nv, sizeof(clk));
+    h->h = clk[0];
+    h->last_h = clk[1];
+    h->time = clk[2];
+    return KAMI_OK;
+}
+
+const char* kami_vbd_last_error_string(void) { return g_last_error.c_str(); }
+
+const char* kami_vbd_version(void) { return "kami-vbd-b200 0.1 (sm_100a)"; }
+
+}  // extern "C"

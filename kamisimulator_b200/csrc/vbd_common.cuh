@@ -1,0 +1,124 @@
+// vbd_common.cuh -- device data layout, parameter blocks and small vector/quaternion helpers
+// shared by the solver's kernels.
+//
+// Device layout ("tiles"): the solver's vertices live in tiles of T = 32*C slots, one tile per
+// warp in the fused kernel.  Lane j of a tile owns the C contiguous slots p = j*C .. j*C+C-1 and
+// slot p is stored at index  tile*T + (p % C)*32 + (p / C),  so the warp's access to "its k-th
+// slot" is one fully coalesced 32-element row.  Strands occupy contiguous slot ranges starting
+// at an even slot, never cross a tile, and padding slots carry no flags.  Because every strand
+// starts at an even slot and C is even, the 2-colour class of a slot (its index parity inside
+// the strand) is simply k & 1 (the row parity).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace kami {
+
+// Vertex flags: bits 1..8 are YarnBall::VertexFlags (YarnBall/YarnBall.h:33-39).
+enum : uint32_t {
+    F_HAS_PREV = 1u,
+    F_HAS_NEXT = 2u,
+    F_HAS_NEXT_ORIENTATION = 4u,
+    F_FIX_ORIENTATION = 8u,
+    F_ROOT = 32u,   // first vertex of its strand (skipped by the SDF pass, cudaSDFCollision.cu:241)
+    F_VALID = 64u,  // a real vertex (padding slots have no flags at all)
+};
+
+// Status word bits raised by the kernels.
+enum : int { STATUS_NONFINITE = 1 };
+
+// Per-solver physical constants (MetaData scalars, YarnBall/YarnBall.h:80-123).
+struct PhysParams {
+    float gx, gy, gz;
+    float damping;             // MetaData::damping (divided by h inside the step)
+    float velocity_decay;
+    float accel_ratio;
+    float ext_mult;
+    float wind_peak, wind_yf, wind_zf, wind_tf, wind_sharp;
+    int num_itr;
+};
+
+// Per-call clock: Sim::advance splits dt into `substeps` of h; lastH is the h of the previous
+// advance call and time is MetaData::time before this call (step.cpp:38-62).
+struct StepParams {
+    float h, last_h, time;
+    int substeps;
+    float rot_x, rot_y, rot_z, rot_w;  // body rotation (x, y, z, w)
+    float tr_x, tr_y, tr_z;            // body translation
+};
+
+// Body SDF: (grad.xyz, phi) packed per node, x fastest.
+struct SdfParams {
+    const float4* grid;  // nullptr: no body collision
+    int nx, ny, nz;
+    float min_x, min_y, min_z;
+    float ds_x, ds_y, ds_z;
+    float inv_x, inv_y, inv_z;
+    float thresh;
+};
+
+// Device state arrays, all indexed by tile slot.
+struct DeviceState {
+    float4* xm;        // position xyz, inverse mass
+    float4* vel;       // velocity xyz, 0
+    float4* vlast;     // velocity at the start of the previous step, 0
+    float4* q;         // segment orientation (x, y, z, w)
+    const float4* qr;  // rest Darboux quaternion scaled by bend/twist stiffness
+    const float4* prm; // lRest, kStretch, 0, flags (bit pattern)
+    int64_t num_tiles;
+    int* status;
+};
+
+// ---- small helpers ---------------------------------------------------------------------------
+__host__ __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
+__host__ __device__ __forceinline__ float3 xyz(float4 a) { return make_float3(a.x, a.y, a.z); }
+__host__ __device__ __forceinline__ float3 operator+(float3 a, float3 b) { return f3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__host__ __device__ __forceinline__ float3 operator-(float3 a, float3 b) { return f3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__host__ __device__ __forceinline__ float3 operator*(float s, float3 a) { return f3(s * a.x, s * a.y, s * a.z); }
+__host__ __device__ __forceinline__ float3 operator*(float3 a, float s) { return f3(a.x * s, a.y * s, a.z * s); }
+__host__ __device__ __forceinline__ float dot3(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__host__ __device__ __forceinline__ float3 cross3(float3 a, float3 b) {
+    return f3(a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y);
+}
+__host__ __device__ __forceinline__ float dot4(float4 a, float4 b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+__host__ __device__ __forceinline__ float4 scale4(float s, float4 a) { return make_float4(s * a.x, s * a.y, s * a.z, s * a.w); }
+__host__ __device__ __forceinline__ float4 add4(float4 a, float4 b) { return make_float4(a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w); }
+
+// Hamilton product with the scalar last (Kit::Rotor operator*, Rotor.h:210-212).
+__host__ __device__ __forceinline__ float4 qmul(float4 l, float4 r) {
+    return make_float4(l.w * r.x + r.w * l.x + (l.y * r.z - r.y * l.z), l.w * r.y + r.w * l.y + (l.z * r.x - r.z * l.x),
+                       l.w * r.z + r.w * l.z + (l.x * r.y - r.x * l.y), l.w * r.w - (l.x * r.x + l.y * r.y + l.z * r.z));
+}
+// l * conj(r)
+__host__ __device__ __forceinline__ float4 qmul_conj(float4 l, float4 r) {
+    return qmul(l, make_float4(-r.x, -r.y, -r.z, r.w));
+}
+// Material axis d3 = q e_x q* (Rotor::rotate applied to e_x, Rotor.h:114-123, expanded).
+__host__ __device__ __forceinline__ float3 d3_of(float4 q) {
+    return f3(q.w * q.w + q.x * q.x - q.y * q.y - q.z * q.z, 2.f * (q.x * q.y + q.w * q.z), 2.f * (q.x * q.z - q.w * q.y));
+}
+// Rotor::rotate (Rotor.h:114-123) for a general vector.
+__host__ __device__ __forceinline__ float3 qrotate(float4 r, float3 v) {
+    float3 qv = f3(r.x, r.y, r.z);
+    float3 a = r.w * v + cross3(qv, v);
+    float c = dot3(v, qv);
+    return r.w * a + cross3(qv, a) + c * qv;
+}
+
+__device__ __forceinline__ float3 shfl_up3(float3 v, int d) {
+    return f3(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d), __shfl_up_sync(0xffffffffu, v.z, d));
+}
+__device__ __forceinline__ float3 shfl_down3(float3 v, int d) {
+    return f3(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d),
+              __shfl_down_sync(0xffffffffu, v.z, d));
+}
+__device__ __forceinline__ float4 shfl_up4(float4 v, int d) {
+    return make_float4(__shfl_up_sync(0xffffffffu, v.x, d), __shfl_up_sync(0xffffffffu, v.y, d),
+                       __shfl_up_sync(0xffffffffu, v.z, d), __shfl_up_sync(0xffffffffu, v.w, d));
+}
+__device__ __forceinline__ float4 shfl_down4(float4 v, int d) {
+    return make_float4(__shfl_down_sync(0xffffffffu, v.x, d), __shfl_down_sync(0xffffffffu, v.y, d),
+                       __shfl_down_sync(0xffffffffu, v.z, d), __shfl_down_sync(0xffffffffu, v.w, d));
+}
+
+}  // namespace kami

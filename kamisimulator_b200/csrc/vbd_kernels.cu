@@ -1,0 +1,454 @@
+// vbd_kernels.cu -- sm_100a kernels of the Stable Cosserat Rods VBD step.
+//
+// Two forms share the tile-major float4 structure-of-arrays layout of vbd_common.cuh:
+//
+//  * sweep form: one kernel per phase (predict; per iteration: even-vertex, odd-vertex,
+//    even-segment, odd-segment sweeps; finish + SDF), each thread owning one slot and reading
+//    its neighbours from global memory.  This is the plain per-groom form; the host replays the
+//    whole step from a CUDA graph, as Sim::rebuildCUDAGraph does (YarnBall/sim/step.cpp:9-36).
+//
+//  * fused form: one kernel per step.  Each warp owns one tile (a strand, or several short
+//    strands, of up to 32*C vertices) in registers for every substep and iteration; neighbour
+//    coupling across lanes goes through warp shuffles.  Predict, all iterations, the velocity
+//    update and the SDF projection run back to back, so HBM sees each vertex twice per step
+//    (one float4 load per array, one store per dynamic array).
+#include "vbd_kernels.h"
+#include "vbd_math.cuh"
+
+namespace kami {
+
+// ------------------------------------------------------------------------------------------
+// tile index helpers
+__device__ __forceinline__ int64_t next_slot(int64_t g, int C) {
+    // slot p+1 of the slot stored at g (caller guarantees p < T-1)
+    int64_t T = 32LL * C;
+    int64_t tile = g / T;
+    int r = (int)(g - tile * T);
+    int k = r >> 5, lane = r & 31;
+    return (k < C - 1) ? g + 32 : tile * T + lane + 1;
+}
+__device__ __forceinline__ int64_t prev_slot(int64_t g, int C) {
+    int64_t T = 32LL * C;
+    int64_t tile = g / T;
+    int r = (int)(g - tile * T);
+    int k = r >> 5, lane = r & 31;
+    return (k > 0) ? g - 32 : tile * T + (int64_t)(C - 1) * 32 + lane - 1;
+}
+
+// ==========================================================================================
+// sweep form
+// ==========================================================================================
+
+// initItr for every slot; writes y4 = (y, 1/(invMass h^2)), dx4 = (dx, 0), vlast = v.
+__global__ void sweep_predict_kernel(DeviceState st, float4* __restrict__ y4, float4* __restrict__ dx4,
+                                     const StepParams* __restrict__ spp, PhysParams pp, int64_t num_slots) {
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= num_slots) return;
+    const StepParams sp = *spp;
+    float4 xm = st.xm[g];
+    float3 v = xyz(st.vel[g]);
+    float3 vl = xyz(st.vlast[g]);
+    float3 dx, y;
+    vbd_predict(xyz(xm), v, vl, xm.w, pp, sp.h, sp.last_h, sp.time, dx, y);
+    st.vlast[g] = make_float4(v.x, v.y, v.z, 0.f);
+    y4[g] = make_float4(y.x, y.y, y.z, 0.f);
+    dx4[g] = make_float4(dx.x, dx.y, dx.z, 0.f);
+}
+
+// Segment constants of the segment starting at slot g (whose next slot is gn).
+struct SegData {
+    float3 e;
+    float invl, kk, dd;
+    float3 d3;
+};
+__device__ __forceinline__ SegData seg_data(const DeviceState& st, const float4* q, int64_t g, int64_t gn, float4 prm) {
+    SegData s;
+    s.e = xyz(st.xm[gn]) - xyz(st.xm[g]);
+    s.invl = 1.f / prm.x;
+    s.kk = prm.y * s.invl;
+    s.dd = s.kk * s.invl;
+    s.d3 = d3_of(q[g]);
+    return s;
+}
+
+// Position sweep.  COLOUR2: threads cover the rows of one colour (k = 2r + colour), read and
+// write dx in place.  JACOBI: threads cover every row, read dx_in and write dx_out.
+template <bool JACOBI>
+__global__ void sweep_position_kernel(DeviceState st, const float4* __restrict__ y4, const float4* __restrict__ qcur,
+                                      const float4* dx_in, float4* dx_out, const StepParams* __restrict__ spp,
+                                      PhysParams pp, int C, int colour, int64_t num_threads) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= num_threads) return;
+    int rows = JACOBI ? C : C / 2;
+    int64_t tile = t / (32LL * rows);
+    int rem = (int)(t - tile * 32LL * rows);
+    int r = rem >> 5, lane = rem & 31;
+    int k = JACOBI ? r : 2 * r + colour;
+    int64_t g = tile * 32LL * C + (int64_t)k * 32 + lane;
+    float4 prm = st.prm[g];
+    uint32_t fl = __float_as_uint(prm.w);
+    float4 d = dx_in[g];
+    float3 dx = xyz(d);
+    float4 xm = st.xm[g];
+    if (!(fl & F_VALID) || xm.w == 0.f) {
+        if (JACOBI) dx_out[g] = d;
+        return;
+    }
+    const float h = spp->h;
+    const float damp = pp.damping / h;
+    SegData sn{}, sp{};
+    float3 dxn = f3(0.f, 0.f, 0.f), dxp = f3(0.f, 0.f, 0.f);
+    if (fl & F_HAS_NEXT) {
+        int64_t gn = next_slot(g, C);
+        sn = seg_data(st, qcur, g, gn, prm);
+        dxn = xyz(dx_in[gn]);
+    }
+    if (fl & F_HAS_PREV) {
+        int64_t gp = prev_slot(g, C);
+        sp = seg_data(st, qcur, gp, g, st.prm[gp]);
+        dxp = xyz(dx_in[gp]);
+    }
+    BlockConst bc = vbd_block_const(xm.w, fl, sn.dd, sp.dd, h, damp);
+    float3 nd = vbd_position(dx, xyz(y4[g]), fl, bc, sn.e, sn.invl, sn.kk, sn.dd, sn.d3, dxn, sp.e, sp.invl, sp.kk,
+                             sp.dd, sp.d3, dxp, damp, pp.accel_ratio);
+    dx_out[g] = make_float4(nd.x, nd.y, nd.z, 0.f);
+}
+
+// Orientation sweep, same thread mapping as the position sweep.
+template <bool JACOBI>
+__global__ void sweep_orientation_kernel(DeviceState st, const float4* __restrict__ dx4, const float4* q_in,
+                                         float4* q_out, int C, int colour, int64_t num_threads) {
+    int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= num_threads) return;
+    int rows = JACOBI ? C : C / 2;
+    int64_t tile = t / (32LL * rows);
+    int rem = (int)(t - tile * 32LL * rows);
+    int r = rem >> 5, lane = rem & 31;
+    int k = JACOBI ? r : 2 * r + colour;
+    int64_t g = tile * 32LL * C + (int64_t)k * 32 + lane;
+    float4 prm = st.prm[g];
+    uint32_t fl = __float_as_uint(prm.w);
+    float4 q = q_in[g];
+    if (!(fl & F_HAS_NEXT) || (fl & F_FIX_ORIENTATION)) {
+        if (JACOBI) q_out[g] = q;
+        return;
+    }
+    int64_t gn = next_slot(g, C);
+    float3 e = xyz(st.xm[gn]) - xyz(st.xm[g]);
+    float3 dx = xyz(dx4[g]), dxn = xyz(dx4[gn]);
+    float4 qp = make_float4(0.f, 0.f, 0.f, 1.f), qrp = qp, qn = qp;
+    if (fl & F_HAS_PREV) {
+        int64_t gp = prev_slot(g, C);
+        qp = q_in[gp];
+        qrp = st.qr[gp];
+    }
+    if (fl & F_HAS_NEXT_ORIENTATION) qn = q_in[gn];
+    float m2k = -2.f * prm.y * (1.f / prm.x);
+    q_out[g] = vbd_orientation(q, fl, e, dx, dxn, m2k, qp, qrp, qn, st.qr[g]);
+}
+
+// endItr for every slot, then (on the last substep) the SDF pass and the finiteness check.
+__global__ void sweep_finish_kernel(DeviceState st, const float4* __restrict__ dx4, const StepParams* __restrict__ spp,
+                                    PhysParams pp, SdfParams sdf, int apply_sdf, int64_t num_slots) {
+    int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    bool bad = false;
+    if (g < num_slots) {
+        const StepParams sp = *spp;
+        float4 xm = st.xm[g];
+        uint32_t fl = __float_as_uint(st.prm[g].w);
+        float3 x = xyz(xm), v = xyz(st.vel[g]);
+        vbd_finish(x, v, xyz(dx4[g]), xm.w, sp.h, pp.velocity_decay);
+        if (apply_sdf && sdf.grid && (fl & F_VALID) && !(fl & F_ROOT)) vbd_sdf(x, v, sdf, sp);
+        st.xm[g] = make_float4(x.x, x.y, x.z, xm.w);
+        st.vel[g] = make_float4(v.x, v.y, v.z, 0.f);
+        if (apply_sdf) bad = !finite3(x) || !finite3(v) || !finite4(st.q[g]);
+    }
+    if (__any_sync(0xffffffffu, bad) && (threadIdx.x & 31) == 0) atomicOr(st.status, STATUS_NONFINITE);
+}
+
+// ==========================================================================================
+// fused form
+// ==========================================================================================
+
+template <int C, bool JACOBI>
+__global__ void __launch_bounds__(128) fused_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf) {
+    static_assert(C % 2 == 0, "slots per lane must be even");
+    const int lane = threadIdx.x & 31;
+    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (tile >= st.num_tiles) return;  // uniform per warp
+    const int64_t base = tile * (32LL * C) + lane;
+
+    float3 x[C], v[C], vl[C], dx[C], y[C], e[C], d3[C];
+    float4 q[C], qr[C];
+    float im[C], invl[C], kk[C], dd[C];
+    uint32_t fl[C];
+    BlockConst bc[C];
+
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+        const int64_t g = base + 32LL * k;
+        float4 a = st.xm[g];
+        x[k] = xyz(a);
+        im[k] = a.w;
+        v[k] = xyz(st.vel[g]);
+        vl[k] = xyz(st.vlast[g]);
+        q[k] = st.q[g];
+        qr[k] = st.qr[g];
+        float4 p = st.prm[g];
+        invl[k] = 1.f / p.x;
+        kk[k] = p.y * invl[k];
+        dd[k] = kk[k] * invl[k];
+        fl[k] = __float_as_uint(p.w);
+    }
+    // static halo: constants of the previous lane's last segment (segment i-1 of slot 0)
+    const float4 qrP = shfl_up4(qr[C - 1], 1);
+    const float invlP = __shfl_up_sync(0xffffffffu, invl[C - 1], 1);
+    const float kkP = __shfl_up_sync(0xffffffffu, kk[C - 1], 1);
+    const float ddP = __shfl_up_sync(0xffffffffu, dd[C - 1], 1);
+
+    const float h = sp.h;
+    const float damp = pp.damping / h;
+    const float accel = pp.accel_ratio;
+
+    for (int s = 0; s < sp.substeps; s++) {
+        // segment vectors (constant within a substep)
+#pragma unroll
+        for (int k = 0; k < C - 1; k++) e[k] = x[k + 1] - x[k];
+        e[C - 1] = shfl_down3(x[0], 1) - x[C - 1];
+        const float3 eP = shfl_up3(e[C - 1], 1);
+
+#pragma unroll
+        for (int k = 0; k < C; k++) {
+            vbd_predict(x[k], v[k], vl[k], im[k], pp, h, sp.last_h, sp.time, dx[k], y[k]);
+            vl[k] = v[k];
+            bc[k] = vbd_block_const(im[k], fl[k], dd[k], k > 0 ? dd[k - 1] : ddP, h, damp);
+            d3[k] = d3_of(q[k]);
+        }
+        float4 qP = shfl_up4(q[C - 1], 1);
+        float3 d3P = d3_of(qP);
+
+        for (int it = 0; it < pp.num_itr; it++) {
+            if (!JACOBI) {
+                // ---- positions, even slots
+                const float3 dxP = shfl_up3(dx[C - 1], 1);
+#pragma unroll
+                for (int k = 0; k < C; k += 2) {
+                    if (im[k] != 0.f) {
+                        const bool k0 = (k == 0);
+                        dx[k] = vbd_position(dx[k], y[k], fl[k], bc[k], e[k], invl[k], kk[k], dd[k], d3[k], dx[k + 1],
+                                             k0 ? eP : e[k > 0 ? k - 1 : 0], k0 ? invlP : invl[k > 0 ? k - 1 : 0],
+                                             k0 ? kkP : kk[k > 0 ? k - 1 : 0], k0 ? ddP : dd[k > 0 ? k - 1 : 0],
+                                             k0 ? d3P : d3[k > 0 ? k - 1 : 0], k0 ? dxP : dx[k > 0 ? k - 1 : 0], damp,
+                                             accel);
+                    }
+                }
+                // ---- positions, odd slots
+                const float3 dxN = shfl_down3(dx[0], 1);
+#pragma unroll
+                for (int k = 1; k < C; k += 2) {
+                    if (im[k] != 0.f) {
+                        const bool kl = (k == C - 1);
+                        dx[k] = vbd_position(dx[k], y[k], fl[k], bc[k], e[k], invl[k], kk[k], dd[k], d3[k],
+                                             kl ? dxN : dx[k + 1 < C ? k + 1 : k], e[k - 1], invl[k - 1], kk[k - 1],
+                                             dd[k - 1], d3[k - 1], dx[k - 1], damp, accel);
+                    }
+                }
+                // ---- orientations, even segments
+#pragma unroll
+                for (int k = 0; k < C; k += 2) {
+                    if ((fl[k] & F_HAS_NEXT) && !(fl[k] & F_FIX_ORIENTATION)) {
+                        const bool k0 = (k == 0);
+                        q[k] = vbd_orientation(q[k], fl[k], e[k], dx[k], dx[k + 1], -2.f * kk[k],
+                                               k0 ? qP : q[k > 0 ? k - 1 : 0], k0 ? qrP : qr[k > 0 ? k - 1 : 0],
+                                               q[k + 1], qr[k]);
+                        d3[k] = d3_of(q[k]);
+                    }
+                }
+                // ---- orientations, odd segments
+                const float4 qN = shfl_down4(q[0], 1);
+#pragma unroll
+                for (int k = 1; k < C; k += 2) {
+                    if ((fl[k] & F_HAS_NEXT) && !(fl[k] & F_FIX_ORIENTATION)) {
+                        const bool kl = (k == C - 1);
+                        q[k] = vbd_orientation(q[k], fl[k], e[k], dx[k], kl ? dxN : dx[k + 1 < C ? k + 1 : k],
+                                               -2.f * kk[k], q[k - 1], qr[k - 1], kl ? qN : q[k + 1 < C ? k + 1 : k],
+                                               qr[k]);
+                        d3[k] = d3_of(q[k]);
+                    }
+                }
+                qP = shfl_up4(q[C - 1], 1);
+                d3P = d3_of(qP);
+            } else {
+                // ---- positions, all slots from the previous sweep
+                const float3 dxP = shfl_up3(dx[C - 1], 1);
+                const float3 dxN = shfl_down3(dx[0], 1);
+                float3 nd[C];
+#pragma unroll
+                for (int k = 0; k < C; k++) {
+                    nd[k] = dx[k];
+                    if (im[k] != 0.f) {
+                        const bool k0 = (k == 0), kl = (k == C - 1);
+                        const int kp = k > 0 ? k - 1 : 0, kn = k + 1 < C ? k + 1 : k;
+                        nd[k] = vbd_position(dx[k], y[k], fl[k], bc[k], e[k], invl[k], kk[k], dd[k], d3[k],
+                                             kl ? dxN : dx[kn], k0 ? eP : e[kp], k0 ? invlP : invl[kp],
+                                             k0 ? kkP : kk[kp], k0 ? ddP : dd[kp], k0 ? d3P : d3[kp],
+                                             k0 ? dxP : dx[kp], damp, accel);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < C; k++) dx[k] = nd[k];
+                // ---- orientations, all segments from the previous sweep
+                const float3 dxN2 = shfl_down3(dx[0], 1);
+                const float4 qN = shfl_down4(q[0], 1);
+                float4 nq[C];
+#pragma unroll
+                for (int k = 0; k < C; k++) {
+                    nq[k] = q[k];
+                    if ((fl[k] & F_HAS_NEXT) && !(fl[k] & F_FIX_ORIENTATION)) {
+                        const bool k0 = (k == 0), kl = (k == C - 1);
+                        const int kp = k > 0 ? k - 1 : 0, kn = k + 1 < C ? k + 1 : k;
+                        nq[k] = vbd_orientation(q[k], fl[k], e[k], dx[k], kl ? dxN2 : dx[kn], -2.f * kk[k],
+                                                k0 ? qP : q[kp], k0 ? qrP : qr[kp], kl ? qN : q[kn], qr[k]);
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < C; k++) {
+                    q[k] = nq[k];
+                    d3[k] = d3_of(q[k]);
+                }
+                qP = shfl_up4(q[C - 1], 1);
+                d3P = d3_of(qP);
+            }
+        }
+#pragma unroll
+        for (int k = 0; k < C; k++) vbd_finish(x[k], v[k], dx[k], im[k], h, pp.velocity_decay);
+    }
+
+    bool bad = false;
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+        if (sdf.grid && (fl[k] & F_VALID) && !(fl[k] & F_ROOT)) vbd_sdf(x[k], v[k], sdf, sp);
+        bad |= !finite3(x[k]) || !finite3(v[k]) || !finite4(q[k]);
+        const int64_t g = base + 32LL * k;
+        st.xm[g] = make_float4(x[k].x, x[k].y, x[k].z, im[k]);
+        st.vel[g] = make_float4(v[k].x, v[k].y, v[k].z, 0.f);
+        st.vlast[g] = make_float4(vl[k].x, vl[k].y, vl[k].z, 0.f);
+        st.q[g] = q[k];
+    }
+    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(st.status, STATUS_NONFINITE);
+}
+
+// ==========================================================================================
+// boundary gather / scatter (API vertex order <-> tile slots)
+// ==========================================================================================
+__global__ void scatter3_kernel(const float* __restrict__ src, float4* __restrict__ dst,
+                                const int64_t* __restrict__ slot_of, int64_t nv) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    float4* d = dst + slot_of[i];
+    float4 o = *d;
+    *d = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], o.w);
+}
+__global__ void gather3_kernel(const float4* __restrict__ src, float* __restrict__ dst,
+                               const int64_t* __restrict__ slot_of, int64_t nv) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    float4 a = src[slot_of[i]];
+    dst[3 * i] = a.x;
+    dst[3 * i + 1] = a.y;
+    dst[3 * i + 2] = a.z;
+}
+__global__ void scatter4_kernel(const float4* __restrict__ src, float4* __restrict__ dst,
+                                const int64_t* __restrict__ slot_of, int64_t nv) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    dst[slot_of[i]] = src[i];
+}
+__global__ void gather4_kernel(const float4* __restrict__ src, float4* __restrict__ dst,
+                               const int64_t* __restrict__ slot_of, int64_t nv) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    dst[i] = src[slot_of[i]];
+}
+
+// ==========================================================================================
+// launchers
+// ==========================================================================================
+static inline unsigned blocks_for(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+cudaError_t launch_sweep_predict(const DeviceState& st, float4* y4, float4* dx4, const StepParams* d_sp,
+                                 const PhysParams& pp, int64_t num_slots, cudaStream_t s) {
+    sweep_predict_kernel<<<blocks_for(num_slots, 256), 256, 0, s>>>(st, y4, dx4, d_sp, pp, num_slots);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_position(const DeviceState& st, const float4* y4, const float4* q, const float4* dx_in,
+                                  float4* dx_out, const StepParams* d_sp, const PhysParams& pp, int C, int colour,
+                                  bool jacobi, cudaStream_t s) {
+    int64_t n = st.num_tiles * 32LL * (jacobi ? C : C / 2);
+    if (jacobi)
+        sweep_position_kernel<true><<<blocks_for(n, 256), 256, 0, s>>>(st, y4, q, dx_in, dx_out, d_sp, pp, C, colour, n);
+    else
+        sweep_position_kernel<false><<<blocks_for(n, 256), 256, 0, s>>>(st, y4, q, dx_in, dx_out, d_sp, pp, C, colour, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_orientation(const DeviceState& st, const float4* dx4, const float4* q_in, float4* q_out, int C,
+                                     int colour, bool jacobi, cudaStream_t s) {
+    int64_t n = st.num_tiles * 32LL * (jacobi ? C : C / 2);
+    if (jacobi)
+        sweep_orientation_kernel<true><<<blocks_for(n, 256), 256, 0, s>>>(st, dx4, q_in, q_out, C, colour, n);
+    else
+        sweep_orientation_kernel<false><<<blocks_for(n, 256), 256, 0, s>>>(st, dx4, q_in, q_out, C, colour, n);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_finish(const DeviceState& st, const float4* dx4, const StepParams* d_sp, const PhysParams& pp,
+                                const SdfParams& sdf, bool apply_sdf, int64_t num_slots, cudaStream_t s) {
+    sweep_finish_kernel<<<blocks_for(num_slots, 256), 256, 0, s>>>(st, dx4, d_sp, pp, sdf, apply_sdf ? 1 : 0, num_slots);
+    return cudaGetLastError();
+}
+
+bool fused_supported(int C) { return C == 2 || C == 4; }
+
+cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
+                              int C, bool jacobi, int warps_per_block, cudaStream_t s) {
+    int threads = 32 * warps_per_block;
+    unsigned blocks = blocks_for(st.num_tiles, warps_per_block);
+    if (blocks == 0) return cudaSuccess;
+#define KAMI_FUSED_CASE(CC)                                                                  \
+    if (C == CC) {                                                                           \
+        if (jacobi)                                                                          \
+            fused_step_kernel<CC, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf);         \
+        else                                                                                 \
+            fused_step_kernel<CC, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf);        \
+        return cudaGetLastError();                                                           \
+    }
+    KAMI_FUSED_CASE(2)
+    KAMI_FUSED_CASE(4)
+#undef KAMI_FUSED_CASE
+    return cudaErrorInvalidValue;
+}
+
+cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
+    if (nv == 0) return cudaSuccess;
+    scatter3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
+    return cudaGetLastError();
+}
+cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
+    if (nv == 0) return cudaSuccess;
+    gather3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
+    return cudaGetLastError();
+}
+cudaError_t launch_scatter4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
+    if (nv == 0) return cudaSuccess;
+    scatter4_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
+    return cudaGetLastError();
+}
+cudaError_t launch_gather4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
+    if (nv == 0) return cudaSuccess;
+    gather4_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
+    return cudaGetLastError();
+}
+
+}  // namespace kami

@@ -1,0 +1,29 @@
+// vbd_kernels.h -- host-side launchers of the solver's kernels (vbd_kernels.cu).
+#pragma once
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "vbd_common.cuh"
+
+namespace kami {
+
+cudaError_t launch_sweep_predict(const DeviceState& st, float4* y4, float4* dx4, const StepParams* d_sp,
+                                 const PhysParams& pp, int64_t num_slots, cudaStream_t s);
+cudaError_t launch_sweep_position(const DeviceState& st, const float4* y4, const float4* q, const float4* dx_in,
+                                  float4* dx_out, const StepParams* d_sp, const PhysParams& pp, int C, int colour,
+                                  bool jacobi, cudaStream_t s);
+cudaError_t launch_sweep_orientation(const DeviceState& st, const float4* dx4, const float4* q_in, float4* q_out, int C,
+                                     int colour, bool jacobi, cudaStream_t s);
+cudaError_t launch_sweep_finish(const DeviceState& st, const float4* dx4, const StepParams* d_sp, const PhysParams& pp,
+                                const SdfParams& sdf, bool apply_sdf, int64_t num_slots, cudaStream_t s);
+
+bool fused_supported(int C);
+cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
+                              int C, bool jacobi, int warps_per_block, cudaStream_t s);
+
+cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
+cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
+cudaError_t launch_scatter4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
+cudaError_t launch_gather4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
+
+}  // namespace kami

@@ -1,0 +1,223 @@
+"""Seeded synthetic grooms and body SDF grids for the solver's workloads.
+
+The reference ships no hair or head data for this path (its USC-HairSalon `.data`
+files and head meshes are downloaded separately), so every workload is generated
+here from a fixed seed:
+
+* ``cantilever``: straight horizontal rods, the geometry of the reference's
+  cantilever harness (src/solvers/CantileverTestSolver.cpp:18-104): 64 rods x 32
+  vertices, 5 mm segments, roots 1 cm apart on the y axis, rods along +x.
+* ``groom``: strands rooted uniformly on the upper (z > 0) hemisphere of a 0.09 m
+  head sphere, growing along the outward normal with a helical curl (radius
+  U[0, 8] mm, pitch U[1, 3] cm), segment length 2 mm x U[0.9, 1.1], per-strand
+  Young's modulus log-uniform in [1, 5] GPa.
+* ``batched grooms``: many independent grooms with log-uniform strand counts and
+  uniform-integer vertex counts per strand.
+* ``sphere_sdf`` / ``capsule_union_sdf``: signed-distance grids sampled at the
+  node positions the reference uses (node (i, j, k) at grid_min + ds * (i, j, k),
+  ds = (grid_max - grid_min) / dims, src/PNMesh.cpp:118-146), stored x-fastest.
+
+Positions are float32 metres; strands are contiguous, described by CSR offsets
+``strand_begin`` (length S + 1).
+"""
+from __future__ import annotations
+
+import dataclasses
+import math
+
+import numpy as np
+
+
+@dataclasses.dataclass
+class Groom:
+    strand_begin: np.ndarray  # int32 [S + 1]
+    positions: np.ndarray  # float32 [V, 3]
+    strand_young: np.ndarray  # float32 [S], GPa
+    strand_dev: np.ndarray  # float32 [S], bend deviation coefficient
+
+    @property
+    def num_strands(self) -> int:
+        return int(self.strand_begin.shape[0] - 1)
+
+    @property
+    def num_vertices(self) -> int:
+        return int(self.positions.shape[0])
+
+    def strand_lengths(self) -> np.ndarray:
+        return np.diff(self.strand_begin)
+
+
+@dataclasses.dataclass
+class SDFGrid:
+    dims: tuple  # (nx, ny, nz)
+    grid_min: tuple
+    grid_max: tuple
+    phi: np.ndarray  # float32 [nz, ny, nx]
+    grad: np.ndarray  # float32 [nz, ny, nx, 3]
+    threshold: float
+
+    def node_positions(self, z0: int = 0, z1: int | None = None) -> np.ndarray:
+        nx, ny, nz = self.dims
+        z1 = nz if z1 is None else z1
+        return _node_positions(self.dims, self.grid_min, self.grid_max, z0, z1)
+
+
+def _node_positions(dims, gmin, gmax, z0, z1):
+    nx, ny, nz = dims
+    gmin = np.asarray(gmin, np.float32)
+    ds = (np.asarray(gmax, np.float32) - gmin) / np.asarray(dims, np.float32)
+    iz, iy, ix = np.meshgrid(np.arange(z0, z1), np.arange(ny), np.arange(nx), indexing="ij")
+    p = np.stack([ix, iy, iz], axis=-1).astype(np.float32)
+    return gmin + ds * p
+
+
+def cantilever(num_rods: int = 64, verts_per_rod: int = 32, segment: float = 5e-3, spacing: float = 1e-2,
+               young: float = 3.9) -> Groom:
+    """Straight rods along +x, roots at (0, spacing * k, 0)."""
+    k = np.arange(num_rods, dtype=np.float32)
+    j = np.arange(verts_per_rod, dtype=np.float32)
+    pos = np.zeros((num_rods, verts_per_rod, 3), np.float32)
+    pos[:, :, 0] = segment * j[None, :]
+    pos[:, :, 1] = spacing * k[:, None]
+    sb = (np.arange(num_rods + 1) * verts_per_rod).astype(np.int32)
+    return Groom(sb, pos.reshape(-1, 3), np.full(num_rods, young, np.float32), np.ones(num_rods, np.float32))
+
+
+def _orthonormal_frames(n: np.ndarray):
+    """Two unit vectors perpendicular to each row of n (rows unit length)."""
+    helper = np.where(np.abs(n[:, 2:3]) < 0.9, np.array([[0.0, 0.0, 1.0]]), np.array([[1.0, 0.0, 0.0]]))
+    t1 = np.cross(n, helper)
+    t1 /= np.linalg.norm(t1, axis=1, keepdims=True)
+    t2 = np.cross(n, t1)
+    return t1, t2
+
+
+def groom_strands(rng: np.random.Generator, lengths: np.ndarray, head_radius: float = 0.09,
+                  seg_len: float = 2e-3, seg_jitter: float = 0.1, curl_radius_max: float = 8e-3,
+                  pitch_range=(1e-2, 3e-2), young_range=(1.0, 5.0)) -> Groom:
+    """Curly strands of the given vertex counts rooted on the upper head hemisphere."""
+    lengths = np.asarray(lengths, np.int64)
+    S = lengths.shape[0]
+    # uniform on the upper hemisphere: z = cos(theta) uniform in (0, 1]
+    z = rng.uniform(0.0, 1.0, S)
+    phi = rng.uniform(0.0, 2.0 * math.pi, S)
+    rxy = np.sqrt(np.maximum(0.0, 1.0 - z * z))
+    n = np.stack([rxy * np.cos(phi), rxy * np.sin(phi), z], axis=1)
+    t1, t2 = _orthonormal_frames(n)
+    curl_r = rng.uniform(0.0, curl_radius_max, S)
+    pitch = rng.uniform(pitch_range[0], pitch_range[1], S)
+    theta0 = rng.uniform(0.0, 2.0 * math.pi, S)
+    young = np.exp(rng.uniform(math.log(young_range[0]), math.log(young_range[1]), S))
+    V = int(lengths.sum())
+    sb = np.zeros(S + 1, np.int64)
+    np.cumsum(lengths, out=sb[1:])
+    strand_of = np.repeat(np.arange(S), lengths)
+    local = np.arange(V) - sb[strand_of]
+    seg = seg_len * rng.uniform(1.0 - seg_jitter, 1.0 + seg_jitter, V)
+    seg[sb[1:] - 1] = 0.0  # no segment after a tip
+    # axial advance per segment so that the helix arc length matches the segment length
+    slope = np.sqrt(1.0 + (2.0 * math.pi * curl_r / pitch) ** 2)
+    dz = seg / slope[strand_of]
+    excl = np.cumsum(dz) - dz  # exclusive prefix sum over all vertices
+    axial = excl - excl[sb[:-1]][strand_of]  # ... restarted at each strand root
+    axial[local == 0] = 0.0
+    ang = theta0[strand_of] + 2.0 * math.pi * axial / pitch[strand_of]
+    r = curl_r[strand_of]
+    off = (r * (np.cos(ang) - np.cos(theta0[strand_of])))[:, None] * t1[strand_of] + \
+          (r * (np.sin(ang) - np.sin(theta0[strand_of])))[:, None] * t2[strand_of]
+    pos = head_radius * n[strand_of] + axial[:, None] * n[strand_of] + off
+    return Groom(sb.astype(np.int32), pos.astype(np.float32), young.astype(np.float32), np.ones(S, np.float32))
+
+
+def groom(num_strands: int = 10_000, verts_per_strand: int = 64, seed: int = 2) -> Groom:
+    rng = np.random.default_rng(seed)
+    return groom_strands(rng, np.full(num_strands, verts_per_strand))
+
+
+def batched_grooms(num_grooms: int = 64, strands_range=(500, 20_000), verts_range=(16, 128), seed: int = 3,
+                   strand_scale: float = 1.0) -> list:
+    """Independent grooms: strand count log-uniform, vertices per strand uniform integer."""
+    rng = np.random.default_rng(seed)
+    out = []
+    for _ in range(num_grooms):
+        s = int(round(math.exp(rng.uniform(math.log(strands_range[0]), math.log(strands_range[1]))) * strand_scale))
+        s = max(1, s)
+        lens = rng.integers(verts_range[0], verts_range[1] + 1, s)
+        out.append(groom_strands(rng, lens))
+    return out
+
+
+def concat_grooms(grooms: list) -> Groom:
+    sbs, pos, young, dev = [np.zeros(1, np.int64)], [], [], []
+    off = 0
+    for g in grooms:
+        sbs.append(g.strand_begin[1:].astype(np.int64) + off)
+        off += g.num_vertices
+        pos.append(g.positions)
+        young.append(g.strand_young)
+        dev.append(g.strand_dev)
+    return Groom(np.concatenate(sbs).astype(np.int32), np.concatenate(pos), np.concatenate(young),
+                 np.concatenate(dev))
+
+
+def sphere_sdf(n: int = 128, radius: float = 0.09, half_extent: float = 0.2, threshold: float = 1e-3) -> SDFGrid:
+    dims = (n, n, n)
+    gmin = (-half_extent,) * 3
+    gmax = (half_extent,) * 3
+    p = _node_positions(dims, gmin, gmax, 0, n).astype(np.float64)
+    d = np.linalg.norm(p, axis=-1)
+    phi = (d - radius).astype(np.float32)
+    grad = (p / np.maximum(d, 1e-12)[..., None]).astype(np.float32)
+    return SDFGrid(dims, gmin, gmax, phi, grad, threshold)
+
+
+def capsule_union_sdf(n: int = 256, num_capsules: int = 12, radius_range=(0.02, 0.08), half_extent: float = 0.3,
+                      threshold: float = 1e-3, seed: int = 5) -> SDFGrid:
+    """Union (min) of random capsules; the gradient is that of the closest capsule."""
+    rng = np.random.default_rng(seed)
+    a = rng.uniform(-0.15, 0.15, (num_capsules, 3))
+    b = a + rng.normal(0.0, 0.08, (num_capsules, 3))
+    r = rng.uniform(radius_range[0], radius_range[1], num_capsules)
+    dims = (n, n, n)
+    gmin = (-half_extent,) * 3
+    gmax = (half_extent,) * 3
+    phi = np.empty((n, n, n), np.float32)
+    grad = np.empty((n, n, n, 3), np.float32)
+    chunk = max(1, (1 << 21) // (n * n))
+    for z0 in range(0, n, chunk):
+        z1 = min(n, z0 + chunk)
+        p = _node_positions(dims, gmin, gmax, z0, z1).reshape(-1, 3).astype(np.float64)
+        best = np.full(p.shape[0], np.inf)
+        bgrad = np.zeros_like(p)
+        for c in range(num_capsules):
+            ab = b[c] - a[c]
+            t = np.clip(((p - a[c]) @ ab) / (ab @ ab), 0.0, 1.0)
+            closest = a[c] + t[:, None] * ab
+            dv = p - closest
+            dist = np.linalg.norm(dv, axis=1)
+            d = dist - r[c]
+            m = d < best
+            best[m] = d[m]
+            bgrad[m] = dv[m] / np.maximum(dist[m], 1e-12)[:, None]
+        phi[z0:z1] = best.reshape(z1 - z0, n, n)
+        grad[z0:z1] = bgrad.reshape(z1 - z0, n, n, 3)
+    return SDFGrid(dims, gmin, gmax, phi, grad, threshold)
+
+
+def head_rotation(t: float, amplitude_deg: float = 30.0, freq_hz: float = 1.0):
+    """Body quaternion (x, y, z, w) for a sinusoidal yaw about the vertical (z) axis."""
+    ang = math.radians(amplitude_deg) * math.sin(2.0 * math.pi * freq_hz * t)
+    return (0.0, 0.0, math.sin(0.5 * ang), math.cos(0.5 * ang))
+
+
+# Solver settings of each workload.  Units: seconds, metres, kg/m^3, GPa.
+WORKLOADS = {
+    "cantilever_64x32": dict(num_itr=10, dt=1.0 / 60.0, frames=100, gravity=(0.0, 0.0, -9.81), sdf=None),
+    "groom_10k_x64": dict(num_itr=20, dt=1.0 / 120.0, frames=200, gravity=(0.0, 0.0, -9.81), sdf="sphere128"),
+    "batched_64_grooms": dict(num_itr=20, dt=1.0 / 120.0, frames=120, gravity=(0.0, 0.0, -9.81), sdf="sphere128"),
+    "adjoint_2k_x48": dict(num_itr=20, dt=1.0 / 120.0, frames=60, gravity=(0.0, 0.0, -9.81), sdf="sphere128"),
+    "large_8x100k_x100": dict(num_itr=30, dt=1.0 / 120.0, frames=240, gravity=(0.0, 0.0, -9.81), sdf="capsules256"),
+}
+
+COMMON = dict(radius=40e-6, density=1300.0, damping=1e-6, velocity_decay=0.05, acceleration_ratio=1.0,
+              ext_mult=1.0)

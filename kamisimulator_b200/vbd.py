@@ -1,0 +1,307 @@
+"""Python binding of the solver's C ABI (include/kami_vbd.h) through ctypes.
+
+``Solver`` mirrors the calls KamiSimulator makes on its StableCosseratRods solver
+(src/solvers/Solver.h:61-84, StableCosseratRodsSolver.cpp:33-277): construct from a
+groom and settings, ``step(dt)`` per internal step, ``set``/``get`` positions and
+velocities for Upload/DownloadHair.  Arrays cross the boundary as float32 numpy
+arrays (host) or torch CUDA tensors (device).  There is no CPU path: without the
+compiled library every call raises.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "lib", "libkami_vbd.so")
+
+KAMI_OK = 0
+STATUS_NAMES = {0: "KAMI_OK", 1: "KAMI_ERR_INVALID_ARGUMENT", 2: "KAMI_ERR_CUDA", 3: "KAMI_ERR_OUT_OF_MEMORY",
+                4: "KAMI_ERR_NONFINITE", 5: "KAMI_ERR_GEOMETRY", 6: "KAMI_ERR_UNSUPPORTED", 7: "KAMI_ERR_TIMEOUT",
+                8: "KAMI_ERR_STATE"}
+SCHEDULES = {"colour2": 0, "jacobi": 1}
+FORMS = {"auto": 0, "sweep": 1, "fused": 2}
+MEM_HOST, MEM_DEVICE = 0, 1
+
+# Every symbol declared in include/kami_vbd.h.
+EXPORTED = [
+    "kami_vbd_desc_init", "kami_vbd_create", "kami_vbd_destroy", "kami_vbd_get_sizes",
+    "kami_vbd_set_positions_velocities", "kami_vbd_get_positions_velocities", "kami_vbd_get_orientations",
+    "kami_vbd_set_orientations", "kami_vbd_get_rest_darboux", "kami_vbd_set_rest_darboux",
+    "kami_vbd_set_body_transform", "kami_vbd_step", "kami_vbd_synchronize", "kami_vbd_state_size",
+    "kami_vbd_get_state", "kami_vbd_set_state", "kami_vbd_last_error_string", "kami_vbd_version",
+]
+
+
+class KamiError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+        self.status = status
+
+
+class SdfDesc(ctypes.Structure):
+    _fields_ = [("dims", ctypes.c_int32 * 3), ("grid_min", ctypes.c_float * 3), ("grid_max", ctypes.c_float * 3),
+                ("threshold", ctypes.c_float), ("phi", ctypes.c_void_p), ("grad", ctypes.c_void_p)]
+
+
+class Desc(ctypes.Structure):
+    _fields_ = [
+        ("num_strands", ctypes.c_int32),
+        ("strand_begin", ctypes.c_void_p),
+        ("positions", ctypes.c_void_p),
+        ("velocities", ctypes.c_void_p),
+        ("radius", ctypes.c_float),
+        ("density", ctypes.c_float),
+        ("stiffness_mode", ctypes.c_int32),
+        ("young", ctypes.c_float),
+        ("deviation", ctypes.c_float),
+        ("strand_young", ctypes.c_void_p),
+        ("strand_deviation", ctypes.c_void_p),
+        ("k_stretch", ctypes.c_float),
+        ("k_bend", ctypes.c_float),
+        ("gravity", ctypes.c_float * 3),
+        ("damping", ctypes.c_float),
+        ("velocity_decay", ctypes.c_float),
+        ("acceleration_ratio", ctypes.c_float),
+        ("external_force_multiplier", ctypes.c_float),
+        ("wind_peak", ctypes.c_float),
+        ("wind_y_freq", ctypes.c_float),
+        ("wind_z_freq", ctypes.c_float),
+        ("wind_time_freq", ctypes.c_float),
+        ("wind_sharpness", ctypes.c_float),
+        ("num_itr", ctypes.c_int32),
+        ("max_h", ctypes.c_float),
+        ("schedule", ctypes.c_int32),
+        ("form", ctypes.c_int32),
+        ("pin_roots", ctypes.c_int32),
+        ("device", ctypes.c_int32),
+        ("sdf", ctypes.POINTER(SdfDesc)),
+    ]
+
+
+_lib = None
+
+
+def load_library(path: str = LIB_PATH):
+    """Loads the compiled library; raises if it has not been built (there is no fallback)."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise RuntimeError(f"the CUDA solver library {path} is missing; build it with __graft_entry__.build()")
+    lib = ctypes.CDLL(path)
+    vp, i32, i64, f32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+    sig = {
+        "kami_vbd_desc_init": [ctypes.POINTER(Desc)],
+        "kami_vbd_create": [ctypes.POINTER(Desc), ctypes.POINTER(vp)],
+        "kami_vbd_destroy": [vp],
+        "kami_vbd_get_sizes": [vp, ctypes.POINTER(i64), ctypes.POINTER(i32), ctypes.POINTER(i32)],
+        "kami_vbd_set_positions_velocities": [vp, vp, vp, i32],
+        "kami_vbd_get_positions_velocities": [vp, vp, vp, i32],
+        "kami_vbd_get_orientations": [vp, vp, i32],
+        "kami_vbd_set_orientations": [vp, vp, i32],
+        "kami_vbd_get_rest_darboux": [vp, vp, i32],
+        "kami_vbd_set_rest_darboux": [vp, vp, i32],
+        "kami_vbd_set_body_transform": [vp, vp, vp],
+        "kami_vbd_step": [vp, f32, vp],
+        "kami_vbd_synchronize": [vp],
+        "kami_vbd_state_size": [vp, ctypes.POINTER(ctypes.c_size_t)],
+        "kami_vbd_get_state": [vp, vp, ctypes.c_size_t, i32],
+        "kami_vbd_set_state": [vp, vp, ctypes.c_size_t, i32],
+    }
+    for name, args in sig.items():
+        fn = getattr(lib, name)
+        fn.argtypes = args
+        fn.restype = ctypes.c_int
+    lib.kami_vbd_last_error_string.restype = ctypes.c_char_p
+    lib.kami_vbd_last_error_string.argtypes = []
+    lib.kami_vbd_version.restype = ctypes.c_char_p
+    lib.kami_vbd_version.argtypes = []
+    _lib = lib
+    return lib
+
+
+def _check(rc):
+    if rc != KAMI_OK:
+        msg = _lib.kami_vbd_last_error_string().decode()
+        raise KamiError(rc, msg)
+
+
+def _ptr(a):
+    """Host numpy array or torch tensor -> (pointer, memory kind)."""
+    if a is None:
+        return None, MEM_HOST
+    if hasattr(a, "data_ptr"):
+        if a.is_cuda:
+            return ctypes.c_void_p(a.data_ptr()), MEM_DEVICE
+        return ctypes.c_void_p(a.data_ptr()), MEM_HOST
+    return a.ctypes.data_as(ctypes.c_void_p), MEM_HOST
+
+
+def _f32(a, shape=None):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    if shape is not None:
+        a = a.reshape(shape)
+    return a
+
+
+class Solver:
+    """One StableCosseratRods solver instance on the GPU (a YarnBall::Sim plus its SDF pass)."""
+
+    def __init__(self, groom, *, num_itr=8, max_h=4e-4, gravity=(0.0, -9.8, 0.0), radius=4e-5, density=1300.0,
+                 damping=1e-6, velocity_decay=0.05, acceleration_ratio=1.0, ext_mult=1.0,
+                 wind=(0.0, 1.0, 0.7, 0.4, 3.0), schedule="colour2", form="auto", sdf=None, stiffness_mode=0,
+                 young=5.0, deviation=1.0, per_strand=True, k_stretch=3e3, k_bend=6e-4, pin_roots=True,
+                 velocities=None, device=-1):
+        self.lib = load_library()
+        self._h = None
+        sb = np.ascontiguousarray(groom.strand_begin, np.int32)
+        pos = _f32(groom.positions)
+        vel = None if velocities is None else _f32(velocities)
+        sy = np.ascontiguousarray(groom.strand_young, np.float32) if per_strand else None
+        sd = np.ascontiguousarray(groom.strand_dev, np.float32) if per_strand else None
+        d = Desc()
+        _check(self.lib.kami_vbd_desc_init(ctypes.byref(d)))
+        d.num_strands = groom.num_strands
+        d.strand_begin = sb.ctypes.data
+        d.positions = pos.ctypes.data
+        d.velocities = vel.ctypes.data if vel is not None else None
+        d.radius, d.density = radius, density
+        d.stiffness_mode = stiffness_mode
+        d.young, d.deviation = young, deviation
+        d.strand_young = sy.ctypes.data if sy is not None else None
+        d.strand_deviation = sd.ctypes.data if sd is not None else None
+        d.k_stretch, d.k_bend = k_stretch, k_bend
+        d.gravity[:] = gravity
+        d.damping, d.velocity_decay, d.acceleration_ratio = damping, velocity_decay, acceleration_ratio
+        d.external_force_multiplier = ext_mult
+        d.wind_peak, d.wind_y_freq, d.wind_z_freq, d.wind_time_freq, d.wind_sharpness = wind
+        d.num_itr = num_itr
+        d.max_h = max_h
+        d.schedule = SCHEDULES[schedule]
+        d.form = FORMS[form]
+        d.pin_roots = int(pin_roots)
+        d.device = device
+        keep = [sb, pos, vel, sy, sd]
+        if sdf is not None:
+            phi = np.ascontiguousarray(sdf.phi, np.float32)
+            grad = np.ascontiguousarray(sdf.grad, np.float32)
+            sd_ = SdfDesc()
+            sd_.dims[:] = sdf.dims
+            sd_.grid_min[:] = sdf.grid_min
+            sd_.grid_max[:] = sdf.grid_max
+            sd_.threshold = sdf.threshold
+            sd_.phi = phi.ctypes.data
+            sd_.grad = grad.ctypes.data
+            keep += [phi, grad, sd_]
+            d.sdf = ctypes.pointer(sd_)
+        h = ctypes.c_void_p()
+        _check(self.lib.kami_vbd_create(ctypes.byref(d), ctypes.byref(h)))
+        self._h = h
+        nv, ns, c = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()
+        _check(self.lib.kami_vbd_get_sizes(h, ctypes.byref(nv), ctypes.byref(ns), ctypes.byref(c)))
+        self.num_vertices, self.num_strands, self.slots_per_lane = nv.value, ns.value, c.value
+        del keep
+
+    # -- lifecycle
+    def close(self):
+        if self._h is not None:
+            self.lib.kami_vbd_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    @property
+    def handle(self):
+        return self._h
+
+    # -- stepping
+    def step(self, dt, stream=None):
+        s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+        _check(self.lib.kami_vbd_step(self._h, ctypes.c_float(dt), s))
+
+    def synchronize(self):
+        _check(self.lib.kami_vbd_synchronize(self._h))
+
+    def set_body_transform(self, rot, trans):
+        r = (ctypes.c_float * 4)(*rot)
+        t = (ctypes.c_float * 3)(*trans)
+        _check(self.lib.kami_vbd_set_body_transform(self._h, r, t))
+
+    # -- boundary data
+    def set_positions_velocities(self, x=None, v=None):
+        if x is not None and not hasattr(x, "data_ptr"):
+            x = _f32(x, (-1, 3))
+        if v is not None and not hasattr(v, "data_ptr"):
+            v = _f32(v, (-1, 3))
+        px, mx = _ptr(x)
+        pv, mv = _ptr(v)
+        mem = mx if x is not None else mv
+        _check(self.lib.kami_vbd_set_positions_velocities(self._h, px, pv, mem))
+
+    def get_positions_velocities(self, x_out=None, v_out=None):
+        if x_out is None and v_out is None:
+            x_out = np.empty((self.num_vertices, 3), np.float32)
+            v_out = np.empty((self.num_vertices, 3), np.float32)
+        px, mx = _ptr(x_out)
+        pv, mv = _ptr(v_out)
+        _check(self.lib.kami_vbd_get_positions_velocities(self._h, px, pv, mx if x_out is not None else mv))
+        return x_out, v_out
+
+    def get_orientations(self, out=None):
+        out = np.empty((self.num_vertices, 4), np.float32) if out is None else out
+        p, m = _ptr(out)
+        _check(self.lib.kami_vbd_get_orientations(self._h, p, m))
+        return out
+
+    def set_orientations(self, q):
+        q = q if hasattr(q, "data_ptr") else _f32(q, (-1, 4))
+        p, m = _ptr(q)
+        _check(self.lib.kami_vbd_set_orientations(self._h, p, m))
+
+    def get_rest_darboux(self, out=None):
+        out = np.empty((self.num_vertices, 4), np.float32) if out is None else out
+        p, m = _ptr(out)
+        _check(self.lib.kami_vbd_get_rest_darboux(self._h, p, m))
+        return out
+
+    def set_rest_darboux(self, qr):
+        qr = qr if hasattr(qr, "data_ptr") else _f32(qr, (-1, 4))
+        p, m = _ptr(qr)
+        _check(self.lib.kami_vbd_set_rest_darboux(self._h, p, m))
+
+    def state_size(self):
+        n = ctypes.c_size_t()
+        _check(self.lib.kami_vbd_state_size(self._h, ctypes.byref(n)))
+        return n.value
+
+    def get_state(self):
+        buf = np.empty(self.state_size() // 4, np.float32)
+        _check(self.lib.kami_vbd_get_state(self._h, buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes, MEM_HOST))
+        return buf
+
+    def set_state(self, buf):
+        buf = np.ascontiguousarray(buf, np.float32)
+        _check(self.lib.kami_vbd_set_state(self._h, buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes, MEM_HOST))
+
+    def split_state(self, buf):
+        nv = self.num_vertices
+        return dict(x=buf[:3 * nv].reshape(nv, 3), v=buf[3 * nv:6 * nv].reshape(nv, 3),
+                    v_last=buf[6 * nv:9 * nv].reshape(nv, 3), q=buf[9 * nv:13 * nv].reshape(nv, 4),
+                    clock=buf[13 * nv:13 * nv + 3])
+
+
+def version():
+    return load_library().kami_vbd_version().decode()

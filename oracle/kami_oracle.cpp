@@ -1,0 +1,596 @@
+// kami_oracle.cpp -- TEST INFRASTRUCTURE ONLY.
+//
+// CPU restatement of the Stable Cosserat Rods vertex-block-descent (VBD) step of
+// KamiSimulator's StableCosseratRods solver, templated on the scalar type so the
+// same update runs in FP32 (parity checker) and FP64 (trajectory-error replay).
+// Only tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg load this
+// library, always as the checker; no product code links or calls it.
+//
+// Each function names the reference file:line it restates (paths are relative to
+// the KamiSimulator project root).  Arithmetic follows the reference's operation
+// order where that is cheap to keep, including its quirks:
+//   * hess3(float d) fills all six packed entries, so the inertia block is
+//     (m/h^2) * ones(3,3), not (m/h^2) * I  (KittenEngine/includes/modules/SymMat.h:16-18,
+//     used at YarnBall/sim/cosserat.cu:117);
+//   * setYoung works in millimetre units (YarnBall/YBSimulator.cu:300-320);
+//   * the SDF lookup rounds to the nearest node but interpolates from idx-0.5
+//     (SDFCollisionSolver/cudaSDFCollision.cu:88-96 vs :139-142);
+//   * the SDF velocity fix subtracts (v/|v| . n) n (cudaSDFCollision.cu:261-263);
+//   * the initial guess uses lastH, the step of the previous advance() call
+//     (YarnBall/sim/iteration.cu:49, YarnBall/sim/step.cpp:38-42).
+//
+// Two deterministic schedules are provided because the reference's own kernels
+// race at block boundaries (cosserat.cu:142-143 vs :285, :316-335):
+//   schedule 1 "jacobi":  every vertex/segment reads the previous sweep's values
+//                         (the reference's intent);
+//   schedule 0 "colour2": Gauss-Seidel over a 2-colouring by local index parity
+//                         within each strand: even vertices, odd vertices, then
+//                         even segments, odd segments.
+#include <cmath>
+#include <cstdint>
+#include <cstring>
+#include <vector>
+#include <algorithm>
+#ifdef _OPENMP
+#include <omp.h>
+#endif
+
+namespace {
+
+constexpr double kPi = 3.141592653589793238462643;  // myPi, YBSimulator.cu:55
+
+// Vertex flags, YarnBall/YarnBall.h:33-39.
+constexpr uint32_t HAS_PREV = 1, HAS_NEXT = 2, HAS_NEXT_ORIENTATION = 4, FIX_ORIENTATION = 8;
+
+template <typename T>
+struct V3 {
+    T x, y, z;
+};
+template <typename T>
+struct Q4 {  // Kit::Rotor layout: (x, y, z) bivector part, w scalar last (Rotor.h:39-48)
+    T x, y, z, w;
+};
+
+template <typename T> inline V3<T> v3(T x, T y, T z) { return {x, y, z}; }
+template <typename T> inline V3<T> operator+(V3<T> a, V3<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+template <typename T> inline V3<T> operator-(V3<T> a, V3<T> b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+template <typename T> inline V3<T> operator-(V3<T> a) { return {-a.x, -a.y, -a.z}; }
+template <typename T> inline V3<T> operator*(T s, V3<T> a) { return {s * a.x, s * a.y, s * a.z}; }
+template <typename T> inline V3<T> operator*(V3<T> a, T s) { return {a.x * s, a.y * s, a.z * s}; }
+template <typename T> inline V3<T> operator/(V3<T> a, T s) { return {a.x / s, a.y / s, a.z / s}; }
+template <typename T> inline T dot(V3<T> a, V3<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+template <typename T> inline V3<T> cross(V3<T> a, V3<T> b) {
+    return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y};
+}
+template <typename T> inline T length(V3<T> a) { return std::sqrt(dot(a, a)); }
+template <typename T> inline T dot4(Q4<T> a, Q4<T> b) { return a.x * b.x + a.y * b.y + a.z * b.z + a.w * b.w; }
+template <typename T> inline T length4(Q4<T> a) { return std::sqrt(dot4(a, a)); }
+template <typename T> inline Q4<T> qadd(Q4<T> a, Q4<T> b) { return {a.x + b.x, a.y + b.y, a.z + b.z, a.w + b.w}; }
+template <typename T> inline Q4<T> qscale(T s, Q4<T> a) { return {s * a.x, s * a.y, s * a.z, s * a.w}; }
+template <typename T> inline V3<T> qvec(Q4<T> a) { return {a.x, a.y, a.z}; }
+template <typename T> inline Q4<T> qconj(Q4<T> a) { return {-a.x, -a.y, -a.z, a.w}; }  // Rotor::inverse, Rotor.h:109
+
+// Rotor product, Rotor.h:210-212.
+template <typename T>
+inline Q4<T> qmul(Q4<T> l, Q4<T> r) {
+    V3<T> q = l.w * qvec(r) + r.w * qvec(l) + cross(qvec(l), qvec(r));
+    return {q.x, q.y, q.z, l.w * r.w - dot(qvec(l), qvec(r))};
+}
+
+// Rotor::rotate, Rotor.h:114-123.
+template <typename T>
+inline V3<T> qrotate(Q4<T> r, V3<T> v) {
+    V3<T> qv = qvec(r);
+    V3<T> a = r.w * v + cross(qv, v);
+    T c = dot(v, qv);
+    return r.w * a + cross(qv, a) + c * qv;
+}
+
+template <typename T>
+inline V3<T> normalize3(V3<T> a) {  // glm::normalize: v * inversesqrt(dot(v, v))
+    T s = T(1) / std::sqrt(dot(a, a));
+    return a * s;
+}
+template <typename T>
+inline Q4<T> normalize4(Q4<T> a) {
+    T s = T(1) / std::sqrt(dot4(a, a));
+    return qscale(s, a);
+}
+
+// Rotor::fromTo, Rotor.h:79-88, with orthoBasisX (KittenEngine Common.h:220-232).
+template <typename T>
+inline Q4<T> fromTo(V3<T> from, V3<T> to) {
+    V3<T> h = (from + to) * T(0.5);
+    T l = dot(h, h);
+    if (l > 0) {
+        h = h * (T(1) / std::sqrt(l));
+    } else {
+        V3<T> n = from;
+        if (n.z >= n.y) {
+            T a = T(1) / (T(1) + n.z);
+            T b = -n.x * n.y * a;
+            h = v3<T>(b, T(1) - n.y * n.y * a, -n.y);
+        } else {
+            T a = T(1) / (T(1) + n.y);
+            T b = -n.x * n.z * a;
+            h = v3<T>(T(1) - n.x * n.x * a, -n.x, b);
+        }
+    }
+    V3<T> c = cross(from, h);
+    return {c.x, c.y, c.z, dot(from, h)};
+}
+
+// glm::inverse(mat3) (extern/glm/glm/detail/func_matrix.inl compute_inverse<3,3>) applied to
+// a packed symmetric hess3 converted with hess3::operator mat3 (SymMat.h:66-75), then mat3*vec3.
+template <typename T>
+inline V3<T> solveHess3(const T H[6], V3<T> f) {
+    T m[3][3];  // m[col][row]
+    m[0][0] = H[0];
+    m[1][1] = H[1];
+    m[2][2] = H[2];
+    m[0][1] = m[1][0] = H[3];
+    m[0][2] = m[2][0] = H[4];
+    m[1][2] = m[2][1] = H[5];
+    T det = +m[0][0] * (m[1][1] * m[2][2] - m[2][1] * m[1][2]) - m[1][0] * (m[0][1] * m[2][2] - m[2][1] * m[0][2]) +
+            m[2][0] * (m[0][1] * m[1][2] - m[1][1] * m[0][2]);
+    T od = T(1) / det;
+    T inv[3][3];
+    inv[0][0] = +(m[1][1] * m[2][2] - m[2][1] * m[1][2]) * od;
+    inv[1][0] = -(m[1][0] * m[2][2] - m[2][0] * m[1][2]) * od;
+    inv[2][0] = +(m[1][0] * m[2][1] - m[2][0] * m[1][1]) * od;
+    inv[0][1] = -(m[0][1] * m[2][2] - m[2][1] * m[0][2]) * od;
+    inv[1][1] = +(m[0][0] * m[2][2] - m[2][0] * m[0][2]) * od;
+    inv[2][1] = -(m[0][0] * m[2][1] - m[2][0] * m[0][1]) * od;
+    inv[0][2] = +(m[0][1] * m[1][2] - m[1][1] * m[0][2]) * od;
+    inv[1][2] = -(m[0][0] * m[1][2] - m[1][0] * m[0][2]) * od;
+    inv[2][2] = +(m[0][0] * m[1][1] - m[1][0] * m[0][1]) * od;
+    return {inv[0][0] * f.x + inv[1][0] * f.y + inv[2][0] * f.z, inv[0][1] * f.x + inv[1][1] * f.y + inv[2][1] * f.z,
+            inv[0][2] * f.x + inv[1][2] * f.y + inv[2][2] * f.z};
+}
+
+template <typename T> inline V3<T> ld3(const T* a, int64_t i) { return {a[3 * i], a[3 * i + 1], a[3 * i + 2]}; }
+template <typename T> inline void st3(T* a, int64_t i, V3<T> v) { a[3 * i] = v.x; a[3 * i + 1] = v.y; a[3 * i + 2] = v.z; }
+template <typename T> inline Q4<T> ld4(const T* a, int64_t i) { return {a[4 * i], a[4 * i + 1], a[4 * i + 2], a[4 * i + 3]}; }
+template <typename T> inline void st4(T* a, int64_t i, Q4<T> q) { a[4 * i] = q.x; a[4 * i + 1] = q.y; a[4 * i + 2] = q.z; a[4 * i + 3] = q.w; }
+
+}  // namespace
+
+extern "C" {
+
+// Parameters of one solver instance (scalars of YarnBall::MetaData, YarnBall.h:61-124,
+// plus the SDFSimulationParams of cudaSDFCollision.cuh:23-48 that the SDF pass reads).
+typedef struct oracle_params {
+    float gravity[3];
+    float damping;            // MetaData::damping (1e-6)
+    float velocity_decay;     // MetaData::velocityDecay
+    float acceleration_ratio; // MetaData::accelerationRatio (1)
+    float ext_mult;           // MetaData::ExternalForceMultiplier
+    float wind_peak, wind_y_freq, wind_z_freq, wind_time_freq, wind_sharpness;
+    int32_t num_itr;
+    int32_t schedule;  // 0 = colour2 Gauss-Seidel, 1 = jacobi
+    float max_h;       // Sim::maxH
+    int32_t sdf_enabled;
+    int32_t sdf_dims[3];
+    float sdf_min[3];
+    float sdf_max[3];
+    float sdf_threshold;
+    const float* sdf_phi;   // [nz][ny][nx]
+    const float* sdf_grad;  // [nz][ny][nx][3]
+    float body_rot[4];      // (x, y, z, w)
+    float body_trans[3];
+    int32_t num_threads;    // <= 0: OpenMP default
+} oracle_params;
+
+}  // extern "C"
+
+namespace {
+
+template <typename T>
+struct Topology {
+    int64_t nv;
+    int32_t ns;
+    const int32_t* sb;
+    std::vector<int32_t> local;  // local index of each vertex inside its strand
+    Topology(int64_t nv_, int32_t ns_, const int32_t* sb_) : nv(nv_), ns(ns_), sb(sb_), local(nv_) {
+        for (int32_t s = 0; s < ns; s++)
+            for (int32_t i = sb[s]; i < sb[s + 1]; i++) local[i] = i - sb[s];
+    }
+};
+
+// createFromCurves (YarnBall/io/reader.cpp:16-50) + Sim::Sim (YBSimulator.cu:81-127) +
+// Sim::configure (YBSimulator.cu:161-241) + setYoung (:300-320) / setKStretch (:276-284) /
+// setKBend (:286-298) + root pinning (StableCosseratRods/StableCosseratRodsSolver.cpp:203-205).
+// strand_young / strand_dev give one Young's modulus [GPa] / bend deviation per strand; the
+// reference's setYoung applies a single pair to every vertex, and a per-strand pair is the same
+// formula applied strand by strand.
+template <typename T>
+int configureT(int64_t nv, int32_t ns, const int32_t* sb, const float* pos, float radius, float density,
+               int32_t stiffness_mode, const float* strand_young, const float* strand_dev, float k_stretch_in,
+               float k_bend_in, int32_t pin_roots, T* inv_mass, T* l_rest, T* k_stretch, uint32_t* flags, T* q,
+               T* q_rest) {
+    if (nv < 3) return 1;  // Sim::Sim throws "Too little vertices"
+    std::vector<uint32_t> fl(nv, HAS_NEXT);
+    fl[nv - 1] = 0;
+    for (int32_t s = 0; s < ns; s++) fl[sb[s + 1] - 1] = 0;  // cut off each curve end
+    std::vector<T> im(nv, T(1)), lr(nv, T(1));
+    std::vector<Q4<T>> qs(nv);
+    Q4<T> lastQ = {0, 0, 0, 1};
+    const T r = (T)radius;
+    for (int64_t i = 0; i < nv; i++) {
+        if (i < nv - 1) {
+            bool hasNext = (fl[i] & HAS_NEXT) != 0;
+            fl[i + 1] = hasNext ? (fl[i + 1] | HAS_PREV) : (fl[i + 1] & ~HAS_PREV);
+            bool hasNextNext = hasNext && (fl[i + 1] & HAS_NEXT);
+            fl[i] = hasNextNext ? (fl[i] | HAS_NEXT_ORIENTATION) : (fl[i] & ~HAS_NEXT_ORIENTATION);
+            if (!hasNext) fl[i] |= FIX_ORIENTATION;
+        }
+        if (!(fl[i] & HAS_PREV) && !(fl[i] & HAS_NEXT)) return 2;  // dangling segment
+        lr[i] = T(1) / (T)nv;
+        T mass = 0;
+        if (fl[i] & HAS_PREV) mass += lr[i - 1];
+        if (fl[i] & HAS_NEXT) {
+            V3<T> p0 = v3<T>(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+            V3<T> p1 = v3<T>(pos[3 * i + 3], pos[3 * i + 4], pos[3 * i + 5]);
+            V3<T> seg = p1 - p0;
+            lr[i] = length(seg);
+            if (lr[i] == 0 || !std::isfinite((double)lr[i])) return 3;  // 0 length segment
+            lastQ = fromTo<T>(v3<T>(1, 0, 0), normalize3(seg));
+            mass += lr[i];
+        }
+        qs[i] = lastQ;
+        // mass = (l_{i-1} + l_i) r^2 pi rho / 2, YBSimulator.cu:227-229
+        mass = (T)((double)mass * ((double)(r * r) * kPi * (double)density * 0.5));
+        if (mass != 0)
+            im[i] *= T(1) / mass;
+        else
+            im[i] = 0;
+    }
+    std::vector<Q4<T>> qr(nv, Q4<T>{0, 0, 0, 1});
+    for (int64_t i = 0; i < nv - 1; i++) qr[i] = normalize4(qmul(qconj(qs[i]), qs[i + 1]));
+    std::vector<T> ks(nv, T(100));
+    // strand of each vertex
+    std::vector<int32_t> strandOf(nv, 0);
+    for (int32_t s = 0; s < ns; s++)
+        for (int32_t i = sb[s]; i < sb[s + 1]; i++) strandOf[i] = s;
+    if (stiffness_mode == 0) {
+        const T mmrad = (T)radius * T(1000);
+        for (int64_t i = 0; i < nv; i++) {
+            T young = (T)strand_young[strandOf[i]];
+            T dev = (T)strand_dev[strandOf[i]];
+            T len = lr[i];
+            T ss = (T)((double)young * kPi * (double)mmrad * (double)mmrad);
+            T bt = (T)((double)(ss * dev * mmrad * mmrad) * 0.25 / (double)(len * len));
+            ks[i] = ss;
+            qr[i] = qscale(bt, qr[i]);
+        }
+    } else {
+        for (int64_t i = 0; i < nv; i++) {
+            T kb = (T)k_bend_in * T(4);
+            qr[i] = qscale(kb / lr[i], normalize4(qr[i]));
+            ks[i] = (T)k_stretch_in * lr[i];
+        }
+    }
+    if (pin_roots)
+        for (int32_t s = 0; s < ns; s++) im[sb[s]] = 0;
+    for (int64_t i = 0; i < nv; i++) {
+        inv_mass[i] = im[i];
+        l_rest[i] = lr[i];
+        k_stretch[i] = ks[i];
+        flags[i] = fl[i];
+        st4(q, i, qs[i]);
+        st4(q_rest, i, qr[i]);
+    }
+    return 0;
+}
+
+template <typename T>
+struct StepCtx {
+    const oracle_params* p;
+    int64_t nv;
+    const T* im;
+    const T* lr;
+    const T* ks;
+    const uint32_t* fl;
+    const T* qr;
+    const int32_t* local;
+    T* x;
+    T* v;
+    T* vl;
+    T* q;
+    std::vector<T> y, dx, dxNew, qNew;
+};
+
+// initItr, YarnBall/sim/iteration.cu:8-59.  y - x is kept in ctx.y (the reference keeps it in d_vels).
+template <typename T>
+void predict(StepCtx<T>& c, T h, T lastH, T time) {
+    const oracle_params* p = c.p;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < c.nv; i++) {
+        V3<T> g = v3<T>(p->gravity[0], p->gravity[1], p->gravity[2]);
+        V3<T> vel = ld3(c.v, i);
+        T windx = 0;
+        if (p->wind_peak != 0) {
+            T ypos = c.x[3 * i + 1], zpos = c.x[3 * i + 2];
+            T wy = ypos > 0 ? (T)std::cos(2 * M_PI * (double)((T)p->wind_y_freq * ypos + (T)p->wind_time_freq * time)) : T(0);
+            T wz = (T)std::cos(2 * M_PI * (double)((T)p->wind_z_freq * std::abs(zpos) + (T)p->wind_time_freq * time));
+            T prod = wy * wz;
+            T sg = prod > 0 ? T(1) : (prod < 0 ? T(-1) : T(0));
+            T pw = std::pow(prod, (T)p->wind_sharpness) * sg;
+            windx = (T)p->wind_peak * ((T(0) < pw) ? pw : T(0));
+        }
+        V3<T> ext = (g + v3<T>(windx, 0, 0)) * (T)p->ext_mult;
+        V3<T> dx = h * vel;
+        V3<T> lastVel = ld3(c.vl, i);
+        st3(c.vl, i, vel);
+        V3<T> y = vel;  // roots keep the velocity in d_vels
+        if (c.im[i] != 0) {
+            y = dx + (h * h) * ext;
+            T ext2 = dot(ext, ext);
+            if (ext2 > 0) {
+                V3<T> a = (vel - lastVel) / lastH;
+                T s = dot(a, ext) / ext2;
+                s = s < 0 ? T(0) : (s > 1 ? T(1) : s);
+                dx = dx + (h * h * s) * ext;
+            }
+        }
+        st3(c.y.data(), i, y);
+        st3(c.dx.data(), i, dx);
+    }
+}
+
+// cosseratItr, YarnBall/sim/cosserat.cu:112-161 and :246-285, for one vertex i, without the
+// hair-hair collision terms (:163-227; disabled on this path) and with the step limit at
+// infinity (recomputeStepLimitKernel<false,*>, collision.cu:95-131).  dxr is the dx array the
+// vertex reads.  Returns the new dx_i (or the old one when the vertex is pinned).
+template <typename T>
+V3<T> positionUpdate(const StepCtx<T>& c, const T* dxr, int64_t i, T h) {
+    const T damping = (T)c.p->damping / h;
+    V3<T> vi_dx = ld3(dxr, i);
+    if (c.im[i] == 0) return vi_dx;
+    T H[6];
+    T inert = T(1) / (c.im[i] * h * h);
+    for (int k = 0; k < 6; k++) H[k] = inert;  // hess3(float) fills all six entries (SymMat.h:16-18)
+    V3<T> f = (T(1) / (h * h * c.im[i])) * (ld3(c.y.data(), i) - vi_dx);
+    if (c.fl[i] & HAS_NEXT) {  // segment i, as thread i computes it (:141-161)
+        V3<T> xi = ld3(c.x, i), xj = ld3(c.x, i + 1), vj_dx = ld3(dxr, i + 1);
+        T invl = T(1) / c.lr[i];
+        V3<T> cc = ((xj - xi) + (vj_dx - vi_dx)) * invl - qrotate(ld4(c.q, i), v3<T>(1, 0, 0));
+        T k = c.ks[i] * invl;
+        T d = k * invl;
+        f = f + (k * cc - (damping * d) * vi_dx);
+        d *= 1 + damping;
+        H[0] += d;
+        H[1] += d;
+        H[2] += d;
+    }
+    if (c.fl[i] & HAS_PREV) {  // segment i-1, as thread i-1 computes f2/H2 and passes it on (:157, :269-274)
+        int64_t j = i - 1;
+        V3<T> xj = ld3(c.x, j), xi = ld3(c.x, i), dj = ld3(dxr, j);
+        T invl = T(1) / c.lr[j];
+        V3<T> cc = ((xi - xj) + (vi_dx - dj)) * invl - qrotate(ld4(c.q, j), v3<T>(1, 0, 0));
+        T k = c.ks[j] * invl;
+        T d = k * invl;
+        V3<T> f2 = -k * cc - (damping * d) * vi_dx;
+        d *= 1 + damping;
+        f = f + f2;
+        H[0] += d;
+        H[1] += d;
+        H[2] += d;
+    }
+    V3<T> delta = (T)c.p->acceleration_ratio * solveHess3(H, f);
+    return vi_dx + delta;
+}
+
+// quaternionLambdaItr, YarnBall/sim/cosserat.cu:290-337, for one segment i.  qr_ is the q array
+// it reads.  Returns the new q_i (or the old one when the segment is not updated).
+template <typename T>
+Q4<T> quaternionUpdate(const StepCtx<T>& c, const T* qread, int64_t i) {
+    Q4<T> vi_q = ld4(qread, i);
+    uint32_t fl = c.fl[i];
+    if (!(!(fl & FIX_ORIENTATION) && (fl & HAS_NEXT))) return vi_q;
+    V3<T> vi_dx = ld3(c.dx.data(), i);
+    V3<T> vj_pos = ld3(c.x, i + 1);
+    V3<T> vj_dx = ld3(c.dx.data(), i + 1);
+    V3<T> vp = ((vj_pos - ld3(c.x, i)) + (vj_dx - vi_dx)) / c.lr[i];
+    vp = vp * (T(-2) * c.ks[i]);
+    Q4<T> b = {0, 0, 0, 0};
+    if (fl & HAS_PREV) {
+        Q4<T> qRest = ld4(c.qr, i - 1);
+        Q4<T> vj_q = ld4(qread, i - 1);
+        T phi = dot4(qmul(qconj(vj_q), vi_q), qRest) > 0 ? T(1) : T(-1);
+        b = qadd(b, qscale(phi, qmul(vj_q, qRest)));
+    }
+    if (fl & HAS_NEXT_ORIENTATION) {
+        Q4<T> qRest = ld4(c.qr, i);
+        Q4<T> vj_q = ld4(qread, i + 1);
+        T phi = dot4(qmul(qconj(vi_q), vj_q), qRest) > 0 ? T(1) : T(-1);
+        b = qadd(b, qscale(phi, qmul(vj_q, qconj(qRest))));
+    }
+    T lambda = length(vp) + length4(b);
+    Q4<T> V = {vp.x, vp.y, vp.z, 0};
+    Q4<T> E = {1, 0, 0, 0};
+    Q4<T> r = qadd(qmul(qmul(V, b), E), qscale(lambda, b));
+    return normalize4(r);
+}
+
+// endItr, YarnBall/sim/iteration.cu:62-74.
+template <typename T>
+void finish(StepCtx<T>& c, T h) {
+    const T invH = T(1) / h;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < c.nv; i++) {
+        V3<T> dx = ld3(c.dx.data(), i);
+        if (c.im[i] != 0) st3(c.v, i, dx * invH * (T(1) - (T)c.p->velocity_decay * h));
+        st3(c.x, i, ld3(c.x, i) + dx);
+    }
+}
+
+// SDFHeadCollision + TriInterpSDF + index helpers, SDFCollisionSolver/cudaSDFCollision.cu:88-155 and
+// :205-268; grid spacing from SDFBodyCollisionSolver::InitParams (SDFBodyCollisionSolver.cpp:46-82).
+template <typename T>
+void sdfProject(StepCtx<T>& c) {
+    const oracle_params* p = c.p;
+    const int nx = p->sdf_dims[0], ny = p->sdf_dims[1], nz = p->sdf_dims[2];
+    T ds[3], invDs[3];
+    for (int a = 0; a < 3; a++) {
+        ds[a] = ((T)p->sdf_max[a] - (T)p->sdf_min[a]) / ((T)1 * (T)p->sdf_dims[a]);
+        invDs[a] = T(1) / ds[a];
+    }
+    const Q4<T> invq = {-(T)p->body_rot[0], -(T)p->body_rot[1], -(T)p->body_rot[2], (T)p->body_rot[3]};
+    const V3<T> tr = v3<T>(p->body_trans[0], p->body_trans[1], p->body_trans[2]);
+    const V3<T> gmin = v3<T>(p->sdf_min[0], p->sdf_min[1], p->sdf_min[2]);
+    const T thresh = (T)p->sdf_threshold;
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < c.nv; i++) {
+        if (c.local[i] == 0) continue;  // strand root
+        V3<T> pos = ld3(c.x, i);
+        V3<T> lp = qrotate(invq, pos - tr) - gmin;
+        int idx[3];
+        T lpa[3] = {lp.x, lp.y, lp.z};
+        for (int a = 0; a < 3; a++) idx[a] = (int)((double)(lpa[a] * invDs[a]) + 0.5);
+        if (idx[0] < 0 || idx[0] >= nx || idx[1] < 0 || idx[1] >= ny || idx[2] < 0 || idx[2] >= nz) continue;
+        T corner[2][2][2][4];
+        for (int dz = 0; dz < 2; dz++)
+            for (int dy = 0; dy < 2; dy++)
+                for (int dx = 0; dx < 2; dx++) {
+                    int cx = idx[0] + dx, cy = idx[1] + dy, cz = idx[2] + dz;
+                    bool inside = cx >= 0 && cx < nx && cy >= 0 && cy < ny && cz >= 0 && cz < nz;
+                    int qx = std::max(0, std::min(cx, nx - 1)), qy = std::max(0, std::min(cy, ny - 1)),
+                        qz = std::max(0, std::min(cz, nz - 1));
+                    int64_t li = (int64_t)qx + (int64_t)qy * nx + (int64_t)qz * nx * ny;
+                    int64_t gi = (int64_t)cx + (int64_t)cy * nx + (int64_t)cz * nx * ny;
+                    for (int a = 0; a < 3; a++) corner[dz][dy][dx][a] = inside ? (T)p->sdf_grad[3 * gi + a] : T(0);
+                    corner[dz][dy][dx][3] = (T)p->sdf_phi[li];
+                }
+        T ud[3];
+        for (int a = 0; a < 3; a++) ud[a] = (T)((double)invDs[a] * ((double)lpa[a] - ((double)idx[a] - 0.5) * (double)ds[a]));
+        T res[4];
+        for (int k = 0; k < 4; k++) {
+            T c00 = corner[0][0][0][k] * (T(1) - ud[0]) + corner[0][0][1][k] * ud[0];
+            T c01 = corner[1][0][0][k] * (T(1) - ud[0]) + corner[1][0][1][k] * ud[0];
+            T c10 = corner[0][1][0][k] * (T(1) - ud[0]) + corner[0][1][1][k] * ud[0];
+            T c11 = corner[1][1][0][k] * (T(1) - ud[0]) + corner[1][1][1][k] * ud[0];
+            T c0 = c00 * (T(1) - ud[1]) + c10 * ud[1];
+            T c1 = c01 * (T(1) - ud[1]) + c11 * ud[1];
+            res[k] = c0 * (T(1) - ud[2]) + c1 * ud[2];
+        }
+        V3<T> n = normalize3(v3<T>(res[0], res[1], res[2]));
+        T phi = res[3] - thresh;
+        if (phi < 0) {
+            st3(c.x, i, pos - phi * n);
+            V3<T> vel = ld3(c.v, i);
+            T vl = length(vel);
+            if (vl >= T(1e-6)) {
+                V3<T> vn = vel / vl;
+                st3(c.v, i, vel - dot(vn, n) * n);
+            }
+        }
+    }
+}
+
+// Sim::advance (YarnBall/sim/step.cpp:38-62) followed by the SDF pass that
+// StableCosseratRodsSolver::SolveNextStep runs after it (StableCosseratRodsSolver.cpp:216-234).
+// clock = {meta.h, meta.lastH, meta.time}; updated in place.
+template <typename T>
+int advanceT(const oracle_params* p, int64_t nv, int32_t ns, const int32_t* sb, const T* im, const T* lr,
+             const T* ks, const uint32_t* fl, const T* qr, T* x, T* v, T* vl, T* q, double* clock, float dt) {
+#ifdef _OPENMP
+    if (p->num_threads > 0) omp_set_num_threads(p->num_threads);
+#endif
+    if (dt <= 0) return 0;
+    Topology<T> topo(nv, ns, sb);
+    int steps = std::max(1, (int)std::ceil(dt / p->max_h));
+    T lastH = (T)clock[0];
+    T h = (T)(dt / (float)steps);
+    if (sizeof(T) == 8) h = (T)((double)dt / (double)steps);
+    T time = (T)clock[2];
+    StepCtx<T> c;
+    c.p = p;
+    c.nv = nv;
+    c.im = im;
+    c.lr = lr;
+    c.ks = ks;
+    c.fl = fl;
+    c.qr = qr;
+    c.local = topo.local.data();
+    c.x = x;
+    c.v = v;
+    c.vl = vl;
+    c.q = q;
+    c.y.assign(3 * nv, T(0));
+    c.dx.assign(3 * nv, T(0));
+    c.dxNew.assign(3 * nv, T(0));
+    c.qNew.assign(4 * nv, T(0));
+    for (int s = 0; s < steps; s++) {
+        predict(c, h, lastH, time);
+        for (int it = 0; it < p->num_itr; it++) {
+            if (p->schedule == 1) {
+#pragma omp parallel for schedule(static)
+                for (int64_t i = 0; i < nv; i++) st3(c.dxNew.data(), i, positionUpdate(c, c.dx.data(), i, h));
+                std::swap(c.dx, c.dxNew);
+#pragma omp parallel for schedule(static)
+                for (int64_t i = 0; i < nv; i++) st4(c.qNew.data(), i, quaternionUpdate(c, c.q, i));
+                std::memcpy(c.q, c.qNew.data(), sizeof(T) * 4 * nv);
+            } else {
+                for (int colour = 0; colour < 2; colour++) {
+#pragma omp parallel for schedule(static)
+                    for (int64_t i = 0; i < nv; i++)
+                        if ((topo.local[i] & 1) == colour) st3(c.dx.data(), i, positionUpdate(c, c.dx.data(), i, h));
+                }
+                for (int colour = 0; colour < 2; colour++) {
+#pragma omp parallel for schedule(static)
+                    for (int64_t i = 0; i < nv; i++)
+                        if ((topo.local[i] & 1) == colour) st4(c.q, i, quaternionUpdate(c, c.q, i));
+                }
+            }
+        }
+        finish(c, h);
+    }
+    if (p->sdf_enabled) sdfProject(c);
+    clock[0] = (double)h;
+    clock[1] = (double)lastH;
+    clock[2] = (double)((T)clock[2] + (T)dt);
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int oracle_configure_f32(int64_t nv, int32_t ns, const int32_t* sb, const float* pos, float radius, float density,
+                         int32_t stiffness_mode, const float* strand_young, const float* strand_dev, float k_stretch,
+                         float k_bend, int32_t pin_roots, float* inv_mass, float* l_rest, float* k_stretch_out,
+                         uint32_t* flags, float* q, float* q_rest) {
+    return configureT<float>(nv, ns, sb, pos, radius, density, stiffness_mode, strand_young, strand_dev, k_stretch,
+                             k_bend, pin_roots, inv_mass, l_rest, k_stretch_out, flags, q, q_rest);
+}
+
+int oracle_configure_f64(int64_t nv, int32_t ns, const int32_t* sb, const float* pos, float radius, float density,
+                         int32_t stiffness_mode, const float* strand_young, const float* strand_dev, float k_stretch,
+                         float k_bend, int32_t pin_roots, double* inv_mass, double* l_rest, double* k_stretch_out,
+                         uint32_t* flags, double* q, double* q_rest) {
+    return configureT<double>(nv, ns, sb, pos, radius, density, stiffness_mode, strand_young, strand_dev, k_stretch,
+                              k_bend, pin_roots, inv_mass, l_rest, k_stretch_out, flags, q, q_rest);
+}
+
+int oracle_advance_f32(const oracle_params* p, int64_t nv, int32_t ns, const int32_t* sb, const float* im,
+                       const float* lr, const float* ks, const uint32_t* fl, const float* qr, float* x, float* v,
+                       float* vl, float* q, double* clock, float dt) {
+    return advanceT<float>(p, nv, ns, sb, im, lr, ks, fl, qr, x, v, vl, q, clock, dt);
+}
+
+int oracle_advance_f64(const oracle_params* p, int64_t nv, int32_t ns, const int32_t* sb, const double* im,
+                       const double* lr, const double* ks, const uint32_t* fl, const double* qr, double* x, double* v,
+                       double* vl, double* q, double* clock, float dt) {
+    return advanceT<double>(p, nv, ns, sb, im, lr, ks, fl, qr, x, v, vl, q, clock, dt);
+}
+
+int oracle_num_threads(void) {
+#ifdef _OPENMP
+    return omp_get_max_threads();
+#else
+    return 1;
+#endif
+}
+
+}  // extern "C"

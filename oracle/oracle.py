@@ -1,0 +1,187 @@
+"""ctypes front-end of the CPU oracle -- TEST INFRASTRUCTURE ONLY.
+
+The oracle (oracle/kami_oracle.cpp) restates the reference's Stable Cosserat Rods
+VBD step on the CPU, in FP32 or FP64.  Only tests/, __graft_entry__.smoke() and
+bench.py's CPU-baseline leg use this module, always as the checker.
+
+``OracleSim`` mirrors YarnBall::Sim as StableCosseratRodsSolver drives it
+(src/solvers/StableCosseratRods/StableCosseratRodsSolver.cpp:112-234):
+construct from curves, configure, setYoung, pin roots, then advance(dt) + SDF pass.
+"""
+from __future__ import annotations
+
+import ctypes
+import os
+import subprocess
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+_LIB_PATH = os.path.join(_HERE, "_build", "libkami_oracle.so")
+_lib = None
+
+SCHEDULES = {"colour2": 0, "jacobi": 1}
+
+HAS_PREV, HAS_NEXT, HAS_NEXT_ORIENTATION, FIX_ORIENTATION = 1, 2, 4, 8
+
+
+class OracleParams(ctypes.Structure):
+    _fields_ = [
+        ("gravity", ctypes.c_float * 3),
+        ("damping", ctypes.c_float),
+        ("velocity_decay", ctypes.c_float),
+        ("acceleration_ratio", ctypes.c_float),
+        ("ext_mult", ctypes.c_float),
+        ("wind_peak", ctypes.c_float),
+        ("wind_y_freq", ctypes.c_float),
+        ("wind_z_freq", ctypes.c_float),
+        ("wind_time_freq", ctypes.c_float),
+        ("wind_sharpness", ctypes.c_float),
+        ("num_itr", ctypes.c_int32),
+        ("schedule", ctypes.c_int32),
+        ("max_h", ctypes.c_float),
+        ("sdf_enabled", ctypes.c_int32),
+        ("sdf_dims", ctypes.c_int32 * 3),
+        ("sdf_min", ctypes.c_float * 3),
+        ("sdf_max", ctypes.c_float * 3),
+        ("sdf_threshold", ctypes.c_float),
+        ("sdf_phi", ctypes.c_void_p),
+        ("sdf_grad", ctypes.c_void_p),
+        ("body_rot", ctypes.c_float * 4),
+        ("body_trans", ctypes.c_float * 3),
+        ("num_threads", ctypes.c_int32),
+    ]
+
+
+def build():
+    subprocess.run(["make", "-s", "-C", _HERE], check=True)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        if not os.path.exists(_LIB_PATH):
+            build()
+        lib = ctypes.CDLL(_LIB_PATH)
+        for suffix, ct in (("f32", ctypes.c_float), ("f64", ctypes.c_double)):
+            fn = getattr(lib, f"oracle_configure_{suffix}")
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.c_int64, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float,
+                           ctypes.c_float, ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float,
+                           ctypes.c_float, ctypes.c_int32] + [ctypes.c_void_p] * 6
+            fn = getattr(lib, f"oracle_advance_{suffix}")
+            fn.restype = ctypes.c_int
+            fn.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_int64, ctypes.c_int32] + [ctypes.c_void_p] * 11 + [
+                ctypes.c_float]
+        lib.oracle_num_threads.restype = ctypes.c_int
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p) if a is not None else None
+
+
+def configure(groom, radius=40e-6, density=1300.0, stiffness_mode=0, k_stretch=3e3, k_bend=6e-4, pin_roots=True,
+              dtype=np.float32):
+    """Per-vertex material arrays exactly as Sim::configure + setYoung produce them."""
+    lib = load()
+    nv = groom.num_vertices
+    ns = groom.num_strands
+    sb = np.ascontiguousarray(groom.strand_begin, np.int32)
+    pos = np.ascontiguousarray(groom.positions, np.float32)
+    young = np.ascontiguousarray(groom.strand_young, np.float32)
+    dev = np.ascontiguousarray(groom.strand_dev, np.float32)
+    out = dict(inv_mass=np.zeros(nv, dtype), l_rest=np.zeros(nv, dtype), k_stretch=np.zeros(nv, dtype),
+               flags=np.zeros(nv, np.uint32), q=np.zeros((nv, 4), dtype), q_rest=np.zeros((nv, 4), dtype))
+    fn = lib.oracle_configure_f32 if dtype == np.float32 else lib.oracle_configure_f64
+    rc = fn(nv, ns, _p(sb), _p(pos), radius, density, stiffness_mode, _p(young), _p(dev), k_stretch, k_bend,
+            int(pin_roots), _p(out["inv_mass"]), _p(out["l_rest"]), _p(out["k_stretch"]), _p(out["flags"]),
+            _p(out["q"]), _p(out["q_rest"]))
+    if rc != 0:
+        raise ValueError(f"oracle configure failed with code {rc}")
+    return out
+
+
+class OracleSim:
+    """YarnBall::Sim + the SDF pass, restated on the CPU in FP32 or FP64."""
+
+    def __init__(self, groom, *, num_itr=10, max_h=None, gravity=(0.0, 0.0, -9.81), radius=40e-6, density=1300.0,
+                 damping=1e-6, velocity_decay=0.05, acceleration_ratio=1.0, ext_mult=1.0, wind=(0.0, 0.0, 0.0, 0.0, 3.0),
+                 schedule="colour2", sdf=None, body_rot=(0.0, 0.0, 0.0, 1.0), body_trans=(0.0, 0.0, 0.0),
+                 stiffness_mode=0, k_stretch=3e3, k_bend=6e-4, pin_roots=True, dtype=np.float32, num_threads=0,
+                 velocities=None):
+        self.dtype = dtype
+        self.lib = load()
+        self.groom = groom
+        self.nv = groom.num_vertices
+        self.ns = groom.num_strands
+        self.sb = np.ascontiguousarray(groom.strand_begin, np.int32)
+        m = configure(groom, radius, density, stiffness_mode, k_stretch, k_bend, pin_roots, dtype)
+        self.inv_mass, self.l_rest, self.k_stretch = m["inv_mass"], m["l_rest"], m["k_stretch"]
+        self.flags, self.q, self.q_rest = m["flags"], m["q"], m["q_rest"]
+        self.x = np.ascontiguousarray(groom.positions, dtype).copy()
+        self.v = np.zeros((self.nv, 3), dtype) if velocities is None else np.ascontiguousarray(velocities, dtype).copy()
+        self.v_last = np.zeros((self.nv, 3), dtype)
+        max_h = 4e-4 if max_h is None else max_h
+        # meta.h starts at maxH (YBSimulator.cu:85), lastH is taken from it on the first advance
+        self.clock = np.array([np.float32(max_h), 0.0, 0.0], np.float64)
+        p = OracleParams()
+        p.gravity[:] = gravity
+        p.damping, p.velocity_decay, p.acceleration_ratio, p.ext_mult = damping, velocity_decay, acceleration_ratio, ext_mult
+        p.wind_peak, p.wind_y_freq, p.wind_z_freq, p.wind_time_freq, p.wind_sharpness = wind
+        p.num_itr = num_itr
+        p.schedule = SCHEDULES[schedule]
+        p.max_h = max_h
+        p.num_threads = num_threads
+        self._sdf_keep = None
+        if sdf is not None:
+            phi = np.ascontiguousarray(sdf.phi, np.float32)
+            grad = np.ascontiguousarray(sdf.grad, np.float32)
+            self._sdf_keep = (phi, grad)
+            p.sdf_enabled = 1
+            p.sdf_dims[:] = sdf.dims
+            p.sdf_min[:] = sdf.grid_min
+            p.sdf_max[:] = sdf.grid_max
+            p.sdf_threshold = sdf.threshold
+            p.sdf_phi = phi.ctypes.data
+            p.sdf_grad = grad.ctypes.data
+        p.body_rot[:] = body_rot
+        p.body_trans[:] = body_trans
+        self.params = p
+
+    def set_body_transform(self, rot, trans):
+        self.params.body_rot[:] = rot
+        self.params.body_trans[:] = trans
+
+    def advance(self, dt):
+        fn = self.lib.oracle_advance_f32 if self.dtype == np.float32 else self.lib.oracle_advance_f64
+        rc = fn(ctypes.byref(self.params), self.nv, self.ns, _p(self.sb), _p(self.inv_mass), _p(self.l_rest),
+                _p(self.k_stretch), _p(self.flags), _p(self.q_rest), _p(self.x), _p(self.v), _p(self.v_last),
+                _p(self.q), _p(self.clock), dt)
+        if rc != 0:
+            raise RuntimeError(f"oracle advance failed with code {rc}")
+
+    def state(self):
+        return dict(x=self.x.copy(), v=self.v.copy(), v_last=self.v_last.copy(), q=self.q.copy(),
+                    clock=self.clock.copy())
+
+    def load_state(self, st):
+        self.x[...] = st["x"]
+        self.v[...] = st["v"]
+        self.v_last[...] = st["v_last"]
+        self.q[...] = st["q"]
+        self.clock[...] = st["clock"]
+
+
+def twist_angles(q_ref, q_new):
+    """Twist of q_new relative to q_ref about the material axis e_x: 2 atan2(dq.xyz . e_x, dq.w), dq = q_ref^-1 q_new."""
+    a = np.asarray(q_ref, np.float64)
+    b = np.asarray(q_new, np.float64)
+    ax, ay, az, aw = -a[:, 0], -a[:, 1], -a[:, 2], a[:, 3]
+    bx, by, bz, bw = b[:, 0], b[:, 1], b[:, 2], b[:, 3]
+    # (conj(a) * b).x and .w
+    dx = aw * bx + bw * ax + (ay * bz - by * az)
+    dw = aw * bw - (ax * bx + ay * by + az * bz)
+    ang = 2.0 * np.arctan2(dx, dw)
+    return (ang + np.pi) % (2.0 * np.pi) - np.pi

@@ -1,0 +1,108 @@
+"""CPU tests of the C-ABI library: it loads, exports every declared symbol, and rejects bad input
+on the host before touching a device."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from kamisimulator_b200 import synth, vbd
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_symbols():
+    names = []
+    for fname in sorted(os.listdir(os.path.join(ROOT, "include"))):
+        if fname.endswith(".h"):
+            text = open(os.path.join(ROOT, "include", fname)).read()
+            names += re.findall(r"^\s*(?:const\s+)?[a-z_]+\*?\s+\**(kami_\w+)\s*\(", text, re.M)
+    return names
+
+
+def test_library_exports_every_declared_symbol():
+    lib = vbd.load_library()
+    names = declared_symbols()
+    assert len(names) >= 18
+    for n in names:
+        assert hasattr(lib, n), n
+    assert set(vbd.EXPORTED) <= set(names)
+
+
+def test_version_and_defaults():
+    assert "sm_100a" in vbd.version()
+    lib = vbd.load_library()
+    d = vbd.Desc()
+    assert lib.kami_vbd_desc_init(ctypes.byref(d)) == 0
+    # JsonParams() defaults (StableCosseratRodsSolver.h:86-111), Sim defaults (YBSimulator.cu:81-111)
+    assert d.num_itr == 8
+    assert d.velocity_decay == pytest.approx(0.05)
+    assert d.radius == pytest.approx(4e-5)
+    assert d.density == pytest.approx(1300.0)
+    assert d.young == pytest.approx(5.0)
+    assert d.damping == pytest.approx(1e-6)
+    assert d.max_h == pytest.approx(4e-4)
+    assert d.wind_peak == 0.0
+    assert d.pin_roots == 1
+
+
+def _create(desc):
+    lib = vbd.load_library()
+    h = ctypes.c_void_p()
+    rc = lib.kami_vbd_create(ctypes.byref(desc) if desc is not None else None, ctypes.byref(h))
+    return rc, lib.kami_vbd_last_error_string().decode()
+
+
+def _desc(groom, keep):
+    lib = vbd.load_library()
+    d = vbd.Desc()
+    lib.kami_vbd_desc_init(ctypes.byref(d))
+    sb = np.ascontiguousarray(groom.strand_begin, np.int32)
+    pos = np.ascontiguousarray(groom.positions, np.float32)
+    keep += [sb, pos]
+    d.num_strands = groom.num_strands
+    d.strand_begin = sb.ctypes.data
+    d.positions = pos.ctypes.data
+    return d
+
+
+def test_host_side_errors():
+    keep = []
+    rc, msg = _create(None)
+    assert rc == 1 and "null" in msg
+    g = synth.cantilever(4, 8)
+    d = _desc(g, keep)
+    d.schedule = 7
+    rc, msg = _create(d)
+    assert rc == 1 and "schedule" in msg
+    d = _desc(g, keep)
+    d.num_itr = -1
+    assert _create(d)[0] == 1
+    d = _desc(g, keep)
+    d.max_h = 0.0
+    assert _create(d)[0] == 1
+    # a one-vertex strand is a dangling segment (Sim::configure, YBSimulator.cu:185-186)
+    g1 = synth.Groom(np.array([0, 1, 9], np.int32), g.positions[:9].copy(), np.ones(2, np.float32),
+                     np.ones(2, np.float32))
+    rc, msg = _create(_desc(g1, keep))
+    assert rc == 5 and "dangling" in msg
+    # zero-length segment (YBSimulator.cu:197)
+    g2 = synth.cantilever(4, 8)
+    g2.positions[3] = g2.positions[2]
+    rc, msg = _create(_desc(g2, keep))
+    assert rc == 5 and "zero-length" in msg
+    # SDF descriptor checks
+    d = _desc(g, keep)
+    sd = vbd.SdfDesc()
+    sd.dims[:] = (4, 4, 0)
+    d.sdf = ctypes.pointer(sd)
+    assert _create(d)[0] == 1
+
+
+def test_null_handle_calls_fail_cleanly():
+    lib = vbd.load_library()
+    assert lib.kami_vbd_step(None, ctypes.c_float(0.01), None) == 1
+    assert lib.kami_vbd_destroy(None) == 0
+    n = ctypes.c_size_t()
+    assert lib.kami_vbd_state_size(None, ctypes.byref(n)) == 1
