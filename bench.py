@@ -1,0 +1,379 @@
+"""Benchmark of the Stable Cosserat Rods VBD step on B200.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+Headline workload: the synthetic groom of 10,000 strands x 64 vertices (roots on the upper
+hemisphere of a 0.09 m head sphere, helical curl, per-strand E log-uniform in [1, 5] GPa), 20 VBD
+iterations per 1/120 s step, the head-sphere SDF on a 128^3 grid, colour2 schedule, FP32.
+Metric: VBD vertex-iterations per second (vertices x iterations x steps / time), whole job.
+
+`value` times the fused step kernel with the state resident in HBM; the 95 MB working set fits
+the 126 MB L2, so a 256 MiB buffer is written between timed steps and only the step kernels are
+timed (CUDA events on the launching stream).  `e2e` is the same metric through the C ABI with
+host buffers: every step uploads positions/velocities from pinned host memory
+(kami_vbd_set_positions_velocities, UploadHair), steps, and reads them back
+(kami_vbd_get_positions_velocities, DownloadHair).  Extra `forms` report the plain per-groom sweep
+form and the batched form on 64 uneven grooms.  With N > 1 (torchrun) each rank steps its own groom
+(weak scaling, no collective on the data path); times are maxima over ranks.
+
+--impl reference times the CPU restatement of the reference's update (oracle/, Jacobi schedule =
+the reference's cosseratItr/quaternionLambdaItr order) with every host thread on a bounded sample
+of the same groom; the reference has no CPU implementation of this step of its own.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+WORKLOAD = "groom_10k_x64"
+DT = 1.0 / 120.0
+NUM_ITR = 20
+METRIC = "VBD vertex-iters/s"
+UNIT = "vertex-iters/s"
+BYTES_PER_VERTEX_STEP = 160  # fused kernel: 6 float4 loads + 4 float4 stores per vertex
+FALLBACK_HBM_GBS = 6650.0
+
+
+def settings():
+    from kamisimulator_b200 import synth
+
+    return dict(num_itr=NUM_ITR, max_h=DT, gravity=(0.0, 0.0, -9.81), radius=40e-6, density=1300.0,
+                velocity_decay=0.05, damping=1e-6, sdf=synth.sphere_sdf(128, threshold=1e-3))
+
+
+def config_dict(extra=None):
+    c = {"workload": f"{WORKLOAD}: 10,000 strands x 64 vertices, {NUM_ITR} VBD iterations, dt 1/120 s, "
+                     "head-sphere SDF 128^3, colour2 schedule",
+         "strands": 10000, "verts_per_strand": 64, "num_itr": NUM_ITR, "dt": DT, "sdf_grid": [128, 128, 128],
+         "l2": "flushed between timed steps (256 MiB write), working set 95 MB < L2"}
+    if extra:
+        c.update(extra)
+    return c
+
+
+def hbm_peak():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return FALLBACK_HBM_GBS, "fallback"
+
+
+def ncu_traffic():
+    """Per-launch DRAM bytes of the fused step kernel from the committed ncu capture summary."""
+    p = os.path.join(ROOT, "profiles", "fused_step_groom_10k_x64.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return d.get("dram_bytes_per_launch"), d
+    except Exception:
+        return None, None
+
+
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpus):
+        self.gpus = gpus
+        self.proc = None
+
+    def __enter__(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                                          "-lms", "50"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+        except Exception:
+            self.proc = None
+        return self
+
+    def __exit__(self, *exc):
+        self.out = ""
+        if self.proc is not None:
+            time.sleep(0.12)
+            self.proc.terminate()
+            try:
+                self.out, _ = self.proc.communicate(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in (getattr(self, "out", "") or "").splitlines():
+            parts = [p.strip() for p in line.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                idx = int(parts[0])
+            except ValueError:
+                continue
+            if idx not in self.gpus:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax.append(float(parts[2]))
+            except ValueError:
+                pass
+            for name, val in zip(names, parts[5:9]):
+                if val.lower().startswith("active"):
+                    reasons.add(name)
+        if not sm:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(smax), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def dist_setup():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return world, rank, local
+
+
+# --------------------------------------------------------------------------------------------------
+# reference arm: CPU restatement of the reference's update on every host thread
+# --------------------------------------------------------------------------------------------------
+def run_reference(args):
+    world, rank, _ = dist_setup()
+    if rank != 0:
+        return
+    from kamisimulator_b200 import synth
+    from oracle.oracle import OracleSim, load
+
+    lib = load()
+    threads = lib.oracle_num_threads()
+    full = synth.groom()
+    st = settings()
+    # calibrate on one full-size frame, then bound each timed step to a strand subset
+    cal = OracleSim(full, schedule="jacobi", num_threads=threads, **st)
+    t0 = time.perf_counter()
+    cal.advance(DT)
+    t_full = time.perf_counter() - t0
+    budget = 100.0 / max(1, args.steps + args.warmup)
+    strands = int(max(64, min(10000, 10000 * budget / max(t_full, 1e-6))))
+    sub = synth.groom(strands, 64, seed=2)
+    sim = OracleSim(sub, schedule="jacobi", num_threads=threads, **st)
+    for _ in range(args.warmup):
+        sim.advance(DT)
+    t0 = time.perf_counter()
+    for _ in range(args.steps):
+        sim.advance(DT)
+    el = time.perf_counter() - t0
+    units = sub.num_vertices * NUM_ITR * args.steps
+    value = units / el
+    sample = (f"{strands} of the 10,000 strands (x 64 vertices) per step, jacobi schedule, FP32, "
+              f"{args.steps} steps; full-size frame took {t_full:.3f} s")
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": 1e3 * el / args.steps * (10000 / strands),
+            "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+            "config": config_dict({"sample_strands": strands,
+                                   "schedule": "jacobi (the reference's cosseratItr / quaternionLambdaItr order)"}),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port", "sample": sample},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line), flush=True)
+
+
+# --------------------------------------------------------------------------------------------------
+# our arm
+# --------------------------------------------------------------------------------------------------
+def time_steps(solver, steps, stream, flush):
+    import torch
+
+    starts = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    ends = [torch.cuda.Event(enable_timing=True) for _ in range(steps)]
+    for k in range(steps):
+        flush.fill_(k & 0xFF)
+        starts[k].record(stream)
+        solver.step(DT, stream=stream)
+        ends[k].record(stream)
+    torch.cuda.synchronize()
+    return sum(a.elapsed_time(b) for a, b in zip(starts, ends))
+
+
+def cpu_baseline_sample():
+    from kamisimulator_b200 import synth
+    from oracle.oracle import OracleSim, load
+
+    threads = load().oracle_num_threads()
+    g = synth.groom()
+    sim = OracleSim(g, schedule="colour2", num_threads=threads, **settings())
+    frames, t0 = 0, time.perf_counter()
+    while frames < 3 or (time.perf_counter() - t0 < 10.0 and frames < 60):
+        sim.advance(DT)
+        frames += 1
+    el = time.perf_counter() - t0
+    return {"value": g.num_vertices * NUM_ITR * frames / el, "unit": UNIT, "cores": threads, "kind": "port",
+            "sample": f"{frames} full-size frames of the 10,000 x 64 groom, colour2 schedule, FP32 "
+                      f"(oracle/kami_oracle.cpp, OpenMP)"}
+
+
+def extra_forms(args, torch, stream, flush):
+    """Plain per-groom sweep form on the headline groom, and batched vs plain on 64 uneven grooms."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.vbd import Solver
+
+    out = {}
+    g = synth.groom()
+    st = settings()
+    s = Solver(g, form="sweep", **st)
+    for _ in range(3):
+        s.step(DT, stream=stream)
+    n = max(20, args.steps // 20)
+    ms = time_steps(s, n, stream, flush)
+    out["plain_sweep"] = {"value": g.num_vertices * NUM_ITR * n / (ms / 1e3), "ms_per_step": ms / n,
+                          "what": "same groom, one kernel per colour sweep (4 per iteration) replayed from a CUDA graph"}
+    s.close()
+
+    grooms = synth.batched_grooms(64)
+    allg = synth.concat_grooms(grooms)
+    V = allg.num_vertices
+    b = Solver(allg, form="fused", **st)
+    for _ in range(2):
+        b.step(DT, stream=stream)
+    nb = 10
+    ms_b = time_steps(b, nb, stream, flush)
+    b.close()
+    plain = [Solver(gg, form="sweep", **st) for gg in grooms]
+    for p in plain:
+        p.step(DT, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    npl = 3
+    e0.record(stream)
+    for _ in range(npl):
+        for p in plain:  # the CantileverTestSolver pattern: instances stepped one after another
+            p.step(DT, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_p = e0.elapsed_time(e1)
+    for p in plain:
+        p.close()
+    vb = V * NUM_ITR * nb / (ms_b / 1e3)
+    vp = V * NUM_ITR * npl / (ms_p / 1e3)
+    out["batched_64_grooms"] = {"value": vb, "ms_per_step": ms_b / nb, "vertices": V,
+                                "plain_per_groom_value": vp, "plain_ms_per_step": ms_p / npl,
+                                "batched_over_plain": vb / vp,
+                                "what": "64 grooms, strands log-uniform [500, 20000], 16-128 vertices: one fused "
+                                        "launch per step vs 64 sweep-form graphs stepped in sequence"}
+    return out
+
+
+def run_ours(args):
+    import torch
+
+    world, rank, local = dist_setup()
+    if world > 1:
+        import datetime
+
+        import torch.distributed as dist
+
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    else:
+        torch.cuda.set_device(local)
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.vbd import Solver
+
+    g = synth.groom()
+    st = settings()
+    V = g.num_vertices
+    solver = Solver(g, form="fused", device=local, **st)
+    stream = torch.cuda.current_stream()
+    flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        solver.step(DT, stream=stream)
+    torch.cuda.synchronize()
+
+    def barrier():
+        if world > 1:
+            torch.distributed.barrier()
+        torch.cuda.synchronize()
+
+    gpus = list(range(world)) if world > 1 else [local]
+    with ClockSampler(gpus) as clk:
+        barrier()
+        step_ms = time_steps(solver, args.steps, stream, flush)
+        barrier()
+    t = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    max_ms = float(t.item())
+    units = world * V * NUM_ITR * args.steps
+    value = units / (max_ms / 1e3)
+    ms_step = max_ms / args.steps
+
+    # end to end through the C ABI with pinned host buffers
+    xh = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
+    vh = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
+    solver.get_positions_velocities(xh.numpy(), vh.numpy())
+    e2e_steps = max(10, args.steps // 10)
+    barrier()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(e2e_steps):
+        solver.set_positions_velocities(xh.numpy(), vh.numpy())
+        solver.step(DT, stream=stream)
+        solver.get_positions_velocities(xh.numpy(), vh.numpy())
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
+    if world > 1:
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    e2e_value = world * V * NUM_ITR * e2e_steps / (float(t.item()) / 1e3)
+    solver.close()
+
+    line = None
+    if rank == 0:
+        peak, peak_kind = hbm_peak()
+        achieved = V * BYTES_PER_VERTEX_STEP / (ms_step / 1e3) / 1e9
+        traffic, _ = ncu_traffic()
+        line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+                "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
+                "vs_baseline": None, "dtype": "f32", "data": "synthetic",
+                "config": config_dict({"form": "fused", "per_gpu": "one 10,000 x 64 groom per GPU"}),
+                "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": "fused_step_kernel<2,false>",
+                             "bytes_per_launch": V * BYTES_PER_VERTEX_STEP, "peak_source": peak_kind},
+                "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * V, "d2h_bytes_per_step": 24 * V,
+                        "steps": e2e_steps},
+                "gpu_launches": args.steps, "clocks": clk.summary()}
+    if world == 1 and rank == 0 and not args.skip_extra:
+        line["forms"] = extra_forms(args, torch, stream, flush)
+        line["cpu_baseline"] = cpu_baseline_sample()
+    if world > 1:
+        torch.distributed.barrier()
+        torch.distributed.destroy_process_group()
+    if line is not None:
+        print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=2000)
+    ap.add_argument("--warmup", type=int, default=10)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+    if args.impl == "reference":
+        run_reference(args)
+    else:
+        run_ours(args)
+
+
+if __name__ == "__main__":
+    main()
