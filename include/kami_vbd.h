@@ -168,6 +168,45 @@ kami_status kami_vbd_state_size(kami_vbd_handle h, size_t* bytes);
 kami_status kami_vbd_get_state(kami_vbd_handle h, void* dst, size_t bytes, int32_t memory);
 kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes, int32_t memory);
 
+/* ---- one step without any device allocation ----------------------------------------------------
+ * No counterpart in the reference (every reference path allocates through YarnBall::Sim).
+ *
+ * For callers that cannot let a library call cudaMalloc: an engine that owns all device memory
+ * itself (a fixed pool or a hard memory budget), or a real-time frame loop where an allocation,
+ * which can synchronise the whole device, would break the frame deadline.  Creating a handle
+ * allocates, so such a caller keeps the solver state in its own device buffers, in boundary order,
+ * and advances it with this entry point, which allocates nothing.
+ *
+ * It runs one KamiSimulator internal step like kami_vbd_step with the colour2 schedule and the sweep
+ * kernels, but with no SDF pass and no finiteness check.  Scratch lives in a fixed __device__ array
+ * for at most KAMI_NOALLOC_MAX_VERTICES vertices (12 MiB held by every device that loads the library
+ * until exit); larger inputs are rejected with KAMI_ERR_UNSUPPORTED.  The first call on a device
+ * resolves that array's address, so make it before any stream capture.  All calls share the scratch:
+ * calls whose work overlaps on the GPU race and must be serialised by the caller.  Per-vertex
+ * arrays hold what kami_vbd_create derives (inverse mass with pinned roots at 0, rest length,
+ * stretch stiffness, orientations, stiffness-scaled rest Darboux quaternions). */
+#define KAMI_NOALLOC_MAX_VERTICES 262144
+
+typedef struct kami_vbd_noalloc_args {
+    int64_t num_vertices;
+    int32_t num_strands;
+    const int32_t* strand_begin;    /* device, num_strands + 1 CSR offsets */
+    float* positions;               /* device, 3 * V, updated in place */
+    float* velocities;              /* device, 3 * V, updated in place */
+    float* last_velocities;         /* device, 3 * V, updated in place (zero before the first call) */
+    float* orientations;            /* device, 4 * V (x, y, z, w), updated in place */
+    const float* rest_darboux;      /* device, 4 * V */
+    const float* inv_mass;          /* device, V */
+    const float* rest_length;       /* device, V */
+    const float* stretch_stiffness; /* device, V */
+    float clock[3];                 /* host: h of the previous call (max_h before the first), lastH, time */
+} kami_vbd_noalloc_args;
+
+/* settings: scalar fields of a kami_vbd_desc (gravity, damping, velocity_decay, acceleration_ratio,
+ * external_force_multiplier, wind, num_itr, max_h, schedule); geometry fields are ignored.
+ * Asynchronous on `stream` (a cudaStream_t; NULL = legacy default stream); args->clock is updated. */
+kami_status kami_vbd_step_noalloc(const kami_vbd_desc* settings, kami_vbd_noalloc_args* args, float dt, void* stream);
+
 /* Description of the last error on the calling thread ("" if none). */
 const char* kami_vbd_last_error_string(void);
 

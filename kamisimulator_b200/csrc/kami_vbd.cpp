@@ -43,6 +43,10 @@ kami_status cuda_fail(cudaError_t e, const char* what) {
 
 }  // namespace
 
+namespace kami {
+void set_last_error(const char* msg) { g_last_error = msg; }
+}  // namespace kami
+
 struct kami_vbd_solver {
     int device = 0;
     cudaStream_t stream = nullptr;

@@ -49,4 +49,7 @@ struct MaterialDesc {
 int build_material(const int32_t* sb, int32_t ns, const float* pos, const MaterialDesc& md, Material& out,
                    std::string& err);
 
+// Sets the message returned by kami_vbd_last_error_string on the calling thread.
+void set_last_error(const char* msg);
+
 }  // namespace kami
