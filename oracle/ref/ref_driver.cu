@@ -1,0 +1,174 @@
+// ref_driver.cu -- TEST INFRASTRUCTURE ONLY.
+//
+// A thin C driver around KamiSimulator's own Stable Cosserat Rods code, compiled from the
+// reference sources in place (oracle/ref/Makefile) into oracle/_ref/libkami_ref.so.  The tests use
+// it on a GPU to pin the CPU oracle to the reference itself: material set-up (Sim::configure +
+// setYoung, YarnBall/YBSimulator.cu:161-320), the racy Jacobi step (Sim::advance,
+// YarnBall/sim/step.cpp:38-62, kernels in YarnBall/sim/{iteration,cosserat}.cu) and the SDF pass
+// (SDFHeadCollision, SDFCollisionSolver/cudaSDFCollision.cu:205-268).  Nothing in the product loads it.
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <cstring>
+#include <memory>
+#include <vector>
+
+#include "solvers/SDFCollisionSolver/cudaSDFCollision.cuh"
+#include "solvers/StableCosseratRods/YarnBall/YBSimulator.h"
+
+namespace YarnBall {
+extern std::shared_ptr<Sim> createFromCurves(std::vector<std::vector<glm::vec3>>& curves, std::vector<bool>& isCurveClosed,
+                                             int numVerts);
+}
+
+namespace {
+struct Holder {
+    std::shared_ptr<YarnBall::Sim> sim;
+};
+}  // namespace
+
+extern "C" {
+
+// Builds a Sim the way StableCosseratRodsSolver::BuildYarnBallHair does (StableCosseratRodsSolver.cpp:112-212),
+// with the radius given directly (MetaData::radius), one Young's modulus / deviation for all strands,
+// maxH = max_h and meta.h = max_h, no hair-hair collision and no wind.
+void* ref_create(int64_t nv, int32_t ns, const int32_t* sb, const float* pos, float radius, float density, float young,
+                 float deviation, const float* gravity, float velocity_decay, int32_t num_itr, float max_h,
+                 int32_t pin_roots) {
+    try {
+        std::vector<std::vector<glm::vec3>> curves(ns);
+        std::vector<bool> closed(ns, false);
+        for (int32_t s = 0; s < ns; s++)
+            for (int32_t i = sb[s]; i < sb[s + 1]; i++) curves[s].push_back(glm::vec3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]));
+        auto sim = YarnBall::createFromCurves(curves, closed, (int)nv);
+        sim->meta.radius = radius;
+        sim->meta.barrierThickness = 1e-7f;  // only used by hair-hair collision (off); keeps uploadMeta's check quiet
+        sim->meta.numItr = num_itr;
+        sim->meta.velocityDecay = velocity_decay;
+        sim->meta.gravity = glm::vec3(gravity[0], gravity[1], gravity[2]);
+        sim->meta.useStepSizeLimit = false;
+        sim->meta.enableHairHairColl = false;
+        sim->meta.ExternalForceMultiplier = 1.f;
+        sim->meta.windPeak = 0.f;
+        sim->maxH = max_h;
+        sim->meta.h = max_h;
+        sim->printErrors = false;
+        sim->configure(density);
+        sim->setYoung(young, deviation);
+        if (pin_roots)
+            for (int32_t s = 0; s < ns; s++) sim->verts[sb[s]].invMass = 0;
+        sim->upload();
+        return new Holder{sim};
+    } catch (...) {
+        return nullptr;
+    }
+}
+
+void ref_destroy(void* h) { delete (Holder*)h; }
+
+int ref_material(void* h, float* inv_mass, float* l_rest, float* k_stretch, uint32_t* flags, float* q, float* q_rest) {
+    auto& sim = ((Holder*)h)->sim;
+    const int nv = sim->meta.numVerts;
+    for (int i = 0; i < nv; i++) {
+        inv_mass[i] = sim->verts[i].invMass;
+        l_rest[i] = sim->verts[i].lRest;
+        k_stretch[i] = sim->verts[i].kStretch;
+        flags[i] = sim->verts[i].flags;
+        std::memcpy(q + 4 * i, &sim->qs[i].v, 4 * sizeof(float));
+        std::memcpy(q_rest + 4 * i, &sim->qRests[i], 4 * sizeof(float));
+    }
+    return 0;
+}
+
+// Overwrites positions, velocities, last velocities, orientations and the clock.
+int ref_set_state(void* h, const float* x, const float* v, const float* vlast, const float* q, const float* clock) {
+    auto& sim = ((Holder*)h)->sim;
+    const int nv = sim->meta.numVerts;
+    for (int i = 0; i < nv; i++) {
+        sim->verts[i].pos = glm::vec3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+        sim->vels[i] = glm::vec3(v[3 * i], v[3 * i + 1], v[3 * i + 2]);
+        std::memcpy(&sim->qs[i].v, q + 4 * i, 4 * sizeof(float));
+    }
+    sim->upload();
+    if (cudaMemcpy(sim->meta.d_lastVels, vlast, sizeof(float) * 3 * nv, cudaMemcpyHostToDevice) != cudaSuccess) return 1;
+    sim->meta.h = clock[0];
+    sim->meta.lastH = clock[1];
+    sim->meta.time = clock[2];
+    return 0;
+}
+
+int ref_advance(void* h, float dt) {
+    auto& sim = ((Holder*)h)->sim;
+    sim->advance(dt);
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
+}
+
+int ref_download(void* h, float* x, float* v, float* q) {
+    auto& sim = ((Holder*)h)->sim;
+    sim->download();
+    const int nv = sim->meta.numVerts;
+    for (int i = 0; i < nv; i++) {
+        std::memcpy(x + 3 * i, &sim->verts[i].pos, 3 * sizeof(float));
+        std::memcpy(v + 3 * i, &sim->vels[i], 3 * sizeof(float));
+        std::memcpy(q + 4 * i, &sim->qs[i].v, 4 * sizeof(float));
+    }
+    return 0;
+}
+
+// One SDFHeadCollision pass over np particles, with the grid spacing SDFBodyCollisionSolver::InitParams
+// computes (SDFBodyCollisionSolver.cpp:142-159).  local_idx[i] == 0 marks strand roots.
+int ref_sdf_project(int64_t np, float* pos, float* vel, const int32_t* local_idx, const int32_t* dims, const float* gmin,
+                    const float* gmax, float thresh, const float* phi, const float* grad, const float* rot,
+                    const float* trans) {
+    SDFSimulationParams p{};
+    p.Dt = 1.f;
+    p.InvDt = 1.f;
+    p.SDFDim = make_int3(dims[0], dims[1], dims[2]);
+    p.NumParticles = (size_t)np;
+    p.NumSdfCells = (size_t)dims[0] * dims[1] * dims[2];
+    p.ThreshSdf = thresh;
+    p.HeadMin = make_float3(gmin[0], gmin[1], gmin[2]);
+    p.HeadMax = make_float3(gmax[0], gmax[1], gmax[2]);
+    float dxS = (gmax[0] - gmin[0]) / (1.f * dims[0]);
+    float dyS = (gmax[1] - gmin[1]) / (1.f * dims[1]);
+    float dzS = (gmax[2] - gmin[2]) / (1.f * dims[2]);
+    p.SdfInvSqDs = make_float3(1.f / (dxS * dxS), 1.f / (dyS * dyS), 1.f / (dzS * dzS));
+    p.SDFInvDs = make_float3(1.f / dxS, 1.f / dyS, 1.f / dzS);
+    p.SdfDs = make_float3(dxS, dyS, dzS);
+    p.rotation = make_float4(rot[0], rot[1], rot[2], rot[3]);
+    p.translate = make_float3(trans[0], trans[1], trans[2]);
+    KamiCopySDFSimParamsToDevice(&p);
+    std::vector<ParticleForSDFColl> parts(np);
+    for (int64_t i = 0; i < np; i++) {
+        parts[i].Position = make_float3(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]);
+        parts[i].Velocity = make_float3(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
+        parts[i].LocalIdx = local_idx[i];
+        parts[i].GlobalIdx = (int)i;
+    }
+    SDFDeviceBuffers b{};
+    size_t cells = p.NumSdfCells;
+    if (cudaMalloc(&b.Particles, sizeof(ParticleForSDFColl) * np) != cudaSuccess) return 1;
+    if (cudaMalloc(&b.SDF, sizeof(float) * cells) != cudaSuccess) return 1;
+    if (cudaMalloc(&b.NablaSDF, sizeof(float3) * cells) != cudaSuccess) return 1;
+    cudaMemcpy(b.Particles, parts.data(), sizeof(ParticleForSDFColl) * np, cudaMemcpyHostToDevice);
+    cudaMemcpy(b.SDF, phi, sizeof(float) * cells, cudaMemcpyHostToDevice);
+    cudaMemcpy(b.NablaSDF, grad, sizeof(float3) * cells, cudaMemcpyHostToDevice);
+    int blocks = (int)((np + 255) / 256);
+    KamiLaunchKernelSDFHeadCollision(make_int2(blocks, 256), b);
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaMemcpy(parts.data(), b.Particles, sizeof(ParticleForSDFColl) * np, cudaMemcpyDeviceToHost);
+    cudaFree(b.Particles);
+    cudaFree(b.SDF);
+    cudaFree(b.NablaSDF);
+    for (int64_t i = 0; i < np; i++) {
+        pos[3 * i] = parts[i].Position.x;
+        pos[3 * i + 1] = parts[i].Position.y;
+        pos[3 * i + 2] = parts[i].Position.z;
+        vel[3 * i] = parts[i].Velocity.x;
+        vel[3 * i + 1] = parts[i].Velocity.y;
+        vel[3 * i + 2] = parts[i].Velocity.z;
+    }
+    return e == cudaSuccess ? 0 : 1;
+}
+
+}  // extern "C"

@@ -1,0 +1,108 @@
+"""ctypes front-end of oracle/_ref/libkami_ref.so -- TEST INFRASTRUCTURE ONLY.
+
+The library is KamiSimulator's own YarnBall Sim and SDF kernel compiled from the reference
+sources (oracle/ref/Makefile) with a thin C driver (oracle/ref/ref_driver.cu).  It needs a CUDA
+device.  Tests use it to pin the CPU oracle to the reference itself."""
+from __future__ import annotations
+
+import ctypes
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_ref", "libkami_ref.so")
+_lib = None
+
+
+def available():
+    return os.path.exists(LIB_PATH)
+
+
+def load():
+    global _lib
+    if _lib is None:
+        lib = ctypes.CDLL(LIB_PATH)
+        vp, i32, i64, f32 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64, ctypes.c_float
+        lib.ref_create.restype = vp
+        lib.ref_create.argtypes = [i64, i32, vp, vp, f32, f32, f32, f32, vp, f32, i32, f32, i32]
+        lib.ref_destroy.argtypes = [vp]
+        lib.ref_material.argtypes = [vp] + [vp] * 6
+        lib.ref_set_state.argtypes = [vp] + [vp] * 5
+        lib.ref_advance.argtypes = [vp, f32]
+        lib.ref_download.argtypes = [vp, vp, vp, vp]
+        lib.ref_sdf_project.argtypes = [i64, vp, vp, vp, vp, vp, vp, f32, vp, vp, vp, vp]
+        for n in ("ref_material", "ref_set_state", "ref_advance", "ref_download", "ref_sdf_project"):
+            getattr(lib, n).restype = ctypes.c_int
+        _lib = lib
+    return _lib
+
+
+def _p(a):
+    return a.ctypes.data_as(ctypes.c_void_p)
+
+
+class RefSim:
+    """The reference's YarnBall::Sim (Jacobi kernels, racy at block boundaries)."""
+
+    def __init__(self, groom, *, young, deviation=1.0, radius=40e-6, density=1300.0, gravity=(0.0, 0.0, -9.81),
+                 velocity_decay=0.05, num_itr=10, max_h=4e-4, pin_roots=True):
+        self.lib = load()
+        self.nv = groom.num_vertices
+        sb = np.ascontiguousarray(groom.strand_begin, np.int32)
+        pos = np.ascontiguousarray(groom.positions, np.float32)
+        g = np.asarray(gravity, np.float32)
+        self.h = self.lib.ref_create(self.nv, groom.num_strands, _p(sb), _p(pos), radius, density, young, deviation,
+                                     _p(g), velocity_decay, num_itr, max_h, int(pin_roots))
+        if not self.h:
+            raise RuntimeError("reference Sim construction failed")
+
+    def close(self):
+        if self.h:
+            self.lib.ref_destroy(self.h)
+            self.h = None
+
+    def material(self):
+        nv = self.nv
+        out = dict(inv_mass=np.zeros(nv, np.float32), l_rest=np.zeros(nv, np.float32),
+                   k_stretch=np.zeros(nv, np.float32), flags=np.zeros(nv, np.uint32), q=np.zeros((nv, 4), np.float32),
+                   q_rest=np.zeros((nv, 4), np.float32))
+        self.lib.ref_material(self.h, _p(out["inv_mass"]), _p(out["l_rest"]), _p(out["k_stretch"]), _p(out["flags"]),
+                              _p(out["q"]), _p(out["q_rest"]))
+        return out
+
+    def set_state(self, x, v, v_last, q, clock):
+        arrs = [np.ascontiguousarray(a, np.float32) for a in (x, v, v_last, q, clock)]
+        if self.lib.ref_set_state(self.h, *[_p(a) for a in arrs]) != 0:
+            raise RuntimeError("ref_set_state failed")
+
+    def advance(self, dt):
+        if self.lib.ref_advance(self.h, dt) != 0:
+            raise RuntimeError("ref_advance failed")
+
+    def download(self):
+        x = np.zeros((self.nv, 3), np.float32)
+        v = np.zeros((self.nv, 3), np.float32)
+        q = np.zeros((self.nv, 4), np.float32)
+        self.lib.ref_download(self.h, _p(x), _p(v), _p(q))
+        return x, v, q
+
+
+def sdf_project(pos, vel, local_idx, sdf, rot=(0.0, 0.0, 0.0, 1.0), trans=(0.0, 0.0, 0.0)):
+    """One pass of the reference's SDFHeadCollision kernel; returns new (pos, vel)."""
+    lib = load()
+    p = np.ascontiguousarray(pos, np.float32).copy()
+    v = np.ascontiguousarray(vel, np.float32).copy()
+    li = np.ascontiguousarray(local_idx, np.int32)
+    dims = np.asarray(sdf.dims, np.int32)
+    gmin = np.asarray(sdf.grid_min, np.float32)
+    gmax = np.asarray(sdf.grid_max, np.float32)
+    phi = np.ascontiguousarray(sdf.phi, np.float32)
+    grad = np.ascontiguousarray(sdf.grad, np.float32)
+    r = np.asarray(rot, np.float32)
+    t = np.asarray(trans, np.float32)
+    rc = lib.ref_sdf_project(p.shape[0], _p(p), _p(v), _p(li), _p(dims), _p(gmin), _p(gmax), sdf.threshold, _p(phi),
+                             _p(grad), _p(r), _p(t))
+    if rc != 0:
+        raise RuntimeError("ref_sdf_project failed")
+    return p, v

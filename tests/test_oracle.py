@@ -239,3 +239,57 @@ def test_golden_fixture_regression():
         s.advance(1 / 60)
     np.testing.assert_allclose(s.x, ref["x"], atol=1e-12)
     np.testing.assert_allclose(s.q, ref["q"], atol=1e-12)
+
+
+# ---- pins against KamiSimulator's own code, run on a GPU (tests/golden/make_ref_fixtures.py) ----
+def _ref_pins():
+    import os
+    return np.load(os.path.join(os.path.dirname(__file__), "golden", "ref_pins.npz"))
+
+
+@pytest.mark.parametrize("case", ["cant", "groom"])
+def test_configure_matches_reference_fixture(case):
+    ref = _ref_pins()
+    if case == "cant":
+        g = synth.cantilever()
+    else:
+        g = synth.groom(100, 64, seed=2)
+        g.strand_young[:] = 2.0
+    o = orc.configure(g, dtype=np.float32)
+    np.testing.assert_array_equal(o["flags"], ref[f"{case}_flags"])
+    for k in ("inv_mass", "l_rest", "k_stretch", "q", "q_rest"):
+        np.testing.assert_allclose(o[k], ref[f"{case}_{k}"], rtol=5e-7, atol=1e-7, err_msg=k)  # <= 4 ulp
+
+
+def test_jacobi_trajectories_match_reference_fixture():
+    """The reference's Jacobi kernels race at block boundaries (run-to-run spread ~3e-8 m here)."""
+    ref = _ref_pins()
+    g = synth.groom(100, 64, seed=2)
+    g.strand_young[:] = 2.0
+    s = orc.OracleSim(g, num_itr=20, max_h=1 / 120, schedule="jacobi")
+    for f in range(3):
+        s.advance(1 / 120)
+        assert np.abs(s.x - ref["jgroom_x"][f]).max() < 1e-6
+        assert np.abs(orc.twist_angles(ref["jgroom_q"][f], s.q)).max() < 1e-5
+    g = synth.cantilever(8, 16, young=1e-3)
+    s = orc.OracleSim(g, num_itr=10, max_h=1 / 60, schedule="jacobi")
+    for f in range(6):
+        s.advance(1 / 60)
+        assert np.abs(s.x - ref["jsoft_x"][f]).max() < 1e-6
+        assert np.abs(orc.twist_angles(ref["jsoft_q"][f], s.q)).max() < 1e-5
+
+
+@pytest.mark.parametrize("name", ["sphere", "capsules"])
+def test_sdf_pass_matches_reference_fixture(name):
+    ref = _ref_pins()
+    sdf = synth.sphere_sdf(32) if name == "sphere" else synth.capsule_union_sdf(24, num_capsules=5)
+    p, v, li = ref[f"sdf_{name}_p"], ref[f"sdf_{name}_v"], ref[f"sdf_{name}_li"]
+    # 250 strands of 8 particles: local index = position in the strand, as in the fixture
+    g = synth.Groom(np.arange(0, p.shape[0] + 1, 8, dtype=np.int32), p, np.ones(p.shape[0] // 8, np.float32),
+                    np.ones(p.shape[0] // 8, np.float32))
+    assert np.array_equal(li, np.arange(p.shape[0]) % 8)
+    s = orc.OracleSim(g, num_itr=0, max_h=1.0, gravity=(0, 0, 0), sdf=sdf, pin_roots=False, velocity_decay=0.0)
+    s.set_body_transform(tuple(ref[f"sdf_{name}_rot"]), tuple(ref[f"sdf_{name}_tr"]))
+    s.advance(1e-3)  # zero velocity, zero gravity: positions unchanged, then the SDF pass
+    assert np.mean(np.any(ref[f"sdf_{name}_pout"] != p, axis=1)) > 0.01
+    np.testing.assert_allclose(s.x, ref[f"sdf_{name}_pout"], atol=1e-6)

@@ -1,0 +1,94 @@
+"""Pins against KamiSimulator's own code built from source (oracle/_ref/libkami_ref.so): the
+reference's material set-up, its Jacobi step kernels and its SDF kernel, run live on the GPU and
+compared with the CPU oracle and with this solver's CUDA kernels.
+
+The reference's Jacobi kernels race at block boundaries, so their results vary from run to run;
+each comparison is reported next to that run-to-run spread."""
+import numpy as np
+import pytest
+
+from kamisimulator_b200 import synth
+from oracle import oracle as orc
+from oracle import ref_sim
+from tests import helpers
+from tests.helpers import POS_TOL, TWIST_TOL
+
+pytestmark = [pytest.mark.gpu,
+              pytest.mark.skipif(not ref_sim.available(), reason="oracle/_ref not built (needs the reference sources)")]
+
+
+@pytest.mark.parametrize("case", ["cantilever", "groom"])
+def test_material_matches_reference(case):
+    if case == "cantilever":
+        g, E = synth.cantilever(), 3.9
+    else:
+        g, E = synth.groom(300, 64, seed=2), 2.0
+        g.strand_young[:] = E
+    r = ref_sim.RefSim(g, young=E, num_itr=10, max_h=1 / 60)
+    m = r.material()
+    r.close()
+    o = orc.configure(g, dtype=np.float32)
+    np.testing.assert_array_equal(o["flags"], m["flags"])
+    for k in ("inv_mass", "l_rest", "k_stretch", "q", "q_rest"):
+        np.testing.assert_allclose(o[k], m[k], rtol=5e-7, atol=1e-7, err_msg=k)  # <= 4 ulp
+    # this solver's own set-up (vbd_host.cpp), read back through the C ABI
+    s = helpers.gpu_solver(g, dict(num_itr=10, max_h=1 / 60, radius=40e-6))
+    np.testing.assert_allclose(s.get_orientations(), m["q"], rtol=5e-7, atol=1e-7)
+    np.testing.assert_allclose(s.get_rest_darboux(), m["q_rest"], rtol=5e-7, atol=1e-7)
+    s.close()
+
+
+@pytest.mark.parametrize("form", ["fused", "sweep"])
+def test_jacobi_step_matches_reference_kernels(form):
+    """Reference Sim (racy Jacobi) vs the oracle's and this solver's Jacobi schedule, 6 steps of a
+    300 x 64 groom cut with 20 iterations."""
+    g = synth.groom(300, 64, seed=2)
+    g.strand_young[:] = 2.0
+    st = dict(num_itr=20, max_h=1 / 120, gravity=(0.0, 0.0, -9.81), radius=40e-6, schedule="jacobi")
+    refs = [ref_sim.RefSim(g, young=2.0, num_itr=20, max_h=1 / 120) for _ in range(2)]
+    o = helpers.oracle_sim(g, st, np.float32)
+    s = helpers.gpu_solver(g, st, form=form)
+    worst = dict(oracle=0.0, ours=0.0, spread=0.0, twist=0.0)
+    for _ in range(6):
+        for r in refs:
+            r.advance(1 / 120)
+        o.advance(1 / 120)
+        s.step(1 / 120)
+        (x0, _, q0), (x1, _, _) = refs[0].download(), refs[1].download()
+        xs, _ = s.get_positions_velocities()
+        worst["spread"] = max(worst["spread"], float(np.abs(x0 - x1).max()))
+        worst["oracle"] = max(worst["oracle"], float(np.abs(o.x - x0).max()))
+        worst["ours"] = max(worst["ours"], float(np.abs(xs - x0).max()))
+        worst["twist"] = max(worst["twist"], float(np.abs(orc.twist_angles(q0, s.get_orientations())).max()))
+    for r in refs:
+        r.close()
+    s.close()
+    print("reference pin", worst)
+    assert worst["oracle"] <= POS_TOL and worst["ours"] <= POS_TOL and worst["twist"] <= TWIST_TOL, worst
+
+
+def test_sdf_pass_matches_reference_kernel():
+    rng = np.random.default_rng(4)
+    for sdf, rot, tr in ((synth.sphere_sdf(64), (0.0, 0.0, 0.0, 1.0), (0.0, 0.0, 0.0)),
+                         (synth.capsule_union_sdf(40, num_capsules=6), synth.head_rotation(0.1), (0.02, 0.0, -0.01))):
+        n_strands, per = 4000, 4
+        p = rng.uniform(-0.25, 0.25, (n_strands * per, 3)).astype(np.float32)
+        li = np.tile(np.arange(per), n_strands).astype(np.int32)
+        rp, rv = ref_sim.sdf_project(p, np.zeros_like(p), li, sdf, rot, tr)
+        # the same pass through the oracle and through this solver: a zero-iteration, zero-gravity step
+        # leaves positions unchanged, then projects
+        g = synth.Groom(np.arange(0, n_strands * per + 1, per, dtype=np.int32), p, np.ones(n_strands, np.float32),
+                        np.ones(n_strands, np.float32))
+        st = dict(num_itr=0, max_h=1.0, gravity=(0.0, 0.0, 0.0), radius=40e-6, sdf=sdf, pin_roots=False,
+                  velocity_decay=0.0)
+        o = helpers.oracle_sim(g, st, np.float32)
+        o.set_body_transform(rot, tr)
+        o.advance(1e-3)
+        s = helpers.gpu_solver(g, st, form="fused")
+        s.set_body_transform(rot, tr)
+        s.step(1e-3)
+        xs, _ = s.get_positions_velocities()
+        s.close()
+        assert np.mean(np.any(rp != p, axis=1)) > 0.01  # the pass really projected some particles
+        assert float(np.abs(o.x - rp).max()) <= 1e-6
+        assert float(np.abs(xs - rp).max()) <= 1e-6
