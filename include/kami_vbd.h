@@ -106,6 +106,12 @@ typedef struct kami_vbd_desc {
     int32_t device;    /* CUDA device ordinal; -1 = current device */
 
     const kami_vbd_sdf_desc* sdf; /* NULL: no body collision (EnableSDF false) */
+
+    /* Device tile shape (no counterpart in the reference; 0 = automatic).  slots_per_lane: even C,
+     * each warp tile holds 32*C vertex slots (the fused form supports C = 2 and 4);
+     * warps_per_block: warps per CTA of the fused kernel. */
+    int32_t slots_per_lane;
+    int32_t warps_per_block;
 } kami_vbd_desc;
 
 typedef struct kami_vbd_solver* kami_vbd_handle;

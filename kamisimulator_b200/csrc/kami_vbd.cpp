@@ -312,6 +312,15 @@ kami_status kami_vbd_create(const kami_vbd_desc* d, kami_vbd_handle* out) {
 
     // tile layout and form
     int C = slots_per_lane_for(h->strand_begin.data(), h->ns);
+    if (d->slots_per_lane != 0) {
+        if (d->slots_per_lane < C || (d->slots_per_lane & 1))
+            return bail(fail(KAMI_ERR_INVALID_ARGUMENT, "slots_per_lane %d must be even and >= %d for these strands",
+                             d->slots_per_lane, C));
+        C = d->slots_per_lane;
+    }
+    if (d->warps_per_block < 0 || d->warps_per_block > 32 || (d->warps_per_block & (d->warps_per_block - 1)))
+        return bail(fail(KAMI_ERR_INVALID_ARGUMENT, "warps_per_block must be 0 or a power of two <= 32"));
+    if (d->warps_per_block > 0) h->warps_per_block = d->warps_per_block;
     int form = d->form;
     if (form == KAMI_FORM_AUTO) form = fused_supported(C) ? KAMI_FORM_FUSED : KAMI_FORM_SWEEP;
     if (form == KAMI_FORM_FUSED && !fused_supported(C))

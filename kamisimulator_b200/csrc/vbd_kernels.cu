@@ -12,6 +12,7 @@
 //    coupling across lanes goes through warp shuffles.  Predict, all iterations, the velocity
 //    update and the SDF projection run back to back, so HBM sees each vertex twice per step
 //    (one float4 load per array, one store per dynamic array).
+#include "vbd_fused.cuh"
 #include "vbd_kernels.h"
 #include "vbd_math.cuh"
 
@@ -170,173 +171,7 @@ __global__ void sweep_finish_kernel(DeviceState st, const float4* __restrict__ d
 // fused form
 // ==========================================================================================
 
-template <int C, bool JACOBI>
-__global__ void __launch_bounds__(128) fused_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf) {
-    static_assert(C % 2 == 0, "slots per lane must be even");
-    const int lane = threadIdx.x & 31;
-    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (tile >= st.num_tiles) return;  // uniform per warp
-    const int64_t base = tile * (32LL * C) + lane;
-
-    float3 x[C], v[C], vl[C], dx[C], y[C], e[C], d3[C];
-    float4 q[C], qr[C];
-    float im[C], invl[C], kk[C], dd[C];
-    uint32_t fl[C];
-    BlockConst bc[C];
-
-#pragma unroll
-    for (int k = 0; k < C; k++) {
-        const int64_t g = base + 32LL * k;
-        float4 a = st.xm[g];
-        x[k] = xyz(a);
-        im[k] = a.w;
-        v[k] = xyz(st.vel[g]);
-        vl[k] = xyz(st.vlast[g]);
-        q[k] = st.q[g];
-        qr[k] = st.qr[g];
-        float4 p = st.prm[g];
-        invl[k] = 1.f / p.x;
-        kk[k] = p.y * invl[k];
-        dd[k] = kk[k] * invl[k];
-        fl[k] = __float_as_uint(p.w);
-    }
-    // static halo: constants of the previous lane's last segment (segment i-1 of slot 0)
-    const float4 qrP = shfl_up4(qr[C - 1], 1);
-    const float invlP = __shfl_up_sync(0xffffffffu, invl[C - 1], 1);
-    const float kkP = __shfl_up_sync(0xffffffffu, kk[C - 1], 1);
-    const float ddP = __shfl_up_sync(0xffffffffu, dd[C - 1], 1);
-
-    const float h = sp.h;
-    const float damp = pp.damping / h;
-    const float accel = pp.accel_ratio;
-
-    for (int s = 0; s < sp.substeps; s++) {
-        // segment vectors (constant within a substep)
-#pragma unroll
-        for (int k = 0; k < C - 1; k++) e[k] = x[k + 1] - x[k];
-        e[C - 1] = shfl_down3(x[0], 1) - x[C - 1];
-        const float3 eP = shfl_up3(e[C - 1], 1);
-
-#pragma unroll
-        for (int k = 0; k < C; k++) {
-            vbd_predict(x[k], v[k], vl[k], im[k], pp, h, sp.last_h, sp.time, dx[k], y[k]);
-            vl[k] = v[k];
-            bc[k] = vbd_block_const(im[k], fl[k], dd[k], k > 0 ? dd[k - 1] : ddP, h, damp);
-            d3[k] = d3_of(q[k]);
-        }
-        float4 qP = shfl_up4(q[C - 1], 1);
-        float3 d3P = d3_of(qP);
-
-        for (int it = 0; it < pp.num_itr; it++) {
-            if (!JACOBI) {
-                // ---- positions, even slots
-                const float3 dxP = shfl_up3(dx[C - 1], 1);
-#pragma unroll
-                for (int k = 0; k < C; k += 2) {
-                    if (im[k] != 0.f) {
-                        const bool k0 = (k == 0);
-                        dx[k] = vbd_position(dx[k], y[k], fl[k], bc[k], e[k], invl[k], kk[k], dd[k], d3[k], dx[k + 1],
-                                             k0 ? eP : e[k > 0 ? k - 1 : 0], k0 ? invlP : invl[k > 0 ? k - 1 : 0],
-                                             k0 ? kkP : kk[k > 0 ? k - 1 : 0], k0 ? ddP : dd[k > 0 ? k - 1 : 0],
-                                             k0 ? d3P : d3[k > 0 ? k - 1 : 0], k0 ? dxP : dx[k > 0 ? k - 1 : 0], damp,
-                                             accel);
-                    }
-                }
-                // ---- positions, odd slots
-                const float3 dxN = shfl_down3(dx[0], 1);
-#pragma unroll
-                for (int k = 1; k < C; k += 2) {
-                    if (im[k] != 0.f) {
-                        const bool kl = (k == C - 1);
-                        dx[k] = vbd_position(dx[k], y[k], fl[k], bc[k], e[k], invl[k], kk[k], dd[k], d3[k],
-                                             kl ? dxN : dx[k + 1 < C ? k + 1 : k], e[k - 1], invl[k - 1], kk[k - 1],
-                                             dd[k - 1], d3[k - 1], dx[k - 1], damp, accel);
-                    }
-                }
-                // ---- orientations, even segments
-#pragma unroll
-                for (int k = 0; k < C; k += 2) {
-                    if ((fl[k] & F_HAS_NEXT) && !(fl[k] & F_FIX_ORIENTATION)) {
-                        const bool k0 = (k == 0);
-                        q[k] = vbd_orientation(q[k], fl[k], e[k], dx[k], dx[k + 1], -2.f * kk[k],
-                                               k0 ? qP : q[k > 0 ? k - 1 : 0], k0 ? qrP : qr[k > 0 ? k - 1 : 0],
-                                               q[k + 1], qr[k]);
-                        d3[k] = d3_of(q[k]);
-                    }
-                }
-                // ---- orientations, odd segments
-                const float4 qN = shfl_down4(q[0], 1);
-#pragma unroll
-                for (int k = 1; k < C; k += 2) {
-                    if ((fl[k] & F_HAS_NEXT) && !(fl[k] & F_FIX_ORIENTATION)) {
-                        const bool kl = (k == C - 1);
-                        q[k] = vbd_orientation(q[k], fl[k], e[k], dx[k], kl ? dxN : dx[k + 1 < C ? k + 1 : k],
-                                               -2.f * kk[k], q[k - 1], qr[k - 1], kl ? qN : q[k + 1 < C ? k + 1 : k],
-                                               qr[k]);
-                        d3[k] = d3_of(q[k]);
-                    }
-                }
-                qP = shfl_up4(q[C - 1], 1);
-                d3P = d3_of(qP);
-            } else {
-                // ---- positions, all slots from the previous sweep
-                const float3 dxP = shfl_up3(dx[C - 1], 1);
-                const float3 dxN = shfl_down3(dx[0], 1);
-                float3 nd[C];
-#pragma unroll
-                for (int k = 0; k < C; k++) {
-                    nd[k] = dx[k];
-                    if (im[k] != 0.f) {
-                        const bool k0 = (k == 0), kl = (k == C - 1);
-                        const int kp = k > 0 ? k - 1 : 0, kn = k + 1 < C ? k + 1 : k;
-                        nd[k] = vbd_position(dx[k], y[k], fl[k], bc[k], e[k], invl[k], kk[k], dd[k], d3[k],
-                                             kl ? dxN : dx[kn], k0 ? eP : e[kp], k0 ? invlP : invl[kp],
-                                             k0 ? kkP : kk[kp], k0 ? ddP : dd[kp], k0 ? d3P : d3[kp],
-                                             k0 ? dxP : dx[kp], damp, accel);
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < C; k++) dx[k] = nd[k];
-                // ---- orientations, all segments from the previous sweep
-                const float3 dxN2 = shfl_down3(dx[0], 1);
-                const float4 qN = shfl_down4(q[0], 1);
-                float4 nq[C];
-#pragma unroll
-                for (int k = 0; k < C; k++) {
-                    nq[k] = q[k];
-                    if ((fl[k] & F_HAS_NEXT) && !(fl[k] & F_FIX_ORIENTATION)) {
-                        const bool k0 = (k == 0), kl = (k == C - 1);
-                        const int kp = k > 0 ? k - 1 : 0, kn = k + 1 < C ? k + 1 : k;
-                        nq[k] = vbd_orientation(q[k], fl[k], e[k], dx[k], kl ? dxN2 : dx[kn], -2.f * kk[k],
-                                                k0 ? qP : q[kp], k0 ? qrP : qr[kp], kl ? qN : q[kn], qr[k]);
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < C; k++) {
-                    q[k] = nq[k];
-                    d3[k] = d3_of(q[k]);
-                }
-                qP = shfl_up4(q[C - 1], 1);
-                d3P = d3_of(qP);
-            }
-        }
-#pragma unroll
-        for (int k = 0; k < C; k++) vbd_finish(x[k], v[k], dx[k], im[k], h, pp.velocity_decay);
-    }
-
-    bool bad = false;
-#pragma unroll
-    for (int k = 0; k < C; k++) {
-        if (sdf.grid && (fl[k] & F_VALID) && !(fl[k] & F_ROOT)) vbd_sdf(x[k], v[k], sdf, sp);
-        bad |= !finite3(x[k]) || !finite3(v[k]) || !finite4(q[k]);
-        const int64_t g = base + 32LL * k;
-        st.xm[g] = make_float4(x[k].x, x[k].y, x[k].z, im[k]);
-        st.vel[g] = make_float4(v[k].x, v[k].y, v[k].z, 0.f);
-        st.vlast[g] = make_float4(vl[k].x, vl[k].y, vl[k].z, 0.f);
-        st.q[g] = q[k];
-    }
-    if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(st.status, STATUS_NONFINITE);
-}
+// fused_step_kernel: see vbd_fused.cuh
 
 // ==========================================================================================
 // boundary gather / scatter (API vertex order <-> tile slots)

@@ -78,6 +78,8 @@ class Desc(ctypes.Structure):
         ("pin_roots", ctypes.c_int32),
         ("device", ctypes.c_int32),
         ("sdf", ctypes.POINTER(SdfDesc)),
+        ("slots_per_lane", ctypes.c_int32),
+        ("warps_per_block", ctypes.c_int32),
     ]
 
 
@@ -154,7 +156,7 @@ class Solver:
                  damping=1e-6, velocity_decay=0.05, acceleration_ratio=1.0, ext_mult=1.0,
                  wind=(0.0, 1.0, 0.7, 0.4, 3.0), schedule="colour2", form="auto", sdf=None, stiffness_mode=0,
                  young=5.0, deviation=1.0, per_strand=True, k_stretch=3e3, k_bend=6e-4, pin_roots=True,
-                 velocities=None, device=-1):
+                 velocities=None, device=-1, slots_per_lane=0, warps_per_block=0):
         self.lib = load_library()
         self._h = None
         sb = np.ascontiguousarray(groom.strand_begin, np.int32)
@@ -184,6 +186,8 @@ class Solver:
         d.form = FORMS[form]
         d.pin_roots = int(pin_roots)
         d.device = device
+        d.slots_per_lane = slots_per_lane
+        d.warps_per_block = warps_per_block
         keep = [sb, pos, vel, sy, sd]
         if sdf is not None:
             phi = np.ascontiguousarray(sdf.phi, np.float32)

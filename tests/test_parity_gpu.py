@@ -205,3 +205,34 @@ def test_nonfinite_input_raises_status():
     s.step(1 / 60)
     s.get_positions_velocities()
     s.close()
+
+
+@pytest.mark.parametrize("form", ["fused", "sweep"])
+@pytest.mark.parametrize("pin_roots", [True, False])
+def test_nonfinite_strand_does_not_leak(form, pin_roots):
+    """A strand that turns non-finite leaves every other strand untouched (bit for bit), as the
+    reference's per-vertex flag tests guarantee; strands are packed several per tile here."""
+    from kamisimulator_b200.vbd import KamiError
+
+    g = helpers.soft_groom(64, (5, 30), seed=17)
+    st = helpers.soft_settings(pin_roots=pin_roots)
+    clean = helpers.gpu_solver(g, st, form=form)
+    bad = helpers.gpu_solver(g, st, form=form)
+    victim = 10
+    a, b = g.strand_begin[victim], g.strand_begin[victim + 1]
+    x = g.positions.copy()
+    x[(a + b) // 2] = np.nan
+    bad.set_positions_velocities(x, None)
+    for _ in range(3):
+        clean.step(1 / 60)
+        bad.step(1 / 60)
+    xc, _ = clean.get_positions_velocities()
+    with pytest.raises(KamiError):
+        bad.get_positions_velocities()
+    xb = bad.split_state(bad.get_state())["x"]
+    keep = np.ones(g.num_vertices, bool)
+    keep[a:b] = False
+    np.testing.assert_array_equal(xb[keep], xc[keep])
+    assert not np.isfinite(xb[a:b]).all()
+    clean.close()
+    bad.close()
