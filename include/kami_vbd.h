@@ -174,6 +174,31 @@ kami_status kami_vbd_state_size(kami_vbd_handle h, size_t* bytes);
 kami_status kami_vbd_get_state(kami_vbd_handle h, void* dst, size_t bytes, int32_t memory);
 kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes, int32_t memory);
 
+/* ---- differentiable stepping ---------------------------------------------------------------------
+ * No counterpart in the reference, which has no adjoint.  The fused colour2 step (no wind, one
+ * substep per step) can record its iterates on a tape; kami_vbd_backward then runs the hand-written
+ * adjoint of the recorded steps in reverse.  Typical use, checkpointing every k steps: restore a
+ * checkpoint with kami_vbd_set_state, record the k steps of that segment, call kami_vbd_backward
+ * with the adjoint of the segment's final state, and continue with the next earlier segment. */
+
+/* Allocates a tape for up to max_steps recorded steps and the adjoint buffers (d loss / d qRest
+ * starts at zero).  KAMI_ERR_UNSUPPORTED for the sweep form, the Jacobi schedule or wind. */
+kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps);
+
+/* kami_vbd_step that also records its iterates; dt must not exceed max_h (a single substep). */
+kami_status kami_vbd_step_record(kami_vbd_handle h, float dt, void* stream);
+
+/* In: the adjoint (d loss / d state) of the state after the last recorded step, boundary order:
+ * adj_x, adj_v, adj_vlast 3*V floats, adj_q 4*V floats.  Out (in place): the adjoint of the state
+ * before the first recorded step.  Adds d loss / d qRest of the recorded steps to the accumulated
+ * gradient and empties the tape.  Synchronous. */
+kami_status kami_vbd_backward(kami_vbd_handle h, float* adj_x, float* adj_v, float* adj_vlast, float* adj_q,
+                              int32_t memory, void* stream);
+
+/* The accumulated d loss / d qRest (4*V floats, boundary order), and its reset to zero. */
+kami_status kami_vbd_get_rest_darboux_grad(kami_vbd_handle h, float* xyzw, int32_t memory);
+kami_status kami_vbd_zero_rest_darboux_grad(kami_vbd_handle h);
+
 /* ---- one step without any device allocation ----------------------------------------------------
  * No counterpart in the reference (every reference path allocates through YarnBall::Sim).
  *

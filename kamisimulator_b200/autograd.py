@@ -1,0 +1,64 @@
+"""torch.autograd binding of the solver's hand-written adjoint (kami_vbd_backward).
+
+``StrandStiffnessRollout`` maps per-strand bend/twist stiffness scales to the positions after a
+rollout of ``frames`` steps.  The rest Darboux quaternions, whose magnitude is the bend/twist
+stiffness (Sim::setYoung, YarnBall/YBSimulator.cu:300-320), are  qRest_i = scale[strand(i)] *
+unit_i.  The forward pass keeps a device checkpoint of the full state every ``checkpoint_every``
+steps.  The backward pass walks the segments in reverse: it restores the segment's checkpoint,
+records its steps, and runs the adjoint back to the checkpoint.  The solver must use the fused form
+with the colour2 schedule, no wind and dt <= max_h.
+"""
+from __future__ import annotations
+
+import torch
+
+
+class StrandStiffnessRollout(torch.autograd.Function):
+    @staticmethod
+    def forward(ctx, scale, solver, unit, strand_of, init_state, frames, dt, checkpoint_every):
+        """scale: (S,) CUDA float32; unit: (V, 4) CUDA rest Darboux at scale 1; strand_of: (V,) long;
+        init_state: flat CUDA float32 state (Solver.get_state_into layout).  Returns (V, 3) positions."""
+        k = max(1, int(checkpoint_every))
+        qr = (unit * scale[strand_of][:, None]).contiguous()
+        torch.cuda.synchronize()
+        solver.set_rest_darboux(qr)
+        solver.set_state_from(init_state)
+        ckpts = []
+        for f in range(frames):
+            if f % k == 0:
+                ckpts.append(solver.get_state_into(torch.empty_like(init_state)))
+            solver.step(dt)
+        x = torch.empty((solver.num_vertices, 3), dtype=torch.float32, device=init_state.device)
+        solver.get_positions_velocities(x, None)
+        ctx.solver, ctx.ckpts, ctx.frames, ctx.dt, ctx.k = solver, ckpts, frames, dt, k
+        ctx.save_for_backward(unit, strand_of, scale)
+        return x
+
+    @staticmethod
+    def backward(ctx, gx):
+        unit, strand_of, scale = ctx.saved_tensors
+        solver, k = ctx.solver, ctx.k
+        nv = solver.num_vertices
+        dev = gx.device
+        ax = gx.detach().to(torch.float32).contiguous().clone()
+        av = torch.zeros((nv, 3), dtype=torch.float32, device=dev)
+        avl = torch.zeros_like(av)
+        aq = torch.zeros((nv, 4), dtype=torch.float32, device=dev)
+        solver.tape_reserve(k)
+        solver.zero_rest_darboux_grad()
+        torch.cuda.synchronize()
+        for seg in reversed(range(len(ctx.ckpts))):
+            solver.set_state_from(ctx.ckpts[seg])
+            n = min(k, ctx.frames - seg * k)
+            for _ in range(n):
+                solver.step_record(ctx.dt)
+            solver.backward(ax, av, avl, aq)
+        gqr = torch.empty((nv, 4), dtype=torch.float32, device=dev)
+        solver.get_rest_darboux_grad(gqr)
+        per_vertex = (gqr * unit).sum(-1)
+        gscale = torch.zeros_like(scale).index_add_(0, strand_of, per_vertex)
+        return gscale, None, None, None, None, None, None, None
+
+
+def rollout_positions(scale, solver, unit, strand_of, init_state, frames, dt, checkpoint_every=10):
+    return StrandStiffnessRollout.apply(scale, solver, unit, strand_of, init_state, frames, dt, checkpoint_every)

@@ -81,6 +81,25 @@ struct kami_vbd_solver {
     cudaGraphExec_t graph = nullptr;
     int graph_substeps = -1;
 
+    // differentiable stepping: the tape of recorded steps and the adjoint state
+    int tape_capacity = 0;
+    std::vector<StepParams> tape_steps;
+    float4 *d_tdx = nullptr, *d_tq = nullptr, *d_tx = nullptr, *d_tv = nullptr, *d_tvl = nullptr;
+    float4 *d_gx = nullptr, *d_gv = nullptr, *d_gvl = nullptr, *d_gq = nullptr, *d_gqr = nullptr;
+
+    TapeView tape(int step) const {
+        TapeView t;
+        t.dx = d_tdx;
+        t.q = d_tq;
+        t.x = d_tx;
+        t.v = d_tv;
+        t.vl = d_tvl;
+        t.slots = layout.num_slots;
+        t.num_itr = pp.num_itr;
+        t.step = step;
+        return t;
+    }
+
     DeviceState dstate() const {
         DeviceState s;
         s.xm = d_xm;
@@ -102,9 +121,10 @@ void release(kami_vbd_solver* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
-    void* ptrs[] = {h->d_slot_of, h->d_xm, h->d_vel, h->d_vlast, h->d_q,      h->d_qr,     h->d_prm,
-                    h->d_y,       h->d_dx, h->d_dx2, h->d_q2,    h->d_step,   h->d_stage,  h->d_status,
-                    h->d_sdf};
+    void* ptrs[] = {h->d_slot_of, h->d_xm, h->d_vel, h->d_vlast, h->d_q,     h->d_qr,    h->d_prm,
+                    h->d_y,       h->d_dx, h->d_dx2, h->d_q2,    h->d_step,  h->d_stage, h->d_status,
+                    h->d_sdf,     h->d_tdx, h->d_tq, h->d_tx,    h->d_tv,    h->d_tvl,   h->d_gx,
+                    h->d_gv,      h->d_gvl, h->d_gq, h->d_gqr};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
@@ -507,10 +527,7 @@ kami_status kami_vbd_set_body_transform(kami_vbd_handle h, const float rotation_
     return KAMI_OK;
 }
 
-kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
-    KAMI_TRY(valid_handle(h));
-    if (!(dt > 0.f)) return KAMI_OK;  // Sim::advance returns for h <= 0 (step.cpp:113)
-    if (!std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
+static StepParams advance_clock(kami_vbd_solver* h, float dt) {
     const int steps = std::max(1, (int)std::ceil(dt / h->max_h));
     h->last_h = h->h;
     h->h = dt / (float)steps;
@@ -526,6 +543,15 @@ kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
     sp.tr_x = h->tr[0];
     sp.tr_y = h->tr[1];
     sp.tr_z = h->tr[2];
+    return sp;
+}
+
+kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
+    KAMI_TRY(valid_handle(h));
+    if (!(dt > 0.f)) return KAMI_OK;  // Sim::advance returns for h <= 0 (step.cpp:113)
+    if (!std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
+    const StepParams sp = advance_clock(h, dt);
+    const int steps = sp.substeps;
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
         if (h->form == KAMI_FORM_FUSED) {
             KAMI_CUDA(launch_fused_step(h->dstate(), h->pp, sp, h->sdf, h->layout.C, h->schedule == KAMI_SCHEDULE_JACOBI,
@@ -541,6 +567,120 @@ kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
     });
     if (st != KAMI_OK) return st;
     h->time += dt;
+    return KAMI_OK;
+}
+
+// ---- differentiable stepping ----------------------------------------------------------------------
+
+static kami_status adjoint_supported(kami_vbd_solver* h) {
+    if (h->form != KAMI_FORM_FUSED || h->schedule != KAMI_SCHEDULE_COLOUR2)
+        return fail(KAMI_ERR_UNSUPPORTED, "the adjoint covers the fused form with the colour2 schedule");
+    if (h->pp.wind_peak != 0.f) return fail(KAMI_ERR_UNSUPPORTED, "the adjoint does not cover wind");
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps) {
+    KAMI_TRY(valid_handle(h));
+    KAMI_TRY(adjoint_supported(h));
+    if (max_steps <= 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "max_steps must be > 0");
+    KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    const size_t S = (size_t)h->layout.num_slots, N1 = (size_t)h->pp.num_itr + 1;
+    float4** tape_arrays[] = {&h->d_tdx, &h->d_tq, &h->d_tx, &h->d_tv, &h->d_tvl};
+    for (float4** p : tape_arrays)
+        if (*p) {
+            cudaFree(*p);
+            *p = nullptr;
+        }
+    h->tape_capacity = 0;
+    h->tape_steps.clear();
+    cudaError_t e = dalloc(&h->d_tdx, (size_t)max_steps * N1 * S);
+    if (e == cudaSuccess) e = dalloc(&h->d_tq, (size_t)max_steps * N1 * S);
+    if (e == cudaSuccess) e = dalloc(&h->d_tx, (size_t)max_steps * S);
+    if (e == cudaSuccess) e = dalloc(&h->d_tv, (size_t)max_steps * S);
+    if (e == cudaSuccess) e = dalloc(&h->d_tvl, (size_t)max_steps * S);
+    float4** adj_arrays[] = {&h->d_gx, &h->d_gv, &h->d_gvl, &h->d_gq, &h->d_gqr};
+    for (float4** p : adj_arrays)
+        if (e == cudaSuccess && !*p) {
+            e = dalloc(p, S);
+            if (e == cudaSuccess) e = cudaMemset(*p, 0, sizeof(float4) * S);
+        }
+    if (e != cudaSuccess) return cuda_fail(e, "allocating the tape");
+    h->tape_capacity = max_steps;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_step_record(kami_vbd_handle h, float dt, void* stream) {
+    KAMI_TRY(valid_handle(h));
+    if (h->tape_capacity == 0) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
+    if ((int)h->tape_steps.size() >= h->tape_capacity)
+        return fail(KAMI_ERR_STATE, "the tape holds %d steps; run kami_vbd_backward first", h->tape_capacity);
+    if (!(dt > 0.f) || !std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite and > 0");
+    if (std::max(1, (int)std::ceil(dt / h->max_h)) != 1)
+        return fail(KAMI_ERR_UNSUPPORTED, "recorded steps must be single substeps (dt <= max_h)");
+    const StepParams sp = advance_clock(h, dt);
+    const int step = (int)h->tape_steps.size();
+    kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
+        KAMI_CUDA(launch_fused_record(h->dstate(), h->pp, sp, h->sdf, h->tape(step), h->layout.C, h->warps_per_block, s),
+                  "recorded step launch");
+        return KAMI_OK;
+    });
+    if (st != KAMI_OK) return st;
+    h->tape_steps.push_back(sp);
+    h->time += dt;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_backward(kami_vbd_handle h, float* adj_x, float* adj_v, float* adj_vlast, float* adj_q,
+                              int32_t memory, void* stream) {
+    KAMI_TRY(valid_handle(h));
+    if (h->tape_capacity == 0 || h->tape_steps.empty()) return fail(KAMI_ERR_STATE, "no recorded steps to differentiate");
+    if (!adj_x || !adj_v || !adj_vlast || !adj_q) return fail(KAMI_ERR_INVALID_ARGUMENT, "null adjoint array");
+    if (memory != KAMI_MEMORY_HOST && memory != KAMI_MEMORY_DEVICE) return fail(KAMI_ERR_INVALID_ARGUMENT, "bad memory kind");
+    const size_t S = (size_t)h->layout.num_slots;
+    AdjointState ad;
+    ad.gx = h->d_gx;
+    ad.gv = h->d_gv;
+    ad.gvl = h->d_gvl;
+    ad.gq = h->d_gq;
+    ad.gqr = h->d_gqr;
+    float* ins3[] = {adj_x, adj_v, adj_vlast};
+    float4* adj3[] = {h->d_gx, h->d_gv, h->d_gvl};
+    for (int a = 0; a < 3; a++) {
+        KAMI_CUDA(cudaMemsetAsync(adj3[a], 0, sizeof(float4) * S, h->stream), "adjoint reset");
+        KAMI_TRY(stage_in(h, ins3[a], 3, memory));
+        KAMI_CUDA(launch_scatter3(h->d_stage, adj3[a], h->d_slot_of, h->nv, h->stream), "scatter adjoint");
+    }
+    KAMI_CUDA(cudaMemsetAsync(h->d_gq, 0, sizeof(float4) * S, h->stream), "adjoint reset");
+    KAMI_TRY(stage_in(h, adj_q, 4, memory));
+    KAMI_CUDA(launch_scatter4((const float4*)h->d_stage, h->d_gq, h->d_slot_of, h->nv, h->stream), "scatter adjoint");
+    kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
+        for (int step = (int)h->tape_steps.size() - 1; step >= 0; step--)
+            KAMI_CUDA(launch_adjoint_step(h->dstate(), h->pp, h->tape_steps[step], h->sdf, h->tape(step), ad, h->layout.C, s),
+                      "adjoint step launch");
+        return KAMI_OK;
+    });
+    if (st != KAMI_OK) return st;
+    h->tape_steps.clear();
+    for (int a = 0; a < 3; a++) {
+        KAMI_CUDA(launch_gather3(adj3[a], h->d_stage, h->d_slot_of, h->nv, h->stream), "gather adjoint");
+        KAMI_TRY(stage_out(h, ins3[a], 3, memory));
+    }
+    KAMI_CUDA(launch_gather4(h->d_gq, (float4*)h->d_stage, h->d_slot_of, h->nv, h->stream), "gather adjoint");
+    KAMI_TRY(stage_out(h, adj_q, 4, memory));
+    KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_get_rest_darboux_grad(kami_vbd_handle h, float* xyzw, int32_t memory) {
+    KAMI_TRY(valid_handle(h));
+    if (!h->d_gqr) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
+    return get4(h, h->d_gqr, xyzw, memory);
+}
+
+kami_status kami_vbd_zero_rest_darboux_grad(kami_vbd_handle h) {
+    KAMI_TRY(valid_handle(h));
+    if (!h->d_gqr) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
+    KAMI_CUDA(cudaMemsetAsync(h->d_gqr, 0, sizeof(float4) * h->layout.num_slots, h->stream), "gradient reset");
     return KAMI_OK;
 }
 

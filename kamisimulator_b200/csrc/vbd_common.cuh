@@ -69,6 +69,30 @@ struct DeviceState {
     int* status;
 };
 
+// Iterates of recorded steps for the adjoint: for step s, iteration it (0 = after the predict) and
+// slot g, dx at dx[(s*(N+1) + it)*S + g] and q at q[(s*(N+1) + it)*S + g]; the state at the start
+// of step s at x/v/vl[s*S + g].  N = iterations per step, S = slots.
+struct TapeView {
+    float4* dx;
+    float4* q;
+    float4* x;
+    float4* v;
+    float4* vl;
+    int64_t slots;
+    int num_itr;
+    int step;
+};
+
+// Adjoint state of the solver, tile slots: d loss / d (x, v, vlast, q), and the accumulated
+// d loss / d qRest.
+struct AdjointState {
+    float4* gx;
+    float4* gv;
+    float4* gvl;
+    float4* gq;
+    float4* gqr;
+};
+
 // ---- small helpers ---------------------------------------------------------------------------
 __host__ __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }
 __host__ __device__ __forceinline__ float3 xyz(float4 a) { return make_float3(a.x, a.y, a.z); }

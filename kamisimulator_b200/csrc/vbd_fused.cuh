@@ -65,8 +65,12 @@ __device__ __forceinline__ float4 fused_orientation(float4 q, bool upd, bool pre
     return upd ? n : q;
 }
 
-template <int C, bool JACOBI>
-__global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf) {
+// RECORD (colour2, one substep) additionally writes the step's start state and the iterates to a
+// tape for the adjoint (vbd_adjoint.cuh).
+template <int C, bool JACOBI, bool RECORD>
+__global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                         TapeView tp) {
+    static_assert(!(RECORD && JACOBI), "the tape records the colour2 schedule");
     static_assert(C % 2 == 0, "slots per lane must be even");
     const int lane = threadIdx.x & 31;
     const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -96,6 +100,17 @@ __global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysPar
         mov[k] = im[k] != 0.f;
         ddN[k] = (fl[k] & F_HAS_NEXT) ? kk[k] * invl[k] : 0.f;
         kkN[k] = (fl[k] & F_HAS_NEXT) ? kk[k] : 0.f;
+    }
+    const int64_t tS = tp.slots;
+    const int64_t tbase = ((int64_t)tp.step * (tp.num_itr + 1)) * tS + base;  // tape row of iteration 0
+    if (RECORD) {
+#pragma unroll
+        for (int k = 0; k < C; k++) {
+            const int64_t g = base + 32LL * k, o = (int64_t)tp.step * tS + g;
+            tp.x[o] = make_float4(x[k].x, x[k].y, x[k].z, im[k]);
+            tp.v[o] = make_float4(v[k].x, v[k].y, v[k].z, 0.f);
+            tp.vl[o] = make_float4(vl[k].x, vl[k].y, vl[k].z, 0.f);
+        }
     }
     // constants of the previous lane's last segment (segment i-1 of slot 0)
     const float4 qrH = shfl_up4(qr[C - 1], 1);
@@ -134,6 +149,13 @@ __global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysPar
         }
         float4 qP = shfl_up4(q[C - 1], 1);
         float3 d3P = d3_of(qP);
+        if (RECORD) {
+#pragma unroll
+            for (int k = 0; k < C; k++) {
+                tp.dx[tbase + 32LL * k] = make_float4(dx[k].x, dx[k].y, dx[k].z, 0.f);
+                tp.q[tbase + 32LL * k] = q[k];
+            }
+        }
 
         for (int it = 0; it < pp.num_itr; it++) {
             if (!JACOBI) {
@@ -181,6 +203,14 @@ __global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysPar
                 }
                 qP = shfl_up4(q[C - 1], 1);
                 d3P = d3_of(qP);
+                if (RECORD) {
+                    const int64_t row = tbase + (int64_t)(it + 1) * tS;
+#pragma unroll
+                    for (int k = 0; k < C; k++) {
+                        tp.dx[row + 32LL * k] = make_float4(dx[k].x, dx[k].y, dx[k].z, 0.f);
+                        tp.q[row + 32LL * k] = q[k];
+                    }
+                }
             } else {
                 // positions, every slot from the previous sweep
                 const float3 dxP = shfl_up3(dx[C - 1], 1);

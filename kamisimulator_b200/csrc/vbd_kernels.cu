@@ -251,13 +251,14 @@ cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const
     int threads = 32 * warps_per_block;
     unsigned blocks = blocks_for(st.num_tiles, warps_per_block);
     if (blocks == 0) return cudaSuccess;
-#define KAMI_FUSED_CASE(CC)                                                                  \
-    if (C == CC) {                                                                           \
-        if (jacobi)                                                                          \
-            fused_step_kernel<CC, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf);         \
-        else                                                                                 \
-            fused_step_kernel<CC, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf);        \
-        return cudaGetLastError();                                                           \
+    const TapeView none{};
+#define KAMI_FUSED_CASE(CC)                                                                        \
+    if (C == CC) {                                                                                 \
+        if (jacobi)                                                                                \
+            fused_step_kernel<CC, true, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, none);  \
+        else                                                                                       \
+            fused_step_kernel<CC, false, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, none); \
+        return cudaGetLastError();                                                                 \
     }
     KAMI_FUSED_CASE(2)
     KAMI_FUSED_CASE(4)

@@ -32,6 +32,8 @@ EXPORTED = [
     "kami_vbd_set_orientations", "kami_vbd_get_rest_darboux", "kami_vbd_set_rest_darboux",
     "kami_vbd_set_body_transform", "kami_vbd_step", "kami_vbd_synchronize", "kami_vbd_state_size",
     "kami_vbd_get_state", "kami_vbd_set_state", "kami_vbd_last_error_string", "kami_vbd_version",
+    "kami_vbd_tape_reserve", "kami_vbd_step_record", "kami_vbd_backward", "kami_vbd_get_rest_darboux_grad",
+    "kami_vbd_zero_rest_darboux_grad",
 ]
 
 
@@ -112,6 +114,11 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_state_size": [vp, ctypes.POINTER(ctypes.c_size_t)],
         "kami_vbd_get_state": [vp, vp, ctypes.c_size_t, i32],
         "kami_vbd_set_state": [vp, vp, ctypes.c_size_t, i32],
+        "kami_vbd_tape_reserve": [vp, i32],
+        "kami_vbd_step_record": [vp, f32, vp],
+        "kami_vbd_backward": [vp, vp, vp, vp, vp, i32, vp],
+        "kami_vbd_get_rest_darboux_grad": [vp, vp, i32],
+        "kami_vbd_zero_rest_darboux_grad": [vp],
     }
     for name, args in sig.items():
         fn = getattr(lib, name)
@@ -299,6 +306,40 @@ class Solver:
     def set_state(self, buf):
         buf = np.ascontiguousarray(buf, np.float32)
         _check(self.lib.kami_vbd_set_state(self._h, buf.ctypes.data_as(ctypes.c_void_p), buf.nbytes, MEM_HOST))
+
+    def get_state_into(self, out):
+        """Snapshot into a preallocated buffer (numpy, or a torch CUDA tensor for a device copy)."""
+        p, m = _ptr(out)
+        nbytes = out.numel() * out.element_size() if hasattr(out, "numel") else out.nbytes
+        _check(self.lib.kami_vbd_get_state(self._h, p, nbytes, m))
+        return out
+
+    def set_state_from(self, buf):
+        p, m = _ptr(buf)
+        nbytes = buf.numel() * buf.element_size() if hasattr(buf, "numel") else buf.nbytes
+        _check(self.lib.kami_vbd_set_state(self._h, p, nbytes, m))
+
+    # -- differentiable stepping
+    def tape_reserve(self, max_steps):
+        _check(self.lib.kami_vbd_tape_reserve(self._h, max_steps))
+
+    def step_record(self, dt, stream=None):
+        s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+        _check(self.lib.kami_vbd_step_record(self._h, ctypes.c_float(dt), s))
+
+    def backward(self, gx, gv, gvl, gq):
+        """In place: adjoint of the state after the recorded steps -> adjoint before them."""
+        ptrs = [_ptr(a) for a in (gx, gv, gvl, gq)]
+        _check(self.lib.kami_vbd_backward(self._h, ptrs[0][0], ptrs[1][0], ptrs[2][0], ptrs[3][0], ptrs[0][1], None))
+
+    def get_rest_darboux_grad(self, out=None):
+        out = np.empty((self.num_vertices, 4), np.float32) if out is None else out
+        p, m = _ptr(out)
+        _check(self.lib.kami_vbd_get_rest_darboux_grad(self._h, p, m))
+        return out
+
+    def zero_rest_darboux_grad(self):
+        _check(self.lib.kami_vbd_zero_rest_darboux_grad(self._h))
 
     def split_state(self, buf):
         nv = self.num_vertices

@@ -1,0 +1,187 @@
+"""The hand-written adjoint (kami_vbd_step_record / kami_vbd_backward, torch.autograd binding)
+against an FP64 autograd restatement (oracle/torch_ref.py) and central finite differences of the
+FP64 oracle.  Bar: gradient relative error <= 1e-3."""
+import numpy as np
+import pytest
+
+from kamisimulator_b200 import synth
+from tests import helpers
+
+pytestmark = pytest.mark.gpu
+
+GRAD_TOL = 1e-3
+
+
+def _setup(num_strands=24, lengths=(6, 20), seed=5, young_scale=1e-3, sdf=True, num_itr=5, velocities=True):
+    import torch
+
+    g = helpers.soft_groom(num_strands, lengths, seed=seed, young_scale=young_scale)
+    s = synth.sphere_sdf(48, threshold=2e-3) if sdf else None
+    st = dict(num_itr=num_itr, max_h=1 / 60, gravity=(0.3, -0.4, -9.81), radius=40e-6, sdf=s)
+    v0 = helpers.random_velocities(g, 0.15, seed=seed + 1) if velocities else None
+    solver = helpers.gpu_solver(g, st, form="fused", velocities=v0)
+    unit = torch.tensor(solver.get_rest_darboux(), device="cuda")
+    strand_of = torch.tensor(np.repeat(np.arange(g.num_strands), np.diff(g.strand_begin)), device="cuda")
+    init = torch.tensor(solver.get_state(), device="cuda")
+    return g, st, solver, unit, strand_of, init, v0
+
+
+def _torch_reference(g, st, v0, scale, frames, c, dt=1 / 60):
+    """FP64 autograd rollout: returns (loss, d loss/d scale, d loss/d (x0, v0, q0))."""
+    import torch
+
+    from oracle import oracle as orc
+    from oracle.torch_ref import TorchVBD
+
+    m = orc.configure(g, radius=st["radius"], dtype=np.float64)
+    tv = TorchVBD(g, m, num_itr=st["num_itr"], max_h=st["max_h"], gravity=st["gravity"], sdf=st["sdf"])
+    strand_of = torch.tensor(np.repeat(np.arange(g.num_strands), np.diff(g.strand_begin)))
+    sc = torch.tensor(np.asarray(scale, np.float64), requires_grad=True)
+    x0 = torch.tensor(g.positions.astype(np.float64), requires_grad=True)
+    vv = torch.tensor((v0 if v0 is not None else np.zeros_like(g.positions)).astype(np.float64), requires_grad=True)
+    q0 = torch.tensor(m["q"], requires_grad=True)
+    qr = torch.tensor(m["q_rest"]) * sc[strand_of][:, None]
+    state = (x0, vv, torch.zeros_like(x0), q0, float(np.float32(st["max_h"])))
+    for _ in range(frames):
+        state = tv.step(state, qr, dt)
+    loss = (torch.tensor(c) * state[0]).sum()
+    loss.backward()
+    return loss.item(), sc.grad.numpy(), x0.grad.numpy(), vv.grad.numpy(), q0.grad.numpy()
+
+
+def _rel(a, b):
+    return float(np.linalg.norm(np.asarray(a) - np.asarray(b)) / max(np.linalg.norm(b), 1e-30))
+
+
+@pytest.mark.parametrize("sdf", [False, True])
+def test_stiffness_gradient_matches_fp64_autograd(sdf):
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+
+    g, st, solver, unit, strand_of, init, v0 = _setup(sdf=sdf)
+    rng = np.random.default_rng(0)
+    scale0 = rng.uniform(0.7, 1.4, g.num_strands).astype(np.float32)
+    c = rng.normal(size=(g.num_vertices, 3))
+    frames = 6
+    scale = torch.tensor(scale0, device="cuda", requires_grad=True)
+    x = rollout_positions(scale, solver, unit, strand_of, init, frames, 1 / 60, checkpoint_every=2)
+    loss = (torch.tensor(c, dtype=torch.float32, device="cuda") * x).sum()
+    loss.backward()
+    g_gpu = scale.grad.cpu().numpy()
+    l_ref, g_ref, *_ = _torch_reference(g, st, v0, scale0, frames, c)
+    assert abs(loss.item() - l_ref) <= 1e-4 * abs(l_ref) + 1e-6
+    assert np.linalg.norm(g_ref) > 0
+    assert _rel(g_gpu, g_ref) <= GRAD_TOL, (_rel(g_gpu, g_ref), g_gpu[:5], g_ref[:5])
+    solver.close()
+
+
+def test_state_adjoint_matches_fp64_autograd():
+    """kami_vbd_backward's adjoint of the initial positions, velocities and orientations."""
+    import torch
+
+    g, st, solver, unit, strand_of, init, v0 = _setup(num_strands=16, lengths=(6, 16), sdf=True)
+    c = np.random.default_rng(1).normal(size=(g.num_vertices, 3))
+    frames = 4
+    solver.tape_reserve(frames)
+    for _ in range(frames):
+        solver.step_record(1 / 60)
+    ax = torch.tensor(c, dtype=torch.float32, device="cuda")
+    av = torch.zeros_like(ax)
+    avl = torch.zeros_like(ax)
+    aq = torch.zeros((g.num_vertices, 4), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    solver.backward(ax, av, avl, aq)
+    _, _, gx_ref, gv_ref, gq_ref = _torch_reference(g, st, v0, g.strand_dev * 0 + 1, frames, c)
+    assert _rel(ax.cpu().numpy(), gx_ref) <= GRAD_TOL
+    assert _rel(av.cpu().numpy(), gv_ref) <= GRAD_TOL
+    assert _rel(aq.cpu().numpy(), gq_ref) <= GRAD_TOL
+    solver.close()
+
+
+def test_directional_derivative_matches_central_fd():
+    """<d loss / d scale, u> against central differences of the FP64 oracle, h = 1e-3 relative."""
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+    from oracle import oracle as orc
+
+    g, st, solver, unit, strand_of, init, v0 = _setup(num_strands=20, lengths=(8, 18), seed=9, sdf=True)
+    rng = np.random.default_rng(2)
+    scale0 = rng.uniform(0.8, 1.25, g.num_strands)
+    c = rng.normal(size=(g.num_vertices, 3))
+    frames = 5
+    scale = torch.tensor(scale0.astype(np.float32), device="cuda", requires_grad=True)
+    x = rollout_positions(scale, solver, unit, strand_of, init, frames, 1 / 60, checkpoint_every=5)
+    (torch.tensor(c, dtype=torch.float32, device="cuda") * x).sum().backward()
+    grad = scale.grad.cpu().numpy().astype(np.float64)
+    unit64 = orc.configure(g, radius=st["radius"], dtype=np.float64)["q_rest"]
+    so = np.repeat(np.arange(g.num_strands), np.diff(g.strand_begin))
+
+    def loss(sc):
+        o = orc.OracleSim(g, dtype=np.float64, velocities=v0, **st)
+        o.q_rest[...] = unit64 * sc[so][:, None]
+        for _ in range(frames):
+            o.advance(1 / 60)
+        return float((c * o.x).sum())
+
+    for trial in range(3):
+        u = rng.normal(size=g.num_strands)
+        u /= np.linalg.norm(u)
+        hstep = 1e-3 * np.abs(scale0).mean()
+        fd = (loss(scale0 + hstep * u) - loss(scale0 - hstep * u)) / (2 * hstep)
+        ad = float(grad @ u)
+        assert abs(ad - fd) <= GRAD_TOL * max(abs(fd), 1e-3 * np.linalg.norm(grad)), (trial, ad, fd)
+    solver.close()
+
+
+def test_checkpoint_interval_does_not_change_the_gradient():
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+
+    g, st, solver, unit, strand_of, init, _ = _setup(num_strands=20, sdf=True)
+    c = torch.tensor(np.random.default_rng(3).normal(size=(g.num_vertices, 3)), dtype=torch.float32, device="cuda")
+    grads = []
+    for k in (1, 3, 7):
+        scale = torch.ones(g.num_strands, device="cuda", requires_grad=True)
+        x = rollout_positions(scale, solver, unit, strand_of, init, 7, 1 / 60, checkpoint_every=k)
+        (c * x).sum().backward()
+        grads.append(scale.grad.cpu().numpy())
+    assert _rel(grads[0], grads[2]) <= 1e-5
+    assert _rel(grads[1], grads[2]) <= 1e-5
+    solver.close()
+
+
+def test_stiffness_fit_reduces_loss_on_the_2000_strand_workload():
+    """Per-strand bend/twist stiffness fit: 2,000 strands x 48 vertices, 20 iterations, dt 1/120,
+    head-sphere SDF, target = the rollout at true stiffness; start at truth x U[0.5, 2]."""
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+
+    g = synth.groom(2000, 48, seed=4)
+    st = dict(num_itr=20, max_h=1 / 120, gravity=(0.0, 0.0, -9.81), radius=40e-6, sdf=synth.sphere_sdf(128))
+    solver = helpers.gpu_solver(g, st, form="fused")
+    unit = torch.tensor(solver.get_rest_darboux(), device="cuda")
+    strand_of = torch.tensor(np.repeat(np.arange(g.num_strands), np.diff(g.strand_begin)), device="cuda")
+    init = torch.tensor(solver.get_state(), device="cuda")
+    frames = 20
+    with torch.no_grad():
+        target = rollout_positions(torch.ones(g.num_strands, device="cuda"), solver, unit, strand_of, init, frames,
+                                   1 / 120, 10)
+    rng = np.random.default_rng(6)
+    logs = torch.tensor(np.log(rng.uniform(0.5, 2.0, g.num_strands)), dtype=torch.float32, device="cuda",
+                        requires_grad=True)
+    opt = torch.optim.Adam([logs], lr=0.1)
+    losses = []
+    for _ in range(6):
+        opt.zero_grad()
+        x = rollout_positions(torch.exp(logs), solver, unit, strand_of, init, frames, 1 / 120, 10)
+        loss = ((x - target) ** 2).sum()
+        loss.backward()
+        assert torch.isfinite(logs.grad).all()
+        opt.step()
+        losses.append(loss.item())
+    assert losses[-1] < 0.8 * losses[0], losses
+    solver.close()
