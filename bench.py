@@ -240,16 +240,22 @@ def extra_forms(args, torch, stream, flush):
     allg = synth.concat_grooms(grooms)
     V = allg.num_vertices
     b = Solver(allg, form="fused", **st)
-    for _ in range(2):
-        b.step(DT, stream=stream)
-    nb = 10
-    ms_b = time_steps(b, nb, stream, flush)
+    best, tuned_rate = b.autotune(DT, trial_steps=8)
+    nb = 24
+    b.step_n(DT, nb, stream=stream)  # warm-up: captures the graph for n = nb
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    flush.fill_(1)
+    e0.record(stream)
+    b.step_n(DT, nb, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms_b = e0.elapsed_time(e1)
     b.close()
     plain = [Solver(gg, form="sweep", **st) for gg in grooms]
     for p in plain:
         p.step(DT, stream=stream)
     torch.cuda.synchronize()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     npl = 3
     e0.record(stream)
     for _ in range(npl):
@@ -263,11 +269,71 @@ def extra_forms(args, torch, stream, flush):
     vb = V * NUM_ITR * nb / (ms_b / 1e3)
     vp = V * NUM_ITR * npl / (ms_p / 1e3)
     out["batched_64_grooms"] = {"value": vb, "ms_per_step": ms_b / nb, "vertices": V,
+                                "tuning": {"slots_per_lane": best[0], "warps_per_block": best[1],
+                                           "steps_per_launch": best[2]},
                                 "plain_per_groom_value": vp, "plain_ms_per_step": ms_p / npl,
                                 "batched_over_plain": vb / vp,
-                                "what": "64 grooms, strands log-uniform [500, 20000], 16-128 vertices: one fused "
-                                        "launch per step vs 64 sweep-form graphs stepped in sequence"}
+                                "what": "64 grooms (strands log-uniform [500, 20000], 16-128 vertices) in one handle, "
+                                        f"{nb} steps per kami_vbd_step_n (autotuned tile shape, CUDA graph) vs 64 "
+                                        "sweep-form handles stepped one after another"}
+    out["adjoint_2k_x48"] = adjoint_timing(torch, stream)
     return out
+
+
+def adjoint_timing(torch, stream):
+    """Device time per step of the forward step, the recorded forward and the adjoint (reverse) step
+    on 2,000 strands x 48 vertices, plus one host-timed autograd round (60 steps, checkpoint 10)."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.autograd import rollout_positions
+    from kamisimulator_b200.vbd import Solver
+
+    g = synth.groom(2000, 48, seed=4)
+    st = settings()
+    solver = Solver(g, form="fused", **st)
+    k = 10
+    solver.tape_reserve(k)
+    init = solver.get_state()
+
+    def timed(fn):
+        solver.set_state(init)
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        fn()
+        b.record(stream)
+        torch.cuda.synchronize()
+        return a.elapsed_time(b) / k
+
+    gx = torch.randn((g.num_vertices, 3), device="cuda")
+    zero3, zero4 = torch.zeros_like(gx), torch.zeros((g.num_vertices, 4), device="cuda")
+    for _ in range(2):  # second pass is the measurement
+        fwd = timed(lambda: [solver.step(DT, stream=stream) for _ in range(k)])
+        rec = timed(lambda: [solver.step_record(DT, stream=stream) for _ in range(k)])
+        args = (gx.clone(), zero3.clone(), zero3.clone(), zero4.clone())
+        torch.cuda.synchronize()
+        a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        a.record(stream)
+        solver.backward(*args)
+        b.record(stream)
+        torch.cuda.synchronize()
+        adj = a.elapsed_time(b) / k
+    unit = torch.tensor(solver.get_rest_darboux(), device="cuda")
+    strand_of = torch.tensor(np.repeat(np.arange(g.num_strands), np.diff(g.strand_begin)), device="cuda")
+    init_d = torch.tensor(init, device="cuda")
+    scale = torch.ones(g.num_strands, device="cuda", requires_grad=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x = rollout_positions(scale, solver, unit, strand_of, init_d, 60, DT, k)
+    (x ** 2).sum().backward()
+    torch.cuda.synchronize()
+    round_s = time.perf_counter() - t0
+    solver.close()
+    return {"forward_ms_per_step": fwd, "recorded_forward_ms_per_step": rec, "adjoint_ms_per_step": adj,
+            "adjoint_over_forward": adj / fwd, "backward_with_recompute_over_forward": (rec + adj) / fwd,
+            "autograd_round_s": round_s,
+            "what": "2,000 strands x 48 vertices, 20 iterations, dt 1/120, sphere SDF; device time per step of "
+                    "kami_vbd_step, kami_vbd_step_record and kami_vbd_backward (10 recorded steps); "
+                    "autograd_round_s: host time of one 60-step rollout + backward with checkpoints every 10"}
 
 
 def run_ours(args):

@@ -174,6 +174,29 @@ kami_status kami_vbd_state_size(kami_vbd_handle h, size_t* bytes);
 kami_status kami_vbd_get_state(kami_vbd_handle h, void* dst, size_t bytes, int32_t memory);
 kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes, int32_t memory);
 
+/* ---- batched stepping and tile shape (no counterpart in the reference) -------------------------
+ * One handle may hold many grooms (concatenate their strands): every strand is packed into warp
+ * tiles, so one launch steps all of them. */
+
+/* n consecutive kami_vbd_step(dt) calls.  The fused form runs steps_per_launch steps per launch with
+ * the state kept on chip between them, and replays the launches from a CUDA graph (captured on the
+ * first call for a given n).  body_transforms: host, 7 floats per step (rotation x y z w,
+ * translation), or NULL to keep the current transform.  Asynchronous. */
+kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float* body_transforms, void* stream);
+
+/* Tile shape: slots per lane C (even, >= the longest strand / 32; changing it moves the state to the
+ * new tiles), warps per CTA (1, 2, 4, 8) and steps per launch for kami_vbd_step_n (1..1024).
+ * 0 leaves a value unchanged. */
+kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32_t warps_per_block,
+                                int32_t steps_per_launch);
+kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int32_t* warps_per_block,
+                                int32_t* steps_per_launch);
+
+/* Times every tile shape on this handle's own strands (C in {min..4}, warps per CTA in {1,2,4,8},
+ * steps per launch in {1,4,16}, trial_steps steps of dt each), keeps the fastest and restores the
+ * simulation state and clock.  best = {C, warps, steps per launch}; best_rate in vertex-iters/s. */
+kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, int32_t best[3], double* best_rate);
+
 /* ---- differentiable stepping ---------------------------------------------------------------------
  * No counterpart in the reference, which has no adjoint.  The fused colour2 step (no wind, one
  * substep per step) can record its iterates on a tape; kami_vbd_backward then runs the hand-written

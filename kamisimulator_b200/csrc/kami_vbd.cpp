@@ -81,6 +81,14 @@ struct kami_vbd_solver {
     cudaGraphExec_t graph = nullptr;
     int graph_substeps = -1;
 
+    // multi-step launches (kami_vbd_step_n) and tuning
+    int steps_per_launch = 8;
+    StepParams* d_steps = nullptr;
+    int d_steps_cap = 0;
+    std::vector<StepParams> h_steps;
+    cudaGraphExec_t graph_n = nullptr;
+    int graph_n_steps = -1, graph_n_F = -1;
+
     // differentiable stepping: the tape of recorded steps and the adjoint state
     int tape_capacity = 0;
     std::vector<StepParams> tape_steps;
@@ -121,6 +129,8 @@ void release(kami_vbd_solver* h) {
     cudaSetDevice(h->device);
     if (h->stream) cudaStreamSynchronize(h->stream);
     if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->graph_n) cudaGraphExecDestroy(h->graph_n);
+    if (h->d_steps) cudaFree(h->d_steps);
     void* ptrs[] = {h->d_slot_of, h->d_xm, h->d_vel, h->d_vlast, h->d_q,     h->d_qr,    h->d_prm,
                     h->d_y,       h->d_dx, h->d_dx2, h->d_q2,    h->d_step,  h->d_stage, h->d_status,
                     h->d_sdf,     h->d_tdx, h->d_tq, h->d_tx,    h->d_tv,    h->d_tvl,   h->d_gx,
@@ -567,6 +577,227 @@ kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
     });
     if (st != KAMI_OK) return st;
     h->time += dt;
+    return KAMI_OK;
+}
+
+// ---- multi-step launches, tile shape and autotuning --------------------------------------------------
+
+static void drop_graphs(kami_vbd_solver* h) {
+    if (h->graph) cudaGraphExecDestroy(h->graph);
+    if (h->graph_n) cudaGraphExecDestroy(h->graph_n);
+    h->graph = h->graph_n = nullptr;
+    h->graph_substeps = h->graph_n_steps = h->graph_n_F = -1;
+}
+
+// Moves the live state to tiles of 32*C slots (gathered to boundary order and scattered back).
+static kami_status relayout(kami_vbd_solver* h, int C) {
+    if (C == h->layout.C) return KAMI_OK;
+    std::string err;
+    TileLayout nl;
+    if (!pack_tiles(h->strand_begin.data(), h->ns, C, nl, err)) return fail(KAMI_ERR_UNSUPPORTED, "%s", err.c_str());
+    KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    const int64_t nv = h->nv, S = nl.num_slots;
+    float4* tmp = nullptr;
+    KAMI_CUDA(dalloc(&tmp, 6 * nv), "relayout buffer");
+    float4* olds[6] = {h->d_xm, h->d_vel, h->d_vlast, h->d_q, h->d_qr, h->d_prm};
+    cudaError_t e = cudaSuccess;
+    for (int a = 0; a < 6 && e == cudaSuccess; a++) e = launch_gather4(olds[a], tmp + a * nv, h->d_slot_of, nv, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    // padding slots: zero position/mass, identity orientations, lRest 1 and no flags
+    std::vector<float4> zero(S, make_float4(0.f, 0.f, 0.f, 0.f)), ident(S, make_float4(0.f, 0.f, 0.f, 1.f)),
+        pad(S, make_float4(1.f, 0.f, 0.f, 0.f));
+    const std::vector<float4>* init[6] = {&zero, &zero, &zero, &ident, &ident, &pad};
+    float4* news[6] = {};
+    for (int a = 0; a < 6 && e == cudaSuccess; a++) {
+        e = dalloc(&news[a], S);
+        if (e == cudaSuccess) e = cudaMemcpy(news[a], init[a]->data(), sizeof(float4) * S, cudaMemcpyHostToDevice);
+    }
+    if (e == cudaSuccess)
+        e = cudaMemcpy(h->d_slot_of, nl.slot_of.data(), sizeof(int64_t) * nv, cudaMemcpyHostToDevice);
+    for (int a = 0; a < 6 && e == cudaSuccess; a++) e = launch_scatter4(tmp + a * nv, news[a], h->d_slot_of, nv, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    cudaFree(tmp);
+    if (e != cudaSuccess) {
+        for (float4* p : news)
+            if (p) cudaFree(p);
+        return cuda_fail(e, "relayout");
+    }
+    for (float4* p : olds) cudaFree(p);
+    h->d_xm = news[0];
+    h->d_vel = news[1];
+    h->d_vlast = news[2];
+    h->d_q = news[3];
+    h->d_qr = news[4];
+    h->d_prm = news[5];
+    // slot-indexed scratch follows the new layout; the tape and adjoint buffers are dropped
+    float4** scratch[] = {&h->d_y, &h->d_dx, &h->d_dx2, &h->d_q2, &h->d_tdx, &h->d_tq, &h->d_tx, &h->d_tv, &h->d_tvl,
+                          &h->d_gx, &h->d_gv, &h->d_gvl, &h->d_gq, &h->d_gqr};
+    bool had[14];
+    for (int i = 0; i < 14; i++) {
+        had[i] = *scratch[i] != nullptr;
+        if (*scratch[i]) cudaFree(*scratch[i]);
+        *scratch[i] = nullptr;
+    }
+    h->tape_capacity = 0;
+    h->tape_steps.clear();
+    for (int i = 0; i < 4 && e == cudaSuccess; i++)
+        if (had[i]) e = dalloc(scratch[i], S);
+    h->layout = nl;
+    drop_graphs(h);
+    if (e != cudaSuccess) return cuda_fail(e, "relayout scratch");
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32_t warps_per_block,
+                                int32_t steps_per_launch) {
+    KAMI_TRY(valid_handle(h));
+    if (slots_per_lane != 0) {
+        const int cmin = slots_per_lane_for(h->strand_begin.data(), h->ns);
+        if (slots_per_lane < cmin || (slots_per_lane & 1))
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "slots_per_lane must be even and >= %d", cmin);
+        if (h->form == KAMI_FORM_FUSED && !fused_supported(slots_per_lane))
+            return fail(KAMI_ERR_UNSUPPORTED, "the fused form supports 2 or 4 slots per lane");
+        KAMI_TRY(relayout(h, slots_per_lane));
+    }
+    if (warps_per_block != 0) {
+        if (warps_per_block < 0 || warps_per_block > 8 || (warps_per_block & (warps_per_block - 1)))
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "warps_per_block must be 1, 2, 4 or 8");
+        if (warps_per_block != h->warps_per_block) drop_graphs(h);
+        h->warps_per_block = warps_per_block;
+    }
+    if (steps_per_launch != 0) {
+        if (steps_per_launch < 1 || steps_per_launch > 1024)
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "steps_per_launch must be in [1, 1024]");
+        if (steps_per_launch != h->steps_per_launch) drop_graphs(h);
+        h->steps_per_launch = steps_per_launch;
+    }
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int32_t* warps_per_block,
+                                int32_t* steps_per_launch) {
+    if (!h) return fail(KAMI_ERR_INVALID_ARGUMENT, "null handle");
+    if (slots_per_lane) *slots_per_lane = h->layout.C;
+    if (warps_per_block) *warps_per_block = h->warps_per_block;
+    if (steps_per_launch) *steps_per_launch = h->steps_per_launch;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float* body_transforms, void* stream) {
+    KAMI_TRY(valid_handle(h));
+    if (n < 1) return fail(KAMI_ERR_INVALID_ARGUMENT, "n must be >= 1");
+    if (!(dt > 0.f) || !std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite and > 0");
+    if (h->form != KAMI_FORM_FUSED) {
+        for (int j = 0; j < n; j++) {
+            if (body_transforms) kami_vbd_set_body_transform(h, body_transforms + 7 * j, body_transforms + 7 * j + 4);
+            KAMI_TRY(kami_vbd_step(h, dt, stream));
+        }
+        return KAMI_OK;
+    }
+    if (n > h->d_steps_cap) {
+        KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        if (h->d_steps) cudaFree(h->d_steps);
+        h->d_steps = nullptr;
+        h->d_steps_cap = 0;
+        KAMI_CUDA(dalloc(&h->d_steps, (size_t)n), "step parameter array");
+        h->d_steps_cap = n;
+        drop_graphs(h);
+    }
+    h->h_steps.resize(n);
+    for (int j = 0; j < n; j++) {
+        if (body_transforms) kami_vbd_set_body_transform(h, body_transforms + 7 * j, body_transforms + 7 * j + 4);
+        h->h_steps[j] = advance_clock(h, dt);
+        h->time += dt;
+    }
+    const int F = std::min(h->steps_per_launch, n);
+    if (!h->graph_n || h->graph_n_steps != n || h->graph_n_F != F) {
+        if (h->graph_n) cudaGraphExecDestroy(h->graph_n);
+        h->graph_n = nullptr;
+        KAMI_CUDA(cudaStreamBeginCapture(h->stream, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
+        cudaError_t err = cudaSuccess;
+        for (int j0 = 0; j0 < n && err == cudaSuccess; j0 += F)
+            err = launch_fused_step(h->dstate(), h->pp, h->h_steps[0], h->sdf, h->layout.C,
+                                    h->schedule == KAMI_SCHEDULE_JACOBI, h->warps_per_block, h->stream, h->d_steps + j0,
+                                    std::min(F, n - j0));
+        cudaGraph_t g = nullptr;
+        cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
+        if (err != cudaSuccess || e2 != cudaSuccess) {
+            if (g) cudaGraphDestroy(g);
+            return cuda_fail(err != cudaSuccess ? err : e2, "capturing the multi-step graph");
+        }
+        cudaError_t e3 = cudaGraphInstantiate(&h->graph_n, g, 0);
+        cudaGraphDestroy(g);
+        if (e3 != cudaSuccess) return cuda_fail(e3, "cudaGraphInstantiate");
+        h->graph_n_steps = n;
+        h->graph_n_F = F;
+    }
+    return on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
+        KAMI_CUDA(cudaMemcpyAsync(h->d_steps, h->h_steps.data(), sizeof(StepParams) * n, cudaMemcpyHostToDevice, s),
+                  "step parameters");
+        KAMI_CUDA(cudaGraphLaunch(h->graph_n, s), "cudaGraphLaunch");
+        return KAMI_OK;
+    });
+}
+
+kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, int32_t best[3], double* best_rate) {
+    KAMI_TRY(valid_handle(h));
+    if (h->form != KAMI_FORM_FUSED) return fail(KAMI_ERR_UNSUPPORTED, "the autotuner tunes the fused form");
+    if (trial_steps < 1 || !(dt > 0.f)) return fail(KAMI_ERR_INVALID_ARGUMENT, "need trial_steps >= 1 and dt > 0");
+    // snapshot of the simulation state and clock, restored after every trial
+    size_t bytes = 0;
+    kami_vbd_state_size(h, &bytes);
+    void* snap = nullptr;
+    KAMI_CUDA(cudaMalloc(&snap, bytes), "autotune snapshot");
+    kami_status st = kami_vbd_get_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    if (st == KAMI_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
+        st = fail(KAMI_ERR_CUDA, "cudaEventCreate");
+    const int cmin = slots_per_lane_for(h->strand_begin.data(), h->ns);
+    const int Fs[3] = {1, 4, 16};
+    double rate_best = -1.0;
+    int pick[3] = {h->layout.C, h->warps_per_block, h->steps_per_launch};
+    for (int C = cmin; C <= 4 && st == KAMI_OK; C += 2) {
+        for (int W = 1; W <= 8 && st == KAMI_OK; W *= 2) {
+            for (int fi = 0; fi < 3 && st == KAMI_OK; fi++) {
+                const int F = std::min(Fs[fi], trial_steps);
+                st = kami_vbd_set_tuning(h, C, W, F);
+                if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
+                if (st == KAMI_OK) st = kami_vbd_step_n(h, dt, trial_steps, nullptr, nullptr);  // warm-up, builds the graph
+                if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
+                if (st != KAMI_OK) break;
+                cudaEventRecord(e0, h->stream);
+                st = kami_vbd_step_n(h, dt, trial_steps, nullptr, nullptr);
+                cudaEventRecord(e1, h->stream);
+                if (st != KAMI_OK) break;
+                if (cudaEventSynchronize(e1) != cudaSuccess) {
+                    st = fail(KAMI_ERR_CUDA, "autotune timing");
+                    break;
+                }
+                float ms = 0.f;
+                cudaEventElapsedTime(&ms, e0, e1);
+                const double rate = (double)h->nv * h->pp.num_itr * trial_steps / (ms * 1e-3);
+                if (rate > rate_best) {
+                    rate_best = rate;
+                    pick[0] = C;
+                    pick[1] = W;
+                    pick[2] = F;
+                }
+                if (Fs[fi] >= trial_steps) break;
+            }
+        }
+    }
+    if (st == KAMI_OK) st = kami_vbd_set_tuning(h, pick[0], pick[1], pick[2]);
+    if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
+    if (e0) cudaEventDestroy(e0);
+    if (e1) cudaEventDestroy(e1);
+    cudaFree(snap);
+    if (st != KAMI_OK) return st;
+    if (best) {
+        best[0] = pick[0];
+        best[1] = pick[1];
+        best[2] = pick[2];
+    }
+    if (best_rate) *best_rate = rate_best;
     return KAMI_OK;
 }
 

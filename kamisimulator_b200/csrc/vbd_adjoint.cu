@@ -169,8 +169,9 @@ __device__ __forceinline__ void sdf_adjoint(float3 x, float3 v, float3& gx, floa
     gx = gx + qrotate(rot, ub);
 }
 
-template <int C>
-__global__ void __launch_bounds__(128) adjoint_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+// MINB blocks of 128 threads per SM: MINB = 4 caps the registers at 128 so 16 warps share an SM.
+template <int C, int MINB>
+__global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                            TapeView tp, AdjointState ad) {
     const int lane = threadIdx.x & 31;
     const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
@@ -245,14 +246,19 @@ __global__ void __launch_bounds__(128) adjoint_step_kernel(DeviceState st, PhysP
         gqr[k] = zero4();
     }
 
+    // iterate values after (n) and before (o) the iteration being reversed; the "before" values of
+    // one iteration are the "after" values of the next one down, so each tape row is read once
+    float3 dxn[C], dxo[C];
+    float4 qn[C], qo[C];
+#pragma unroll
+    for (int k = 0; k < C; k++) {
+        dxn[k] = xyz(tp.dx[row0 + (int64_t)N * S + 32LL * k]);
+        qn[k] = tp.q[row0 + (int64_t)N * S + 32LL * k];
+    }
     for (int it = N; it >= 1; it--) {
-        float3 dxn[C], dxo[C];
-        float4 qn[C], qo[C];
 #pragma unroll
         for (int k = 0; k < C; k++) {
-            dxn[k] = xyz(tp.dx[row0 + (int64_t)it * S + 32LL * k]);
             dxo[k] = xyz(tp.dx[row0 + (int64_t)(it - 1) * S + 32LL * k]);
-            qn[k] = tp.q[row0 + (int64_t)it * S + 32LL * k];
             qo[k] = tp.q[row0 + (int64_t)(it - 1) * S + 32LL * k];
         }
         float4 p1b[C], tq[C];
@@ -373,6 +379,8 @@ __global__ void __launch_bounds__(128) adjoint_step_kernel(DeviceState st, PhysP
         for (int k = 0; k < C; k++) {
             gq[k] = add4(gq[k], d3_vjp(qo[k], gd3[k]));
             gd3[k] = zero3();
+            dxn[k] = dxo[k];
+            qn[k] = qo[k];
         }
     }
 
@@ -417,9 +425,9 @@ cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, con
     const unsigned blocks = (unsigned)((st.num_tiles + warps_per_block - 1) / warps_per_block);
     if (blocks == 0) return cudaSuccess;
     if (C == 2)
-        fused_step_kernel<2, false, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, tp);
+        fused_step_kernel<2, false, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, tp, nullptr, 1);
     else if (C == 4)
-        fused_step_kernel<4, false, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, tp);
+        fused_step_kernel<4, false, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, tp, nullptr, 1);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();
@@ -431,9 +439,9 @@ cudaError_t launch_adjoint_step(const DeviceState& st, const PhysParams& pp, con
     const unsigned blocks = (unsigned)((st.num_tiles + wpb - 1) / wpb);
     if (blocks == 0) return cudaSuccess;
     if (C == 2)
-        adjoint_step_kernel<2><<<blocks, 32 * wpb, 0, s>>>(st, pp, sp, sdf, tp, ad);
+        adjoint_step_kernel<2, 4><<<blocks, 32 * wpb, 0, s>>>(st, pp, sp, sdf, tp, ad);
     else if (C == 4)
-        adjoint_step_kernel<4><<<blocks, 32 * wpb, 0, s>>>(st, pp, sp, sdf, tp, ad);
+        adjoint_step_kernel<4, 2><<<blocks, 32 * wpb, 0, s>>>(st, pp, sp, sdf, tp, ad);
     else
         return cudaErrorInvalidValue;
     return cudaGetLastError();

@@ -65,11 +65,13 @@ __device__ __forceinline__ float4 fused_orientation(float4 q, bool upd, bool pre
     return upd ? n : q;
 }
 
-// RECORD (colour2, one substep) additionally writes the step's start state and the iterates to a
-// tape for the adjoint (vbd_adjoint.cuh).
+// One launch runs `nsteps` consecutive steps, step j with clock and body transform steps[j] (or
+// `sp` when steps is null), keeping the tile's state in registers between them.  RECORD (colour2,
+// one step of one substep) additionally writes the step's start state and the iterates to a tape
+// for the adjoint (vbd_adjoint.cuh).
 template <int C, bool JACOBI, bool RECORD>
 __global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
-                                                         TapeView tp) {
+                                                         TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
     static_assert(!(RECORD && JACOBI), "the tape records the colour2 schedule");
     static_assert(C % 2 == 0, "slots per lane must be even");
     const int lane = threadIdx.x & 31;
@@ -117,9 +119,12 @@ __global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysPar
     const float ddH = __shfl_up_sync(0xffffffffu, ddN[C - 1], 1);
     const float kkH = __shfl_up_sync(0xffffffffu, kkN[C - 1], 1);
 
+    const float accel = pp.accel_ratio;
+    bool bad = false;
+    for (int step = 0; step < nsteps; step++) {
+    if (steps) sp = steps[step];
     const float h = sp.h;
     const float damp = pp.damping / h;
-    const float accel = pp.accel_ratio;
 
     for (int s = 0; s < sp.substeps; s++) {
         {
@@ -250,12 +255,15 @@ __global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysPar
 #pragma unroll
         for (int k = 0; k < C; k++) vbd_finish(x[k], v[k], dx[k], im[k], h, pp.velocity_decay);
     }
-
-    bool bad = false;
 #pragma unroll
     for (int k = 0; k < C; k++) {
         if (sdf.grid && (fl[k] & F_VALID) && !(fl[k] & F_ROOT)) vbd_sdf(x[k], v[k], sdf, sp);
         bad |= !finite3(x[k]) || !finite3(v[k]) || !finite4(q[k]);
+    }
+    }  // steps
+
+#pragma unroll
+    for (int k = 0; k < C; k++) {
         const int64_t g = base + 32LL * k;
         st.xm[g] = make_float4(x[k].x, x[k].y, x[k].z, im[k]);
         st.vel[g] = make_float4(v[k].x, v[k].y, v[k].z, 0.f);

@@ -247,7 +247,8 @@ cudaError_t launch_sweep_finish(const DeviceState& st, const float4* dx4, const 
 bool fused_supported(int C) { return C == 2 || C == 4; }
 
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
-                              int C, bool jacobi, int warps_per_block, cudaStream_t s) {
+                              int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps,
+                              int nsteps) {
     int threads = 32 * warps_per_block;
     unsigned blocks = blocks_for(st.num_tiles, warps_per_block);
     if (blocks == 0) return cudaSuccess;
@@ -255,9 +256,9 @@ cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const
 #define KAMI_FUSED_CASE(CC)                                                                        \
     if (C == CC) {                                                                                 \
         if (jacobi)                                                                                \
-            fused_step_kernel<CC, true, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, none);  \
+            fused_step_kernel<CC, true, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, none, d_steps, nsteps);  \
         else                                                                                       \
-            fused_step_kernel<CC, false, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, none); \
+            fused_step_kernel<CC, false, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, none, d_steps, nsteps); \
         return cudaGetLastError();                                                                 \
     }
     KAMI_FUSED_CASE(2)

@@ -18,8 +18,11 @@ cudaError_t launch_sweep_finish(const DeviceState& st, const float4* dx4, const 
                                 const SdfParams& sdf, bool apply_sdf, int64_t num_slots, cudaStream_t s);
 
 bool fused_supported(int C);
+// nsteps consecutive steps in one launch: parameters from d_steps[0..nsteps) (device), or sp when
+// d_steps is null (then nsteps must be 1).
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
-                              int C, bool jacobi, int warps_per_block, cudaStream_t s);
+                              int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps = nullptr,
+                              int nsteps = 1);
 
 cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                                 const TapeView& tp, int C, int warps_per_block, cudaStream_t s);

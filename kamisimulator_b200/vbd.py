@@ -32,6 +32,7 @@ EXPORTED = [
     "kami_vbd_set_orientations", "kami_vbd_get_rest_darboux", "kami_vbd_set_rest_darboux",
     "kami_vbd_set_body_transform", "kami_vbd_step", "kami_vbd_synchronize", "kami_vbd_state_size",
     "kami_vbd_get_state", "kami_vbd_set_state", "kami_vbd_last_error_string", "kami_vbd_version",
+    "kami_vbd_step_n", "kami_vbd_set_tuning", "kami_vbd_get_tuning", "kami_vbd_autotune",
     "kami_vbd_tape_reserve", "kami_vbd_step_record", "kami_vbd_backward", "kami_vbd_get_rest_darboux_grad",
     "kami_vbd_zero_rest_darboux_grad",
 ]
@@ -114,6 +115,10 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_state_size": [vp, ctypes.POINTER(ctypes.c_size_t)],
         "kami_vbd_get_state": [vp, vp, ctypes.c_size_t, i32],
         "kami_vbd_set_state": [vp, vp, ctypes.c_size_t, i32],
+        "kami_vbd_step_n": [vp, f32, i32, vp, vp],
+        "kami_vbd_set_tuning": [vp, i32, i32, i32],
+        "kami_vbd_get_tuning": [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)],
+        "kami_vbd_autotune": [vp, f32, i32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)],
         "kami_vbd_tape_reserve": [vp, i32],
         "kami_vbd_step_record": [vp, f32, vp],
         "kami_vbd_backward": [vp, vp, vp, vp, vp, i32, vp],
@@ -242,6 +247,31 @@ class Solver:
     def step(self, dt, stream=None):
         s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
         _check(self.lib.kami_vbd_step(self._h, ctypes.c_float(dt), s))
+
+    def step_n(self, dt, n, body_transforms=None, stream=None):
+        """n steps of dt; body_transforms: (n, 7) rotation xyzw + translation per step, or None."""
+        s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+        bt = None
+        if body_transforms is not None:
+            bt = _f32(body_transforms, (n, 7))
+        _check(self.lib.kami_vbd_step_n(self._h, ctypes.c_float(dt), n,
+                                        bt.ctypes.data_as(ctypes.c_void_p) if bt is not None else None, s))
+
+    def set_tuning(self, slots_per_lane=0, warps_per_block=0, steps_per_launch=0):
+        _check(self.lib.kami_vbd_set_tuning(self._h, slots_per_lane, warps_per_block, steps_per_launch))
+        self.slots_per_lane = self.get_tuning()[0]
+
+    def get_tuning(self):
+        c, w, f = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _check(self.lib.kami_vbd_get_tuning(self._h, ctypes.byref(c), ctypes.byref(w), ctypes.byref(f)))
+        return c.value, w.value, f.value
+
+    def autotune(self, dt, trial_steps=16):
+        best = (ctypes.c_int32 * 3)()
+        rate = ctypes.c_double()
+        _check(self.lib.kami_vbd_autotune(self._h, ctypes.c_float(dt), trial_steps, best, ctypes.byref(rate)))
+        self.slots_per_lane = best[0]
+        return (best[0], best[1], best[2]), rate.value
 
     def synchronize(self):
         _check(self.lib.kami_vbd_synchronize(self._h))
