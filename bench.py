@@ -270,7 +270,7 @@ def extra_forms(args, torch, stream, flush):
     vp = V * NUM_ITR * npl / (ms_p / 1e3)
     out["batched_64_grooms"] = {"value": vb, "ms_per_step": ms_b / nb, "vertices": V,
                                 "tuning": {"slots_per_lane": best[0], "warps_per_block": best[1],
-                                           "steps_per_launch": best[2]},
+                                           "steps_per_launch": best[2], "register_cap": best[3]},
                                 "plain_per_groom_value": vp, "plain_ms_per_step": ms_p / npl,
                                 "batched_over_plain": vb / vp,
                                 "what": "64 grooms (strands log-uniform [500, 20000], 16-128 vertices) in one handle, "
@@ -356,6 +356,7 @@ def run_ours(args):
     st = settings()
     V = g.num_vertices
     solver = Solver(g, form="fused", device=local, **st)
+    tuned, _ = solver.autotune(DT, trial_steps=8)  # the library's autotuner; restores the state
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
@@ -408,9 +409,11 @@ def run_ours(args):
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
-                "config": config_dict({"form": "fused", "per_gpu": "one 10,000 x 64 groom per GPU"}),
+                "config": config_dict({"form": "fused", "per_gpu": "one 10,000 x 64 groom per GPU",
+                                       "tuning": dict(zip(("slots_per_lane", "warps_per_block", "steps_per_launch",
+                                                           "register_cap"), tuned))}),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
-                             "frac": achieved / peak, "traffic": traffic, "kernel": "fused_step_kernel<2,false>",
+                             "frac": achieved / peak, "traffic": traffic, "kernel": "fused_step_kernel (colour2, one step per launch)",
                              "bytes_per_launch": V * BYTES_PER_VERTEX_STEP, "peak_source": peak_kind},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * V, "d2h_bytes_per_step": 24 * V,
                         "steps": e2e_steps},
@@ -432,10 +435,15 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
+    ap.add_argument("--only", choices=["adjoint"], help="run a single extra measurement (profiling runs)")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
-    if args.impl == "reference":
+    if args.only == "adjoint":
+        import torch
+
+        print(json.dumps(adjoint_timing(torch, torch.cuda.current_stream())), flush=True)
+    elif args.impl == "reference":
         run_reference(args)
     else:
         run_ours(args)

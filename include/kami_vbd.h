@@ -185,17 +185,19 @@ kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes,
 kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float* body_transforms, void* stream);
 
 /* Tile shape: slots per lane C (even, >= the longest strand / 32; changing it moves the state to the
- * new tiles), warps per CTA (1, 2, 4, 8) and steps per launch for kami_vbd_step_n (1..1024).
- * 0 leaves a value unchanged. */
+ * new tiles), warps per CTA (1, 2, 4, 8), steps per launch for kami_vbd_step_n (1..1024) and the
+ * register cap of the fused kernel (1 = none, 120 = at most 120 registers, C = 2 only: 17 instead of
+ * 16 warps per SM).  0 leaves a value unchanged. */
 kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32_t warps_per_block,
-                                int32_t steps_per_launch);
+                                int32_t steps_per_launch, int32_t register_cap);
 kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int32_t* warps_per_block,
-                                int32_t* steps_per_launch);
+                                int32_t* steps_per_launch, int32_t* register_cap);
 
-/* Times every tile shape on this handle's own strands (C in {min..4}, warps per CTA in {1,2,4,8},
- * steps per launch in {1,4,16}, trial_steps steps of dt each), keeps the fastest and restores the
- * simulation state and clock.  best = {C, warps, steps per launch}; best_rate in vertex-iters/s. */
-kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, int32_t best[3], double* best_rate);
+/* Times every tile shape on this handle's own strands (C in {min..4}, register cap {none, 120} for
+ * C = 2, warps per CTA in {1,2,4,8}, steps per launch in {1,4,16}; trial_steps steps of dt each),
+ * keeps the fastest and restores the simulation state and clock.
+ * best = {C, warps, steps per launch, register cap}; best_rate in vertex-iters/s. */
+kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, int32_t best[4], double* best_rate);
 
 /* ---- differentiable stepping ---------------------------------------------------------------------
  * No counterpart in the reference, which has no adjoint.  The fused colour2 step (no wind, one

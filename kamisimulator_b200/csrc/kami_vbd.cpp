@@ -83,6 +83,7 @@ struct kami_vbd_solver {
 
     // multi-step launches (kami_vbd_step_n) and tuning
     int steps_per_launch = 8;
+    int reg_cap = 0;  // 0: fused kernel without a register cap; 120: the 120-register variant (C = 2)
     StepParams* d_steps = nullptr;
     int d_steps_cap = 0;
     std::vector<StepParams> h_steps;
@@ -565,7 +566,7 @@ kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
         if (h->form == KAMI_FORM_FUSED) {
             KAMI_CUDA(launch_fused_step(h->dstate(), h->pp, sp, h->sdf, h->layout.C, h->schedule == KAMI_SCHEDULE_JACOBI,
-                                        h->warps_per_block, s),
+                                        h->warps_per_block, s, nullptr, 1, h->reg_cap),
                       "fused step launch");
         } else {
             KAMI_TRY(build_sweep_graph(h, steps));
@@ -649,7 +650,7 @@ static kami_status relayout(kami_vbd_solver* h, int C) {
 }
 
 kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32_t warps_per_block,
-                                int32_t steps_per_launch) {
+                                int32_t steps_per_launch, int32_t register_cap) {
     KAMI_TRY(valid_handle(h));
     if (slots_per_lane != 0) {
         const int cmin = slots_per_lane_for(h->strand_begin.data(), h->ns);
@@ -671,15 +672,23 @@ kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32
         if (steps_per_launch != h->steps_per_launch) drop_graphs(h);
         h->steps_per_launch = steps_per_launch;
     }
+    if (register_cap != 0) {
+        if (register_cap != 1 && register_cap != 120)
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "register_cap must be 0 (unchanged), 1 (none) or 120");
+        const int cap = register_cap == 120 ? 120 : 0;
+        if (cap != h->reg_cap) drop_graphs(h);
+        h->reg_cap = cap;
+    }
     return KAMI_OK;
 }
 
 kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int32_t* warps_per_block,
-                                int32_t* steps_per_launch) {
+                                int32_t* steps_per_launch, int32_t* register_cap) {
     if (!h) return fail(KAMI_ERR_INVALID_ARGUMENT, "null handle");
     if (slots_per_lane) *slots_per_lane = h->layout.C;
     if (warps_per_block) *warps_per_block = h->warps_per_block;
     if (steps_per_launch) *steps_per_launch = h->steps_per_launch;
+    if (register_cap) *register_cap = h->reg_cap == 120 ? 120 : 1;
     return KAMI_OK;
 }
 
@@ -718,7 +727,7 @@ kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float*
         for (int j0 = 0; j0 < n && err == cudaSuccess; j0 += F)
             err = launch_fused_step(h->dstate(), h->pp, h->h_steps[0], h->sdf, h->layout.C,
                                     h->schedule == KAMI_SCHEDULE_JACOBI, h->warps_per_block, h->stream, h->d_steps + j0,
-                                    std::min(F, n - j0));
+                                    std::min(F, n - j0), h->reg_cap);
         cudaGraph_t g = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
         if (err != cudaSuccess || e2 != cudaSuccess) {
@@ -739,7 +748,7 @@ kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float*
     });
 }
 
-kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, int32_t best[3], double* best_rate) {
+kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, int32_t best[4], double* best_rate) {
     KAMI_TRY(valid_handle(h));
     if (h->form != KAMI_FORM_FUSED) return fail(KAMI_ERR_UNSUPPORTED, "the autotuner tunes the fused form");
     if (trial_steps < 1 || !(dt > 0.f)) return fail(KAMI_ERR_INVALID_ARGUMENT, "need trial_steps >= 1 and dt > 0");
@@ -755,12 +764,14 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
     const int cmin = slots_per_lane_for(h->strand_begin.data(), h->ns);
     const int Fs[3] = {1, 4, 16};
     double rate_best = -1.0;
-    int pick[3] = {h->layout.C, h->warps_per_block, h->steps_per_launch};
+    int pick[4] = {h->layout.C, h->warps_per_block, h->steps_per_launch, h->reg_cap == 120 ? 120 : 1};
     for (int C = cmin; C <= 4 && st == KAMI_OK; C += 2) {
+        for (int R = 0; R < (C == 2 ? 2 : 1) && st == KAMI_OK; R++) {
+        const int cap = R ? 120 : 1;
         for (int W = 1; W <= 8 && st == KAMI_OK; W *= 2) {
             for (int fi = 0; fi < 3 && st == KAMI_OK; fi++) {
                 const int F = std::min(Fs[fi], trial_steps);
-                st = kami_vbd_set_tuning(h, C, W, F);
+                st = kami_vbd_set_tuning(h, C, W, F, cap);
                 if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
                 if (st == KAMI_OK) st = kami_vbd_step_n(h, dt, trial_steps, nullptr, nullptr);  // warm-up, builds the graph
                 if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
@@ -781,22 +792,21 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
                     pick[0] = C;
                     pick[1] = W;
                     pick[2] = F;
+                    pick[3] = cap;
                 }
                 if (Fs[fi] >= trial_steps) break;
             }
         }
+        }
     }
-    if (st == KAMI_OK) st = kami_vbd_set_tuning(h, pick[0], pick[1], pick[2]);
+    if (st == KAMI_OK) st = kami_vbd_set_tuning(h, pick[0], pick[1], pick[2], pick[3]);
     if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);
     cudaFree(snap);
     if (st != KAMI_OK) return st;
-    if (best) {
-        best[0] = pick[0];
-        best[1] = pick[1];
-        best[2] = pick[2];
-    }
+    if (best)
+        for (int i = 0; i < 4; i++) best[i] = pick[i];
     if (best_rate) *best_rate = rate_best;
     return KAMI_OK;
 }

@@ -27,6 +27,14 @@
 namespace kami {
 
 __device__ __forceinline__ float4 qconj(float4 a) { return make_float4(-a.x, -a.y, -a.z, a.w); }
+
+// 16-byte asynchronous global -> shared copies (each lane copies and later reads only its own cells).
+__device__ __forceinline__ void cp_async16(void* smem, const void* gmem) {
+    const unsigned s = (unsigned)__cvta_generic_to_shared(smem);
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 16;\n" ::"r"(s), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all_but_one() { asm volatile("cp.async.wait_group 1;\n" ::: "memory"); }
 __device__ __forceinline__ float4 zero4() { return make_float4(0.f, 0.f, 0.f, 0.f); }
 __device__ __forceinline__ float3 zero3() { return f3(0.f, 0.f, 0.f); }
 
@@ -247,19 +255,38 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
     }
 
     // iterate values after (n) and before (o) the iteration being reversed; the "before" values of
-    // one iteration are the "after" values of the next one down, so each tape row is read once
+    // one iteration are the "after" values of the next one down, so each tape row is read once.  The
+    // row of the next iteration down is prefetched into shared memory (double buffer per warp) while
+    // the current one is reversed.
+    __shared__ float4 pref[4][2][2][C][32];  // [warp in CTA][buffer][dx | q][slot row][lane]
+    float4 (*mine)[2][C][32] = pref[threadIdx.x >> 5];
     float3 dxn[C], dxo[C];
     float4 qn[C], qo[C];
 #pragma unroll
     for (int k = 0; k < C; k++) {
         dxn[k] = xyz(tp.dx[row0 + (int64_t)N * S + 32LL * k]);
         qn[k] = tp.q[row0 + (int64_t)N * S + 32LL * k];
+        if (N >= 1) {
+            cp_async16(&mine[0][0][k][lane], &tp.dx[row0 + (int64_t)(N - 1) * S + 32LL * k]);
+            cp_async16(&mine[0][1][k][lane], &tp.q[row0 + (int64_t)(N - 1) * S + 32LL * k]);
+        }
     }
+    cp_async_commit();
     for (int it = N; it >= 1; it--) {
+        const int buf = (N - it) & 1;
+        if (it >= 2) {
+#pragma unroll
+            for (int k = 0; k < C; k++) {
+                cp_async16(&mine[buf ^ 1][0][k][lane], &tp.dx[row0 + (int64_t)(it - 2) * S + 32LL * k]);
+                cp_async16(&mine[buf ^ 1][1][k][lane], &tp.q[row0 + (int64_t)(it - 2) * S + 32LL * k]);
+            }
+        }
+        cp_async_commit();
+        cp_async_wait_all_but_one();  // this iteration's row has landed
 #pragma unroll
         for (int k = 0; k < C; k++) {
-            dxo[k] = xyz(tp.dx[row0 + (int64_t)(it - 1) * S + 32LL * k]);
-            qo[k] = tp.q[row0 + (int64_t)(it - 1) * S + 32LL * k];
+            dxo[k] = xyz(mine[buf][0][k][lane]);
+            qo[k] = mine[buf][1][k][lane];
         }
         float4 p1b[C], tq[C];
         float3 tv[C];

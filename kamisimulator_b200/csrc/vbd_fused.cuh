@@ -70,8 +70,8 @@ __device__ __forceinline__ float4 fused_orientation(float4 q, bool upd, bool pre
 // one step of one substep) additionally writes the step's start state and the iterates to a tape
 // for the adjoint (vbd_adjoint.cuh).
 template <int C, bool JACOBI, bool RECORD>
-__global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
-                                                         TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
+__device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
     static_assert(!(RECORD && JACOBI), "the tape records the colour2 schedule");
     static_assert(C % 2 == 0, "slots per lane must be even");
     const int lane = threadIdx.x & 31;
@@ -271,6 +271,20 @@ __global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysPar
         st.q[g] = q[k];
     }
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(st.status, STATUS_NONFINITE);
+}
+
+template <int C, bool JACOBI, bool RECORD>
+__global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                         TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
+    fused_step_body<C, JACOBI, RECORD>(st, pp, sp, sdf, tp, steps, nsteps);
+}
+
+// The same step with at most 120 registers per thread, so 17 warps (instead of 16) share an SM: a
+// launch whose tile count is just above a multiple of 16 warps per SM then needs one wave less.
+template <int C, bool JACOBI>
+__global__ void __maxnreg__(120) fused_step_kernel_r120(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                       TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
+    fused_step_body<C, JACOBI, false>(st, pp, sp, sdf, tp, steps, nsteps);
 }
 
 }  // namespace kami

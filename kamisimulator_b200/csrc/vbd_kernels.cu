@@ -248,10 +248,17 @@ bool fused_supported(int C) { return C == 2 || C == 4; }
 
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps,
-                              int nsteps) {
+                              int nsteps, int reg_cap) {
     int threads = 32 * warps_per_block;
     unsigned blocks = blocks_for(st.num_tiles, warps_per_block);
     if (blocks == 0) return cudaSuccess;
+    if (reg_cap == 120 && C == 2) {
+        if (jacobi)
+            fused_step_kernel_r120<2, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, TapeView{}, d_steps, nsteps);
+        else
+            fused_step_kernel_r120<2, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, TapeView{}, d_steps, nsteps);
+        return cudaGetLastError();
+    }
     const TapeView none{};
 #define KAMI_FUSED_CASE(CC)                                                                        \
     if (C == CC) {                                                                                 \

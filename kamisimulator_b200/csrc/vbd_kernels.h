@@ -22,7 +22,7 @@ bool fused_supported(int C);
 // d_steps is null (then nsteps must be 1).
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps = nullptr,
-                              int nsteps = 1);
+                              int nsteps = 1, int reg_cap = 0);
 
 cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                                 const TapeView& tp, int C, int warps_per_block, cudaStream_t s);

@@ -116,8 +116,8 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_get_state": [vp, vp, ctypes.c_size_t, i32],
         "kami_vbd_set_state": [vp, vp, ctypes.c_size_t, i32],
         "kami_vbd_step_n": [vp, f32, i32, vp, vp],
-        "kami_vbd_set_tuning": [vp, i32, i32, i32],
-        "kami_vbd_get_tuning": [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)],
+        "kami_vbd_set_tuning": [vp, i32, i32, i32, i32],
+        "kami_vbd_get_tuning": [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)],
         "kami_vbd_autotune": [vp, f32, i32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)],
         "kami_vbd_tape_reserve": [vp, i32],
         "kami_vbd_step_record": [vp, f32, vp],
@@ -257,21 +257,23 @@ class Solver:
         _check(self.lib.kami_vbd_step_n(self._h, ctypes.c_float(dt), n,
                                         bt.ctypes.data_as(ctypes.c_void_p) if bt is not None else None, s))
 
-    def set_tuning(self, slots_per_lane=0, warps_per_block=0, steps_per_launch=0):
-        _check(self.lib.kami_vbd_set_tuning(self._h, slots_per_lane, warps_per_block, steps_per_launch))
+    def set_tuning(self, slots_per_lane=0, warps_per_block=0, steps_per_launch=0, register_cap=0):
+        _check(self.lib.kami_vbd_set_tuning(self._h, slots_per_lane, warps_per_block, steps_per_launch, register_cap))
         self.slots_per_lane = self.get_tuning()[0]
 
     def get_tuning(self):
-        c, w, f = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
-        _check(self.lib.kami_vbd_get_tuning(self._h, ctypes.byref(c), ctypes.byref(w), ctypes.byref(f)))
-        return c.value, w.value, f.value
+        c, w, f, r = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int32()
+        _check(self.lib.kami_vbd_get_tuning(self._h, ctypes.byref(c), ctypes.byref(w), ctypes.byref(f),
+                                            ctypes.byref(r)))
+        return c.value, w.value, f.value, r.value
 
     def autotune(self, dt, trial_steps=16):
-        best = (ctypes.c_int32 * 3)()
+        """Returns ((slots_per_lane, warps_per_block, steps_per_launch, register_cap), vertex-iters/s)."""
+        best = (ctypes.c_int32 * 4)()
         rate = ctypes.c_double()
         _check(self.lib.kami_vbd_autotune(self._h, ctypes.c_float(dt), trial_steps, best, ctypes.byref(rate)))
         self.slots_per_lane = best[0]
-        return (best[0], best[1], best[2]), rate.value
+        return tuple(best), rate.value
 
     def synchronize(self):
         _check(self.lib.kami_vbd_synchronize(self._h))

@@ -52,6 +52,9 @@ def test_relayout_keeps_the_trajectory():
         b.step(1 / 120)
     b.set_tuning(slots_per_lane=4, warps_per_block=2)
     assert b.get_tuning()[:2] == (4, 2)
+    # the 120-register variant of the C = 2 kernel gives the same trajectory
+    a.set_tuning(register_cap=120)
+    assert a.get_tuning()[3] == 120
     np.testing.assert_array_equal(a.get_state(), b.get_state())
     for _ in range(3):
         a.step(1 / 120)
@@ -70,7 +73,7 @@ def test_autotune_picks_a_shape_and_restores_the_state():
     s.step(1 / 120)
     before = s.get_state()
     best, rate = s.autotune(1 / 120, trial_steps=8)
-    assert best[0] in (4,) and best[1] in (1, 2, 4, 8) and best[2] in (1, 4, 8)
+    assert best[0] in (4,) and best[1] in (1, 2, 4, 8) and best[2] in (1, 4, 8) and best[3] in (1, 120)
     assert rate > 0
     np.testing.assert_array_equal(s.get_state(), before)
     ref = helpers.gpu_solver(g, st, form="fused")
