@@ -135,6 +135,23 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+def max_over_ranks(value, world, device="cuda"):
+    """Largest `value` over all ranks (the job's time is the slowest rank's); identity for one rank."""
+    if world <= 1:
+        return float(value)
+    import torch
+    import torch.distributed as dist
+
+    t = torch.tensor([float(value)], dtype=torch.float64, device=device)
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def job_throughput(world, vertices_per_rank, num_itr, steps, max_ms):
+    """Whole-job vertex-iterations per second: every rank steps its own groom (weak scaling)."""
+    return world * vertices_per_rank * num_itr * steps / (max_ms / 1e3)
+
+
 def dist_setup():
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -373,12 +390,8 @@ def run_ours(args):
         barrier()
         step_ms = time_steps(solver, args.steps, stream, flush)
         barrier()
-    t = torch.tensor([step_ms], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    max_ms = float(t.item())
-    units = world * V * NUM_ITR * args.steps
-    value = units / (max_ms / 1e3)
+    max_ms = max_over_ranks(step_ms, world)
+    value = job_throughput(world, V, NUM_ITR, args.steps, max_ms)
     ms_step = max_ms / args.steps
 
     # end to end through the C ABI with pinned host buffers
@@ -395,10 +408,7 @@ def run_ours(args):
         solver.get_positions_velocities(xh.numpy(), vh.numpy())
     e1.record(stream)
     torch.cuda.synchronize()
-    t = torch.tensor([e0.elapsed_time(e1)], dtype=torch.float64, device="cuda")
-    if world > 1:
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-    e2e_value = world * V * NUM_ITR * e2e_steps / (float(t.item()) / 1e3)
+    e2e_value = job_throughput(world, V, NUM_ITR, e2e_steps, max_over_ranks(e0.elapsed_time(e1), world))
     solver.close()
 
     line = None

@@ -1,0 +1,54 @@
+"""The multi-rank logic of bench.py on CPU: two gloo ranks (torch.distributed), no GPU.
+
+Each rank steps its own groom (weak scaling, no data-path collective); the job time is the slowest
+rank's, and the reference arm runs on rank 0 only."""
+import os
+import socket
+
+import pytest
+import torch.multiprocessing as mp
+
+
+def _free_port():
+    with socket.socket() as s:
+        s.bind(("127.0.0.1", 0))
+        return s.getsockname()[1]
+
+
+def _rank_main(rank, world, port, out):
+    import torch.distributed as dist
+
+    import bench
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        local_ms = 10.0 * (rank + 1)  # rank 1 is the slow one
+        m = bench.max_over_ranks(local_ms, world, device="cpu")
+        out[rank] = (m, bench.job_throughput(world, 640000, 20, 100, m))
+        dist.barrier()
+    finally:
+        dist.destroy_process_group()
+
+
+def test_max_over_ranks_and_weak_scaling_throughput():
+    world = 2
+    port = _free_port()
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.spawn(_rank_main, args=(world, port, out), nprocs=world, join=True)
+    assert out[0][0] == 20.0 and out[1][0] == 20.0
+    # 2 ranks x 640,000 vertices x 20 iterations x 100 steps in 20 ms
+    assert out[0][1] == pytest.approx(2 * 640000 * 20 * 100 / 0.020)
+
+
+def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
+    import bench
+
+    class Args:
+        steps, warmup, gpus = 3, 3, 2
+
+    monkeypatch.setenv("WORLD_SIZE", "2")
+    monkeypatch.setenv("RANK", "1")
+    bench.run_reference(Args())
+    assert capsys.readouterr().out == ""

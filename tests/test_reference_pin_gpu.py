@@ -92,3 +92,41 @@ def test_sdf_pass_matches_reference_kernel():
         assert np.mean(np.any(rp != p, axis=1)) > 0.01  # the pass really projected some particles
         assert float(np.abs(o.x - rp).max()) <= 1e-6
         assert float(np.abs(xs - rp).max()) <= 1e-6
+
+
+def test_reference_gpu_speed_on_the_groom():
+    """The reference's own CUDA Sim (Jacobi kernels, one CUDA graph per advance, error check per
+    advance) against this solver on the 10,000 x 64 groom, 20 iterations, dt = max_h = 1/120, no SDF.
+    Reported (pytest -s); the assertion only checks that the fused form is faster."""
+    import time
+
+    import torch
+
+    g = synth.groom(10000, 64, seed=2)
+    g.strand_young[:] = 2.0
+    r = ref_sim.RefSim(g, young=2.0, num_itr=20, max_h=1 / 120)
+    for _ in range(3):
+        r.advance(1 / 120)
+    n = 50
+    t0 = time.perf_counter()
+    for _ in range(n):
+        r.advance(1 / 120)  # returns after the reference's own stream synchronisation
+    ref_ms = (time.perf_counter() - t0) * 1e3 / n
+    r.close()
+    out = {"reference_ms_per_step": ref_ms,
+           "reference_vertex_iters_per_s": g.num_vertices * 20 / (ref_ms * 1e-3)}
+    st = dict(num_itr=20, max_h=1 / 120, gravity=(0.0, 0.0, -9.81), radius=40e-6)
+    for form, sched in (("fused", "jacobi"), ("fused", "colour2"), ("sweep", "jacobi")):
+        s = helpers.gpu_solver(g, dict(st, schedule=sched), form=form)
+        for _ in range(3):
+            s.step(1 / 120)
+        s.synchronize()
+        t0 = time.perf_counter()
+        for _ in range(n):
+            s.step(1 / 120)
+        s.synchronize()
+        ms = (time.perf_counter() - t0) * 1e3 / n
+        out[f"ours_{form}_{sched}_ms_per_step"] = ms
+        s.close()
+    print("reference GPU speed", out)
+    assert out["ours_fused_jacobi_ms_per_step"] < ref_ms
