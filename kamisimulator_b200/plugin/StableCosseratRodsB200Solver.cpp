@@ -1,0 +1,189 @@
+// StableCosseratRodsB200Solver.cpp -- the Solver plugin on the C ABI (see kami_plugin.h).
+#include <cmath>
+#include <fstream>
+#include <sstream>
+#include <stdexcept>
+
+#include "json_lite.h"
+#include "kami_plugin.h"
+
+namespace kami {
+
+namespace {
+
+std::string read_file(const std::string& path) {
+    std::ifstream f(path);
+    if (!f) throw std::runtime_error("cannot open settings file " + path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    return ss.str();
+}
+
+}  // namespace
+
+StableCosseratRodsB200Solver::~StableCosseratRodsB200Solver() {
+    if (handle_) kami_vbd_destroy(handle_);
+}
+
+void StableCosseratRodsB200Solver::check(kami_status st, const char* what) {
+    if (st != KAMI_OK) throw std::runtime_error(std::string(what) + ": " + kami_vbd_last_error_string());
+}
+
+void StableCosseratRodsB200Solver::SetBodyTransform(const float rotation_xyzw[4], const float translate[3]) {
+    if (handle_) check(kami_vbd_set_body_transform(handle_, rotation_xyzw, translate), "SetBodyTransform");
+}
+
+// StableCosseratRodsSolver::LoadSettingJsonContent + BuildYarnBallHair (StableCosseratRodsSolver.cpp:76-212).
+kami_vbd_desc StableCosseratRodsB200Solver::BuildDescriptor(const std::string& settingJsonPath) {
+    kami_vbd_desc d;
+    check(kami_vbd_desc_init(&d), "kami_vbd_desc_init");
+    // reference solver defaults (JsonParams(), StableCosseratRodsSolver.h:86-111) beyond the C-ABI ones
+    bool use_young = true;
+    float curve_radius = 4e-5f;
+    d.num_itr = 8;
+    d.wind_peak = 40.f;
+    d.gravity[0] = 0.f;
+    d.gravity[1] = -9.8f;  // MetaData default (YBSimulator.cu:84)
+    d.gravity[2] = 0.f;
+    enable_sdf_ = true;
+    sdf_threshold_ = 0.015f;
+    std::map<std::string, JsonValue> j;
+    if (!settingJsonPath.empty()) {
+        settings_dump_ = read_file(settingJsonPath);
+        j = parse_json_object(settings_dump_);
+    }
+    auto num = [&](const char* k, float& dst) {
+        auto it = j.find(k);
+        if (it != j.end() && it->second.kind == JsonValue::Number) dst = (float)it->second.number;
+    };
+    auto boolean = [&](const char* k, bool& dst) {
+        auto it = j.find(k);
+        if (it != j.end() && it->second.kind == JsonValue::Bool) dst = it->second.boolean;
+    };
+    float num_itr = (float)d.num_itr, sag_free = 0.f;
+    bool hair_hair = false;
+    num("NumItr", num_itr);
+    num("YoungsModule", d.young);
+    num("StiffnessDeviationCoeff", d.deviation);
+    num("StretchK", d.k_stretch);
+    num("BendK", d.k_bend);
+    num("CurveRadius", curve_radius);
+    num("Density", d.density);
+    num("VelocityDecay", d.velocity_decay);
+    num("ExternalForceMultiplier", d.external_force_multiplier);
+    num("WindPeak", d.wind_peak);
+    num("WindYFreq", d.wind_y_freq);
+    num("WindZFreq", d.wind_z_freq);
+    num("WindTimeFreq", d.wind_time_freq);
+    num("WindSharpness", d.wind_sharpness);
+    num("SagFreeItr", sag_free);
+    num("MaxTimeStep", d.max_h);
+    num("SDFThreshold", sdf_threshold_);
+    boolean("UseYoungsModule", use_young);
+    boolean("EnableSDF", enable_sdf_);
+    boolean("EnableHairHairColl", hair_hair);
+    if (hair_hair) throw std::runtime_error("EnableHairHairColl is not supported by the B200 solver");
+    if (sag_free > 0) throw std::runtime_error("SagFreeItr > 0 is not supported by the B200 solver");
+    auto g = j.find("Gravity");
+    if (g != j.end() && g->second.kind == JsonValue::Array && g->second.array.size() == 3)
+        for (int a = 0; a < 3; a++) d.gravity[a] = (float)g->second.array[a];
+    auto sch = j.find("Schedule");
+    if (sch != j.end() && sch->second.kind == JsonValue::String) {
+        if (sch->second.text == "jacobi") d.schedule = KAMI_SCHEDULE_JACOBI;
+        else if (sch->second.text == "colour2") d.schedule = KAMI_SCHEDULE_COLOUR2;
+        else throw std::runtime_error("Schedule must be \"colour2\" or \"jacobi\"");
+    }
+    auto frm = j.find("Form");
+    if (frm != j.end() && frm->second.kind == JsonValue::String) {
+        if (frm->second.text == "fused") d.form = KAMI_FORM_FUSED;
+        else if (frm->second.text == "sweep") d.form = KAMI_FORM_SWEEP;
+        else if (frm->second.text == "auto") d.form = KAMI_FORM_AUTO;
+        else throw std::runtime_error("Form must be \"auto\", \"fused\" or \"sweep\"");
+    }
+    d.num_itr = (int32_t)num_itr;
+    d.radius = 0.05f * curve_radius;  // StableCosseratRodsSolver.cpp:177-179
+    d.stiffness_mode = use_young ? KAMI_STIFFNESS_YOUNG : KAMI_STIFFNESS_K;
+    d.pin_roots = 1;
+
+    // the Hair's strands with >= 4 vertices, packed (StableCosseratRodsSolver.cpp:127-173)
+    Hair& hair = *hair_;
+    strand_refs_.clear();
+    strand_begin_.assign(1, 0);
+    packed_pos_.clear();
+    for (uint32_t s = 0; s < hair.num_strands; s++) {
+        const uint32_t n = hair.strand_vert_count[s];
+        if (n < 4) continue;
+        strand_refs_.push_back((int)s);
+        for (uint32_t v = 0; v < n; v++) packed_pos_.insert(packed_pos_.end(), hair.pos(s, v), hair.pos(s, v) + 3);
+        strand_begin_.push_back(strand_begin_.back() + (int32_t)n);
+    }
+    packed_vel_.assign(packed_pos_.size(), 0.f);
+    d.num_strands = (int32_t)strand_refs_.size();
+    d.strand_begin = strand_begin_.data();
+    d.positions = packed_pos_.data();
+    d.velocities = nullptr;
+    d.sdf = nullptr;
+    if (enable_sdf_ && has_body_) {
+        sdf_desc_ = kami_vbd_sdf_desc{};
+        for (int a = 0; a < 3; a++) {
+            sdf_desc_.dims[a] = body_.dims[a];
+            sdf_desc_.grid_min[a] = body_.grid_min[a];
+            sdf_desc_.grid_max[a] = body_.grid_max[a];
+        }
+        sdf_desc_.threshold = sdf_threshold_;
+        sdf_desc_.phi = body_.phi.data();
+        sdf_desc_.grad = body_.grad.data();
+        d.sdf = &sdf_desc_;
+    }
+    return d;
+}
+
+void StableCosseratRodsB200Solver::Construct(const std::string& settingJsonPath) {
+    kami_vbd_desc d = BuildDescriptor(settingJsonPath);
+    if (d.num_strands == 0) throw std::runtime_error("the Hair has no strand with at least 4 vertices");
+    if (handle_) kami_vbd_destroy(handle_);
+    handle_ = nullptr;
+    check(kami_vbd_create(&d, &handle_), "Construct");
+}
+
+void StableCosseratRodsB200Solver::SolveNextStep(float dt) { check(kami_vbd_step(handle_, dt, nullptr), "SolveNextStep"); }
+
+// Sim -> Hair (StableCosseratRodsSolver.cpp:258-277)
+void StableCosseratRodsB200Solver::DownloadHair() {
+    check(kami_vbd_get_positions_velocities(handle_, packed_pos_.data(), packed_vel_.data(), KAMI_MEMORY_HOST),
+          "DownloadHair");
+    Hair& hair = *hair_;
+    for (size_t i = 0; i < strand_refs_.size(); i++) {
+        const uint32_t s = (uint32_t)strand_refs_[i];
+        for (int32_t v = 0; v < strand_begin_[i + 1] - strand_begin_[i]; v++)
+            for (int a = 0; a < 3; a++) {
+                hair.pos(s, v)[a] = packed_pos_[3 * (strand_begin_[i] + v) + a];
+                hair.vel(s, v)[a] = packed_vel_[3 * (strand_begin_[i] + v) + a];
+            }
+    }
+}
+
+// Hair -> Sim (StableCosseratRodsSolver.cpp:238-256)
+void StableCosseratRodsB200Solver::UploadHair() {
+    Hair& hair = *hair_;
+    for (size_t i = 0; i < strand_refs_.size(); i++) {
+        const uint32_t s = (uint32_t)strand_refs_[i];
+        for (int32_t v = 0; v < strand_begin_[i + 1] - strand_begin_[i]; v++)
+            for (int a = 0; a < 3; a++) {
+                packed_pos_[3 * (strand_begin_[i] + v) + a] = hair.pos(s, v)[a];
+                packed_vel_[3 * (strand_begin_[i] + v) + a] = hair.vel(s, v)[a];
+            }
+    }
+    check(kami_vbd_set_positions_velocities(handle_, packed_pos_.data(), packed_vel_.data(), KAMI_MEMORY_HOST),
+          "UploadHair");
+}
+
+std::string StableCosseratRodsB200Solver::GetInfoString() {
+    std::stringstream ss;
+    ss << "Solver: Stable Cosserat Rods (B200, " << kami_vbd_version() << ")\n";
+    ss << "Simulated strands: " << strand_refs_.size() << "\n";
+    ss << "Json:\n" << settings_dump_;
+    return ss.str();
+}
+
+}  // namespace kami

@@ -1,0 +1,93 @@
+// kami_plugin.h -- the C++ solver plugin that drops into KamiSimulator's Solver interface
+// (src/solvers/Solver.h:13-85), on top of the C ABI in include/kami_vbd.h.
+//
+// Hair mirrors the part of KamiSimulator's Hair the StableCosseratRods solver reads and writes
+// (src/Hair.h:10-52, LinearUtil.h:150-176): a padded [strand][vertex] array of positions and
+// velocities plus the vertex count of each strand.  Solver mirrors the reference's abstract plugin
+// (same method names and meanings: Construct(settings json), SolveNextStep(dt in seconds),
+// UploadHair, DownloadHair, GetInfoString).
+#pragma once
+#include <cstdint>
+#include <memory>
+#include <string>
+#include <vector>
+
+#include "kami_vbd.h"
+
+namespace kami {
+
+struct Hair {
+    uint32_t num_strands = 0;
+    uint32_t max_verts = 0;                 // hairSize.y
+    std::vector<uint32_t> strand_vert_count;
+    std::vector<float> positions;           // num_strands * max_verts * 3
+    std::vector<float> velocities;          // same layout
+    float* pos(uint32_t s, uint32_t v) { return &positions[((size_t)s * max_verts + v) * 3]; }
+    float* vel(uint32_t s, uint32_t v) { return &velocities[((size_t)s * max_verts + v) * 3]; }
+};
+
+class Solver {
+   public:
+    explicit Solver(std::shared_ptr<Hair> hair) : hair_(std::move(hair)) {}
+    virtual ~Solver() = default;
+    virtual void Construct(const std::string& settingJsonPath = "") = 0;
+    virtual void SolveNextStep(float dt) = 0;  // dt in seconds (1 / (fps * internal steps))
+    virtual void UploadHair() = 0;
+    virtual void DownloadHair() = 0;
+    virtual std::string GetInfoString() = 0;
+
+   protected:
+    std::shared_ptr<Hair> hair_;
+};
+
+// Body collision input: the head's signed-distance grid (as SDFBodyCollisionSolver builds it from
+// the body mesh) and its rigid transform.
+struct BodySDF {
+    int32_t dims[3] = {0, 0, 0};
+    float grid_min[3] = {0, 0, 0}, grid_max[3] = {0, 0, 0};
+    std::vector<float> phi, grad;
+};
+
+// The StableCosseratRods solver on B200.  Settings keys are those of the reference's solver JSON
+// (StableCosseratRodsSolver.h:41-112): NumItr, UseYoungsModule, YoungsModule,
+// StiffnessDeviationCoeff, StretchK, BendK, CurveRadius (the simulated radius is 0.05 x CurveRadius,
+// StableCosseratRodsSolver.cpp:177-179), Density, VelocityDecay, ExternalForceMultiplier, Wind*,
+// EnableSDF, EnableHairHairColl, SagFreeItr, SubdivCoeff, EnableResample, plus SDFThreshold
+// (SDFBodyCollisionSolver.h:25) and the extensions MaxTimeStep (the reference fixes 4e-4 s),
+// Gravity [x, y, z], Schedule ("colour2" | "jacobi") and Form ("auto" | "fused" | "sweep").
+// Strands with fewer than 4 vertices are skipped, as there (StableCosseratRodsSolver.cpp:134-136).
+// Resampling and subdivision are Hair preprocessing that KamiSimulator runs before Construct.
+class StableCosseratRodsB200Solver : public Solver {
+   public:
+    explicit StableCosseratRodsB200Solver(std::shared_ptr<Hair> hair) : Solver(std::move(hair)) {}
+    ~StableCosseratRodsB200Solver() override;
+
+    void SetBody(const BodySDF& body) { body_ = body; has_body_ = true; }
+    void SetBodyTransform(const float rotation_xyzw[4], const float translate[3]);
+
+    // Fills the C-ABI descriptor from the settings file and the Hair, without touching a device.
+    kami_vbd_desc BuildDescriptor(const std::string& settingJsonPath);
+
+    void Construct(const std::string& settingJsonPath = "") override;
+    void SolveNextStep(float dt) override;
+    void UploadHair() override;
+    void DownloadHair() override;
+    std::string GetInfoString() override;
+
+    kami_vbd_handle handle() const { return handle_; }
+
+   private:
+    kami_vbd_handle handle_ = nullptr;
+    BodySDF body_;
+    bool has_body_ = false;
+    bool enable_sdf_ = true;
+    float sdf_threshold_ = 0.015f;
+    std::string settings_dump_;
+    std::vector<int> strand_refs_;      // Hair strand of each simulated strand
+    std::vector<int32_t> strand_begin_;
+    std::vector<float> packed_pos_, packed_vel_;
+    kami_vbd_sdf_desc sdf_desc_{};
+    void check(kami_status st, const char* what);
+};
+
+}  // namespace kami

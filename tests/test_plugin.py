@@ -1,0 +1,100 @@
+"""The C++ Solver plugin (kamisimulator_b200/plugin): KamiSimulator's solver calls
+(Construct(settings json), SolveNextStep(dt), DownloadHair) on a Hair-like padded strand array."""
+import json
+import os
+import subprocess
+
+import numpy as np
+import pytest
+
+from kamisimulator_b200 import synth
+from tests import helpers
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+DRIVER = os.path.join(ROOT, "kamisimulator_b200", "lib", "kami_solver_driver")
+
+# the keys and values of the reference's scripts/json/StCossRods.json
+REFERENCE_SETTINGS = {
+    "EnableResample": True, "EnableSDF": True, "EnableHairHairColl": False, "UseYoungsModule": True, "NumItr": 32,
+    "SagFreeItr": 0, "SubdivCoeff": 3, "StretchK": 3e3, "BendK": 6e-4, "YoungsModule": 5,
+    "StiffnessDeviationCoeff": 1, "CurveRadius": 4e-5, "Density": 1.3e6, "ResampleLen": 1e-3,
+    "VelocityDecay": 0.05, "ExternalForceMultiplier": 1, "WindPeak": 40, "WindYFreq": 1, "WindZFreq": 0.7,
+    "WindTimeFreq": 0.4, "WindSharpness": 3.0,
+}
+
+
+def write_hair(path, groom, pad_to=None):
+    counts = np.diff(groom.strand_begin).astype(np.uint32)
+    mv = int(pad_to or counts.max())
+    arr = np.zeros((groom.num_strands, mv, 3), np.float32)
+    for s in range(groom.num_strands):
+        a, b = groom.strand_begin[s], groom.strand_begin[s + 1]
+        arr[s, : b - a] = groom.positions[a:b]
+    with open(path, "wb") as f:
+        f.write(np.array([groom.num_strands, mv], np.uint32).tobytes())
+        f.write(counts.tobytes())
+        f.write(arr.tobytes())
+    return counts, mv
+
+
+def read_out(path, ns, mv):
+    data = np.fromfile(path, np.float32)
+    n = ns * mv * 3
+    return data[:n].reshape(ns, mv, 3), data[n:2 * n].reshape(ns, mv, 3)
+
+
+def test_descriptor_from_reference_settings(tmp_path):
+    # strands of 3 vertices are skipped, as StableCosseratRodsSolver::BuildYarnBallHair does
+    lens = np.array([10, 3, 12, 2, 8])
+    g = synth.groom_strands(np.random.default_rng(0), lens)
+    write_hair(tmp_path / "hair.bin", g)
+    (tmp_path / "s.json").write_text(json.dumps(REFERENCE_SETTINGS))
+    out = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
+                         capture_output=True, text=True, check=True).stdout
+    d = json.loads(out)
+    assert d["num_strands"] == 3 and d["num_vertices"] == 30
+    assert d["num_itr"] == 32
+    assert d["radius"] == pytest.approx(0.05 * 4e-5)  # StableCosseratRodsSolver.cpp:177-179
+    assert d["density"] == pytest.approx(1.3e6)
+    assert d["young"] == pytest.approx(5.0) and d["deviation"] == pytest.approx(1.0) and d["stiffness_mode"] == 0
+    assert d["wind_peak"] == pytest.approx(40.0) and d["velocity_decay"] == pytest.approx(0.05)
+    assert d["max_h"] == pytest.approx(4e-4)  # Sim::maxH
+    assert d["gravity"] == pytest.approx([0.0, -9.8, 0.0])
+
+
+def test_unsupported_settings_are_rejected(tmp_path):
+    g = synth.cantilever(2, 8)
+    write_hair(tmp_path / "hair.bin", g)
+    (tmp_path / "s.json").write_text(json.dumps({"EnableHairHairColl": True}))
+    r = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
+                       capture_output=True, text=True)
+    assert r.returncode == 1 and "EnableHairHairColl" in r.stderr
+
+
+@pytest.mark.gpu
+def test_plugin_steps_match_the_c_abi_and_the_oracle(tmp_path):
+    g = helpers.soft_groom(40, (6, 30), seed=12)
+    counts, mv = write_hair(tmp_path / "hair.bin", g, pad_to=40)
+    settings = {"NumItr": 6, "UseYoungsModule": True, "YoungsModule": 1e-4, "StiffnessDeviationCoeff": 0.5,
+                "CurveRadius": 40e-6 / 0.05, "Density": 1300, "VelocityDecay": 0.05, "WindPeak": 0,
+                "EnableSDF": False, "MaxTimeStep": 1 / 60, "Gravity": [0.3, -0.4, -9.81]}
+    (tmp_path / "s.json").write_text(json.dumps(settings))
+    steps = 5
+    subprocess.run([DRIVER, str(tmp_path / "s.json"), str(tmp_path / "hair.bin"), str(steps), str(1 / 60),
+                    str(tmp_path / "out.bin")], check=True, capture_output=True)
+    pos, _ = read_out(tmp_path / "out.bin", g.num_strands, mv)
+    packed = np.concatenate([pos[s, : counts[s]] for s in range(g.num_strands)])
+    st = dict(num_itr=6, max_h=1 / 60, gravity=(0.3, -0.4, -9.81), radius=40e-6, velocity_decay=0.05)
+    g.strand_young[:] = 1e-4
+    g.strand_dev[:] = 0.5
+    s = helpers.gpu_solver(g, st)
+    o = helpers.oracle_sim(g, st, np.float32)
+    for _ in range(steps):
+        s.step(1 / 60)
+        o.advance(1 / 60)
+    x, _ = s.get_positions_velocities()
+    s.close()
+    # the plugin's radius is 0.05 x CurveRadius in float, within an ulp of the 40 um given to the C ABI here
+    np.testing.assert_allclose(packed, x, atol=1e-6)
+    assert np.abs(packed - o.x).max() <= helpers.POS_TOL
+    assert np.abs(packed - g.positions).max() > 1e-3  # the strands moved
