@@ -97,4 +97,4 @@ def test_plugin_steps_match_the_c_abi_and_the_oracle(tmp_path):
     # the plugin's radius is 0.05 x CurveRadius in float, within an ulp of the 40 um given to the C ABI here
     np.testing.assert_allclose(packed, x, atol=1e-6)
     assert np.abs(packed - o.x).max() <= helpers.POS_TOL
-    assert np.abs(packed - g.positions).max() > 1e-3  # the strands moved
+    assert np.abs(packed - g.positions).max() > 1e-4  # the strands moved
