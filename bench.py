@@ -297,6 +297,80 @@ def extra_forms(args, torch, stream, flush):
     return out
 
 
+def large_timing(torch, stream, frames=24, adjoint_frames=30, tape_gb=60.0):
+    """8 instances x 100,000 strands x 100 vertices (80 M vertices), union-of-12-capsules SDF on 256^3,
+    head yawing +-30 deg at 1 Hz, 30 iterations, dt 1/120: kami_vbd_step_n over `frames` frames with
+    one body transform per frame (a sample of the 240-frame run).  Then the adjoint over the last
+    `adjoint_frames` frames of the run (frames 210-239 of the head motion): a checkpointed rollout
+    and its backward to d loss / d per-strand stiffness, the tape bounded to `tape_gb` by tile
+    windows; host-timed (the backward is a host loop over windows and checkpoints)."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.vbd import Solver
+
+    t0 = time.perf_counter()
+    rng = np.random.default_rng(11)
+    inst = [synth.groom_strands(rng, np.full(100_000, 100)) for _ in range(8)]
+    g = synth.concat_grooms(inst)
+    del inst
+    sdf = synth.capsule_union_sdf(256, num_capsules=12, radius_range=(0.02, 0.08))
+    gen_s = time.perf_counter() - t0
+    st = dict(num_itr=30, max_h=DT, gravity=(0.0, 0.0, -9.81), radius=40e-6, density=1300.0, velocity_decay=0.05,
+              damping=1e-6, sdf=sdf)
+    t0 = time.perf_counter()
+    s = Solver(g, form="fused", **st)
+    create_s = time.perf_counter() - t0
+    V = g.num_vertices
+    counts = np.diff(g.strand_begin)
+    del g
+    best, _ = s.autotune(DT, trial_steps=4)
+    bt = np.array([list(synth.head_rotation(f * DT)) + [0.0, 0.0, 0.0] for f in range(frames)], np.float32)
+    s.step_n(DT, frames, bt, stream=stream)  # warm-up, graph capture
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    s.step_n(DT, frames, bt, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1)
+    s.synchronize()
+    out = {"value": V * 30 * frames / (ms / 1e3), "ms_per_step": ms / frames, "vertices": V, "frames_timed": frames,
+           "tuning": dict(zip(("slots_per_lane", "warps_per_block", "steps_per_launch", "register_cap"), best)),
+           "generate_s": gen_s, "create_s": create_s}
+    out["adjoint"] = large_adjoint(torch, s, counts, adjoint_frames, tape_gb)
+    s.close()
+    return out
+
+
+def large_adjoint(torch, s, counts, frames, tape_gb, k=10):
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.autograd import rollout_positions
+
+    first = 240 - frames
+    body = np.array([list(synth.head_rotation((first + f) * DT)) + [0.0, 0.0, 0.0] for f in range(frames)], np.float32)
+    init = s.get_state_into(torch.empty(s.state_size() // 4, dtype=torch.float32, device="cuda"))
+    unit = s.get_rest_darboux(torch.empty((s.num_vertices, 4), dtype=torch.float32, device="cuda"))
+    strand_of = torch.repeat_interleave(torch.arange(len(counts), device="cuda"), torch.as_tensor(counts, device="cuda"))
+    tiles = s.tile_count()
+    slots_per_tile = 32 * s.get_tuning()[0]
+    per_tile = k * ((30 + 1) * 32 + 48) * slots_per_tile  # tape bytes per tile for k recorded steps
+    chunk = max(1, min(tiles, int(tape_gb * 1e9 // per_tile)))
+    c = torch.randn((s.num_vertices, 3), device="cuda")
+    scale = torch.ones(len(counts), device="cuda", requires_grad=True)
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    x = rollout_positions(scale, s, unit, strand_of, init, frames, DT, k, tiles_per_chunk=chunk, body_transforms=body)
+    torch.cuda.synchronize()
+    t1 = time.perf_counter()
+    (c * x).sum().backward()
+    torch.cuda.synchronize()
+    t2 = time.perf_counter()
+    finite = bool(torch.isfinite(scale.grad).all().item())
+    return {"frames": frames, "checkpoint_every": k, "tiles": tiles, "tiles_per_window": chunk,
+            "windows": -(-tiles // chunk), "tape_gb": chunk * per_tile / 1e9, "forward_s": t1 - t0,
+            "backward_s": t2 - t1, "gradient_finite": finite,
+            "what": "d sum(c . x_239) / d per-strand stiffness over frames 210-239, head motion replayed"}
+
+
 def adjoint_timing(torch, stream):
     """Device time per step of the forward step, the recorded forward and the adjoint (reverse) step
     on 2,000 strands x 48 vertices, plus one host-timed autograd round (60 steps, checkpoint 10)."""
@@ -308,7 +382,7 @@ def adjoint_timing(torch, stream):
     st = settings()
     solver = Solver(g, form="fused", **st)
     k = 10
-    solver.tape_reserve(k)
+    solver.tape_reserve(k, 0)
     init = solver.get_state()
 
     def timed(fn):
@@ -445,7 +519,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
-    ap.add_argument("--only", choices=["adjoint"], help="run a single extra measurement (profiling runs)")
+    ap.add_argument("--only", choices=["adjoint", "large"], help="run a single extra measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -453,6 +527,10 @@ def main():
         import torch
 
         print(json.dumps(adjoint_timing(torch, torch.cuda.current_stream())), flush=True)
+    elif args.only == "large":
+        import torch
+
+        print(json.dumps(large_timing(torch, torch.cuda.current_stream())), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -92,6 +92,8 @@ struct kami_vbd_solver {
 
     // differentiable stepping: the tape of recorded steps and the adjoint state
     int tape_capacity = 0;
+    int64_t tape_tiles = 0;               // tiles the tape holds per step
+    int64_t win_begin = 0, win_end = 0;   // tile window that recording and the adjoint cover
     std::vector<StepParams> tape_steps;
     float4 *d_tdx = nullptr, *d_tq = nullptr, *d_tx = nullptr, *d_tv = nullptr, *d_tvl = nullptr;
     float4 *d_gx = nullptr, *d_gv = nullptr, *d_gvl = nullptr, *d_gq = nullptr, *d_gqr = nullptr;
@@ -103,10 +105,16 @@ struct kami_vbd_solver {
         t.x = d_tx;
         t.v = d_tv;
         t.vl = d_tvl;
-        t.slots = layout.num_slots;
+        t.slots = tape_tiles * 32LL * layout.C;
         t.num_itr = pp.num_itr;
         t.step = step;
+        t.tile_begin = win_begin;
         return t;
+    }
+    DeviceState window_state() const {  // the device state seen through the tape window
+        DeviceState s = dstate();
+        s.num_tiles = win_end;
+        return s;
     }
 
     DeviceState dstate() const {
@@ -640,6 +648,7 @@ static kami_status relayout(kami_vbd_solver* h, int C) {
         *scratch[i] = nullptr;
     }
     h->tape_capacity = 0;
+    h->tape_tiles = 0;
     h->tape_steps.clear();
     for (int i = 0; i < 4 && e == cudaSuccess; i++)
         if (had[i]) e = dalloc(scratch[i], S);
@@ -820,12 +829,21 @@ static kami_status adjoint_supported(kami_vbd_solver* h) {
     return KAMI_OK;
 }
 
-kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps) {
+kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps, int64_t max_tiles) {
     KAMI_TRY(valid_handle(h));
     KAMI_TRY(adjoint_supported(h));
     if (max_steps <= 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "max_steps must be > 0");
+    if (max_tiles < 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "max_tiles must be >= 0");
     KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    const int64_t tiles = (max_tiles == 0 || max_tiles > h->layout.num_tiles) ? h->layout.num_tiles : max_tiles;
+    if (h->tape_capacity == max_steps && h->tape_tiles == tiles) {  // already the requested size
+        h->tape_steps.clear();
+        h->win_begin = 0;
+        h->win_end = tiles;
+        return KAMI_OK;
+    }
     const size_t S = (size_t)h->layout.num_slots, N1 = (size_t)h->pp.num_itr + 1;
+    const size_t TS = (size_t)tiles * 32 * h->layout.C;  // tape slots per step
     float4** tape_arrays[] = {&h->d_tdx, &h->d_tq, &h->d_tx, &h->d_tv, &h->d_tvl};
     for (float4** p : tape_arrays)
         if (*p) {
@@ -833,12 +851,13 @@ kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps) {
             *p = nullptr;
         }
     h->tape_capacity = 0;
+    h->tape_tiles = 0;
     h->tape_steps.clear();
-    cudaError_t e = dalloc(&h->d_tdx, (size_t)max_steps * N1 * S);
-    if (e == cudaSuccess) e = dalloc(&h->d_tq, (size_t)max_steps * N1 * S);
-    if (e == cudaSuccess) e = dalloc(&h->d_tx, (size_t)max_steps * S);
-    if (e == cudaSuccess) e = dalloc(&h->d_tv, (size_t)max_steps * S);
-    if (e == cudaSuccess) e = dalloc(&h->d_tvl, (size_t)max_steps * S);
+    cudaError_t e = dalloc(&h->d_tdx, (size_t)max_steps * N1 * TS);
+    if (e == cudaSuccess) e = dalloc(&h->d_tq, (size_t)max_steps * N1 * TS);
+    if (e == cudaSuccess) e = dalloc(&h->d_tx, (size_t)max_steps * TS);
+    if (e == cudaSuccess) e = dalloc(&h->d_tv, (size_t)max_steps * TS);
+    if (e == cudaSuccess) e = dalloc(&h->d_tvl, (size_t)max_steps * TS);
     float4** adj_arrays[] = {&h->d_gx, &h->d_gv, &h->d_gvl, &h->d_gq, &h->d_gqr};
     for (float4** p : adj_arrays)
         if (e == cudaSuccess && !*p) {
@@ -847,6 +866,28 @@ kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps) {
         }
     if (e != cudaSuccess) return cuda_fail(e, "allocating the tape");
     h->tape_capacity = max_steps;
+    h->tape_tiles = tiles;
+    h->win_begin = 0;
+    h->win_end = tiles;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_get_tile_count(kami_vbd_handle h, int64_t* num_tiles) {
+    if (!h || !num_tiles) return fail(KAMI_ERR_INVALID_ARGUMENT, "null argument");
+    *num_tiles = h->layout.num_tiles;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_set_tape_window(kami_vbd_handle h, int64_t tile_begin, int64_t tile_end) {
+    if (!h) return fail(KAMI_ERR_INVALID_ARGUMENT, "null handle");
+    if (h->tape_capacity == 0) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
+    if (!h->tape_steps.empty()) return fail(KAMI_ERR_STATE, "the tape holds recorded steps; run kami_vbd_backward first");
+    if (tile_begin < 0 || tile_end <= tile_begin || tile_end > h->layout.num_tiles)
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "bad tile window [%lld, %lld)", (long long)tile_begin, (long long)tile_end);
+    if (tile_end - tile_begin > h->tape_tiles)
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "the tape holds %lld tiles per step", (long long)h->tape_tiles);
+    h->win_begin = tile_begin;
+    h->win_end = tile_end;
     return KAMI_OK;
 }
 
@@ -861,7 +902,8 @@ kami_status kami_vbd_step_record(kami_vbd_handle h, float dt, void* stream) {
     const StepParams sp = advance_clock(h, dt);
     const int step = (int)h->tape_steps.size();
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
-        KAMI_CUDA(launch_fused_record(h->dstate(), h->pp, sp, h->sdf, h->tape(step), h->layout.C, h->warps_per_block, s),
+        KAMI_CUDA(launch_fused_record(h->window_state(), h->pp, sp, h->sdf, h->tape(step), h->layout.C,
+                                      h->warps_per_block, s),
                   "recorded step launch");
         return KAMI_OK;
     });
@@ -896,7 +938,8 @@ kami_status kami_vbd_backward(kami_vbd_handle h, float* adj_x, float* adj_v, flo
     KAMI_CUDA(launch_scatter4((const float4*)h->d_stage, h->d_gq, h->d_slot_of, h->nv, h->stream), "scatter adjoint");
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
         for (int step = (int)h->tape_steps.size() - 1; step >= 0; step--)
-            KAMI_CUDA(launch_adjoint_step(h->dstate(), h->pp, h->tape_steps[step], h->sdf, h->tape(step), ad, h->layout.C, s),
+            KAMI_CUDA(launch_adjoint_step(h->window_state(), h->pp, h->tape_steps[step], h->sdf, h->tape(step), ad,
+                                          h->layout.C, s),
                       "adjoint step launch");
         return KAMI_OK;
     });

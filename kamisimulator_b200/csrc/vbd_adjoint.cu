@@ -182,13 +182,14 @@ template <int C, int MINB>
 __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                            TapeView tp, AdjointState ad) {
     const int lane = threadIdx.x & 31;
-    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t tile = tp.tile_begin + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (tile >= st.num_tiles) return;  // uniform per warp
     const int64_t base = tile * (32LL * C) + lane;
     const int64_t S = tp.slots;
     const int N = tp.num_itr;
-    const int64_t row0 = ((int64_t)tp.step * (N + 1)) * S + base;
-    const int64_t srow = (int64_t)tp.step * S + base;
+    const int64_t tslot = base - tp.tile_begin * 32LL * C;  // this lane's slot in the tape window
+    const int64_t row0 = ((int64_t)tp.step * (N + 1)) * S + tslot;
+    const int64_t srow = (int64_t)tp.step * S + tslot;
 
     float3 x[C], v[C], vl[C], e[C], gdx[C], ge[C], gy[C], gx[C], gv[C], gvl[C], gd3[C];
     float4 qr[C], gq[C], gqr[C];
@@ -449,7 +450,8 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
 cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                                 const TapeView& tp, int C, int warps_per_block, cudaStream_t s) {
     const int threads = 32 * warps_per_block;
-    const unsigned blocks = (unsigned)((st.num_tiles + warps_per_block - 1) / warps_per_block);
+    const int64_t tiles = st.num_tiles - tp.tile_begin;
+    const unsigned blocks = (unsigned)((tiles + warps_per_block - 1) / warps_per_block);
     if (blocks == 0) return cudaSuccess;
     if (C == 2)
         fused_step_kernel<2, false, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, tp, nullptr, 1);
@@ -463,7 +465,8 @@ cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, con
 cudaError_t launch_adjoint_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                                 const TapeView& tp, const AdjointState& ad, int C, cudaStream_t s) {
     const int wpb = 4;
-    const unsigned blocks = (unsigned)((st.num_tiles + wpb - 1) / wpb);
+    const int64_t tiles = st.num_tiles - tp.tile_begin;
+    const unsigned blocks = (unsigned)((tiles + wpb - 1) / wpb);
     if (blocks == 0) return cudaSuccess;
     if (C == 2)
         adjoint_step_kernel<2, 4><<<blocks, 32 * wpb, 0, s>>>(st, pp, sp, sdf, tp, ad);

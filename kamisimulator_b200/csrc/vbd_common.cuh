@@ -72,6 +72,8 @@ struct DeviceState {
 // Iterates of recorded steps for the adjoint: for step s, iteration it (0 = after the predict) and
 // slot g, dx at dx[(s*(N+1) + it)*S + g] and q at q[(s*(N+1) + it)*S + g]; the state at the start
 // of step s at x/v/vl[s*S + g].  N = iterations per step, S = slots.
+// A tape may cover a window of tiles [tile_begin, DeviceState::num_tiles): slot g of tile t is then
+// tape slot g - tile_begin * 32C, and `slots` is the window's slot count.
 struct TapeView {
     float4* dx;
     float4* q;
@@ -81,6 +83,7 @@ struct TapeView {
     int64_t slots;
     int num_itr;
     int step;
+    int64_t tile_begin;
 };
 
 // Adjoint state of the solver, tile slots: d loss / d (x, v, vlast, q), and the accumulated

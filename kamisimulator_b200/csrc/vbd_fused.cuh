@@ -75,7 +75,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
     static_assert(!(RECORD && JACOBI), "the tape records the colour2 schedule");
     static_assert(C % 2 == 0, "slots per lane must be even");
     const int lane = threadIdx.x & 31;
-    const int64_t tile = (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t tile = (RECORD ? tp.tile_begin : 0) + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (tile >= st.num_tiles) return;  // uniform per warp
     const int64_t base = tile * (32LL * C) + lane;
 
@@ -104,11 +104,12 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
         kkN[k] = (fl[k] & F_HAS_NEXT) ? kk[k] : 0.f;
     }
     const int64_t tS = tp.slots;
-    const int64_t tbase = ((int64_t)tp.step * (tp.num_itr + 1)) * tS + base;  // tape row of iteration 0
+    const int64_t tslot = base - (RECORD ? tp.tile_begin * 32LL * C : 0);  // this lane's slot in the tape window
+    const int64_t tbase = ((int64_t)tp.step * (tp.num_itr + 1)) * tS + tslot;  // tape row of iteration 0
     if (RECORD) {
 #pragma unroll
         for (int k = 0; k < C; k++) {
-            const int64_t g = base + 32LL * k, o = (int64_t)tp.step * tS + g;
+            const int64_t o = (int64_t)tp.step * tS + tslot + 32LL * k;
             tp.x[o] = make_float4(x[k].x, x[k].y, x[k].z, im[k]);
             tp.v[o] = make_float4(v[k].x, v[k].y, v[k].z, 0.f);
             tp.vl[o] = make_float4(vl[k].x, vl[k].y, vl[k].z, 0.f);

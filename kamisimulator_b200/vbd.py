@@ -33,7 +33,7 @@ EXPORTED = [
     "kami_vbd_set_body_transform", "kami_vbd_step", "kami_vbd_synchronize", "kami_vbd_state_size",
     "kami_vbd_get_state", "kami_vbd_set_state", "kami_vbd_last_error_string", "kami_vbd_version",
     "kami_vbd_step_n", "kami_vbd_set_tuning", "kami_vbd_get_tuning", "kami_vbd_autotune",
-    "kami_vbd_tape_reserve", "kami_vbd_step_record", "kami_vbd_backward", "kami_vbd_get_rest_darboux_grad",
+    "kami_vbd_tape_reserve", "kami_vbd_get_tile_count", "kami_vbd_set_tape_window", "kami_vbd_step_record", "kami_vbd_backward", "kami_vbd_get_rest_darboux_grad",
     "kami_vbd_zero_rest_darboux_grad",
 ]
 
@@ -119,7 +119,9 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_set_tuning": [vp, i32, i32, i32, i32],
         "kami_vbd_get_tuning": [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)],
         "kami_vbd_autotune": [vp, f32, i32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)],
-        "kami_vbd_tape_reserve": [vp, i32],
+        "kami_vbd_tape_reserve": [vp, i32, i64],
+        "kami_vbd_get_tile_count": [vp, ctypes.POINTER(i64)],
+        "kami_vbd_set_tape_window": [vp, i64, i64],
         "kami_vbd_step_record": [vp, f32, vp],
         "kami_vbd_backward": [vp, vp, vp, vp, vp, i32, vp],
         "kami_vbd_get_rest_darboux_grad": [vp, vp, i32],
@@ -352,8 +354,16 @@ class Solver:
         _check(self.lib.kami_vbd_set_state(self._h, p, nbytes, m))
 
     # -- differentiable stepping
-    def tape_reserve(self, max_steps):
-        _check(self.lib.kami_vbd_tape_reserve(self._h, max_steps))
+    def tape_reserve(self, max_steps, max_tiles=0):
+        _check(self.lib.kami_vbd_tape_reserve(self._h, max_steps, max_tiles))
+
+    def tile_count(self):
+        n = ctypes.c_int64()
+        _check(self.lib.kami_vbd_get_tile_count(self._h, ctypes.byref(n)))
+        return n.value
+
+    def set_tape_window(self, tile_begin, tile_end):
+        _check(self.lib.kami_vbd_set_tape_window(self._h, tile_begin, tile_end))
 
     def step_record(self, dt, stream=None):
         s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)

@@ -26,8 +26,8 @@ def _setup(num_strands=24, lengths=(6, 20), seed=5, young_scale=1e-3, sdf=True, 
     return g, st, solver, unit, strand_of, init, v0
 
 
-def _torch_reference(g, st, v0, scale, frames, c, dt=1 / 60):
-    """FP64 autograd rollout: returns (loss, d loss/d scale, d loss/d (x0, v0, q0))."""
+def _torch_reference(g, st, v0, scale, frames, c, dt=1 / 60, body=None):
+    """FP64 autograd rollout: returns (loss, d loss/d scale, d loss/d (x0, v0, q0)); body: (frames, 7)."""
     import torch
 
     from oracle import oracle as orc
@@ -42,7 +42,10 @@ def _torch_reference(g, st, v0, scale, frames, c, dt=1 / 60):
     q0 = torch.tensor(m["q"], requires_grad=True)
     qr = torch.tensor(m["q_rest"]) * sc[strand_of][:, None]
     state = (x0, vv, torch.zeros_like(x0), q0, float(np.float32(st["max_h"])))
-    for _ in range(frames):
+    for f in range(frames):
+        if body is not None:
+            tv.rot = torch.tensor(np.float32(body[f][:4]).astype(np.float64))
+            tv.tr = torch.tensor(np.float32(body[f][4:7]).astype(np.float64))
         state = tv.step(state, qr, dt)
     loss = (torch.tensor(c) * state[0]).sum()
     loss.backward()
@@ -76,6 +79,32 @@ def test_stiffness_gradient_matches_fp64_autograd(sdf):
     solver.close()
 
 
+def test_gradient_with_a_moving_body_matches_fp64_autograd():
+    """The head sphere yaws and slides into the strands frame by frame (kami_vbd_set_body_transform
+    before every recorded step); the sliding head decides which vertices are projected."""
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+
+    g, st, solver, unit, strand_of, init, v0 = _setup(num_strands=24, lengths=(6, 20), seed=13, sdf=True)
+    frames = 6
+    body = np.array([list(synth.head_rotation(f / 60, 30.0, 2.0)) + [0.004 * f, -0.002 * f, 0.003 * f]
+                     for f in range(frames)], np.float32)
+    rng = np.random.default_rng(4)
+    scale0 = rng.uniform(0.7, 1.4, g.num_strands).astype(np.float32)
+    c = rng.normal(size=(g.num_vertices, 3))
+    scale = torch.tensor(scale0, device="cuda", requires_grad=True)
+    x = rollout_positions(scale, solver, unit, strand_of, init, frames, 1 / 60, checkpoint_every=4,
+                          tiles_per_chunk=2, body_transforms=body)
+    (torch.tensor(c, dtype=torch.float32, device="cuda") * x).sum().backward()
+    l_ref, g_ref, *_ = _torch_reference(g, st, v0, scale0, frames, c, body=body)
+    _, g_still, *_ = _torch_reference(g, st, v0, scale0, frames, c)
+    assert _rel(g_still, g_ref) > 1e-2  # the motion changes the gradient
+    g_gpu = scale.grad.cpu().numpy()
+    assert _rel(g_gpu, g_ref) <= GRAD_TOL, (_rel(g_gpu, g_ref), g_gpu[:5], g_ref[:5])
+    solver.close()
+
+
 def test_state_adjoint_matches_fp64_autograd():
     """kami_vbd_backward's adjoint of the initial positions, velocities and orientations."""
     import torch
@@ -83,7 +112,7 @@ def test_state_adjoint_matches_fp64_autograd():
     g, st, solver, unit, strand_of, init, v0 = _setup(num_strands=16, lengths=(6, 16), sdf=True)
     c = np.random.default_rng(1).normal(size=(g.num_vertices, 3))
     frames = 4
-    solver.tape_reserve(frames)
+    solver.tape_reserve(frames, 0)
     for _ in range(frames):
         solver.step_record(1 / 60)
     ax = torch.tensor(c, dtype=torch.float32, device="cuda")
@@ -132,6 +161,42 @@ def test_directional_derivative_matches_central_fd():
         fd = (loss(scale0 + hstep * u) - loss(scale0 - hstep * u)) / (2 * hstep)
         ad = float(grad @ u)
         assert abs(ad - fd) <= GRAD_TOL * max(abs(fd), 1e-3 * np.linalg.norm(grad)), (trial, ad, fd)
+    solver.close()
+
+
+def test_tile_windows_do_not_change_the_gradient():
+    """Differentiating window by window (a tape of 3 tiles) gives the whole-groom gradient."""
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+
+    g, st, solver, unit, strand_of, init, _ = _setup(num_strands=40, lengths=(6, 30), sdf=True)
+    assert solver.tile_count() > 6
+    from kamisimulator_b200.vbd import KamiError
+
+    solver.tape_reserve(2, 3)
+    with pytest.raises(KamiError):
+        solver.set_tape_window(0, 4)  # wider than the tape
+    with pytest.raises(KamiError):
+        solver.set_tape_window(5, 5)
+    with pytest.raises(KamiError):
+        solver.set_tape_window(solver.tile_count() - 1, solver.tile_count() + 1)
+    solver.set_tape_window(solver.tile_count() - 3, solver.tile_count())
+    solver.step_record(1 / 60)
+    with pytest.raises(KamiError):
+        solver.set_tape_window(0, 3)  # steps recorded on another window
+    c = torch.tensor(np.random.default_rng(8).normal(size=(g.num_vertices, 3)), dtype=torch.float32, device="cuda")
+    grads, per_vertex = [], []
+    for chunk in (0, 3):
+        scale = torch.ones(g.num_strands, device="cuda", requires_grad=True)
+        x = rollout_positions(scale, solver, unit, strand_of, init, 5, 1 / 60, checkpoint_every=2,
+                              tiles_per_chunk=chunk)
+        (c * x).sum().backward()
+        grads.append(scale.grad.cpu().numpy())
+        per_vertex.append(solver.get_rest_darboux_grad())
+    # the kernels' output is identical; the per-strand sum (torch index_add_, atomics) is not ordered
+    np.testing.assert_array_equal(per_vertex[0], per_vertex[1])
+    np.testing.assert_allclose(grads[0], grads[1], rtol=1e-6, atol=0)
     solver.close()
 
 
