@@ -254,17 +254,16 @@ def extra_forms(args, torch, stream, flush):
     s.close()
 
     grooms = synth.batched_grooms(64)
-    allg = synth.concat_grooms(grooms)
-    V = allg.num_vertices
-    b = Solver(allg, form="fused", **st)
+    V = sum(gg.num_vertices for gg in grooms)
+    b = Solver(grooms, form="fused", **st)  # kami_vbd_batch_create
     best, tuned_rate = b.autotune(DT, trial_steps=8)
     nb = 24
-    b.step_n(DT, nb, stream=stream)  # warm-up: captures the graph for n = nb
+    b.batch_step(DT, nb, stream=stream)  # warm-up: captures the graph for n = nb
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     flush.fill_(1)
     e0.record(stream)
-    b.step_n(DT, nb, stream=stream)
+    b.batch_step(DT, nb, stream=stream)
     e1.record(stream)
     torch.cuda.synchronize()
     ms_b = e0.elapsed_time(e1)
@@ -290,8 +289,9 @@ def extra_forms(args, torch, stream, flush):
                                            "steps_per_launch": best[2], "register_cap": best[3]},
                                 "plain_per_groom_value": vp, "plain_ms_per_step": ms_p / npl,
                                 "batched_over_plain": vb / vp,
-                                "what": "64 grooms (strands log-uniform [500, 20000], 16-128 vertices) in one handle, "
-                                        f"{nb} steps per kami_vbd_step_n (autotuned tile shape, CUDA graph) vs 64 "
+                                "what": "64 grooms (strands log-uniform [500, 20000], 16-128 vertices) in one "
+                                        f"kami_vbd_batch_create handle, {nb} steps per kami_vbd_batch_step "
+                                        "(autotuned tile shape, CUDA graph) vs 64 "
                                         "sweep-form handles stepped one after another"}
     out["adjoint_2k_x48"] = adjoint_timing(torch, stream)
     return out
@@ -299,7 +299,7 @@ def extra_forms(args, torch, stream, flush):
 
 def large_timing(torch, stream, frames=24, adjoint_frames=30, tape_gb=60.0):
     """8 instances x 100,000 strands x 100 vertices (80 M vertices), union-of-12-capsules SDF on 256^3,
-    head yawing +-30 deg at 1 Hz, 30 iterations, dt 1/120: kami_vbd_step_n over `frames` frames with
+    head yawing +-30 deg at 1 Hz, 30 iterations, dt 1/120: kami_vbd_batch_step over `frames` frames with
     one body transform per frame (a sample of the 240-frame run).  Then the adjoint over the last
     `adjoint_frames` frames of the run (frames 210-239 of the head motion): a checkpointed rollout
     and its backward to d loss / d per-strand stiffness, the tape bounded to `tape_gb` by tile
@@ -310,25 +310,23 @@ def large_timing(torch, stream, frames=24, adjoint_frames=30, tape_gb=60.0):
     t0 = time.perf_counter()
     rng = np.random.default_rng(11)
     inst = [synth.groom_strands(rng, np.full(100_000, 100)) for _ in range(8)]
-    g = synth.concat_grooms(inst)
-    del inst
     sdf = synth.capsule_union_sdf(256, num_capsules=12, radius_range=(0.02, 0.08))
     gen_s = time.perf_counter() - t0
     st = dict(num_itr=30, max_h=DT, gravity=(0.0, 0.0, -9.81), radius=40e-6, density=1300.0, velocity_decay=0.05,
               damping=1e-6, sdf=sdf)
     t0 = time.perf_counter()
-    s = Solver(g, form="fused", **st)
+    s = Solver(inst, form="fused", **st)  # kami_vbd_batch_create over the 8 instances
     create_s = time.perf_counter() - t0
-    V = g.num_vertices
-    counts = np.diff(g.strand_begin)
-    del g
+    V = s.num_vertices
+    counts = np.concatenate([np.diff(g.strand_begin) for g in inst])
+    del inst
     best, _ = s.autotune(DT, trial_steps=4)
     bt = np.array([list(synth.head_rotation(f * DT)) + [0.0, 0.0, 0.0] for f in range(frames)], np.float32)
-    s.step_n(DT, frames, bt, stream=stream)  # warm-up, graph capture
+    s.batch_step(DT, frames, bt, stream=stream)  # warm-up, graph capture
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
-    s.step_n(DT, frames, bt, stream=stream)
+    s.batch_step(DT, frames, bt, stream=stream)
     e1.record(stream)
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)

@@ -127,6 +127,29 @@ kami_status kami_vbd_desc_init(kami_vbd_desc* d);
  * pinning (StableCosseratRodsSolver.cpp:203-209) + SDFBodyCollisionSolver::Construct (:11-21). */
 kami_status kami_vbd_create(const kami_vbd_desc* desc, kami_vbd_handle* out);
 
+/* Batched form: one handle over num_grooms independent grooms (descs[0..num_grooms-1]).  Their
+ * strands are packed together into warp tiles, so one launch steps every groom.  Each groom's
+ * material (masses, rest lengths, orientations, stiffness, root pinning and the set's last-vertex
+ * flags) is set up exactly as kami_vbd_create would set it up for that groom alone.  The grooms
+ * must agree on the solver-wide settings (gravity, damping, decay, acceleration ratio, external
+ * force multiplier, wind, num_itr, max_h, schedule, form, device, tile shape, SDF); they may
+ * differ in geometry, radius, density and stiffness.  At the boundary the grooms' vertices follow
+ * one another in groom order (kami_vbd_batch_groom_range).  Replaces: one YarnBall::Sim per groom
+ * stepped in sequence (the CantileverTestSolver pattern). */
+kami_status kami_vbd_batch_create(int32_t num_grooms, const kami_vbd_desc* descs, kami_vbd_handle* out);
+
+/* Number of grooms of a handle (1 for kami_vbd_create). */
+kami_status kami_vbd_batch_count(kami_vbd_handle h, int32_t* num_grooms);
+
+/* Where groom `groom` sits in the handle's boundary order: its first strand and strand count, its
+ * first vertex and vertex count (any output may be NULL). */
+kami_status kami_vbd_batch_groom_range(kami_vbd_handle h, int32_t groom, int32_t* strand_begin, int32_t* num_strands,
+                                       int64_t* vertex_begin, int64_t* num_vertices);
+
+/* Steps every groom of the handle n times: kami_vbd_step_n (persistent multi-step launches
+ * replayed from a CUDA graph). */
+kami_status kami_vbd_batch_step(kami_vbd_handle h, float dt, int32_t n, const float* body_transforms, void* stream);
+
 /* Releases every device and host resource of the handle.  Replaces: Sim::~Sim (YBSimulator.cu:129-157). */
 kami_status kami_vbd_destroy(kami_vbd_handle h);
 

@@ -55,6 +55,7 @@ struct kami_vbd_solver {
     int64_t nv = 0;
     int32_t ns = 0;
     std::vector<int32_t> strand_begin;
+    std::vector<int32_t> groom_strand_begin;  // strand offsets of the grooms of a batch handle
     TileLayout layout;
     int64_t* d_slot_of = nullptr;
 
@@ -297,9 +298,7 @@ kami_status kami_vbd_desc_init(kami_vbd_desc* d) {
     return KAMI_OK;
 }
 
-kami_status kami_vbd_create(const kami_vbd_desc* d, kami_vbd_handle* out) {
-    if (!d || !out) return fail(KAMI_ERR_INVALID_ARGUMENT, "null descriptor or output handle");
-    *out = nullptr;
+static kami_status validate_desc(const kami_vbd_desc* d) {
     if (d->num_strands <= 0 || !d->strand_begin || !d->positions)
         return fail(KAMI_ERR_INVALID_ARGUMENT, "need num_strands > 0, strand_begin and positions");
     if (d->strand_begin[0] != 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "strand_begin[0] must be 0");
@@ -321,6 +320,49 @@ kami_status kami_vbd_create(const kami_vbd_desc* d, kami_vbd_handle* out) {
         for (int a = 0; a < 3; a++)
             if (!(s->grid_max[a] > s->grid_min[a])) return fail(KAMI_ERR_INVALID_ARGUMENT, "SDF grid_max must exceed grid_min");
     }
+    return KAMI_OK;
+}
+
+// The settings one handle applies to all its strands: grooms of a batch must agree on them.
+static const char* differing_setting(const kami_vbd_desc* a, const kami_vbd_desc* b) {
+    for (int i = 0; i < 3; i++)
+        if (a->gravity[i] != b->gravity[i]) return "gravity";
+    if (a->damping != b->damping) return "damping";
+    if (a->velocity_decay != b->velocity_decay) return "velocity_decay";
+    if (a->acceleration_ratio != b->acceleration_ratio) return "acceleration_ratio";
+    if (a->external_force_multiplier != b->external_force_multiplier) return "external_force_multiplier";
+    if (a->wind_peak != b->wind_peak || a->wind_y_freq != b->wind_y_freq || a->wind_z_freq != b->wind_z_freq ||
+        a->wind_time_freq != b->wind_time_freq || a->wind_sharpness != b->wind_sharpness)
+        return "wind";
+    if (a->num_itr != b->num_itr) return "num_itr";
+    if (a->max_h != b->max_h) return "max_h";
+    if (a->schedule != b->schedule) return "schedule";
+    if (a->form != b->form) return "form";
+    if (a->device != b->device) return "device";
+    if (a->slots_per_lane != b->slots_per_lane || a->warps_per_block != b->warps_per_block) return "tile shape";
+    if ((a->sdf == nullptr) != (b->sdf == nullptr)) return "sdf";
+    if (a->sdf && a->sdf != b->sdf) {
+        const kami_vbd_sdf_desc *x = a->sdf, *y = b->sdf;
+        for (int i = 0; i < 3; i++)
+            if (x->dims[i] != y->dims[i] || x->grid_min[i] != y->grid_min[i] || x->grid_max[i] != y->grid_max[i])
+                return "sdf";
+        if (x->threshold != y->threshold || x->phi != y->phi || x->grad != y->grad) return "sdf";
+    }
+    return nullptr;
+}
+
+// Builds one handle over the strands of n descriptors (n = 1: kami_vbd_create).  Each groom's
+// material is set up on its own, as one YarnBall::Sim per groom would do it; the solver-wide
+// settings come from the first descriptor.
+static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_handle* out) {
+    if (!descs || !out || n <= 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "null descriptor or output handle");
+    *out = nullptr;
+    for (int32_t g = 0; g < n; g++) {
+        KAMI_TRY(validate_desc(&descs[g]));
+        if (const char* what = differing_setting(&descs[0], &descs[g]))
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "groom %d differs from groom 0 in %s", g, what);
+    }
+    const kami_vbd_desc* d = &descs[0];
 
     kami_vbd_solver* h = new (std::nothrow) kami_vbd_solver();
     if (!h) return fail(KAMI_ERR_OUT_OF_MEMORY, "host allocation failed");
@@ -328,26 +370,61 @@ kami_status kami_vbd_create(const kami_vbd_desc* d, kami_vbd_handle* out) {
         release(h);
         return st;
     };
-    h->ns = d->num_strands;
-    h->strand_begin.assign(d->strand_begin, d->strand_begin + d->num_strands + 1);
-    h->nv = h->strand_begin.back();
+    int64_t total_strands = 0, total_vertices = 0;
+    for (int32_t g = 0; g < n; g++) {
+        total_strands += descs[g].num_strands;
+        total_vertices += descs[g].strand_begin[descs[g].num_strands];
+    }
+    if (total_strands > INT32_MAX || total_vertices > INT32_MAX)
+        return bail(fail(KAMI_ERR_UNSUPPORTED, "a handle holds at most 2^31 - 1 strands and vertices"));
+    h->ns = (int32_t)total_strands;
+    h->strand_begin.assign(1, 0);
+    h->strand_begin.reserve(total_strands + 1);
+    h->groom_strand_begin.assign(1, 0);
 
-    // per-vertex material in boundary order
-    MaterialDesc md;
-    md.radius = d->radius;
-    md.density = d->density;
-    md.stiffness_mode = d->stiffness_mode;
-    md.strand_young = d->strand_young;
-    md.strand_dev = d->strand_deviation;
-    md.young = d->young;
-    md.deviation = d->deviation;
-    md.k_stretch = d->k_stretch;
-    md.k_bend = d->k_bend;
-    md.pin_roots = d->pin_roots != 0;
+    // per-vertex positions, velocities and material in boundary order, groom after groom
+    std::vector<float> positions, velocities;
+    positions.reserve(3 * total_vertices);
+    velocities.reserve(3 * total_vertices);
     Material m;
+    for (int32_t g = 0; g < n; g++) {
+        const kami_vbd_desc* e = &descs[g];
+        const int32_t base = h->strand_begin.back();
+        for (int32_t s = 1; s <= e->num_strands; s++) h->strand_begin.push_back(base + e->strand_begin[s]);
+        h->groom_strand_begin.push_back(h->groom_strand_begin.back() + e->num_strands);
+        const int32_t nvg = e->strand_begin[e->num_strands];
+        positions.insert(positions.end(), e->positions, e->positions + 3 * (size_t)nvg);
+        if (e->velocities)
+            velocities.insert(velocities.end(), e->velocities, e->velocities + 3 * (size_t)nvg);
+        else
+            velocities.insert(velocities.end(), 3 * (size_t)nvg, 0.f);
+        MaterialDesc md;
+        md.radius = e->radius;
+        md.density = e->density;
+        md.stiffness_mode = e->stiffness_mode;
+        md.strand_young = e->strand_young;
+        md.strand_dev = e->strand_deviation;
+        md.young = e->young;
+        md.deviation = e->deviation;
+        md.k_stretch = e->k_stretch;
+        md.k_bend = e->k_bend;
+        md.pin_roots = e->pin_roots != 0;
+        Material mg;
+        std::string err;
+        int rc = build_material(e->strand_begin, e->num_strands, e->positions, md, mg, err);
+        if (rc != 0) {
+            if (n > 1) err = "groom " + std::to_string(g) + ": " + err;
+            return bail(fail(rc == 1 ? KAMI_ERR_INVALID_ARGUMENT : KAMI_ERR_GEOMETRY, "%s", err.c_str()));
+        }
+        m.inv_mass.insert(m.inv_mass.end(), mg.inv_mass.begin(), mg.inv_mass.end());
+        m.l_rest.insert(m.l_rest.end(), mg.l_rest.begin(), mg.l_rest.end());
+        m.k_stretch.insert(m.k_stretch.end(), mg.k_stretch.begin(), mg.k_stretch.end());
+        m.flags.insert(m.flags.end(), mg.flags.begin(), mg.flags.end());
+        m.q.insert(m.q.end(), mg.q.begin(), mg.q.end());
+        m.q_rest.insert(m.q_rest.end(), mg.q_rest.begin(), mg.q_rest.end());
+    }
+    h->nv = h->strand_begin.back();
     std::string err;
-    int rc = build_material(h->strand_begin.data(), h->ns, d->positions, md, m, err);
-    if (rc != 0) return bail(fail(rc == 1 ? KAMI_ERR_INVALID_ARGUMENT : KAMI_ERR_GEOMETRY, "%s", err.c_str()));
 
     // tile layout and form
     int C = slots_per_lane_for(h->strand_begin.data(), h->ns);
@@ -385,8 +462,8 @@ kami_status kami_vbd_create(const kami_vbd_desc* d, kami_vbd_handle* out) {
         qr(S, make_float4(0.f, 0.f, 0.f, 1.f)), prm(S, make_float4(1.f, 0.f, 0.f, 0.f));
     for (int64_t i = 0; i < h->nv; i++) {
         const int64_t g = h->layout.slot_of[i];
-        xm[g] = make_float4(d->positions[3 * i], d->positions[3 * i + 1], d->positions[3 * i + 2], m.inv_mass[i]);
-        if (d->velocities) vel[g] = make_float4(d->velocities[3 * i], d->velocities[3 * i + 1], d->velocities[3 * i + 2], 0.f);
+        xm[g] = make_float4(positions[3 * i], positions[3 * i + 1], positions[3 * i + 2], m.inv_mass[i]);
+        vel[g] = make_float4(velocities[3 * i], velocities[3 * i + 1], velocities[3 * i + 2], 0.f);
         q[g] = make_float4(m.q[4 * i], m.q[4 * i + 1], m.q[4 * i + 2], m.q[4 * i + 3]);
         qr[g] = make_float4(m.q_rest[4 * i], m.q_rest[4 * i + 1], m.q_rest[4 * i + 2], m.q_rest[4 * i + 3]);
         uint32_t fl = m.flags[i];
@@ -472,6 +549,36 @@ kami_status kami_vbd_create(const kami_vbd_desc* d, kami_vbd_handle* out) {
     }
     *out = h;
     return KAMI_OK;
+}
+
+kami_status kami_vbd_create(const kami_vbd_desc* desc, kami_vbd_handle* out) { return create_impl(desc, 1, out); }
+
+kami_status kami_vbd_batch_create(int32_t num_grooms, const kami_vbd_desc* descs, kami_vbd_handle* out) {
+    if (num_grooms <= 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "num_grooms must be > 0");
+    return create_impl(descs, num_grooms, out);
+}
+
+kami_status kami_vbd_batch_count(kami_vbd_handle h, int32_t* num_grooms) {
+    if (!h || !num_grooms) return fail(KAMI_ERR_INVALID_ARGUMENT, "null argument");
+    *num_grooms = (int32_t)h->groom_strand_begin.size() - 1;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_batch_groom_range(kami_vbd_handle h, int32_t groom, int32_t* strand_begin, int32_t* num_strands,
+                                       int64_t* vertex_begin, int64_t* num_vertices) {
+    if (!h) return fail(KAMI_ERR_INVALID_ARGUMENT, "null handle");
+    const int32_t n = (int32_t)h->groom_strand_begin.size() - 1;
+    if (groom < 0 || groom >= n) return fail(KAMI_ERR_INVALID_ARGUMENT, "groom %d out of range [0, %d)", groom, n);
+    const int32_t s0 = h->groom_strand_begin[groom], s1 = h->groom_strand_begin[groom + 1];
+    if (strand_begin) *strand_begin = s0;
+    if (num_strands) *num_strands = s1 - s0;
+    if (vertex_begin) *vertex_begin = h->strand_begin[s0];
+    if (num_vertices) *num_vertices = (int64_t)h->strand_begin[s1] - h->strand_begin[s0];
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_batch_step(kami_vbd_handle h, float dt, int32_t n, const float* body_transforms, void* stream) {
+    return kami_vbd_step_n(h, dt, n, body_transforms, stream);
 }
 
 kami_status kami_vbd_destroy(kami_vbd_handle h) {

@@ -34,7 +34,8 @@ EXPORTED = [
     "kami_vbd_get_state", "kami_vbd_set_state", "kami_vbd_last_error_string", "kami_vbd_version",
     "kami_vbd_step_n", "kami_vbd_set_tuning", "kami_vbd_get_tuning", "kami_vbd_autotune",
     "kami_vbd_tape_reserve", "kami_vbd_get_tile_count", "kami_vbd_set_tape_window", "kami_vbd_step_record", "kami_vbd_backward", "kami_vbd_get_rest_darboux_grad",
-    "kami_vbd_zero_rest_darboux_grad",
+    "kami_vbd_zero_rest_darboux_grad", "kami_vbd_batch_create", "kami_vbd_batch_count", "kami_vbd_batch_groom_range",
+    "kami_vbd_batch_step",
 ]
 
 
@@ -101,6 +102,11 @@ def load_library(path: str = LIB_PATH):
     sig = {
         "kami_vbd_desc_init": [ctypes.POINTER(Desc)],
         "kami_vbd_create": [ctypes.POINTER(Desc), ctypes.POINTER(vp)],
+        "kami_vbd_batch_create": [i32, ctypes.POINTER(Desc), ctypes.POINTER(vp)],
+        "kami_vbd_batch_count": [vp, ctypes.POINTER(i32)],
+        "kami_vbd_batch_groom_range": [vp, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i64),
+                                       ctypes.POINTER(i64)],
+        "kami_vbd_batch_step": [vp, f32, i32, vp, vp],
         "kami_vbd_destroy": [vp],
         "kami_vbd_get_sizes": [vp, ctypes.POINTER(i64), ctypes.POINTER(i32), ctypes.POINTER(i32)],
         "kami_vbd_set_positions_velocities": [vp, vp, vp, i32],
@@ -171,38 +177,15 @@ class Solver:
                  wind=(0.0, 1.0, 0.7, 0.4, 3.0), schedule="colour2", form="auto", sdf=None, stiffness_mode=0,
                  young=5.0, deviation=1.0, per_strand=True, k_stretch=3e3, k_bend=6e-4, pin_roots=True,
                  velocities=None, device=-1, slots_per_lane=0, warps_per_block=0):
+        """groom: one groom (kami_vbd_create) or a list of grooms (kami_vbd_batch_create, one handle
+        stepping all of them; velocities is then None or a list with one entry per groom)."""
         self.lib = load_library()
         self._h = None
-        sb = np.ascontiguousarray(groom.strand_begin, np.int32)
-        pos = _f32(groom.positions)
-        vel = None if velocities is None else _f32(velocities)
-        sy = np.ascontiguousarray(groom.strand_young, np.float32) if per_strand else None
-        sd = np.ascontiguousarray(groom.strand_dev, np.float32) if per_strand else None
-        d = Desc()
-        _check(self.lib.kami_vbd_desc_init(ctypes.byref(d)))
-        d.num_strands = groom.num_strands
-        d.strand_begin = sb.ctypes.data
-        d.positions = pos.ctypes.data
-        d.velocities = vel.ctypes.data if vel is not None else None
-        d.radius, d.density = radius, density
-        d.stiffness_mode = stiffness_mode
-        d.young, d.deviation = young, deviation
-        d.strand_young = sy.ctypes.data if sy is not None else None
-        d.strand_deviation = sd.ctypes.data if sd is not None else None
-        d.k_stretch, d.k_bend = k_stretch, k_bend
-        d.gravity[:] = gravity
-        d.damping, d.velocity_decay, d.acceleration_ratio = damping, velocity_decay, acceleration_ratio
-        d.external_force_multiplier = ext_mult
-        d.wind_peak, d.wind_y_freq, d.wind_z_freq, d.wind_time_freq, d.wind_sharpness = wind
-        d.num_itr = num_itr
-        d.max_h = max_h
-        d.schedule = SCHEDULES[schedule]
-        d.form = FORMS[form]
-        d.pin_roots = int(pin_roots)
-        d.device = device
-        d.slots_per_lane = slots_per_lane
-        d.warps_per_block = warps_per_block
-        keep = [sb, pos, vel, sy, sd]
+        grooms = list(groom) if isinstance(groom, (list, tuple)) else [groom]
+        if velocities is None or not isinstance(groom, (list, tuple)):
+            velocities = [velocities] * len(grooms)
+        keep = []
+        sdf_ptr = None
         if sdf is not None:
             phi = np.ascontiguousarray(sdf.phi, np.float32)
             grad = np.ascontiguousarray(sdf.grad, np.float32)
@@ -214,14 +197,68 @@ class Solver:
             sd_.phi = phi.ctypes.data
             sd_.grad = grad.ctypes.data
             keep += [phi, grad, sd_]
-            d.sdf = ctypes.pointer(sd_)
+            sdf_ptr = ctypes.pointer(sd_)
+        descs = (Desc * len(grooms))()
+        for d, g, v in zip(descs, grooms, velocities):
+            sb = np.ascontiguousarray(g.strand_begin, np.int32)
+            pos = _f32(g.positions)
+            vel = None if v is None else _f32(v)
+            sy = np.ascontiguousarray(g.strand_young, np.float32) if per_strand else None
+            sd = np.ascontiguousarray(g.strand_dev, np.float32) if per_strand else None
+            keep += [sb, pos, vel, sy, sd]
+            _check(self.lib.kami_vbd_desc_init(ctypes.byref(d)))
+            d.num_strands = g.num_strands
+            d.strand_begin = sb.ctypes.data
+            d.positions = pos.ctypes.data
+            d.velocities = vel.ctypes.data if vel is not None else None
+            d.radius, d.density = radius, density
+            d.stiffness_mode = stiffness_mode
+            d.young, d.deviation = young, deviation
+            d.strand_young = sy.ctypes.data if sy is not None else None
+            d.strand_deviation = sd.ctypes.data if sd is not None else None
+            d.k_stretch, d.k_bend = k_stretch, k_bend
+            d.gravity[:] = gravity
+            d.damping, d.velocity_decay, d.acceleration_ratio = damping, velocity_decay, acceleration_ratio
+            d.external_force_multiplier = ext_mult
+            d.wind_peak, d.wind_y_freq, d.wind_z_freq, d.wind_time_freq, d.wind_sharpness = wind
+            d.num_itr = num_itr
+            d.max_h = max_h
+            d.schedule = SCHEDULES[schedule]
+            d.form = FORMS[form]
+            d.pin_roots = int(pin_roots)
+            d.device = device
+            d.slots_per_lane = slots_per_lane
+            d.warps_per_block = warps_per_block
+            d.sdf = sdf_ptr
         h = ctypes.c_void_p()
-        _check(self.lib.kami_vbd_create(ctypes.byref(d), ctypes.byref(h)))
+        if isinstance(groom, (list, tuple)):
+            _check(self.lib.kami_vbd_batch_create(len(grooms), descs, ctypes.byref(h)))
+        else:
+            _check(self.lib.kami_vbd_create(ctypes.byref(descs[0]), ctypes.byref(h)))
         self._h = h
         nv, ns, c = ctypes.c_int64(), ctypes.c_int32(), ctypes.c_int32()
         _check(self.lib.kami_vbd_get_sizes(h, ctypes.byref(nv), ctypes.byref(ns), ctypes.byref(c)))
         self.num_vertices, self.num_strands, self.slots_per_lane = nv.value, ns.value, c.value
+        ng = ctypes.c_int32()
+        _check(self.lib.kami_vbd_batch_count(h, ctypes.byref(ng)))
+        self.num_grooms = ng.value
         del keep
+
+    def groom_range(self, groom):
+        """(first strand, strands, first vertex, vertices) of one groom of a batch handle."""
+        s0, ns, v0, nv = ctypes.c_int32(), ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int64()
+        _check(self.lib.kami_vbd_batch_groom_range(self._h, groom, ctypes.byref(s0), ctypes.byref(ns),
+                                                   ctypes.byref(v0), ctypes.byref(nv)))
+        return s0.value, ns.value, v0.value, nv.value
+
+    def batch_step(self, dt, n, body_transforms=None, stream=None):
+        """kami_vbd_batch_step: every groom of the handle, n steps."""
+        s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+        bt = None if body_transforms is None else _f32(body_transforms, (-1, 7))
+        if bt is not None and bt.shape[0] != n:
+            raise ValueError("body_transforms needs one row per step")
+        _check(self.lib.kami_vbd_batch_step(self._h, ctypes.c_float(dt), n,
+                                            None if bt is None else bt.ctypes.data_as(ctypes.c_void_p), s))
 
     # -- lifecycle
     def close(self):

@@ -84,3 +84,45 @@ def test_autotune_picks_a_shape_and_restores_the_state():
     assert np.abs(s.get_positions_velocities()[0] - ref.get_positions_velocities()[0]).max() <= 1e-6
     s.close()
     ref.close()
+
+
+def test_batch_handle_equals_one_handle_per_groom():
+    """kami_vbd_batch_create over 4 uneven grooms sets up each groom exactly as its own
+    kami_vbd_create handle would, and kami_vbd_batch_step with a moving body tracks single steps
+    of every groom and the FP32 oracle.  The fused kernel's FMA contraction depends on where a
+    strand sits in its warp tile (register or shuffled neighbour), and the batch packs strands
+    differently from one groom alone, so the dynamics agree to an ulp-level bound, not bitwise."""
+    grooms = synth.batched_grooms(4, strands_range=(50, 400), verts_range=(16, 128), seed=21)
+    st = _settings()
+    vel = [helpers.random_velocities(g, 0.1, seed=i) for i, g in enumerate(grooms)]
+    from kamisimulator_b200.vbd import Solver
+
+    b = Solver(grooms, form="fused", velocities=vel, slots_per_lane=4, **st)
+    assert b.num_grooms == 4
+    singles = [Solver(g, form="fused", velocities=v, slots_per_lane=4, **st) for g, v in zip(grooms, vel)]
+    ranges = [b.groom_range(i) for i in range(4)]
+    qb0, qrb = b.get_orientations(), b.get_rest_darboux()
+    for (s0, ns, v0, nv), g, s in zip(ranges, grooms, singles):
+        assert ns == g.num_strands and nv == g.num_vertices
+        np.testing.assert_array_equal(qb0[v0:v0 + nv], s.get_orientations())
+        np.testing.assert_array_equal(qrb[v0:v0 + nv], s.get_rest_darboux())
+    frames = 6
+    bt = np.array([list(synth.head_rotation(f / 120.0)) + [0.0, 0.001 * f, 0.0] for f in range(frames)], np.float32)
+    b.batch_step(1 / 120, frames, bt)
+    o = helpers.oracle_sim(grooms[1], st, np.float32, velocities=vel[1])
+    for f in range(frames):
+        o.set_body_transform(bt[f, :4], bt[f, 4:])
+        o.advance(1 / 120)
+    for s in singles:
+        for f in range(frames):
+            s.set_body_transform(bt[f, :4], bt[f, 4:])
+            s.step(1 / 120)
+    xb, vb = b.get_positions_velocities()
+    for i, ((s0, ns, v0, nv), s) in enumerate(zip(ranges, singles)):
+        x, v = s.get_positions_velocities()
+        assert np.abs(xb[v0:v0 + nv] - x).max() <= 1e-6
+        assert np.abs(vb[v0:v0 + nv] - v).max() <= 1e-4  # velocity = dx / h, h = 1/120
+        if i == 1:
+            assert np.abs(xb[v0:v0 + nv] - o.x).max() <= helpers.POS_TOL
+        s.close()
+    b.close()

@@ -106,3 +106,25 @@ def test_null_handle_calls_fail_cleanly():
     assert lib.kami_vbd_destroy(None) == 0
     n = ctypes.c_size_t()
     assert lib.kami_vbd_state_size(None, ctypes.byref(n)) == 1
+
+
+def test_batch_rejects_grooms_with_different_solver_settings():
+    """The check runs on the host before any device work, so it needs no GPU (1 = KAMI_ERR_INVALID_ARGUMENT)."""
+    g0, g1 = synth.cantilever(2, 8), synth.cantilever(3, 6)
+    descs = (vbd.Desc * 2)()
+    lib = vbd.load_library()
+    keep = []
+    for d, g in zip(descs, (g0, g1)):
+        sb = np.ascontiguousarray(g.strand_begin, np.int32)
+        pos = np.ascontiguousarray(g.positions, np.float32)
+        keep += [sb, pos]
+        assert lib.kami_vbd_desc_init(ctypes.byref(d)) == 0
+        d.num_strands, d.strand_begin, d.positions = g.num_strands, sb.ctypes.data, pos.ctypes.data
+    descs[1].num_itr = descs[0].num_itr + 1
+    h = ctypes.c_void_p()
+    assert lib.kami_vbd_batch_create(2, descs, ctypes.byref(h)) == 1
+    assert "groom 1 differs from groom 0 in num_itr" in lib.kami_vbd_last_error_string().decode()
+    assert lib.kami_vbd_batch_create(0, descs, ctypes.byref(h)) == 1
+    descs[1].num_itr = descs[0].num_itr
+    descs[1].strand_begin = None
+    assert lib.kami_vbd_batch_create(2, descs, ctypes.byref(h)) == 1
