@@ -33,7 +33,9 @@ typedef enum kami_status {
     KAMI_ERR_GEOMETRY = 5,         /* zero-length or dangling segment (Sim::configure, YBSimulator.cu:185-197) */
     KAMI_ERR_UNSUPPORTED = 6,      /* request outside what this build supports (e.g. strand longer than a tile) */
     KAMI_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
-    KAMI_ERR_STATE = 8             /* call made in the wrong order (e.g. backward without a recorded forward) */
+    KAMI_ERR_STATE = 8,            /* call made in the wrong order (e.g. backward without a recorded forward) */
+    KAMI_ERR_CONTACTS = 9          /* a segment had more than 16 hair-hair contacts (MAX_COLLISIONS_PER_SEGMENT,
+                                      YarnBall.h:19; Sim::checkErrors throws there, YBSimulator.cu:396-398) */
 } kami_status;
 
 /* Gauss-Seidel order of the position and orientation sweeps. */
@@ -112,6 +114,20 @@ typedef struct kami_vbd_desc {
      * warps_per_block: warps per CTA of the fused kernel. */
     int32_t slots_per_lane;
     int32_t warps_per_block;
+
+    /* Hair-hair collision: EnableHairHairColl (StableCosseratRodsSolver.cpp:176-186) with the
+     * MetaData constants of YarnBall.h:93-114.  Runs on the sweep form (form AUTO picks it).
+     * Contacts are detected every detection_period substeps from the predicted motion and resolved
+     * with an IPC barrier plus friction inside the position sweeps; a segment holds at most 16. */
+    int32_t hair_hair;         /* 1: on */
+    float barrier_thickness;   /* barrierThickness [m]; the solver sets 2 (1 - 0.05) CurveRadius */
+    float k_collision;         /* kCollision (1e-5) */
+    float k_friction;          /* kFriction (5) */
+    float friction_coeff;      /* frictionCoeff (0.1) */
+    float detection_scaler;    /* detectionScaler (1.2), must be > 1 */
+    int32_t detection_period;  /* detectionPeriod: substeps between detections (1); <= 0 never detects */
+    int32_t step_limit;        /* useStepSizeLimit (1, as the solver sets it with EnableHairHairColl) */
+    int32_t velocity_radius;   /* useVelocityRadius (1) */
 } kami_vbd_desc;
 
 typedef struct kami_vbd_solver* kami_vbd_handle;

@@ -3,6 +3,8 @@
 
 #include <cuda_runtime.h>
 
+#include <algorithm>
+#include <cfloat>
 #include <cmath>
 #include <cstdarg>
 #include <cstdio>
@@ -91,6 +93,16 @@ struct kami_vbd_solver {
     cudaGraphExec_t graph_n = nullptr;
     int graph_n_steps = -1, graph_n_F = -1;
 
+    // hair-hair collision (sweep form): parameters and arrays, the substep counter that paces
+    // detection (Sim::stepCounter, step.cpp:52), and whether the contact lists must be rebuilt
+    bool hair_hair = false;
+    int detection_period = 1;
+    CollParams cp{};
+    int64_t counter = 0;
+    bool coll_stale = true;
+    float4* d_snap = nullptr;
+    std::vector<char> graph_detect;  // substeps of the cached sweep graph that run detection
+
     // differentiable stepping: the tape of recorded steps and the adjoint state
     int tape_capacity = 0;
     int64_t tape_tiles = 0;               // tiles the tape holds per step
@@ -147,6 +159,12 @@ void release(kami_vbd_solver* h) {
                     h->d_gv,      h->d_gvl, h->d_gq, h->d_gqr};
     for (void* p : ptrs)
         if (p) cudaFree(p);
+    const CollParams& c = h->cp;
+    void* cptrs[] = {(void*)c.vid, (void*)c.gid, c.cols,   c.ncols,  c.maxstep,  c.bmin,    c.bmax,
+                     c.cell,       c.count,      c.start,  c.cursor, c.sorted,   c.ext_bits, c.scan_tmp,
+                     h->d_snap};
+    for (void* p : cptrs)
+        if (p) cudaFree(p);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
     if (h->ev_b) cudaEventDestroy(h->ev_b);
     if (h->stream) cudaStreamDestroy(h->stream);
@@ -181,6 +199,10 @@ kami_status check_status_word(kami_vbd_solver* h) {
         KAMI_CUDA(cudaMemsetAsync(h->d_status, 0, sizeof(int), h->stream), "status reset");
         if (word & STATUS_NONFINITE)
             return fail(KAMI_ERR_NONFINITE, "non-finite position, velocity or orientation produced by a step");
+        if (word & STATUS_CONTACTS)
+            return fail(KAMI_ERR_CONTACTS,
+                        "a segment has more than 16 hair-hair contacts (MAX_COLLISIONS_PER_SEGMENT exceeded); "
+                        "the step dropped the extra contacts");
         return fail(KAMI_ERR_CUDA, "device status word 0x%x", word);
     }
     return KAMI_OK;
@@ -212,8 +234,20 @@ kami_status valid_handle(kami_vbd_solver* h) {
         if (s_ != KAMI_OK) return s_;       \
     } while (0)
 
+// Which substeps of the next step run collision detection: every detectionPeriod-th substep of the
+// handle's life (step.cpp:53), and the first one after the contact lists went stale.
+static std::vector<char> detect_pattern(const kami_vbd_solver* h, int substeps) {
+    std::vector<char> d(substeps, 0);
+    if (!h->hair_hair) return d;
+    for (int sub = 0; sub < substeps; sub++)
+        d[sub] = h->detection_period > 0 && (h->counter + sub) % h->detection_period == 0;
+    if (h->coll_stale && h->detection_period > 0 && substeps > 0) d[0] = 1;
+    return d;
+}
+
 kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
-    if (h->graph && h->graph_substeps == substeps) return KAMI_OK;
+    const std::vector<char> detect = detect_pattern(h, substeps);
+    if (h->graph && h->graph_substeps == substeps && h->graph_detect == detect) return KAMI_OK;
     if (h->graph) {
         cudaGraphExecDestroy(h->graph);
         h->graph = nullptr;
@@ -224,18 +258,34 @@ kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
     cudaStream_t s = h->stream;
     KAMI_CUDA(cudaStreamBeginCapture(s, cudaStreamCaptureModeThreadLocal), "cudaStreamBeginCapture");
     cudaError_t err = cudaSuccess;
+    const size_t b4 = sizeof(float4) * h->layout.num_slots;
     for (int sub = 0; sub < substeps && err == cudaSuccess; sub++) {
         err = launch_sweep_predict(st, h->d_y, h->d_dx, h->d_step, h->pp, h->layout.num_slots, s);
+        if (h->hair_hair) {
+            if (err == cudaSuccess && detect[sub]) err = launch_coll_detect(st, h->d_dx, h->cp, s);
+            if (err == cudaSuccess) err = launch_coll_steplimit(st, h->d_dx, h->cp, s);
+        }
         float4* dx_cur = h->d_dx;
         float4* dx_alt = h->d_dx2;
         float4* q_cur = h->d_q;
         float4* q_alt = h->d_q2;
         for (int it = 0; it < h->pp.num_itr && err == cudaSuccess; it++) {
             if (jac) {
-                err = launch_sweep_position(st, h->d_y, q_cur, dx_cur, dx_alt, h->d_step, h->pp, C, 0, true, s);
+                if (h->hair_hair)
+                    err = launch_sweep_position_coll(st, h->d_y, q_cur, dx_cur, dx_alt, dx_cur, h->d_step, h->pp, h->cp, 0,
+                                                     true, s);
+                else
+                    err = launch_sweep_position(st, h->d_y, q_cur, dx_cur, dx_alt, h->d_step, h->pp, C, 0, true, s);
                 std::swap(dx_cur, dx_alt);
                 if (err == cudaSuccess) err = launch_sweep_orientation(st, dx_cur, q_cur, q_alt, C, 0, true, s);
                 std::swap(q_cur, q_alt);
+            } else if (h->hair_hair) {
+                err = cudaMemcpyAsync(h->d_snap, dx_cur, b4, cudaMemcpyDeviceToDevice, s);  // partners' dx
+                for (int c = 0; c < 2 && err == cudaSuccess; c++)
+                    err = launch_sweep_position_coll(st, h->d_y, q_cur, dx_cur, dx_cur, h->d_snap, h->d_step, h->pp, h->cp,
+                                                     c, false, s);
+                for (int c = 0; c < 2 && err == cudaSuccess; c++)
+                    err = launch_sweep_orientation(st, dx_cur, q_cur, q_cur, C, c, false, s);
             } else {
                 for (int c = 0; c < 2 && err == cudaSuccess; c++)
                     err = launch_sweep_position(st, h->d_y, q_cur, dx_cur, dx_cur, h->d_step, h->pp, C, c, false, s);
@@ -259,6 +309,7 @@ kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
     cudaGraphDestroy(g);
     if (e3 != cudaSuccess) return cuda_fail(e3, "cudaGraphInstantiate");
     h->graph_substeps = substeps;
+    h->graph_detect = detect;
     return KAMI_OK;
 }
 
@@ -295,6 +346,15 @@ kami_status kami_vbd_desc_init(kami_vbd_desc* d) {
     d->pin_roots = 1;
     d->device = -1;
     d->sdf = nullptr;
+    d->hair_hair = 0;
+    d->barrier_thickness = 2.f * (1.f - 0.05f) * 4e-5f;  // StableCosseratRodsSolver.cpp:176-180 at CurveRadius 4e-5
+    d->k_collision = 1e-5f;                               // Sim::Sim, YBSimulator.cu:91-102
+    d->k_friction = 5.f;
+    d->friction_coeff = 0.1f;
+    d->detection_scaler = 1.2f;
+    d->detection_period = 1;
+    d->step_limit = 1;  // StableCosseratRodsSolver.cpp:184: useStepSizeLimit = EnableHairHairColl
+    d->velocity_radius = 1;
     return KAMI_OK;
 }
 
@@ -320,6 +380,16 @@ static kami_status validate_desc(const kami_vbd_desc* d) {
         for (int a = 0; a < 3; a++)
             if (!(s->grid_max[a] > s->grid_min[a])) return fail(KAMI_ERR_INVALID_ARGUMENT, "SDF grid_max must exceed grid_min");
     }
+    if (d->hair_hair) {
+        if (!(d->barrier_thickness > 0.f)) return fail(KAMI_ERR_INVALID_ARGUMENT, "barrier_thickness must be > 0");
+        if (!(d->detection_scaler > 1.f))  // Sim::uploadMeta, YBSimulator.cu:326
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "detection_scaler must be greater than 1");
+        if (!(d->k_collision >= 0.f) || !(d->k_friction >= 0.f) || !(d->friction_coeff >= 0.f))
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "collision stiffness and friction must be >= 0");
+        if (d->form == KAMI_FORM_FUSED)
+            return fail(KAMI_ERR_UNSUPPORTED, "hair-hair collision runs on the sweep form (strands of one warp tile "
+                                              "meet partners in other tiles)");
+    }
     return KAMI_OK;
 }
 
@@ -340,6 +410,13 @@ static const char* differing_setting(const kami_vbd_desc* a, const kami_vbd_desc
     if (a->form != b->form) return "form";
     if (a->device != b->device) return "device";
     if (a->slots_per_lane != b->slots_per_lane || a->warps_per_block != b->warps_per_block) return "tile shape";
+    if (a->hair_hair != b->hair_hair) return "hair_hair";
+    if (a->hair_hair &&
+        (a->radius != b->radius || a->barrier_thickness != b->barrier_thickness || a->k_collision != b->k_collision ||
+         a->k_friction != b->k_friction || a->friction_coeff != b->friction_coeff ||
+         a->detection_scaler != b->detection_scaler || a->detection_period != b->detection_period ||
+         a->step_limit != b->step_limit || a->velocity_radius != b->velocity_radius))
+        return "radius or hair-hair collision settings";
     if ((a->sdf == nullptr) != (b->sdf == nullptr)) return "sdf";
     if (a->sdf && a->sdf != b->sdf) {
         const kami_vbd_sdf_desc *x = a->sdf, *y = b->sdf;
@@ -349,6 +426,64 @@ static const char* differing_setting(const kami_vbd_desc* a, const kami_vbd_desc
         if (x->threshold != y->threshold || x->phi != y->phi || x->grad != y->grad) return "sdf";
     }
     return nullptr;
+}
+
+// Hair-hair collision arrays: per-slot boundary vertex and groom indices, contact lists, step
+// limits, boxes and the spatial hash (a power-of-two table of at least twice the slot count).
+static kami_status setup_collisions(kami_vbd_solver* h, const kami_vbd_desc* d) {
+    const int64_t S = h->layout.num_slots;
+    if (S >= INT32_MAX) return fail(KAMI_ERR_UNSUPPORTED, "hair-hair collision supports fewer than 2^31 slots");
+    h->hair_hair = true;
+    h->detection_period = d->detection_period;
+    CollParams& c = h->cp;
+    c.det_r = d->radius + 0.5f * d->barrier_thickness;  // Sim::uploadMeta, YBSimulator.cu:323-324
+    c.scaled_r = c.det_r * d->detection_scaler;
+    c.scaler = d->detection_scaler;
+    c.radius2 = 2.f * d->radius;
+    c.invb = 1.f / d->barrier_thickness;
+    c.kcol = d->k_collision * c.invb;
+    c.kfric = d->k_friction;
+    c.mu = d->friction_coeff;
+    c.use_vel = d->velocity_radius != 0;
+    c.limit = d->step_limit != 0;
+    c.num_slots = S;
+    c.C = h->layout.C;
+    int bits = 10;
+    while ((1LL << bits) < 2 * S && bits < 30) bits++;
+    c.table_bits = bits;
+    const int64_t table = 1LL << bits;
+    std::vector<int32_t> vid(S, -1), gid(S, -1);
+    const int32_t ng = (int32_t)h->groom_strand_begin.size() - 1;
+    for (int32_t g = 0; g < ng; g++)
+        for (int64_t i = h->strand_begin[h->groom_strand_begin[g]]; i < h->strand_begin[h->groom_strand_begin[g + 1]]; i++) {
+            vid[h->layout.slot_of[i]] = (int32_t)i;
+            gid[h->layout.slot_of[i]] = g;
+        }
+    int32_t *dvid = nullptr, *dgid = nullptr;
+    cudaError_t e = dalloc(&dvid, S);
+    if (e == cudaSuccess) e = dalloc(&dgid, S);
+    c.vid = dvid;
+    c.gid = dgid;
+    if (e == cudaSuccess) e = dalloc(&c.cols, (size_t)MAX_CONTACTS * S);
+    if (e == cudaSuccess) e = dalloc(&c.ncols, S);
+    if (e == cudaSuccess) e = dalloc(&c.maxstep, S);
+    if (e == cudaSuccess) e = dalloc(&c.bmin, S);
+    if (e == cudaSuccess) e = dalloc(&c.bmax, S);
+    if (e == cudaSuccess) e = dalloc(&c.cell, S);
+    if (e == cudaSuccess) e = dalloc(&c.count, table);
+    if (e == cudaSuccess) e = dalloc(&c.start, table);
+    if (e == cudaSuccess) e = dalloc(&c.cursor, table);
+    if (e == cudaSuccess) e = dalloc(&c.sorted, S);
+    if (e == cudaSuccess) e = dalloc(&c.ext_bits, 1);
+    if (e == cudaSuccess) e = dalloc(&c.scan_tmp, coll_scan_tmp_size(table));
+    if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_COLOUR2) e = dalloc(&h->d_snap, S);
+    if (e != cudaSuccess) return cuda_fail(e, "allocating hair-hair collision arrays");
+    e = cudaMemcpy(dvid, vid.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemcpy(dgid, gid.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMemset(c.ncols, 0, sizeof(int32_t) * S);
+    if (e != cudaSuccess) return cuda_fail(e, "uploading hair-hair collision arrays");
+    h->coll_stale = true;
+    return KAMI_OK;
 }
 
 // Builds one handle over the strands of n descriptors (n = 1: kami_vbd_create).  Each groom's
@@ -438,7 +573,18 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
         return bail(fail(KAMI_ERR_INVALID_ARGUMENT, "warps_per_block must be 0 or a power of two <= 32"));
     if (d->warps_per_block > 0) h->warps_per_block = d->warps_per_block;
     int form = d->form;
-    if (form == KAMI_FORM_AUTO) form = fused_supported(C) ? KAMI_FORM_FUSED : KAMI_FORM_SWEEP;
+    if (form == KAMI_FORM_AUTO) form = (fused_supported(C) && !d->hair_hair) ? KAMI_FORM_FUSED : KAMI_FORM_SWEEP;
+    if (d->hair_hair) {
+        // Sim::uploadMeta (YBSimulator.cu:328-332): contacts must fit between a segment's ends
+        float min_seg = FLT_MAX;
+        for (int64_t i = 0; i < h->nv; i++)
+            if (m.flags[i] & F_HAS_NEXT) min_seg = std::min(min_seg, m.l_rest[i]);
+        if (2.f * min_seg < 2.f * d->radius + d->barrier_thickness)
+            return bail(fail(KAMI_ERR_GEOMETRY,
+                             "use thinner strands or longer segments: 2 x shortest segment (%g) must be >= "
+                             "2 x radius + barrier_thickness (%g)",
+                             2.0 * min_seg, 2.0 * d->radius + d->barrier_thickness));
+    }
     if (form == KAMI_FORM_FUSED && !fused_supported(C))
         return bail(fail(KAMI_ERR_UNSUPPORTED, "fused form supports strands of up to 128 vertices"));
     h->form = form;
@@ -546,6 +692,10 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
         sp.inv_y = 1.f / sp.ds_y;
         sp.inv_z = 1.f / sp.ds_z;
         sp.thresh = s->threshold;
+    }
+    if (d->hair_hair) {
+        kami_status cs = setup_collisions(h, d);
+        if (cs != KAMI_OK) return bail(cs);
     }
     *out = h;
     return KAMI_OK;
@@ -688,11 +838,13 @@ kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
             h->h_step = sp;
             KAMI_CUDA(cudaMemcpyAsync(h->d_step, &h->h_step, sizeof(StepParams), cudaMemcpyHostToDevice, s), "step params");
             KAMI_CUDA(cudaGraphLaunch(h->graph, s), "cudaGraphLaunch");
+            if (h->hair_hair) h->coll_stale = false;
         }
         return KAMI_OK;
     });
     if (st != KAMI_OK) return st;
     h->time += dt;
+    h->counter += steps;
     return KAMI_OK;
 }
 
@@ -768,6 +920,8 @@ static kami_status relayout(kami_vbd_solver* h, int C) {
 kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32_t warps_per_block,
                                 int32_t steps_per_launch, int32_t register_cap) {
     KAMI_TRY(valid_handle(h));
+    if (slots_per_lane != 0 && h->hair_hair && slots_per_lane != h->layout.C)
+        return fail(KAMI_ERR_UNSUPPORTED, "the tile shape of a handle with hair-hair collision is fixed at creation");
     if (slots_per_lane != 0) {
         const int cmin = slots_per_lane_for(h->strand_begin.data(), h->ns);
         if (slots_per_lane < cmin || (slots_per_lane & 1))
@@ -833,6 +987,7 @@ kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float*
         if (body_transforms) kami_vbd_set_body_transform(h, body_transforms + 7 * j, body_transforms + 7 * j + 4);
         h->h_steps[j] = advance_clock(h, dt);
         h->time += dt;
+        h->counter += h->h_steps[j].substeps;
     }
     const int F = std::min(h->steps_per_launch, n);
     if (!h->graph_n || h->graph_n_steps != n || h->graph_n_F != F) {
@@ -1017,6 +1172,7 @@ kami_status kami_vbd_step_record(kami_vbd_handle h, float dt, void* stream) {
     if (st != KAMI_OK) return st;
     h->tape_steps.push_back(sp);
     h->time += dt;
+    h->counter += sp.substeps;
     return KAMI_OK;
 }
 
@@ -1102,7 +1258,11 @@ kami_status kami_vbd_get_state(kami_vbd_handle h, void* dst, size_t bytes, int32
     KAMI_CUDA(launch_gather4(h->d_q, (float4*)h->d_stage, h->d_slot_of, nv, h->stream), "gather state");
     KAMI_CUDA(cudaMemcpyAsync(f + 9 * nv, h->d_stage, sizeof(float) * 4 * nv, kind, h->stream), "state copy");
     KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
-    const float clk[4] = {h->h, h->last_h, h->time, 0.f};
+    // the fourth word holds the substep counter (uint32 bits), which paces hair-hair detection
+    const uint32_t ctr = (uint32_t)h->counter;
+    float ctr_f;
+    std::memcpy(&ctr_f, &ctr, 4);
+    const float clk[4] = {h->h, h->last_h, h->time, ctr_f};
     if (memory == KAMI_MEMORY_DEVICE)
         KAMI_CUDA(cudaMemcpy(f + 13 * nv, clk, sizeof(clk), cudaMemcpyHostToDevice), "state clock");
     else
@@ -1134,6 +1294,10 @@ kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes,
     h->h = clk[0];
     h->last_h = clk[1];
     h->time = clk[2];
+    uint32_t ctr;
+    std::memcpy(&ctr, &clk[3], 4);
+    h->counter = ctr;
+    h->coll_stale = true;  // the contact lists belong to the state before
     return KAMI_OK;
 }
 

@@ -1,0 +1,456 @@
+// vbd_collision.cu -- hair-hair collision of the sweep form (EnableHairHairColl).
+//
+// Detection (once every detectionPeriod substeps, after the predict, as Sim::advance calls
+// detectCollisions, YarnBall/sim/step.cpp:53):
+//   1. every segment's box around its two end points, padded by scaledDetectionRadius plus its
+//      velocity radius (buildAABBs, collision.cu:8-32), and the largest box extent;
+//   2. a spatial hash of the box centres on cells of that extent: bucket counts, an exclusive scan
+//      and a scatter group the segments by bucket;
+//   3. each segment scans the 27 cells around its centre and keeps the partners that pass the
+//      distance test of buildCollisionList (collision.cu:36-92), in ascending partner order.
+// Two boxes that overlap have centres less than one extent apart on every axis, so the 27 cells
+// find every pair the reference's LBVH query finds (KittenGpuLBVH/lbvh.cu:197-292); the distance
+// test, evaluated once per pair with the lower vertex index first, then decides.
+//
+// The step limit (recomputeStepLimitKernel, collision.cu:95-131) runs on every substep, and the
+// position sweep adds each contact's IPC barrier and friction terms (cosseratItr,
+// cosserat.cu:163-227).  The partner segment's displacement is read from a snapshot taken at the
+// start of the iteration, so the sweep does not race on the partner's vertices.
+#include "vbd_kernels.h"
+#include "vbd_math.cuh"
+
+namespace kami {
+namespace {
+
+constexpr uint32_t NO_CELL = 0xffffffffu;
+
+__device__ __forceinline__ float len2(float3 a) { return dot3(a, a); }
+// glm::mix(x, y, t) = x (1 - t) + y t
+__device__ __forceinline__ float3 mixv(float3 a, float3 b, float t) { return a * (1.f - t) + b * t; }
+__device__ __forceinline__ float clamp01(float v) { return fminf(fmaxf(v, 0.f), 1.f); }
+__device__ __forceinline__ bool finite3c(float3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
+
+// Kit::segmentClosestPoints (KittenEngine/includes/modules/Common.h:294-312): the closest points
+// are mix(a0, a1, u) and mix(b0, b1, w).
+__device__ __forceinline__ float2 seg_closest(float3 a0, float3 a1, float3 b0, float3 b1) {
+    const float3 A0 = a1 - a0, A1 = b1 - b0;
+    const float a = len2(A0), b = dot3(A0, A1), c = len2(A1);
+    const float3 diff = b0 - a0;
+    float w = b * dot3(A0, diff) - a * dot3(A1, diff);
+    w /= a * c - b * b;
+    if (!isfinite(w)) w = 0.5f;
+    w = clamp01(w);
+    const float u = clamp01(dot3(mixv(b0, b1, w) - a0, A0) / a);
+    w = clamp01(dot3(mixv(a0, a1, u) - b0, A1) / c);
+    return make_float2(u, w);
+}
+
+// Spatial hash of a cell (the three large primes of Teschner et al., "Optimized Spatial Hashing
+// for Collision Detection of Deformable Objects", VMV 2003).
+__device__ __forceinline__ uint32_t cell_hash(uint32_t x, uint32_t y, uint32_t z, uint32_t mask) {
+    return ((x * 73856093u) ^ (y * 19349663u) ^ (z * 83492791u)) & mask;
+}
+
+__device__ __forceinline__ float cell_size(const CollParams& cp) { return __uint_as_float(*cp.ext_bits) * 1.01f; }
+
+// glm::inverse(mat3) of the packed symmetric Hessian (hess3::operator mat3, SymMat.h:66-75)
+// applied to f: the adjugate over the determinant.
+__device__ __forceinline__ float3 solve_sym3(const float H[6], float3 f) {
+    const float m00 = H[0], m11 = H[1], m22 = H[2], m01 = H[3], m02 = H[4], m12 = H[5];
+    const float det = m00 * (m11 * m22 - m12 * m12) - m01 * (m01 * m22 - m12 * m02) + m02 * (m01 * m12 - m11 * m02);
+    const float od = 1.f / det;
+    const float i00 = (m11 * m22 - m12 * m12) * od;
+    const float i10 = -(m01 * m22 - m02 * m12) * od;
+    const float i20 = (m01 * m12 - m02 * m11) * od;
+    const float i01 = -(m01 * m22 - m12 * m02) * od;
+    const float i11 = (m00 * m22 - m02 * m02) * od;
+    const float i21 = -(m00 * m12 - m02 * m01) * od;
+    const float i02 = (m01 * m12 - m11 * m02) * od;
+    const float i12 = -(m00 * m12 - m01 * m02) * od;
+    const float i22 = (m00 * m11 - m01 * m01) * od;
+    return f3(i00 * f.x + i10 * f.y + i20 * f.z, i01 * f.x + i11 * f.y + i21 * f.z, i02 * f.x + i12 * f.y + i22 * f.z);
+}
+
+// ---- detection --------------------------------------------------------------------------------
+
+__global__ void coll_box_kernel(DeviceState st, const float4* __restrict__ dx4, CollParams cp) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    float ext = 0.f;
+    if (g < cp.num_slots) {
+        const uint32_t fl = __float_as_uint(st.prm[g].w);
+        if (fl & F_HAS_NEXT) {
+            const int64_t gn = next_slot(g, cp.C);
+            const float3 p0 = xyz(st.xm[g]), p1 = xyz(st.xm[gn]);
+            float vr = 0.f;
+            if (cp.use_vel) vr = sqrtf(fmaxf(len2(xyz(dx4[g])), len2(xyz(dx4[gn]))));
+            const float pad = cp.scaled_r + vr;
+            const float3 lo = f3(fminf(p0.x, p1.x) - pad, fminf(p0.y, p1.y) - pad, fminf(p0.z, p1.z) - pad);
+            const float3 hi = f3(fmaxf(p0.x, p1.x) + pad, fmaxf(p0.y, p1.y) + pad, fmaxf(p0.z, p1.z) + pad);
+            cp.bmin[g] = make_float4(lo.x, lo.y, lo.z, vr);
+            cp.bmax[g] = make_float4(hi.x, hi.y, hi.z, 1.f);
+            const float e = fmaxf(fmaxf(hi.x - lo.x, hi.y - lo.y), hi.z - lo.z);
+            if (isfinite(e)) ext = e;
+        } else {
+            cp.bmax[g] = make_float4(0.f, 0.f, 0.f, 0.f);
+        }
+    }
+    for (int o = 16; o; o >>= 1) ext = fmaxf(ext, __shfl_xor_sync(0xffffffffu, ext, o));
+    if ((threadIdx.x & 31) == 0 && ext > 0.f) atomicMax(cp.ext_bits, __float_as_uint(ext));
+}
+
+__device__ __forceinline__ bool box_cell(const CollParams& cp, int64_t g, int3& ci) {
+    const float4 lo = cp.bmin[g], hi = cp.bmax[g];
+    if (hi.w == 0.f) return false;
+    const float3 c = f3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
+    const float cs = cell_size(cp);
+    if (!finite3c(c) || !(cs > 0.f)) return false;
+    const float inv = 1.f / cs;
+    ci = make_int3(__float2int_rd(c.x * inv), __float2int_rd(c.y * inv), __float2int_rd(c.z * inv));
+    return true;
+}
+
+__global__ void coll_hash_kernel(CollParams cp) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= cp.num_slots) return;
+    int3 ci;
+    if (!box_cell(cp, g, ci)) {
+        cp.cell[g] = NO_CELL;
+        return;
+    }
+    const uint32_t mask = (1u << cp.table_bits) - 1u;
+    const uint32_t h = cell_hash((uint32_t)ci.x, (uint32_t)ci.y, (uint32_t)ci.z, mask);
+    cp.cell[g] = h;
+    atomicAdd(&cp.count[h], 1);
+}
+
+__global__ void coll_scatter_kernel(CollParams cp) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= cp.num_slots) return;
+    const uint32_t h = cp.cell[g];
+    if (h == NO_CELL) return;
+    const int32_t pos = atomicAdd(&cp.cursor[h], 1);
+    cp.sorted[pos] = (int32_t)g;
+}
+
+__global__ void coll_query_kernel(DeviceState st, CollParams cp) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= cp.num_slots) return;
+    int3 ci;
+    if (!box_cell(cp, g, ci)) {
+        cp.ncols[g] = 0;
+        return;
+    }
+    const float4 loa = cp.bmin[g], hia = cp.bmax[g];
+    const int32_t va = cp.vid[g], ga = cp.gid[g];
+    const float slack = 1e-3f * cell_size(cp);  // box overlap is a pre-filter: never reject a pair the distance test keeps
+    const float3 xa0 = xyz(st.xm[g]), xa1 = xyz(st.xm[next_slot(g, cp.C)]);
+    const uint32_t mask = (1u << cp.table_bits) - 1u;
+    int32_t lst[MAX_CONTACTS], key[MAX_CONTACTS];
+    int n = 0;
+    bool over = false;
+    for (int dz = -1; dz <= 1; dz++)
+        for (int dy = -1; dy <= 1; dy++)
+            for (int dxc = -1; dxc <= 1; dxc++) {
+                const uint32_t h = cell_hash((uint32_t)ci.x + (uint32_t)dxc, (uint32_t)ci.y + (uint32_t)dy,
+                                             (uint32_t)ci.z + (uint32_t)dz, mask);
+                const int32_t b = cp.start[h], e = b + cp.count[h];
+                for (int32_t k = b; k < e; k++) {
+                    const int32_t j = cp.sorted[k];
+                    if (j == g || cp.gid[j] != ga) continue;
+                    const int32_t vb = cp.vid[j];
+                    if (abs(vb - va) <= 2) continue;  // neighbouring segments (collision.cu:52)
+                    const float4 lob = cp.bmin[j], hib = cp.bmax[j];
+                    if (lob.x > hia.x + slack || loa.x > hib.x + slack || lob.y > hia.y + slack ||
+                        loa.y > hib.y + slack || lob.z > hia.z + slack || loa.z > hib.z + slack)
+                        continue;
+                    bool dup = false;
+                    for (int m = 0; m < n && m < MAX_CONTACTS; m++) dup |= lst[m] == j;
+                    if (dup) continue;  // two of the 27 cells can share a bucket
+                    const float3 xb0 = xyz(st.xm[j]), xb1 = xyz(st.xm[next_slot(j, cp.C)]);
+                    const bool af = va < vb;
+                    const float3 p0 = af ? xa0 : xb0, p1 = af ? xa1 : xb1, q0 = af ? xb0 : xa0, q1 = af ? xb1 : xa1;
+                    const float3 A1 = p1 - p0, B0 = q0 - p0, B1 = q1 - p0;
+                    const float2 uv = seg_closest(f3(0.f, 0.f, 0.f), A1, B0, B1);
+                    const float3 nrm = uv.x * A1 - mixv(B0, B1, uv.y);
+                    const float d2 = len2(nrm);
+                    float r = 2.f * cp.scaled_r;
+                    if (cp.use_vel) {
+                        r += af ? loa.w : lob.w;
+                        r += af ? lob.w : loa.w;
+                    }
+                    if (d2 < r * r) {
+                        if (n < MAX_CONTACTS) {
+                            lst[n] = j;
+                            key[n] = vb;
+                        } else {
+                            over = true;
+                        }
+                        n++;
+                    }
+                }
+            }
+    const int m = min(n, MAX_CONTACTS);
+    for (int i = 1; i < m; i++) {  // ascending partner vertex index
+        const int32_t kk = key[i], vv = lst[i];
+        int j = i - 1;
+        while (j >= 0 && key[j] > kk) {
+            key[j + 1] = key[j];
+            lst[j + 1] = lst[j];
+            j--;
+        }
+        key[j + 1] = kk;
+        lst[j + 1] = vv;
+    }
+    for (int i = 0; i < m; i++) cp.cols[(int64_t)i * cp.num_slots + g] = lst[i];
+    cp.ncols[g] = m;
+    if (over) atomicOr(st.status, STATUS_CONTACTS);
+}
+
+// Exclusive scan of int32 counts, 4096 per block (1024 threads x 4): per-block scan + block sums.
+__global__ void __launch_bounds__(1024) scan_block_kernel(const int32_t* in, int32_t* out, int32_t* sums, int64_t n) {
+    __shared__ int32_t warp_tot[32];
+    const int64_t base = (int64_t)blockIdx.x * 4096 + (int64_t)threadIdx.x * 4;
+    int32_t v[4];
+    for (int i = 0; i < 4; i++) v[i] = (base + i < n) ? in[base + i] : 0;
+    const int32_t tsum = v[0] + v[1] + v[2] + v[3];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    int32_t incl = tsum;
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t t = __shfl_up_sync(0xffffffffu, incl, o);
+        if (lane >= o) incl += t;
+    }
+    if (lane == 31) warp_tot[warp] = incl;
+    __syncthreads();
+    if (warp == 0) {
+        int32_t wv = warp_tot[lane];
+        int32_t wi = wv;
+        for (int o = 1; o < 32; o <<= 1) {
+            const int32_t t = __shfl_up_sync(0xffffffffu, wi, o);
+            if (lane >= o) wi += t;
+        }
+        warp_tot[lane] = wi - wv;  // exclusive offset of each warp
+        if (lane == 31) sums[blockIdx.x] = wi;
+    }
+    __syncthreads();
+    int32_t run = warp_tot[warp] + incl - tsum;
+    for (int i = 0; i < 4; i++) {
+        if (base + i < n) out[base + i] = run;
+        run += v[i];
+    }
+}
+
+__global__ void scan_add_kernel(int32_t* out, const int32_t* offs, int64_t n) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] += offs[i / 4096];
+}
+
+cudaError_t exclusive_scan(const int32_t* in, int32_t* out, int64_t n, int32_t* tmp, cudaStream_t s) {
+    const int64_t blocks = (n + 4095) / 4096;
+    scan_block_kernel<<<(unsigned)blocks, 1024, 0, s>>>(in, out, tmp, n);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess || blocks == 1) return e;
+    e = exclusive_scan(tmp, tmp, blocks, tmp + blocks, s);
+    if (e != cudaSuccess) return e;
+    scan_add_kernel<<<(unsigned)((n + 255) / 256), 256, 0, s>>>(out, tmp, n);
+    return cudaGetLastError();
+}
+
+// ---- step limit ---------------------------------------------------------------------------------
+
+__global__ void coll_steplimit_kernel(DeviceState st, const float4* __restrict__ dx4, CollParams cp) {
+    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (g >= cp.num_slots) return;
+    const uint32_t fl = __float_as_uint(st.prm[g].w);
+    float min_dist = INFINITY;
+    if (cp.limit && (fl & F_HAS_NEXT)) {
+        const float margin = (1.f - 0.1f) * 0.5f;  // (1 - SAFETY_MARGIN) / 2, collision.cu:102, :126
+        const float3 a0 = xyz(st.xm[g]);
+        const float3 A1 = xyz(st.xm[next_slot(g, cp.C)]) - a0;
+        min_dist = cp.det_r * (cp.scaler - 1.f);
+        if (cp.use_vel) min_dist += sqrtf(len2(xyz(dx4[g])));
+        const int n = cp.ncols[g];
+        for (int k = 0; k < n; k++) {
+            const int64_t o = cp.cols[(int64_t)k * cp.num_slots + g];
+            const float3 B0 = xyz(st.xm[o]) - a0, B1 = xyz(st.xm[next_slot(o, cp.C)]) - a0;
+            const float2 uv = seg_closest(f3(0.f, 0.f, 0.f), A1, B0, B1);
+            const float l = sqrtf(len2(uv.x * A1 - mixv(B0, B1, uv.y)));
+            min_dist = fminf(min_dist, margin * l);
+        }
+    }
+    cp.maxstep[g] = min_dist;
+}
+
+// ---- position sweep with contacts -----------------------------------------------------------------
+
+// One contact of segment (x0, x1) (displacements d0, d1) with the segment starting at slot o: the
+// IPC barrier and friction terms of cosserat.cu:177-226, for the segment's first vertex (own) or
+// its second vertex.
+__device__ __forceinline__ void contact_term(const DeviceState& st, const CollParams& cp, const float4* __restrict__ snap,
+                                             float3 x0, float3 x1, float3 d0, float3 d1, int64_t o, bool own,
+                                             float damp, float3& f, float H[6]) {
+    const int64_t on = next_slot(o, cp.C);
+    const float3 b0 = xyz(st.xm[o]), b1 = xyz(st.xm[on]);
+    const float3 db0 = xyz(snap[o]), db1 = xyz(snap[on]);
+    const float2 uv = seg_closest(f3(0.f, 0.f, 0.f), (x1 - x0) + (d1 - d0), (b0 - x0) + (db0 - d0), (b1 - x0) + (db1 - d0));
+    const float3 dpos = mixv(x0, x1, uv.x) - mixv(b0, b1, uv.y);
+    const float3 ddpos = mixv(d0, d1, uv.x) - mixv(db0, db1, uv.y);
+    float3 nrm = dpos + ddpos;
+    float d = sqrtf(len2(nrm));
+    nrm = nrm * (1.f / d);
+    const float wt = own ? 1.f - uv.x : uv.x;
+    d = d - cp.radius2;
+    d *= cp.invb;
+    if (d > 1.f) return;  // not touching
+    d = fmaxf(d, 1e-3f);
+    const float invd = 1.f / d;
+    const float logd = logf(d);
+    float dH = (-3.f + (2.f + invd) * invd - 2.f * logd) * cp.kcol * cp.invb;
+    const float ff = -(1.f - d) * (d - 1.f + 2.f * d * logd) * invd * cp.kcol;
+    const float3 mydx = own ? d0 : d1;
+    f = f + (ff * wt - damp * dH * wt * wt * dot3(nrm, mydx)) * nrm;
+    dH *= 1.f + damp;
+    float op[6] = {nrm.x * nrm.x, nrm.y * nrm.y, nrm.z * nrm.z, nrm.x * nrm.y, nrm.x * nrm.z, nrm.y * nrm.z};
+#pragma unroll
+    for (int k = 0; k < 6; k++) H[k] += op[k] * (dH * wt * wt);
+    const float3 u = ddpos - dot3(nrm, ddpos) * nrm;
+    const float ul = sqrtf(len2(u));
+    if (ul > 0.f) {
+        const float f1 = fminf(cp.kfric, cp.mu * ff / ul);
+        op[0] -= 1.f;
+        op[1] -= 1.f;
+        op[2] -= 1.f;
+        f = f - (f1 * wt) * u;
+#pragma unroll
+        for (int k = 0; k < 6; k++) H[k] -= op[k] * (wt * wt * f1);
+    }
+}
+
+// The position sweep of the sweep form with hair-hair contacts: cosseratItr (cosserat.cu:112-285)
+// with its full 3x3 block and the step-limit clamp.  Thread mapping and the in-place (colour2) /
+// double-buffered (jacobi) update as in sweep_position_kernel; `snap` holds the partners' dx.
+template <bool JACOBI>
+__global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restrict__ y4, const float4* __restrict__ qcur,
+                                           const float4* dx_in, float4* dx_out, const float4* snap,
+                                           const StepParams* __restrict__ spp, PhysParams pp, CollParams cp, int colour,
+                                           int64_t num_threads) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= num_threads) return;
+    const int C = cp.C;
+    const int rows = JACOBI ? C : C / 2;
+    const int64_t tile = t / (32LL * rows);
+    const int rem = (int)(t - tile * 32LL * rows);
+    const int r = rem >> 5, lane = rem & 31;
+    const int k = JACOBI ? r : 2 * r + colour;
+    const int64_t g = tile * 32LL * C + (int64_t)k * 32 + lane;
+    const float4 prm = st.prm[g];
+    const uint32_t fl = __float_as_uint(prm.w);
+    const float4 d4 = dx_in[g];
+    const float4 xm = st.xm[g];
+    if (!(fl & F_VALID) || xm.w == 0.f) {
+        if (JACOBI) dx_out[g] = d4;
+        return;
+    }
+    const float h = spp->h;
+    const float damp = pp.damping / h;
+    const float im = xm.w;
+    const float3 vi = xyz(xm), vi_dx = xyz(d4);
+    float H[6];
+    const float inert = 1.f / (im * h * h);
+#pragma unroll
+    for (int n = 0; n < 6; n++) H[n] = inert;  // hess3(float) fills all six entries (SymMat.h:16-18)
+    float3 f = (1.f / (h * h * im)) * (xyz(y4[g]) - vi_dx);
+    float step_limit = INFINITY;
+    if (fl & F_HAS_NEXT) {
+        const int64_t gn = next_slot(g, C);
+        const float3 xj = xyz(st.xm[gn]), vj_dx = xyz(dx_in[gn]);
+        const float invl = 1.f / prm.x;
+        const float3 cc = ((xj - vi) + (vj_dx - vi_dx)) * invl - d3_of(qcur[g]);
+        const float kk = prm.y * invl;
+        float dd = kk * invl;
+        f = f + (kk * cc - (damp * dd) * vi_dx);
+        dd *= 1.f + damp;
+        H[0] += dd;
+        H[1] += dd;
+        H[2] += dd;
+        step_limit = cp.maxstep[g];
+        const int n = cp.ncols[g];
+        for (int m = 0; m < n; m++)
+            contact_term(st, cp, snap, vi, xj, vi_dx, vj_dx, cp.cols[(int64_t)m * cp.num_slots + g], true, damp, f, H);
+    }
+    if (fl & F_HAS_PREV) {
+        const int64_t gp = prev_slot(g, C);
+        const float4 pp4 = st.prm[gp];
+        const float3 xp = xyz(st.xm[gp]), dp = xyz(dx_in[gp]);
+        const float invl = 1.f / pp4.x;
+        const float3 cc = ((vi - xp) + (vi_dx - dp)) * invl - d3_of(qcur[gp]);
+        const float kk = pp4.y * invl;
+        float dd = kk * invl;
+        float3 f2 = (-kk) * cc - (damp * dd) * vi_dx;
+        dd *= 1.f + damp;
+        float H2[6] = {dd, dd, dd, 0.f, 0.f, 0.f};
+        const int n = cp.ncols[gp];
+        for (int m = 0; m < n; m++)
+            contact_term(st, cp, snap, xp, vi, dp, vi_dx, cp.cols[(int64_t)m * cp.num_slots + gp], false, damp, f2, H2);
+        step_limit = fminf(step_limit, cp.maxstep[gp]);
+        f = f + f2;
+#pragma unroll
+        for (int q = 0; q < 6; q++) H[q] += H2[q];
+    }
+    const float3 delta = pp.accel_ratio * solve_sym3(H, f);
+    float3 out = vi_dx + delta;
+    const float l = sqrtf(len2(out));
+    if (l > step_limit && l > 0.f) out = out * (step_limit / l);
+    dx_out[g] = make_float4(out.x, out.y, out.z, 0.f);
+}
+
+inline unsigned blocks_of(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
+
+}  // namespace
+
+int64_t coll_scan_tmp_size(int64_t n) {
+    int64_t total = 0;
+    while (n > 4096) {
+        n = (n + 4095) / 4096;
+        total += n;
+    }
+    return total + 1;
+}
+
+cudaError_t launch_coll_detect(const DeviceState& st, const float4* dx4, const CollParams& cp, cudaStream_t s) {
+    const int64_t S = cp.num_slots;
+    const int64_t table = 1LL << cp.table_bits;
+    cudaError_t e = cudaMemsetAsync(cp.ext_bits, 0, sizeof(unsigned), s);
+    if (e != cudaSuccess) return e;
+    coll_box_kernel<<<blocks_of(S, 256), 256, 0, s>>>(st, dx4, cp);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = cudaMemsetAsync(cp.count, 0, sizeof(int32_t) * table, s)) != cudaSuccess) return e;
+    coll_hash_kernel<<<blocks_of(S, 256), 256, 0, s>>>(cp);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    if ((e = exclusive_scan(cp.count, cp.start, table, cp.scan_tmp, s)) != cudaSuccess) return e;
+    if ((e = cudaMemcpyAsync(cp.cursor, cp.start, sizeof(int32_t) * table, cudaMemcpyDeviceToDevice, s)) != cudaSuccess)
+        return e;
+    coll_scatter_kernel<<<blocks_of(S, 256), 256, 0, s>>>(cp);
+    if ((e = cudaGetLastError()) != cudaSuccess) return e;
+    coll_query_kernel<<<blocks_of(S, 128), 128, 0, s>>>(st, cp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_coll_steplimit(const DeviceState& st, const float4* dx4, const CollParams& cp, cudaStream_t s) {
+    coll_steplimit_kernel<<<blocks_of(cp.num_slots, 256), 256, 0, s>>>(st, dx4, cp);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_sweep_position_coll(const DeviceState& st, const float4* y4, const float4* q, const float4* dx_in,
+                                       float4* dx_out, const float4* snap, const StepParams* d_sp, const PhysParams& pp,
+                                       const CollParams& cp, int colour, bool jacobi, cudaStream_t s) {
+    const int64_t n = st.num_tiles * 32LL * (jacobi ? cp.C : cp.C / 2);
+    if (jacobi)
+        sweep_position_coll_kernel<true><<<blocks_of(n, 128), 128, 0, s>>>(st, y4, q, dx_in, dx_out, snap, d_sp, pp, cp,
+                                                                          colour, n);
+    else
+        sweep_position_coll_kernel<false><<<blocks_of(n, 128), 128, 0, s>>>(st, y4, q, dx_in, dx_out, snap, d_sp, pp, cp,
+                                                                           colour, n);
+    return cudaGetLastError();
+}
+
+}  // namespace kami

@@ -25,7 +25,13 @@ enum : uint32_t {
 };
 
 // Status word bits raised by the kernels.
-enum : int { STATUS_NONFINITE = 1 };
+enum : int {
+    STATUS_NONFINITE = 1,
+    STATUS_CONTACTS = 2,  // a segment found more than MAX_CONTACTS hair-hair contacts
+};
+
+// Partners a segment can hold: MAX_COLLISIONS_PER_SEGMENT, YarnBall/YarnBall.h:19.
+constexpr int MAX_CONTACTS = 16;
 
 // Per-solver physical constants (MetaData scalars, YarnBall/YarnBall.h:80-123).
 struct PhysParams {
@@ -95,6 +101,56 @@ struct AdjointState {
     float4* gq;
     float4* gqr;
 };
+
+// Hair-hair collision: constants (MetaData, YarnBall/YarnBall.h:93-114) and the device arrays of
+// detection (padded segment boxes, a spatial hash of their centres, per-segment contact lists)
+// and of the step limit.  Slots are int32 here: a handle with hair-hair collision has < 2^31 slots.
+struct CollParams {
+    float scaled_r;  // scaledDetectionRadius = (radius + barrier / 2) * detectionScaler
+    float det_r;     // detectionRadius = radius + barrier / 2
+    float scaler;    // detectionScaler
+    float radius2;   // 2 * radius: the contact distance before the barrier
+    float invb;      // 1 / barrierThickness
+    float kcol;      // kCollision / barrierThickness
+    float kfric;     // kFriction
+    float mu;        // frictionCoeff
+    int use_vel;     // useVelocityRadius
+    int limit;       // useStepSizeLimit
+    const int32_t* vid;  // boundary vertex index of each slot (-1: padding)
+    const int32_t* gid;  // groom of each slot (batch handles)
+    int32_t* cols;       // [MAX_CONTACTS][S] partner segment (first slot), ascending by partner vid
+    int32_t* ncols;      // [S]
+    float* maxstep;      // [S] step limit of the segment starting at the slot
+    float4* bmin;        // [S] padded box: min xyz, velocity radius
+    float4* bmax;        // [S] padded box: max xyz, 1 when the slot starts a segment
+    uint32_t* cell;      // [S] hash bucket of the segment's box centre
+    int32_t* count;      // [table] segments per bucket
+    int32_t* start;      // [table] first entry of each bucket in `sorted`
+    int32_t* cursor;     // [table] scatter cursor
+    int32_t* sorted;     // [S] segments grouped by bucket
+    unsigned* ext_bits;  // largest padded box extent (float bits): the cell size
+    int32_t* scan_tmp;   // block sums of the bucket scan
+    int table_bits;
+    int64_t num_slots;
+    int C;
+};
+
+// ---- tile slot neighbours ----------------------------------------------------------------------
+// Storage index of slot p+1 / p-1 of the strand slot stored at g (the caller knows it exists).
+__host__ __device__ __forceinline__ int64_t next_slot(int64_t g, int C) {
+    const int64_t T = 32LL * C;
+    const int64_t tile = g / T;
+    const int r = (int)(g - tile * T);
+    const int k = r >> 5, lane = r & 31;
+    return (k < C - 1) ? g + 32 : tile * T + lane + 1;
+}
+__host__ __device__ __forceinline__ int64_t prev_slot(int64_t g, int C) {
+    const int64_t T = 32LL * C;
+    const int64_t tile = g / T;
+    const int r = (int)(g - tile * T);
+    const int k = r >> 5, lane = r & 31;
+    return (k > 0) ? g - 32 : tile * T + (int64_t)(C - 1) * 32 + lane - 1;
+}
 
 // ---- small helpers ---------------------------------------------------------------------------
 __host__ __device__ __forceinline__ float3 f3(float x, float y, float z) { return make_float3(x, y, z); }

@@ -18,24 +18,6 @@
 
 namespace kami {
 
-// ------------------------------------------------------------------------------------------
-// tile index helpers
-__device__ __forceinline__ int64_t next_slot(int64_t g, int C) {
-    // slot p+1 of the slot stored at g (caller guarantees p < T-1)
-    int64_t T = 32LL * C;
-    int64_t tile = g / T;
-    int r = (int)(g - tile * T);
-    int k = r >> 5, lane = r & 31;
-    return (k < C - 1) ? g + 32 : tile * T + lane + 1;
-}
-__device__ __forceinline__ int64_t prev_slot(int64_t g, int C) {
-    int64_t T = 32LL * C;
-    int64_t tile = g / T;
-    int r = (int)(g - tile * T);
-    int k = r >> 5, lane = r & 31;
-    return (k > 0) ? g - 32 : tile * T + (int64_t)(C - 1) * 32 + lane - 1;
-}
-
 // ==========================================================================================
 // sweep form
 // ==========================================================================================

@@ -29,6 +29,15 @@ cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, con
 cudaError_t launch_adjoint_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                                 const TapeView& tp, const AdjointState& ad, int C, cudaStream_t s);
 
+// Hair-hair collision (vbd_collision.cu).  coll_scan_tmp_size: int32 elements of scratch the
+// bucket scan of a table of n buckets needs.
+int64_t coll_scan_tmp_size(int64_t n);
+cudaError_t launch_coll_detect(const DeviceState& st, const float4* dx4, const CollParams& cp, cudaStream_t s);
+cudaError_t launch_coll_steplimit(const DeviceState& st, const float4* dx4, const CollParams& cp, cudaStream_t s);
+cudaError_t launch_sweep_position_coll(const DeviceState& st, const float4* y4, const float4* q, const float4* dx_in,
+                                       float4* dx_out, const float4* snap, const StepParams* d_sp, const PhysParams& pp,
+                                       const CollParams& cp, int colour, bool jacobi, cudaStream_t s);
+
 cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
 cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
 cudaError_t launch_scatter4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);

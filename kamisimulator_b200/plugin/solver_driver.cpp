@@ -41,10 +41,11 @@ int main(int argc, char** argv) {
             std::printf("{\"num_strands\": %d, \"num_vertices\": %d, \"radius\": %.9g, \"density\": %.9g, "
                         "\"num_itr\": %d, \"young\": %.9g, \"deviation\": %.9g, \"stiffness_mode\": %d, "
                         "\"velocity_decay\": %.9g, \"wind_peak\": %.9g, \"max_h\": %.9g, \"schedule\": %d, "
-                        "\"form\": %d, \"gravity\": [%.9g, %.9g, %.9g]}\n",
+                        "\"form\": %d, \"gravity\": [%.9g, %.9g, %.9g], \"hair_hair\": %d, "
+                        "\"barrier_thickness\": %.9g, \"step_limit\": %d}\n",
                         d.num_strands, d.strand_begin[d.num_strands], d.radius, d.density, d.num_itr, d.young,
                         d.deviation, d.stiffness_mode, d.velocity_decay, d.wind_peak, d.max_h, d.schedule, d.form,
-                        d.gravity[0], d.gravity[1], d.gravity[2]);
+                        d.gravity[0], d.gravity[1], d.gravity[2], d.hair_hair, d.barrier_thickness, d.step_limit);
             return 0;
         }
         if (argc < 6) {

@@ -160,6 +160,53 @@ def concat_grooms(grooms: list) -> Groom:
                  np.concatenate(dev))
 
 
+# ---- hair-hair contact scenes ---------------------------------------------------------------------
+
+def bar_and_drape(verts: int = 25, segment: float = 1e-3, gap: float = 3e-4, bar_young: float = 5.0,
+                  drape_young: float = 1e-6) -> Groom:
+    """A stiff strand along x (root at -x) and a soft strand along y, `gap` above it, crossing it at
+    the middle: under gravity the soft strand falls onto the stiff one."""
+    half = segment * (verts - 1) / 2
+    t = np.linspace(-half, half, verts)
+    a = np.stack([t, np.zeros(verts), np.zeros(verts)], 1)
+    b = np.stack([np.zeros(verts), t, np.full(verts, gap)], 1)
+    return Groom(strand_begin=np.array([0, verts, 2 * verts], np.int32),
+                 positions=np.concatenate([a, b]).astype(np.float32),
+                 strand_young=np.array([bar_young, drape_young], np.float32), strand_dev=np.ones(2, np.float32))
+
+
+def tangle(num_strands: int = 24, verts: int = 24, segment: float = 1e-3, layer: float = 2e-4, seed: int = 0,
+           young: float = 1e-5) -> Groom:
+    """Horizontal strands through a common vertical axis, each `layer` above the previous one, in
+    random directions: falling under gravity they pile onto each other (many crossing contacts)."""
+    rng = np.random.default_rng(seed)
+    half = segment * (verts - 1) / 2
+    pos = []
+    for k in range(num_strands):
+        th = rng.uniform(0, 2 * np.pi)
+        d = np.array([np.cos(th), np.sin(th), 0.0])
+        c = np.array([rng.uniform(-2e-3, 2e-3), rng.uniform(-2e-3, 2e-3), k * layer])
+        pos.append(c + (np.arange(verts)[:, None] * segment - half) * d)
+    return Groom(strand_begin=np.arange(num_strands + 1, dtype=np.int32) * verts,
+                 positions=np.concatenate(pos).astype(np.float32),
+                 strand_young=np.full(num_strands, young, np.float32), strand_dev=np.ones(num_strands, np.float32))
+
+
+def contact_fence(num_posts: int = 20, spacing: float = 3e-5, verts: int = 8, segment: float = 1e-3) -> Groom:
+    """`num_posts` parallel strands `spacing` apart and one strand across all of them: its middle
+    segment touches every post, more than the 16 contacts a segment can hold."""
+    half = segment * (verts - 1) / 2
+    t = np.arange(verts) * segment - half
+    pos = []
+    for k in range(num_posts):
+        x = (k - (num_posts - 1) / 2) * spacing
+        pos.append(np.stack([np.full(verts, x), t, np.zeros(verts)], 1))
+    pos.append(np.stack([t, np.zeros(verts), np.full(verts, 4e-5)], 1))
+    n = num_posts + 1
+    return Groom(strand_begin=np.arange(n + 1, dtype=np.int32) * verts, positions=np.concatenate(pos).astype(np.float32),
+                 strand_young=np.full(n, 1.0, np.float32), strand_dev=np.ones(n, np.float32))
+
+
 def sphere_sdf(n: int = 128, radius: float = 0.09, half_extent: float = 0.2, threshold: float = 1e-3) -> SDFGrid:
     dims = (n, n, n)
     gmin = (-half_extent,) * 3

@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libkami_vbd.so")
 KAMI_OK = 0
 STATUS_NAMES = {0: "KAMI_OK", 1: "KAMI_ERR_INVALID_ARGUMENT", 2: "KAMI_ERR_CUDA", 3: "KAMI_ERR_OUT_OF_MEMORY",
                 4: "KAMI_ERR_NONFINITE", 5: "KAMI_ERR_GEOMETRY", 6: "KAMI_ERR_UNSUPPORTED", 7: "KAMI_ERR_TIMEOUT",
-                8: "KAMI_ERR_STATE"}
+                8: "KAMI_ERR_STATE", 9: "KAMI_ERR_CONTACTS"}
 SCHEDULES = {"colour2": 0, "jacobi": 1}
 FORMS = {"auto": 0, "sweep": 1, "fused": 2}
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -84,6 +84,15 @@ class Desc(ctypes.Structure):
         ("sdf", ctypes.POINTER(SdfDesc)),
         ("slots_per_lane", ctypes.c_int32),
         ("warps_per_block", ctypes.c_int32),
+        ("hair_hair", ctypes.c_int32),
+        ("barrier_thickness", ctypes.c_float),
+        ("k_collision", ctypes.c_float),
+        ("k_friction", ctypes.c_float),
+        ("friction_coeff", ctypes.c_float),
+        ("detection_scaler", ctypes.c_float),
+        ("detection_period", ctypes.c_int32),
+        ("step_limit", ctypes.c_int32),
+        ("velocity_radius", ctypes.c_int32),
     ]
 
 
@@ -176,7 +185,9 @@ class Solver:
                  damping=1e-6, velocity_decay=0.05, acceleration_ratio=1.0, ext_mult=1.0,
                  wind=(0.0, 1.0, 0.7, 0.4, 3.0), schedule="colour2", form="auto", sdf=None, stiffness_mode=0,
                  young=5.0, deviation=1.0, per_strand=True, k_stretch=3e3, k_bend=6e-4, pin_roots=True,
-                 velocities=None, device=-1, slots_per_lane=0, warps_per_block=0):
+                 velocities=None, device=-1, slots_per_lane=0, warps_per_block=0, hair_hair=False,
+                 barrier_thickness=None, k_collision=None, k_friction=None, friction_coeff=None,
+                 detection_scaler=None, detection_period=None, step_limit=None, velocity_radius=None):
         """groom: one groom (kami_vbd_create) or a list of grooms (kami_vbd_batch_create, one handle
         stepping all of them; velocities is then None or a list with one entry per groom)."""
         self.lib = load_library()
@@ -230,6 +241,13 @@ class Solver:
             d.slots_per_lane = slots_per_lane
             d.warps_per_block = warps_per_block
             d.sdf = sdf_ptr
+            d.hair_hair = int(bool(hair_hair))
+            for name, val in (("barrier_thickness", barrier_thickness), ("k_collision", k_collision),
+                              ("k_friction", k_friction), ("friction_coeff", friction_coeff),
+                              ("detection_scaler", detection_scaler), ("detection_period", detection_period),
+                              ("step_limit", step_limit), ("velocity_radius", velocity_radius)):
+                if val is not None:
+                    setattr(d, name, val)
         h = ctypes.c_void_p()
         if isinstance(groom, (list, tuple)):
             _check(self.lib.kami_vbd_batch_create(len(grooms), descs, ctypes.byref(h)))

@@ -29,6 +29,7 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <vector>
 #include <algorithm>
 #ifdef _OPENMP
@@ -179,6 +180,17 @@ typedef struct oracle_params {
     float body_rot[4];      // (x, y, z, w)
     float body_trans[3];
     int32_t num_threads;    // <= 0: OpenMP default
+    // hair-hair collision (MetaData, YarnBall.h:93-114; StableCosseratRodsSolver.cpp:176-186)
+    int32_t hair_hair;        // enableHairHairColl
+    float radius;             // MetaData::radius
+    float barrier_thickness;  // barrierThickness
+    float k_collision;        // kCollision
+    float k_friction;         // kFriction
+    float friction_coeff;     // frictionCoeff
+    float detection_scaler;   // detectionScaler
+    int32_t detection_period; // detectionPeriod
+    int32_t step_limit;       // useStepSizeLimit
+    int32_t velocity_radius;  // useVelocityRadius
 } oracle_params;
 
 }  // extern "C"
@@ -283,6 +295,27 @@ int configureT(int64_t nv, int32_t ns, const int32_t* sb, const float* pos, floa
     return 0;
 }
 
+constexpr int kMaxCollisions = 16;  // MAX_COLLISIONS_PER_SEGMENT, YarnBall.h:19
+
+// Kit::segmentClosestPoints (KittenEngine/includes/modules/Common.h:294-312): closest points
+// mix(a0, a1, uv.x) and mix(b0, b1, uv.y) of two segments.  glm::mix(x, y, t) = x (1 - t) + y t.
+template <typename T>
+inline void segClosest(V3<T> a0, V3<T> a1, V3<T> b0, V3<T> b1, T& u, T& w) {
+    V3<T> A0 = a1 - a0, A1 = b1 - b0;
+    T a = dot(A0, A0), b = dot(A0, A1), c = dot(A1, A1);
+    V3<T> diff = b0 - a0;
+    T vy = b * dot(A0, diff) - a * dot(A1, diff);
+    vy /= a * c - b * b;
+    if (!std::isfinite((double)vy)) vy = T(0.5);
+    vy = std::min(std::max(vy, T(0)), T(1));
+    V3<T> pb = b0 * (T(1) - vy) + b1 * vy;
+    T vx = std::min(std::max(dot(pb - a0, A0) / a, T(0)), T(1));
+    V3<T> pa = a0 * (T(1) - vx) + a1 * vx;
+    vy = std::min(std::max(dot(pa - b0, A1) / c, T(0)), T(1));
+    u = vx;
+    w = vy;
+}
+
 template <typename T>
 struct StepCtx {
     const oracle_params* p;
@@ -298,7 +331,139 @@ struct StepCtx {
     T* vl;
     T* q;
     std::vector<T> y, dx, dxNew, qNew;
+    // hair-hair collision state: partner segments of each segment (ascending), their count, the
+    // step limit of each segment, and the partner dx snapshot of the current iteration
+    std::vector<int32_t> cols, ncols;
+    std::vector<T> maxStep, snap;
 };
+
+// The collision detection of detectCollisions (YBSimulator.cu:424-456): buildAABBs +
+// LBVH query + buildCollisionList (collision.cu:8-92).  The LBVH only proposes pairs whose padded
+// AABBs overlap, and every pair that passes the distance test below has overlapping padded
+// AABBs, so the result is the set of segment pairs (a, b), |a - b| > 2, with
+// |closest(a, b)| < 2 scaledDetectionRadius (+ the velocity radii).  Each pair is tested once,
+// with the lower index as segment a; each segment lists its partners in ascending order.  Returns
+// 1 when a segment has more than 16 partners (ERROR_MAX_COLLISIONS_PER_SEGMENT_EXCEEDED).
+template <typename T>
+int detectCollisions(StepCtx<T>& c) {
+    const oracle_params* p = c.p;
+    const T detR = (T)p->radius + T(0.5f) * (T)p->barrier_thickness;  // Sim::uploadMeta, YBSimulator.cu:323-324
+    const T scaled = detR * (T)p->detection_scaler;
+    const int64_t nv = c.nv;
+    c.cols.assign(kMaxCollisions * nv, -1);
+    c.ncols.assign(nv, 0);
+    std::vector<T> vr(nv, T(0));  // velocity radius of each segment
+    if (p->velocity_radius)
+        for (int64_t i = 0; i < nv; i++)
+            if (c.fl[i] & HAS_NEXT) {
+                V3<T> d0 = ld3(c.dx.data(), i), d1 = ld3(c.dx.data(), i + 1);
+                vr[i] = std::sqrt(std::max(dot(d0, d0), dot(d1, d1)));
+            }
+    int overflow = 0;
+#pragma omp parallel for schedule(dynamic, 16) reduction(| : overflow)
+    for (int64_t i = 0; i < nv; i++) {
+        if (!(c.fl[i] & HAS_NEXT)) continue;
+        int n = 0;
+        for (int64_t j = 0; j < nv; j++) {
+            if (j == i || !(c.fl[j] & HAS_NEXT) || std::llabs(j - i) <= 2) continue;
+            const int64_t a = std::min(i, j), b = std::max(i, j);
+            V3<T> a0 = ld3(c.x, a);
+            V3<T> A1 = ld3(c.x, a + 1) - a0, B0 = ld3(c.x, b) - a0, B1 = ld3(c.x, b + 1) - a0;
+            T u, w;
+            segClosest(v3<T>(0, 0, 0), A1, B0, B1, u, w);
+            V3<T> nrm = u * A1 - (B0 * (T(1) - w) + B1 * w);
+            T d2 = dot(nrm, nrm);
+            T r = T(2) * scaled;
+            if (p->velocity_radius) {
+                r += vr[a];
+                r += vr[b];
+            }
+            if (d2 < r * r) {
+                if (n < kMaxCollisions)
+                    c.cols[(int64_t)n * nv + i] = (int32_t)j;
+                else
+                    overflow = 1;
+                n++;
+            }
+        }
+        c.ncols[i] = std::min(n, kMaxCollisions);
+    }
+    return overflow;
+}
+
+// recomputeStepLimitKernel (collision.cu:95-131): the largest move of each segment's first
+// vertex for which the detection above still sees every contact.
+template <typename T>
+void recomputeStepLimit(StepCtx<T>& c) {
+    const oracle_params* p = c.p;
+    const T detR = (T)p->radius + T(0.5f) * (T)p->barrier_thickness;
+    c.maxStep.assign(c.nv, std::numeric_limits<T>::infinity());
+    if (!p->step_limit) return;
+    const T margin = (T)((1.f - 0.1f) * 0.5f);
+#pragma omp parallel for schedule(static)
+    for (int64_t i = 0; i < c.nv; i++) {
+        if (!(c.fl[i] & HAS_NEXT)) continue;
+        V3<T> a0 = ld3(c.x, i);
+        V3<T> A1 = ld3(c.x, i + 1) - a0;
+        T minDist = detR * ((T)p->detection_scaler - T(1));
+        if (p->velocity_radius) minDist += length(ld3(c.dx.data(), i));
+        for (int k = 0; k < c.ncols[i]; k++) {
+            int64_t o = c.cols[(int64_t)k * c.nv + i];
+            V3<T> B0 = ld3(c.x, o) - a0, B1 = ld3(c.x, o + 1) - a0;
+            T u, w;
+            segClosest(v3<T>(0, 0, 0), A1, B0, B1, u, w);
+            T l = length(u * A1 - (B0 * (T(1) - w) + B1 * w));
+            minDist = std::min(minDist, margin * l);
+        }
+        c.maxStep[i] = minDist;
+    }
+}
+
+// The IPC barrier + friction energy of one contact of segment s = (v0, v1) with partner segment
+// (b0, b1), cosserat.cu:163-227, added to the force / Hessian of v0 (own = true, weight 1 - t) or
+// of v1 (own = false, weight t).  x0/x1 and d0/d1 are the segment's positions and current dx; the
+// partner's dx come from the iteration's snapshot.
+template <typename T>
+void contactTerm(const StepCtx<T>& c, V3<T> x0, V3<T> x1, V3<T> d0, V3<T> d1, int64_t o, bool own, T damping,
+                 V3<T>& f, T H[6]) {
+    const oracle_params* p = c.p;
+    const T invb = T(1) / (T)p->barrier_thickness;
+    const T radius = T(2) * (T)p->radius;
+    const T kCol = (T)p->k_collision * invb;
+    V3<T> b0 = ld3(c.x, o), b1 = ld3(c.x, o + 1);
+    V3<T> db0 = ld3(c.snap.data(), o), db1 = ld3(c.snap.data(), o + 1);
+    T u, w;
+    segClosest(v3<T>(0, 0, 0), (x1 - x0) + (d1 - d0), (b0 - x0) + (db0 - d0), (b1 - x0) + (db1 - d0), u, w);
+    V3<T> dpos = (x0 * (T(1) - u) + x1 * u) - (b0 * (T(1) - w) + b1 * w);
+    V3<T> ddpos = (d0 * (T(1) - u) + d1 * u) - (db0 * (T(1) - w) + db1 * w);
+    V3<T> nrm = dpos + ddpos;
+    T d = length(nrm);
+    nrm = nrm * (T(1) / d);
+    const T wt = own ? T(1) - u : u;
+    d = d - radius;
+    d *= invb;
+    if (d > 1) return;
+    d = std::max(d, T(1e-3f));
+    T invd = T(1) / d;
+    T logd = std::log(d);
+    T dH = (T(-3) + (T(2) + invd) * invd - T(2) * logd) * kCol * invb;
+    T ff = -(T(1) - d) * (d - T(1) + T(2) * d * logd) * invd * kCol;
+    V3<T> mydx = own ? d0 : d1;
+    f = f + (ff * wt - damping * dH * wt * wt * dot(nrm, mydx)) * nrm;
+    dH *= T(1) + damping;
+    T op[6] = {nrm.x * nrm.x, nrm.y * nrm.y, nrm.z * nrm.z, nrm.x * nrm.y, nrm.x * nrm.z, nrm.y * nrm.z};
+    for (int k = 0; k < 6; k++) H[k] += op[k] * (dH * wt * wt);
+    V3<T> uu = ddpos - dot(nrm, ddpos) * nrm;
+    T ul = length(uu);
+    if (ul > 0) {
+        T f1 = std::min((T)p->k_friction, (T)p->friction_coeff * ff / ul);
+        op[0] -= 1;
+        op[1] -= 1;
+        op[2] -= 1;
+        f = f - (f1 * wt) * uu;
+        for (int k = 0; k < 6; k++) H[k] -= op[k] * (wt * wt * f1);
+    }
+}
 
 // initItr, YarnBall/sim/iteration.cu:8-59.  y - x is kept in ctx.y (the reference keeps it in d_vels).
 template <typename T>
@@ -338,19 +503,21 @@ void predict(StepCtx<T>& c, T h, T lastH, T time) {
     }
 }
 
-// cosseratItr, YarnBall/sim/cosserat.cu:112-161 and :246-285, for one vertex i, without the
-// hair-hair collision terms (:163-227; disabled on this path) and with the step limit at
-// infinity (recomputeStepLimitKernel<false,*>, collision.cu:95-131).  dxr is the dx array the
-// vertex reads.  Returns the new dx_i (or the old one when the vertex is pinned).
+// cosseratItr, YarnBall/sim/cosserat.cu:112-161 and :246-285, for one vertex i.  With hair-hair
+// collision on, each segment adds its contacts' barrier and friction terms (:163-227) and the move
+// is clamped to the step limit of the vertex's segments (:157, :270, :281-282).  dxr is the dx
+// array the vertex reads.  Returns the new dx_i (or the old one when the vertex is pinned).
 template <typename T>
 V3<T> positionUpdate(const StepCtx<T>& c, const T* dxr, int64_t i, T h) {
     const T damping = (T)c.p->damping / h;
+    const bool coll = c.p->hair_hair != 0;
     V3<T> vi_dx = ld3(dxr, i);
     if (c.im[i] == 0) return vi_dx;
     T H[6];
     T inert = T(1) / (c.im[i] * h * h);
     for (int k = 0; k < 6; k++) H[k] = inert;  // hess3(float) fills all six entries (SymMat.h:16-18)
     V3<T> f = (T(1) / (h * h * c.im[i])) * (ld3(c.y.data(), i) - vi_dx);
+    T stepLimit = std::numeric_limits<T>::infinity();
     if (c.fl[i] & HAS_NEXT) {  // segment i, as thread i computes it (:141-161)
         V3<T> xi = ld3(c.x, i), xj = ld3(c.x, i + 1), vj_dx = ld3(dxr, i + 1);
         T invl = T(1) / c.lr[i];
@@ -362,6 +529,11 @@ V3<T> positionUpdate(const StepCtx<T>& c, const T* dxr, int64_t i, T h) {
         H[0] += d;
         H[1] += d;
         H[2] += d;
+        if (coll) {
+            stepLimit = c.maxStep[i];
+            for (int n = 0; n < c.ncols[i]; n++)
+                contactTerm(c, xi, xj, vi_dx, vj_dx, c.cols[(int64_t)n * c.nv + i], true, damping, f, H);
+        }
     }
     if (c.fl[i] & HAS_PREV) {  // segment i-1, as thread i-1 computes f2/H2 and passes it on (:157, :269-274)
         int64_t j = i - 1;
@@ -372,13 +544,22 @@ V3<T> positionUpdate(const StepCtx<T>& c, const T* dxr, int64_t i, T h) {
         T d = k * invl;
         V3<T> f2 = -k * cc - (damping * d) * vi_dx;
         d *= 1 + damping;
+        T H2[6] = {d, d, d, 0, 0, 0};
+        if (coll) {
+            for (int n = 0; n < c.ncols[j]; n++)
+                contactTerm(c, xj, xi, dj, vi_dx, c.cols[(int64_t)n * c.nv + j], false, damping, f2, H2);
+            stepLimit = std::min(stepLimit, c.maxStep[j]);
+        }
         f = f + f2;
-        H[0] += d;
-        H[1] += d;
-        H[2] += d;
+        for (int n = 0; n < 6; n++) H[n] += H2[n];
     }
     V3<T> delta = (T)c.p->acceleration_ratio * solveHess3(H, f);
-    return vi_dx + delta;
+    V3<T> out = vi_dx + delta;
+    if (coll) {
+        T l = length(out);
+        if (l > stepLimit && l > 0) out = out * (stepLimit / l);
+    }
+    return out;
 }
 
 // quaternionLambdaItr, YarnBall/sim/cosserat.cu:290-337, for one segment i.  qr_ is the q array
@@ -521,9 +702,22 @@ int advanceT(const oracle_params* p, int64_t nv, int32_t ns, const int32_t* sb, 
     c.dx.assign(3 * nv, T(0));
     c.dxNew.assign(3 * nv, T(0));
     c.qNew.assign(4 * nv, T(0));
-    for (int s = 0; s < steps; s++) {
+    int64_t counter = (int64_t)clock[3];
+    int rc = 0;
+    if (p->hair_hair) {
+        c.cols.assign(kMaxCollisions * nv, -1);
+        c.ncols.assign(nv, 0);
+    }
+    for (int s = 0; s < steps; s++, counter++) {
         predict(c, h, lastH, time);
+        if (p->hair_hair) {
+            // Sim::advance: detection every detectionPeriod substeps (step.cpp:53), then the graph's
+            // recomputeStepLimit (step.cpp:19)
+            if (p->detection_period > 0 && counter % p->detection_period == 0) rc |= detectCollisions(c);
+            recomputeStepLimit(c);
+        }
         for (int it = 0; it < p->num_itr; it++) {
+            if (p->hair_hair) c.snap = c.dx;  // partner dx of this iteration (both schedules)
             if (p->schedule == 1) {
 #pragma omp parallel for schedule(static)
                 for (int64_t i = 0; i < nv; i++) st3(c.dxNew.data(), i, positionUpdate(c, c.dx.data(), i, h));
@@ -550,7 +744,8 @@ int advanceT(const oracle_params* p, int64_t nv, int32_t ns, const int32_t* sb, 
     clock[0] = (double)h;
     clock[1] = (double)lastH;
     clock[2] = (double)((T)clock[2] + (T)dt);
-    return 0;
+    clock[3] = (double)counter;
+    return rc ? 4 : 0;
 }
 
 }  // namespace

@@ -50,6 +50,16 @@ class OracleParams(ctypes.Structure):
         ("body_rot", ctypes.c_float * 4),
         ("body_trans", ctypes.c_float * 3),
         ("num_threads", ctypes.c_int32),
+        ("hair_hair", ctypes.c_int32),
+        ("radius", ctypes.c_float),
+        ("barrier_thickness", ctypes.c_float),
+        ("k_collision", ctypes.c_float),
+        ("k_friction", ctypes.c_float),
+        ("friction_coeff", ctypes.c_float),
+        ("detection_scaler", ctypes.c_float),
+        ("detection_period", ctypes.c_int32),
+        ("step_limit", ctypes.c_int32),
+        ("velocity_radius", ctypes.c_int32),
     ]
 
 
@@ -110,7 +120,10 @@ class OracleSim:
                  damping=1e-6, velocity_decay=0.05, acceleration_ratio=1.0, ext_mult=1.0, wind=(0.0, 0.0, 0.0, 0.0, 3.0),
                  schedule="colour2", sdf=None, body_rot=(0.0, 0.0, 0.0, 1.0), body_trans=(0.0, 0.0, 0.0),
                  stiffness_mode=0, k_stretch=3e3, k_bend=6e-4, pin_roots=True, dtype=np.float32, num_threads=0,
-                 velocities=None):
+                 velocities=None, hair_hair=False, barrier_thickness=7.6e-5, k_collision=1e-5, k_friction=5.0,
+                 friction_coeff=0.1, detection_scaler=1.2, detection_period=1, step_limit=None, velocity_radius=True):
+        """hair_hair: the hair-hair collision path (EnableHairHairColl); step_limit defaults to it, as
+        StableCosseratRodsSolver sets useStepSizeLimit = EnableHairHairColl (.cpp:184)."""
         self.dtype = dtype
         self.lib = load()
         self.groom = groom
@@ -125,7 +138,8 @@ class OracleSim:
         self.v_last = np.zeros((self.nv, 3), dtype)
         max_h = 4e-4 if max_h is None else max_h
         # meta.h starts at maxH (YBSimulator.cu:85), lastH is taken from it on the first advance
-        self.clock = np.array([np.float32(max_h), 0.0, 0.0], np.float64)
+        # h, lastH, time, substep counter (Sim::stepCounter, step.cpp:52)
+        self.clock = np.array([np.float32(max_h), 0.0, 0.0, 0.0], np.float64)
         p = OracleParams()
         p.gravity[:] = gravity
         p.damping, p.velocity_decay, p.acceleration_ratio, p.ext_mult = damping, velocity_decay, acceleration_ratio, ext_mult
@@ -148,6 +162,12 @@ class OracleSim:
             p.sdf_grad = grad.ctypes.data
         p.body_rot[:] = body_rot
         p.body_trans[:] = body_trans
+        p.hair_hair = int(bool(hair_hair))
+        p.radius = radius
+        p.barrier_thickness, p.k_collision, p.k_friction = barrier_thickness, k_collision, k_friction
+        p.friction_coeff, p.detection_scaler, p.detection_period = friction_coeff, detection_scaler, detection_period
+        p.step_limit = int(bool(hair_hair if step_limit is None else step_limit))
+        p.velocity_radius = int(bool(velocity_radius))
         self.params = p
 
     def set_body_transform(self, rot, trans):
@@ -159,6 +179,8 @@ class OracleSim:
         rc = fn(ctypes.byref(self.params), self.nv, self.ns, _p(self.sb), _p(self.inv_mass), _p(self.l_rest),
                 _p(self.k_stretch), _p(self.flags), _p(self.q_rest), _p(self.x), _p(self.v), _p(self.v_last),
                 _p(self.q), _p(self.clock), dt)
+        if rc == 4:
+            raise RuntimeError("a segment has more than 16 contacts (MAX_COLLISIONS_PER_SEGMENT exceeded)")
         if rc != 0:
             raise RuntimeError(f"oracle advance failed with code {rc}")
 

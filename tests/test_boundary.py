@@ -128,3 +128,42 @@ def test_batch_rejects_grooms_with_different_solver_settings():
     descs[1].num_itr = descs[0].num_itr
     descs[1].strand_begin = None
     assert lib.kami_vbd_batch_create(2, descs, ctypes.byref(h)) == 1
+
+
+def _desc_for(g, lib, keep):
+    d = vbd.Desc()
+    assert lib.kami_vbd_desc_init(ctypes.byref(d)) == 0
+    sb = np.ascontiguousarray(g.strand_begin, np.int32)
+    pos = np.ascontiguousarray(g.positions, np.float32)
+    keep += [sb, pos]
+    d.num_strands, d.strand_begin, d.positions = g.num_strands, sb.ctypes.data, pos.ctypes.data
+    return d
+
+
+def test_hair_hair_settings_are_checked_on_the_host():
+    """1 = INVALID_ARGUMENT, 5 = GEOMETRY, 6 = UNSUPPORTED; no device is touched."""
+    lib = vbd.load_library()
+    keep = []
+    h = ctypes.c_void_p()
+    g = synth.cantilever(2, 8)
+    d = _desc_for(g, lib, keep)
+    d.hair_hair = 1
+    d.form = vbd.FORMS["fused"]
+    assert lib.kami_vbd_create(ctypes.byref(d), ctypes.byref(h)) == 6
+    assert "sweep form" in lib.kami_vbd_last_error_string().decode()
+    d.form = vbd.FORMS["auto"]
+    d.detection_scaler = 1.0  # Sim::uploadMeta: "Detection scaler must be greater than 1."
+    assert lib.kami_vbd_create(ctypes.byref(d), ctypes.byref(h)) == 1
+    d.detection_scaler = 1.2
+    d.barrier_thickness = 0.011  # 2 x 5 mm segments < 2 r + barrier
+    assert lib.kami_vbd_create(ctypes.byref(d), ctypes.byref(h)) == 5
+    assert "longer segments" in lib.kami_vbd_last_error_string().decode()
+
+
+def test_desc_defaults_for_hair_hair():
+    d = vbd.Desc()
+    assert vbd.load_library().kami_vbd_desc_init(ctypes.byref(d)) == 0
+    assert d.hair_hair == 0 and d.detection_period == 1 and d.step_limit == 1 and d.velocity_radius == 1
+    assert d.barrier_thickness == pytest.approx(2 * 0.95 * 4e-5)  # StableCosseratRodsSolver.cpp:176-180
+    assert d.k_collision == pytest.approx(1e-5) and d.k_friction == pytest.approx(5.0)
+    assert d.friction_coeff == pytest.approx(0.1) and d.detection_scaler == pytest.approx(1.2)

@@ -65,10 +65,21 @@ def test_descriptor_from_reference_settings(tmp_path):
 def test_unsupported_settings_are_rejected(tmp_path):
     g = synth.cantilever(2, 8)
     write_hair(tmp_path / "hair.bin", g)
-    (tmp_path / "s.json").write_text(json.dumps({"EnableHairHairColl": True}))
+    (tmp_path / "s.json").write_text(json.dumps({"SagFreeItr": 10}))
     r = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
                        capture_output=True, text=True)
-    assert r.returncode == 1 and "EnableHairHairColl" in r.stderr
+    assert r.returncode == 1 and "SagFreeItr" in r.stderr
+
+
+def test_hair_hair_settings(tmp_path):
+    g = synth.cantilever(2, 8)
+    write_hair(tmp_path / "hair.bin", g)
+    (tmp_path / "s.json").write_text(json.dumps({"EnableHairHairColl": True, "CurveRadius": 5e-5}))
+    out = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
+                         capture_output=True, text=True, check=True).stdout
+    d = json.loads(out)
+    assert d["hair_hair"] == 1 and d["step_limit"] == 1
+    assert d["barrier_thickness"] == pytest.approx(2 * 0.95 * 5e-5)  # StableCosseratRodsSolver.cpp:180
 
 
 @pytest.mark.gpu
