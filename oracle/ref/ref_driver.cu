@@ -19,6 +19,18 @@
 namespace YarnBall {
 extern std::shared_ptr<Sim> createFromCurves(std::vector<std::vector<glm::vec3>>& curves, std::vector<bool>& isCurveClosed,
                                              int numVerts);
+// the reference's step kernels (YarnBall/sim/{iteration,cosserat,collision}.cu), declared as
+// YBSimulator.cu:29-50 declares them
+extern __global__ void cosseratItr(MetaData* data);
+extern __global__ void quaternionLambdaItr(MetaData* data);
+extern __global__ void initItr(MetaData* data);
+extern __global__ void endItr(MetaData* data);
+template <bool USE_VEL_RADIUS>
+extern __global__ void buildCollisionList(MetaData* data, int maxCols, int* errorReturn);
+extern template __global__ void buildCollisionList<true>(MetaData* data, int maxCols, int* errorReturn);
+template <bool LIMIT, bool USE_VEL_RADIUS>
+extern __global__ void recomputeStepLimitKernel(MetaData* data);
+extern template __global__ void recomputeStepLimitKernel<true, true>(MetaData* data);
 }
 
 namespace {
@@ -97,9 +109,74 @@ int ref_set_state(void* h, const float* x, const float* v, const float* vlast, c
     return 0;
 }
 
+// One substep of the reference's hair-hair path with its own kernels, in Sim::advance's order
+// (step.cpp:44-58): initItr, detection, then the step graph (recomputeStepLimit, numItr x
+// (cosseratItr, quaternionLambdaItr), endItr), with the launch shapes of YBSimulator.cu:414-420.
+// Detection is buildCollisionList<true> (collision.cu:36-92) over every pair of segments instead of
+// the LBVH query's overlapping pairs: the distance test decides either way, and the LBVH as shipped
+// cannot run (LBVH::compute reads d_flags[0] before sizing it, KittenGpuLBVH/lbvh.cu:366-370).  Uses
+// useStepSizeLimit and useVelocityRadius, as StableCosseratRodsSolver sets them.  Returns the
+// reference's error word, or -1 when a CUDA call failed.
+int ref_step_hair_hair(void* h, float dt, float barrier) {
+    auto& sim = ((Holder*)h)->sim;
+    YarnBall::MetaData m = sim->meta;
+    const int nv = m.numVerts;
+    m.barrierThickness = barrier;
+    m.enableHairHairColl = true;
+    m.useStepSizeLimit = true;
+    m.useVelocityRadius = true;
+    m.detectionRadius = m.radius + 0.5f * m.barrierThickness;  // Sim::uploadMeta, YBSimulator.cu:323-324
+    m.scaledDetectionRadius = m.detectionRadius * m.detectionScaler;
+    m.lastH = m.h;
+    m.h = dt;
+    std::vector<glm::ivec2> pairs;
+    for (int i = 0; i < nv; i++)
+        for (int j = i + 1; j < nv; j++)
+            if ((sim->verts[i].flags & (uint32_t)YarnBall::VertexFlags::hasNext) &&
+                (sim->verts[j].flags & (uint32_t)YarnBall::VertexFlags::hasNext))
+                pairs.push_back(glm::ivec2(i, j));
+    YarnBall::MetaData* dm = nullptr;
+    glm::ivec2* dpairs = nullptr;
+    int* derr = nullptr;
+    int err[2] = {0, 0};
+    bool ok = !pairs.empty() && cudaMalloc(&dm, sizeof(m)) == cudaSuccess &&
+              cudaMalloc(&dpairs, sizeof(glm::ivec2) * pairs.size()) == cudaSuccess &&
+              cudaMalloc(&derr, 2 * sizeof(int)) == cudaSuccess;
+    if (ok) {
+        m.d_boundColList = dpairs;
+        ok = cudaMemcpy(dm, &m, sizeof(m), cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemcpy(dpairs, pairs.data(), sizeof(glm::ivec2) * pairs.size(), cudaMemcpyHostToDevice) == cudaSuccess &&
+             cudaMemset(derr, 0, 2 * sizeof(int)) == cudaSuccess && cudaMemset(m.d_numCols, 0, sizeof(int) * nv) == cudaSuccess;
+    }
+    if (ok) {
+        const int np = (int)pairs.size();
+        YarnBall::initItr<<<(nv + 255) / 256, 256>>>(dm);
+        YarnBall::buildCollisionList<true><<<(np + 127) / 128, 128>>>(dm, np, derr);
+        YarnBall::recomputeStepLimitKernel<true, true><<<(nv + 127) / 128, 128>>>(dm);
+        for (int it = 0; it < m.numItr; it++) {
+            YarnBall::cosseratItr<<<((nv - 1) + (VERTEX_PER_BLOCK - 1)) / (VERTEX_PER_BLOCK - 1), BLOCK_SIZE>>>(dm);
+            YarnBall::quaternionLambdaItr<<<(nv + 127) / 128, 128>>>(dm);
+        }
+        YarnBall::endItr<<<(nv + 255) / 256, 256>>>(dm);
+        ok = cudaDeviceSynchronize() == cudaSuccess && cudaMemcpy(err, derr, sizeof(err), cudaMemcpyDeviceToHost) == cudaSuccess;
+    }
+    if (dm) cudaFree(dm);
+    if (dpairs) cudaFree(dpairs);
+    if (derr) cudaFree(derr);
+    if (!ok) return -1;
+    sim->meta.lastH = m.lastH;
+    sim->meta.h = m.h;
+    sim->meta.time += dt;
+    return err[0];
+}
+
 int ref_advance(void* h, float dt) {
     auto& sim = ((Holder*)h)->sim;
-    sim->advance(dt);
+    try {
+        sim->advance(dt);
+    } catch (...) {
+        return 2;
+    }
     return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
 }
 

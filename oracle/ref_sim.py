@@ -30,6 +30,8 @@ def load():
         lib.ref_material.argtypes = [vp] + [vp] * 6
         lib.ref_set_state.argtypes = [vp] + [vp] * 5
         lib.ref_advance.argtypes = [vp, f32]
+        lib.ref_step_hair_hair.argtypes = [vp, f32, f32]
+        lib.ref_step_hair_hair.restype = ctypes.c_int
         lib.ref_download.argtypes = [vp, vp, vp, vp]
         lib.ref_sdf_project.argtypes = [i64, vp, vp, vp, vp, vp, vp, f32, vp, vp, vp, vp]
         for n in ("ref_material", "ref_set_state", "ref_advance", "ref_download", "ref_sdf_project"):
@@ -75,6 +77,14 @@ class RefSim:
         arrs = [np.ascontiguousarray(a, np.float32) for a in (x, v, v_last, q, clock)]
         if self.lib.ref_set_state(self.h, *[_p(a) for a in arrs]) != 0:
             raise RuntimeError("ref_set_state failed")
+
+    def step_hair_hair(self, dt, barrier_thickness):
+        """One substep of the reference's hair-hair path with its own kernels, detection over every
+        segment pair (the reference's LBVH cannot run as shipped); returns its error word."""
+        rc = self.lib.ref_step_hair_hair(self.h, dt, barrier_thickness)
+        if rc < 0:
+            raise RuntimeError("ref_step_hair_hair failed")
+        return rc
 
     def advance(self, dt):
         if self.lib.ref_advance(self.h, dt) != 0:

@@ -67,6 +67,54 @@ def test_jacobi_step_matches_reference_kernels(form):
     assert worst["oracle"] <= POS_TOL and worst["ours"] <= POS_TOL and worst["twist"] <= TWIST_TOL, worst
 
 
+def test_hair_hair_step_matches_reference_kernels():
+    """The reference's own hair-hair kernels (buildCollisionList's distance test and list
+    assembly, recomputeStepLimitKernel, cosseratItr's contact terms, in Sim::advance's order)
+    against the oracle's and this solver's Jacobi schedule with contacts, one step at a time from
+    shared states.  Two soft 16-vertex strands cross 60 um apart, the upper one pressing down.  The
+    reference's detection runs over every segment pair: its LBVH cannot run as shipped (LBVH::compute
+    reads d_flags[0] before sizing it, KittenGpuLBVH/lbvh.cu:366-370), and any broadphase that keeps
+    the overlapping boxes hands the same pairs to the distance test."""
+    g = synth.bar_and_drape(verts=16, gap=6e-5, bar_young=3e-5, drape_young=3e-5)
+    v0 = np.zeros((g.num_vertices, 3), np.float32)
+    v0[16:, 2] = -0.02
+    st = dict(num_itr=10, max_h=1 / 120, gravity=(0.0, 0.0, -2.0), radius=2e-6, schedule="jacobi", hair_hair=True,
+              barrier_thickness=7.6e-5)
+    o = helpers.oracle_sim(g, st, np.float32, v0)
+    free = helpers.oracle_sim(g, dict(st, hair_hair=False), np.float32, v0)
+    s = helpers.gpu_solver(g, st, form="sweep")
+    refs = [ref_sim.RefSim(g, young=3e-5, radius=2e-6, num_itr=10, max_h=1 / 120, gravity=(0.0, 0.0, -2.0))
+            for _ in range(2)]
+    worst = dict(oracle=0.0, ours=0.0, spread=0.0, twist=0.0, contact_effect=0.0)
+    for _ in range(6):
+        state = (o.x.copy(), o.v.copy(), o.v_last.copy(), o.q.copy(), o.clock.copy())
+        outs = []
+        for r in refs:
+            r.set_state(*state[:4], state[4][:3])
+            assert r.step_hair_hair(1 / 120, 7.6e-5) == 0  # no MAX_COLLISIONS_PER_SEGMENT overflow
+            outs.append(r.download())
+        counter = np.array([int(o.clock[3])], np.uint32).view(np.float32)[0]
+        s.set_state(np.concatenate([a.ravel() for a in state[:4]] +
+                                   [np.array([o.clock[0], o.clock[1], o.clock[2], counter], np.float32)]).astype(np.float32))
+        free.load_state(o.state())
+        o.advance(1 / 120)
+        free.advance(1 / 120)
+        s.step(1 / 120)
+        (x0, _, q0), (x1, _, _) = outs
+        xs, _ = s.get_positions_velocities()
+        worst["spread"] = max(worst["spread"], float(np.abs(x0 - x1).max()))
+        worst["oracle"] = max(worst["oracle"], float(np.abs(o.x - x0).max()))
+        worst["ours"] = max(worst["ours"], float(np.abs(xs - x0).max()))
+        worst["twist"] = max(worst["twist"], float(np.abs(orc.twist_angles(q0, s.get_orientations())).max()))
+        worst["contact_effect"] = max(worst["contact_effect"], float(np.abs(free.x - o.x).max()))
+    for r in refs:
+        r.close()
+    s.close()
+    print("hair-hair reference pin", worst)
+    assert worst["contact_effect"] > 3e-5  # the contacts move the strands in these steps
+    assert worst["oracle"] <= POS_TOL and worst["ours"] <= POS_TOL and worst["twist"] <= TWIST_TOL, worst
+
+
 def test_sdf_pass_matches_reference_kernel():
     rng = np.random.default_rng(4)
     for sdf, rot, tr in ((synth.sphere_sdf(64), (0.0, 0.0, 0.0, 1.0), (0.0, 0.0, 0.0)),
