@@ -34,8 +34,9 @@ typedef enum kami_status {
     KAMI_ERR_UNSUPPORTED = 6,      /* request outside what this build supports (e.g. strand longer than a tile) */
     KAMI_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
     KAMI_ERR_STATE = 8,            /* call made in the wrong order (e.g. backward without a recorded forward) */
-    KAMI_ERR_CONTACTS = 9          /* a segment had more than 16 hair-hair contacts (MAX_COLLISIONS_PER_SEGMENT,
+    KAMI_ERR_CONTACTS = 9,         /* a segment had more than 16 hair-hair contacts (MAX_COLLISIONS_PER_SEGMENT,
                                       YarnBall.h:19; Sim::checkErrors throws there, YBSimulator.cu:396-398) */
+    KAMI_ERR_IO = 10               /* a file could not be opened, read or written, or is not a USC .data file */
 } kami_status;
 
 /* Gauss-Seidel order of the position and orientation sweeps. */
@@ -184,6 +185,32 @@ kami_status kami_vbd_get_positions_velocities(kami_vbd_handle h, float* xyz, flo
 
 /* Segment orientations (4*V floats, x y z w per vertex; the tip copies its previous segment).
  * Replaces: the qs part of Sim::download (YBSimulator.cu:355-360). */
+/* Device-resident Hair.  KamiSimulator's Hair keeps positions and velocities in padded
+ * [strand][vertex] arrays: xyz of Hair strand u, vertex v at (u * max_verts + v) * 3
+ * (EigenVecX3f2DArray, LinearUtil.cpp:159, :247-253).  kami_vbd_set_hair_layout tells the solver
+ * which Hair strand each of its strands is (strand_refs[s], NULL = identity; strands of fewer than 4
+ * vertices are not in the solver, StableCosseratRodsSolver.cpp:134-136).  Then
+ * kami_vbd_upload_hair / kami_vbd_download_hair replace UploadHair / DownloadHair
+ * (StableCosseratRodsSolver.cpp:238-277) with one gather/scatter kernel over the padded arrays:
+ * with device arrays nothing crosses PCIe; with host arrays each array is copied whole (download
+ * copies it in and out, so the entries the solver does not own keep their values). */
+kami_status kami_vbd_set_hair_layout(kami_vbd_handle h, int32_t hair_strands, int32_t max_verts,
+                                     const int32_t* strand_refs);
+kami_status kami_vbd_upload_hair(kami_vbd_handle h, const float* xyz, const float* vxyz, int32_t memory);
+kami_status kami_vbd_download_hair(kami_vbd_handle h, float* xyz, float* vxyz, int32_t memory);
+
+/* USC-HairSalon .data files (importers/USCHairsalonImporter.cpp:56-80, exporters/
+ * USCHairsalonExporter.cpp:6-18): uint32 strand count, then per strand a uint32 vertex count and
+ * that many float xyz triples.  kami_usc_info reads the strand table.  kami_usc_read fills
+ * strand_vert_count[num_strands] and xyz, packed in strand order (max_verts = 0) or padded to
+ * [strand][max_verts] like the Hair arrays (the reference's full import uses 100).  kami_usc_write
+ * writes the same layouts; unlike ExportUSCHairCore it takes the full path (no ".data" appended).
+ * Malformed or truncated files return KAMI_ERR_IO. */
+kami_status kami_usc_info(const char* path, int32_t* num_strands, int64_t* num_vertices, int32_t* max_strand_verts);
+kami_status kami_usc_read(const char* path, int32_t max_verts, int32_t* strand_vert_count, float* xyz);
+kami_status kami_usc_write(const char* path, int32_t num_strands, const int32_t* strand_vert_count, int32_t max_verts,
+                           const float* xyz);
+
 kami_status kami_vbd_get_orientations(kami_vbd_handle h, float* xyzw, int32_t memory);
 kami_status kami_vbd_set_orientations(kami_vbd_handle h, const float* xyzw, int32_t memory);
 

@@ -103,6 +103,12 @@ struct kami_vbd_solver {
     float4* d_snap = nullptr;
     std::vector<char> graph_detect;  // substeps of the cached sweep graph that run detection
 
+    // device-resident Hair: padded entry of each boundary vertex, and a staging copy of a padded
+    // array for host transfers
+    int64_t* d_hair_index = nullptr;
+    float* d_hair_stage = nullptr;
+    int64_t hair_entries = 0;  // Hair strands x max_verts
+
     // differentiable stepping: the tape of recorded steps and the adjoint state
     int tape_capacity = 0;
     int64_t tape_tiles = 0;               // tiles the tape holds per step
@@ -162,7 +168,7 @@ void release(kami_vbd_solver* h) {
     const CollParams& c = h->cp;
     void* cptrs[] = {(void*)c.vid, (void*)c.gid, c.cols,   c.ncols,  c.maxstep,  c.bmin,    c.bmax,
                      c.cell,       c.count,      c.start,  c.cursor, c.sorted,   c.ext_bits, c.scan_tmp,
-                     h->d_snap};
+                     h->d_snap,    h->d_hair_index, h->d_hair_stage};
     for (void* p : cptrs)
         if (p) cudaFree(p);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
@@ -1229,6 +1235,82 @@ kami_status kami_vbd_zero_rest_darboux_grad(kami_vbd_handle h) {
     if (!h->d_gqr) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
     KAMI_CUDA(cudaMemsetAsync(h->d_gqr, 0, sizeof(float4) * h->layout.num_slots, h->stream), "gradient reset");
     return KAMI_OK;
+}
+
+kami_status kami_vbd_set_hair_layout(kami_vbd_handle h, int32_t hair_strands, int32_t max_verts,
+                                     const int32_t* strand_refs) {
+    KAMI_TRY(valid_handle(h));
+    if (hair_strands <= 0 || max_verts <= 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "hair_strands and max_verts must be > 0");
+    std::vector<char> used(hair_strands, 0);
+    std::vector<int64_t> index(h->nv);
+    for (int32_t s = 0; s < h->ns; s++) {
+        const int32_t u = strand_refs ? strand_refs[s] : s;
+        if (u < 0 || u >= hair_strands) return fail(KAMI_ERR_INVALID_ARGUMENT, "strand_refs[%d] = %d is not a Hair strand", s, u);
+        if (used[u]) return fail(KAMI_ERR_INVALID_ARGUMENT, "Hair strand %d is referenced twice", u);
+        used[u] = 1;
+        const int32_t len = h->strand_begin[s + 1] - h->strand_begin[s];
+        if (len > max_verts)
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "strand %d has %d vertices, more than max_verts = %d", s, len, max_verts);
+        for (int32_t v = 0; v < len; v++) index[h->strand_begin[s] + v] = (int64_t)u * max_verts + v;
+    }
+    KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    if (h->d_hair_index) cudaFree(h->d_hair_index);
+    if (h->d_hair_stage) cudaFree(h->d_hair_stage);
+    h->d_hair_index = nullptr;
+    h->d_hair_stage = nullptr;
+    h->hair_entries = 0;
+    KAMI_CUDA(dalloc(&h->d_hair_index, h->nv), "Hair layout");
+    KAMI_CUDA(cudaMemcpy(h->d_hair_index, index.data(), sizeof(int64_t) * h->nv, cudaMemcpyHostToDevice), "Hair layout");
+    h->hair_entries = (int64_t)hair_strands * max_verts;
+    return KAMI_OK;
+}
+
+static kami_status hair_stage(kami_vbd_solver* h) {
+    if (!h->d_hair_stage) KAMI_CUDA(dalloc(&h->d_hair_stage, 3 * h->hair_entries), "Hair staging buffer");
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_upload_hair(kami_vbd_handle h, const float* xyz, const float* vxyz, int32_t memory) {
+    KAMI_TRY(valid_handle(h));
+    if (!h->d_hair_index) return fail(KAMI_ERR_STATE, "call kami_vbd_set_hair_layout first");
+    if (memory != KAMI_MEMORY_HOST && memory != KAMI_MEMORY_DEVICE) return fail(KAMI_ERR_INVALID_ARGUMENT, "bad memory kind");
+    const float* srcs[2] = {xyz, vxyz};
+    float4* dsts[2] = {h->d_xm, h->d_vel};
+    const size_t bytes = sizeof(float) * 3 * h->hair_entries;
+    for (int a = 0; a < 2; a++) {
+        if (!srcs[a]) continue;
+        const float* src = srcs[a];
+        if (memory == KAMI_MEMORY_HOST) {
+            KAMI_TRY(hair_stage(h));
+            KAMI_CUDA(cudaMemcpyAsync(h->d_hair_stage, src, bytes, cudaMemcpyHostToDevice, h->stream), "Hair copy in");
+            src = h->d_hair_stage;
+        }
+        KAMI_CUDA(launch_hair_in(src, dsts[a], h->d_slot_of, h->d_hair_index, h->nv, h->stream), "Hair scatter");
+    }
+    if (memory == KAMI_MEMORY_HOST) KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_download_hair(kami_vbd_handle h, float* xyz, float* vxyz, int32_t memory) {
+    KAMI_TRY(valid_handle(h));
+    if (!h->d_hair_index) return fail(KAMI_ERR_STATE, "call kami_vbd_set_hair_layout first");
+    if (memory != KAMI_MEMORY_HOST && memory != KAMI_MEMORY_DEVICE) return fail(KAMI_ERR_INVALID_ARGUMENT, "bad memory kind");
+    float* dsts[2] = {xyz, vxyz};
+    const float4* srcs[2] = {h->d_xm, h->d_vel};
+    const size_t bytes = sizeof(float) * 3 * h->hair_entries;
+    for (int a = 0; a < 2; a++) {
+        if (!dsts[a]) continue;
+        if (memory == KAMI_MEMORY_DEVICE) {
+            KAMI_CUDA(launch_hair_out(srcs[a], dsts[a], h->d_slot_of, h->d_hair_index, h->nv, h->stream), "Hair gather");
+        } else {
+            // the padded entries the solver does not own (skipped strands, padding) keep their values
+            KAMI_TRY(hair_stage(h));
+            KAMI_CUDA(cudaMemcpyAsync(h->d_hair_stage, dsts[a], bytes, cudaMemcpyHostToDevice, h->stream), "Hair copy in");
+            KAMI_CUDA(launch_hair_out(srcs[a], h->d_hair_stage, h->d_slot_of, h->d_hair_index, h->nv, h->stream), "Hair gather");
+            KAMI_CUDA(cudaMemcpyAsync(dsts[a], h->d_hair_stage, bytes, cudaMemcpyDeviceToHost, h->stream), "Hair copy out");
+        }
+    }
+    return check_status_word(h);
 }
 
 kami_status kami_vbd_synchronize(kami_vbd_handle h) {

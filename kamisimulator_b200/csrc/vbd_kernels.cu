@@ -256,6 +256,41 @@ cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const
     return cudaErrorInvalidValue;
 }
 
+// KamiSimulator's padded Hair arrays (xyz of Hair strand u, vertex v at (u * max_verts + v) * 3,
+// LinearUtil.cpp:159, :247-253) <-> tile slots; hair_index[i] is the padded entry of boundary vertex i.
+__global__ void hair_in_kernel(const float* __restrict__ src, float4* __restrict__ dst, const int64_t* __restrict__ slot_of,
+                               const int64_t* __restrict__ hair_index, int64_t nv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const int64_t p = hair_index[i];
+    float4* d = dst + slot_of[i];
+    const float4 o = *d;
+    *d = make_float4(src[3 * p], src[3 * p + 1], src[3 * p + 2], o.w);
+}
+__global__ void hair_out_kernel(const float4* __restrict__ src, float* __restrict__ dst, const int64_t* __restrict__ slot_of,
+                                const int64_t* __restrict__ hair_index, int64_t nv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
+    const int64_t p = hair_index[i];
+    const float4 a = src[slot_of[i]];
+    dst[3 * p] = a.x;
+    dst[3 * p + 1] = a.y;
+    dst[3 * p + 2] = a.z;
+}
+
+cudaError_t launch_hair_in(const float* src, float4* dst, const int64_t* slot_of, const int64_t* hair_index, int64_t nv,
+                           cudaStream_t s) {
+    if (nv == 0) return cudaSuccess;
+    hair_in_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, hair_index, nv);
+    return cudaGetLastError();
+}
+cudaError_t launch_hair_out(const float4* src, float* dst, const int64_t* slot_of, const int64_t* hair_index, int64_t nv,
+                            cudaStream_t s) {
+    if (nv == 0) return cudaSuccess;
+    hair_out_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, hair_index, nv);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
     if (nv == 0) return cudaSuccess;
     scatter3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);

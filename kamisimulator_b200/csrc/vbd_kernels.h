@@ -38,6 +38,12 @@ cudaError_t launch_sweep_position_coll(const DeviceState& st, const float4* y4, 
                                        float4* dx_out, const float4* snap, const StepParams* d_sp, const PhysParams& pp,
                                        const CollParams& cp, int colour, bool jacobi, cudaStream_t s);
 
+// padded Hair arrays <-> tile slots (hair_index: padded entry of each boundary vertex)
+cudaError_t launch_hair_in(const float* src, float4* dst, const int64_t* slot_of, const int64_t* hair_index, int64_t nv,
+                           cudaStream_t s);
+cudaError_t launch_hair_out(const float4* src, float* dst, const int64_t* slot_of, const int64_t* hair_index, int64_t nv,
+                            cudaStream_t s);
+
 cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
 cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
 cudaError_t launch_scatter4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);

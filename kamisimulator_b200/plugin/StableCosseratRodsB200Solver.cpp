@@ -149,37 +149,22 @@ void StableCosseratRodsB200Solver::Construct(const std::string& settingJsonPath)
     if (handle_) kami_vbd_destroy(handle_);
     handle_ = nullptr;
     check(kami_vbd_create(&d, &handle_), "Construct");
+    // the Hair's padded arrays are read and written in place, through the strandRefs mapping
+    check(kami_vbd_set_hair_layout(handle_, (int32_t)hair_->num_strands, (int32_t)hair_->max_verts, strand_refs_.data()),
+          "Construct");
 }
 
 void StableCosseratRodsB200Solver::SolveNextStep(float dt) { check(kami_vbd_step(handle_, dt, nullptr), "SolveNextStep"); }
 
-// Sim -> Hair (StableCosseratRodsSolver.cpp:258-277)
+// Sim -> Hair (StableCosseratRodsSolver.cpp:258-277): one gather on the GPU into the padded arrays
 void StableCosseratRodsB200Solver::DownloadHair() {
-    check(kami_vbd_get_positions_velocities(handle_, packed_pos_.data(), packed_vel_.data(), KAMI_MEMORY_HOST),
+    check(kami_vbd_download_hair(handle_, hair_->positions.data(), hair_->velocities.data(), KAMI_MEMORY_HOST),
           "DownloadHair");
-    Hair& hair = *hair_;
-    for (size_t i = 0; i < strand_refs_.size(); i++) {
-        const uint32_t s = (uint32_t)strand_refs_[i];
-        for (int32_t v = 0; v < strand_begin_[i + 1] - strand_begin_[i]; v++)
-            for (int a = 0; a < 3; a++) {
-                hair.pos(s, v)[a] = packed_pos_[3 * (strand_begin_[i] + v) + a];
-                hair.vel(s, v)[a] = packed_vel_[3 * (strand_begin_[i] + v) + a];
-            }
-    }
 }
 
 // Hair -> Sim (StableCosseratRodsSolver.cpp:238-256)
 void StableCosseratRodsB200Solver::UploadHair() {
-    Hair& hair = *hair_;
-    for (size_t i = 0; i < strand_refs_.size(); i++) {
-        const uint32_t s = (uint32_t)strand_refs_[i];
-        for (int32_t v = 0; v < strand_begin_[i + 1] - strand_begin_[i]; v++)
-            for (int a = 0; a < 3; a++) {
-                packed_pos_[3 * (strand_begin_[i] + v) + a] = hair.pos(s, v)[a];
-                packed_vel_[3 * (strand_begin_[i] + v) + a] = hair.vel(s, v)[a];
-            }
-    }
-    check(kami_vbd_set_positions_velocities(handle_, packed_pos_.data(), packed_vel_.data(), KAMI_MEMORY_HOST),
+    check(kami_vbd_upload_hair(handle_, hair_->positions.data(), hair_->velocities.data(), KAMI_MEMORY_HOST),
           "UploadHair");
 }
 

@@ -4,8 +4,11 @@
 //   kami_solver_driver settings.json hair.bin steps dt out.bin [sdf.bin]
 //   kami_solver_driver --dry-run settings.json hair.bin        (prints the descriptor, no device)
 //
-// hair.bin: uint32 strands, uint32 max_verts, uint32 counts[strands], float positions[strands][max_verts][3]
-// out.bin:  float positions[strands][max_verts][3], float velocities[...]
+// hair.bin: uint32 strands, uint32 max_verts, uint32 counts[strands], float positions[strands][max_verts][3],
+//           or a USC-HairSalon .data file (read into a Hair of 100 vertices per strand, as
+//           ImportUSCHairSalonToHair does, importers/USCHairsalonImporter.cpp:56-80)
+// out.bin:  float positions[strands][max_verts][3], float velocities[...], or a .data file of the
+//           final positions (ExportHairAsUSCHairsalon, exporters/USCHairsalonExporter.cpp:20-26)
 // sdf.bin:  int32 dims[3], float min[3], float max[3], float phi[n], float grad[3n]
 #include <cstdio>
 #include <cstring>
@@ -17,7 +20,27 @@
 
 using namespace kami;
 
+static bool is_usc(const char* path) {
+    const size_t n = std::strlen(path);
+    return n > 5 && std::strcmp(path + n - 5, ".data") == 0;
+}
+
 static std::shared_ptr<Hair> read_hair(const char* path) {
+    if (is_usc(path)) {
+        int32_t ns = 0, mx = 0;
+        int64_t nv = 0;
+        if (kami_usc_info(path, &ns, &nv, &mx) != KAMI_OK) throw std::runtime_error(kami_vbd_last_error_string());
+        auto h = std::make_shared<Hair>();
+        h->num_strands = (uint32_t)ns;
+        h->max_verts = 100;
+        std::vector<int32_t> counts(ns);
+        h->positions.assign((size_t)ns * h->max_verts * 3, 0.f);
+        if (kami_usc_read(path, (int32_t)h->max_verts, counts.data(), h->positions.data()) != KAMI_OK)
+            throw std::runtime_error(kami_vbd_last_error_string());
+        h->strand_vert_count.assign(counts.begin(), counts.end());
+        h->velocities.assign(h->positions.size(), 0.f);
+        return h;
+    }
     std::ifstream f(path, std::ios::binary);
     if (!f) throw std::runtime_error("cannot open hair file");
     auto h = std::make_shared<Hair>();
@@ -75,9 +98,16 @@ int main(int argc, char** argv) {
             s.SolveNextStep(dt);
             s.DownloadHair();
         }
-        std::ofstream o(argv[5], std::ios::binary);
-        o.write((const char*)hair->positions.data(), 4 * hair->positions.size());
-        o.write((const char*)hair->velocities.data(), 4 * hair->velocities.size());
+        if (is_usc(argv[5])) {
+            std::vector<int32_t> counts(hair->strand_vert_count.begin(), hair->strand_vert_count.end());
+            if (kami_usc_write(argv[5], (int32_t)hair->num_strands, counts.data(), (int32_t)hair->max_verts,
+                               hair->positions.data()) != KAMI_OK)
+                throw std::runtime_error(kami_vbd_last_error_string());
+        } else {
+            std::ofstream o(argv[5], std::ios::binary);
+            o.write((const char*)hair->positions.data(), 4 * hair->positions.size());
+            o.write((const char*)hair->velocities.data(), 4 * hair->velocities.size());
+        }
         std::cout << s.GetInfoString().substr(0, 80) << std::endl;
         return 0;
     } catch (const std::exception& e) {

@@ -20,7 +20,7 @@ LIB_PATH = os.path.join(_HERE, "lib", "libkami_vbd.so")
 KAMI_OK = 0
 STATUS_NAMES = {0: "KAMI_OK", 1: "KAMI_ERR_INVALID_ARGUMENT", 2: "KAMI_ERR_CUDA", 3: "KAMI_ERR_OUT_OF_MEMORY",
                 4: "KAMI_ERR_NONFINITE", 5: "KAMI_ERR_GEOMETRY", 6: "KAMI_ERR_UNSUPPORTED", 7: "KAMI_ERR_TIMEOUT",
-                8: "KAMI_ERR_STATE", 9: "KAMI_ERR_CONTACTS"}
+                8: "KAMI_ERR_STATE", 9: "KAMI_ERR_CONTACTS", 10: "KAMI_ERR_IO"}
 SCHEDULES = {"colour2": 0, "jacobi": 1}
 FORMS = {"auto": 0, "sweep": 1, "fused": 2}
 MEM_HOST, MEM_DEVICE = 0, 1
@@ -35,7 +35,8 @@ EXPORTED = [
     "kami_vbd_step_n", "kami_vbd_set_tuning", "kami_vbd_get_tuning", "kami_vbd_autotune",
     "kami_vbd_tape_reserve", "kami_vbd_get_tile_count", "kami_vbd_set_tape_window", "kami_vbd_step_record", "kami_vbd_backward", "kami_vbd_get_rest_darboux_grad",
     "kami_vbd_zero_rest_darboux_grad", "kami_vbd_batch_create", "kami_vbd_batch_count", "kami_vbd_batch_groom_range",
-    "kami_vbd_batch_step",
+    "kami_vbd_batch_step", "kami_vbd_set_hair_layout", "kami_vbd_upload_hair", "kami_vbd_download_hair",
+    "kami_usc_info", "kami_usc_read", "kami_usc_write",
 ]
 
 
@@ -116,6 +117,12 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_batch_groom_range": [vp, i32, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i64),
                                        ctypes.POINTER(i64)],
         "kami_vbd_batch_step": [vp, f32, i32, vp, vp],
+        "kami_vbd_set_hair_layout": [vp, i32, i32, vp],
+        "kami_vbd_upload_hair": [vp, vp, vp, i32],
+        "kami_vbd_download_hair": [vp, vp, vp, i32],
+        "kami_usc_info": [ctypes.c_char_p, ctypes.POINTER(i32), ctypes.POINTER(i64), ctypes.POINTER(i32)],
+        "kami_usc_read": [ctypes.c_char_p, i32, vp, vp],
+        "kami_usc_write": [ctypes.c_char_p, i32, vp, i32, vp],
         "kami_vbd_destroy": [vp],
         "kami_vbd_get_sizes": [vp, ctypes.POINTER(i64), ctypes.POINTER(i32), ctypes.POINTER(i32)],
         "kami_vbd_set_positions_velocities": [vp, vp, vp, i32],
@@ -268,6 +275,29 @@ class Solver:
         _check(self.lib.kami_vbd_batch_groom_range(self._h, groom, ctypes.byref(s0), ctypes.byref(ns),
                                                    ctypes.byref(v0), ctypes.byref(nv)))
         return s0.value, ns.value, v0.value, nv.value
+
+    def set_hair_layout(self, hair_strands, max_verts, strand_refs=None):
+        """The padded Hair arrays ([hair_strands][max_verts] xyz) the solver reads and writes;
+        strand_refs[s]: the Hair strand of solver strand s (None: the identity)."""
+        refs = None if strand_refs is None else np.ascontiguousarray(strand_refs, np.int32)
+        _check(self.lib.kami_vbd_set_hair_layout(self._h, hair_strands, max_verts,
+                                                 None if refs is None else refs.ctypes.data_as(ctypes.c_void_p)))
+
+    def upload_hair(self, x=None, v=None):
+        """UploadHair from padded arrays (numpy host arrays or torch CUDA tensors)."""
+        if x is not None and not hasattr(x, "data_ptr"):
+            x = _f32(x)
+        if v is not None and not hasattr(v, "data_ptr"):
+            v = _f32(v)
+        px, mx = _ptr(x)
+        pv, mv = _ptr(v)
+        _check(self.lib.kami_vbd_upload_hair(self._h, px, pv, mx if x is not None else mv))
+
+    def download_hair(self, x=None, v=None):
+        """DownloadHair into padded arrays, in place (entries the solver does not own are kept)."""
+        px, mx = _ptr(x)
+        pv, mv = _ptr(v)
+        _check(self.lib.kami_vbd_download_hair(self._h, px, pv, mx if x is not None else mv))
 
     def batch_step(self, dt, n, body_transforms=None, stream=None):
         """kami_vbd_batch_step: every groom of the handle, n steps."""
@@ -447,3 +477,26 @@ class Solver:
 
 def version():
     return load_library().kami_vbd_version().decode()
+
+
+def read_usc(path, max_verts=0):
+    """A USC-HairSalon .data file: (vertex count per strand int32 [S], xyz float32) with xyz packed
+    [V, 3] (max_verts = 0) or padded [S, max_verts, 3] like KamiSimulator's Hair arrays."""
+    lib = load_library()
+    ns, nv, mx = ctypes.c_int32(), ctypes.c_int64(), ctypes.c_int32()
+    _check(lib.kami_usc_info(os.fsencode(path), ctypes.byref(ns), ctypes.byref(nv), ctypes.byref(mx)))
+    counts = np.zeros(ns.value, np.int32)
+    shape = (ns.value, max_verts, 3) if max_verts > 0 else (nv.value, 3)
+    xyz = np.zeros(shape, np.float32)
+    _check(lib.kami_usc_read(os.fsencode(path), max_verts, counts.ctypes.data_as(ctypes.c_void_p),
+                             xyz.ctypes.data_as(ctypes.c_void_p)))
+    return counts, xyz
+
+
+def write_usc(path, counts, xyz, max_verts=0):
+    """Writes a USC-HairSalon .data file from packed ([V, 3]) or padded ([S, max_verts, 3]) xyz."""
+    lib = load_library()
+    c = np.ascontiguousarray(counts, np.int32)
+    a = np.ascontiguousarray(xyz, np.float32)
+    _check(lib.kami_usc_write(os.fsencode(path), c.shape[0], c.ctypes.data_as(ctypes.c_void_p), max_verts,
+                              a.ctypes.data_as(ctypes.c_void_p)))

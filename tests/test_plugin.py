@@ -109,3 +109,30 @@ def test_plugin_steps_match_the_c_abi_and_the_oracle(tmp_path):
     np.testing.assert_allclose(packed, x, atol=1e-6)
     assert np.abs(packed - o.x).max() <= helpers.POS_TOL
     assert np.abs(packed - g.positions).max() > 1e-4  # the strands moved
+
+
+@pytest.mark.gpu
+def test_plugin_reads_and_writes_usc_data_files(tmp_path):
+    """The driver loads a USC-HairSalon .data file into a Hair of 100 vertices per strand (skipping
+    strands under 4 vertices), steps it, and exports the Hair as .data: the same result as the
+    binary Hair path."""
+    from kamisimulator_b200 import vbd
+
+    g = helpers.soft_groom(30, (2, 40), seed=14)
+    counts = np.diff(g.strand_begin).astype(np.int32)
+    vbd.write_usc(tmp_path / "in.data", counts, g.positions)
+    write_hair(tmp_path / "hair.bin", g, pad_to=100)
+    settings = {"NumItr": 6, "UseYoungsModule": True, "YoungsModule": 1e-4, "CurveRadius": 40e-6 / 0.05,
+                "WindPeak": 0, "EnableSDF": False, "MaxTimeStep": 1 / 60, "Gravity": [0.3, -0.4, -9.81]}
+    (tmp_path / "s.json").write_text(json.dumps(settings))
+    for src, dst in (("in.data", "out.data"), ("hair.bin", "out.bin")):
+        subprocess.run([DRIVER, str(tmp_path / "s.json"), str(tmp_path / src), "4", str(1 / 60), str(tmp_path / dst)],
+                       check=True, capture_output=True)
+    c, xd = vbd.read_usc(tmp_path / "out.data", max_verts=100)
+    xb, _ = read_out(tmp_path / "out.bin", g.num_strands, 100)
+    np.testing.assert_array_equal(c, counts)
+    for s in range(g.num_strands):
+        np.testing.assert_array_equal(xd[s, :counts[s]], xb[s, :counts[s]])
+    moved = [s for s in range(g.num_strands) if counts[s] >= 4]
+    assert max(np.abs(xd[s, :counts[s]] - g.positions[g.strand_begin[s]:g.strand_begin[s + 1]]).max()
+               for s in moved) > 1e-4
