@@ -199,6 +199,20 @@ kami_status kami_vbd_set_hair_layout(kami_vbd_handle h, int32_t hair_strands, in
 kami_status kami_vbd_upload_hair(kami_vbd_handle h, const float* xyz, const float* vxyz, int32_t memory);
 kami_status kami_vbd_download_hair(kami_vbd_handle h, float* xyz, float* vxyz, int32_t memory);
 
+/* Body SDF grid baked from a closed, consistently wound triangle mesh on the GPU.  Replaces the
+ * CPU bake of PNMesh::GenerateSDF + StoreSDFQueries (PNMesh.cpp:100-173; Discregrid in
+ * utilities/Geometry.cpp:5-35).  Node (i, j, k) sits at grid_min + ds (i, j, k), ds = (grid_max -
+ * grid_min) / dims, x fastest, as kami_vbd_sdf_desc expects.  phi: the exact signed distance to the
+ * mesh (negative inside; sign by the angle-weighted pseudonormal of the nearest feature, as
+ * Discregrid's TriangleMeshDistance decides it) -- the function the reference's cubic Lagrange grid
+ * approximates.  grad (3 per node): inside, the unit gradient of the distance; elsewhere the unit
+ * direction from the grid centre, StoreSDFQueries' choice for nodes at distance >= 0 (zero at a
+ * node exactly at the centre).  The reference samples its grid over the mesh's bounding box.
+ * memory: phi/grad in host or device memory; device: CUDA ordinal, -1 = current. */
+kami_status kami_sdf_bake(const float* vertices, int32_t num_vertices, const int32_t* triangles, int32_t num_triangles,
+                          const int32_t dims[3], const float grid_min[3], const float grid_max[3], float* phi,
+                          float* grad, int32_t memory, int32_t device);
+
 /* USC-HairSalon .data files (importers/USCHairsalonImporter.cpp:56-80, exporters/
  * USCHairsalonExporter.cpp:6-18): uint32 strand count, then per strand a uint32 vertex count and
  * that many float xyz triples.  kami_usc_info reads the strand table.  kami_usc_read fills

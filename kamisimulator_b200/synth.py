@@ -207,6 +207,61 @@ def contact_fence(num_posts: int = 20, spacing: float = 3e-5, verts: int = 8, se
                  strand_young=np.full(n, 1.0, np.float32), strand_dev=np.ones(n, np.float32))
 
 
+# ---- body meshes for the SDF bake ----------------------------------------------------------------
+
+def icosphere(subdivisions: int = 3, radius: float = 0.09, centre=(0.0, 0.0, 0.0)):
+    """Closed triangle mesh of a sphere (vertices float32 [V, 3], triangles int32 [T, 3], outward
+    counter-clockwise winding)."""
+    t = (1.0 + 5.0 ** 0.5) / 2.0
+    v = [(-1, t, 0), (1, t, 0), (-1, -t, 0), (1, -t, 0), (0, -1, t), (0, 1, t), (0, -1, -t), (0, 1, -t),
+         (t, 0, -1), (t, 0, 1), (-t, 0, -1), (-t, 0, 1)]
+    f = [(0, 11, 5), (0, 5, 1), (0, 1, 7), (0, 7, 10), (0, 10, 11), (1, 5, 9), (5, 11, 4), (11, 10, 2), (10, 7, 6),
+         (7, 1, 8), (3, 9, 4), (3, 4, 2), (3, 2, 6), (3, 6, 8), (3, 8, 9), (4, 9, 5), (2, 4, 11), (6, 2, 10),
+         (8, 6, 7), (9, 8, 1)]
+    verts = [np.array(p, np.float64) / np.linalg.norm(p) for p in v]
+    for _ in range(subdivisions):
+        cache, nf = {}, []
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = verts[a] + verts[b]
+                verts.append(m / np.linalg.norm(m))
+                cache[key] = len(verts) - 1
+            return cache[key]
+
+        for a, b, c in f:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [(a, ab, ca), (b, bc, ab), (c, ca, bc), (ab, bc, ca)]
+        f = nf
+    V = np.asarray(verts) * radius + np.asarray(centre)
+    return V.astype(np.float32), np.asarray(f, np.int32)
+
+
+def torus(major: float = 0.06, minor: float = 0.025, n_major: int = 32, n_minor: int = 16, centre=(0.0, 0.0, 0.0)):
+    """Closed, non-convex triangle mesh of a torus around the z axis (outward winding)."""
+    u = np.arange(n_major) * 2 * np.pi / n_major
+    w = np.arange(n_minor) * 2 * np.pi / n_minor
+    U, W = np.meshgrid(u, w, indexing="ij")
+    x = (major + minor * np.cos(W)) * np.cos(U)
+    y = (major + minor * np.cos(W)) * np.sin(U)
+    z = minor * np.sin(W)
+    V = np.stack([x, y, z], -1).reshape(-1, 3) + np.asarray(centre)
+    tris = []
+    for i in range(n_major):
+        for j in range(n_minor):
+            a, b = i * n_minor + j, ((i + 1) % n_major) * n_minor + j
+            c, d = ((i + 1) % n_major) * n_minor + (j + 1) % n_minor, i * n_minor + (j + 1) % n_minor
+            tris += [(a, b, c), (a, c, d)]
+    return V.astype(np.float32), np.asarray(tris, np.int32)
+
+
+def mesh_bounds(vertices):
+    """The mesh's bounding box: the grid StoreSDFQueries samples (PNMesh.cpp:117-121)."""
+    v = np.asarray(vertices, np.float32)
+    return tuple(float(a) for a in v.min(0)), tuple(float(a) for a in v.max(0))
+
+
 def sphere_sdf(n: int = 128, radius: float = 0.09, half_extent: float = 0.2, threshold: float = 1e-3) -> SDFGrid:
     dims = (n, n, n)
     gmin = (-half_extent,) * 3

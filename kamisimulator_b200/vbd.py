@@ -36,7 +36,7 @@ EXPORTED = [
     "kami_vbd_tape_reserve", "kami_vbd_get_tile_count", "kami_vbd_set_tape_window", "kami_vbd_step_record", "kami_vbd_backward", "kami_vbd_get_rest_darboux_grad",
     "kami_vbd_zero_rest_darboux_grad", "kami_vbd_batch_create", "kami_vbd_batch_count", "kami_vbd_batch_groom_range",
     "kami_vbd_batch_step", "kami_vbd_set_hair_layout", "kami_vbd_upload_hair", "kami_vbd_download_hair",
-    "kami_usc_info", "kami_usc_read", "kami_usc_write",
+    "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake",
 ]
 
 
@@ -120,6 +120,7 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_set_hair_layout": [vp, i32, i32, vp],
         "kami_vbd_upload_hair": [vp, vp, vp, i32],
         "kami_vbd_download_hair": [vp, vp, vp, i32],
+        "kami_sdf_bake": [vp, i32, vp, i32, vp, vp, vp, vp, vp, i32, i32],
         "kami_usc_info": [ctypes.c_char_p, ctypes.POINTER(i32), ctypes.POINTER(i64), ctypes.POINTER(i32)],
         "kami_usc_read": [ctypes.c_char_p, i32, vp, vp],
         "kami_usc_write": [ctypes.c_char_p, i32, vp, i32, vp],
@@ -500,3 +501,23 @@ def write_usc(path, counts, xyz, max_verts=0):
     a = np.ascontiguousarray(xyz, np.float32)
     _check(lib.kami_usc_write(os.fsencode(path), c.shape[0], c.ctypes.data_as(ctypes.c_void_p), max_verts,
                               a.ctypes.data_as(ctypes.c_void_p)))
+
+
+def bake_sdf(vertices, triangles, dims, grid_min, grid_max, threshold=1e-3, device=-1):
+    """kami_sdf_bake on the GPU: an SDFGrid-like object (dims, grid_min, grid_max, phi [nz, ny, nx],
+    grad [nz, ny, nx, 3], threshold) ready for Solver(..., sdf=...)."""
+    from types import SimpleNamespace
+
+    lib = load_library()
+    v = np.ascontiguousarray(vertices, np.float32)
+    t = np.ascontiguousarray(triangles, np.int32)
+    d = np.asarray(dims, np.int32)
+    lo = np.asarray(grid_min, np.float32)
+    hi = np.asarray(grid_max, np.float32)
+    nx, ny, nz = (int(a) for a in dims)
+    phi = np.zeros((nz, ny, nx), np.float32)
+    grad = np.zeros((nz, ny, nx, 3), np.float32)
+    c = lambda a: a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    _check(lib.kami_sdf_bake(c(v), v.shape[0], c(t), t.shape[0], c(d), c(lo), c(hi), c(phi), c(grad), MEM_HOST, device))
+    return SimpleNamespace(dims=tuple(int(a) for a in dims), grid_min=tuple(float(a) for a in lo),
+                           grid_max=tuple(float(a) for a in hi), phi=phi, grad=grad, threshold=threshold)

@@ -29,7 +29,9 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <array>
 #include <limits>
+#include <map>
 #include <vector>
 #include <algorithm>
 #ifdef _OPENMP
@@ -778,6 +780,134 @@ int oracle_advance_f64(const oracle_params* p, int64_t nv, int32_t ns, const int
                        const double* lr, const double* ks, const uint32_t* fl, const double* qr, double* x, double* v,
                        double* vl, double* q, double* clock, float dt) {
     return advanceT<double>(p, nv, ns, sb, im, lr, ks, fl, qr, x, v, vl, q, clock, dt);
+}
+
+// Body SDF bake, FP64, by brute force over the triangles: the grid PNMesh::StoreSDFQueries fills
+// (PNMesh.cpp:109-173) from the exact signed distance that Discregrid::TriangleMeshDistance gives
+// (extern/Discregrid/geometry/TriangleMeshDistance.h:280-318) rather than from its cubic Lagrange
+// resampling.  Closest point on a triangle with its Voronoi feature: Ericson, Real-Time Collision
+// Detection (2005), 5.1.5.  Sign: the angle-weighted pseudonormal of that feature (Baerentzen and
+// Aanaes, IEEE TVCG 11(3), 2005).  grad: inside (distance < 0), the unit gradient of the distance;
+// otherwise the unit direction from the grid centre, as StoreSDFQueries sets it (zero at the centre
+// node, where the reference divides 0 by 0).
+int oracle_sdf_bake_f64(int32_t nv, const float* verts, int32_t nt, const int32_t* tris, const int32_t* dims,
+                        const float* gmin, const float* gmax, double* phi, double* grad) {
+    typedef V3<double> D3;
+    auto vert = [&](int32_t i) { return v3<double>(verts[3 * i], verts[3 * i + 1], verts[3 * i + 2]); };
+    std::vector<D3> fn(nt), vn(nv, v3<double>(0, 0, 0));
+    std::vector<std::array<D3, 3>> en(nt);
+    std::map<std::pair<int32_t, int32_t>, D3> edge_sum;
+    for (int32_t t = 0; t < nt; t++) {
+        const int32_t* T = tris + 3 * t;
+        D3 a = vert(T[0]), b = vert(T[1]), c = vert(T[2]);
+        D3 n = cross(b - a, c - a);
+        n = n / length(n);
+        fn[t] = n;
+        D3 p[3] = {a, b, c};
+        for (int k = 0; k < 3; k++) {
+            D3 e1 = p[(k + 1) % 3] - p[k], e2 = p[(k + 2) % 3] - p[k];
+            double ang = std::acos(std::max(-1.0, std::min(1.0, dot(e1, e2) / (length(e1) * length(e2)))));
+            vn[T[k]] = vn[T[k]] + ang * n;
+            int32_t i0 = T[k], i1 = T[(k + 1) % 3];
+            auto key = std::make_pair(std::min(i0, i1), std::max(i0, i1));
+            auto it = edge_sum.find(key);
+            if (it == edge_sum.end()) edge_sum[key] = n; else it->second = it->second + n;
+        }
+    }
+    for (auto& n : vn) { double l = length(n); if (l > 0) n = n / l; }
+    for (int32_t t = 0; t < nt; t++)
+        for (int k = 0; k < 3; k++) {  // edge k joins corners k and k+1
+            int32_t i0 = tris[3 * t + k], i1 = tris[3 * t + (k + 1) % 3];
+            D3 e = edge_sum[std::make_pair(std::min(i0, i1), std::max(i0, i1))];
+            en[t][k] = e / length(e);
+        }
+    const int64_t nx = dims[0], ny = dims[1], nz = dims[2];
+    D3 lo = v3<double>(gmin[0], gmin[1], gmin[2]);
+    D3 ds = v3<double>(((double)gmax[0] - gmin[0]) / nx, ((double)gmax[1] - gmin[1]) / ny, ((double)gmax[2] - gmin[2]) / nz);
+    D3 centre = v3<double>(0.5 * ((double)gmax[0] + gmin[0]), 0.5 * ((double)gmax[1] + gmin[1]), 0.5 * ((double)gmax[2] + gmin[2]));
+#pragma omp parallel for schedule(dynamic, 64)
+    for (int64_t node = 0; node < nx * ny * nz; node++) {
+        const int64_t i = node % nx, j = (node / nx) % ny, k = node / (nx * ny);
+        D3 x = v3<double>(lo.x + ds.x * i, lo.y + ds.y * j, lo.z + ds.z * k);
+        double best = std::numeric_limits<double>::infinity();
+        D3 bcp = x;
+        int32_t bt = -1, bf = 0;
+        for (int32_t t = 0; t < nt; t++) {
+            const int32_t* T = tris + 3 * t;
+            D3 a = vert(T[0]), b = vert(T[1]), c = vert(T[2]);
+            D3 ab = b - a, ac = c - a, ap = x - a;
+            double d1 = dot(ab, ap), d2 = dot(ac, ap);
+            D3 cp;
+            int f;  // 0,1,2 vertices; 3 edge ab, 4 edge bc, 5 edge ca; 6 face
+            if (d1 <= 0 && d2 <= 0) { cp = a; f = 0; }
+            else {
+                D3 bp = x - b;
+                double d3 = dot(ab, bp), d4 = dot(ac, bp);
+                if (d3 >= 0 && d4 <= d3) { cp = b; f = 1; }
+                else {
+                    double vc = d1 * d4 - d3 * d2;
+                    if (vc <= 0 && d1 >= 0 && d3 <= 0) { double v = d1 / (d1 - d3); cp = a + v * ab; f = 3; }
+                    else {
+                        D3 cpp = x - c;
+                        double d5 = dot(ab, cpp), d6 = dot(ac, cpp);
+                        if (d6 >= 0 && d5 <= d6) { cp = c; f = 2; }
+                        else {
+                            double vb = d5 * d2 - d1 * d6;
+                            if (vb <= 0 && d2 >= 0 && d6 <= 0) { double w = d2 / (d2 - d6); cp = a + w * ac; f = 5; }
+                            else {
+                                double va = d3 * d6 - d5 * d4;
+                                if (va <= 0 && (d4 - d3) >= 0 && (d5 - d6) >= 0) {
+                                    double w = (d4 - d3) / ((d4 - d3) + (d5 - d6)); cp = b + w * (c - b); f = 4;
+                                } else {
+                                    double den = 1.0 / (va + vb + vc);
+                                    double v = vb * den, w = vc * den;
+                                    cp = a + v * ab + w * ac; f = 6;
+                                }
+                            }
+                        }
+                    }
+                }
+            }
+            D3 dd = x - cp;
+            double q = dot(dd, dd);
+            if (q < best) { best = q; bt = t; bf = f; bcp = cp; }
+        }
+        double dist = std::sqrt(best);
+        D3 pn;
+        if (bf < 3) pn = vn[tris[3 * bt + bf]];
+        else if (bf == 3) pn = en[bt][0];
+        else if (bf == 4) pn = en[bt][1];
+        else if (bf == 5) pn = en[bt][2];
+        else pn = fn[bt];
+        D3 u = x - bcp;
+        double sgn = dot(u, pn) >= 0 ? 1.0 : -1.0;
+        phi[node] = sgn * dist;
+        D3 g;
+        if (sgn * dist < 0) g = (bcp - x) / dist;
+        else {  // radial; the grid centre itself (0/0 there) gets a zero gradient
+            D3 r = x - centre;
+            double l = length(r);
+            g = l > 0 ? r / l : v3<double>(0, 0, 0);
+        }
+        grad[3 * node] = g.x;
+        grad[3 * node + 1] = g.y;
+        grad[3 * node + 2] = g.z;
+    }
+    return 0;
+}
+
+// Signed distance (as oracle_sdf_bake_f64 computes it) at np arbitrary points: a bake on a
+// 1 x 1 x 1 grid per point.
+int oracle_sdf_points_f64(int32_t nv, const float* verts, int32_t nt, const int32_t* tris, int64_t np, const double* pts,
+                          double* dist) {
+    const int32_t one[3] = {1, 1, 1};
+    for (int64_t i = 0; i < np; i++) {
+        const float lo[3] = {(float)pts[3 * i], (float)pts[3 * i + 1], (float)pts[3 * i + 2]};
+        const float hi[3] = {lo[0] + 1.f, lo[1] + 1.f, lo[2] + 1.f};
+        double g[3];
+        oracle_sdf_bake_f64(nv, verts, nt, tris, one, lo, hi, &dist[i], g);
+    }
+    return 0;
 }
 
 int oracle_num_threads(void) {

@@ -84,6 +84,11 @@ def load():
             fn.argtypes = [ctypes.POINTER(OracleParams), ctypes.c_int64, ctypes.c_int32] + [ctypes.c_void_p] * 11 + [
                 ctypes.c_float]
         lib.oracle_num_threads.restype = ctypes.c_int
+        lib.oracle_sdf_bake_f64.restype = ctypes.c_int
+        lib.oracle_sdf_bake_f64.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 6
+        lib.oracle_sdf_points_f64.restype = ctypes.c_int
+        lib.oracle_sdf_points_f64.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
+                                              ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
         _lib = lib
     return _lib
 
@@ -207,3 +212,32 @@ def twist_angles(q_ref, q_new):
     dw = aw * bw - (ax * bx + ay * by + az * bz)
     ang = 2.0 * np.arctan2(dx, dw)
     return (ang + np.pi) % (2.0 * np.pi) - np.pi
+
+
+def sdf_bake(vertices, triangles, dims, grid_min, grid_max):
+    """FP64 body SDF of a closed triangle mesh on the grid nodes grid_min + ds (i, j, k):
+    (phi [nz, ny, nx], grad [nz, ny, nx, 3])."""
+    lib = load()
+    v = np.ascontiguousarray(vertices, np.float32)
+    t = np.ascontiguousarray(triangles, np.int32)
+    d = np.asarray(dims, np.int32)
+    lo = np.asarray(grid_min, np.float32)
+    hi = np.asarray(grid_max, np.float32)
+    nx, ny, nz = (int(a) for a in dims)
+    phi = np.zeros((nz, ny, nx), np.float64)
+    grad = np.zeros((nz, ny, nx, 3), np.float64)
+    rc = lib.oracle_sdf_bake_f64(v.shape[0], _p(v), t.shape[0], _p(t), _p(d), _p(lo), _p(hi), _p(phi), _p(grad))
+    if rc != 0:
+        raise RuntimeError("oracle SDF bake failed")
+    return phi, grad
+
+
+def sdf_points(vertices, triangles, points):
+    """FP64 signed distance to a closed triangle mesh at float32-rounded points [..., 3]."""
+    lib = load()
+    v = np.ascontiguousarray(vertices, np.float32)
+    t = np.ascontiguousarray(triangles, np.int32)
+    p = np.ascontiguousarray(np.asarray(points, np.float32), np.float64).reshape(-1, 3)
+    out = np.zeros(p.shape[0], np.float64)
+    lib.oracle_sdf_points_f64(v.shape[0], _p(v), t.shape[0], _p(t), p.shape[0], _p(p), _p(out))
+    return out.reshape(np.asarray(points).shape[:-1])

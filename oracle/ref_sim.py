@@ -116,3 +116,43 @@ def sdf_project(pos, vel, local_idx, sdf, rot=(0.0, 0.0, 0.0, 1.0), trans=(0.0, 
     if rc != 0:
         raise RuntimeError("ref_sdf_project failed")
     return p, v
+
+
+SDF_LIB_PATH = os.path.join(_HERE, "_ref", "libkami_ref_sdf.so")
+
+
+def sdf_available():
+    return os.path.exists(SDF_LIB_PATH)
+
+
+def _sdf_lib():
+    lib = ctypes.CDLL(SDF_LIB_PATH)
+    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+    lib.ref_sdf_signed_distance.argtypes = [i32, vp, i32, vp, i64, vp, vp]
+    lib.ref_sdf_bake.argtypes = [i32, vp, i32, vp, vp, vp, vp, vp, vp]
+    return lib
+
+
+def sdf_signed_distance(vertices, triangles, points):
+    """Discregrid's TriangleMeshDistance::signed_distance, compiled from the reference's sources."""
+    v = np.ascontiguousarray(vertices, np.float32)
+    t = np.ascontiguousarray(triangles, np.int32)
+    p = np.ascontiguousarray(points, np.float64).reshape(-1, 3)
+    out = np.zeros(p.shape[0], np.float64)
+    _sdf_lib().ref_sdf_signed_distance(v.shape[0], _p(v), t.shape[0], _p(t), p.shape[0], _p(p), _p(out))
+    return out
+
+
+def sdf_bake(vertices, triangles, dims, grid_min, grid_max):
+    """The reference's bake: Kami::SDF::Init (cubic Lagrange grid of Discregrid's distance at
+    resolution dims) sampled at the grid nodes as PNMesh::StoreSDFQueries does; (phi, grad)."""
+    v = np.ascontiguousarray(vertices, np.float32)
+    t = np.ascontiguousarray(triangles, np.int32)
+    d = np.asarray(dims, np.int32)
+    lo = np.asarray(grid_min, np.float32)
+    hi = np.asarray(grid_max, np.float32)
+    nx, ny, nz = (int(a) for a in dims)
+    phi = np.zeros((nz, ny, nx), np.float32)
+    grad = np.zeros((nz, ny, nx, 3), np.float32)
+    _sdf_lib().ref_sdf_bake(v.shape[0], _p(v), t.shape[0], _p(t), _p(d), _p(lo), _p(hi), _p(phi), _p(grad))
+    return phi, grad
