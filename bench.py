@@ -294,7 +294,65 @@ def extra_forms(args, torch, stream, flush):
                                         "(autotuned tile shape, CUDA graph) vs 64 "
                                         "sweep-form handles stepped one after another"}
     out["adjoint_2k_x48"] = adjoint_timing(torch, stream)
+    out["sdf_bake_128"] = sdf_bake_timing()
+    try:
+        out["hair_hair_sweep"] = hair_hair_timing(torch, stream)
+    except Exception as e:  # a contact-list overflow (KAMI_ERR_CONTACTS) is reported, not fatal
+        out["hair_hair_sweep"] = {"error": str(e)}
     return out
+
+
+def sdf_bake_timing():
+    """kami_sdf_bake of a 128^3 grid from a 20,480-triangle icosphere head (host arrays in and out,
+    host-timed: pseudonormals, copies and the kernel), against the FP64 oracle on an 8^3 subset."""
+    from kamisimulator_b200 import synth, vbd
+    from oracle import oracle as orc
+
+    V, T = synth.icosphere(5, radius=0.09)
+    lo, hi = (-0.15,) * 3, (0.15,) * 3
+    vbd.bake_sdf(V, T, (16, 16, 16), lo, hi)  # warm-up (context, module)
+    t0 = time.perf_counter()
+    vbd.bake_sdf(V, T, (128, 128, 128), lo, hi)
+    gpu_s = time.perf_counter() - t0
+    t0 = time.perf_counter()
+    orc.sdf_bake(V, T, (8, 8, 8), lo, hi)
+    cpu_s = time.perf_counter() - t0
+    pairs = 128 ** 3 * T.shape[0]
+    return {"seconds": gpu_s, "node_triangle_tests_per_s": pairs / gpu_s,
+            "cpu_oracle_node_triangle_tests_per_s": 8 ** 3 * T.shape[0] / cpu_s, "cpu_threads": orc.load().oracle_num_threads(),
+            "what": "128^3 nodes x 20,480 triangles, exact signed distance + gradients, whole kami_sdf_bake call"}
+
+
+def hair_hair_timing(torch, stream, steps=50, h=4e-4):
+    """The sweep form with hair-hair collision (detection every substep) on a 2,000 x 48 groom with
+    its strands' roots on the head, at the reference's substep maxH = 4e-4 s (the velocity radius of
+    the detection grows with the substep; at 1/120 s a dense groom exceeds 16 contacts per segment):
+    vertex-iterations/s, CUDA events around kami_vbd_step."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.vbd import Solver
+
+    g = synth.groom(2000, 48, seed=4)
+    st = dict(settings(), radius=2e-6, max_h=h)
+    s = Solver(g, form="sweep", hair_hair=True, barrier_thickness=7.6e-5, **st)
+    free = Solver(g, form="sweep", **st)
+    res = {}
+    for name, solver in (("hair_hair", s), ("no_contacts", free)):
+        for _ in range(10):
+            solver.step(h, stream=stream)
+        torch.cuda.synchronize()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(steps):
+            solver.step(h, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1) / steps
+        res[name] = {"value": g.num_vertices * NUM_ITR * 1000.0 / ms, "ms_per_step": ms}
+        solver.synchronize()
+        solver.close()
+    res["what"] = ("2,000 strands x 48 vertices, 20 iterations, substeps of 4e-4 s, head SDF; sweep form with and without "
+                   "hair-hair collision (radius 2 um, barrier 76 um as the solver sets them at CurveRadius 40 um)")
+    return res
 
 
 def large_timing(torch, stream, frames=24, adjoint_frames=30, tape_gb=60.0):
@@ -517,7 +575,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
-    ap.add_argument("--only", choices=["adjoint", "large"], help="run a single extra measurement")
+    ap.add_argument("--only", choices=["adjoint", "large", "hairhair", "bake"], help="run a single extra measurement")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
@@ -529,6 +587,12 @@ def main():
         import torch
 
         print(json.dumps(large_timing(torch, torch.cuda.current_stream())), flush=True)
+    elif args.only == "hairhair":
+        import torch
+
+        print(json.dumps(hair_hair_timing(torch, torch.cuda.current_stream())), flush=True)
+    elif args.only == "bake":
+        print(json.dumps(sdf_bake_timing()), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     else:
