@@ -129,6 +129,11 @@ typedef struct kami_vbd_desc {
     int32_t detection_period;  /* detectionPeriod: substeps between detections (1); <= 0 never detects */
     int32_t step_limit;        /* useStepSizeLimit (1, as the solver sets it with EnableHairHairColl) */
     int32_t velocity_radius;   /* useVelocityRadius (1) */
+
+    /* SagFreeItr: passes of sag-free initialisation run at creation, after root pinning, as
+     * BuildYarnBallHair does (StableCosseratRodsSolver.cpp:208; Sim::SagFree, YBSimulator.cu:480-674);
+     * 0 = none.  kami_vbd_sag_free runs it on demand. */
+    int32_t sag_free_itr;
 } kami_vbd_desc;
 
 typedef struct kami_vbd_solver* kami_vbd_handle;
@@ -185,6 +190,12 @@ kami_status kami_vbd_get_positions_velocities(kami_vbd_handle h, float* xyz, flo
 
 /* Segment orientations (4*V floats, x y z w per vertex; the tip copies its previous segment).
  * Replaces: the qs part of Sim::download (YBSimulator.cu:355-360). */
+/* Sag-free initialisation (Sim::SagFree, YBSimulator.cu:480-674) on the GPU, one thread per strand:
+ * rest lengths that cancel the stretch force of the hanging mass, and orientations / rest Darboux
+ * turned to cancel the bending torque under the handle's gravity, `iterations` passes.  Positions
+ * are unchanged.  Call it before stepping, as the reference does at construction. */
+kami_status kami_vbd_sag_free(kami_vbd_handle h, int32_t iterations);
+
 /* Device-resident Hair.  KamiSimulator's Hair keeps positions and velocities in padded
  * [strand][vertex] arrays: xyz of Hair strand u, vertex v at (u * max_verts + v) * 3
  * (EigenVecX3f2DArray, LinearUtil.cpp:159, :247-253).  kami_vbd_set_hair_layout tells the solver

@@ -386,6 +386,7 @@ static kami_status validate_desc(const kami_vbd_desc* d) {
         for (int a = 0; a < 3; a++)
             if (!(s->grid_max[a] > s->grid_min[a])) return fail(KAMI_ERR_INVALID_ARGUMENT, "SDF grid_max must exceed grid_min");
     }
+    if (d->sag_free_itr < 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "sag_free_itr must be >= 0");
     if (d->hair_hair) {
         if (!(d->barrier_thickness > 0.f)) return fail(KAMI_ERR_INVALID_ARGUMENT, "barrier_thickness must be > 0");
         if (!(d->detection_scaler > 1.f))  // Sim::uploadMeta, YBSimulator.cu:326
@@ -417,6 +418,7 @@ static const char* differing_setting(const kami_vbd_desc* a, const kami_vbd_desc
     if (a->device != b->device) return "device";
     if (a->slots_per_lane != b->slots_per_lane || a->warps_per_block != b->warps_per_block) return "tile shape";
     if (a->hair_hair != b->hair_hair) return "hair_hair";
+    if (a->sag_free_itr != b->sag_free_itr) return "sag_free_itr";
     if (a->hair_hair &&
         (a->radius != b->radius || a->barrier_thickness != b->barrier_thickness || a->k_collision != b->k_collision ||
          a->k_friction != b->k_friction || a->friction_coeff != b->friction_coeff ||
@@ -702,6 +704,10 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
     if (d->hair_hair) {
         kami_status cs = setup_collisions(h, d);
         if (cs != KAMI_OK) return bail(cs);
+    }
+    if (d->sag_free_itr > 0) {
+        kami_status ss = kami_vbd_sag_free(h, d->sag_free_itr);
+        if (ss != KAMI_OK) return bail(ss);
     }
     *out = h;
     return KAMI_OK;
@@ -1234,6 +1240,26 @@ kami_status kami_vbd_zero_rest_darboux_grad(kami_vbd_handle h) {
     KAMI_TRY(valid_handle(h));
     if (!h->d_gqr) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
     KAMI_CUDA(cudaMemsetAsync(h->d_gqr, 0, sizeof(float4) * h->layout.num_slots, h->stream), "gradient reset");
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_sag_free(kami_vbd_handle h, int32_t iterations) {
+    KAMI_TRY(valid_handle(h));
+    if (iterations < 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "iterations must be >= 0");
+    if (iterations == 0) return KAMI_OK;
+    int32_t* d_sb = nullptr;
+    float* d_fs = nullptr;
+    cudaError_t e = dalloc(&d_sb, (size_t)h->ns + 1);
+    if (e == cudaSuccess) e = dalloc(&d_fs, (size_t)h->layout.num_slots);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(d_sb, h->strand_begin.data(), sizeof(int32_t) * (h->ns + 1), cudaMemcpyHostToDevice, h->stream);
+    if (e == cudaSuccess)
+        e = launch_sag_free(h->dstate(), make_float3(h->pp.gx, h->pp.gy, h->pp.gz), d_sb, h->d_slot_of, h->ns, d_fs,
+                            iterations, h->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(h->stream);
+    if (d_sb) cudaFree(d_sb);
+    if (d_fs) cudaFree(d_fs);
+    if (e != cudaSuccess) return cuda_fail(e, "sag-free initialisation");
     return KAMI_OK;
 }
 

@@ -38,6 +38,10 @@ cudaError_t launch_sweep_position_coll(const DeviceState& st, const float4* y4, 
                                        float4* dx_out, const float4* snap, const StepParams* d_sp, const PhysParams& pp,
                                        const CollParams& cp, int colour, bool jacobi, cudaStream_t s);
 
+// sag-free initialisation (sag_free.cu): `iterations` passes, one thread per strand; fs: a float per slot
+cudaError_t launch_sag_free(const DeviceState& st, float3 gravity, const int32_t* strand_begin, const int64_t* slot_of,
+                            int32_t num_strands, float* fs, int iterations, cudaStream_t s);
+
 // padded Hair arrays <-> tile slots (hair_index: padded entry of each boundary vertex)
 cudaError_t launch_hair_in(const float* src, float4* dst, const int64_t* slot_of, const int64_t* hair_index, int64_t nv,
                            cudaStream_t s);

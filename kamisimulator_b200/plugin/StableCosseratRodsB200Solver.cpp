@@ -82,7 +82,6 @@ kami_vbd_desc StableCosseratRodsB200Solver::BuildDescriptor(const std::string& s
     boolean("UseYoungsModule", use_young);
     boolean("EnableSDF", enable_sdf_);
     boolean("EnableHairHairColl", hair_hair);
-    if (sag_free > 0) throw std::runtime_error("SagFreeItr > 0 is not supported by the B200 solver");
     auto g = j.find("Gravity");
     if (g != j.end() && g->second.kind == JsonValue::Array && g->second.array.size() == 3)
         for (int a = 0; a < 3; a++) d.gravity[a] = (float)g->second.array[a];
@@ -103,6 +102,7 @@ kami_vbd_desc StableCosseratRodsB200Solver::BuildDescriptor(const std::string& s
     d.radius = 0.05f * curve_radius;  // StableCosseratRodsSolver.cpp:177-179
     // hair-hair collision: barrier, step limit and velocity radius as the reference solver sets them
     // (StableCosseratRodsSolver.cpp:180-186); it runs on the sweep form
+    d.sag_free_itr = sag_free > 0 ? (int32_t)sag_free : 0;  // StableCosseratRodsSolver.cpp:208
     d.hair_hair = hair_hair ? 1 : 0;
     d.barrier_thickness = 2.f * (1.f - 0.05f) * curve_radius;
     d.step_limit = hair_hair ? 1 : 0;

@@ -55,7 +55,8 @@ struct BodySDF {
 // EnableSDF, EnableHairHairColl, SagFreeItr, SubdivCoeff, EnableResample, plus SDFThreshold
 // (SDFBodyCollisionSolver.h:25) and the extensions MaxTimeStep (the reference fixes 4e-4 s),
 // Gravity [x, y, z], Schedule ("colour2" | "jacobi") and Form ("auto" | "fused" | "sweep").
-// EnableHairHairColl turns on hair-hair collision with the reference solver's barrier
+// SagFreeItr runs that many passes of sag-free initialisation at Construct
+// (StableCosseratRodsSolver.cpp:208).  EnableHairHairColl turns on hair-hair collision with the reference solver's barrier
 // (2 (1 - 0.05) CurveRadius), step limit and velocity radius (StableCosseratRodsSolver.cpp:176-186).
 // Strands with fewer than 4 vertices are skipped, as there (StableCosseratRodsSolver.cpp:134-136).
 // Resampling and subdivision are Hair preprocessing that KamiSimulator runs before Construct.

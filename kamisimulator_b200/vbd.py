@@ -36,7 +36,7 @@ EXPORTED = [
     "kami_vbd_tape_reserve", "kami_vbd_get_tile_count", "kami_vbd_set_tape_window", "kami_vbd_step_record", "kami_vbd_backward", "kami_vbd_get_rest_darboux_grad",
     "kami_vbd_zero_rest_darboux_grad", "kami_vbd_batch_create", "kami_vbd_batch_count", "kami_vbd_batch_groom_range",
     "kami_vbd_batch_step", "kami_vbd_set_hair_layout", "kami_vbd_upload_hair", "kami_vbd_download_hair",
-    "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake",
+    "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake", "kami_vbd_sag_free",
 ]
 
 
@@ -94,6 +94,7 @@ class Desc(ctypes.Structure):
         ("detection_period", ctypes.c_int32),
         ("step_limit", ctypes.c_int32),
         ("velocity_radius", ctypes.c_int32),
+        ("sag_free_itr", ctypes.c_int32),
     ]
 
 
@@ -121,6 +122,7 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_upload_hair": [vp, vp, vp, i32],
         "kami_vbd_download_hair": [vp, vp, vp, i32],
         "kami_sdf_bake": [vp, i32, vp, i32, vp, vp, vp, vp, vp, i32, i32],
+        "kami_vbd_sag_free": [vp, i32],
         "kami_usc_info": [ctypes.c_char_p, ctypes.POINTER(i32), ctypes.POINTER(i64), ctypes.POINTER(i32)],
         "kami_usc_read": [ctypes.c_char_p, i32, vp, vp],
         "kami_usc_write": [ctypes.c_char_p, i32, vp, i32, vp],
@@ -195,7 +197,8 @@ class Solver:
                  young=5.0, deviation=1.0, per_strand=True, k_stretch=3e3, k_bend=6e-4, pin_roots=True,
                  velocities=None, device=-1, slots_per_lane=0, warps_per_block=0, hair_hair=False,
                  barrier_thickness=None, k_collision=None, k_friction=None, friction_coeff=None,
-                 detection_scaler=None, detection_period=None, step_limit=None, velocity_radius=None):
+                 detection_scaler=None, detection_period=None, step_limit=None, velocity_radius=None,
+                 sag_free_itr=0):
         """groom: one groom (kami_vbd_create) or a list of grooms (kami_vbd_batch_create, one handle
         stepping all of them; velocities is then None or a list with one entry per groom)."""
         self.lib = load_library()
@@ -250,6 +253,7 @@ class Solver:
             d.warps_per_block = warps_per_block
             d.sdf = sdf_ptr
             d.hair_hair = int(bool(hair_hair))
+            d.sag_free_itr = int(sag_free_itr)
             for name, val in (("barrier_thickness", barrier_thickness), ("k_collision", k_collision),
                               ("k_friction", k_friction), ("friction_coeff", friction_coeff),
                               ("detection_scaler", detection_scaler), ("detection_period", detection_period),
@@ -276,6 +280,10 @@ class Solver:
         _check(self.lib.kami_vbd_batch_groom_range(self._h, groom, ctypes.byref(s0), ctypes.byref(ns),
                                                    ctypes.byref(v0), ctypes.byref(nv)))
         return s0.value, ns.value, v0.value, nv.value
+
+    def sag_free(self, iterations=1):
+        """kami_vbd_sag_free: sag-free rest lengths and rest angles under the handle's gravity."""
+        _check(self.lib.kami_vbd_sag_free(self._h, iterations))
 
     def set_hair_layout(self, hair_strands, max_verts, strand_refs=None):
         """The padded Hair arrays ([hair_strands][max_verts] xyz) the solver reads and writes;

@@ -910,6 +910,167 @@ int oracle_sdf_points_f64(int32_t nv, const float* verts, int32_t nt, const int3
     return 0;
 }
 
+// Sim::SagFree / SingleSagFree (YarnBall/YBSimulator.cu:480-674), strand by strand with the
+// reference's float / double mix.  Part 1, tip to root: each segment's rest length becomes the
+// root of the quadratic that cancels the stretch force of the mass below it (the root nearer the
+// old length; 1.5 x when there is none; clamped to [1e-6, 1.5 x]).  Part 2, root to tip: each
+// segment's orientation turns in the plane of its axis and the bending force towards the angle
+// whose bending torque cancels the force's torque, bracketed within 1e-4 rad of the force's
+// direction; the rotations accumulate towards the tip, and the rest Darboux of the previous
+// segment is re-aimed keeping its magnitude (the bend/twist stiffness).  Positions do not change.
+namespace {
+const double kSagPi = 3.141592653589793238462643;
+const double kSag2Pi = 6.2831853071795864769252867665590057683943;
+const double kSagPi2 = 1.5707963267948966192313216916397;
+
+double sag_fmod(double x, double y) {  // my_fmod, YBSimulator.cu:59-72
+    long double lx = x, ly = y;
+    return ly != 0 ? (double)(lx - (long long int)(lx / ly) * ly) : 0.0;
+}
+double fit_angle(double a) { return sag_fmod(sag_fmod(a + kSagPi, kSag2Pi) + kSag2Pi, kSag2Pi) - kSagPi; }
+double sgn(double x) { return (double)((0.0 < x) - (x < 0.0)); }
+
+struct F3 {
+    float x, y, z;
+};
+inline F3 f3m(float a, F3 v) { return {a * v.x, a * v.y, a * v.z}; }
+inline F3 f3a(F3 a, F3 b) { return {a.x + b.x, a.y + b.y, a.z + b.z}; }
+inline F3 f3s(F3 a, F3 b) { return {a.x - b.x, a.y - b.y, a.z - b.z}; }
+inline float f3d(F3 a, F3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+inline F3 f3c(F3 a, F3 b) { return {a.y * b.z - b.y * a.z, a.z * b.x - b.z * a.x, a.x * b.y - b.x * a.y}; }
+inline F3 f3n(F3 a) { return f3m(1.f / std::sqrt(f3d(a, a)), a); }  // glm::normalize (v * inversesqrt(dot))
+struct FQ {
+    F3 q;
+    float w;
+};
+inline FQ fqmul(FQ l, FQ r) {  // Rotor operator*, Rotor.h:210-212
+    return {f3a(f3a(f3m(l.w, r.q), f3m(r.w, l.q)), f3c(l.q, r.q)), l.w * r.w - f3d(l.q, r.q)};
+}
+inline F3 fqrot(FQ r, F3 v) {  // Rotor::rotate, Rotor.h:114-123
+    F3 a = f3a(f3m(r.w, v), f3c(r.q, v));
+    float c = f3d(v, r.q);
+    return f3a(f3a(f3m(r.w, a), f3c(r.q, a)), f3m(c, r.q));
+}
+inline F3 fqd3(FQ r) { return f3n(fqrot(r, F3{1.f, 0.f, 0.f})); }  // getD3, Rotor.h:206
+}  // namespace
+
+int oracle_sag_free_f32(int32_t ns, const int32_t* sb, const float* pos, const float* gravity, const float* inv_mass,
+                        const float* k_stretch, float* l_rest, float* q, float* q_rest, int32_t iterations) {
+    const F3 g = {gravity[0], gravity[1], gravity[2]};
+    for (int32_t it = 0; it < iterations; it++) {
+#pragma omp parallel for schedule(dynamic, 16)
+        for (int32_t s = 0; s < ns; s++) {
+            const int rootv = sb[s], nextv = sb[s + 1];
+            const float eps = 1e-6f;
+            auto Q = [&](int i) { return FQ{{q[4 * i], q[4 * i + 1], q[4 * i + 2]}, q[4 * i + 3]}; };
+            std::vector<F3> f_srs(nextv - rootv, F3{0.f, 0.f, 0.f});
+            // 1. rest lengths, tip to root
+            float totalMassFromTip = 1 / inv_mass[nextv - 1];
+            for (int v = 0; rootv + v < nextv - 1; ++v) {
+                const int vId = nextv - 2 - v;
+                const F3 axis = fqd3(Q(vId));
+                const float kS = k_stretch[vId];
+                const float oldRestLen = l_rest[vId];
+                if (inv_mass[vId])
+                    totalMassFromTip += 0.5 / inv_mass[vId];
+                else
+                    totalMassFromTip += 0.5 * (l_rest[vId] / l_rest[vId + 1]) / inv_mass[vId + 1];
+                double f_s_g = f3d(axis, g) * totalMassFromTip;
+                double f_s = -f_s_g;
+                if (f_s == 0) {
+                    l_rest[vId] = oldRestLen;
+                } else if (1 - 4 * f_s * oldRestLen / kS < 0) {
+                    l_rest[vId] = 1.5f * oldRestLen;
+                } else {
+                    double fsk = f_s / kS;
+                    double fskinv = kS / f_s;
+                    double ans1 = (1 + std::sqrt(1 - 4 * oldRestLen * fsk)) * 0.5f * fskinv;
+                    double ans2 = (1 - std::sqrt(1 - 4 * oldRestLen * fsk)) * 0.5f * fskinv;
+                    l_rest[vId] = std::abs(oldRestLen - ans1) >= std::abs(oldRestLen - ans2) ? ans2 : ans1;
+                }
+                l_rest[vId] = std::min(std::max(l_rest[vId], eps), 1.5f * oldRestLen);
+                if (rootv + v < nextv - 2) f_srs[vId - rootv - 1] = f3m((float)-f_s, axis);
+                totalMassFromTip += 0.5 / inv_mass[vId];
+            }
+            // 2. rest angles, root to tip
+            const float nearestAngle = 1e-4f;
+            float totalMassToTip = 0;
+            for (int v = 1; rootv + v < nextv; ++v) {
+                if (inv_mass[rootv + v])
+                    totalMassToTip += 1 / inv_mass[rootv + v];
+                else
+                    totalMassToTip += (l_rest[rootv + v] / l_rest[rootv + v - 1]) / inv_mass[rootv + v - 1];
+            }
+            FQ accumQ = {{0.f, 0.f, 0.f}, 1.f};
+            for (int v = 1; rootv + v < nextv - 1; ++v) {
+                const int vId = rootv + v;
+                const FQ cQk = fqmul(accumQ, Q(vId));
+                if (inv_mass[vId])
+                    totalMassToTip -= 0.5 / inv_mass[vId];
+                else
+                    totalMassToTip -= 0.5 * (l_rest[vId] / l_rest[vId + 1]) / inv_mass[vId + 1];
+                const F3 axisk = fqd3(cQk);
+                const F3 f_b = f3a(f_srs[v], f3m(totalMassToTip, g));
+                if (f3d(f_b, axisk) < 1 - nearestAngle) {
+                    const float* qr = q_rest + 4 * vId;
+                    const float kBend = std::sqrt(qr[0] * qr[0] + qr[1] * qr[1] + qr[2] * qr[2] + qr[3] * qr[3]);
+                    const F3 planeNormal = f3n(f3c(axisk, f_b));
+                    const F3 torqueDir = f3c(planeNormal, axisk);
+                    const F3 seg = f3s(F3{pos[3 * vId + 3], pos[3 * vId + 4], pos[3 * vId + 5]},
+                                       F3{pos[3 * vId], pos[3 * vId + 1], pos[3 * vId + 2]});
+                    const float torque = f3d(torqueDir, f_b) * std::sqrt(f3d(seg, seg));
+                    const float T = torque / kBend;
+                    const float lfb = std::sqrt(f3d(f_b, f_b));  // f_b / glm::length(f_b) in float, then dvec3
+                    const double fbn[3] = {(double)(f_b.x / lfb), (double)(f_b.y / lfb), (double)(f_b.z / lfb)};
+                    const double cosm = -((double)axisk.x * fbn[0] + (double)axisk.y * fbn[1] + (double)axisk.z * fbn[2]);
+                    const double maxrad = std::acos(cosm);
+                    const double maxTheta1 = fit_angle(maxrad + nearestAngle), maxTheta2 = fit_angle(maxrad - nearestAngle);
+                    const double maxTheta = std::abs(maxTheta1) >= std::abs(maxTheta2) ? maxTheta2 : maxTheta1;
+                    const float left = maxTheta >= 0 ? 0 : (float)maxTheta;
+                    const float right = maxTheta >= 0 ? (float)maxTheta : 0;
+                    double resTheta = 0;
+                    if (std::abs(T) > 2) {
+                        resTheta = maxTheta;
+                    } else {
+                        double theta1 = fit_angle(2 * std::acos(1 - (0.5 * T * T)));
+                        double theta2 = fit_angle(2 * std::acos(-1 + (0.5 * T * T)));
+                        double cT1 = -sgn(maxTheta) * 100, cT2 = -sgn(maxTheta) * 100;
+                        if (std::abs(theta1) <= kSagPi2) cT1 = theta1;
+                        if (std::abs(theta2) > kSagPi2) cT2 = theta2;
+                        if (sgn(cT1) == sgn(maxTheta) && sgn(cT2) == sgn(maxTheta))
+                            resTheta = std::min(cT1, cT2);
+                        else {
+                            if (sgn(cT1) == sgn(maxTheta)) resTheta = cT1;
+                            if (sgn(cT2) == sgn(maxTheta)) resTheta = cT2;
+                        }
+                    }
+                    resTheta = std::min(std::max(resTheta, (double)left), (double)right);
+                    float half = (float)resTheta;  // Rotor::angleAxis(float rad, axis), Rotor.h:51-54
+                    half *= 0.5f;
+                    const FQ qTheta = {f3m(std::sin(half), planeNormal), std::cos(half)};
+                    accumQ = fqmul(accumQ, qTheta);
+                    const FQ nq = fqmul(accumQ, Q(vId));
+                    q[4 * vId] = nq.q.x;
+                    q[4 * vId + 1] = nq.q.y;
+                    q[4 * vId + 2] = nq.q.z;
+                    q[4 * vId + 3] = nq.w;
+                    const FQ pq = Q(vId - 1);
+                    const FQ d = fqmul(FQ{f3m(-1.f, pq.q), pq.w}, nq);
+                    float* pr = q_rest + 4 * (vId - 1);
+                    const float len = std::sqrt(pr[0] * pr[0] + pr[1] * pr[1] + pr[2] * pr[2] + pr[3] * pr[3]);
+                    const float dl = 1.f / std::sqrt(d.q.x * d.q.x + d.q.y * d.q.y + d.q.z * d.q.z + d.w * d.w);
+                    pr[0] = d.q.x * dl * len;
+                    pr[1] = d.q.y * dl * len;
+                    pr[2] = d.q.z * dl * len;
+                    pr[3] = d.w * dl * len;
+                }
+                totalMassToTip -= 0.5 / inv_mass[vId];
+            }
+        }
+    }
+    return 0;
+}
+
 int oracle_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

@@ -86,6 +86,8 @@ def load():
         lib.oracle_num_threads.restype = ctypes.c_int
         lib.oracle_sdf_bake_f64.restype = ctypes.c_int
         lib.oracle_sdf_bake_f64.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 6
+        lib.oracle_sag_free_f32.restype = ctypes.c_int
+        lib.oracle_sag_free_f32.argtypes = [ctypes.c_int32] + [ctypes.c_void_p] * 8 + [ctypes.c_int32]
         lib.oracle_sdf_points_f64.restype = ctypes.c_int
         lib.oracle_sdf_points_f64.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                               ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
@@ -241,3 +243,19 @@ def sdf_points(vertices, triangles, points):
     out = np.zeros(p.shape[0], np.float64)
     lib.oracle_sdf_points_f64(v.shape[0], _p(v), t.shape[0], _p(t), p.shape[0], _p(p), _p(out))
     return out.reshape(np.asarray(points).shape[:-1])
+
+
+def sag_free(groom, material, gravity, iterations):
+    """Sim::SagFree restated (FP32 material): returns new (l_rest, q, q_rest); `material` is
+    configure(..., dtype=float32) with roots pinned."""
+    lib = load()
+    sb = np.ascontiguousarray(groom.strand_begin, np.int32)
+    pos = np.ascontiguousarray(groom.positions, np.float32)
+    g = np.asarray(gravity, np.float32)
+    lr = np.array(material["l_rest"], np.float32)
+    q = np.array(material["q"], np.float32)
+    qr = np.array(material["q_rest"], np.float32)
+    im = np.ascontiguousarray(material["inv_mass"], np.float32)
+    ks = np.ascontiguousarray(material["k_stretch"], np.float32)
+    lib.oracle_sag_free_f32(groom.num_strands, _p(sb), _p(pos), _p(g), _p(im), _p(ks), _p(lr), _p(q), _p(qr), iterations)
+    return lr, q, qr

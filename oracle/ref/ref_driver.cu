@@ -78,6 +78,16 @@ void* ref_create(int64_t nv, int32_t ns, const int32_t* sb, const float* pos, fl
 
 void ref_destroy(void* h) { delete (Holder*)h; }
 
+// Sim::SagFree (YBSimulator.cu:480-674) on the host arrays, with every strand's first vertex as its
+// root, as BuildYarnBallHair passes them (StableCosseratRodsSolver.cpp:208); ref_material reads
+// the result.
+int ref_sag_free(void* h, int32_t ns, const int32_t* sb, int32_t iterations) {
+    auto& sim = ((Holder*)h)->sim;
+    std::vector<int> roots(sb, sb + ns);
+    sim->SagFree(roots, (uint32_t)iterations);
+    return 0;
+}
+
 int ref_material(void* h, float* inv_mass, float* l_rest, float* k_stretch, uint32_t* flags, float* q, float* q_rest) {
     auto& sim = ((Holder*)h)->sim;
     const int nv = sim->meta.numVerts;

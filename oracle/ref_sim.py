@@ -30,6 +30,8 @@ def load():
         lib.ref_material.argtypes = [vp] + [vp] * 6
         lib.ref_set_state.argtypes = [vp] + [vp] * 5
         lib.ref_advance.argtypes = [vp, f32]
+        lib.ref_sag_free.argtypes = [vp, i32, vp, i32]
+        lib.ref_sag_free.restype = ctypes.c_int
         lib.ref_step_hair_hair.argtypes = [vp, f32, f32]
         lib.ref_step_hair_hair.restype = ctypes.c_int
         lib.ref_download.argtypes = [vp, vp, vp, vp]
@@ -77,6 +79,11 @@ class RefSim:
         arrs = [np.ascontiguousarray(a, np.float32) for a in (x, v, v_last, q, clock)]
         if self.lib.ref_set_state(self.h, *[_p(a) for a in arrs]) != 0:
             raise RuntimeError("ref_set_state failed")
+
+    def sag_free(self, strand_begin, iterations):
+        """Sim::SagFree on the reference's host arrays (roots = first vertex of each strand)."""
+        sb = np.ascontiguousarray(strand_begin, np.int32)
+        self.lib.ref_sag_free(self.h, sb.shape[0] - 1, _p(sb), iterations)
 
     def step_hair_hair(self, dt, barrier_thickness):
         """One substep of the reference's hair-hair path with its own kernels, detection over every

@@ -62,13 +62,22 @@ def test_descriptor_from_reference_settings(tmp_path):
     assert d["gravity"] == pytest.approx([0.0, -9.8, 0.0])
 
 
-def test_unsupported_settings_are_rejected(tmp_path):
+def test_invalid_settings_are_rejected(tmp_path):
     g = synth.cantilever(2, 8)
     write_hair(tmp_path / "hair.bin", g)
-    (tmp_path / "s.json").write_text(json.dumps({"SagFreeItr": 10}))
+    (tmp_path / "s.json").write_text(json.dumps({"Schedule": "gauss-seidel"}))
     r = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
                        capture_output=True, text=True)
-    assert r.returncode == 1 and "SagFreeItr" in r.stderr
+    assert r.returncode == 1 and "Schedule" in r.stderr
+
+
+def test_sag_free_setting(tmp_path):
+    g = synth.cantilever(2, 8)
+    write_hair(tmp_path / "hair.bin", g)
+    (tmp_path / "s.json").write_text(json.dumps({"SagFreeItr": 3}))
+    out = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
+                         capture_output=True, text=True, check=True).stdout
+    assert json.loads(out)["sag_free_itr"] == 3
 
 
 def test_hair_hair_settings(tmp_path):
