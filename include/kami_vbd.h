@@ -190,6 +190,23 @@ kami_status kami_vbd_get_positions_velocities(kami_vbd_handle h, float* xyz, flo
 
 /* Segment orientations (4*V floats, x y z w per vertex; the tip copies its previous segment).
  * Replaces: the qs part of Sim::download (YBSimulator.cu:355-360). */
+/* Hair preprocessing that StableCosseratRodsSolver runs before it builds the simulation, on the
+ * GPU (one thread per strand), over padded [strand][max_verts] xyz arrays in host memory.
+ * kami_hair_subdivide = Kami::HairMods::DivideHair (utilities/HairModification.cpp:12-80), SubdivCoeff
+ * = mul: mul - 1 evenly spaced points inserted into every segment of positions (and velocities,
+ * when given); output rows of (max_verts - 1) * mul + 1 (out_* rows beyond a strand's end keep
+ * their values); out_counts = (count - 1) * mul + 1.
+ * kami_hair_resample = BuildYarnBallHair's EnableResample step (StableCosseratRodsSolver.cpp:141-163,
+ * Resample::resampleCMR in YarnBall/io/resample.h): each strand of >= 4 points is resampled, in
+ * place, along its Catmull-Rom spline to segments of target_len (from its 2nd to its next-to-last
+ * point), subsampled to max_verts when longer; counts are updated; shorter strands are left as they
+ * are.  Results equal the reference's to the bit (the file is compiled without FMA contraction). */
+kami_status kami_hair_subdivide(int32_t num_strands, const int32_t* counts, int32_t max_verts, const float* xyz,
+                                const float* vxyz, int32_t mul, int32_t* out_counts, float* out_xyz, float* out_vxyz,
+                                int32_t device);
+kami_status kami_hair_resample(int32_t num_strands, int32_t* counts, int32_t max_verts, float* xyz, float target_len,
+                               int32_t device);
+
 /* Sag-free initialisation (Sim::SagFree, YBSimulator.cu:480-674) on the GPU, one thread per strand:
  * rest lengths that cancel the stretch force of the hanging mass, and orientations / rest Darboux
  * turned to cancel the bending torque under the handle's gravity, `iterations` passes.  Positions

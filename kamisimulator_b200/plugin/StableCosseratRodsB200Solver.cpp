@@ -143,7 +143,44 @@ kami_vbd_desc StableCosseratRodsB200Solver::BuildDescriptor(const std::string& s
     return d;
 }
 
+void StableCosseratRodsB200Solver::Preprocess(const std::string& settingJsonPath) {
+    // JsonParams defaults (StableCosseratRodsSolver.h:86-111)
+    float subdiv = 3.f, resample_len = 1e-3f;
+    bool resample = true;
+    if (!settingJsonPath.empty()) {
+        auto j = parse_json_object(read_file(settingJsonPath));
+        auto it = j.find("SubdivCoeff");
+        if (it != j.end() && it->second.kind == JsonValue::Number) subdiv = (float)it->second.number;
+        it = j.find("ResampleLen");
+        if (it != j.end() && it->second.kind == JsonValue::Number) resample_len = (float)it->second.number;
+        it = j.find("EnableResample");
+        if (it != j.end() && it->second.kind == JsonValue::Bool) resample = it->second.boolean;
+    }
+    Hair& hair = *hair_;
+    std::vector<int32_t> counts(hair.strand_vert_count.begin(), hair.strand_vert_count.end());
+    const int32_t mul = (int32_t)subdiv;
+    if (mul > 1) {  // Construct: DivideHair when SubdivCoeff > 1 (StableCosseratRodsSolver.cpp:40)
+        const uint32_t out_verts = (hair.max_verts - 1) * (uint32_t)mul + 1;
+        std::vector<int32_t> oc(hair.num_strands);
+        std::vector<float> ox((size_t)hair.num_strands * out_verts * 3, 0.f), ov(ox.size(), 0.f);
+        check(kami_hair_subdivide((int32_t)hair.num_strands, counts.data(), (int32_t)hair.max_verts, hair.positions.data(),
+                                  hair.velocities.data(), mul, oc.data(), ox.data(), ov.data(), -1),
+              "Construct (SubdivCoeff)");
+        hair.max_verts = out_verts;
+        hair.positions.swap(ox);
+        hair.velocities.swap(ov);
+        counts.swap(oc);
+    }
+    if (resample) {
+        check(kami_hair_resample((int32_t)hair.num_strands, counts.data(), (int32_t)hair.max_verts, hair.positions.data(),
+                                 resample_len, -1),
+              "Construct (EnableResample)");
+    }
+    hair.strand_vert_count.assign(counts.begin(), counts.end());
+}
+
 void StableCosseratRodsB200Solver::Construct(const std::string& settingJsonPath) {
+    Preprocess(settingJsonPath);
     kami_vbd_desc d = BuildDescriptor(settingJsonPath);
     if (d.num_strands == 0) throw std::runtime_error("the Hair has no strand with at least 4 vertices");
     if (handle_) kami_vbd_destroy(handle_);

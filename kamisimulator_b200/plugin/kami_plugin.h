@@ -59,7 +59,9 @@ struct BodySDF {
 // (StableCosseratRodsSolver.cpp:208).  EnableHairHairColl turns on hair-hair collision with the reference solver's barrier
 // (2 (1 - 0.05) CurveRadius), step limit and velocity radius (StableCosseratRodsSolver.cpp:176-186).
 // Strands with fewer than 4 vertices are skipped, as there (StableCosseratRodsSolver.cpp:134-136).
-// Resampling and subdivision are Hair preprocessing that KamiSimulator runs before Construct.
+// Construct first subdivides the Hair (SubdivCoeff, default 3) and resamples its strands to
+// ResampleLen (EnableResample, default on) on the GPU, as the reference solver does; BuildDescriptor
+// (and the driver's dry run) describes the Hair as it is.
 class StableCosseratRodsB200Solver : public Solver {
    public:
     explicit StableCosseratRodsB200Solver(std::shared_ptr<Hair> hair) : Solver(std::move(hair)) {}
@@ -91,6 +93,9 @@ class StableCosseratRodsB200Solver : public Solver {
     std::vector<float> packed_pos_, packed_vel_;
     kami_vbd_sdf_desc sdf_desc_{};
     void check(kami_status st, const char* what);
+    // SubdivCoeff (DivideHair) and EnableResample / ResampleLen on the Hair, as Construct and
+    // BuildYarnBallHair do them (StableCosseratRodsSolver.cpp:40, :141-163)
+    void Preprocess(const std::string& settingJsonPath);
 };
 
 }  // namespace kami

@@ -37,6 +37,7 @@ EXPORTED = [
     "kami_vbd_zero_rest_darboux_grad", "kami_vbd_batch_create", "kami_vbd_batch_count", "kami_vbd_batch_groom_range",
     "kami_vbd_batch_step", "kami_vbd_set_hair_layout", "kami_vbd_upload_hair", "kami_vbd_download_hair",
     "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake", "kami_vbd_sag_free",
+    "kami_hair_subdivide", "kami_hair_resample",
 ]
 
 
@@ -123,6 +124,8 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_download_hair": [vp, vp, vp, i32],
         "kami_sdf_bake": [vp, i32, vp, i32, vp, vp, vp, vp, vp, i32, i32],
         "kami_vbd_sag_free": [vp, i32],
+        "kami_hair_subdivide": [i32, vp, i32, vp, vp, i32, vp, vp, vp, i32],
+        "kami_hair_resample": [i32, vp, i32, vp, f32, i32],
         "kami_usc_info": [ctypes.c_char_p, ctypes.POINTER(i32), ctypes.POINTER(i64), ctypes.POINTER(i32)],
         "kami_usc_read": [ctypes.c_char_p, i32, vp, vp],
         "kami_usc_write": [ctypes.c_char_p, i32, vp, i32, vp],
@@ -529,3 +532,30 @@ def bake_sdf(vertices, triangles, dims, grid_min, grid_max, threshold=1e-3, devi
     _check(lib.kami_sdf_bake(c(v), v.shape[0], c(t), t.shape[0], c(d), c(lo), c(hi), c(phi), c(grad), MEM_HOST, device))
     return SimpleNamespace(dims=tuple(int(a) for a in dims), grid_min=tuple(float(a) for a in lo),
                            grid_max=tuple(float(a) for a in hi), phi=phi, grad=grad, threshold=threshold)
+
+
+def hair_subdivide(counts, xyz, mul, vxyz=None, device=-1):
+    """DivideHair on padded [S, max_verts, 3] arrays: returns (counts, xyz[, vxyz]) with rows of
+    (max_verts - 1) * mul + 1 (zeros past each strand's end)."""
+    lib = load_library()
+    c = np.ascontiguousarray(counts, np.int32)
+    x = np.ascontiguousarray(xyz, np.float32)
+    ns, mv = x.shape[0], x.shape[1]
+    out_mv = (mv - 1) * mul + 1
+    oc = np.zeros(ns, np.int32)
+    ox = np.zeros((ns, out_mv, 3), np.float32)
+    v = None if vxyz is None else np.ascontiguousarray(vxyz, np.float32)
+    ov = None if v is None else np.zeros_like(ox)
+    p = lambda a: None if a is None else a.ctypes.data_as(ctypes.c_void_p)  # noqa: E731
+    _check(lib.kami_hair_subdivide(ns, p(c), mv, p(x), p(v), mul, p(oc), p(ox), p(ov), device))
+    return (oc, ox) if v is None else (oc, ox, ov)
+
+
+def hair_resample(counts, xyz, target_len, device=-1):
+    """BuildYarnBallHair's resampling on padded [S, max_verts, 3] arrays: returns new (counts, xyz)."""
+    lib = load_library()
+    c = np.array(counts, np.int32)
+    x = np.array(xyz, np.float32)
+    _check(lib.kami_hair_resample(x.shape[0], c.ctypes.data_as(ctypes.c_void_p), x.shape[1],
+                                  x.ctypes.data_as(ctypes.c_void_p), ctypes.c_float(target_len), device))
+    return c, x

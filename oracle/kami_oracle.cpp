@@ -1071,6 +1071,151 @@ int oracle_sag_free_f32(int32_t ns, const int32_t* sb, const float* pos, const f
     return 0;
 }
 
+// Resample::resampleCMR (YarnBall/io/resample.h:10-170) for one strand, in double: uniform
+// Catmull-Rom samples (Kit::cmrSpline, KittenEngine Common.h:625-635) marched at parameter steps of
+// 0.2 and refined by eight secant steps to the target segment length, from both ends, merged at the
+// closest pair of samples when both have more than 32; done for the target length and again for
+// the average length of the first result, keeping the one whose segment lengths vary less.
+// Entries the reference would write outside its lists (fewer than 9 samples, or a merge point
+// within 8 samples of an end) are skipped.
+namespace {
+struct DV {
+    double x, y, z;
+};
+inline DV dmix(DV a, DV b, double t) { return {a.x * (1.0 - t) + b.x * t, a.y * (1.0 - t) + b.y * t, a.z * (1.0 - t) + b.z * t}; }
+inline double dlen2(DV a, DV b) { double x = a.x - b.x, y = a.y - b.y, z = a.z - b.z; return x * x + y * y + z * z; }
+inline double glm_clamp(double x, double lo, double hi) {
+    x = (x < lo) ? lo : x;
+    return (hi < x) ? hi : x;
+}
+struct Curve {
+    const float* p;
+    int n;
+    DV at(int i) const { return {p[3 * i], p[3 * i + 1], p[3 * i + 2]}; }
+    DV sample(double t) const {  // sampleCurve, resample.h:10-18
+        int si = (int)std::floor(t);
+        si = si < 1 ? 1 : (si > n - 3 ? n - 3 : si);
+        DV p0 = at(si - 1), p1 = at(si), p2 = at(si + 1), p3 = at(si + 2);
+        double u = t - si;
+        DV a0 = dmix(p0, p1, u + 1), a1 = dmix(p1, p2, u + 0), a2 = dmix(p2, p3, u - 1);
+        DV b0 = dmix(a0, a1, (u + 1) * 0.5f), b1 = dmix(a1, a2, (u + 0) * 0.5f);
+        return dmix(b0, b1, u);
+    }
+};
+std::vector<double> cmr_coords(const Curve& c, double start, double end, double tar) {
+    std::vector<double> ts;
+    const double step = end > start ? 0.2 : -0.2;
+    const double r2 = tar * tar;
+    double i = start;
+    DV last = c.sample(i);
+    ts.push_back(i);
+    while ((end > start) ? i < end : i > end) {
+        i += step;
+        DV pos = c.sample(i);
+        double l0 = dlen2(pos, last);
+        if (l0 > r2) {
+            l0 = std::sqrt(l0);
+            double lo = i - step, hi = i;
+            if (lo > hi) std::swap(lo, hi);
+            const double t0 = i;
+            i -= 0.5 * step;
+            for (int k = 0; k < 8; k++) {
+                double d = std::sqrt(dlen2(c.sample(i), last));
+                i += (i - t0) * (tar - d) / (d - l0);
+            }
+            i = glm_clamp(i, lo, hi);
+            ts.push_back(i);
+            last = c.sample(i);
+        }
+    }
+    if (ts.size() == 1) {
+        ts.push_back(end);
+    } else {
+        double d = std::sqrt(dlen2(c.sample(ts.back()), c.sample(end)));
+        double dt = ts.back() - ts[ts.size() - 2];
+        if (d > 0.5f * tar)
+            ts.push_back(end);
+        else
+            ts.back() = end;
+        dt -= ts.back() - ts[ts.size() - 2];
+        const int N = std::min((int)ts.size(), 8);
+        for (int k = 0; k < N; k++) {
+            long idx = (long)ts.size() - 2 - k;
+            if (idx >= 0) ts[idx] -= dt * (N - k) / (double)N;
+        }
+    }
+    return ts;
+}
+std::vector<double> cmr_coords_two_way(const Curve& c, double start, double end, double tar) {
+    std::vector<double> F = cmr_coords(c, start, end, tar), B = cmr_coords(c, end, start, tar);
+    const int BORDER = 8;
+    if ((int)F.size() > 4 * BORDER && (int)B.size() > 4 * BORDER) {
+        double minErr = std::numeric_limits<double>::infinity();
+        int sx = 2 * BORDER, sy = 2 * BORDER;
+        for (long i = BORDER, j = (long)B.size() - 1 - BORDER; i < (long)F.size() - 8; i++) {
+            double t = F[i];
+            while (j > 0 && B[j] < t) j--;
+            double t0 = B[j + 1];
+            if (minErr > std::abs(t - t0)) { minErr = std::abs(t - t0); sx = (int)i; sy = (int)j + 1; }
+            double t1 = B[j];
+            if (minErr > std::abs(t1 - t)) { minErr = std::abs(t1 - t); sx = (int)i; sy = (int)j; }
+        }
+        std::vector<double> m(F.begin(), F.begin() + sx);
+        double mid = 0.5 * (F[sx] + B[sy]);
+        m.push_back(mid);
+        for (int k = sy - 1; k >= 0; k--) m.push_back(B[k]);
+        double dt = F[sx] - mid;
+        for (int k = 0; k < BORDER; k++) {
+            long idx = sx - k - 1;
+            if (idx >= 0 && idx < (long)m.size()) m[idx] -= dt * (BORDER - k) / (1. + BORDER);
+        }
+        dt = B[sy] - mid;
+        for (int k = 0; k < BORDER; k++) {
+            long idx = sx + k + 1;
+            if (idx >= 0 && idx < (long)m.size()) m[idx] -= dt * (BORDER - k) / (1. + BORDER);
+        }
+        return m;
+    }
+    return F;
+}
+}  // namespace
+
+// One strand's resampled points (float xyz) into out, at most max_out of them: returns the count
+// resampleCMR produces (the caller resizes when it exceeds the Hair's row, as BuildYarnBallHair does).
+int64_t oracle_resample_cmr(const float* pts, int32_t n, double tar, float* out, int64_t max_out) {
+    if (n < 4) return -1;
+    Curve c{pts, n};
+    const double start = 1, end = n - 2;
+    std::vector<double> ts0 = cmr_coords_two_way(c, start, end, tar);
+    double total = 0, err0 = 0;
+    DV last = c.sample(ts0[0]);
+    for (size_t i = 1; i < ts0.size(); i++) {
+        DV pos = c.sample(ts0[i]);
+        double len = std::sqrt(dlen2(pos, last));
+        err0 = std::max(err0, std::abs(len - tar));
+        total += len;
+        last = pos;
+    }
+    const double avg = total / (ts0.size() - 1);
+    std::vector<double> ts1 = cmr_coords_two_way(c, start, end, avg);
+    last = c.sample(ts1[0]);
+    double err1 = 0;
+    for (size_t i = 1; i < ts1.size(); i++) {
+        DV pos = c.sample(ts1[i]);
+        double len = std::sqrt(dlen2(pos, last));
+        err1 = std::max(err1, std::abs(len - avg));
+        last = pos;
+    }
+    const std::vector<double>& ts = err0 < err1 ? ts0 : ts1;
+    for (size_t i = 0; i < ts.size() && (int64_t)i < max_out; i++) {
+        DV p = c.sample(ts[i]);
+        out[3 * i] = (float)p.x;
+        out[3 * i + 1] = (float)p.y;
+        out[3 * i + 2] = (float)p.z;
+    }
+    return (int64_t)ts.size();
+}
+
 int oracle_num_threads(void) {
 #ifdef _OPENMP
     return omp_get_max_threads();

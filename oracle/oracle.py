@@ -88,6 +88,9 @@ def load():
         lib.oracle_sdf_bake_f64.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32] + [ctypes.c_void_p] * 6
         lib.oracle_sag_free_f32.restype = ctypes.c_int
         lib.oracle_sag_free_f32.argtypes = [ctypes.c_int32] + [ctypes.c_void_p] * 8 + [ctypes.c_int32]
+        lib.oracle_resample_cmr.restype = ctypes.c_int64
+        lib.oracle_resample_cmr.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p,
+                                            ctypes.c_int64]
         lib.oracle_sdf_points_f64.restype = ctypes.c_int
         lib.oracle_sdf_points_f64.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                               ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
@@ -259,3 +262,16 @@ def sag_free(groom, material, gravity, iterations):
     ks = np.ascontiguousarray(material["k_stretch"], np.float32)
     lib.oracle_sag_free_f32(groom.num_strands, _p(sb), _p(pos), _p(g), _p(im), _p(ks), _p(lr), _p(q), _p(qr), iterations)
     return lr, q, qr
+
+
+def resample_cmr(points, target):
+    """Resample::resampleCMR(curve, 1, n - 2, target) restated: the resampled strand (float32 [m, 3])."""
+    lib = load()
+    p = np.ascontiguousarray(points, np.float32)
+    cap = 5 * p.shape[0] + 16
+    out = np.zeros((cap, 3), np.float32)
+    # the target is a float setting (JsonParams::ResampleLen) widened to double, as BuildYarnBallHair passes it
+    n = lib.oracle_resample_cmr(_p(p), p.shape[0], float(np.float32(target)), _p(out), cap)
+    if n < 0:
+        raise ValueError("a strand needs at least 4 points")
+    return out[:min(n, cap)].copy()

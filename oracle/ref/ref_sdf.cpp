@@ -1,7 +1,7 @@
 // ref_sdf.cpp -- TEST INFRASTRUCTURE ONLY.
 //
 // KamiSimulator's body SDF bake compiled from the reference sources in place (oracle/ref/Makefile)
-// into oracle/_ref/libkami_ref_sdf.so, CPU only: Kami::SDF (utilities/Geometry.cpp:5-35), which
+// into oracle/_ref/libkami_ref_cpu.so, CPU only: Kami::SDF (utilities/Geometry.cpp:5-35), which
 // builds Discregrid's TriangleMeshDistance and a CubicLagrangeDiscreteGrid of it, and the per-node
 // loop of PNMesh::StoreSDFQueries (PNMesh.cpp:109-173), restated here because PNMesh.cpp needs the
 // rest of the application.  Tests use it to pin the CPU oracle and the GPU bake.

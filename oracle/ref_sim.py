@@ -125,19 +125,40 @@ def sdf_project(pos, vel, local_idx, sdf, rot=(0.0, 0.0, 0.0, 1.0), trans=(0.0, 
     return p, v
 
 
-SDF_LIB_PATH = os.path.join(_HERE, "_ref", "libkami_ref_sdf.so")
+CPU_LIB_PATH = os.path.join(_HERE, "_ref", "libkami_ref_cpu.so")
 
 
-def sdf_available():
-    return os.path.exists(SDF_LIB_PATH)
+def cpu_available():
+    """The reference's CPU parts built from source (SDF bake, strand resampler); no GPU needed."""
+    return os.path.exists(CPU_LIB_PATH)
+
+
+_cpu = None
 
 
 def _sdf_lib():
-    lib = ctypes.CDLL(SDF_LIB_PATH)
-    vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
-    lib.ref_sdf_signed_distance.argtypes = [i32, vp, i32, vp, i64, vp, vp]
-    lib.ref_sdf_bake.argtypes = [i32, vp, i32, vp, vp, vp, vp, vp, vp]
-    return lib
+    global _cpu
+    if _cpu is None:
+        lib = ctypes.CDLL(CPU_LIB_PATH)
+        vp, i32, i64 = ctypes.c_void_p, ctypes.c_int32, ctypes.c_int64
+        lib.ref_sdf_signed_distance.argtypes = [i32, vp, i32, vp, i64, vp, vp]
+        lib.ref_sdf_bake.argtypes = [i32, vp, i32, vp, vp, vp, vp, vp, vp]
+        lib.ref_resample_cmr.argtypes = [vp, i32, ctypes.c_double, vp, i64]
+        lib.ref_resample_cmr.restype = i64
+        _cpu = lib
+    return _cpu
+
+
+def resample_cmr(points, target):
+    """Resample::resampleCMR(curve, 1, n - 2, target) of the reference, compiled from source.  It
+    corrupts the heap when a pass yields 8 samples or fewer (resample.h:78-79): call it only for
+    strands whose resampled length is well above that."""
+    p = np.ascontiguousarray(points, np.float32)
+    cap = 5 * p.shape[0] + 16
+    out = np.zeros((cap, 3), np.float32)
+    # the target is a float setting (JsonParams::ResampleLen) widened to double, as BuildYarnBallHair passes it
+    n = _sdf_lib().ref_resample_cmr(_p(p), p.shape[0], float(np.float32(target)), _p(out), cap)
+    return out[:min(n, cap)].copy()
 
 
 def sdf_signed_distance(vertices, triangles, points):

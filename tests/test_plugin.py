@@ -97,7 +97,8 @@ def test_plugin_steps_match_the_c_abi_and_the_oracle(tmp_path):
     counts, mv = write_hair(tmp_path / "hair.bin", g, pad_to=40)
     settings = {"NumItr": 6, "UseYoungsModule": True, "YoungsModule": 1e-4, "StiffnessDeviationCoeff": 0.5,
                 "CurveRadius": 40e-6 / 0.05, "Density": 1300, "VelocityDecay": 0.05, "WindPeak": 0,
-                "EnableSDF": False, "MaxTimeStep": 1 / 60, "Gravity": [0.3, -0.4, -9.81]}
+                "EnableSDF": False, "MaxTimeStep": 1 / 60, "Gravity": [0.3, -0.4, -9.81],
+                "SubdivCoeff": 1, "EnableResample": False}
     (tmp_path / "s.json").write_text(json.dumps(settings))
     steps = 5
     subprocess.run([DRIVER, str(tmp_path / "s.json"), str(tmp_path / "hair.bin"), str(steps), str(1 / 60),
@@ -132,7 +133,8 @@ def test_plugin_reads_and_writes_usc_data_files(tmp_path):
     vbd.write_usc(tmp_path / "in.data", counts, g.positions)
     write_hair(tmp_path / "hair.bin", g, pad_to=100)
     settings = {"NumItr": 6, "UseYoungsModule": True, "YoungsModule": 1e-4, "CurveRadius": 40e-6 / 0.05,
-                "WindPeak": 0, "EnableSDF": False, "MaxTimeStep": 1 / 60, "Gravity": [0.3, -0.4, -9.81]}
+                "WindPeak": 0, "EnableSDF": False, "MaxTimeStep": 1 / 60, "Gravity": [0.3, -0.4, -9.81],
+                "SubdivCoeff": 1, "EnableResample": False}
     (tmp_path / "s.json").write_text(json.dumps(settings))
     for src, dst in (("in.data", "out.data"), ("hair.bin", "out.bin")):
         subprocess.run([DRIVER, str(tmp_path / "s.json"), str(tmp_path / src), "4", str(1 / 60), str(tmp_path / dst)],
@@ -145,3 +147,41 @@ def test_plugin_reads_and_writes_usc_data_files(tmp_path):
     moved = [s for s in range(g.num_strands) if counts[s] >= 4]
     assert max(np.abs(xd[s, :counts[s]] - g.positions[g.strand_begin[s]:g.strand_begin[s + 1]]).max()
                for s in moved) > 1e-4
+
+
+@pytest.mark.gpu
+def test_plugin_subdivides_and_resamples_the_hair(tmp_path):
+    """With the reference solver's defaults (SubdivCoeff 3, EnableResample at ResampleLen), Construct
+    subdivides and resamples the Hair first: the result equals kami_hair_subdivide +
+    kami_hair_resample followed by the C ABI."""
+    from kamisimulator_b200 import vbd
+
+    g = helpers.soft_groom(20, (6, 14), seed=15)
+    counts, mv = write_hair(tmp_path / "hair.bin", g, pad_to=16)
+    settings = {"NumItr": 6, "UseYoungsModule": True, "YoungsModule": 1e-4, "CurveRadius": 40e-6 / 0.05,
+                "WindPeak": 0, "EnableSDF": False, "MaxTimeStep": 1 / 60, "Gravity": [0.3, -0.4, -9.81],
+                "ResampleLen": 1.5e-3}
+    (tmp_path / "s.json").write_text(json.dumps(settings))
+    subprocess.run([DRIVER, str(tmp_path / "s.json"), str(tmp_path / "hair.bin"), "3", str(1 / 60),
+                    str(tmp_path / "out.bin")], check=True, capture_output=True)
+    padded = np.zeros((g.num_strands, 16, 3), np.float32)
+    for s in range(g.num_strands):
+        padded[s, :counts[s]] = g.positions[g.strand_begin[s]:g.strand_begin[s + 1]]
+    c3, x3 = vbd.hair_subdivide(counts, padded, 3)
+    cr, xr = vbd.hair_resample(c3, x3, 1.5e-3)
+    assert (cr != c3).any()
+    keep = [s for s in range(g.num_strands) if cr[s] >= 4]
+    pos = np.concatenate([xr[s, :cr[s]] for s in keep])
+    gg = synth.Groom(strand_begin=np.concatenate([[0], np.cumsum([cr[s] for s in keep])]).astype(np.int32),
+                     positions=pos, strand_young=np.full(len(keep), 1e-4, np.float32),
+                     strand_dev=np.ones(len(keep), np.float32))
+    st = dict(num_itr=6, max_h=1 / 60, gravity=(0.3, -0.4, -9.81), radius=np.float32(0.05) * np.float32(40e-6 / 0.05),
+              velocity_decay=0.05)
+    s = helpers.gpu_solver(gg, st, form="fused")
+    for _ in range(3):
+        s.step(1 / 60)
+    x = s.get_positions_velocities()[0]
+    s.close()
+    out, _ = read_out(tmp_path / "out.bin", g.num_strands, (16 - 1) * 3 + 1)
+    got = np.concatenate([out[s, :cr[s]] for s in keep])
+    np.testing.assert_allclose(got, x, atol=1e-6)

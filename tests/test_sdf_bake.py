@@ -1,5 +1,5 @@
 """Body SDF bake: the FP64 oracle against the reference's own code built from source on the CPU
-(oracle/_ref/libkami_ref_sdf.so: Kami::SDF over Discregrid, utilities/Geometry.cpp:5-35, and
+(oracle/_ref/libkami_ref_cpu.so: Kami::SDF over Discregrid, utilities/Geometry.cpp:5-35, and
 PNMesh::StoreSDFQueries' node loop), and the host-side checks of kami_sdf_bake."""
 import ctypes
 
@@ -10,7 +10,7 @@ from kamisimulator_b200 import synth, vbd
 from oracle import oracle as orc
 from oracle import ref_sim
 
-needs_ref = pytest.mark.skipif(not ref_sim.sdf_available(), reason="oracle/_ref not built (needs the reference sources)")
+needs_ref = pytest.mark.skipif(not ref_sim.cpu_available(), reason="oracle/_ref not built (needs the reference sources)")
 MESHES = {"icosphere": lambda: synth.icosphere(3), "torus": lambda: synth.torus()}
 
 
