@@ -955,9 +955,11 @@ kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32
         h->steps_per_launch = steps_per_launch;
     }
     if (register_cap != 0) {
-        if (register_cap != 1 && register_cap != 120)
-            return fail(KAMI_ERR_INVALID_ARGUMENT, "register_cap must be 0 (unchanged), 1 (none) or 120");
-        const int cap = register_cap == 120 ? 120 : 0;
+        if (register_cap != 1 && register_cap != 2 && register_cap != 120)
+            return fail(KAMI_ERR_INVALID_ARGUMENT, "register_cap must be 0 (unchanged), 1 (none), 2 (packed x2) or 120");
+        if (register_cap == 2 && (h->layout.C != 4 || h->schedule != KAMI_SCHEDULE_COLOUR2))
+            return fail(KAMI_ERR_UNSUPPORTED, "the packed FP32x2 variant runs the colour2 step with 4 slots per lane");
+        const int cap = register_cap == 1 ? 0 : register_cap;
         if (cap != h->reg_cap) drop_graphs(h);
         h->reg_cap = cap;
     }
@@ -970,7 +972,7 @@ kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int3
     if (slots_per_lane) *slots_per_lane = h->layout.C;
     if (warps_per_block) *warps_per_block = h->warps_per_block;
     if (steps_per_launch) *steps_per_launch = h->steps_per_launch;
-    if (register_cap) *register_cap = h->reg_cap == 120 ? 120 : 1;
+    if (register_cap) *register_cap = h->reg_cap ? h->reg_cap : 1;
     return KAMI_OK;
 }
 
@@ -1047,10 +1049,12 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
     const int cmin = slots_per_lane_for(h->strand_begin.data(), h->ns);
     const int Fs[3] = {1, 4, 16};
     double rate_best = -1.0;
-    int pick[4] = {h->layout.C, h->warps_per_block, h->steps_per_launch, h->reg_cap == 120 ? 120 : 1};
+    int pick[4] = {h->layout.C, h->warps_per_block, h->steps_per_launch, h->reg_cap ? h->reg_cap : 1};
+    const bool colour2 = h->schedule == KAMI_SCHEDULE_COLOUR2;
     for (int C = cmin; C <= 4 && st == KAMI_OK; C += 2) {
-        for (int R = 0; R < (C == 2 ? 2 : 1) && st == KAMI_OK; R++) {
-        const int cap = R ? 120 : 1;
+        // kernel variants: C = 2 plain or 120 registers; C = 4 plain or packed FP32x2 (colour2)
+        for (int R = 0; R < (C == 2 || colour2 ? 2 : 1) && st == KAMI_OK; R++) {
+        const int cap = R ? (C == 2 ? 120 : 2) : 1;
         for (int W = 1; W <= 8 && st == KAMI_OK; W *= 2) {
             for (int fi = 0; fi < 3 && st == KAMI_OK; fi++) {
                 const int F = std::min(Fs[fi], trial_steps);

@@ -65,13 +65,138 @@ __device__ __forceinline__ float4 fused_orientation(float4 q, bool upd, bool pre
     return upd ? n : q;
 }
 
+// ---- packed FP32x2 form (sm_100 FFMA2 / FADD2 / FMUL2) ---------------------------------------------
+// With 4 slots per lane, slots {0, 2} and {1, 3} are each one colour, and every operand of a colour's
+// update pairs up with the same operand of the other slot of that colour.  The x2 kernel variant
+// keeps each pair in a float2 and updates both slots with one packed instruction per operation.
+struct F2x3 {
+    float2 x, y, z;
+};
+struct F2x4 {
+    float2 x, y, z, w;
+};
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 neg2(float2 a) { return make_float2(-a.x, -a.y); }
+__device__ __forceinline__ float2 sub2(float2 a, float2 b) { return __fadd2_rn(a, neg2(b)); }
+__device__ __forceinline__ float2 sel2(bool cx, bool cy, float2 a, float2 b) {
+    return make_float2(cx ? a.x : b.x, cy ? a.y : b.y);
+}
+__device__ __forceinline__ F2x3 sel23(bool cx, bool cy, F2x3 a, F2x3 b) {
+    return {sel2(cx, cy, a.x, b.x), sel2(cx, cy, a.y, b.y), sel2(cx, cy, a.z, b.z)};
+}
+__device__ __forceinline__ F2x4 sel24(bool cx, bool cy, F2x4 a, F2x4 b) {
+    return {sel2(cx, cy, a.x, b.x), sel2(cx, cy, a.y, b.y), sel2(cx, cy, a.z, b.z), sel2(cx, cy, a.w, b.w)};
+}
+__device__ __forceinline__ F2x3 pack3(float3 a, float3 b) {
+    return {make_float2(a.x, b.x), make_float2(a.y, b.y), make_float2(a.z, b.z)};
+}
+__device__ __forceinline__ F2x4 pack4(float4 a, float4 b) {
+    return {make_float2(a.x, b.x), make_float2(a.y, b.y), make_float2(a.z, b.z), make_float2(a.w, b.w)};
+}
+__device__ __forceinline__ float3 lo3(F2x3 a) { return f3(a.x.x, a.y.x, a.z.x); }
+__device__ __forceinline__ float3 hi3(F2x3 a) { return f3(a.x.y, a.y.y, a.z.y); }
+__device__ __forceinline__ float4 lo4(F2x4 a) { return make_float4(a.x.x, a.y.x, a.z.x, a.w.x); }
+__device__ __forceinline__ float4 hi4(F2x4 a) { return make_float4(a.x.y, a.y.y, a.z.y, a.w.y); }
+
+// d3 = q e_x q* for a pair (d3_of, vbd_common.cuh)
+__device__ __forceinline__ F2x3 d3_of2(F2x4 q) {
+    F2x3 d;
+    d.x = sub2(fma2(q.w, q.w, mul2(q.x, q.x)), fma2(q.y, q.y, mul2(q.z, q.z)));
+    const float2 s1 = fma2(q.x, q.y, mul2(q.w, q.z));
+    d.y = add2(s1, s1);
+    const float2 s2 = fma2(q.x, q.z, mul2(neg2(q.w), q.y));
+    d.z = add2(s2, s2);
+    return d;
+}
+
+// Hamilton product l r with the scalar last (qmul), and l conj(r) (qmul_conj), for pairs
+__device__ __forceinline__ F2x4 qmul2(F2x4 l, F2x4 r) {
+    F2x4 o;
+    o.x = fma2(l.w, r.x, fma2(r.w, l.x, sub2(mul2(l.y, r.z), mul2(r.y, l.z))));
+    o.y = fma2(l.w, r.y, fma2(r.w, l.y, sub2(mul2(l.z, r.x), mul2(r.z, l.x))));
+    o.z = fma2(l.w, r.z, fma2(r.w, l.z, sub2(mul2(l.x, r.y), mul2(r.x, l.y))));
+    o.w = sub2(mul2(l.w, r.w), fma2(l.x, r.x, fma2(l.y, r.y, mul2(l.z, r.z))));
+    return o;
+}
+__device__ __forceinline__ F2x4 qmul_conj2(F2x4 l, F2x4 r) {
+    return qmul2(l, F2x4{neg2(r.x), neg2(r.y), neg2(r.z), r.w});
+}
+__device__ __forceinline__ float2 dot42(F2x4 a, F2x4 b) {
+    return fma2(a.x, b.x, fma2(a.y, b.y, fma2(a.z, b.z, mul2(a.w, b.w))));
+}
+__device__ __forceinline__ float2 dot32(F2x3 a, F2x3 b) { return fma2(a.x, b.x, fma2(a.y, b.y, mul2(a.z, b.z))); }
+__device__ __forceinline__ float2 sqrt_nonneg2(float2 x) {
+    return make_float2(sqrt_nonneg(x.x), sqrt_nonneg(x.y));
+}
+
+// fused_position for a pair of same-colour slots; nkkN = -kkN, nas = -(a + s) are precomputed.
+__device__ __forceinline__ F2x3 fused_position2(F2x3 dx, F2x3 F0, float2 ddN, float2 nkkN, F2x3 d3N, F2x3 dxN,
+                                                float2 ddP, float2 kkP, F2x3 d3P, F2x3 dxP, float2 nas, float2 isA,
+                                                float2 isB, const bool* hn, const bool* hp, const bool* upd) {
+    dxN = sel23(hn[0], hn[1], dxN, dx);
+    dxP = sel23(hp[0], hp[1], dxP, dx);
+    d3P = sel23(hp[0], hp[1], d3P, d3N);
+    F2x3 f;
+    f.x = fma2(kkP, d3P.x, fma2(nkkN, d3N.x, fma2(nas, dx.x, fma2(ddP, dxP.x, fma2(ddN, dxN.x, F0.x)))));
+    f.y = fma2(kkP, d3P.y, fma2(nkkN, d3N.y, fma2(nas, dx.y, fma2(ddP, dxP.y, fma2(ddN, dxN.y, F0.y)))));
+    f.z = fma2(kkP, d3P.z, fma2(nkkN, d3N.z, fma2(nas, dx.z, fma2(ddP, dxP.z, fma2(ddN, dxN.z, F0.z)))));
+    const float2 m = mul2(add2(add2(f.x, f.y), f.z), make_float2(1.f / 3.f, 1.f / 3.f));
+    const float2 mb = mul2(m, isB);
+    F2x3 n;
+    n.x = fma2(sub2(f.x, m), isA, add2(dx.x, mb));
+    n.y = fma2(sub2(f.y, m), isA, add2(dx.y, mb));
+    n.z = fma2(sub2(f.z, m), isA, add2(dx.z, mb));
+    return sel23(upd[0], upd[1], n, dx);
+}
+
+// fused_orientation for a pair of same-colour segments
+__device__ __forceinline__ F2x4 fused_orientation2(F2x4 q, const bool* upd, const bool* pre, const bool* nxt, F2x3 Ve,
+                                                   float2 m2k, F2x3 dx, F2x3 dxN, F2x4 qPrev, F2x4 qrPrev,
+                                                   F2x4 qNext, F2x4 qr) {
+    F2x3 V;
+    V.x = fma2(m2k, sub2(dxN.x, dx.x), Ve.x);
+    V.y = fma2(m2k, sub2(dxN.y, dx.y), Ve.y);
+    V.z = fma2(m2k, sub2(dxN.z, dx.z), Ve.z);
+    qPrev = sel24(pre[0], pre[1], qPrev, q);
+    qNext = sel24(nxt[0], nxt[1], qNext, q);
+    const F2x4 P1 = qmul2(qPrev, qrPrev);
+    const F2x4 P2 = qmul_conj2(qNext, qr);
+    const float2 d1 = dot42(q, P1), d2 = dot42(q, P2);
+    const float2 s1 = make_float2(pre[0] ? (d1.x > 0.f ? 1.f : -1.f) : 0.f, pre[1] ? (d1.y > 0.f ? 1.f : -1.f) : 0.f);
+    const float2 s2 = make_float2(nxt[0] ? (d2.x > 0.f ? 1.f : -1.f) : 0.f, nxt[1] ? (d2.y > 0.f ? 1.f : -1.f) : 0.f);
+    F2x4 b;
+    b.x = fma2(s1, P1.x, mul2(s2, P2.x));
+    b.y = fma2(s1, P1.y, mul2(s2, P2.y));
+    b.z = fma2(s1, P1.z, mul2(s2, P2.z));
+    b.w = fma2(s1, P1.w, mul2(s2, P2.w));
+    const float2 lambda = add2(sqrt_nonneg2(dot32(V, V)), sqrt_nonneg2(dot42(b, b)));
+    // P = V b e_x with V = (V, 0): R = (Pw + l b.x, Pq.z + l b.y, -Pq.y + l b.z, -Pq.x + l b.w),
+    // Pq = b.w V + V x bq, Pw = -V . bq
+    const float2 Pqx = fma2(b.w, V.x, sub2(mul2(V.y, b.z), mul2(b.y, V.z)));
+    const float2 Pqy = fma2(b.w, V.y, sub2(mul2(V.z, b.x), mul2(b.z, V.x)));
+    const float2 Pqz = fma2(b.w, V.z, sub2(mul2(V.x, b.y), mul2(b.x, V.y)));
+    const float2 Pw = neg2(fma2(V.x, b.x, fma2(V.y, b.y, mul2(V.z, b.z))));
+    F2x4 R;
+    R.x = fma2(lambda, b.x, Pw);
+    R.y = fma2(lambda, b.y, Pqz);
+    R.z = fma2(lambda, b.z, neg2(Pqy));
+    R.w = fma2(lambda, b.w, neg2(Pqx));
+    const float2 rr = dot42(R, R);
+    const float2 inv = make_float2(rsqrtf(rr.x), rsqrtf(rr.y));
+    const F2x4 n = {mul2(inv, R.x), mul2(inv, R.y), mul2(inv, R.z), mul2(inv, R.w)};
+    return sel24(upd[0], upd[1], n, q);
+}
+
 // One launch runs `nsteps` consecutive steps, step j with clock and body transform steps[j] (or
 // `sp` when steps is null), keeping the tile's state in registers between them.  RECORD (colour2,
 // one step of one substep) additionally writes the step's start state and the iterates to a tape
 // for the adjoint (vbd_adjoint.cuh).
-template <int C, bool JACOBI, bool RECORD>
+template <int C, bool JACOBI, bool RECORD, bool PAIRED = false>
 __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                 TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
+    static_assert(!PAIRED || (C == 4 && !JACOBI && !RECORD), "the packed form is the colour2 step with 4 slots per lane");
     static_assert(!(RECORD && JACOBI), "the tape records the colour2 schedule");
     static_assert(C % 2 == 0, "slots per lane must be even");
     const int lane = threadIdx.x & 31;
@@ -163,6 +288,67 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
             }
         }
 
+        if constexpr (PAIRED) {
+            // pairs of same-colour slots: A = {0, 2}, B = {1, 3}.  A's neighbours are B's slots
+            // (and the previous lane's slot 3 for slot 0); B's are A's (and the next lane's slot 0
+            // for slot 3).
+            F2x3 dxA = pack3(dx[0], dx[2]), dxB = pack3(dx[1], dx[3]);
+            F2x4 qA = pack4(q[0], q[2]), qB = pack4(q[1], q[3]);
+            F2x3 d3A = pack3(d3[0], d3[2]), d3B = pack3(d3[1], d3[3]);
+            const F2x3 F0A = pack3(F0[0], F0[2]), F0B = pack3(F0[1], F0[3]);
+            const F2x3 VeA = pack3(Ve[0], Ve[2]), VeB = pack3(Ve[1], Ve[3]);
+            const float2 ddNA = make_float2(ddN[0], ddN[2]), ddNB = make_float2(ddN[1], ddN[3]);
+            const float2 nkkNA = make_float2(-kkN[0], -kkN[2]), nkkNB = make_float2(-kkN[1], -kkN[3]);
+            const float2 ddPA = make_float2(ddH, ddN[1]), kkPA = make_float2(kkH, kkN[1]);
+            const float2 kkPB = make_float2(kkN[0], kkN[2]);
+            const float2 nasA = make_float2(-as_[0], -as_[2]), nasB = make_float2(-as_[1], -as_[3]);
+            const float2 isAA = make_float2(isA[0], isA[2]), isAB = make_float2(isA[1], isA[3]);
+            const float2 isBA = make_float2(isB[0], isB[2]), isBB = make_float2(isB[1], isB[3]);
+            const float2 m2kA = make_float2(-2.f * kk[0], -2.f * kk[2]), m2kB = make_float2(-2.f * kk[1], -2.f * kk[3]);
+            const F2x4 qrA = pack4(qr[0], qr[2]), qrB = pack4(qr[1], qr[3]), qrPA = pack4(qrH, qr[1]);
+            bool hnA[2], hpA[2], mvA[2], uoA[2], nxA[2], hnB[2], hpB[2], mvB[2], uoB[2], nxB[2];
+#pragma unroll
+            for (int j = 0; j < 2; j++) {
+                const uint32_t fa = fl[2 * j], fb = fl[2 * j + 1];
+                hnA[j] = fa & F_HAS_NEXT;
+                hpA[j] = fa & F_HAS_PREV;
+                mvA[j] = mov[2 * j];
+                uoA[j] = (fa & F_HAS_NEXT) && !(fa & F_FIX_ORIENTATION);
+                nxA[j] = fa & F_HAS_NEXT_ORIENTATION;
+                hnB[j] = fb & F_HAS_NEXT;
+                hpB[j] = fb & F_HAS_PREV;
+                mvB[j] = mov[2 * j + 1];
+                uoB[j] = (fb & F_HAS_NEXT) && !(fb & F_FIX_ORIENTATION);
+                nxB[j] = fb & F_HAS_NEXT_ORIENTATION;
+            }
+            for (int it = 0; it < pp.num_itr; it++) {
+                // positions, even slots
+                const F2x3 dxPA = pack3(shfl_up3(hi3(dxB), 1), lo3(dxB));
+                const F2x3 d3PA = pack3(shfl_up3(hi3(d3B), 1), lo3(d3B));
+                dxA = fused_position2(dxA, F0A, ddNA, nkkNA, d3A, dxB, ddPA, kkPA, d3PA, dxPA, nasA, isAA, isBA, hnA,
+                                      hpA, mvA);
+                // positions, odd slots
+                const F2x3 dxNB = pack3(hi3(dxA), shfl_down3(lo3(dxA), 1));
+                dxB = fused_position2(dxB, F0B, ddNB, nkkNB, d3B, dxNB, ddNA, kkPB, d3A, dxA, nasB, isAB, isBB, hnB, hpB,
+                                      mvB);
+                // orientations, even segments
+                const F2x4 qPA = pack4(shfl_up4(hi4(qB), 1), lo4(qB));
+                qA = fused_orientation2(qA, uoA, hpA, nxA, VeA, m2kA, dxA, dxB, qPA, qrPA, qB, qrA);
+                d3A = d3_of2(qA);
+                // orientations, odd segments
+                const F2x4 qNB = pack4(hi4(qA), shfl_down4(lo4(qA), 1));
+                qB = fused_orientation2(qB, uoB, hpB, nxB, VeB, m2kB, dxB, dxNB, qA, qrA, qNB, qrB);
+                d3B = d3_of2(qB);
+            }
+            dx[0] = lo3(dxA);
+            dx[2] = hi3(dxA);
+            dx[1] = lo3(dxB);
+            dx[3] = hi3(dxB);
+            q[0] = lo4(qA);
+            q[2] = hi4(qA);
+            q[1] = lo4(qB);
+            q[3] = hi4(qB);
+        } else {  // (braced: an unbraced discarded `else for` also dropped the loop after it)
         for (int it = 0; it < pp.num_itr; it++) {
             if (!JACOBI) {
                 // positions, even slots (neighbours are odd: own registers or the previous lane)
@@ -253,6 +439,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                 d3P = d3_of(qP);
             }
         }
+        }  // scalar iterations
 #pragma unroll
         for (int k = 0; k < C; k++) vbd_finish(x[k], v[k], dx[k], im[k], h, pp.velocity_decay);
     }
@@ -278,6 +465,13 @@ template <int C, bool JACOBI, bool RECORD>
 __global__ void __launch_bounds__(256) fused_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                          TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
     fused_step_body<C, JACOBI, RECORD>(st, pp, sp, sdf, tp, steps, nsteps);
+}
+
+// The colour2 step with 4 slots per lane in the packed FP32x2 form (the `x2` kernel variant).
+template <int C>
+__global__ void __launch_bounds__(256) fused_step_kernel_x2(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                            TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
+    fused_step_body<C, false, false, true>(st, pp, sp, sdf, tp, steps, nsteps);
 }
 
 // The same step with at most 120 registers per thread, so 17 warps (instead of 16) share an SM: a

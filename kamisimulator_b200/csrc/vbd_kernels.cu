@@ -234,6 +234,10 @@ cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const
     int threads = 32 * warps_per_block;
     unsigned blocks = blocks_for(st.num_tiles, warps_per_block);
     if (blocks == 0) return cudaSuccess;
+    if (reg_cap == 2 && C == 4 && !jacobi) {
+        fused_step_kernel_x2<4><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, TapeView{}, d_steps, nsteps);
+        return cudaGetLastError();
+    }
     if (reg_cap == 120 && C == 2) {
         if (jacobi)
             fused_step_kernel_r120<2, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, TapeView{}, d_steps, nsteps);

@@ -73,7 +73,7 @@ def test_autotune_picks_a_shape_and_restores_the_state():
     s.step(1 / 120)
     before = s.get_state()
     best, rate = s.autotune(1 / 120, trial_steps=8)
-    assert best[0] in (4,) and best[1] in (1, 2, 4, 8) and best[2] in (1, 4, 8) and best[3] in (1, 120)
+    assert best[0] in (4,) and best[1] in (1, 2, 4, 8) and best[2] in (1, 4, 8) and best[3] in (1, 2, 120)
     assert rate > 0
     np.testing.assert_array_equal(s.get_state(), before)
     ref = helpers.gpu_solver(g, st, form="fused")
@@ -126,3 +126,45 @@ def test_batch_handle_equals_one_handle_per_groom():
             assert np.abs(xb[v0:v0 + nv] - o.x).max() <= helpers.POS_TOL
         s.close()
     b.close()
+
+
+def test_packed_x2_variant_matches_the_plain_kernel_and_the_oracle():
+    """register_cap = 2: the colour2 step with 4 slots per lane in packed FP32x2 arithmetic, on
+    uneven strands with the head SDF, against the plain 4-slot kernel and the FP32 oracle."""
+    from tests.test_parity_gpu import _lockstep
+
+    g = helpers.soft_groom(120, (4, 60), seed=23)
+    v = helpers.random_velocities(g, 0.2, seed=2)
+    st = helpers.soft_settings(schedule="colour2", max_h=1 / 120, num_itr=6, sdf=synth.sphere_sdf(64, threshold=2e-3))
+    from kamisimulator_b200.vbd import KamiError, Solver
+
+    a = Solver(g, form="fused", velocities=v, slots_per_lane=4, **st)
+    b = Solver(g, form="fused", velocities=v, slots_per_lane=4, **st)
+    b.set_tuning(register_cap=2)
+    assert b.get_tuning()[3] == 2
+    for _ in range(6):
+        a.step(1 / 60)
+        b.step(1 / 60)
+    xa, xb = a.get_positions_velocities()[0], b.get_positions_velocities()[0]
+    assert np.abs(xa - xb).max() <= 1e-6
+    c = Solver(g, form="fused", velocities=v, slots_per_lane=2, **st)
+    with pytest.raises(KamiError, match="packed"):
+        c.set_tuning(register_cap=2)
+    for s in (a, b, c):
+        s.close()
+    # against the oracle, per frame from shared states
+    import kamisimulator_b200.vbd as vbd
+
+    orig = vbd.Solver.__init__
+
+    def packed_init(self, *args, **kw):
+        kw["slots_per_lane"] = 4
+        orig(self, *args, **kw)
+        self.set_tuning(register_cap=2)
+
+    vbd.Solver.__init__ = packed_init
+    try:
+        ex, et = _lockstep(g, st, "fused", 8, 1 / 60, velocities=v, reseed_each_frame=True)
+    finally:
+        vbd.Solver.__init__ = orig
+    assert ex <= helpers.POS_TOL and et <= helpers.TWIST_TOL, (ex, et)
