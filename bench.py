@@ -10,9 +10,11 @@ Metric: VBD vertex-iterations per second (vertices x iterations x steps / time),
 `value` times the fused step kernel with the state resident in HBM; the 95 MB working set fits
 the 126 MB L2, so a 256 MiB buffer is written between timed steps and only the step kernels are
 timed (CUDA events on the launching stream).  `e2e` is the same metric through the C ABI with
-host buffers: every step uploads positions/velocities from pinned host memory
-(kami_vbd_set_positions_velocities, UploadHair), steps, and reads them back
-(kami_vbd_get_positions_velocities, DownloadHair).  Extra `forms` report the plain per-groom sweep
+host buffers: every frame is one kami_vbd_step_host call, which uploads positions/velocities from
+pinned host memory (UploadHair), steps and reads them back (DownloadHair), overlapping the copies of
+one strand group with the step of another; `three_calls_value` is the same frame as
+kami_vbd_set_positions_velocities, kami_vbd_step, kami_vbd_get_positions_velocities in turn.  Extra
+`forms` report the plain per-groom sweep
 form and the batched form on 64 uneven grooms.  With N > 1 (torchrun) each rank steps its own groom
 (weak scaling, no collective on the data path); times are maxima over ranks.
 
@@ -524,21 +526,33 @@ def run_ours(args):
     value = job_throughput(world, V, NUM_ITR, args.steps, max_ms)
     ms_step = max_ms / args.steps
 
-    # end to end through the C ABI with pinned host buffers
+    # end to end through the C ABI with pinned host buffers: one kami_vbd_step_host call per frame
+    # (upload, step, download, pipelined over strand groups), and for comparison the same frame as
+    # three calls (kami_vbd_set_positions_velocities, kami_vbd_step, kami_vbd_get_positions_velocities)
     xh = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
     vh = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
     solver.get_positions_velocities(xh.numpy(), vh.numpy())
     e2e_steps = max(10, args.steps // 10)
-    barrier()
-    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-    e0.record(stream)
-    for _ in range(e2e_steps):
+
+    def e2e_run(frame):
+        barrier()
+        e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        for _ in range(e2e_steps):
+            frame()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return job_throughput(world, V, NUM_ITR, e2e_steps, max_over_ranks(e0.elapsed_time(e1), world))
+
+    def three_calls():
         solver.set_positions_velocities(xh.numpy(), vh.numpy())
         solver.step(DT, stream=stream)
         solver.get_positions_velocities(xh.numpy(), vh.numpy())
-    e1.record(stream)
-    torch.cuda.synchronize()
-    e2e_value = job_throughput(world, V, NUM_ITR, e2e_steps, max_over_ranks(e0.elapsed_time(e1), world))
+
+    for _ in range(3):
+        solver.step_host(DT, xh, vh)
+    e2e_value = e2e_run(lambda: solver.step_host(DT, xh, vh))
+    e2e_three_calls = e2e_run(three_calls)
     solver.close()
 
     line = None
@@ -556,7 +570,8 @@ def run_ours(args):
                              "frac": achieved / peak, "traffic": traffic, "kernel": "fused_step_kernel (colour2, one step per launch)",
                              "bytes_per_launch": V * BYTES_PER_VERTEX_STEP, "peak_source": peak_kind},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * V, "d2h_bytes_per_step": 24 * V,
-                        "steps": e2e_steps},
+                        "steps": e2e_steps, "call": "kami_vbd_step_host (pinned host buffers)",
+                        "three_calls_value": e2e_three_calls},
                 "gpu_launches": args.steps, "clocks": clk.summary()}
     if world == 1 and rank == 0 and not args.skip_extra:
         line["forms"] = extra_forms(args, torch, stream, flush)

@@ -188,6 +188,20 @@ kami_status kami_vbd_set_positions_velocities(kami_vbd_handle h, const float* xy
  * device status word was raised since the last check. */
 kami_status kami_vbd_get_positions_velocities(kami_vbd_handle h, float* xyz, float* vxyz, int32_t memory);
 
+/* One frame of the plugin's host loop from host buffers to host buffers: UploadHair, SolveNextStep(dt),
+ * DownloadHair (StableCosseratRodsSolver.cpp:216-277, i.e. Sim::uploadPosAndVel, Sim::advance and
+ * the SDF pass, Sim::downloadPosAndVel).  The result is that of kami_vbd_set_positions_velocities,
+ * kami_vbd_step and kami_vbd_get_positions_velocities with host memory (3*V floats per array;
+ * xyz_out / vxyz_out may be xyz / vxyz).  With the fused form, no hair-hair collision and all four
+ * arrays each inside one page-locked host allocation mapped into the device's address space
+ * (cudaHostAlloc / cudaMallocHost, pinned torch tensors), the frame is one kernel launch: each warp
+ * reads its tile's strands from the host buffers, steps them and writes them back, so both PCIe
+ * directions overlap the arithmetic of other tiles and no copy engine or staging pass is involved.
+ * Otherwise the three calls run in turn.  Blocks until the outputs are written; reports
+ * KAMI_ERR_NONFINITE as kami_vbd_get_positions_velocities does. */
+kami_status kami_vbd_step_host(kami_vbd_handle h, float dt, const float* xyz, const float* vxyz, float* xyz_out,
+                               float* vxyz_out);
+
 /* Segment orientations (4*V floats, x y z w per vertex; the tip copies its previous segment).
  * Replaces: the qs part of Sim::download (YBSimulator.cu:355-360). */
 /* Hair preprocessing that StableCosseratRodsSolver runs before it builds the simulation, on the

@@ -1,6 +1,7 @@
 // kami_vbd.cpp -- implementation of the C ABI in include/kami_vbd.h.
 #include "kami_vbd.h"
 
+#include <cuda.h>  // CUpointer_attribute; the driver call is looked up at run time
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -69,6 +70,11 @@ struct kami_vbd_solver {
     StepParams h_step{};
     // boundary staging (4 floats per boundary vertex)
     float* d_stage = nullptr;
+    // frames over mapped host buffers (kami_vbd_step_host): the runs of each tile's strands, built
+    // for tiles of 32 * runs_C slots
+    int4* d_runs = nullptr;
+    int32_t* d_run_begin = nullptr;
+    int runs_C = 0;
     int* d_status = nullptr;
     float4* d_sdf = nullptr;
     SdfParams sdf{};
@@ -173,6 +179,8 @@ void release(kami_vbd_solver* h) {
         if (p) cudaFree(p);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
     if (h->ev_b) cudaEventDestroy(h->ev_b);
+    if (h->d_runs) cudaFree(h->d_runs);
+    if (h->d_run_begin) cudaFree(h->d_run_begin);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -867,6 +875,114 @@ static void drop_graphs(kami_vbd_solver* h) {
     if (h->graph_n) cudaGraphExecDestroy(h->graph_n);
     h->graph = h->graph_n = nullptr;
     h->graph_substeps = h->graph_n_steps = h->graph_n_F = -1;
+}
+
+// ---- frames over host buffers -------------------------------------------------------------------------
+
+// Runs of each tile's strands for the fused frame kernel (HostIO): strand s is one run of
+// consecutive tile positions starting at the position of its first vertex.
+static kami_status build_host_runs(kami_vbd_solver* h) {
+    const int C = h->layout.C;
+    const int64_t T = 32LL * C, tiles = h->layout.num_tiles;
+    std::vector<int32_t> begin(tiles + 1, 0);
+    std::vector<int64_t> tile_of(h->ns);
+    for (int32_t s = 0; s < h->ns; s++) {
+        tile_of[s] = h->layout.slot_of[h->strand_begin[s]] / T;
+        begin[tile_of[s] + 1]++;
+    }
+    for (int64_t t = 0; t < tiles; t++) begin[t + 1] += begin[t];
+    std::vector<int32_t> next(begin.begin(), begin.end() - 1);
+    std::vector<int4> runs(h->ns);
+    for (int32_t s = 0; s < h->ns; s++) {
+        const int64_t q = h->layout.slot_of[h->strand_begin[s]] % T;  // (p % C) * 32 + p / C
+        const int p0 = (int)((q % 32) * C + q / 32);
+        const int32_t v0 = h->strand_begin[s], n = h->strand_begin[s + 1] - v0;
+        // the kernel stages positions [p0, p0 + n) of the tile: they must be the strand's slots
+        if (p0 + n > T) return fail(KAMI_ERR_UNSUPPORTED, "strand %d overruns its tile", s);
+        for (int32_t j = 0; j < n; j++) {
+            const int p = p0 + j;
+            if (h->layout.slot_of[v0 + j] != tile_of[s] * T + (int64_t)(p % C) * 32 + p / C)
+                return fail(KAMI_ERR_UNSUPPORTED, "strand %d is not one run of tile positions", s);
+        }
+        runs[next[tile_of[s]]++] = make_int4(p0, v0, n, 0);
+    }
+    KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+    if (h->d_runs) cudaFree(h->d_runs);
+    if (h->d_run_begin) cudaFree(h->d_run_begin);
+    h->d_runs = nullptr;
+    h->d_run_begin = nullptr;
+    h->runs_C = 0;
+    KAMI_CUDA(dalloc(&h->d_runs, runs.size()), "strand runs");
+    KAMI_CUDA(dalloc(&h->d_run_begin, begin.size()), "strand runs");
+    KAMI_CUDA(cudaMemcpy(h->d_runs, runs.data(), sizeof(int4) * runs.size(), cudaMemcpyHostToDevice), "strand runs");
+    KAMI_CUDA(cudaMemcpy(h->d_run_begin, begin.data(), sizeof(int32_t) * begin.size(), cudaMemcpyHostToDevice),
+              "strand runs");
+    h->runs_C = C;
+    return KAMI_OK;
+}
+
+// The device address of host array [p, p + n floats) when the whole range lies in one page-locked
+// allocation mapped into the device's address space; null otherwise.
+static float* mapped_range(const void* p, int64_t n) {
+    using PtrAttr = CUresult (*)(void*, CUpointer_attribute, CUdeviceptr);
+    static PtrAttr ptr_attr = [] {
+        void* f = nullptr;
+        cudaDriverEntryPointQueryResult q = cudaDriverEntryPointSymbolNotFound;
+        if (cudaGetDriverEntryPoint("cuPointerGetAttribute", &f, cudaEnableDefault, &q) != cudaSuccess ||
+            q != cudaDriverEntryPointSuccess) {
+            cudaGetLastError();
+            return (PtrAttr) nullptr;
+        }
+        return (PtrAttr)f;
+    }();
+    if (!ptr_attr || !p || ((uintptr_t)p & 3) != 0 || n <= 0) return nullptr;
+    cudaPointerAttributes a{};
+    if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (a.type != cudaMemoryTypeHost || !a.devicePointer) return nullptr;
+    CUdeviceptr start = 0;
+    size_t size = 0;
+    const CUdeviceptr d = (CUdeviceptr)(uintptr_t)a.devicePointer;
+    if (ptr_attr(&start, CU_POINTER_ATTRIBUTE_RANGE_START_ADDR, d) != CUDA_SUCCESS ||
+        ptr_attr(&size, CU_POINTER_ATTRIBUTE_RANGE_SIZE, d) != CUDA_SUCCESS)
+        return nullptr;
+    if (d < start || d + sizeof(float) * (size_t)n > start + size) return nullptr;
+    return (float*)a.devicePointer;
+}
+
+kami_status kami_vbd_step_host(kami_vbd_handle h, float dt, const float* xyz, const float* vxyz, float* xyz_out,
+                               float* vxyz_out) {
+    KAMI_TRY(valid_handle(h));
+    if (!xyz || !vxyz || !xyz_out || !vxyz_out) return fail(KAMI_ERR_INVALID_ARGUMENT, "null position or velocity array");
+    if (!std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
+    HostIO io{};
+    const int64_t n = 3 * h->nv;
+    bool direct = dt > 0.f && h->form == KAMI_FORM_FUSED && !h->hair_hair;
+    if (direct) {
+        io.x_in = mapped_range(xyz, n);
+        io.v_in = mapped_range(vxyz, n);
+        io.x_out = mapped_range(xyz_out, n);
+        io.v_out = mapped_range(vxyz_out, n);
+        direct = io.x_in && io.v_in && io.x_out && io.v_out;
+    }
+    if (!direct) {
+        // pageable buffers, no step, or strands coupled within the step: upload, step and download in turn
+        KAMI_TRY(kami_vbd_set_positions_velocities(h, xyz, vxyz, KAMI_MEMORY_HOST));
+        KAMI_TRY(kami_vbd_step(h, dt, nullptr));
+        return kami_vbd_get_positions_velocities(h, xyz_out, vxyz_out, KAMI_MEMORY_HOST);
+    }
+    if (h->runs_C != h->layout.C) KAMI_TRY(build_host_runs(h));
+    io.runs = h->d_runs;
+    io.run_begin = h->d_run_begin;
+    const StepParams sp = advance_clock(h, dt);
+    KAMI_CUDA(launch_fused_frame(h->dstate(), h->pp, sp, h->sdf, io, h->layout.C, h->schedule == KAMI_SCHEDULE_JACOBI,
+                                 h->warps_per_block, h->stream, h->reg_cap),
+              "fused frame launch");
+    h->time += dt;
+    h->counter += sp.substeps;
+    return check_status_word(h);
 }
 
 // Moves the live state to tiles of 32*C slots (gathered to boundary order and scattered back).

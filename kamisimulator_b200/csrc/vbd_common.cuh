@@ -92,6 +92,20 @@ struct TapeView {
     int64_t tile_begin;
 };
 
+// Host buffers that a fused step reads and writes itself (page-locked and mapped, device-visible
+// addresses): positions and velocities, 3 floats per boundary vertex.  Each strand of a tile is a
+// run of consecutive tile positions p (slot (p % C) * 32 + p / C of the tile) holding consecutive
+// boundary vertices; runs[r] = (first position, first boundary vertex, vertex count, 0), and the
+// runs of tile t are [run_begin[t], run_begin[t + 1]).
+struct HostIO {
+    const float* x_in;
+    const float* v_in;
+    float* x_out;
+    float* v_out;
+    const int4* runs;
+    const int32_t* run_begin;
+};
+
 // Adjoint state of the solver, tile slots: d loss / d (x, v, vlast, q), and the accumulated
 // d loss / d qRest.
 struct AdjointState {

@@ -192,15 +192,21 @@ __device__ __forceinline__ F2x4 fused_orientation2(F2x4 q, const bool* upd, cons
 // One launch runs `nsteps` consecutive steps, step j with clock and body transform steps[j] (or
 // `sp` when steps is null), keeping the tile's state in registers between them.  RECORD (colour2,
 // one step of one substep) additionally writes the step's start state and the iterates to a tape
-// for the adjoint (vbd_adjoint.cuh).
-template <int C, bool JACOBI, bool RECORD, bool PAIRED = false>
+// for the adjoint (vbd_adjoint.cuh).  HOSTIO steps tile `tile` of a host frame (fused_frame_kernel):
+// `stage` holds the tile's positions then velocities from the host buffers of `hio`, 3 floats per
+// tile position p = lane * C + k, and the step writes its results back to the host buffers
+// through the same area, as well as to the device state.
+template <int C, bool JACOBI, bool RECORD, bool PAIRED = false, bool HOSTIO = false>
 __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
-                                                TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
+                                                TapeView tp, const StepParams* __restrict__ steps, int nsteps,
+                                                HostIO hio = HostIO{}, int64_t frame_tile = 0, float* stage = nullptr) {
     static_assert(!PAIRED || (C == 4 && !JACOBI && !RECORD), "the packed form is the colour2 step with 4 slots per lane");
+    static_assert(!(HOSTIO && RECORD), "recorded steps keep their state on the device");
     static_assert(!(RECORD && JACOBI), "the tape records the colour2 schedule");
     static_assert(C % 2 == 0, "slots per lane must be even");
     const int lane = threadIdx.x & 31;
-    const int64_t tile = (RECORD ? tp.tile_begin : 0) + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    const int64_t tile = HOSTIO ? frame_tile
+                                : (RECORD ? tp.tile_begin : 0) + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (tile >= st.num_tiles) return;  // uniform per warp
     const int64_t base = tile * (32LL * C) + lane;
 
@@ -227,6 +233,19 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
         mov[k] = im[k] != 0.f;
         ddN[k] = (fl[k] & F_HAS_NEXT) ? kk[k] * invl[k] : 0.f;
         kkN[k] = (fl[k] & F_HAS_NEXT) ? kk[k] : 0.f;
+    }
+    float* const sx = stage;
+    float* const sv = stage + 3 * 32 * C;
+    if constexpr (HOSTIO) {
+#pragma unroll
+        for (int k = 0; k < C; k++) {
+            if (fl[k] & F_VALID) {  // padding slots keep their device values
+                const int o = 3 * (lane * C + k);
+                x[k] = f3(sx[o], sx[o + 1], sx[o + 2]);
+                v[k] = f3(sv[o], sv[o + 1], sv[o + 2]);
+            }
+        }
+        __syncwarp();
     }
     const int64_t tS = tp.slots;
     const int64_t tslot = base - (RECORD ? tp.tile_begin * 32LL * C : 0);  // this lane's slot in the tape window
@@ -458,6 +477,29 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
         st.vlast[g] = make_float4(vl[k].x, vl[k].y, vl[k].z, 0.f);
         st.q[g] = q[k];
     }
+    if constexpr (HOSTIO) {
+#pragma unroll
+        for (int k = 0; k < C; k++) {
+            const int o = 3 * (lane * C + k);
+            sx[o] = x[k].x;
+            sx[o + 1] = x[k].y;
+            sx[o + 2] = x[k].z;
+            sv[o] = v[k].x;
+            sv[o + 1] = v[k].y;
+            sv[o + 2] = v[k].z;
+        }
+        __syncwarp();
+        const int r_end = hio.run_begin[tile + 1];
+        for (int r = hio.run_begin[tile]; r < r_end; r++) {
+            const int4 run = hio.runs[r];
+            float* gx = hio.x_out + 3LL * run.y;
+            float* gv = hio.v_out + 3LL * run.y;
+            for (int j = lane; j < 3 * run.z; j += 32) {
+                gx[j] = sx[3 * run.x + j];
+                gv[j] = sv[3 * run.x + j];
+            }
+        }
+    }
     if (__any_sync(0xffffffffu, bad) && lane == 0) atomicOr(st.status, STATUS_NONFINITE);
 }
 
@@ -472,6 +514,44 @@ template <int C>
 __global__ void __launch_bounds__(256) fused_step_kernel_x2(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                             TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
     fused_step_body<C, false, false, true>(st, pp, sp, sdf, tp, steps, nsteps);
+}
+
+// ---- host frames: one launch uploads, steps and downloads ---------------------------------------------
+
+// One upload-step-download frame in one launch: each warp copies its tile's strands from the host
+// buffers into its staging area (6 * 32C floats of dynamic shared memory; coalesced 4-byte loads
+// over PCIe), steps the tile and writes it back (fused_step_body, HOSTIO).  The waves of tiles keep
+// the host reads of one wave apart from the host writes of the wave before, which is faster here
+// than interleaving them: SM-issued reads and writes over PCIe slow each other down.
+template <int C, bool JACOBI, bool PAIRED>
+__device__ __forceinline__ void fused_frame(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf, HostIO hio) {
+    extern __shared__ float kami_frame_stage[];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
+    if (t >= st.num_tiles) return;  // uniform per warp
+    float* const stage = kami_frame_stage + w * (6 * 32 * C);
+    const int r_end = hio.run_begin[t + 1];
+    for (int r = hio.run_begin[t]; r < r_end; r++) {
+        const int4 run = hio.runs[r];
+        const float* gx = hio.x_in + 3LL * run.y;
+        const float* gv = hio.v_in + 3LL * run.y;
+        for (int j = lane; j < 3 * run.z; j += 32) {
+            stage[3 * run.x + j] = gx[j];
+            stage[3 * 32 * C + 3 * run.x + j] = gv[j];
+        }
+    }
+    __syncwarp();
+    fused_step_body<C, JACOBI, false, PAIRED, true>(st, pp, sp, sdf, TapeView{}, nullptr, 1, hio, t, stage);
+}
+template <int C, bool JACOBI, bool PAIRED>
+__global__ void __launch_bounds__(256) fused_frame_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                          HostIO hio) {
+    fused_frame<C, JACOBI, PAIRED>(st, pp, sp, sdf, hio);
+}
+template <int C, bool JACOBI>
+__global__ void __maxnreg__(120) fused_frame_kernel_r120(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                        HostIO hio) {
+    fused_frame<C, JACOBI, false>(st, pp, sp, sdf, hio);
 }
 
 // The same step with at most 120 registers per thread, so 17 warps (instead of 16) share an SM: a

@@ -12,6 +12,8 @@
 //    coupling across lanes goes through warp shuffles.  Predict, all iterations, the velocity
 //    update and the SDF projection run back to back, so HBM sees each vertex twice per step
 //    (one float4 load per array, one store per dynamic array).
+#include <algorithm>
+
 #include "vbd_fused.cuh"
 #include "vbd_kernels.h"
 #include "vbd_math.cuh"
@@ -227,6 +229,34 @@ cudaError_t launch_sweep_finish(const DeviceState& st, const float4* dx4, const 
 }
 
 bool fused_supported(int C) { return C == 2 || C == 4; }
+
+namespace {
+// Launches a frame kernel: one warp per tile, 6 * 32C floats of staging per warp.
+template <typename K>
+cudaError_t launch_frame(K kernel, int C, const DeviceState& st, const PhysParams& pp, const StepParams& sp,
+                         const SdfParams& sdf, const HostIO& hio, int warps_per_block, cudaStream_t s) {
+    const size_t smem = sizeof(float) * 6 * 32 * (size_t)C * warps_per_block;
+    kernel<<<blocks_for(st.num_tiles, warps_per_block), 32 * warps_per_block, smem, s>>>(st, pp, sp, sdf, hio);
+    return cudaGetLastError();
+}
+}  // namespace
+
+cudaError_t launch_fused_frame(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
+                               const HostIO& hio, int C, bool jacobi, int warps_per_block, cudaStream_t s, int reg_cap) {
+    if (blocks_for(st.num_tiles, warps_per_block) == 0) return cudaSuccess;
+    if (reg_cap == 2 && C == 4 && !jacobi)
+        return launch_frame(fused_frame_kernel<4, false, true>, 4, st, pp, sp, sdf, hio, warps_per_block, s);
+    if (reg_cap == 120 && C == 2)
+        return jacobi ? launch_frame(fused_frame_kernel_r120<2, true>, 2, st, pp, sp, sdf, hio, warps_per_block, s)
+                      : launch_frame(fused_frame_kernel_r120<2, false>, 2, st, pp, sp, sdf, hio, warps_per_block, s);
+    if (C == 2)
+        return jacobi ? launch_frame(fused_frame_kernel<2, true, false>, 2, st, pp, sp, sdf, hio, warps_per_block, s)
+                      : launch_frame(fused_frame_kernel<2, false, false>, 2, st, pp, sp, sdf, hio, warps_per_block, s);
+    if (C == 4)
+        return jacobi ? launch_frame(fused_frame_kernel<4, true, false>, 4, st, pp, sp, sdf, hio, warps_per_block, s)
+                      : launch_frame(fused_frame_kernel<4, false, false>, 4, st, pp, sp, sdf, hio, warps_per_block, s);
+    return cudaErrorInvalidValue;
+}
 
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps,

@@ -24,6 +24,11 @@ cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps = nullptr,
                               int nsteps = 1, int reg_cap = 0);
 
+// One step as an upload-step-download frame over the host buffers of hio (fused_frame_kernel);
+// same tile shapes and register variants as launch_fused_step.
+cudaError_t launch_fused_frame(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
+                               const HostIO& hio, int C, bool jacobi, int warps_per_block, cudaStream_t s, int reg_cap);
+
 cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                                 const TapeView& tp, int C, int warps_per_block, cudaStream_t s);
 cudaError_t launch_adjoint_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,

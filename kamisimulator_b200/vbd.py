@@ -37,7 +37,7 @@ EXPORTED = [
     "kami_vbd_zero_rest_darboux_grad", "kami_vbd_batch_create", "kami_vbd_batch_count", "kami_vbd_batch_groom_range",
     "kami_vbd_batch_step", "kami_vbd_set_hair_layout", "kami_vbd_upload_hair", "kami_vbd_download_hair",
     "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake", "kami_vbd_sag_free",
-    "kami_hair_subdivide", "kami_hair_resample",
+    "kami_hair_subdivide", "kami_hair_resample", "kami_vbd_step_host",
 ]
 
 
@@ -139,6 +139,7 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_set_rest_darboux": [vp, vp, i32],
         "kami_vbd_set_body_transform": [vp, vp, vp],
         "kami_vbd_step": [vp, f32, vp],
+        "kami_vbd_step_host": [vp, f32, vp, vp, vp, vp],
         "kami_vbd_synchronize": [vp],
         "kami_vbd_state_size": [vp, ctypes.POINTER(ctypes.c_size_t)],
         "kami_vbd_get_state": [vp, vp, ctypes.c_size_t, i32],
@@ -182,6 +183,12 @@ def _ptr(a):
             return ctypes.c_void_p(a.data_ptr()), MEM_DEVICE
         return ctypes.c_void_p(a.data_ptr()), MEM_HOST
     return a.ctypes.data_as(ctypes.c_void_p), MEM_HOST
+
+
+def torch_float32():
+    import torch
+
+    return torch.float32
 
 
 def _f32(a, shape=None):
@@ -400,6 +407,25 @@ class Solver:
         px, mx = _ptr(x_out)
         pv, mv = _ptr(v_out)
         _check(self.lib.kami_vbd_get_positions_velocities(self._h, px, pv, mx if x_out is not None else mv))
+        return x_out, v_out
+
+    def step_host(self, dt, x, v, x_out=None, v_out=None):
+        """One frame from host arrays to host arrays (kami_vbd_step_host): upload positions and
+        velocities, step, download; pipelined over strand groups.  x_out / v_out default to x / v
+        (updated in place).  Pinned torch CPU tensors let the copies run asynchronously."""
+        x_out = x if x_out is None else x_out
+        v_out = v if v_out is None else v_out
+        for a in (x, v, x_out, v_out):
+            if hasattr(a, "data_ptr"):
+                if a.is_cuda or a.dtype != torch_float32() or not a.is_contiguous():
+                    raise ValueError("step_host takes contiguous float32 host arrays")
+            elif a.dtype != np.float32 or not a.flags.c_contiguous:
+                raise ValueError("step_host takes contiguous float32 host arrays")
+            n = a.numel() if hasattr(a, "numel") else a.size
+            if n != 3 * self.num_vertices:
+                raise ValueError(f"step_host arrays hold 3 x {self.num_vertices} floats, got {n}")
+        ptrs = [_ptr(a)[0] for a in (x, v, x_out, v_out)]
+        _check(self.lib.kami_vbd_step_host(self._h, ctypes.c_float(dt), *ptrs))
         return x_out, v_out
 
     def get_orientations(self, out=None):
