@@ -8,7 +8,8 @@
 //     f  = F0 + ddN dx_next + ddP dx_prev - (a + s) dx - kkN d3_i + kkP d3_{i-1}
 //     F0 = a y + ddN e_i - ddP e_{i-1},  kk = kStretch / l,  dd = kk / l,  s = (ddN + ddP)(1 + damping/h)
 //   (ddN/kkN are zero for a vertex without a next segment, ddP/kkP are the previous slot's),
-//   then dx += (f - mean f) accel/s + mean f accel/(s + 3a)   (the exact inverse of a 1 1^T + s I);
+//   then dx += (f - mean f) accel/s + mean f accel/(s + 3a)   (the exact inverse of a 1 1^T + s I),
+//   evaluated as dx + f isA + mean f isD with isA = accel/s, isD = accel/(s + 3a) - isA;
 //   orientation (quaternionLambdaItr, cosserat.cu:290-337) with V = -2 kk (e_i + dx_next - dx).
 // Missing neighbours enter as zero coefficients or are discarded by selects, so the iteration
 // loop has no data-dependent branches.
@@ -26,7 +27,7 @@ __device__ __forceinline__ float sqrt_nonneg(float x) { return x * rsqrtf(fmaxf(
 // reference's flag tests guarantee.
 __device__ __forceinline__ float3 fused_position(float3 dx, float3 F0, float ddN, float kkN, float3 d3N, float3 dxN,
                                                  float ddP, float kkP, float3 d3P, float3 dxP, float as_, float isA,
-                                                 float isB, bool hn, bool hp, bool upd) {
+                                                 float isD, bool hn, bool hp, bool upd) {
     dxN = hn ? dxN : dx;
     dxP = hp ? dxP : dx;
     d3P = hp ? d3P : d3N;
@@ -35,8 +36,8 @@ __device__ __forceinline__ float3 fused_position(float3 dx, float3 F0, float ddN
     f.y = F0.y + ddN * dxN.y + ddP * dxP.y - as_ * dx.y - kkN * d3N.y + kkP * d3P.y;
     f.z = F0.z + ddN * dxN.z + ddP * dxP.z - as_ * dx.z - kkN * d3N.z + kkP * d3P.z;
     const float m = (f.x + f.y + f.z) * (1.f / 3.f);
-    const float mb = m * isB;
-    const float3 n = f3(dx.x + (f.x - m) * isA + mb, dx.y + (f.y - m) * isA + mb, dx.z + (f.z - m) * isA + mb);
+    const float3 n = f3(fmaf(m, isD, fmaf(f.x, isA, dx.x)), fmaf(m, isD, fmaf(f.y, isA, dx.y)),
+                        fmaf(m, isD, fmaf(f.z, isA, dx.z)));
     return upd ? n : dx;
 }
 
@@ -134,7 +135,7 @@ __device__ __forceinline__ float2 sqrt_nonneg2(float2 x) {
 // fused_position for a pair of same-colour slots; nkkN = -kkN, nas = -(a + s) are precomputed.
 __device__ __forceinline__ F2x3 fused_position2(F2x3 dx, F2x3 F0, float2 ddN, float2 nkkN, F2x3 d3N, F2x3 dxN,
                                                 float2 ddP, float2 kkP, F2x3 d3P, F2x3 dxP, float2 nas, float2 isA,
-                                                float2 isB, const bool* hn, const bool* hp, const bool* upd) {
+                                                float2 isD, const bool* hn, const bool* hp, const bool* upd) {
     dxN = sel23(hn[0], hn[1], dxN, dx);
     dxP = sel23(hp[0], hp[1], dxP, dx);
     d3P = sel23(hp[0], hp[1], d3P, d3N);
@@ -143,11 +144,10 @@ __device__ __forceinline__ F2x3 fused_position2(F2x3 dx, F2x3 F0, float2 ddN, fl
     f.y = fma2(kkP, d3P.y, fma2(nkkN, d3N.y, fma2(nas, dx.y, fma2(ddP, dxP.y, fma2(ddN, dxN.y, F0.y)))));
     f.z = fma2(kkP, d3P.z, fma2(nkkN, d3N.z, fma2(nas, dx.z, fma2(ddP, dxP.z, fma2(ddN, dxN.z, F0.z)))));
     const float2 m = mul2(add2(add2(f.x, f.y), f.z), make_float2(1.f / 3.f, 1.f / 3.f));
-    const float2 mb = mul2(m, isB);
     F2x3 n;
-    n.x = fma2(sub2(f.x, m), isA, add2(dx.x, mb));
-    n.y = fma2(sub2(f.y, m), isA, add2(dx.y, mb));
-    n.z = fma2(sub2(f.z, m), isA, add2(dx.z, mb));
+    n.x = fma2(m, isD, fma2(f.x, isA, dx.x));
+    n.y = fma2(m, isD, fma2(f.y, isA, dx.y));
+    n.z = fma2(m, isD, fma2(f.z, isA, dx.z));
     return sel23(upd[0], upd[1], n, dx);
 }
 
@@ -212,7 +212,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
 
     float3 x[C], v[C], vl[C], dx[C], d3[C], F0[C], Ve[C];
     float4 q[C], qr[C];
-    float im[C], invl[C], kk[C], ddN[C], kkN[C], as_[C], isA[C], isB[C];
+    float im[C], invl[C], kk[C], ddN[C], kkN[C], as_[C], isA[C], isD[C];
     uint32_t fl[C];
     bool mov[C];  // the vertex's position is updated (not pinned, not padding)
 
@@ -291,14 +291,14 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                 const float sk = (ddN[k] + ddP) * (1.f + damp);
                 as_[k] = a + sk;
                 isA[k] = im[k] != 0.f ? accel / sk : 0.f;
-                isB[k] = im[k] != 0.f ? accel / (sk + 3.f * a) : 0.f;
+                isD[k] = im[k] != 0.f ? accel / (sk + 3.f * a) - isA[k] : 0.f;
                 F0[k] = a * y + ddN[k] * e[k] - ddP * eP;
                 Ve[k] = (-2.f * kk[k]) * e[k];
                 d3[k] = d3_of(q[k]);
             }
         }
         float4 qP = shfl_up4(q[C - 1], 1);
-        float3 d3P = d3_of(qP);
+        float3 d3P = shfl_up3(d3[C - 1], 1);  // the previous lane's d3_of(qP)
         if (RECORD) {
 #pragma unroll
             for (int k = 0; k < C; k++) {
@@ -322,7 +322,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
             const float2 kkPB = make_float2(kkN[0], kkN[2]);
             const float2 nasA = make_float2(-as_[0], -as_[2]), nasB = make_float2(-as_[1], -as_[3]);
             const float2 isAA = make_float2(isA[0], isA[2]), isAB = make_float2(isA[1], isA[3]);
-            const float2 isBA = make_float2(isB[0], isB[2]), isBB = make_float2(isB[1], isB[3]);
+            const float2 isDA = make_float2(isD[0], isD[2]), isDB = make_float2(isD[1], isD[3]);
             const float2 m2kA = make_float2(-2.f * kk[0], -2.f * kk[2]), m2kB = make_float2(-2.f * kk[1], -2.f * kk[3]);
             const F2x4 qrA = pack4(qr[0], qr[2]), qrB = pack4(qr[1], qr[3]), qrPA = pack4(qrH, qr[1]);
             bool hnA[2], hpA[2], mvA[2], uoA[2], nxA[2], hnB[2], hpB[2], mvB[2], uoB[2], nxB[2];
@@ -344,11 +344,11 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                 // positions, even slots
                 const F2x3 dxPA = pack3(shfl_up3(hi3(dxB), 1), lo3(dxB));
                 const F2x3 d3PA = pack3(shfl_up3(hi3(d3B), 1), lo3(d3B));
-                dxA = fused_position2(dxA, F0A, ddNA, nkkNA, d3A, dxB, ddPA, kkPA, d3PA, dxPA, nasA, isAA, isBA, hnA,
+                dxA = fused_position2(dxA, F0A, ddNA, nkkNA, d3A, dxB, ddPA, kkPA, d3PA, dxPA, nasA, isAA, isDA, hnA,
                                       hpA, mvA);
                 // positions, odd slots
                 const F2x3 dxNB = pack3(hi3(dxA), shfl_down3(lo3(dxA), 1));
-                dxB = fused_position2(dxB, F0B, ddNB, nkkNB, d3B, dxNB, ddNA, kkPB, d3A, dxA, nasB, isAB, isBB, hnB, hpB,
+                dxB = fused_position2(dxB, F0B, ddNB, nkkNB, d3B, dxNB, ddNA, kkPB, d3A, dxA, nasB, isAB, isDB, hnB, hpB,
                                       mvB);
                 // orientations, even segments
                 const F2x4 qPA = pack4(shfl_up4(hi4(qB), 1), lo4(qB));
@@ -378,7 +378,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                         const int kp = k > 0 ? k - 1 : 0;
                         dx[k] = fused_position(dx[k], F0[k], ddN[k], kkN[k], d3[k], dx[k + 1], k ? ddN[kp] : ddH,
                                                k ? kkN[kp] : kkH, k ? d3[kp] : d3P, k ? dx[kp] : dxP, as_[k], isA[k],
-                                               isB[k], fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k]);
+                                               isD[k], fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k]);
                     }
                 }
                 // positions, odd slots
@@ -387,7 +387,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                 for (int k = 1; k < C; k += 2) {
                     const int kn = k + 1 < C ? k + 1 : k;
                     dx[k] = fused_position(dx[k], F0[k], ddN[k], kkN[k], d3[k], k == C - 1 ? dxN0 : dx[kn], ddN[k - 1],
-                                           kkN[k - 1], d3[k - 1], dx[k - 1], as_[k], isA[k], isB[k],
+                                           kkN[k - 1], d3[k - 1], dx[k - 1], as_[k], isA[k], isD[k],
                                            fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k]);
                 }
                 // orientations, even segments
@@ -413,7 +413,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     d3[k] = d3_of(q[k]);
                 }
                 qP = shfl_up4(q[C - 1], 1);
-                d3P = d3_of(qP);
+                d3P = shfl_up3(d3[C - 1], 1);
                 if (RECORD) {
                     const int64_t row = tbase + (int64_t)(it + 1) * tS;
 #pragma unroll
@@ -432,7 +432,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     const int kp = k > 0 ? k - 1 : 0, kn = k + 1 < C ? k + 1 : k;
                     nd[k] = fused_position(dx[k], F0[k], ddN[k], kkN[k], d3[k], k == C - 1 ? dxN0 : dx[kn],
                                            k ? ddN[kp] : ddH, k ? kkN[kp] : kkH, k ? d3[kp] : d3P, k ? dx[kp] : dxP,
-                                           as_[k], isA[k], isB[k], fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k]);
+                                           as_[k], isA[k], isD[k], fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k]);
                 }
 #pragma unroll
                 for (int k = 0; k < C; k++) dx[k] = nd[k];
@@ -455,7 +455,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     d3[k] = d3_of(q[k]);
                 }
                 qP = shfl_up4(q[C - 1], 1);
-                d3P = d3_of(qP);
+                d3P = shfl_up3(d3[C - 1], 1);
             }
         }
         }  // scalar iterations
