@@ -505,7 +505,11 @@ def run_ours(args):
     st = settings()
     V = g.num_vertices
     solver = Solver(g, form="fused", device=local, **st)
-    tuned, _ = solver.autotune(DT, trial_steps=8)  # the library's autotuner; restores the state
+    if args.tuning:  # a fixed tile shape (profiling runs: no autotune launches before the timed ones)
+        solver.set_tuning(*[int(t) for t in args.tuning.split(",")])
+        tuned = solver.get_tuning()
+    else:
+        tuned, _ = solver.autotune(DT, trial_steps=8)  # the library's autotuner; restores the state
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
@@ -591,6 +595,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
     ap.add_argument("--only", choices=["adjoint", "large", "hairhair", "bake"], help="run a single extra measurement")
+    ap.add_argument("--tuning", help="fixed tile shape C,warps,steps_per_launch,register_cap instead of autotuning")
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
