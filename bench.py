@@ -42,7 +42,12 @@ DT = 1.0 / 120.0
 NUM_ITR = 20
 METRIC = "VBD vertex-iters/s"
 UNIT = "vertex-iters/s"
-BYTES_PER_VERTEX_STEP = 160  # fused kernel: 6 float4 loads + 4 float4 stores per vertex (see DESIGN.md)
+BYTES_PER_VERTEX_STEP = 160  # fused kernel: 6 float4 loads + 4 float4 stores per vertex
+# FLOPs of one vertex-iteration of the reference algorithm (cosseratItr 242 + quaternionLambdaItr
+# 250), counted by the oracle's op-counting scalar; tests/test_oracle.py keeps this in step with it.
+REFERENCE_FLOP_PER_VERTEX_ITER = 492
+# Nominal FP32 peak of a B200: 148 SMs x 128 FMA lanes x 2 FLOP x 1965 MHz.
+FP32_PEAK_TFLOPS = 148 * 128 * 2 * 1.965e9 / 1e12
 FALLBACK_HBM_GBS = 6650.0
 
 
@@ -563,7 +568,19 @@ def run_ours(args):
     if rank == 0:
         peak, peak_kind = hbm_peak()
         achieved = V * BYTES_PER_VERTEX_STEP / (ms_step / 1e3) / 1e9
-        traffic, _ = ncu_traffic()
+        traffic, prof = ncu_traffic()
+        prof = prof or {}
+        per_gpu = value / world
+        kernel_flop = prof.get("fp32_flop_per_vertex_iter")
+        fp32 = {"bound": "fp32 issue", "unit": "TFLOP/s", "peak": FP32_PEAK_TFLOPS,
+                "peak_source": "nominal FP32 (148 SMs x 128 FMA lanes x 2 x 1965 MHz)",
+                "reference_flop_per_vertex_iter": REFERENCE_FLOP_PER_VERTEX_ITER,
+                "reference_equivalent": per_gpu * REFERENCE_FLOP_PER_VERTEX_ITER / 1e12,
+                "kernel_flop_per_vertex_iter": kernel_flop,
+                "achieved": per_gpu * kernel_flop / 1e12 if kernel_flop else None,
+                "issue_active": prof.get("issue_active_pct", 0) / 100 or None,
+                "source": "kernel FLOPs (2 FFMA + FMUL + FADD per thread) and issue-slot use from the committed ncu capture"}
+        fp32["frac"] = fp32["achieved"] / FP32_PEAK_TFLOPS if fp32["achieved"] else None
         line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
                 "warmup": args.warmup, "ms_per_step": ms_step, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
@@ -576,7 +593,7 @@ def run_ours(args):
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * V, "d2h_bytes_per_step": 24 * V,
                         "steps": e2e_steps, "call": "kami_vbd_step_host (pinned host buffers)",
                         "three_calls_value": e2e_three_calls},
-                "gpu_launches": args.steps, "clocks": clk.summary()}
+                "fp32": fp32, "gpu_launches": args.steps, "clocks": clk.summary()}
     if world == 1 and rank == 0 and not args.skip_extra:
         line["forms"] = extra_forms(args, torch, stream, flush)
         line["cpu_baseline"] = cpu_baseline_sample()

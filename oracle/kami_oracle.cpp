@@ -38,6 +38,45 @@
 #include <omp.h>
 #endif
 
+// ---- FLOP counting -------------------------------------------------------------------------------------
+// A double that counts the arithmetic made with it: +, -, *, / and sqrt/log count one operation each
+// (an FMA is two); negation, comparisons, min/max and conversions are free.  oracle_flop_count
+// instantiates the per-vertex updates with it to pin the FLOPs per vertex-iteration of the reference
+// update.  Its overloads are declared before the templates so that their qualified std:: calls see them.
+struct Counted {
+    double v = 0;
+    static int64_t ops;  // single-threaded use only (oracle_flop_count)
+    Counted() = default;
+    Counted(double x) : v(x) {}
+    explicit operator double() const { return v; }
+};
+int64_t Counted::ops = 0;
+inline Counted operator+(Counted a, Counted b) { Counted::ops++; return a.v + b.v; }
+inline Counted operator-(Counted a, Counted b) { Counted::ops++; return a.v - b.v; }
+inline Counted operator*(Counted a, Counted b) { Counted::ops++; return a.v * b.v; }
+inline Counted operator/(Counted a, Counted b) { Counted::ops++; return a.v / b.v; }
+inline Counted operator-(Counted a) { return -a.v; }
+inline Counted operator+(Counted a) { return a; }
+inline Counted& operator+=(Counted& a, Counted b) { return a = a + b; }
+inline Counted& operator-=(Counted& a, Counted b) { return a = a - b; }
+inline Counted& operator*=(Counted& a, Counted b) { return a = a * b; }
+inline Counted& operator/=(Counted& a, Counted b) { return a = a / b; }
+inline bool operator<(Counted a, Counted b) { return a.v < b.v; }
+inline bool operator>(Counted a, Counted b) { return a.v > b.v; }
+inline bool operator<=(Counted a, Counted b) { return a.v <= b.v; }
+inline bool operator>=(Counted a, Counted b) { return a.v >= b.v; }
+inline bool operator==(Counted a, Counted b) { return a.v == b.v; }
+inline bool operator!=(Counted a, Counted b) { return a.v != b.v; }
+namespace std {
+inline Counted sqrt(Counted a) { Counted::ops++; return std::sqrt(a.v); }
+inline Counted log(Counted a) { Counted::ops++; return std::log(a.v); }
+template <>
+class numeric_limits<Counted> : public numeric_limits<double> {
+   public:
+    static Counted infinity() { return numeric_limits<double>::infinity(); }
+};
+}  // namespace std
+
 namespace {
 
 constexpr double kPi = 3.141592653589793238462643;  // myPi, YBSimulator.cu:55
@@ -1222,6 +1261,49 @@ int oracle_num_threads(void) {
 #else
     return 1;
 #endif
+}
+
+// FLOPs of one position update (cosseratItr for an interior vertex: both segments, no hair-hair)
+// and one orientation update (quaternionLambdaItr for a segment with both neighbours), counted on
+// the reference's operation order.  TEST INFRASTRUCTURE (the roofline's FLOP count).
+void oracle_flop_count(int64_t* position_ops, int64_t* orientation_ops) {
+    // a 4-vertex strand, slightly bent; vertex 1 / segment 1 have every neighbour
+    const int nv = 4;
+    std::vector<Counted> im(nv, Counted(1.0 / 3e-7)), lr(nv, Counted(2e-3)), ks(nv, Counted(3e3)), qr(4 * nv),
+        x(3 * nv), v(3 * nv), vl(3 * nv), q(4 * nv);
+    std::vector<uint32_t> fl = {HAS_NEXT | HAS_NEXT_ORIENTATION, HAS_PREV | HAS_NEXT | HAS_NEXT_ORIENTATION,
+                                HAS_PREV | HAS_NEXT, HAS_PREV};
+    for (int i = 0; i < nv; i++) {
+        x[3 * i] = 2e-3 * i;
+        x[3 * i + 1] = 1e-4 * i * i;
+        q[4 * i + 3] = 1.0;
+        qr[4 * i + 3] = 1e-6;
+        qr[4 * i + 2] = 1e-7;
+    }
+    oracle_params prm{};
+    prm.damping = 1e-6f;
+    prm.acceleration_ratio = 1.f;
+    prm.velocity_decay = 0.05f;
+    StepCtx<Counted> c;
+    c.p = &prm;
+    c.nv = nv;
+    c.im = im.data();
+    c.lr = lr.data();
+    c.ks = ks.data();
+    c.fl = fl.data();
+    c.qr = qr.data();
+    c.x = x.data();
+    c.v = v.data();
+    c.vl = vl.data();
+    c.q = q.data();
+    c.y.assign(3 * nv, Counted(1e-5));
+    c.dx.assign(3 * nv, Counted(2e-5));
+    Counted::ops = 0;
+    positionUpdate<Counted>(c, c.dx.data(), 1, Counted(1.0 / 120));
+    *position_ops = Counted::ops;
+    Counted::ops = 0;
+    quaternionUpdate<Counted>(c, q.data(), 1);
+    *orientation_ops = Counted::ops;
 }
 
 }  // extern "C"

@@ -91,6 +91,8 @@ def load():
         lib.oracle_resample_cmr.restype = ctypes.c_int64
         lib.oracle_resample_cmr.argtypes = [ctypes.c_void_p, ctypes.c_int32, ctypes.c_double, ctypes.c_void_p,
                                             ctypes.c_int64]
+        lib.oracle_flop_count.restype = None
+        lib.oracle_flop_count.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
         lib.oracle_sdf_points_f64.restype = ctypes.c_int
         lib.oracle_sdf_points_f64.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                               ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
@@ -275,3 +277,13 @@ def resample_cmr(points, target):
     if n < 0:
         raise ValueError("a strand needs at least 4 points")
     return out[:min(n, cap)].copy()
+
+
+def flop_count():
+    """(position, orientation) FLOPs of one update of the reference algorithm -- cosseratItr for an
+    interior vertex and quaternionLambdaItr for a segment with both neighbours -- counted by running
+    the oracle's templated updates on an op-counting scalar (+ - * / sqrt count one; an FMA two)."""
+    lib = load()
+    a, b = ctypes.c_int64(), ctypes.c_int64()
+    lib.oracle_flop_count(ctypes.byref(a), ctypes.byref(b))
+    return a.value, b.value

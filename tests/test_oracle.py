@@ -293,3 +293,17 @@ def test_sdf_pass_matches_reference_fixture(name):
     s.advance(1e-3)  # zero velocity, zero gravity: positions unchanged, then the SDF pass
     assert np.mean(np.any(ref[f"sdf_{name}_pout"] != p, axis=1)) > 0.01
     np.testing.assert_allclose(s.x, ref[f"sdf_{name}_pout"], atol=1e-6)
+
+
+def test_flop_count_pins_the_roofline_constant():
+    # the FP32 roofline in bench.py divides by the reference algorithm's FLOPs per vertex-iteration;
+    # the constant there must be the oracle's count
+    import ast
+    import os
+
+    pos, ori = orc.flop_count()
+    assert (pos, ori) == (242, 250)
+    src = open(os.path.join(os.path.dirname(os.path.dirname(__file__)), "bench.py")).read()
+    consts = {n.targets[0].id: n.value.value for n in ast.parse(src).body
+              if isinstance(n, ast.Assign) and isinstance(n.targets[0], ast.Name) and isinstance(n.value, ast.Constant)}
+    assert consts["REFERENCE_FLOP_PER_VERTEX_ITER"] == pos + ori
