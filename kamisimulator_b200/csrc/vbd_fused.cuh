@@ -24,13 +24,19 @@ __device__ __forceinline__ float sqrt_nonneg(float x) { return x * rsqrtf(fmaxf(
 // another strand (no segment in between: hn / hp false) are replaced by the vertex's own values
 // before they meet their zero coefficient, and vertices that do not move (upd false) keep dx, so a
 // non-finite strand cannot leak into the strands or padding that share its tile, as the
-// reference's flag tests guarantee.
+// reference's flag tests guarantee.  Strands start at even tile positions, so only the previous
+// neighbour of an even slot and the next neighbour of an odd slot can belong to another strand;
+// the others are the same strand or padding (always finite), and guard_next / guard_prev say
+// which operands need the replacement (the results are the same bit for bit either way).
 __device__ __forceinline__ float3 fused_position(float3 dx, float3 F0, float ddN, float kkN, float3 d3N, float3 dxN,
                                                  float ddP, float kkP, float3 d3P, float3 dxP, float as_, float isA,
-                                                 float isD, bool hn, bool hp, bool upd) {
-    dxN = hn ? dxN : dx;
-    dxP = hp ? dxP : dx;
-    d3P = hp ? d3P : d3N;
+                                                 float isD, bool hn, bool hp, bool upd, bool guard_next,
+                                                 bool guard_prev) {
+    if (guard_next) dxN = hn ? dxN : dx;
+    if (guard_prev) {
+        dxP = hp ? dxP : dx;
+        d3P = hp ? d3P : d3N;
+    }
     float3 f;
     f.x = F0.x + ddN * dxN.x + ddP * dxP.x - as_ * dx.x - kkN * d3N.x + kkP * d3P.x;
     f.y = F0.y + ddN * dxN.y + ddP * dxP.y - as_ * dx.y - kkN * d3N.y + kkP * d3P.y;
@@ -42,13 +48,14 @@ __device__ __forceinline__ float3 fused_position(float3 dx, float3 F0, float ddN
 }
 
 // One orientation update (quaternionLambdaItr), branch-free: pre/nxt say whether the previous /
-// next segment exists, upd whether this segment is updated at all.
+// next segment exists, upd whether this segment is updated at all; guard_prev / guard_next as in
+// fused_position.
 __device__ __forceinline__ float4 fused_orientation(float4 q, bool upd, bool pre, bool nxt, float3 Ve, float m2k,
                                                     float3 dx, float3 dxN, float4 qPrev, float4 qrPrev, float4 qNext,
-                                                    float4 qr) {
+                                                    float4 qr, bool guard_prev, bool guard_next) {
     const float3 V = Ve + m2k * (dxN - dx);
-    qPrev = pre ? qPrev : q;  // operands from another strand never meet arithmetic
-    qNext = nxt ? qNext : q;
+    if (guard_prev) qPrev = pre ? qPrev : q;  // operands from another strand never meet arithmetic
+    if (guard_next) qNext = nxt ? qNext : q;
     const float4 P1 = qmul(qPrev, qrPrev);
     const float4 P2 = qmul_conj(qNext, qr);
     float s1 = dot4(q, P1) > 0.f ? 1.f : -1.f;
@@ -133,12 +140,16 @@ __device__ __forceinline__ float2 sqrt_nonneg2(float2 x) {
 }
 
 // fused_position for a pair of same-colour slots; nkkN = -kkN, nas = -(a + s) are precomputed.
+// guard_next / guard_prev as in fused_position (even pair: previous; odd pair: next).
 __device__ __forceinline__ F2x3 fused_position2(F2x3 dx, F2x3 F0, float2 ddN, float2 nkkN, F2x3 d3N, F2x3 dxN,
                                                 float2 ddP, float2 kkP, F2x3 d3P, F2x3 dxP, float2 nas, float2 isA,
-                                                float2 isD, const bool* hn, const bool* hp, const bool* upd) {
-    dxN = sel23(hn[0], hn[1], dxN, dx);
-    dxP = sel23(hp[0], hp[1], dxP, dx);
-    d3P = sel23(hp[0], hp[1], d3P, d3N);
+                                                float2 isD, const bool* hn, const bool* hp, const bool* upd,
+                                                bool guard_next, bool guard_prev) {
+    if (guard_next) dxN = sel23(hn[0], hn[1], dxN, dx);
+    if (guard_prev) {
+        dxP = sel23(hp[0], hp[1], dxP, dx);
+        d3P = sel23(hp[0], hp[1], d3P, d3N);
+    }
     F2x3 f;
     f.x = fma2(kkP, d3P.x, fma2(nkkN, d3N.x, fma2(nas, dx.x, fma2(ddP, dxP.x, fma2(ddN, dxN.x, F0.x)))));
     f.y = fma2(kkP, d3P.y, fma2(nkkN, d3N.y, fma2(nas, dx.y, fma2(ddP, dxP.y, fma2(ddN, dxN.y, F0.y)))));
@@ -151,16 +162,16 @@ __device__ __forceinline__ F2x3 fused_position2(F2x3 dx, F2x3 F0, float2 ddN, fl
     return sel23(upd[0], upd[1], n, dx);
 }
 
-// fused_orientation for a pair of same-colour segments
+// fused_orientation for a pair of same-colour segments; guard_prev / guard_next as in fused_position.
 __device__ __forceinline__ F2x4 fused_orientation2(F2x4 q, const bool* upd, const bool* pre, const bool* nxt, F2x3 Ve,
                                                    float2 m2k, F2x3 dx, F2x3 dxN, F2x4 qPrev, F2x4 qrPrev,
-                                                   F2x4 qNext, F2x4 qr) {
+                                                   F2x4 qNext, F2x4 qr, bool guard_prev, bool guard_next) {
     F2x3 V;
     V.x = fma2(m2k, sub2(dxN.x, dx.x), Ve.x);
     V.y = fma2(m2k, sub2(dxN.y, dx.y), Ve.y);
     V.z = fma2(m2k, sub2(dxN.z, dx.z), Ve.z);
-    qPrev = sel24(pre[0], pre[1], qPrev, q);
-    qNext = sel24(nxt[0], nxt[1], qNext, q);
+    if (guard_prev) qPrev = sel24(pre[0], pre[1], qPrev, q);
+    if (guard_next) qNext = sel24(nxt[0], nxt[1], qNext, q);
     const F2x4 P1 = qmul2(qPrev, qrPrev);
     const F2x4 P2 = qmul_conj2(qNext, qr);
     const float2 d1 = dot42(q, P1), d2 = dot42(q, P2);
@@ -345,18 +356,18 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                 const F2x3 dxPA = pack3(shfl_up3(hi3(dxB), 1), lo3(dxB));
                 const F2x3 d3PA = pack3(shfl_up3(hi3(d3B), 1), lo3(d3B));
                 dxA = fused_position2(dxA, F0A, ddNA, nkkNA, d3A, dxB, ddPA, kkPA, d3PA, dxPA, nasA, isAA, isDA, hnA,
-                                      hpA, mvA);
+                                      hpA, mvA, false, true);
                 // positions, odd slots
                 const F2x3 dxNB = pack3(hi3(dxA), shfl_down3(lo3(dxA), 1));
                 dxB = fused_position2(dxB, F0B, ddNB, nkkNB, d3B, dxNB, ddNA, kkPB, d3A, dxA, nasB, isAB, isDB, hnB, hpB,
-                                      mvB);
+                                      mvB, true, false);
                 // orientations, even segments
                 const F2x4 qPA = pack4(shfl_up4(hi4(qB), 1), lo4(qB));
-                qA = fused_orientation2(qA, uoA, hpA, nxA, VeA, m2kA, dxA, dxB, qPA, qrPA, qB, qrA);
+                qA = fused_orientation2(qA, uoA, hpA, nxA, VeA, m2kA, dxA, dxB, qPA, qrPA, qB, qrA, true, false);
                 d3A = d3_of2(qA);
                 // orientations, odd segments
                 const F2x4 qNB = pack4(hi4(qA), shfl_down4(lo4(qA), 1));
-                qB = fused_orientation2(qB, uoB, hpB, nxB, VeB, m2kB, dxB, dxNB, qA, qrA, qNB, qrB);
+                qB = fused_orientation2(qB, uoB, hpB, nxB, VeB, m2kB, dxB, dxNB, qA, qrA, qNB, qrB, false, true);
                 d3B = d3_of2(qB);
             }
             dx[0] = lo3(dxA);
@@ -378,7 +389,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                         const int kp = k > 0 ? k - 1 : 0;
                         dx[k] = fused_position(dx[k], F0[k], ddN[k], kkN[k], d3[k], dx[k + 1], k ? ddN[kp] : ddH,
                                                k ? kkN[kp] : kkH, k ? d3[kp] : d3P, k ? dx[kp] : dxP, as_[k], isA[k],
-                                               isD[k], fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k]);
+                                               isD[k], fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k], false, true);
                     }
                 }
                 // positions, odd slots
@@ -388,7 +399,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     const int kn = k + 1 < C ? k + 1 : k;
                     dx[k] = fused_position(dx[k], F0[k], ddN[k], kkN[k], d3[k], k == C - 1 ? dxN0 : dx[kn], ddN[k - 1],
                                            kkN[k - 1], d3[k - 1], dx[k - 1], as_[k], isA[k], isD[k],
-                                           fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k]);
+                                           fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k], true, false);
                 }
                 // orientations, even segments
 #pragma unroll
@@ -397,7 +408,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     const uint32_t f = fl[k];
                     q[k] = fused_orientation(q[k], (f & F_HAS_NEXT) && !(f & F_FIX_ORIENTATION), f & F_HAS_PREV,
                                              f & F_HAS_NEXT_ORIENTATION, Ve[k], -2.f * kk[k], dx[k], dx[k + 1],
-                                             k ? q[kp] : qP, k ? qr[kp] : qrH, q[k + 1], qr[k]);
+                                             k ? q[kp] : qP, k ? qr[kp] : qrH, q[k + 1], qr[k], true, false);
                     d3[k] = d3_of(q[k]);
                 }
                 // orientations, odd segments
@@ -409,7 +420,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     q[k] = fused_orientation(q[k], (f & F_HAS_NEXT) && !(f & F_FIX_ORIENTATION), f & F_HAS_PREV,
                                              f & F_HAS_NEXT_ORIENTATION, Ve[k], -2.f * kk[k], dx[k],
                                              k == C - 1 ? dxN0 : dx[kn], q[k - 1], qr[k - 1],
-                                             k == C - 1 ? qN0 : q[kn], qr[k]);
+                                             k == C - 1 ? qN0 : q[kn], qr[k], false, true);
                     d3[k] = d3_of(q[k]);
                 }
                 qP = shfl_up4(q[C - 1], 1);
@@ -432,7 +443,8 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     const int kp = k > 0 ? k - 1 : 0, kn = k + 1 < C ? k + 1 : k;
                     nd[k] = fused_position(dx[k], F0[k], ddN[k], kkN[k], d3[k], k == C - 1 ? dxN0 : dx[kn],
                                            k ? ddN[kp] : ddH, k ? kkN[kp] : kkH, k ? d3[kp] : d3P, k ? dx[kp] : dxP,
-                                           as_[k], isA[k], isD[k], fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k]);
+                                           as_[k], isA[k], isD[k], fl[k] & F_HAS_NEXT, fl[k] & F_HAS_PREV, mov[k],
+                                           (k & 1) != 0, (k & 1) == 0);
                 }
 #pragma unroll
                 for (int k = 0; k < C; k++) dx[k] = nd[k];
@@ -447,7 +459,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     nq[k] = fused_orientation(q[k], (f & F_HAS_NEXT) && !(f & F_FIX_ORIENTATION), f & F_HAS_PREV,
                                               f & F_HAS_NEXT_ORIENTATION, Ve[k], -2.f * kk[k], dx[k],
                                               k == C - 1 ? dxN1 : dx[kn], k ? q[kp] : qP, k ? qr[kp] : qrH,
-                                              k == C - 1 ? qN0 : q[kn], qr[k]);
+                                              k == C - 1 ? qN0 : q[kn], qr[k], (k & 1) == 0, (k & 1) != 0);
                 }
 #pragma unroll
                 for (int k = 0; k < C; k++) {

@@ -207,17 +207,24 @@ def test_nonfinite_input_raises_status():
     s.close()
 
 
-@pytest.mark.parametrize("form", ["fused", "sweep"])
+@pytest.mark.parametrize("form,tuning,schedule", [
+    ("sweep", None, "colour2"), ("fused", None, "colour2"), ("fused", (2, 4, 8, 120), "colour2"),
+    ("fused", (4, 4, 8, 1), "colour2"), ("fused", (4, 4, 8, 2), "colour2"), ("fused", (4, 4, 8, 1), "jacobi"),
+    ("fused", (2, 4, 8, 120), "jacobi")])
 @pytest.mark.parametrize("pin_roots", [True, False])
-def test_nonfinite_strand_does_not_leak(form, pin_roots):
+def test_nonfinite_strand_does_not_leak(form, tuning, schedule, pin_roots):
     """A strand that turns non-finite leaves every other strand untouched (bit for bit), as the
-    reference's per-vertex flag tests guarantee; strands are packed several per tile here."""
+    reference's per-vertex flag tests guarantee; strands are packed several per tile here, and with
+    4 slots per lane several per lane, for every kernel variant."""
     from kamisimulator_b200.vbd import KamiError
 
     g = helpers.soft_groom(64, (5, 30), seed=17)
-    st = helpers.soft_settings(pin_roots=pin_roots)
+    st = helpers.soft_settings(pin_roots=pin_roots, schedule=schedule)
     clean = helpers.gpu_solver(g, st, form=form)
     bad = helpers.gpu_solver(g, st, form=form)
+    if tuning is not None:
+        clean.set_tuning(*tuning)
+        bad.set_tuning(*tuning)
     victim = 10
     a, b = g.strand_begin[victim], g.strand_begin[victim + 1]
     x = g.positions.copy()
