@@ -72,8 +72,8 @@ __device__ __forceinline__ OrientationAdjoint orientation_adjoint(float4 qbar, f
     const float3 V = m2k * (e + (dxN - dx));
     qPrev = pre ? qPrev : q;
     qNext = nxt ? qNext : q;
-    const float4 P1 = qmul(qPrev, qrPrev);
-    const float4 P2 = qmul_conj(qNext, qr);
+    const float4 P1 = qmul_fma(qPrev, qrPrev);  // as the forward step rounds them
+    const float4 P2 = qmul_conj_fma(qNext, qr);
     float s1 = dot4(q, P1) > 0.f ? 1.f : -1.f;
     float s2 = dot4(q, P2) > 0.f ? 1.f : -1.f;
     s1 = pre ? s1 : 0.f;
@@ -108,8 +108,8 @@ __device__ __forceinline__ OrientationAdjoint orientation_adjoint(float4 qbar, f
     if (nb > 0.f) bb = add4(bb, scale4(lb / nb, b));
     const float4 P1b = scale4(s1, bb), P2b = scale4(s2, bb);
     o.p1bar = P1b;
-    o.q_next = qmul(P2b, qr);         // d/d qNext of qNext conj(qr)
-    o.gqr = qmul(qconj(P2b), qNext);  // d/d qr of qNext conj(qr)
+    o.q_next = qmul_fma(P2b, qr);         // d/d qNext of qNext conj(qr)
+    o.gqr = qmul_fma(qconj(P2b), qNext);  // d/d qr of qNext conj(qr)
     o.vt = m2k * Vb;
     return o;
 }
@@ -321,8 +321,8 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
 #pragma unroll
             for (int j = 0; j < C; j += 2) {
                 const float4 P = p1b[j + 1];
-                gq[j] = add4(gq[j], qmul_conj(P, qr[j]));
-                gqr[j] = add4(gqr[j], qmul(qconj(qn[j]), P));
+                gq[j] = add4(gq[j], qmul_conj_fma(P, qr[j]));
+                gqr[j] = add4(gqr[j], qmul_fma(qconj(qn[j]), P));
                 gq[j] = add4(gq[j], j ? tq[j > 0 ? j - 1 : 0] : tq0);
                 gdx[j] = gdx[j] + (j ? tv[j > 0 ? j - 1 : 0] : tv0);
             }
@@ -354,8 +354,8 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
                 gq[j] = add4(gq[j], tq[j - 1]);
                 gdx[j] = gdx[j] + tv[j - 1];
                 const float4 P = j == C - 1 ? pN : p1b[jn];
-                gq[j] = add4(gq[j], qmul_conj(P, qr[j]));
-                gqr[j] = add4(gqr[j], qmul(qconj(qo[j]), P));
+                gq[j] = add4(gq[j], qmul_conj_fma(P, qr[j]));
+                gqr[j] = add4(gqr[j], qmul_fma(qconj(qo[j]), P));
             }
         }
         float3 fb[C];
