@@ -309,8 +309,10 @@ kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float*
 /* Tile shape: slots per lane C (even, >= the longest strand / 32; changing it moves the state to the
  * new tiles), warps per CTA (1, 2, 4, 8), steps per launch for kami_vbd_step_n (1..1024) and the
  * variant of the fused kernel (register_cap: 1 = plain; 120 = at most 120 registers, C = 2 only: 17
- * instead of 16 warps per SM; 2 = packed FP32x2, C = 4 and colour2 only: each lane updates its two
- * same-colour slots with one paired instruction per operation).  0 leaves a value unchanged. */
+ * instead of 16 warps per SM; 168 = at most 168 registers, C = 4 only: 12 instead of 8 warps per SM;
+ * 2 = packed FP32x2, C = 4 and colour2 only: each lane updates its two same-colour slots with one
+ * paired instruction per operation; a cap for the other C runs the plain kernel).  0 leaves a value
+ * unchanged. */
 kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32_t warps_per_block,
                                 int32_t steps_per_launch, int32_t register_cap);
 kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int32_t* warps_per_block,

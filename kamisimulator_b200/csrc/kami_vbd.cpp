@@ -92,7 +92,7 @@ struct kami_vbd_solver {
 
     // multi-step launches (kami_vbd_step_n) and tuning
     int steps_per_launch = 8;
-    int reg_cap = 0;  // 0: fused kernel without a register cap; 120: the 120-register variant (C = 2)
+    int reg_cap = 0;  // 0: fused kernel without a register cap; 120 / 168: the capped variants (C = 2 / 4); 2: packed
     StepParams* d_steps = nullptr;
     int d_steps_cap = 0;
     std::vector<StepParams> h_steps;
@@ -1071,8 +1071,9 @@ kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32
         h->steps_per_launch = steps_per_launch;
     }
     if (register_cap != 0) {
-        if (register_cap != 1 && register_cap != 2 && register_cap != 120)
-            return fail(KAMI_ERR_INVALID_ARGUMENT, "register_cap must be 0 (unchanged), 1 (none), 2 (packed x2) or 120");
+        if (register_cap != 1 && register_cap != 2 && register_cap != 120 && register_cap != 168)
+            return fail(KAMI_ERR_INVALID_ARGUMENT,
+                        "register_cap must be 0 (unchanged), 1 (none), 2 (packed x2), 120 or 168");
         if (register_cap == 2 && (h->layout.C != 4 || h->schedule != KAMI_SCHEDULE_COLOUR2))
             return fail(KAMI_ERR_UNSUPPORTED, "the packed FP32x2 variant runs the colour2 step with 4 slots per lane");
         const int cap = register_cap == 1 ? 0 : register_cap;
@@ -1168,9 +1169,10 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
     int pick[4] = {h->layout.C, h->warps_per_block, h->steps_per_launch, h->reg_cap ? h->reg_cap : 1};
     const bool colour2 = h->schedule == KAMI_SCHEDULE_COLOUR2;
     for (int C = cmin; C <= 4 && st == KAMI_OK; C += 2) {
-        // kernel variants: C = 2 plain or 120 registers; C = 4 plain or packed FP32x2 (colour2)
-        for (int R = 0; R < (C == 2 || colour2 ? 2 : 1) && st == KAMI_OK; R++) {
-        const int cap = R ? (C == 2 ? 120 : 2) : 1;
+        // kernel variants: C = 2 plain or 120 registers; C = 4 plain, 168 registers or packed FP32x2 (colour2)
+        const int caps[3] = {1, C == 2 ? 120 : 168, 2};
+        for (int R = 0; R < (C == 4 && colour2 ? 3 : 2) && st == KAMI_OK; R++) {
+        const int cap = caps[R];
         for (int W = 1; W <= 8 && st == KAMI_OK; W *= 2) {
             for (int fi = 0; fi < 3 && st == KAMI_OK; fi++) {
                 const int F = std::min(Fs[fi], trial_steps);

@@ -580,6 +580,14 @@ __global__ void __maxnreg__(120) fused_frame_kernel_r120(DeviceState st, PhysPar
     fused_frame<C, JACOBI, false>(st, pp, sp, sdf, hio);
 }
 
+// The step with 4 slots per lane at most 168 registers per thread (a few bytes of spills): 12 instead
+// of 8 warps share an SM, which hides more of the colour sweeps' dependency latency.
+template <int C, bool JACOBI>
+__global__ void __maxnreg__(168) fused_step_kernel_r168(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                       TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
+    fused_step_body<C, JACOBI, false>(st, pp, sp, sdf, tp, steps, nsteps);
+}
+
 // The same step with at most 120 registers per thread, so 17 warps (instead of 16) share an SM: a
 // launch whose tile count is just above a multiple of 16 warps per SM then needs one wave less.
 template <int C, bool JACOBI>

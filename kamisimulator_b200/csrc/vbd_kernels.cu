@@ -268,6 +268,13 @@ cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const
         fused_step_kernel_x2<4><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, TapeView{}, d_steps, nsteps);
         return cudaGetLastError();
     }
+    if (reg_cap == 168 && C == 4) {
+        if (jacobi)
+            fused_step_kernel_r168<4, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, TapeView{}, d_steps, nsteps);
+        else
+            fused_step_kernel_r168<4, false><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, TapeView{}, d_steps, nsteps);
+        return cudaGetLastError();
+    }
     if (reg_cap == 120 && C == 2) {
         if (jacobi)
             fused_step_kernel_r120<2, true><<<blocks, threads, 0, s>>>(st, pp, sp, sdf, TapeView{}, d_steps, nsteps);

@@ -73,7 +73,7 @@ def test_autotune_picks_a_shape_and_restores_the_state():
     s.step(1 / 120)
     before = s.get_state()
     best, rate = s.autotune(1 / 120, trial_steps=8)
-    assert best[0] in (4,) and best[1] in (1, 2, 4, 8) and best[2] in (1, 4, 8) and best[3] in (1, 2, 120)
+    assert best[0] in (4,) and best[1] in (1, 2, 4, 8) and best[2] in (1, 4, 8) and best[3] in (1, 2, 120, 168)
     assert rate > 0
     np.testing.assert_array_equal(s.get_state(), before)
     ref = helpers.gpu_solver(g, st, form="fused")
@@ -128,41 +128,51 @@ def test_batch_handle_equals_one_handle_per_groom():
     b.close()
 
 
-def test_packed_x2_variant_matches_the_plain_kernel_and_the_oracle():
-    """register_cap = 2: the colour2 step with 4 slots per lane in packed FP32x2 arithmetic, on
-    uneven strands with the head SDF, against the plain 4-slot kernel and the FP32 oracle."""
+@pytest.mark.parametrize("cap,schedule", [(2, "colour2"), (168, "colour2"), (168, "jacobi")])
+def test_four_slot_variants_match_the_plain_kernel_and_the_oracle(cap, schedule):
+    """register_cap = 2: the colour2 step with 4 slots per lane in packed FP32x2 arithmetic;
+    register_cap = 168: the 4-slot step held to 168 registers.  On uneven strands with the head SDF,
+    against the plain 4-slot kernel and the FP32 oracle.  The Jacobi schedule on these soft, fast rods
+    turns rounding into about 1.2e-5 rad of twist per frame (the FP32 oracle against the FP64 one
+    shows the same), so under Jacobi the oracle check is left to the stiffer parity cases and the
+    variant is held to the plain kernel instead."""
+    from oracle.oracle import twist_angles
     from tests.test_parity_gpu import _lockstep
 
     g = helpers.soft_groom(120, (4, 60), seed=23)
     v = helpers.random_velocities(g, 0.2, seed=2)
-    st = helpers.soft_settings(schedule="colour2", max_h=1 / 120, num_itr=6, sdf=synth.sphere_sdf(64, threshold=2e-3))
+    st = helpers.soft_settings(schedule=schedule, max_h=1 / 120, num_itr=6, sdf=synth.sphere_sdf(64, threshold=2e-3))
     from kamisimulator_b200.vbd import KamiError, Solver
 
     a = Solver(g, form="fused", velocities=v, slots_per_lane=4, **st)
     b = Solver(g, form="fused", velocities=v, slots_per_lane=4, **st)
-    b.set_tuning(register_cap=2)
-    assert b.get_tuning()[3] == 2
+    b.set_tuning(register_cap=cap)
+    assert b.get_tuning()[3] == cap
     for _ in range(6):
         a.step(1 / 60)
         b.step(1 / 60)
     xa, xb = a.get_positions_velocities()[0], b.get_positions_velocities()[0]
     assert np.abs(xa - xb).max() <= 1e-6
+    assert np.abs(twist_angles(a.get_orientations(), b.get_orientations())).max() <= helpers.TWIST_TOL
     c = Solver(g, form="fused", velocities=v, slots_per_lane=2, **st)
-    with pytest.raises(KamiError, match="packed"):
-        c.set_tuning(register_cap=2)
+    if cap == 2:
+        with pytest.raises(KamiError, match="packed"):
+            c.set_tuning(register_cap=2)
     for s in (a, b, c):
         s.close()
+    if schedule == "jacobi":
+        return
     # against the oracle, per frame from shared states
     import kamisimulator_b200.vbd as vbd
 
     orig = vbd.Solver.__init__
 
-    def packed_init(self, *args, **kw):
+    def variant_init(self, *args, **kw):
         kw["slots_per_lane"] = 4
         orig(self, *args, **kw)
-        self.set_tuning(register_cap=2)
+        self.set_tuning(register_cap=cap)
 
-    vbd.Solver.__init__ = packed_init
+    vbd.Solver.__init__ = variant_init
     try:
         ex, et = _lockstep(g, st, "fused", 8, 1 / 60, velocities=v, reseed_each_frame=True)
     finally:

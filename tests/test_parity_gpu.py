@@ -210,6 +210,7 @@ def test_nonfinite_input_raises_status():
 @pytest.mark.parametrize("form,tuning,schedule", [
     ("sweep", None, "colour2"), ("fused", None, "colour2"), ("fused", (2, 4, 8, 120), "colour2"),
     ("fused", (4, 4, 8, 1), "colour2"), ("fused", (4, 4, 8, 2), "colour2"), ("fused", (4, 4, 8, 1), "jacobi"),
+    ("fused", (4, 4, 8, 168), "colour2"), ("fused", (4, 2, 8, 168), "jacobi"),
     ("fused", (2, 4, 8, 120), "jacobi")])
 @pytest.mark.parametrize("pin_roots", [True, False])
 def test_nonfinite_strand_does_not_leak(form, tuning, schedule, pin_roots):
