@@ -306,7 +306,34 @@ def extra_forms(args, torch, stream, flush):
         out["hair_hair_sweep"] = hair_hair_timing(torch, stream)
     except Exception as e:  # a contact-list overflow (KAMI_ERR_CONTACTS) is reported, not fatal
         out["hair_hair_sweep"] = {"error": str(e)}
+    out["long_strands_3k_x200"] = long_strand_timing(torch, stream, flush)
     return out
+
+
+def long_strand_timing(torch, stream, flush, steps=200):
+    """3,000 strands x 200 vertices (longer than a tile of 128 slots), the headline settings: the
+    fused form in groups of 2 tiles (autotuned) against the sweep form, one step per call, L2
+    flushed between timed steps."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.vbd import Solver
+
+    g = synth.groom(3000, 200, seed=9)
+    st = settings()
+    res = {}
+    for form in ("fused", "sweep"):
+        s = Solver(g, form=form, **st)
+        if form == "fused":
+            res["tuning"] = dict(zip(("slots_per_lane", "warps_per_block", "steps_per_launch", "register_cap"),
+                                     s.autotune(DT, trial_steps=8)[0]))
+        for _ in range(3):
+            s.step(DT, stream=stream)
+        n = steps if form == "fused" else steps // 4
+        ms = time_steps(s, n, stream, flush)
+        res[form] = {"value": g.num_vertices * NUM_ITR * n / (ms / 1e3), "ms_per_step": ms / n}
+        s.close()
+    res["what"] = ("3,000 strands x 200 vertices, 20 iterations, dt 1/120 s, head-sphere SDF 128^3: fused form on groups "
+                   "of tiles (a strand runs on across the warps of a CTA) vs the sweep form")
+    return res
 
 
 def sdf_bake_timing():
@@ -611,7 +638,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
-    ap.add_argument("--only", choices=["adjoint", "large", "hairhair", "bake"], help="run a single extra measurement")
+    ap.add_argument("--only", choices=["adjoint", "large", "hairhair", "bake", "long"],
+                    help="run a single extra measurement")
     ap.add_argument("--tuning", help="fixed tile shape C,warps,steps_per_launch,register_cap instead of autotuning")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -630,6 +658,11 @@ def main():
         print(json.dumps(hair_hair_timing(torch, torch.cuda.current_stream())), flush=True)
     elif args.only == "bake":
         print(json.dumps(sdf_bake_timing()), flush=True)
+    elif args.only == "long":
+        import torch
+
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        print(json.dumps(long_strand_timing(torch, torch.cuda.current_stream(), flush)), flush=True)
     elif args.impl == "reference":
         run_reference(args)
     else:

@@ -48,9 +48,11 @@ typedef enum kami_schedule {
 
 /* Which device implementation steps the solver. */
 typedef enum kami_form {
-    KAMI_FORM_AUTO = 0,  /* fused when every strand fits one warp tile, else sweep */
+    KAMI_FORM_AUTO = 0,  /* fused when every strand fits 8 warp tiles of 128 slots (1024 vertices) and
+                            there is no hair-hair collision, else sweep */
     KAMI_FORM_SWEEP = 1, /* one kernel per colour sweep, replayed from a CUDA graph (the plain per-groom form) */
-    KAMI_FORM_FUSED = 2  /* one kernel per step: each warp owns a strand tile for all iterations */
+    KAMI_FORM_FUSED = 2  /* one kernel per step: each warp owns a strand tile for all iterations; strands
+                            longer than a tile run on across the warps of a group of 2-8 tiles */
 } kami_form;
 
 typedef enum kami_stiffness_mode {
@@ -111,7 +113,8 @@ typedef struct kami_vbd_desc {
     const kami_vbd_sdf_desc* sdf; /* NULL: no body collision (EnableSDF false) */
 
     /* Device tile shape (no counterpart in the reference; 0 = automatic).  slots_per_lane: even C,
-     * each warp tile holds 32*C vertex slots (the fused form supports C = 2 and 4);
+     * each warp tile holds 32*C vertex slots (the fused form supports C = 2 and 4, and puts strands
+     * longer than a tile into groups of as many tiles as they need, up to 8);
      * warps_per_block: warps per CTA of the fused kernel. */
     int32_t slots_per_lane;
     int32_t warps_per_block;

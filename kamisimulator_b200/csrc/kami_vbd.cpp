@@ -588,6 +588,14 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
     if (d->warps_per_block < 0 || d->warps_per_block > 32 || (d->warps_per_block & (d->warps_per_block - 1)))
         return bail(fail(KAMI_ERR_INVALID_ARGUMENT, "warps_per_block must be 0 or a power of two <= 32"));
     if (d->warps_per_block > 0) h->warps_per_block = d->warps_per_block;
+    // the fused form runs strands longer than a tile of 4 slots per lane on groups of up to 8 tiles
+    int K = 1;
+    if (!fused_supported(C) && d->slots_per_lane == 0 && tiles_per_group_for(h->strand_begin.data(), h->ns, 4) > 0) {
+        if (d->form != KAMI_FORM_SWEEP && !d->hair_hair) {
+            C = 4;
+            K = tiles_per_group_for(h->strand_begin.data(), h->ns, 4);
+        }
+    }
     int form = d->form;
     if (form == KAMI_FORM_AUTO) form = (fused_supported(C) && !d->hair_hair) ? KAMI_FORM_FUSED : KAMI_FORM_SWEEP;
     if (d->hair_hair) {
@@ -602,9 +610,9 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
                              2.0 * min_seg, 2.0 * d->radius + d->barrier_thickness));
     }
     if (form == KAMI_FORM_FUSED && !fused_supported(C))
-        return bail(fail(KAMI_ERR_UNSUPPORTED, "fused form supports strands of up to 128 vertices"));
+        return bail(fail(KAMI_ERR_UNSUPPORTED, "fused form supports strands of up to 1024 vertices (8 tiles of 128)"));
     h->form = form;
-    if (!pack_tiles(h->strand_begin.data(), h->ns, C, h->layout, err))
+    if (!pack_tiles(h->strand_begin.data(), h->ns, C, h->layout, err, form == KAMI_FORM_FUSED ? K : 1))
         return bail(fail(KAMI_ERR_UNSUPPORTED, "%s", err.c_str()));
     const int64_t S = h->layout.num_slots;
 
@@ -851,7 +859,7 @@ kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
         if (h->form == KAMI_FORM_FUSED) {
             KAMI_CUDA(launch_fused_step(h->dstate(), h->pp, sp, h->sdf, h->layout.C, h->schedule == KAMI_SCHEDULE_JACOBI,
-                                        h->warps_per_block, s, nullptr, 1, h->reg_cap),
+                                        h->warps_per_block, s, nullptr, 1, h->reg_cap, h->layout.K),
                       "fused step launch");
         } else {
             KAMI_TRY(build_sweep_graph(h, steps));
@@ -959,7 +967,7 @@ kami_status kami_vbd_step_host(kami_vbd_handle h, float dt, const float* xyz, co
     if (!std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
     HostIO io{};
     const int64_t n = 3 * h->nv;
-    bool direct = dt > 0.f && h->form == KAMI_FORM_FUSED && !h->hair_hair;
+    bool direct = dt > 0.f && h->form == KAMI_FORM_FUSED && !h->hair_hair && h->layout.K == 1;
     if (direct) {
         io.x_in = mapped_range(xyz, n);
         io.v_in = mapped_range(vxyz, n);
@@ -985,12 +993,15 @@ kami_status kami_vbd_step_host(kami_vbd_handle h, float dt, const float* xyz, co
     return check_status_word(h);
 }
 
-// Moves the live state to tiles of 32*C slots (gathered to boundary order and scattered back).
+// Moves the live state to tiles of 32*C slots (gathered to boundary order and scattered back); the
+// fused form takes groups of as many tiles as the longest strand needs.
 static kami_status relayout(kami_vbd_solver* h, int C) {
     if (C == h->layout.C) return KAMI_OK;
+    const int K = h->form == KAMI_FORM_FUSED ? tiles_per_group_for(h->strand_begin.data(), h->ns, C) : 1;
+    if (K == 0) return fail(KAMI_ERR_UNSUPPORTED, "a strand is longer than 8 tiles of %d slots", 32 * C);
     std::string err;
     TileLayout nl;
-    if (!pack_tiles(h->strand_begin.data(), h->ns, C, nl, err)) return fail(KAMI_ERR_UNSUPPORTED, "%s", err.c_str());
+    if (!pack_tiles(h->strand_begin.data(), h->ns, C, nl, err, K)) return fail(KAMI_ERR_UNSUPPORTED, "%s", err.c_str());
     KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
     const int64_t nv = h->nv, S = nl.num_slots;
     float4* tmp = nullptr;
@@ -1052,10 +1063,12 @@ kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32
         return fail(KAMI_ERR_UNSUPPORTED, "the tile shape of a handle with hair-hair collision is fixed at creation");
     if (slots_per_lane != 0) {
         const int cmin = slots_per_lane_for(h->strand_begin.data(), h->ns);
-        if (slots_per_lane < cmin || (slots_per_lane & 1))
+        if (h->form == KAMI_FORM_FUSED) {  // longer strands take groups of tiles
+            if (!fused_supported(slots_per_lane))
+                return fail(KAMI_ERR_UNSUPPORTED, "the fused form supports 2 or 4 slots per lane");
+        } else if (slots_per_lane < cmin || (slots_per_lane & 1)) {
             return fail(KAMI_ERR_INVALID_ARGUMENT, "slots_per_lane must be even and >= %d", cmin);
-        if (h->form == KAMI_FORM_FUSED && !fused_supported(slots_per_lane))
-            return fail(KAMI_ERR_UNSUPPORTED, "the fused form supports 2 or 4 slots per lane");
+        }
         KAMI_TRY(relayout(h, slots_per_lane));
     }
     if (warps_per_block != 0) {
@@ -1074,8 +1087,9 @@ kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32
         if (register_cap != 1 && register_cap != 2 && register_cap != 120 && register_cap != 168)
             return fail(KAMI_ERR_INVALID_ARGUMENT,
                         "register_cap must be 0 (unchanged), 1 (none), 2 (packed x2), 120 or 168");
-        if (register_cap == 2 && (h->layout.C != 4 || h->schedule != KAMI_SCHEDULE_COLOUR2))
-            return fail(KAMI_ERR_UNSUPPORTED, "the packed FP32x2 variant runs the colour2 step with 4 slots per lane");
+        if (register_cap == 2 && (h->layout.C != 4 || h->layout.K != 1 || h->schedule != KAMI_SCHEDULE_COLOUR2))
+            return fail(KAMI_ERR_UNSUPPORTED,
+                        "the packed FP32x2 variant runs the colour2 step with 4 slots per lane on single tiles");
         const int cap = register_cap == 1 ? 0 : register_cap;
         if (cap != h->reg_cap) drop_graphs(h);
         h->reg_cap = cap;
@@ -1129,7 +1143,7 @@ kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float*
         for (int j0 = 0; j0 < n && err == cudaSuccess; j0 += F)
             err = launch_fused_step(h->dstate(), h->pp, h->h_steps[0], h->sdf, h->layout.C,
                                     h->schedule == KAMI_SCHEDULE_JACOBI, h->warps_per_block, h->stream, h->d_steps + j0,
-                                    std::min(F, n - j0), h->reg_cap);
+                                    std::min(F, n - j0), h->reg_cap, h->layout.K);
         cudaGraph_t g = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
         if (err != cudaSuccess || e2 != cudaSuccess) {
@@ -1168,12 +1182,16 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
     double rate_best = -1.0;
     int pick[4] = {h->layout.C, h->warps_per_block, h->steps_per_launch, h->reg_cap ? h->reg_cap : 1};
     const bool colour2 = h->schedule == KAMI_SCHEDULE_COLOUR2;
-    for (int C = cmin; C <= 4 && st == KAMI_OK; C += 2) {
-        // kernel variants: C = 2 plain or 120 registers; C = 4 plain, 168 registers or packed FP32x2 (colour2)
+    for (int C = std::min(cmin, 4); C <= 4 && st == KAMI_OK; C += 2) {
+        // tiles per group for this C (strands longer than a tile); groups fix the CTA shape
+        const int K = tiles_per_group_for(h->strand_begin.data(), h->ns, C);
+        if (K == 0) continue;
+        // kernel variants: C = 2 plain or 120 registers; C = 4 plain, 168 registers or packed FP32x2
+        // (colour2, single tiles)
         const int caps[3] = {1, C == 2 ? 120 : 168, 2};
-        for (int R = 0; R < (C == 4 && colour2 ? 3 : 2) && st == KAMI_OK; R++) {
+        for (int R = 0; R < (C == 4 && colour2 && K == 1 ? 3 : 2) && st == KAMI_OK; R++) {
         const int cap = caps[R];
-        for (int W = 1; W <= 8 && st == KAMI_OK; W *= 2) {
+        for (int W = 1; W <= (K == 1 ? 8 : 1) && st == KAMI_OK; W *= 2) {
             for (int fi = 0; fi < 3 && st == KAMI_OK; fi++) {
                 const int F = std::min(Fs[fi], trial_steps);
                 st = kami_vbd_set_tuning(h, C, W, F, cap);
@@ -1222,6 +1240,8 @@ static kami_status adjoint_supported(kami_vbd_solver* h) {
     if (h->form != KAMI_FORM_FUSED || h->schedule != KAMI_SCHEDULE_COLOUR2)
         return fail(KAMI_ERR_UNSUPPORTED, "the adjoint covers the fused form with the colour2 schedule");
     if (h->pp.wind_peak != 0.f) return fail(KAMI_ERR_UNSUPPORTED, "the adjoint does not cover wind");
+    if (h->layout.K != 1)
+        return fail(KAMI_ERR_UNSUPPORTED, "the adjoint covers strands of one tile (at most 128 vertices)");
     return KAMI_OK;
 }
 

@@ -5,9 +5,11 @@
 // warp in the fused kernel.  Lane j of a tile owns the C contiguous slots p = j*C .. j*C+C-1 and
 // slot p is stored at index  tile*T + (p % C)*32 + (p / C),  so the warp's access to "its k-th
 // slot" is one fully coalesced 32-element row.  Strands occupy contiguous slot ranges starting
-// at an even slot, never cross a tile, and padding slots carry no flags.  Because every strand
-// starts at an even slot and C is even, the 2-colour class of a slot (its index parity inside
-// the strand) is simply k & 1 (the row parity).
+// at an even slot and padding slots carry no flags.  A strand stays in one tile, or, in a layout
+// of groups of K tiles (fused form, strands longer than a tile), in one group, running on from
+// lane 31's last slot of a tile into lane 0's first slot of the next.  Because every strand starts
+// at an even slot and C is even, the 2-colour class of a slot (its index parity inside the strand)
+// is simply k & 1 (the row parity).
 #pragma once
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -150,20 +152,23 @@ struct CollParams {
 };
 
 // ---- tile slot neighbours ----------------------------------------------------------------------
-// Storage index of slot p+1 / p-1 of the strand slot stored at g (the caller knows it exists).
+// Storage index of slot p+1 / p-1 of the strand slot stored at g (the caller knows it exists).  In
+// a group of tiles a strand runs on from lane 31's last slot of a tile into lane 0's first slot of
+// the next tile.
 __host__ __device__ __forceinline__ int64_t next_slot(int64_t g, int C) {
     const int64_t T = 32LL * C;
     const int64_t tile = g / T;
     const int r = (int)(g - tile * T);
     const int k = r >> 5, lane = r & 31;
-    return (k < C - 1) ? g + 32 : tile * T + lane + 1;
+    return (k < C - 1) ? g + 32 : (lane < 31 ? tile * T + lane + 1 : (tile + 1) * T);
 }
 __host__ __device__ __forceinline__ int64_t prev_slot(int64_t g, int C) {
     const int64_t T = 32LL * C;
     const int64_t tile = g / T;
     const int r = (int)(g - tile * T);
     const int k = r >> 5, lane = r & 31;
-    return (k > 0) ? g - 32 : tile * T + (int64_t)(C - 1) * 32 + lane - 1;
+    return (k > 0) ? g - 32
+                   : (lane > 0 ? tile * T + (int64_t)(C - 1) * 32 + lane - 1 : (tile - 1) * T + (int64_t)(C - 1) * 32 + 31);
 }
 
 // ---- small helpers ---------------------------------------------------------------------------

@@ -214,6 +214,18 @@ __device__ __forceinline__ F2x4 fused_orientation2(F2x4 q, const bool* upd, cons
     return sel24(upd[0], upd[1], n, q);
 }
 
+// Values a group's warps hand across their tile boundaries (GROUPED: one CTA of K <= 8 warps per
+// group of K tiles, warp w on tile group * K + w): `up` from lane 31 of warp w to lane 0 of warp
+// w + 1 (its previous lane), `down` from lane 0 of warp w to lane 31 of warp w - 1 (its next lane).
+// Each slot is written once per substep or iteration and read after the __syncthreads that follows;
+// the next write to it comes after at least one more __syncthreads, which every reader has passed.
+enum : int { XU_QR, XU_DK, XU_E, XU_DX, XU_Q, XU_D3, XU_N };
+enum : int { XD_X, XD_DX, XD_Q, XD_DX2, XD_N };
+struct GroupExchange {
+    float4 up[8][XU_N];
+    float4 down[8][XD_N];
+};
+
 // One launch runs `nsteps` consecutive steps, step j with clock and body transform steps[j] (or
 // `sp` when steps is null), keeping the tile's state in registers between them.  RECORD (colour2,
 // one step of one substep) additionally writes the step's start state and the iterates to a tape
@@ -221,10 +233,11 @@ __device__ __forceinline__ F2x4 fused_orientation2(F2x4 q, const bool* upd, cons
 // `stage` holds the tile's positions then velocities from the host buffers of `hio`, 3 floats per
 // tile position p = lane * C + k, and the step writes its results back to the host buffers
 // through the same area, as well as to the device state.
-template <int C, bool JACOBI, bool RECORD, bool PAIRED = false, bool HOSTIO = false>
+template <int C, bool JACOBI, bool RECORD, bool PAIRED = false, bool HOSTIO = false, bool GROUPED = false>
 __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                 TapeView tp, const StepParams* __restrict__ steps, int nsteps,
                                                 HostIO hio = HostIO{}, int64_t frame_tile = 0, float* stage = nullptr) {
+    static_assert(!GROUPED || (!RECORD && !HOSTIO && !PAIRED), "tile groups run the plain step");
     static_assert(!PAIRED || (C == 4 && !JACOBI && !RECORD), "the packed form is the colour2 step with 4 slots per lane");
     static_assert(!(HOSTIO && RECORD), "recorded steps keep their state on the device");
     static_assert(!(RECORD && JACOBI), "the tape records the colour2 schedule");
@@ -232,8 +245,27 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
     const int lane = threadIdx.x & 31;
     const int64_t tile = HOSTIO ? frame_tile
                                 : (RECORD ? tp.tile_begin : 0) + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (tile >= st.num_tiles) return;  // uniform per warp
+    if (tile >= st.num_tiles) return;  // uniform per warp (per CTA for groups: num_tiles is a multiple of K)
     const int64_t base = tile * (32LL * C) + lane;
+    // tile groups: neighbours across the warps of the CTA (see GroupExchange)
+    const int gw = threadIdx.x >> 5, gK = blockDim.x >> 5;
+    GroupExchange* gx = nullptr;
+    if constexpr (GROUPED) {
+        __shared__ GroupExchange group_exchange;
+        gx = &group_exchange;
+    }
+    auto up_put = [&](int slot, float4 v) {
+        if (GROUPED && lane == 31) gx->up[gw][slot] = v;
+    };
+    auto up_get = [&](int slot, float4 v) { return (GROUPED && lane == 0 && gw > 0) ? gx->up[gw - 1][slot] : v; };
+    auto down_put = [&](int slot, float4 v) {
+        if (GROUPED && lane == 0) gx->down[gw][slot] = v;
+    };
+    auto down_get = [&](int slot, float4 v) { return (GROUPED && lane == 31 && gw < gK - 1) ? gx->down[gw + 1][slot] : v; };
+    auto group_sync = [&]() {
+        if (GROUPED) __syncthreads();
+    };
+    auto f4 = [](float3 a) { return make_float4(a.x, a.y, a.z, 0.f); };
 
     float3 x[C], v[C], vl[C], dx[C], d3[C], F0[C], Ve[C];
     float4 q[C], qr[C];
@@ -285,9 +317,18 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
         }
     }
     // constants of the previous lane's last segment (segment i-1 of slot 0)
-    const float4 qrH = shfl_up4(qr[C - 1], 1);
-    const float ddH = __shfl_up_sync(0xffffffffu, ddN[C - 1], 1);
-    const float kkH = __shfl_up_sync(0xffffffffu, kkN[C - 1], 1);
+    float4 qrH = shfl_up4(qr[C - 1], 1);
+    float ddH = __shfl_up_sync(0xffffffffu, ddN[C - 1], 1);
+    float kkH = __shfl_up_sync(0xffffffffu, kkN[C - 1], 1);
+    if (GROUPED) {
+        up_put(XU_QR, qr[C - 1]);
+        up_put(XU_DK, make_float4(ddN[C - 1], kkN[C - 1], 0.f, 0.f));
+        group_sync();
+        qrH = up_get(XU_QR, qrH);
+        const float4 dk = up_get(XU_DK, make_float4(ddH, kkH, 0.f, 0.f));
+        ddH = dk.x;
+        kkH = dk.y;
+    }
 
     const float accel = pp.accel_ratio;
     bool bad = false;
@@ -301,10 +342,21 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
             float3 e[C];
 #pragma unroll
             for (int k = 0; k < C - 1; k++) e[k] = x[k + 1] - x[k];
-            e[C - 1] = shfl_down3(x[0], 1) - x[C - 1];
+            float3 xN0 = shfl_down3(x[0], 1);
+            if (GROUPED) {
+                down_put(XD_X, f4(x[0]));
+                group_sync();
+                xN0 = xyz(down_get(XD_X, f4(xN0)));
+            }
+            e[C - 1] = xN0 - x[C - 1];
 #pragma unroll
             for (int k = 0; k < C; k++) e[k] = (fl[k] & F_HAS_NEXT) ? e[k] : f3(0.f, 0.f, 0.f);
-            const float3 eH = shfl_up3(e[C - 1], 1);
+            float3 eH = shfl_up3(e[C - 1], 1);
+            if (GROUPED) {
+                up_put(XU_E, f4(e[C - 1]));
+                group_sync();
+                eH = xyz(up_get(XU_E, f4(eH)));
+            }
 #pragma unroll
             for (int k = 0; k < C; k++) {
                 float3 y;
@@ -395,9 +447,18 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
         } else {  // (braced: an unbraced discarded `else for` also dropped the loop after it)
         for (int it = 0; it < pp.num_itr; it++) {
             if (!JACOBI) {
+                float3 dxP = shfl_up3(dx[C - 1], 1);
+                if (GROUPED) {  // the previous lane's odd values, unchanged until the odd sweeps
+                    up_put(XU_DX, f4(dx[C - 1]));
+                    up_put(XU_Q, q[C - 1]);
+                    up_put(XU_D3, f4(d3[C - 1]));
+                    group_sync();
+                    dxP = xyz(up_get(XU_DX, f4(dxP)));
+                    qP = up_get(XU_Q, qP);
+                    d3P = xyz(up_get(XU_D3, f4(d3P)));
+                }
                 // positions, even slots (neighbours are odd: own registers or the previous lane)
                 {
-                    const float3 dxP = shfl_up3(dx[C - 1], 1);
 #pragma unroll
                     for (int k = 0; k < C; k += 2) {
                         const int kp = k > 0 ? k - 1 : 0;
@@ -407,7 +468,12 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     }
                 }
                 // positions, odd slots
-                const float3 dxN0 = shfl_down3(dx[0], 1);
+                float3 dxN0 = shfl_down3(dx[0], 1);
+                if (GROUPED) {
+                    down_put(XD_DX, f4(dx[0]));
+                    group_sync();
+                    dxN0 = xyz(down_get(XD_DX, f4(dxN0)));
+                }
 #pragma unroll
                 for (int k = 1; k < C; k += 2) {
                     const int kn = k + 1 < C ? k + 1 : k;
@@ -426,7 +492,12 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                     d3[k] = d3_of(q[k]);
                 }
                 // orientations, odd segments
-                const float4 qN0 = shfl_down4(q[0], 1);
+                float4 qN0 = shfl_down4(q[0], 1);
+                if (GROUPED) {
+                    down_put(XD_Q, q[0]);
+                    group_sync();
+                    qN0 = down_get(XD_Q, qN0);
+                }
 #pragma unroll
                 for (int k = 1; k < C; k += 2) {
                     const int kn = k + 1 < C ? k + 1 : k;
@@ -449,8 +520,19 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                 }
             } else {
                 // positions, every slot from the previous sweep
-                const float3 dxP = shfl_up3(dx[C - 1], 1);
-                const float3 dxN0 = shfl_down3(dx[0], 1);
+                float3 dxP = shfl_up3(dx[C - 1], 1);
+                float3 dxN0 = shfl_down3(dx[0], 1);
+                if (GROUPED) {
+                    up_put(XU_DX, f4(dx[C - 1]));
+                    up_put(XU_Q, q[C - 1]);
+                    up_put(XU_D3, f4(d3[C - 1]));
+                    down_put(XD_DX, f4(dx[0]));
+                    group_sync();
+                    dxP = xyz(up_get(XU_DX, f4(dxP)));
+                    qP = up_get(XU_Q, qP);
+                    d3P = xyz(up_get(XU_D3, f4(d3P)));
+                    dxN0 = xyz(down_get(XD_DX, f4(dxN0)));
+                }
                 float3 nd[C];
 #pragma unroll
                 for (int k = 0; k < C; k++) {
@@ -463,8 +545,15 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
 #pragma unroll
                 for (int k = 0; k < C; k++) dx[k] = nd[k];
                 // orientations, every segment from the previous sweep
-                const float3 dxN1 = shfl_down3(dx[0], 1);
-                const float4 qN0 = shfl_down4(q[0], 1);
+                float3 dxN1 = shfl_down3(dx[0], 1);
+                float4 qN0 = shfl_down4(q[0], 1);
+                if (GROUPED) {
+                    down_put(XD_DX2, f4(dx[0]));
+                    down_put(XD_Q, q[0]);
+                    group_sync();
+                    dxN1 = xyz(down_get(XD_DX2, f4(dxN1)));
+                    qN0 = down_get(XD_Q, qN0);
+                }
                 float4 nq[C];
 #pragma unroll
                 for (int k = 0; k < C; k++) {
@@ -586,6 +675,24 @@ template <int C, bool JACOBI>
 __global__ void __maxnreg__(168) fused_step_kernel_r168(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                        TapeView tp, const StepParams* __restrict__ steps, int nsteps) {
     fused_step_body<C, JACOBI, false>(st, pp, sp, sdf, tp, steps, nsteps);
+}
+
+// The step over groups of K tiles (strands longer than a tile): one CTA of K warps per group, plain
+// and with the register caps of the single-tile variants.
+template <int C, bool JACOBI>
+__global__ void __launch_bounds__(256) fused_group_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                          const StepParams* __restrict__ steps, int nsteps) {
+    fused_step_body<C, JACOBI, false, false, false, true>(st, pp, sp, sdf, TapeView{}, steps, nsteps);
+}
+template <int C, bool JACOBI>
+__global__ void __maxnreg__(120) fused_group_kernel_r120(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                        const StepParams* __restrict__ steps, int nsteps) {
+    fused_step_body<C, JACOBI, false, false, false, true>(st, pp, sp, sdf, TapeView{}, steps, nsteps);
+}
+template <int C, bool JACOBI>
+__global__ void __maxnreg__(168) fused_group_kernel_r168(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
+                                                        const StepParams* __restrict__ steps, int nsteps) {
+    fused_step_body<C, JACOBI, false, false, false, true>(st, pp, sp, sdf, TapeView{}, steps, nsteps);
 }
 
 // The same step with at most 120 registers per thread, so 17 warps (instead of 16) share an SM: a

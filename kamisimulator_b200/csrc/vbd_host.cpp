@@ -17,22 +17,33 @@ int slots_per_lane_for(const int32_t* sb, int32_t ns) {
     return std::max(C, 2);
 }
 
-bool pack_tiles(const int32_t* sb, int32_t ns, int C, TileLayout& out, std::string& err) {
-    const int T = 32 * C;
+int tiles_per_group_for(const int32_t* sb, int32_t ns, int C) {
+    int32_t longest = 0;
+    for (int32_t s = 0; s < ns; s++) longest = std::max(longest, sb[s + 1] - sb[s]);
+    longest += longest & 1;
+    for (int K = 1; K <= 8; K *= 2)
+        if (longest <= 32 * C * K) return K;
+    return 0;
+}
+
+bool pack_tiles(const int32_t* sb, int32_t ns, int C, TileLayout& out, std::string& err, int K) {
+    const int Tt = 32 * C;  // slots per tile
+    const int T = Tt * K;   // positions per group
     out.C = C;
+    out.K = K;
     out.slot_of.assign(ns > 0 ? (size_t)sb[ns] : 0, -1);
     std::vector<int32_t> order(ns);
     std::iota(order.begin(), order.end(), 0);
     auto need = [&](int32_t s) { int n = sb[s + 1] - sb[s]; return n + (n & 1); };
     std::stable_sort(order.begin(), order.end(), [&](int32_t a, int32_t b) { return need(a) > need(b); });
-    // open tiles bucketed by free slots; each bucket is a stack of tile ids
+    // open groups bucketed by free positions; each bucket is a stack of group ids
     std::vector<std::vector<int64_t>> bucket(T + 1);
-    std::vector<int> used;  // slots used per tile
+    std::vector<int> used;  // positions used per group
     for (int32_t s : order) {
         const int n = need(s);
         if (n > T) {
             err = "strand " + std::to_string(s) + " has " + std::to_string(sb[s + 1] - sb[s]) +
-                  " vertices, more than a tile of " + std::to_string(T) + " slots";
+                  " vertices, more than a group of " + std::to_string(T) + " slots";
             return false;
         }
         int64_t tile = -1;
@@ -47,17 +58,17 @@ bool pack_tiles(const int32_t* sb, int32_t ns, int C, TileLayout& out, std::stri
             tile = (int64_t)used.size();
             used.push_back(0);
         }
-        const int p0 = used[tile];
+        const int p0 = used[tile];  // `tile` numbers groups here
         for (int32_t j = 0; j < sb[s + 1] - sb[s]; j++) {
-            const int p = p0 + j;
-            out.slot_of[sb[s] + j] = tile * T + (int64_t)(p % C) * 32 + p / C;
+            const int p = p0 + j, pt = p % Tt;
+            out.slot_of[sb[s] + j] = (tile * K + p / Tt) * Tt + (int64_t)(pt % C) * 32 + pt / C;
         }
         used[tile] += n;
         const int free_slots = T - used[tile];
         if (free_slots >= 2) bucket[free_slots].push_back(tile);
     }
-    out.num_tiles = (int64_t)used.size();
-    out.num_slots = out.num_tiles * T;
+    out.num_tiles = (int64_t)used.size() * K;
+    out.num_slots = out.num_tiles * Tt;
     return true;
 }
 

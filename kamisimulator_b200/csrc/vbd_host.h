@@ -11,16 +11,24 @@ namespace kami {
 // Placement of strands into warp tiles of 32*C slots (see vbd_common.cuh for the slot layout).
 struct TileLayout {
     int C = 2;
+    int K = 1;  // tiles per group: a strand may run on from one tile of its group into the next
     int64_t num_tiles = 0;
     int64_t num_slots = 0;
     std::vector<int64_t> slot_of;  // storage index of each boundary-order vertex
 };
 
-// Packs strands (CSR offsets sb[0..ns]) into tiles of 32*C slots.  Each strand takes a
-// contiguous run of slots starting at an even slot (its length rounded up to even).  Strands are
-// placed longest first into the fullest tile that still has room (best fit decreasing), so
-// uneven strands share tiles.  Returns false when a strand is longer than a tile.
-bool pack_tiles(const int32_t* sb, int32_t ns, int C, TileLayout& out, std::string& err);
+// Packs strands (CSR offsets sb[0..ns]) into groups of K tiles of 32*C slots.  A group's positions
+// p = 0 .. 32*C*K-1 run through its tiles in order (position p is slot (p' % C) * 32 + p' / C of the
+// group's tile p / (32*C), p' = p % (32*C)), so a strand may continue from lane 31's last slot of
+// one tile into lane 0's first slot of the next.  Each strand takes a contiguous run of positions
+// starting at an even one (its length rounded up to even).  Strands are placed longest first into
+// the fullest group that still has room (best fit decreasing), so uneven strands share groups.
+// Returns false when a strand is longer than a group.
+bool pack_tiles(const int32_t* sb, int32_t ns, int C, TileLayout& out, std::string& err, int K = 1);
+
+// Smallest power of two K (<= 8) whose groups of K tiles of 32*C slots hold the longest strand;
+// 0 when even 8 tiles are too short.
+int tiles_per_group_for(const int32_t* sb, int32_t ns, int C);
 
 // Smallest even C whose tile (32*C slots) holds the longest strand.
 int slots_per_lane_for(const int32_t* sb, int32_t ns);

@@ -260,7 +260,32 @@ cudaError_t launch_fused_frame(const DeviceState& st, const PhysParams& pp, cons
 
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps,
-                              int nsteps, int reg_cap) {
+                              int nsteps, int reg_cap, int group) {
+    if (group > 1) {
+        if (group > 8 || st.num_tiles % group != 0) return cudaErrorInvalidValue;
+        const unsigned gblocks = (unsigned)(st.num_tiles / group);
+        if (gblocks == 0) return cudaSuccess;
+        const int gthreads = 32 * group;
+#define KAMI_GROUP_LAUNCH(KERNEL, CC)                                                                   \
+    do {                                                                                                \
+        if (jacobi)                                                                                     \
+            KERNEL<CC, true><<<gblocks, gthreads, 0, s>>>(st, pp, sp, sdf, d_steps, nsteps);             \
+        else                                                                                            \
+            KERNEL<CC, false><<<gblocks, gthreads, 0, s>>>(st, pp, sp, sdf, d_steps, nsteps);            \
+    } while (0)
+        if (C == 2 && reg_cap == 120)
+            KAMI_GROUP_LAUNCH(fused_group_kernel_r120, 2);
+        else if (C == 4 && reg_cap == 168)
+            KAMI_GROUP_LAUNCH(fused_group_kernel_r168, 4);
+        else if (C == 2)
+            KAMI_GROUP_LAUNCH(fused_group_kernel, 2);
+        else if (C == 4)
+            KAMI_GROUP_LAUNCH(fused_group_kernel, 4);
+        else
+            return cudaErrorInvalidValue;
+#undef KAMI_GROUP_LAUNCH
+        return cudaGetLastError();
+    }
     int threads = 32 * warps_per_block;
     unsigned blocks = blocks_for(st.num_tiles, warps_per_block);
     if (blocks == 0) return cudaSuccess;

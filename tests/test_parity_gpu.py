@@ -93,14 +93,16 @@ def test_rotating_body():
     assert ex <= POS_TOL and et <= TWIST_TOL, (ex, et)
 
 
-def test_long_strands_take_the_sweep_form():
-    """Strands longer than a fused tile (128) run on the sweep form with wider tiles."""
+@pytest.mark.parametrize("form", ["auto", "sweep"])
+def test_long_strands(form):
+    """Strands longer than a tile of 128 slots: the fused form takes groups of tiles (auto), the sweep
+    form wider tiles."""
     g = helpers.soft_groom(20, (150, 250), seed=5)
     st = helpers.soft_settings(num_itr=4)
-    s = helpers.gpu_solver(g, st, form="auto")
-    assert s.slots_per_lane >= 6
+    s = helpers.gpu_solver(g, st, form=form)
+    assert s.slots_per_lane == 4 if form == "auto" else s.slots_per_lane >= 6
     s.close()
-    ex, et = _lockstep(g, st, "auto", 4, 1 / 60, reseed_each_frame=True)
+    ex, et = _lockstep(g, st, form, 4, 1 / 60, reseed_each_frame=True)
     assert ex <= POS_TOL and et <= TWIST_TOL, (ex, et)
 
 
