@@ -1177,12 +1177,11 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     if (st == KAMI_OK && (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess))
         st = fail(KAMI_ERR_CUDA, "cudaEventCreate");
-    const int cmin = slots_per_lane_for(h->strand_begin.data(), h->ns);
     const int Fs[3] = {1, 4, 16};
     double rate_best = -1.0;
     int pick[4] = {h->layout.C, h->warps_per_block, h->steps_per_launch, h->reg_cap ? h->reg_cap : 1};
     const bool colour2 = h->schedule == KAMI_SCHEDULE_COLOUR2;
-    for (int C = std::min(cmin, 4); C <= 4 && st == KAMI_OK; C += 2) {
+    for (int C = 2; C <= 4 && st == KAMI_OK; C += 2) {  // both, in groups of tiles where strands need them
         // tiles per group for this C (strands longer than a tile); groups fix the CTA shape
         const int K = tiles_per_group_for(h->strand_begin.data(), h->ns, C);
         if (K == 0) continue;
