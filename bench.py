@@ -25,6 +25,7 @@ of the same groom; the reference has no CPU implementation of this step of its o
 from __future__ import annotations
 
 import argparse
+import math
 import json
 import os
 import statistics
@@ -307,7 +308,43 @@ def extra_forms(args, torch, stream, flush):
     except Exception as e:  # a contact-list overflow (KAMI_ERR_CONTACTS) is reported, not fatal
         out["hair_hair_sweep"] = {"error": str(e)}
     out["long_strands_3k_x200"] = long_strand_timing(torch, stream, flush)
+    out["reference_default_settings"] = default_settings_timing(torch, stream)
     return out
+
+
+def default_settings_timing(torch, stream, frames=3):
+    """The reference solver's default settings (scripts/json/StCossRods.json and the defaults of
+    StableCosseratRodsSolver.h:86-110): strands resampled to 1 mm segments, NumItr 32, wind (peak 40,
+    frequencies 1 / 0.7 / 0.4, sharpness 3), the head SDF, and YarnBall's Sim::maxH of 4e-4 s, so a
+    1/60 s frame is 42 substeps.  6,000 strands of 100-300 vertices (10-30 cm); one kami_vbd_step per
+    frame, autotuned tile shape, CUDA events around the frames."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.vbd import Solver
+
+    rng = np.random.default_rng(12)
+    g = synth.groom_strands(rng, rng.integers(100, 301, 6000), seg_len=1e-3)
+    st = dict(num_itr=32, max_h=4e-4, gravity=(0.0, 0.0, -9.81), radius=40e-6, density=1300.0, velocity_decay=0.05,
+              damping=1e-6, wind=(40.0, 1.0, 0.7, 0.4, 3.0), sdf=synth.sphere_sdf(128, threshold=1e-3))
+    dt = 1.0 / 60.0
+    s = Solver(g, form="auto", **st)
+    tuned, _ = s.autotune(dt, trial_steps=2)
+    s.step(dt, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    for _ in range(frames):
+        s.step(dt, stream=stream)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    ms = e0.elapsed_time(e1) / frames
+    s.get_positions_velocities()  # raises if a frame went non-finite
+    s.close()
+    substeps = math.ceil(dt / 4e-4 - 1e-6)
+    return {"value": g.num_vertices * 32 * substeps / (ms / 1e3), "unit": UNIT, "ms_per_frame": ms,
+            "substeps_per_frame": substeps, "vertices": g.num_vertices,
+            "tuning": dict(zip(("slots_per_lane", "warps_per_block", "steps_per_launch", "register_cap"), tuned)),
+            "what": "6,000 strands of 100-300 vertices at 1 mm, NumItr 32, wind, head SDF, 42 substeps of 4e-4 s per "
+                    "1/60 s frame: the reference solver's default settings"}
 
 
 def long_strand_timing(torch, stream, flush, steps=200):
@@ -638,7 +675,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
-    ap.add_argument("--only", choices=["adjoint", "large", "hairhair", "bake", "long"],
+    ap.add_argument("--only", choices=["adjoint", "large", "hairhair", "bake", "long", "default"],
                     help="run a single extra measurement")
     ap.add_argument("--tuning", help="fixed tile shape C,warps,steps_per_launch,register_cap instead of autotuning")
     args = ap.parse_args()
@@ -658,6 +695,10 @@ def main():
         print(json.dumps(hair_hair_timing(torch, torch.cuda.current_stream())), flush=True)
     elif args.only == "bake":
         print(json.dumps(sdf_bake_timing()), flush=True)
+    elif args.only == "default":
+        import torch
+
+        print(json.dumps(default_settings_timing(torch, torch.cuda.current_stream())), flush=True)
     elif args.only == "long":
         import torch
 
