@@ -16,7 +16,7 @@ DRIVER = os.path.join(ROOT, "kamisimulator_b200", "lib", "kami_solver_driver")
 # the keys and values of the reference's scripts/json/StCossRods.json
 REFERENCE_SETTINGS = {
     "EnableResample": True, "EnableSDF": True, "EnableHairHairColl": False, "UseYoungsModule": True, "NumItr": 32,
-    "SagFreeItr": 0, "SubdivCoeff": 3, "StretchK": 3e3, "BendK": 6e-4, "YoungsModule": 5,
+    "SagFreeItr": 1, "SubdivCoeff": 3, "StretchK": 3e3, "BendK": 6e-4, "YoungsModule": 5,
     "StiffnessDeviationCoeff": 1, "CurveRadius": 4e-5, "Density": 1.3e6, "ResampleLen": 1e-3,
     "VelocityDecay": 0.05, "ExternalForceMultiplier": 1, "WindPeak": 40, "WindYFreq": 1, "WindZFreq": 0.7,
     "WindTimeFreq": 0.4, "WindSharpness": 3.0,
@@ -60,6 +60,7 @@ def test_descriptor_from_reference_settings(tmp_path):
     assert d["wind_peak"] == pytest.approx(40.0) and d["velocity_decay"] == pytest.approx(0.05)
     assert d["max_h"] == pytest.approx(4e-4)  # Sim::maxH
     assert d["gravity"] == pytest.approx([0.0, -9.8, 0.0])
+    assert d["sag_free_itr"] == 1
 
 
 def test_invalid_settings_are_rejected(tmp_path):
@@ -184,4 +185,56 @@ def test_plugin_subdivides_and_resamples_the_hair(tmp_path):
     s.close()
     out, _ = read_out(tmp_path / "out.bin", g.num_strands, (16 - 1) * 3 + 1)
     got = np.concatenate([out[s, :cr[s]] for s in keep])
+    np.testing.assert_allclose(got, x, atol=1e-6)
+
+
+def write_sdf(path, sdf):
+    with open(path, "wb") as f:
+        f.write(np.array(sdf.dims, np.int32).tobytes())
+        f.write(np.array(sdf.grid_min, np.float32).tobytes())
+        f.write(np.array(sdf.grid_max, np.float32).tobytes())
+        f.write(np.ascontiguousarray(sdf.phi, np.float32).tobytes())
+        f.write(np.ascontiguousarray(sdf.grad, np.float32).tobytes())
+
+
+@pytest.mark.gpu
+def test_plugin_runs_the_reference_default_settings(tmp_path):
+    """The reference's own default settings (subdivision x3, resampling to 1 mm, one sag-free pass,
+    NumItr 32, wind, the head SDF, Sim::maxH 4e-4 s, so 42 substeps per 1/60 s frame).  The resampled
+    strands are longer than a tile of 128 slots and run on the fused form in groups of tiles; two
+    frames of the plugin equal the same preprocessing and set-up through the C ABI."""
+    from kamisimulator_b200 import vbd
+
+    rng = np.random.default_rng(31)
+    g = synth.groom_strands(rng, rng.integers(8, 31, 30), seg_len=6e-3)
+    pad = 64  # resampled strands are capped at the Hair's row length, (64 - 1) * 3 + 1 after subdivision
+    counts, mv = write_hair(tmp_path / "hair.bin", g, pad_to=pad)
+    sdf = synth.sphere_sdf(64, threshold=1e-3)
+    write_sdf(tmp_path / "sdf.bin", sdf)
+    (tmp_path / "s.json").write_text(json.dumps(dict(REFERENCE_SETTINGS, SDFThreshold=1e-3)))
+    subprocess.run([DRIVER, str(tmp_path / "s.json"), str(tmp_path / "hair.bin"), "2", str(1 / 60),
+                    str(tmp_path / "out.bin"), str(tmp_path / "sdf.bin")], check=True, capture_output=True)
+    padded = np.zeros((g.num_strands, pad, 3), np.float32)
+    for s in range(g.num_strands):
+        padded[s, :counts[s]] = g.positions[g.strand_begin[s]:g.strand_begin[s + 1]]
+    c3, x3 = vbd.hair_subdivide(counts, padded, 3)
+    cr, xr = vbd.hair_resample(c3, x3, 1e-3)
+    assert cr.max() > 128  # longer than a tile
+    keep = [s for s in range(g.num_strands) if cr[s] >= 4]
+    pos = np.concatenate([xr[s, :cr[s]] for s in keep])
+    gg = synth.Groom(strand_begin=np.concatenate([[0], np.cumsum([cr[s] for s in keep])]).astype(np.int32),
+                     positions=pos, strand_young=np.full(len(keep), 5.0, np.float32),
+                     strand_dev=np.ones(len(keep), np.float32))
+    st = dict(num_itr=32, max_h=4e-4, gravity=(0.0, -9.8, 0.0), radius=np.float32(0.05) * np.float32(4e-5),
+              density=1.3e6, velocity_decay=0.05, wind=(40.0, 1.0, 0.7, 0.4, 3.0), sdf=sdf, young=5.0,
+              deviation=1.0, per_strand=False, sag_free_itr=1)
+    s = helpers.gpu_solver(gg, st, form="auto")
+    assert s.slots_per_lane == 4  # fused, in groups of tiles
+    for _ in range(2):
+        s.step(1 / 60)
+    x = s.get_positions_velocities()[0]
+    s.close()
+    out, _ = read_out(tmp_path / "out.bin", g.num_strands, (pad - 1) * 3 + 1)
+    got = np.concatenate([out[s, :cr[s]] for s in keep])
+    assert np.isfinite(got).all()
     np.testing.assert_allclose(got, x, atol=1e-6)
