@@ -892,28 +892,36 @@ static void drop_graphs(kami_vbd_solver* h) {
 static kami_status build_host_runs(kami_vbd_solver* h) {
     const int C = h->layout.C;
     const int64_t T = 32LL * C, tiles = h->layout.num_tiles;
-    std::vector<int32_t> begin(tiles + 1, 0);
-    std::vector<int64_t> tile_of(h->ns);
+    // a strand is one run of consecutive tile positions in each tile it occupies (more than one
+    // when it runs on across the tiles of a group): the kernel stages positions [p0, p0 + n) < T
+    struct Piece {
+        int64_t tile;
+        int4 run;
+    };
+    std::vector<Piece> pieces;
+    pieces.reserve(h->ns);
     for (int32_t s = 0; s < h->ns; s++) {
-        tile_of[s] = h->layout.slot_of[h->strand_begin[s]] / T;
-        begin[tile_of[s] + 1]++;
+        const int32_t v1 = h->strand_begin[s + 1];
+        for (int32_t j = h->strand_begin[s]; j < v1;) {
+            const int64_t g = h->layout.slot_of[j];
+            const int64_t t = g / T, q = g % T;  // q = (p % C) * 32 + p / C
+            const int p0 = (int)((q % 32) * C + q / 32);
+            int32_t n = 1;
+            while (j + n < v1) {
+                const int p = p0 + n;
+                if (p >= T || h->layout.slot_of[j + n] != t * T + (int64_t)(p % C) * 32 + p / C) break;
+                n++;
+            }
+            pieces.push_back({t, make_int4(p0, j, n, 0)});
+            j += n;
+        }
     }
+    std::vector<int32_t> begin(tiles + 1, 0);
+    for (const Piece& pc : pieces) begin[pc.tile + 1]++;
     for (int64_t t = 0; t < tiles; t++) begin[t + 1] += begin[t];
     std::vector<int32_t> next(begin.begin(), begin.end() - 1);
-    std::vector<int4> runs(h->ns);
-    for (int32_t s = 0; s < h->ns; s++) {
-        const int64_t q = h->layout.slot_of[h->strand_begin[s]] % T;  // (p % C) * 32 + p / C
-        const int p0 = (int)((q % 32) * C + q / 32);
-        const int32_t v0 = h->strand_begin[s], n = h->strand_begin[s + 1] - v0;
-        // the kernel stages positions [p0, p0 + n) of the tile: they must be the strand's slots
-        if (p0 + n > T) return fail(KAMI_ERR_UNSUPPORTED, "strand %d overruns its tile", s);
-        for (int32_t j = 0; j < n; j++) {
-            const int p = p0 + j;
-            if (h->layout.slot_of[v0 + j] != tile_of[s] * T + (int64_t)(p % C) * 32 + p / C)
-                return fail(KAMI_ERR_UNSUPPORTED, "strand %d is not one run of tile positions", s);
-        }
-        runs[next[tile_of[s]]++] = make_int4(p0, v0, n, 0);
-    }
+    std::vector<int4> runs(pieces.size());
+    for (const Piece& pc : pieces) runs[next[pc.tile]++] = pc.run;
     KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
     if (h->d_runs) cudaFree(h->d_runs);
     if (h->d_run_begin) cudaFree(h->d_run_begin);
@@ -967,7 +975,7 @@ kami_status kami_vbd_step_host(kami_vbd_handle h, float dt, const float* xyz, co
     if (!std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
     HostIO io{};
     const int64_t n = 3 * h->nv;
-    bool direct = dt > 0.f && h->form == KAMI_FORM_FUSED && !h->hair_hair && h->layout.K == 1;
+    bool direct = dt > 0.f && h->form == KAMI_FORM_FUSED && !h->hair_hair;
     if (direct) {
         io.x_in = mapped_range(xyz, n);
         io.v_in = mapped_range(vxyz, n);
@@ -986,7 +994,7 @@ kami_status kami_vbd_step_host(kami_vbd_handle h, float dt, const float* xyz, co
     io.run_begin = h->d_run_begin;
     const StepParams sp = advance_clock(h, dt);
     KAMI_CUDA(launch_fused_frame(h->dstate(), h->pp, sp, h->sdf, io, h->layout.C, h->schedule == KAMI_SCHEDULE_JACOBI,
-                                 h->warps_per_block, h->stream, h->reg_cap),
+                                 h->warps_per_block, h->stream, h->reg_cap, h->layout.K),
               "fused frame launch");
     h->time += dt;
     h->counter += sp.substeps;

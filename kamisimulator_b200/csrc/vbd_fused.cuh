@@ -237,7 +237,7 @@ template <int C, bool JACOBI, bool RECORD, bool PAIRED = false, bool HOSTIO = fa
 __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                 TapeView tp, const StepParams* __restrict__ steps, int nsteps,
                                                 HostIO hio = HostIO{}, int64_t frame_tile = 0, float* stage = nullptr) {
-    static_assert(!GROUPED || (!RECORD && !HOSTIO && !PAIRED), "tile groups run the plain step");
+    static_assert(!GROUPED || (!RECORD && !PAIRED), "tile groups run the plain step");
     static_assert(!PAIRED || (C == 4 && !JACOBI && !RECORD), "the packed form is the colour2 step with 4 slots per lane");
     static_assert(!(HOSTIO && RECORD), "recorded steps keep their state on the device");
     static_assert(!(RECORD && JACOBI), "the tape records the colour2 schedule");
@@ -638,12 +638,12 @@ __global__ void __launch_bounds__(256) fused_step_kernel_x2(DeviceState st, Phys
 // over PCIe), steps the tile and writes it back (fused_step_body, HOSTIO).  The waves of tiles keep
 // the host reads of one wave apart from the host writes of the wave before, which is faster here
 // than interleaving them: SM-issued reads and writes over PCIe slow each other down.
-template <int C, bool JACOBI, bool PAIRED>
+template <int C, bool JACOBI, bool PAIRED, bool GROUPED = false>
 __device__ __forceinline__ void fused_frame(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf, HostIO hio) {
     extern __shared__ float kami_frame_stage[];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
-    if (t >= st.num_tiles) return;  // uniform per warp
+    if (t >= st.num_tiles) return;  // uniform per warp (per CTA for groups)
     float* const stage = kami_frame_stage + w * (6 * 32 * C);
     const int r_end = hio.run_begin[t + 1];
     for (int r = hio.run_begin[t]; r < r_end; r++) {
@@ -656,7 +656,7 @@ __device__ __forceinline__ void fused_frame(DeviceState st, PhysParams pp, StepP
         }
     }
     __syncwarp();
-    fused_step_body<C, JACOBI, false, PAIRED, true>(st, pp, sp, sdf, TapeView{}, nullptr, 1, hio, t, stage);
+    fused_step_body<C, JACOBI, false, PAIRED, true, GROUPED>(st, pp, sp, sdf, TapeView{}, nullptr, 1, hio, t, stage);
 }
 template <int C, bool JACOBI, bool PAIRED>
 __global__ void __launch_bounds__(256) fused_frame_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
@@ -667,6 +667,12 @@ template <int C, bool JACOBI>
 __global__ void __maxnreg__(120) fused_frame_kernel_r120(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                         HostIO hio) {
     fused_frame<C, JACOBI, false>(st, pp, sp, sdf, hio);
+}
+// The same over groups of tiles: one CTA of K warps per group.
+template <int C, bool JACOBI>
+__global__ void __launch_bounds__(256) fused_frame_group_kernel(DeviceState st, PhysParams pp, StepParams sp,
+                                                                SdfParams sdf, HostIO hio) {
+    fused_frame<C, JACOBI, false, true>(st, pp, sp, sdf, hio);
 }
 
 // The step with 4 slots per lane at most 168 registers per thread (a few bytes of spills): 12 instead

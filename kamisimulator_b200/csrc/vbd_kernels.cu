@@ -242,7 +242,19 @@ cudaError_t launch_frame(K kernel, int C, const DeviceState& st, const PhysParam
 }  // namespace
 
 cudaError_t launch_fused_frame(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
-                               const HostIO& hio, int C, bool jacobi, int warps_per_block, cudaStream_t s, int reg_cap) {
+                               const HostIO& hio, int C, bool jacobi, int warps_per_block, cudaStream_t s, int reg_cap,
+                               int group) {
+    if (group > 1) {  // one CTA of `group` warps per group of tiles
+        if (group > 8 || st.num_tiles % group != 0) return cudaErrorInvalidValue;
+        if (st.num_tiles == 0) return cudaSuccess;
+        if (C == 2)
+            return jacobi ? launch_frame(fused_frame_group_kernel<2, true>, 2, st, pp, sp, sdf, hio, group, s)
+                          : launch_frame(fused_frame_group_kernel<2, false>, 2, st, pp, sp, sdf, hio, group, s);
+        if (C == 4)
+            return jacobi ? launch_frame(fused_frame_group_kernel<4, true>, 4, st, pp, sp, sdf, hio, group, s)
+                          : launch_frame(fused_frame_group_kernel<4, false>, 4, st, pp, sp, sdf, hio, group, s);
+        return cudaErrorInvalidValue;
+    }
     if (blocks_for(st.num_tiles, warps_per_block) == 0) return cudaSuccess;
     if (reg_cap == 2 && C == 4 && !jacobi)
         return launch_frame(fused_frame_kernel<4, false, true>, 4, st, pp, sp, sdf, hio, warps_per_block, s);

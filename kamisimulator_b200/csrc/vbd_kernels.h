@@ -28,7 +28,8 @@ cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const
 // One step as an upload-step-download frame over the host buffers of hio (fused_frame_kernel);
 // same tile shapes and register variants as launch_fused_step.
 cudaError_t launch_fused_frame(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
-                               const HostIO& hio, int C, bool jacobi, int warps_per_block, cudaStream_t s, int reg_cap);
+                               const HostIO& hio, int C, bool jacobi, int warps_per_block, cudaStream_t s, int reg_cap,
+                               int group = 1);
 
 cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                                 const TapeView& tp, int C, int warps_per_block, cudaStream_t s);

@@ -70,7 +70,10 @@ def test_long_strands_step_n_and_host_frames():
     b.set_tuning(steps_per_launch=4)
     b.step_n(1 / 120, frames, bt)
     np.testing.assert_array_equal(a.get_state(), b.get_state())
-    # kami_vbd_step_host takes the three calls for groups of tiles
+    # kami_vbd_step_host: pageable arrays take the three calls; pinned ones the frame kernel over groups,
+    # which equals them to rounding (it is compiled on its own)
+    import torch
+
     x, v = a.get_positions_velocities()
     v = v + np.float32(0.01)
     xo, vo = b.step_host(1 / 120, x.copy(), v.copy())
@@ -79,6 +82,13 @@ def test_long_strands_step_n_and_host_frames():
     xa, va = a.get_positions_velocities()
     np.testing.assert_array_equal(xo, xa)
     np.testing.assert_array_equal(vo, va)
+    xp = torch.from_numpy(xa.copy()).pin_memory()
+    vp = torch.from_numpy(va.copy()).pin_memory()
+    b.step_host(1 / 120, xp, vp)
+    a.step(1 / 120)
+    xa, va = a.get_positions_velocities()
+    np.testing.assert_allclose(xp.numpy(), xa, rtol=0, atol=1e-6)
+    np.testing.assert_allclose(vp.numpy(), va, rtol=0, atol=2e-4)
     a.close()
     b.close()
 
