@@ -334,19 +334,24 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
  * checkpoint with kami_vbd_set_state, record the k steps of that segment, call kami_vbd_backward
  * with the adjoint of the segment's final state, and continue with the next earlier segment. */
 
-/* Allocates a tape for up to max_steps recorded steps of up to max_tiles warp tiles (0 = all tiles)
- * and the adjoint buffers (d loss / d qRest starts at zero); the tile window starts as the first
- * max_tiles tiles.  A tape step costs (num_itr + 1) * 32 + 48 B per slot.  KAMI_ERR_UNSUPPORTED for the
- * sweep form, the Jacobi schedule or wind. */
+/* Allocates a tape for up to max_steps recorded steps of up to max_tiles warp tiles (0 = all tiles;
+ * rounded up to whole groups of tiles) and the adjoint buffers (d loss / d qRest starts at zero); the
+ * tile window starts as the first max_tiles tiles.  A tape step costs (num_itr + 1) * 32 + 48 B per
+ * slot.  KAMI_ERR_UNSUPPORTED for the sweep form, the Jacobi schedule, wind, or strands longer than 4
+ * tiles (groups of more than 4 tiles). */
 kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps, int64_t max_tiles);
 
 /* Number of warp tiles of the device layout. */
 kami_status kami_vbd_get_tile_count(kami_vbd_handle h, int64_t* num_tiles);
 
-/* Restricts recording and the adjoint to tiles [tile_begin, tile_end) (at most the tape's tiles).
- * Strands never cross tiles, so a large groom is differentiated window by window: for each window,
- * restore each checkpoint, record and run kami_vbd_backward; the adjoint of vertices outside the
- * window passes through unchanged. */
+/* Tiles per group of the fused layout: 1 when every strand fits a tile, else the 2, 4 or 8 tiles that
+ * a strand may run on across (no counterpart in the reference). */
+kami_status kami_vbd_get_tiles_per_group(kami_vbd_handle h, int32_t* tiles_per_group);
+
+/* Restricts recording and the adjoint to tiles [tile_begin, tile_end) (at most the tape's tiles; both
+ * multiples of kami_vbd_get_tiles_per_group).  Strands never cross a group of tiles, so a large groom
+ * is differentiated window by window: for each window, restore each checkpoint, record and run
+ * kami_vbd_backward; the adjoint of vertices outside the window passes through unchanged. */
 kami_status kami_vbd_set_tape_window(kami_vbd_handle h, int64_t tile_begin, int64_t tile_end);
 
 /* kami_vbd_step that also records its iterates; dt must not exceed max_h (a single substep). */

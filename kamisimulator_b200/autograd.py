@@ -54,6 +54,8 @@ class StrandStiffnessRollout(torch.autograd.Function):
         aq = torch.zeros((nv, 4), dtype=torch.float32, device=dev)
         tiles = solver.tile_count()
         chunk = ctx.chunk if 0 < ctx.chunk < tiles else tiles
+        group = solver.tiles_per_group()  # tape windows are whole groups of tiles
+        chunk = min(tiles, -(-chunk // group) * group)
         solver.tape_reserve(k, chunk)
         solver.zero_rest_darboux_grad()
         torch.cuda.synchronize()

@@ -1247,8 +1247,8 @@ static kami_status adjoint_supported(kami_vbd_solver* h) {
     if (h->form != KAMI_FORM_FUSED || h->schedule != KAMI_SCHEDULE_COLOUR2)
         return fail(KAMI_ERR_UNSUPPORTED, "the adjoint covers the fused form with the colour2 schedule");
     if (h->pp.wind_peak != 0.f) return fail(KAMI_ERR_UNSUPPORTED, "the adjoint does not cover wind");
-    if (h->layout.K != 1)
-        return fail(KAMI_ERR_UNSUPPORTED, "the adjoint covers strands of one tile (at most 128 vertices)");
+    if (h->layout.K > 4)
+        return fail(KAMI_ERR_UNSUPPORTED, "the adjoint covers groups of up to 4 tiles (strands of up to 512 vertices)");
     return KAMI_OK;
 }
 
@@ -1258,7 +1258,9 @@ kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps, int64_t 
     if (max_steps <= 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "max_steps must be > 0");
     if (max_tiles < 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "max_tiles must be >= 0");
     KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
-    const int64_t tiles = (max_tiles == 0 || max_tiles > h->layout.num_tiles) ? h->layout.num_tiles : max_tiles;
+    const int64_t K = h->layout.K;  // windows are whole groups of tiles
+    int64_t tiles = (max_tiles == 0 || max_tiles > h->layout.num_tiles) ? h->layout.num_tiles : max_tiles;
+    tiles = std::min<int64_t>(h->layout.num_tiles, (tiles + K - 1) / K * K);
     if (h->tape_capacity == max_steps && h->tape_tiles == tiles) {  // already the requested size
         h->tape_steps.clear();
         h->win_begin = 0;
@@ -1301,6 +1303,12 @@ kami_status kami_vbd_get_tile_count(kami_vbd_handle h, int64_t* num_tiles) {
     return KAMI_OK;
 }
 
+kami_status kami_vbd_get_tiles_per_group(kami_vbd_handle h, int32_t* tiles_per_group) {
+    if (!h || !tiles_per_group) return fail(KAMI_ERR_INVALID_ARGUMENT, "null argument");
+    *tiles_per_group = h->layout.K;
+    return KAMI_OK;
+}
+
 kami_status kami_vbd_set_tape_window(kami_vbd_handle h, int64_t tile_begin, int64_t tile_end) {
     if (!h) return fail(KAMI_ERR_INVALID_ARGUMENT, "null handle");
     if (h->tape_capacity == 0) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
@@ -1309,6 +1317,8 @@ kami_status kami_vbd_set_tape_window(kami_vbd_handle h, int64_t tile_begin, int6
         return fail(KAMI_ERR_INVALID_ARGUMENT, "bad tile window [%lld, %lld)", (long long)tile_begin, (long long)tile_end);
     if (tile_end - tile_begin > h->tape_tiles)
         return fail(KAMI_ERR_INVALID_ARGUMENT, "the tape holds %lld tiles per step", (long long)h->tape_tiles);
+    if (tile_begin % h->layout.K != 0 || tile_end % h->layout.K != 0)
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "tape windows are whole groups of %d tiles", h->layout.K);
     h->win_begin = tile_begin;
     h->win_end = tile_end;
     return KAMI_OK;
@@ -1326,7 +1336,7 @@ kami_status kami_vbd_step_record(kami_vbd_handle h, float dt, void* stream) {
     const int step = (int)h->tape_steps.size();
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
         KAMI_CUDA(launch_fused_record(h->window_state(), h->pp, sp, h->sdf, h->tape(step), h->layout.C,
-                                      h->warps_per_block, s),
+                                      h->warps_per_block, s, h->layout.K),
                   "recorded step launch");
         return KAMI_OK;
     });
@@ -1363,7 +1373,7 @@ kami_status kami_vbd_backward(kami_vbd_handle h, float* adj_x, float* adj_v, flo
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
         for (int step = (int)h->tape_steps.size() - 1; step >= 0; step--)
             KAMI_CUDA(launch_adjoint_step(h->window_state(), h->pp, h->tape_steps[step], h->sdf, h->tape(step), ad,
-                                          h->layout.C, s),
+                                          h->layout.C, s, h->layout.K),
                       "adjoint step launch");
         return KAMI_OK;
     });

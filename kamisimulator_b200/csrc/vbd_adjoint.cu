@@ -177,13 +177,50 @@ __device__ __forceinline__ void sdf_adjoint(float3 x, float3 v, float3& gx, floa
     gx = gx + qrotate(rot, ub);
 }
 
+// Adjoint values a group's warps hand across their tile boundaries (GROUPED: one CTA of K <= 4 warps
+// per group of tiles, as GroupExchange in vbd_fused.cuh): `up` from lane 31 of warp w to lane 0 of
+// warp w + 1, `down` from lane 0 of warp w to lane 31 of warp w - 1.  Each slot is written once per
+// iteration and the next write comes after further __syncthreads that its readers have passed.
+enum : int { AU_QR, AU_DD, AU_TQ, AU_TV, AU_QO, AU_F0, AU_GE, AU_N };
+enum : int { AD_X, AD_QN, AD_DXN, AD_PN, AD_FN, AD_N };
+struct AdjointExchange {
+    float4 up[4][AU_N];
+    float4 down[4][AD_N];
+};
+
 // MINB blocks of 128 threads per SM: MINB = 4 caps the registers at 128 so 16 warps share an SM.
-template <int C, int MINB>
+template <int C, int MINB, bool GROUPED = false>
 __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                            TapeView tp, AdjointState ad) {
     const int lane = threadIdx.x & 31;
     const int64_t tile = tp.tile_begin + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
-    if (tile >= st.num_tiles) return;  // uniform per warp
+    if (tile >= st.num_tiles) return;  // uniform per warp (per CTA for groups)
+    const int gw = threadIdx.x >> 5, gK = blockDim.x >> 5;
+    AdjointExchange* gx_ = nullptr;
+    if constexpr (GROUPED) {
+        __shared__ AdjointExchange adjoint_exchange;
+        gx_ = &adjoint_exchange;
+    }
+    // neighbours across the warps of a group; at a group's ends (and without groups) the previous /
+    // next lane of lane 0 / 31 is another strand or nothing, and gets `edge`
+    auto xsync = [&]() {
+        if (GROUPED) __syncthreads();
+    };
+    auto up_put = [&](int slot, float4 v) {
+        if (GROUPED && lane == 31) gx_->up[gw][slot] = v;
+    };
+    auto down_put = [&](int slot, float4 v) {
+        if (GROUPED && lane == 0) gx_->down[gw][slot] = v;
+    };
+    auto up_get = [&](int slot, float4 v, float4 edge) {
+        if (lane != 0) return v;
+        return (GROUPED && gw > 0) ? gx_->up[gw - 1][slot] : edge;
+    };
+    auto down_get = [&](int slot, float4 v, float4 edge) {
+        if (lane != 31) return v;
+        return (GROUPED && gw < gK - 1) ? gx_->down[gw + 1][slot] : edge;
+    };
+    auto f4 = [](float3 a) { return make_float4(a.x, a.y, a.z, 0.f); };
     const int64_t base = tile * (32LL * C) + lane;
     const int64_t S = tp.slots;
     const int N = tp.num_itr;
@@ -214,14 +251,27 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
         ddN[k] = (fl[k] & F_HAS_NEXT) ? kk[k] * invl : 0.f;
         kkN[k] = (fl[k] & F_HAS_NEXT) ? kk[k] : 0.f;
     }
-    const float4 qrH = shfl_up4(qr[C - 1], 1);
-    const float ddH = __shfl_up_sync(0xffffffffu, ddN[C - 1], 1);
+    float4 qrH = shfl_up4(qr[C - 1], 1);
+    float ddH = __shfl_up_sync(0xffffffffu, ddN[C - 1], 1);
+    if (GROUPED) {
+        up_put(AU_QR, qr[C - 1]);
+        up_put(AU_DD, make_float4(ddN[C - 1], 0.f, 0.f, 0.f));
+        xsync();
+        qrH = up_get(AU_QR, qrH, qrH);
+        ddH = up_get(AU_DD, make_float4(ddH, 0.f, 0.f, 0.f), make_float4(ddH, 0.f, 0.f, 0.f)).x;
+    }
     const float h = sp.h;
     const float damp = pp.damping / h;
     const float accel = pp.accel_ratio;
 #pragma unroll
     for (int k = 0; k < C - 1; k++) e[k] = x[k + 1] - x[k];
-    e[C - 1] = shfl_down3(x[0], 1) - x[C - 1];
+    float3 xN0 = shfl_down3(x[0], 1);
+    if (GROUPED) {
+        down_put(AD_X, f4(x[0]));
+        xsync();
+        xN0 = xyz(down_get(AD_X, f4(xN0), f4(xN0)));
+    }
+    e[C - 1] = xN0 - x[C - 1];
 #pragma unroll
     for (int k = 0; k < C; k++) {
         e[k] = (fl[k] & F_HAS_NEXT) ? e[k] : zero3();
@@ -293,8 +343,15 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
         float3 tv[C];
         // ---- orientations, odd segments (read even neighbours' new values)
         {
-            const float4 qnN0 = shfl_down4(qn[0], 1);
-            const float3 dxnN0 = shfl_down3(dxn[0], 1);
+            float4 qnN0 = shfl_down4(qn[0], 1);
+            float3 dxnN0 = shfl_down3(dxn[0], 1);
+            if (GROUPED) {
+                down_put(AD_QN, qn[0]);
+                down_put(AD_DXN, f4(dxn[0]));
+                xsync();
+                qnN0 = down_get(AD_QN, qnN0, qnN0);
+                dxnN0 = xyz(down_get(AD_DXN, f4(dxnN0), f4(dxnN0)));
+            }
 #pragma unroll
             for (int k = 1; k < C; k += 2) {
                 const int kn = k + 1 < C ? k + 1 : k;
@@ -314,10 +371,11 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
             }
             float4 tq0 = shfl_up4(tq[C - 1], 1);
             float3 tv0 = shfl_up3(tv[C - 1], 1);
-            if (lane == 0) {
-                tq0 = zero4();
-                tv0 = zero3();
-            }
+            up_put(AU_TQ, tq[C - 1]);
+            up_put(AU_TV, f4(tv[C - 1]));
+            xsync();
+            tq0 = up_get(AU_TQ, tq0, zero4());
+            tv0 = xyz(up_get(AU_TV, f4(tv0), zero4()));
 #pragma unroll
             for (int j = 0; j < C; j += 2) {
                 const float4 P = p1b[j + 1];
@@ -329,7 +387,12 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
         }
         // ---- orientations, even segments (read odd neighbours' old values)
         {
-            const float4 qoP = shfl_up4(qo[C - 1], 1);
+            float4 qoP = shfl_up4(qo[C - 1], 1);
+            if (GROUPED) {
+                up_put(AU_QO, qo[C - 1]);
+                xsync();
+                qoP = up_get(AU_QO, qoP, qoP);
+            }
 #pragma unroll
             for (int k = 0; k < C; k += 2) {
                 const int kp = k > 0 ? k - 1 : 0;
@@ -347,7 +410,9 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
                 gq[k] = upd ? zero4() : gq[k];
             }
             float4 pN = shfl_down4(p1b[0], 1);
-            if (lane == 31) pN = zero4();
+            down_put(AD_PN, p1b[0]);
+            xsync();
+            pN = down_get(AD_PN, pN, zero4());
 #pragma unroll
             for (int j = 1; j < C; j += 2) {
                 const int jn = j + 1 < C ? j + 1 : j;
@@ -370,7 +435,9 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
                 ge[k] = ge[k] + ddN[k] * fb[k];
             }
             float3 f0 = shfl_up3(fb[C - 1], 1);
-            if (lane == 0) f0 = zero3();
+            up_put(AU_F0, f4(fb[C - 1]));
+            xsync();
+            f0 = xyz(up_get(AU_F0, f4(f0), zero4()));
 #pragma unroll
             for (int j = 0; j < C; j += 2) {
                 const float3 fn = fb[j + 1];  // from the next vertex (its previous-segment terms)
@@ -392,7 +459,9 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
                 ge[k] = ge[k] + ddN[k] * fb[k];
             }
             float3 fN = shfl_down3(fb[0], 1);
-            if (lane == 31) fN = zero3();
+            down_put(AD_FN, f4(fb[0]));
+            xsync();
+            fN = xyz(down_get(AD_FN, f4(fN), zero4()));
 #pragma unroll
             for (int j = 1; j < C; j += 2) {
                 const int jn = j + 1 < C ? j + 1 : j;
@@ -433,7 +502,9 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
     }
     // ---- segment vectors e_k = x_{k+1} - x_k
     float3 geP = shfl_up3(ge[C - 1], 1);
-    if (lane == 0) geP = zero3();
+    up_put(AU_GE, f4(ge[C - 1]));
+    xsync();
+    geP = xyz(up_get(AU_GE, f4(geP), zero4()));
 #pragma unroll
     for (int k = 0; k < C; k++) {
         gx[k] = gx[k] - ge[k] + (k ? ge[k > 0 ? k - 1 : 0] : geP);
@@ -448,7 +519,20 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
 
 // ------------------------------------------------------------------------------------------
 cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
-                                const TapeView& tp, int C, int warps_per_block, cudaStream_t s) {
+                                const TapeView& tp, int C, int warps_per_block, cudaStream_t s, int group) {
+    if (group > 1) {  // one CTA of `group` warps per group of tiles (the window is whole groups)
+        const int64_t tiles = st.num_tiles - tp.tile_begin;
+        if (group > 8 || tiles % group != 0 || tp.tile_begin % group != 0) return cudaErrorInvalidValue;
+        if (tiles == 0) return cudaSuccess;
+        const unsigned gblocks = (unsigned)(tiles / group);
+        if (C == 2)
+            fused_record_group_kernel<2><<<gblocks, 32 * group, 0, s>>>(st, pp, sp, sdf, tp);
+        else if (C == 4)
+            fused_record_group_kernel<4><<<gblocks, 32 * group, 0, s>>>(st, pp, sp, sdf, tp);
+        else
+            return cudaErrorInvalidValue;
+        return cudaGetLastError();
+    }
     const int threads = 32 * warps_per_block;
     const int64_t tiles = st.num_tiles - tp.tile_begin;
     const unsigned blocks = (unsigned)((tiles + warps_per_block - 1) / warps_per_block);
@@ -463,7 +547,20 @@ cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, con
 }
 
 cudaError_t launch_adjoint_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
-                                const TapeView& tp, const AdjointState& ad, int C, cudaStream_t s) {
+                                const TapeView& tp, const AdjointState& ad, int C, cudaStream_t s, int group) {
+    if (group > 1) {  // one CTA of `group` <= 4 warps per group of tiles
+        const int64_t tiles = st.num_tiles - tp.tile_begin;
+        if (group > 4 || tiles % group != 0 || tp.tile_begin % group != 0) return cudaErrorInvalidValue;
+        if (tiles == 0) return cudaSuccess;
+        const unsigned gblocks = (unsigned)(tiles / group);
+        if (C == 2)
+            adjoint_step_kernel<2, 4, true><<<gblocks, 32 * group, 0, s>>>(st, pp, sp, sdf, tp, ad);
+        else if (C == 4)
+            adjoint_step_kernel<4, 2, true><<<gblocks, 32 * group, 0, s>>>(st, pp, sp, sdf, tp, ad);
+        else
+            return cudaErrorInvalidValue;
+        return cudaGetLastError();
+    }
     const int wpb = 4;
     const int64_t tiles = st.num_tiles - tp.tile_begin;
     const unsigned blocks = (unsigned)((tiles + wpb - 1) / wpb);

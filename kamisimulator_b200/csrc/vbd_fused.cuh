@@ -237,7 +237,7 @@ template <int C, bool JACOBI, bool RECORD, bool PAIRED = false, bool HOSTIO = fa
 __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                 TapeView tp, const StepParams* __restrict__ steps, int nsteps,
                                                 HostIO hio = HostIO{}, int64_t frame_tile = 0, float* stage = nullptr) {
-    static_assert(!GROUPED || (!RECORD && !PAIRED), "tile groups run the plain step");
+    static_assert(!GROUPED || !PAIRED, "tile groups run the plain step");
     static_assert(!PAIRED || (C == 4 && !JACOBI && !RECORD), "the packed form is the colour2 step with 4 slots per lane");
     static_assert(!(HOSTIO && RECORD), "recorded steps keep their state on the device");
     static_assert(!(RECORD && JACOBI), "the tape records the colour2 schedule");
@@ -699,6 +699,13 @@ template <int C, bool JACOBI>
 __global__ void __maxnreg__(168) fused_group_kernel_r168(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                         const StepParams* __restrict__ steps, int nsteps) {
     fused_step_body<C, JACOBI, false, false, false, true>(st, pp, sp, sdf, TapeView{}, steps, nsteps);
+}
+
+// The recorded step (kami_vbd_step_record) over groups of tiles: one CTA of K warps per group.
+template <int C>
+__global__ void __launch_bounds__(256) fused_record_group_kernel(DeviceState st, PhysParams pp, StepParams sp,
+                                                                 SdfParams sdf, TapeView tp) {
+    fused_step_body<C, false, true, false, false, true>(st, pp, sp, sdf, tp, nullptr, 1);
 }
 
 // The same step with at most 120 registers per thread, so 17 warps (instead of 16) share an SM: a

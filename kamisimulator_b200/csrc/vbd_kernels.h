@@ -31,10 +31,12 @@ cudaError_t launch_fused_frame(const DeviceState& st, const PhysParams& pp, cons
                                const HostIO& hio, int C, bool jacobi, int warps_per_block, cudaStream_t s, int reg_cap,
                                int group = 1);
 
+// group > 1: groups of tiles, one CTA of `group` warps each (the adjoint takes groups of up to 4);
+// the tape window must be whole groups.
 cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
-                                const TapeView& tp, int C, int warps_per_block, cudaStream_t s);
+                                const TapeView& tp, int C, int warps_per_block, cudaStream_t s, int group = 1);
 cudaError_t launch_adjoint_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
-                                const TapeView& tp, const AdjointState& ad, int C, cudaStream_t s);
+                                const TapeView& tp, const AdjointState& ad, int C, cudaStream_t s, int group = 1);
 
 // Hair-hair collision (vbd_collision.cu).  coll_scan_tmp_size: int32 elements of scratch the
 // bucket scan of a table of n buckets needs.

@@ -37,7 +37,7 @@ EXPORTED = [
     "kami_vbd_zero_rest_darboux_grad", "kami_vbd_batch_create", "kami_vbd_batch_count", "kami_vbd_batch_groom_range",
     "kami_vbd_batch_step", "kami_vbd_set_hair_layout", "kami_vbd_upload_hair", "kami_vbd_download_hair",
     "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake", "kami_vbd_sag_free",
-    "kami_hair_subdivide", "kami_hair_resample", "kami_vbd_step_host",
+    "kami_hair_subdivide", "kami_hair_resample", "kami_vbd_step_host", "kami_vbd_get_tiles_per_group",
 ]
 
 
@@ -140,6 +140,7 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_set_body_transform": [vp, vp, vp],
         "kami_vbd_step": [vp, f32, vp],
         "kami_vbd_step_host": [vp, f32, vp, vp, vp, vp],
+        "kami_vbd_get_tiles_per_group": [vp, ctypes.POINTER(i32)],
         "kami_vbd_synchronize": [vp],
         "kami_vbd_state_size": [vp, ctypes.POINTER(ctypes.c_size_t)],
         "kami_vbd_get_state": [vp, vp, ctypes.c_size_t, i32],
@@ -484,6 +485,12 @@ class Solver:
         n = ctypes.c_int64()
         _check(self.lib.kami_vbd_get_tile_count(self._h, ctypes.byref(n)))
         return n.value
+
+    def tiles_per_group(self):
+        """Tiles a strand may run on across (1 when every strand fits one tile)."""
+        k = ctypes.c_int32()
+        _check(self.lib.kami_vbd_get_tiles_per_group(self._h, ctypes.byref(k)))
+        return k.value
 
     def set_tape_window(self, tile_begin, tile_end):
         _check(self.lib.kami_vbd_set_tape_window(self._h, tile_begin, tile_end))

@@ -200,6 +200,58 @@ def test_tile_windows_do_not_change_the_gradient():
     solver.close()
 
 
+@pytest.mark.parametrize("lengths,group", [((150, 250), 2), ((300, 500), 4)])
+def test_grouped_tiles_gradient_matches_fp64_autograd(lengths, group):
+    """Strands of 150-500 vertices run across groups of 2 and 4 tiles: the recorded step and the
+    adjoint pass neighbour values between the warps of a group.  Windows are whole groups."""
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+    from kamisimulator_b200.vbd import KamiError
+
+    g, st, solver, unit, strand_of, init, v0 = _setup(num_strands=6, lengths=lengths, seed=23)
+    assert solver.tiles_per_group() == group
+    tiles = solver.tile_count()
+    assert tiles % group == 0 and tiles > group
+    solver.tape_reserve(2, 1)  # rounded up to one group
+    with pytest.raises(KamiError):
+        solver.set_tape_window(0, 1)
+    with pytest.raises(KamiError):
+        solver.set_tape_window(1, 1 + group)
+    with pytest.raises(KamiError):
+        solver.set_tape_window(0, 2 * group)  # wider than the tape
+    solver.set_tape_window(group, 2 * group)
+    rng = np.random.default_rng(2)
+    scale0 = rng.uniform(0.7, 1.4, g.num_strands).astype(np.float32)
+    c = rng.normal(size=(g.num_vertices, 3))
+    frames = 4
+    grads, per_vertex = [], []
+    for chunk in (0, 1):  # the whole groom, then window by window (1 tile rounds up to a group)
+        scale = torch.tensor(scale0, device="cuda", requires_grad=True)
+        x = rollout_positions(scale, solver, unit, strand_of, init, frames, 1 / 60, checkpoint_every=2,
+                              tiles_per_chunk=chunk)
+        loss = (torch.tensor(c, dtype=torch.float32, device="cuda") * x).sum()
+        loss.backward()
+        grads.append(scale.grad.cpu().numpy())
+        per_vertex.append(solver.get_rest_darboux_grad())
+    np.testing.assert_array_equal(per_vertex[0], per_vertex[1])
+    l_ref, g_ref, *_ = _torch_reference(g, st, v0, scale0, frames, c)
+    assert abs(loss.item() - l_ref) <= 1e-4 * abs(l_ref) + 1e-6
+    assert np.linalg.norm(g_ref) > 0
+    assert _rel(grads[0], g_ref) <= GRAD_TOL, (_rel(grads[0], g_ref), grads[0][:5], g_ref[:5])
+    solver.close()
+
+
+def test_groups_of_eight_tiles_have_no_adjoint():
+    from kamisimulator_b200.vbd import KamiError
+
+    g, st, solver, *_ = _setup(num_strands=3, lengths=(600, 900), seed=29)
+    assert solver.tiles_per_group() == 8
+    with pytest.raises(KamiError):
+        solver.tape_reserve(2)
+    solver.close()
+
+
 def test_checkpoint_interval_does_not_change_the_gradient():
     import torch
 
