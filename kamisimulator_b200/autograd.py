@@ -6,11 +6,12 @@ stiffness (Sim::setYoung, YarnBall/YBSimulator.cu:300-320), are  qRest_i = scale
 unit_i.  The forward pass keeps a device checkpoint of the full state every ``checkpoint_every``
 steps.  The backward pass walks the segments in reverse: it restores the segment's checkpoint,
 records its steps, and runs the adjoint back to the checkpoint.  With ``tiles_per_chunk`` it does so
-for one window of warp tiles at a time (strands are independent), so the tape memory is bounded by
+for one window of warp tiles at a time (strands are independent; the window is rounded up to whole
+groups of tiles when strands run across several), so the tape memory is bounded by
 the window: (num_itr + 1) * 32 + 48 B per slot and recorded step.  ``body_transforms`` ((frames, 7):
 rotation x y z w, translation per frame) moves the body SDF frame by frame, in the forward pass and
-in the recorded steps alike.  The solver must use the fused form with the colour2 schedule, no wind
-and dt <= max_h.
+in the recorded steps alike.  The solver must use the fused form with the colour2 schedule (wind is
+allowed) and dt <= max_h.
 """
 from __future__ import annotations
 

@@ -18,8 +18,9 @@
 // (quaternionLambdaItr, YarnBall/sim/cosserat.cu:290-337): the sign tests are constants; the
 // normalisation, the lambda norms and both quaternion products are differentiated by hand, using
 // <a b, c> = <b, conj(a) c> = <a, c conj(b)> for the product adjoints.  The segment vectors
-// e = x_{i+1} - x_i enter through the folded force constant and through V, and the start velocity
-// through the inertial target and the initial guess (iteration.cu:8-59).  The parameter gradient
+// e = x_{i+1} - x_i enter through the folded force constant and through V, the start velocity
+// through the inertial target and the initial guess (iteration.cu:8-59), and with wind the start
+// position's y and z through the wind force in both.  The parameter gradient
 // d loss / d qRest accumulates in AdjointState::gqr.
 #include "vbd_fused.cuh"
 #include "vbd_kernels.h"
@@ -175,6 +176,32 @@ __device__ __forceinline__ void sdf_adjoint(float3 x, float3 v, float3& gx, floa
     const float4 duz = sub4(c1, c0);
     const float3 ub = f3(dot4(cb, dux) * sp.inv_x, dot4(cb, duy) * sp.inv_y, dot4(cb, duz) * sp.inv_z);
     gx = gx + qrotate(rot, ub);
+}
+
+// initItr's wind (iteration.cu:18-30), windx = peak * max(0, pow(cY cZ, sharp) sign(cY cZ)) with
+// cY = cos 2 pi (fY y + fT t) for y > 0 (else 0) and cZ = cos 2 pi (fZ |z| + fT t), evaluated as
+// vbd_predict does, and its derivatives d windx / d y, d windx / d z.  Where windx > 0,
+// d windx / d (cY cZ) = peak sharp pw / (cY cZ) (pw = pow(cY cZ, sharp) sign(cY cZ), which holds for
+// either sign of cY cZ); elsewhere windx is 0 and so is its derivative.
+__device__ __forceinline__ float wind_with_grad(float3 x, const PhysParams& pp, float time, float& dwy, float& dwz) {
+    const double two_pi = 2.0 * 3.14159265358979323846;
+    const double ay = two_pi * (double)(pp.wind_yf * x.y + pp.wind_tf * time);
+    const double az = two_pi * (double)(pp.wind_zf * fabsf(x.z) + pp.wind_tf * time);
+    const float wy = x.y > 0.f ? (float)cos(ay) : 0.f;
+    const float wz = (float)cos(az);
+    const float prod = wy * wz;
+    const float sg = prod > 0.f ? 1.f : (prod < 0.f ? -1.f : 0.f);
+    const float pw = powf(prod, pp.wind_sharp) * sg;
+    dwy = 0.f;
+    dwz = 0.f;
+    if (!(0.f < pw)) return 0.f;
+    const float dprod = pp.wind_peak * pp.wind_sharp * pw / prod;
+    const float dy = x.y > 0.f ? (float)(-two_pi * (double)pp.wind_yf * sin(ay)) : 0.f;
+    const float zs = x.z > 0.f ? 1.f : (x.z < 0.f ? -1.f : 0.f);
+    const float dz = (float)(-two_pi * (double)pp.wind_zf * sin(az)) * zs;
+    dwy = dprod * wz * dy;
+    dwz = dprod * wy * dz;
+    return pp.wind_peak * pw;
 }
 
 // Adjoint values a group's warps hand across their tile boundaries (GROUPED: one CTA of K <= 4 warps
@@ -481,23 +508,33 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
         }
     }
 
-    // ---- predict (initItr): dx0 = h v [+ h^2 s ext], y = h v + h^2 ext, vlast_out = v
-    const float3 ext = f3(pp.gx, pp.gy, pp.gz) * pp.ext_mult;
-    const float ext2 = dot3(ext, ext);
+    // ---- predict (initItr): dx0 = h v [+ h^2 s ext], y = h v + h^2 ext, vlast_out = v, where
+    // ext = (g + (windx(x), 0, 0)) * ext_mult and s = clamp(acc . ext / |ext|^2, 0, 1)
 #pragma unroll
     for (int k = 0; k < C; k++) {
         gv[k] = gv[k] + h * gdx[k];
         if (mov[k]) {
+            float dwy = 0.f, dwz = 0.f;
+            const float windx = pp.wind_peak != 0.f ? wind_with_grad(x[k], pp, sp.time, dwy, dwz) : 0.f;
+            const float3 ext = f3(pp.gx + windx, pp.gy, pp.gz) * pp.ext_mult;
+            const float ext2 = dot3(ext, ext);
             gv[k] = gv[k] + h * gy[k];
+            float gex = h * h * gy[k].x;  // d loss / d ext.x
             if (ext2 > 0.f) {
                 const float3 acc = (v[k] - vl[k]) * (1.f / sp.last_h);
                 const float sr = dot3(acc, ext) / ext2;
+                gex += h * h * fminf(fmaxf(sr, 0.f), 1.f) * gdx[k].x;
                 if (sr > 0.f && sr < 1.f) {
-                    const float c = h * h * dot3(ext, gdx[k]) / (sp.last_h * ext2);
+                    const float eg = h * h * dot3(ext, gdx[k]);
+                    const float c = eg / (sp.last_h * ext2);
                     gv[k] = gv[k] + c * ext;
                     gvl[k] = gvl[k] - c * ext;
+                    gex += eg / ext2 * (acc.x - 2.f * sr * ext.x);  // d s / d ext = (acc - 2 s ext) / |ext|^2
                 }
             }
+            const float gw = gex * pp.ext_mult;  // d loss / d windx
+            gx[k].y += gw * dwy;
+            gx[k].z += gw * dwz;
         }
     }
     // ---- segment vectors e_k = x_{k+1} - x_k

@@ -4,8 +4,9 @@ A vectorised torch (float64) version of the same update the C++ oracle restates
 (YarnBall/sim/iteration.cu:8-74, YarnBall/sim/cosserat.cu:112-161, 246-337,
 SDFCollisionSolver/cudaSDFCollision.cu:88-155, 205-268), written so that torch.autograd can
 differentiate a rollout.  It is the FP64 reference gradient for the solver's hand-written
-adjoint, and is only used by tests.  Supported: colour2 schedule, no wind, any substep count,
-SDF pass with a rotated/translated body.  The sign tests of the orientation update and the SDF
+adjoint, and is only used by tests.  Supported: colour2 schedule, wind (iteration.cu:18-30; the
+clock starts at `time` and advances by dt per step), any substep count, SDF pass with a
+rotated/translated body.  The sign tests of the orientation update and the SDF
 branch are treated as constants (their derivative is zero almost everywhere).
 """
 from __future__ import annotations
@@ -44,7 +45,8 @@ class TorchVBD:
     """Holds the static set-up (float64 tensors) of one groom; `step` maps state tensors to state tensors."""
 
     def __init__(self, groom, material, *, num_itr, max_h, gravity, damping=1e-6, velocity_decay=0.05,
-                 accel=1.0, sdf=None, body_rot=(0.0, 0.0, 0.0, 1.0), body_trans=(0.0, 0.0, 0.0)):
+                 accel=1.0, sdf=None, body_rot=(0.0, 0.0, 0.0, 1.0), body_trans=(0.0, 0.0, 0.0),
+                 wind=(0.0, 1.0, 0.7, 0.4, 3.0), ext_mult=1.0, time=0.0):
         t = lambda a: torch.as_tensor(np.asarray(a, np.float64))  # noqa: E731
         self.nv = groom.num_vertices
         sb = groom.strand_begin
@@ -62,6 +64,9 @@ class TorchVBD:
         self.num_itr, self.max_h = num_itr, max_h
         f32 = lambda a: np.asarray(a, np.float32).astype(np.float64)  # noqa: E731  (the oracle takes C floats)
         self.g = t(f32(gravity))
+        self.wind = [float(w) for w in f32(wind)]
+        self.ext_mult = float(f32(ext_mult))
+        self.time = float(np.float32(time))
         self.damping, self.decay, self.accel = float(f32(damping)), float(f32(velocity_decay)), float(f32(accel))
         self.sdf = sdf
         if sdf is not None:
@@ -84,12 +89,27 @@ class TorchVBD:
     def _shift_prev(a):  # a[i-1] at i
         return torch.cat([a[:1], a[:-1]], 0)
 
+    def _wind(self, x):
+        """initItr's wind force along x: peak * max(0, pow(cY cZ, sharp) sign(cY cZ))."""
+        peak, fy, fz, ft, sharp = self.wind
+        ty = 2 * np.pi * (fy * x[:, 1] + ft * self.time)
+        tz = 2 * np.pi * (fz * x[:, 2].abs() + ft * self.time)
+        cy = torch.where(x[:, 1] > 0, torch.cos(ty), torch.zeros_like(ty))
+        p = cy * torch.cos(tz)
+        with torch.no_grad():
+            on = torch.sign(p) * torch.pow(p, sharp) > 0  # NaN (negative base, fractional power) is off
+        ps = torch.where(on, p, torch.ones_like(p))
+        return torch.where(on, peak * torch.sign(ps) * torch.pow(ps, sharp), torch.zeros_like(p))
+
     def _predict(self, x, v, vl, h, last_h):
         free = (self.im != 0)[:, None]
-        ext = self.g
+        ext = self.g * self.ext_mult
+        if self.wind[0] != 0.0:
+            w = self._wind(x) * self.ext_mult
+            ext = ext + torch.stack([w, torch.zeros_like(w), torch.zeros_like(w)], -1)
         dx = h * v
         y = torch.where(free, dx + h * h * ext, v)
-        ext2 = (ext * ext).sum()
+        ext2 = (ext * ext).sum(-1)
         acc = (v - vl) / last_h
         s = torch.clamp((acc * ext).sum(-1) / ext2, 0.0, 1.0)
         dx = torch.where(free, dx + (h * h * s)[:, None] * ext, dx)
@@ -192,4 +212,5 @@ class TorchVBD:
             x = x + dx
         if self.sdf is not None:
             x, v = self._sdf(x, v)
+        self.time = float(np.float32(self.time) + np.float32(dt))  # the solver's float clock
         return (x, v, vl, q, h)

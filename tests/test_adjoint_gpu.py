@@ -12,12 +12,15 @@ pytestmark = pytest.mark.gpu
 GRAD_TOL = 1e-3
 
 
-def _setup(num_strands=24, lengths=(6, 20), seed=5, young_scale=1e-3, sdf=True, num_itr=5, velocities=True):
+def _setup(num_strands=24, lengths=(6, 20), seed=5, young_scale=1e-3, sdf=True, num_itr=5, velocities=True,
+           wind=None):
     import torch
 
     g = helpers.soft_groom(num_strands, lengths, seed=seed, young_scale=young_scale)
     s = synth.sphere_sdf(48, threshold=2e-3) if sdf else None
     st = dict(num_itr=num_itr, max_h=1 / 60, gravity=(0.3, -0.4, -9.81), radius=40e-6, sdf=s)
+    if wind is not None:
+        st["wind"] = wind
     v0 = helpers.random_velocities(g, 0.15, seed=seed + 1) if velocities else None
     solver = helpers.gpu_solver(g, st, form="fused", velocities=v0)
     unit = torch.tensor(solver.get_rest_darboux(), device="cuda")
@@ -34,7 +37,8 @@ def _torch_reference(g, st, v0, scale, frames, c, dt=1 / 60, body=None):
     from oracle.torch_ref import TorchVBD
 
     m = orc.configure(g, radius=st["radius"], dtype=np.float64)
-    tv = TorchVBD(g, m, num_itr=st["num_itr"], max_h=st["max_h"], gravity=st["gravity"], sdf=st["sdf"])
+    kw = {"wind": st["wind"]} if "wind" in st else {}
+    tv = TorchVBD(g, m, num_itr=st["num_itr"], max_h=st["max_h"], gravity=st["gravity"], sdf=st["sdf"], **kw)
     strand_of = torch.tensor(np.repeat(np.arange(g.num_strands), np.diff(g.strand_begin)))
     sc = torch.tensor(np.asarray(scale, np.float64), requires_grad=True)
     x0 = torch.tensor(g.positions.astype(np.float64), requires_grad=True)
@@ -123,6 +127,55 @@ def test_state_adjoint_matches_fp64_autograd():
     solver.backward(ax, av, avl, aq)
     _, _, gx_ref, gv_ref, gq_ref = _torch_reference(g, st, v0, g.strand_dev * 0 + 1, frames, c)
     assert _rel(ax.cpu().numpy(), gx_ref) <= GRAD_TOL
+    assert _rel(av.cpu().numpy(), gv_ref) <= GRAD_TOL
+    assert _rel(aq.cpu().numpy(), gq_ref) <= GRAD_TOL
+    solver.close()
+
+
+@pytest.mark.parametrize("sharpness", [3.0, 2.5])
+def test_wind_adjoint_matches_fp64_autograd(sharpness):
+    """Wind on (initItr's force along x, a function of each vertex's y and z and of the clock): the
+    stiffness gradient through the autograd binding and the adjoint of the initial state, whose y and
+    z enter the wind force.  An odd integer sharpness blows for either sign of cY cZ, a fractional one
+    only where it is positive."""
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+
+    wind = (6.0, 1.0, 0.7, 0.4, sharpness)
+    g, st, solver, unit, strand_of, init, v0 = _setup(num_strands=24, lengths=(6, 20), seed=31, sdf=True, wind=wind)
+    rng = np.random.default_rng(12)
+    scale0 = rng.uniform(0.7, 1.4, g.num_strands).astype(np.float32)
+    c = rng.normal(size=(g.num_vertices, 3))
+    frames = 6
+    scale = torch.tensor(scale0, device="cuda", requires_grad=True)
+    x = rollout_positions(scale, solver, unit, strand_of, init, frames, 1 / 60, checkpoint_every=3)
+    loss = (torch.tensor(c, dtype=torch.float32, device="cuda") * x).sum()
+    loss.backward()
+    l_ref, g_ref, gx_ref, gv_ref, gq_ref = _torch_reference(g, st, v0, scale0, frames, c)
+    calm = dict(st)
+    calm.pop("wind")
+    l_calm, g_calm, gx_calm, *_ = _torch_reference(g, calm, v0, scale0, frames, c)
+    assert _rel(g_calm, g_ref) > 1e-2  # the wind changes the gradient
+    assert abs(loss.item() - l_ref) <= 1e-4 * abs(l_ref) + 1e-6
+    g_gpu = scale.grad.cpu().numpy()
+    assert _rel(g_gpu, g_ref) <= GRAD_TOL, (_rel(g_gpu, g_ref), g_gpu[:5], g_ref[:5])
+    # the state adjoint: the same rollout recorded at unit stiffness scale
+    _, _, gx_ref, gv_ref, gq_ref = _torch_reference(g, st, v0, np.ones(g.num_strands, np.float32), frames, c)
+    _, _, gx_calm, *_ = _torch_reference(g, calm, v0, np.ones(g.num_strands, np.float32), frames, c)
+    torch.cuda.synchronize()
+    solver.set_rest_darboux(unit.contiguous())
+    solver.set_state_from(init)
+    solver.tape_reserve(frames, 0)
+    for _ in range(frames):
+        solver.step_record(1 / 60)
+    ax = torch.tensor(c, dtype=torch.float32, device="cuda")
+    av, avl = torch.zeros_like(ax), torch.zeros_like(ax)
+    aq = torch.zeros((g.num_vertices, 4), dtype=torch.float32, device="cuda")
+    torch.cuda.synchronize()
+    solver.backward(ax, av, avl, aq)
+    assert _rel(gx_calm, gx_ref) > 1e-2  # the wind's dependence on y and z shows in d loss / d x0
+    assert _rel(ax.cpu().numpy(), gx_ref) <= GRAD_TOL, _rel(ax.cpu().numpy(), gx_ref)
     assert _rel(av.cpu().numpy(), gv_ref) <= GRAD_TOL
     assert _rel(aq.cpu().numpy(), gq_ref) <= GRAD_TOL
     solver.close()

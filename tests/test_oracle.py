@@ -307,3 +307,29 @@ def test_flop_count_pins_the_roofline_constant():
     consts = {n.targets[0].id: n.value.value for n in ast.parse(src).body
               if isinstance(n, ast.Assign) and isinstance(n.targets[0], ast.Name) and isinstance(n.value, ast.Constant)}
     assert consts["REFERENCE_FLOP_PER_VERTEX_ITER"] == pos + ori
+
+
+@pytest.mark.parametrize("wind", [(0.0, 1.0, 0.7, 0.4, 3.0), (6.0, 1.0, 0.7, 0.4, 3.0), (6.0, 1.0, 0.7, 0.4, 2.5)])
+def test_fp64_autograd_restatement_follows_the_fp64_oracle(wind):
+    """oracle/torch_ref.py, the FP64 reference of the adjoint tests, against the FP64 oracle over 6
+    frames: SDF on, and wind off, with an odd integer sharpness and with a fractional one."""
+    import torch
+
+    from oracle.torch_ref import TorchVBD
+
+    g = helpers.soft_groom(24, (6, 20), seed=31, young_scale=1e-3)
+    v0 = helpers.random_velocities(g, 0.15, seed=32)
+    sdf = synth.sphere_sdf(48, threshold=2e-3)
+    st = dict(num_itr=5, max_h=1 / 60, gravity=(0.3, -0.4, -9.81), radius=40e-6)
+    o = orc.OracleSim(g, dtype=np.float64, wind=wind, sdf=sdf, velocities=v0, **st)
+    m = orc.configure(g, radius=st["radius"], dtype=np.float64)
+    tv = TorchVBD(g, m, num_itr=5, max_h=1 / 60, gravity=st["gravity"], sdf=sdf, wind=wind)
+    state = (torch.tensor(g.positions.astype(np.float64)), torch.tensor(v0.astype(np.float64)),
+             torch.zeros(g.num_vertices, 3, dtype=torch.float64), torch.tensor(m["q"]), float(np.float32(1 / 60)))
+    qr = torch.tensor(m["q_rest"])
+    for _ in range(6):
+        state = tv.step(state, qr, 1 / 60)
+        o.advance(1 / 60)
+    # the oracle rounds the wind's cosine argument to float, as the reference does
+    np.testing.assert_allclose(state[0].numpy(), o.x, rtol=0, atol=1e-9)
+    np.testing.assert_allclose(state[3].numpy(), o.q, rtol=0, atol=1e-8)
