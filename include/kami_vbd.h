@@ -328,16 +328,16 @@ kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int3
 kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, int32_t best[4], double* best_rate);
 
 /* ---- differentiable stepping ---------------------------------------------------------------------
- * No counterpart in the reference, which has no adjoint.  The fused colour2 step (no wind, one
- * substep per step) can record its iterates on a tape; kami_vbd_backward then runs the hand-written
+ * No counterpart in the reference, which has no adjoint.  The fused colour2 step (wind, SDF and any
+ * number of substeps) can record its iterates on a tape; kami_vbd_backward then runs the hand-written
  * adjoint of the recorded steps in reverse.  Typical use, checkpointing every k steps: restore a
  * checkpoint with kami_vbd_set_state, record the k steps of that segment, call kami_vbd_backward
  * with the adjoint of the segment's final state, and continue with the next earlier segment. */
 
-/* Allocates a tape for up to max_steps recorded steps of up to max_tiles warp tiles (0 = all tiles;
+/* Allocates a tape for up to max_steps recorded substeps of up to max_tiles warp tiles (0 = all tiles;
  * rounded up to whole groups of tiles) and the adjoint buffers (d loss / d qRest starts at zero); the
- * tile window starts as the first max_tiles tiles.  A tape step costs (num_itr + 1) * 32 + 48 B per
- * slot.  KAMI_ERR_UNSUPPORTED for the sweep form, the Jacobi schedule, or strands longer than 4 tiles
+ * tile window starts as the first max_tiles tiles.  A tape substep costs (num_itr + 1) * 32 + 48 B
+ * per slot.  KAMI_ERR_UNSUPPORTED for the sweep form, the Jacobi schedule, or strands longer than 4 tiles
  * (groups of more than 4 tiles). */
 kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps, int64_t max_tiles);
 
@@ -354,7 +354,8 @@ kami_status kami_vbd_get_tiles_per_group(kami_vbd_handle h, int32_t* tiles_per_g
  * kami_vbd_backward; the adjoint of vertices outside the window passes through unchanged. */
 kami_status kami_vbd_set_tape_window(kami_vbd_handle h, int64_t tile_begin, int64_t tile_end);
 
-/* kami_vbd_step that also records its iterates; dt must not exceed max_h (a single substep). */
+/* kami_vbd_step that also records its iterates.  A step of ceil(dt / max_h) substeps takes as many
+ * of the tape's max_steps entries (one per substep; KAMI_ERR_STATE when they do not fit). */
 kami_status kami_vbd_step_record(kami_vbd_handle h, float dt, void* stream);
 
 /* In: the adjoint (d loss / d state) of the state after the last recorded step, boundary order:

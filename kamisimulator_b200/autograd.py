@@ -11,7 +11,7 @@ groups of tiles when strands run across several), so the tape memory is bounded 
 the window: (num_itr + 1) * 32 + 48 B per slot and recorded step.  ``body_transforms`` ((frames, 7):
 rotation x y z w, translation per frame) moves the body SDF frame by frame, in the forward pass and
 in the recorded steps alike.  The solver must use the fused form with the colour2 schedule (wind is
-allowed) and dt <= max_h.
+allowed); a frame of several substeps (dt > max_h) is recorded substep by substep.
 """
 from __future__ import annotations
 
@@ -57,7 +57,7 @@ class StrandStiffnessRollout(torch.autograd.Function):
         chunk = ctx.chunk if 0 < ctx.chunk < tiles else tiles
         group = solver.tiles_per_group()  # tape windows are whole groups of tiles
         chunk = min(tiles, -(-chunk // group) * group)
-        solver.tape_reserve(k, chunk)
+        solver.tape_reserve(k * solver.substeps(ctx.dt), chunk)  # one tape entry per substep
         solver.zero_rest_darboux_grad()
         torch.cuda.synchronize()
         for t0 in range(0, tiles, chunk):

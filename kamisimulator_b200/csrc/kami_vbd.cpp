@@ -119,7 +119,11 @@ struct kami_vbd_solver {
     int tape_capacity = 0;
     int64_t tape_tiles = 0;               // tiles the tape holds per step
     int64_t win_begin = 0, win_end = 0;   // tile window that recording and the adjoint cover
-    std::vector<StepParams> tape_steps;
+    struct TapeStep {
+        StepParams sp;  // one substep (sp.substeps == 1) of a recorded advance
+        bool sdf;       // the advance's last substep, which ends with the body pass
+    };
+    std::vector<TapeStep> tape_steps;
     float4 *d_tdx = nullptr, *d_tq = nullptr, *d_tx = nullptr, *d_tv = nullptr, *d_tvl = nullptr;
     float4 *d_gx = nullptr, *d_gv = nullptr, *d_gvl = nullptr, *d_gq = nullptr, *d_gqr = nullptr;
 
@@ -1326,21 +1330,29 @@ kami_status kami_vbd_set_tape_window(kami_vbd_handle h, int64_t tile_begin, int6
 kami_status kami_vbd_step_record(kami_vbd_handle h, float dt, void* stream) {
     KAMI_TRY(valid_handle(h));
     if (h->tape_capacity == 0) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
-    if ((int)h->tape_steps.size() >= h->tape_capacity)
-        return fail(KAMI_ERR_STATE, "the tape holds %d steps; run kami_vbd_backward first", h->tape_capacity);
     if (!(dt > 0.f) || !std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite and > 0");
-    if (std::max(1, (int)std::ceil(dt / h->max_h)) != 1)
-        return fail(KAMI_ERR_UNSUPPORTED, "recorded steps must be single substeps (dt <= max_h)");
+    const int substeps = std::max(1, (int)std::ceil(dt / h->max_h));
+    if ((int)h->tape_steps.size() + substeps > h->tape_capacity)
+        return fail(KAMI_ERR_STATE, "the tape holds %d substeps, %d are recorded and this step takes %d; run "
+                    "kami_vbd_backward first or reserve more", h->tape_capacity, (int)h->tape_steps.size(), substeps);
     const StepParams sp = advance_clock(h, dt);
-    const int step = (int)h->tape_steps.size();
+    // Sim::advance keeps h, lastH, time and the body fixed over its substeps and runs the body pass once
+    // after them (step.cpp:38-62), so each substep is recorded as a one-substep launch of its own and
+    // only the last one ends with the SDF pass
+    StepParams sp1 = sp;
+    sp1.substeps = 1;
+    SdfParams no_sdf = h->sdf;
+    no_sdf.grid = nullptr;
+    const int first = (int)h->tape_steps.size();
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
-        KAMI_CUDA(launch_fused_record(h->window_state(), h->pp, sp, h->sdf, h->tape(step), h->layout.C,
-                                      h->warps_per_block, s, h->layout.K),
-                  "recorded step launch");
+        for (int k = 0; k < substeps; k++)
+            KAMI_CUDA(launch_fused_record(h->window_state(), h->pp, sp1, k == substeps - 1 ? h->sdf : no_sdf,
+                                          h->tape(first + k), h->layout.C, h->warps_per_block, s, h->layout.K),
+                      "recorded step launch");
         return KAMI_OK;
     });
     if (st != KAMI_OK) return st;
-    h->tape_steps.push_back(sp);
+    for (int k = 0; k < substeps; k++) h->tape_steps.push_back({sp1, k == substeps - 1});
     h->time += dt;
     h->counter += sp.substeps;
     return KAMI_OK;
@@ -1370,10 +1382,14 @@ kami_status kami_vbd_backward(kami_vbd_handle h, float* adj_x, float* adj_v, flo
     KAMI_TRY(stage_in(h, adj_q, 4, memory));
     KAMI_CUDA(launch_scatter4((const float4*)h->d_stage, h->d_gq, h->d_slot_of, h->nv, h->stream), "scatter adjoint");
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
-        for (int step = (int)h->tape_steps.size() - 1; step >= 0; step--)
-            KAMI_CUDA(launch_adjoint_step(h->window_state(), h->pp, h->tape_steps[step], h->sdf, h->tape(step), ad,
+        SdfParams no_sdf = h->sdf;
+        no_sdf.grid = nullptr;
+        for (int step = (int)h->tape_steps.size() - 1; step >= 0; step--) {
+            const auto& ts = h->tape_steps[step];
+            KAMI_CUDA(launch_adjoint_step(h->window_state(), h->pp, ts.sp, ts.sdf ? h->sdf : no_sdf, h->tape(step), ad,
                                           h->layout.C, s, h->layout.K),
                       "adjoint step launch");
+        }
         return KAMI_OK;
     });
     if (st != KAMI_OK) return st;

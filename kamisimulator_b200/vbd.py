@@ -10,6 +10,7 @@ compiled library every call raises.
 from __future__ import annotations
 
 import ctypes
+import math
 import os
 
 import numpy as np
@@ -283,7 +284,12 @@ class Solver:
         ng = ctypes.c_int32()
         _check(self.lib.kami_vbd_batch_count(h, ctypes.byref(ng)))
         self.num_grooms = ng.value
+        self.max_h = float(np.float32(max_h))
         del keep
+
+    def substeps(self, dt):
+        """Substeps of one step of dt, ceil(dt / max_h) in float as kami_vbd_step takes them."""
+        return max(1, math.ceil(np.float32(dt) / np.float32(self.max_h)))
 
     def groom_range(self, groom):
         """(first strand, strands, first vertex, vertices) of one groom of a batch handle."""

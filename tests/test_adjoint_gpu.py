@@ -13,12 +13,12 @@ GRAD_TOL = 1e-3
 
 
 def _setup(num_strands=24, lengths=(6, 20), seed=5, young_scale=1e-3, sdf=True, num_itr=5, velocities=True,
-           wind=None):
+           wind=None, max_h=1 / 60):
     import torch
 
     g = helpers.soft_groom(num_strands, lengths, seed=seed, young_scale=young_scale)
     s = synth.sphere_sdf(48, threshold=2e-3) if sdf else None
-    st = dict(num_itr=num_itr, max_h=1 / 60, gravity=(0.3, -0.4, -9.81), radius=40e-6, sdf=s)
+    st = dict(num_itr=num_itr, max_h=max_h, gravity=(0.3, -0.4, -9.81), radius=40e-6, sdf=s)
     if wind is not None:
         st["wind"] = wind
     v0 = helpers.random_velocities(g, 0.15, seed=seed + 1) if velocities else None
@@ -178,6 +178,36 @@ def test_wind_adjoint_matches_fp64_autograd(sharpness):
     assert _rel(ax.cpu().numpy(), gx_ref) <= GRAD_TOL, _rel(ax.cpu().numpy(), gx_ref)
     assert _rel(av.cpu().numpy(), gv_ref) <= GRAD_TOL
     assert _rel(aq.cpu().numpy(), gq_ref) <= GRAD_TOL
+    solver.close()
+
+
+def test_substeps_adjoint_matches_fp64_autograd():
+    """Frames of 3 substeps (max_h = dt / 3) with wind: each substep is a tape entry, and the SDF pass
+    ends only a frame's last substep, as Sim::advance runs the body pass once per call."""
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+    from kamisimulator_b200.vbd import KamiError
+
+    g, st, solver, unit, strand_of, init, v0 = _setup(num_strands=24, lengths=(6, 20), seed=37, sdf=True,
+                                                      wind=(6.0, 1.0, 0.7, 0.4, 3.0), max_h=1 / 180)
+    assert solver.substeps(1 / 60) == 3
+    solver.tape_reserve(2, 0)
+    with pytest.raises(KamiError):
+        solver.step_record(1 / 60)  # 3 substeps do not fit 2 tape entries
+    solver.set_state_from(init)
+    rng = np.random.default_rng(14)
+    scale0 = rng.uniform(0.7, 1.4, g.num_strands).astype(np.float32)
+    c = rng.normal(size=(g.num_vertices, 3))
+    frames = 4
+    scale = torch.tensor(scale0, device="cuda", requires_grad=True)
+    x = rollout_positions(scale, solver, unit, strand_of, init, frames, 1 / 60, checkpoint_every=2, tiles_per_chunk=2)
+    loss = (torch.tensor(c, dtype=torch.float32, device="cuda") * x).sum()
+    loss.backward()
+    l_ref, g_ref, *_ = _torch_reference(g, st, v0, scale0, frames, c)
+    assert abs(loss.item() - l_ref) <= 1e-4 * abs(l_ref) + 1e-6
+    g_gpu = scale.grad.cpu().numpy()
+    assert _rel(g_gpu, g_ref) <= GRAD_TOL, (_rel(g_gpu, g_ref), g_gpu[:5], g_ref[:5])
     solver.close()
 
 
