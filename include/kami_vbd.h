@@ -337,8 +337,7 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
 /* Allocates a tape for up to max_steps recorded substeps of up to max_tiles warp tiles (0 = all tiles;
  * rounded up to whole groups of tiles) and the adjoint buffers (d loss / d qRest starts at zero); the
  * tile window starts as the first max_tiles tiles.  A tape substep costs (num_itr + 1) * 32 + 48 B
- * per slot.  KAMI_ERR_UNSUPPORTED for the sweep form, the Jacobi schedule, or strands longer than 4 tiles
- * (groups of more than 4 tiles). */
+ * per slot.  KAMI_ERR_UNSUPPORTED for the sweep form or the Jacobi schedule. */
 kami_status kami_vbd_tape_reserve(kami_vbd_handle h, int32_t max_steps, int64_t max_tiles);
 
 /* Number of warp tiles of the device layout. */

@@ -1250,8 +1250,6 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
 static kami_status adjoint_supported(kami_vbd_solver* h) {
     if (h->form != KAMI_FORM_FUSED || h->schedule != KAMI_SCHEDULE_COLOUR2)
         return fail(KAMI_ERR_UNSUPPORTED, "the adjoint covers the fused form with the colour2 schedule");
-    if (h->layout.K > 4)
-        return fail(KAMI_ERR_UNSUPPORTED, "the adjoint covers groups of up to 4 tiles (strands of up to 512 vertices)");
     return KAMI_OK;
 }
 

@@ -204,28 +204,30 @@ __device__ __forceinline__ float wind_with_grad(float3 x, const PhysParams& pp, 
     return pp.wind_peak * pw;
 }
 
-// Adjoint values a group's warps hand across their tile boundaries (GROUPED: one CTA of K <= 4 warps
+// Adjoint values a group's warps hand across their tile boundaries (GROUPED: one CTA of NW = K warps
 // per group of tiles, as GroupExchange in vbd_fused.cuh): `up` from lane 31 of warp w to lane 0 of
 // warp w + 1, `down` from lane 0 of warp w to lane 31 of warp w - 1.  Each slot is written once per
 // iteration and the next write comes after further __syncthreads that its readers have passed.
 enum : int { AU_QR, AU_DD, AU_TQ, AU_TV, AU_QO, AU_F0, AU_GE, AU_N };
 enum : int { AD_X, AD_QN, AD_DXN, AD_PN, AD_FN, AD_N };
+template <int NW>
 struct AdjointExchange {
-    float4 up[4][AU_N];
-    float4 down[4][AD_N];
+    float4 up[NW][AU_N];
+    float4 down[NW][AD_N];
 };
 
-// MINB blocks of 128 threads per SM: MINB = 4 caps the registers at 128 so 16 warps share an SM.
-template <int C, int MINB, bool GROUPED = false>
-__global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
-                                                           TapeView tp, AdjointState ad) {
+// MINB blocks of NT threads per SM: (128, 4) caps the registers at 128 so 16 warps share an SM.
+// NT = 256 is the instantiation for groups of 8 tiles; its prefetch buffer is dynamic shared memory.
+template <int C, int MINB, bool GROUPED = false, int NT = 128>
+__global__ void __launch_bounds__(NT, MINB) adjoint_step_kernel(DeviceState st, PhysParams pp, StepParams sp,
+                                                                SdfParams sdf, TapeView tp, AdjointState ad) {
     const int lane = threadIdx.x & 31;
     const int64_t tile = tp.tile_begin + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (tile >= st.num_tiles) return;  // uniform per warp (per CTA for groups)
     const int gw = threadIdx.x >> 5, gK = blockDim.x >> 5;
-    AdjointExchange* gx_ = nullptr;
+    AdjointExchange<NT / 32>* gx_ = nullptr;
     if constexpr (GROUPED) {
-        __shared__ AdjointExchange adjoint_exchange;
+        __shared__ AdjointExchange<NT / 32> adjoint_exchange;
         gx_ = &adjoint_exchange;
     }
     // neighbours across the warps of a group; at a group's ends (and without groups) the previous /
@@ -336,8 +338,14 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
     // one iteration are the "after" values of the next one down, so each tape row is read once.  The
     // row of the next iteration down is prefetched into shared memory (double buffer per warp) while
     // the current one is reversed.
-    __shared__ float4 pref[4][2][2][C][32];  // [warp in CTA][buffer][dx | q][slot row][lane]
-    float4 (*mine)[2][C][32] = pref[threadIdx.x >> 5];
+    float4 (*mine)[2][C][32];  // this warp's [buffer][dx | q][slot row][lane]
+    if constexpr (NT <= 128) {
+        __shared__ float4 pref[4][2][2][C][32];  // [warp in CTA][buffer][dx | q][slot row][lane]
+        mine = pref[threadIdx.x >> 5];
+    } else {  // 8 warps: 32 KB (C = 2) or 64 KB (C = 4), in dynamic shared memory
+        extern __shared__ float4 adjoint_pref[];
+        mine = reinterpret_cast<float4 (*)[2][C][32]>(adjoint_pref + (size_t)(threadIdx.x >> 5) * 2 * 2 * C * 32);
+    }
     float3 dxn[C], dxo[C];
     float4 qn[C], qo[C];
 #pragma unroll
@@ -532,9 +540,9 @@ __global__ void __launch_bounds__(128, MINB) adjoint_step_kernel(DeviceState st,
                     gex += eg / ext2 * (acc.x - 2.f * sr * ext.x);  // d s / d ext = (acc - 2 s ext) / |ext|^2
                 }
             }
-            const float gw = gex * pp.ext_mult;  // d loss / d windx
-            gx[k].y += gw * dwy;
-            gx[k].z += gw * dwz;
+            const float gwind = gex * pp.ext_mult;  // d loss / d windx
+            gx[k].y += gwind * dwy;
+            gx[k].z += gwind * dwz;
         }
     }
     // ---- segment vectors e_k = x_{k+1} - x_k
@@ -585,11 +593,26 @@ cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, con
 
 cudaError_t launch_adjoint_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                                 const TapeView& tp, const AdjointState& ad, int C, cudaStream_t s, int group) {
-    if (group > 1) {  // one CTA of `group` <= 4 warps per group of tiles
+    if (group > 1) {  // one CTA of `group` warps per group of tiles
         const int64_t tiles = st.num_tiles - tp.tile_begin;
-        if (group > 4 || tiles % group != 0 || tp.tile_begin % group != 0) return cudaErrorInvalidValue;
+        if ((group != 2 && group != 4 && group != 8) || tiles % group != 0 || tp.tile_begin % group != 0)
+            return cudaErrorInvalidValue;
         if (tiles == 0) return cudaSuccess;
         const unsigned gblocks = (unsigned)(tiles / group);
+        if (group == 8) {
+            const size_t smem = sizeof(float4) * 8 * 2 * 2 * C * 32;  // the per-warp prefetch buffers
+            if (C == 2) {
+                adjoint_step_kernel<2, 2, true, 256><<<gblocks, 256, smem, s>>>(st, pp, sp, sdf, tp, ad);
+            } else if (C == 4) {
+                static const cudaError_t attr = cudaFuncSetAttribute(
+                    adjoint_step_kernel<4, 1, true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                if (attr != cudaSuccess) return attr;
+                adjoint_step_kernel<4, 1, true, 256><<<gblocks, 256, smem, s>>>(st, pp, sp, sdf, tp, ad);
+            } else {
+                return cudaErrorInvalidValue;
+            }
+            return cudaGetLastError();
+        }
         if (C == 2)
             adjoint_step_kernel<2, 4, true><<<gblocks, 32 * group, 0, s>>>(st, pp, sp, sdf, tp, ad);
         else if (C == 4)

@@ -31,7 +31,7 @@ cudaError_t launch_fused_frame(const DeviceState& st, const PhysParams& pp, cons
                                const HostIO& hio, int C, bool jacobi, int warps_per_block, cudaStream_t s, int reg_cap,
                                int group = 1);
 
-// group > 1: groups of tiles, one CTA of `group` warps each (the adjoint takes groups of up to 4);
+// group > 1: groups of tiles, one CTA of `group` warps each (2, 4 or 8);
 // the tape window must be whole groups.
 cudaError_t launch_fused_record(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                                 const TapeView& tp, int C, int warps_per_block, cudaStream_t s, int group = 1);

@@ -94,8 +94,6 @@ def test_long_strands_step_n_and_host_frames():
 
 
 def test_long_strands_autotune_and_adjoint_scope():
-    from kamisimulator_b200.vbd import KamiError
-
     g = _mixed(seed=8)
     st = _settings()
     s = helpers.gpu_solver(g, st, form="fused")
@@ -104,12 +102,8 @@ def test_long_strands_autotune_and_adjoint_scope():
     best, rate = s.autotune(1 / 120, trial_steps=4)
     assert best[0] in (2, 4) and best[3] in (1, 120, 168) and rate > 0
     np.testing.assert_array_equal(s.get_state(), before)
-    # the adjoint covers groups of up to 4 tiles; the tuning picked decides the group size
-    if s.tiles_per_group() > 4:
-        with pytest.raises(KamiError):
-            s.tape_reserve(2)
-    else:
-        s.tape_reserve(2)
+    s.tape_reserve(2)  # the adjoint covers every group size the tuning may pick
+    s.step_record(1 / 120)
     s.close()
 
 
