@@ -81,17 +81,21 @@ __device__ __forceinline__ OrientationAdjoint orientation_adjoint(float4 qbar, f
     s2 = nxt ? s2 : 0.f;
     const float4 b = make_float4(s1 * P1.x + s2 * P2.x, s1 * P1.y + s2 * P2.y, s1 * P1.z + s2 * P2.z,
                                  s1 * P1.w + s2 * P2.w);
-    const float nV = sqrtf(dot3(V, V)), nb = sqrtf(dot4(b, b));
+    // |V|, |b| and 1 / |R| as fused_orientation takes them (rsqrt forms), with the reciprocals the
+    // reverse needs: 1 / |V| = iV and 1 / |b| = ib wherever the norm is above 1e-15
+    const float vv = dot3(V, V), bb2 = dot4(b, b);
+    const float iV = rsqrt_ftz(fmaxf(vv, 1e-30f)), ib = rsqrt_ftz(fmaxf(bb2, 1e-30f));
+    const float nV = vv * iV, nb = bb2 * ib;
     const float lambda = nV + nb;
     const float3 bq = f3(b.x, b.y, b.z);
     const float3 Pq = b.w * V + cross3(V, bq);
     const float Pw = -dot3(V, bq);
     const float4 R = make_float4(Pw + lambda * b.x, Pq.z + lambda * b.y, -Pq.y + lambda * b.z, -Pq.x + lambda * b.w);
-    const float nR = sqrtf(dot4(R, R));
-    const float4 n = scale4(1.f / nR, R);
+    const float iR = rsqrt_ftz(dot4(R, R));
+    const float4 n = scale4(iR, R);
     // normalisation
     const float nq = dot4(n, qbar);
-    const float4 Rb = scale4(1.f / nR, make_float4(qbar.x - n.x * nq, qbar.y - n.y * nq, qbar.z - n.z * nq, qbar.w - n.w * nq));
+    const float4 Rb = scale4(iR, make_float4(qbar.x - n.x * nq, qbar.y - n.y * nq, qbar.z - n.z * nq, qbar.w - n.w * nq));
     // R = (Pw + l b.x, Pq.z + l b.y, -Pq.y + l b.z, -Pq.x + l b.w)
     const float Pwb = Rb.x;
     const float3 Pqb = f3(-Rb.w, -Rb.z, Rb.y);
@@ -105,8 +109,8 @@ __device__ __forceinline__ OrientationAdjoint orientation_adjoint(float4 qbar, f
     bb.z += bqb.z;
     bb.w += dot3(V, Pqb);
     // lambda = |V| + |b|
-    if (nV > 0.f) Vb = Vb + (lb / nV) * V;
-    if (nb > 0.f) bb = add4(bb, scale4(lb / nb, b));
+    if (nV > 0.f) Vb = Vb + (lb * iV) * V;
+    if (nb > 0.f) bb = add4(bb, scale4(lb * ib, b));
     const float4 P1b = scale4(s1, bb), P2b = scale4(s2, bb);
     o.p1bar = P1b;
     o.q_next = qmul_fma(P2b, qr);         // d/d qNext of qNext conj(qr)
