@@ -297,6 +297,12 @@ kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
                 std::swap(dx_cur, dx_alt);
                 if (err == cudaSuccess) err = launch_sweep_orientation(st, dx_cur, q_cur, q_alt, C, 0, true, s);
                 std::swap(q_cur, q_alt);
+            } else if (h->hair_hair && h->layout.K == 1 && coll_iteration_supported(C)) {
+                // the whole iteration in one launch: partners read dx_cur, the result goes to the other of
+                // d_dx and d_snap (a colour2 handle has no d_dx2; its snapshot buffer is free here)
+                float4* other = dx_cur == h->d_dx ? h->d_snap : h->d_dx;
+                err = launch_coll_iteration(st, h->d_y, q_cur, dx_cur, other, h->d_step, h->pp, h->cp, s);
+                dx_cur = other;
             } else if (h->hair_hair) {
                 err = cudaMemcpyAsync(h->d_snap, dx_cur, b4, cudaMemcpyDeviceToDevice, s);  // partners' dx
                 for (int c = 0; c < 2 && err == cudaSuccess; c++)

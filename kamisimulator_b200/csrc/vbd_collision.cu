@@ -325,9 +325,66 @@ __device__ __forceinline__ void contact_term(const DeviceState& st, const CollPa
     }
 }
 
-// The position sweep of the sweep form with hair-hair contacts: cosseratItr (cosserat.cu:112-285)
-// with its full 3x3 block and the step-limit clamp.  Thread mapping and the in-place (colour2) /
-// double-buffered (jacobi) update as in sweep_position_kernel; `snap` holds the partners' dx.
+// cosseratItr with contacts for one vertex (cosserat.cu:112-285): the full 3x3 block (hess3(m/h^2),
+// stretch, and each contact's IPC barrier and friction terms for the vertex's two segments), solved
+// with glm's adjugate inverse and clamped to the segments' step limit.  The in-strand operands are
+// the current iterate: the next vertex (xj, dxj), this segment's orientation qg, the previous
+// vertex (xp, dp, its prm pp4) and its segment's orientation qgp; gn / gp are read only when the
+// flags say the neighbour exists.  Partners' dx come from `snap`.
+__device__ __forceinline__ float3 coll_position(const DeviceState& st, const CollParams& cp, const float4* snap,
+                                                int64_t g, int64_t gp, uint32_t fl, float4 xm, float4 prm, float3 vi_dx,
+                                                float3 yv, float3 xj, float3 vj_dx, float4 qg, float3 xp, float3 dp,
+                                                float4 qgp, float4 pp4, float h, const PhysParams& pp) {
+    const float damp = pp.damping / h;
+    const float im = xm.w;
+    const float3 vi = xyz(xm);
+    float H[6];
+    const float inert = 1.f / (im * h * h);
+#pragma unroll
+    for (int n = 0; n < 6; n++) H[n] = inert;  // hess3(float) fills all six entries (SymMat.h:16-18)
+    float3 f = (1.f / (h * h * im)) * (yv - vi_dx);
+    float step_limit = INFINITY;
+    if (fl & F_HAS_NEXT) {
+        const float invl = 1.f / prm.x;
+        const float3 cc = ((xj - vi) + (vj_dx - vi_dx)) * invl - d3_of(qg);
+        const float kk = prm.y * invl;
+        float dd = kk * invl;
+        f = f + (kk * cc - (damp * dd) * vi_dx);
+        dd *= 1.f + damp;
+        H[0] += dd;
+        H[1] += dd;
+        H[2] += dd;
+        step_limit = cp.maxstep[g];
+        const int n = cp.ncols[g];
+        for (int m = 0; m < n; m++)
+            contact_term(st, cp, snap, vi, xj, vi_dx, vj_dx, cp.cols[(int64_t)m * cp.num_slots + g], true, damp, f, H);
+    }
+    if (fl & F_HAS_PREV) {
+        const float invl = 1.f / pp4.x;
+        const float3 cc = ((vi - xp) + (vi_dx - dp)) * invl - d3_of(qgp);
+        const float kk = pp4.y * invl;
+        float dd = kk * invl;
+        float3 f2 = (-kk) * cc - (damp * dd) * vi_dx;
+        dd *= 1.f + damp;
+        float H2[6] = {dd, dd, dd, 0.f, 0.f, 0.f};
+        const int n = cp.ncols[gp];
+        for (int m = 0; m < n; m++)
+            contact_term(st, cp, snap, xp, vi, dp, vi_dx, cp.cols[(int64_t)m * cp.num_slots + gp], false, damp, f2, H2);
+        step_limit = fminf(step_limit, cp.maxstep[gp]);
+        f = f + f2;
+#pragma unroll
+        for (int q = 0; q < 6; q++) H[q] += H2[q];
+    }
+    const float3 delta = pp.accel_ratio * solve_sym3(H, f);
+    float3 out = vi_dx + delta;
+    const float l = sqrtf(len2(out));
+    if (l > step_limit && l > 0.f) out = out * (step_limit / l);
+    return out;
+}
+
+// The position sweep of the sweep form with hair-hair contacts (one thread per slot of one colour,
+// or of all slots under jacobi), in place (colour2) or double-buffered (jacobi) as in
+// sweep_position_kernel; `snap` holds the partners' dx.
 template <bool JACOBI>
 __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restrict__ y4, const float4* __restrict__ qcur,
                                            const float4* dx_in, float4* dx_out, const float4* snap,
@@ -350,57 +407,84 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
         if (JACOBI) dx_out[g] = d4;
         return;
     }
-    const float h = spp->h;
-    const float damp = pp.damping / h;
-    const float im = xm.w;
-    const float3 vi = xyz(xm), vi_dx = xyz(d4);
-    float H[6];
-    const float inert = 1.f / (im * h * h);
-#pragma unroll
-    for (int n = 0; n < 6; n++) H[n] = inert;  // hess3(float) fills all six entries (SymMat.h:16-18)
-    float3 f = (1.f / (h * h * im)) * (xyz(y4[g]) - vi_dx);
-    float step_limit = INFINITY;
+    const float3 zero = f3(0.f, 0.f, 0.f);
+    const float4 unit = make_float4(0.f, 0.f, 0.f, 1.f);
+    float3 xj = zero, vj_dx = zero, xp = zero, dp = zero;
+    float4 qgp = unit, pp4 = make_float4(1.f, 0.f, 0.f, 0.f);
+    int64_t gp = g;
     if (fl & F_HAS_NEXT) {
         const int64_t gn = next_slot(g, C);
-        const float3 xj = xyz(st.xm[gn]), vj_dx = xyz(dx_in[gn]);
-        const float invl = 1.f / prm.x;
-        const float3 cc = ((xj - vi) + (vj_dx - vi_dx)) * invl - d3_of(qcur[g]);
-        const float kk = prm.y * invl;
-        float dd = kk * invl;
-        f = f + (kk * cc - (damp * dd) * vi_dx);
-        dd *= 1.f + damp;
-        H[0] += dd;
-        H[1] += dd;
-        H[2] += dd;
-        step_limit = cp.maxstep[g];
-        const int n = cp.ncols[g];
-        for (int m = 0; m < n; m++)
-            contact_term(st, cp, snap, vi, xj, vi_dx, vj_dx, cp.cols[(int64_t)m * cp.num_slots + g], true, damp, f, H);
+        xj = xyz(st.xm[gn]);
+        vj_dx = xyz(dx_in[gn]);
     }
     if (fl & F_HAS_PREV) {
-        const int64_t gp = prev_slot(g, C);
-        const float4 pp4 = st.prm[gp];
-        const float3 xp = xyz(st.xm[gp]), dp = xyz(dx_in[gp]);
-        const float invl = 1.f / pp4.x;
-        const float3 cc = ((vi - xp) + (vi_dx - dp)) * invl - d3_of(qcur[gp]);
-        const float kk = pp4.y * invl;
-        float dd = kk * invl;
-        float3 f2 = (-kk) * cc - (damp * dd) * vi_dx;
-        dd *= 1.f + damp;
-        float H2[6] = {dd, dd, dd, 0.f, 0.f, 0.f};
-        const int n = cp.ncols[gp];
-        for (int m = 0; m < n; m++)
-            contact_term(st, cp, snap, xp, vi, dp, vi_dx, cp.cols[(int64_t)m * cp.num_slots + gp], false, damp, f2, H2);
-        step_limit = fminf(step_limit, cp.maxstep[gp]);
-        f = f + f2;
-#pragma unroll
-        for (int q = 0; q < 6; q++) H[q] += H2[q];
+        gp = prev_slot(g, C);
+        pp4 = st.prm[gp];
+        xp = xyz(st.xm[gp]);
+        dp = xyz(dx_in[gp]);
+        qgp = qcur[gp];
     }
-    const float3 delta = pp.accel_ratio * solve_sym3(H, f);
-    float3 out = vi_dx + delta;
-    const float l = sqrtf(len2(out));
-    if (l > step_limit && l > 0.f) out = out * (step_limit / l);
+    const float3 out = coll_position(st, cp, snap, g, gp, fl, xm, prm, xyz(d4), xyz(y4[g]), xj, vj_dx,
+                                     (fl & F_HAS_NEXT) ? qcur[g] : unit, xp, dp, qgp, pp4, spp->h, pp);
     dx_out[g] = make_float4(out.x, out.y, out.z, 0.f);
+}
+
+// One colour2 iteration of the sweep form with contacts, one tile per block and one thread per slot
+// (T = 32 C threads, T <= 512 so that the block's registers fit an SM): the even and odd position sweeps, then the even and odd orientation
+// sweeps, separated by __syncthreads, on the tile's positions, displacements and orientations in
+// shared memory.  Partners (other tiles) read the displacement the iteration started from in
+// `snap`, which the launch does not write, so the launch stands for the snapshot copy and the four
+// sweep launches (same operands and arithmetic).  Displacements go to dx_out, orientations are
+// updated in place.
+__global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, const float4* __restrict__ y4, float4* q,
+                                      const float4* __restrict__ snap, float4* __restrict__ dx_out,
+                                      const StepParams* __restrict__ spp, PhysParams pp, CollParams cp) {
+    extern __shared__ float4 coll_tile[];  // x | dx | q, T entries each
+    const int C = cp.C;
+    const int T = 32 * C;
+    float4* sx = coll_tile;
+    float4* sdx = sx + T;
+    float4* sq = sdx + T;
+    const int p = threadIdx.x;  // storage offset in the tile: row p / 32, lane p % 32
+    const int64_t base = (int64_t)blockIdx.x * T;
+    const int64_t g = base + p;
+    const float4 xm = st.xm[g], prm = st.prm[g];
+    sx[p] = xm;
+    sdx[p] = snap[g];
+    sq[p] = q[g];
+    const uint32_t fl = __float_as_uint(prm.w);
+    const int colour = (p >> 5) & 1;  // the row parity (C is even)
+    // in-tile neighbours (strands never cross tiles in the sweep form)
+    const int pn = (fl & F_HAS_NEXT) ? (int)(next_slot(g, C) - base) : p;
+    const int pq = (fl & F_HAS_PREV) ? (int)(prev_slot(g, C) - base) : p;
+    const float h = spp->h;
+    const bool moves = (fl & F_VALID) && xm.w != 0.f;
+    const float3 yv = moves ? xyz(y4[g]) : f3(0.f, 0.f, 0.f);
+    const float4 pp4 = (fl & F_HAS_PREV) ? st.prm[base + pq] : make_float4(1.f, 0.f, 0.f, 0.f);
+    __syncthreads();
+    for (int c = 0; c < 2; c++) {
+        if (colour == c && moves) {
+            const float3 out = coll_position(st, cp, snap, g, base + pq, fl, xm, prm, xyz(sdx[p]), yv, xyz(sx[pn]),
+                                             xyz(sdx[pn]), sq[p], xyz(sx[pq]), xyz(sdx[pq]), sq[pq], pp4, h, pp);
+            sdx[p] = make_float4(out.x, out.y, out.z, 0.f);
+        }
+        __syncthreads();
+    }
+    const bool turns = (fl & F_HAS_NEXT) && !(fl & F_FIX_ORIENTATION);
+    for (int c = 0; c < 2; c++) {
+        if (colour == c && turns) {
+            const float4 unit = make_float4(0.f, 0.f, 0.f, 1.f);
+            const float4 qp = (fl & F_HAS_PREV) ? sq[pq] : unit;
+            const float4 qrp = (fl & F_HAS_PREV) ? st.qr[base + pq] : unit;
+            const float4 qn = (fl & F_HAS_NEXT_ORIENTATION) ? sq[pn] : unit;
+            const float m2k = -2.f * prm.y * (1.f / prm.x);
+            sq[p] = vbd_orientation(sq[p], fl, xyz(sx[pn]) - xyz(xm), xyz(sdx[p]), xyz(sdx[pn]), m2k, qp, qrp, qn,
+                                    st.qr[g]);
+        }
+        __syncthreads();
+    }
+    dx_out[g] = sdx[p];
+    q[g] = sq[p];
 }
 
 inline unsigned blocks_of(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
@@ -437,6 +521,19 @@ cudaError_t launch_coll_detect(const DeviceState& st, const float4* dx4, const C
 
 cudaError_t launch_coll_steplimit(const DeviceState& st, const float4* dx4, const CollParams& cp, cudaStream_t s) {
     coll_steplimit_kernel<<<blocks_of(cp.num_slots, 256), 256, 0, s>>>(st, dx4, cp);
+    return cudaGetLastError();
+}
+
+bool coll_iteration_supported(int C) { return C % 2 == 0 && C >= 2 && 32 * C <= 512; }
+
+cudaError_t launch_coll_iteration(const DeviceState& st, const float4* y4, float4* q, const float4* snap, float4* dx_out,
+                                  const StepParams* d_sp, const PhysParams& pp, const CollParams& cp, cudaStream_t s) {
+    if (!coll_iteration_supported(cp.C)) return cudaErrorInvalidValue;
+    if (!y4 || !q || !snap || !dx_out || !d_sp || snap == dx_out || !cp.cols || !cp.ncols || !cp.maxstep)
+        return cudaErrorInvalidValue;
+    if (st.num_tiles == 0) return cudaSuccess;
+    const int T = 32 * cp.C;
+    coll_iteration_kernel<<<(unsigned)st.num_tiles, T, sizeof(float4) * 3 * T, s>>>(st, y4, q, snap, dx_out, d_sp, pp, cp);
     return cudaGetLastError();
 }
 

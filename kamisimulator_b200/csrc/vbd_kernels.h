@@ -43,6 +43,12 @@ cudaError_t launch_adjoint_step(const DeviceState& st, const PhysParams& pp, con
 int64_t coll_scan_tmp_size(int64_t n);
 cudaError_t launch_coll_detect(const DeviceState& st, const float4* dx4, const CollParams& cp, cudaStream_t s);
 cudaError_t launch_coll_steplimit(const DeviceState& st, const float4* dx4, const CollParams& cp, cudaStream_t s);
+// One colour2 iteration of the sweep form with contacts in one launch (one block per tile, one
+// thread per slot): reads the iteration's starting displacements from snap, writes dx_out, updates
+// q in place.  Tiles of up to 512 slots (coll_iteration_supported).
+bool coll_iteration_supported(int C);
+cudaError_t launch_coll_iteration(const DeviceState& st, const float4* y4, float4* q, const float4* snap, float4* dx_out,
+                                  const StepParams* d_sp, const PhysParams& pp, const CollParams& cp, cudaStream_t s);
 cudaError_t launch_sweep_position_coll(const DeviceState& st, const float4* y4, const float4* q, const float4* dx_in,
                                        float4* dx_out, const float4* snap, const StepParams* d_sp, const PhysParams& pp,
                                        const CollParams& cp, int colour, bool jacobi, cudaStream_t s);
