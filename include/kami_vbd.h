@@ -410,6 +410,12 @@ kami_status kami_vbd_step_noalloc(const kami_vbd_desc* settings, kami_vbd_noallo
 /* Description of the last error on the calling thread ("" if none). */
 const char* kami_vbd_last_error_string(void);
 
+/* ---- measurement -----------------------------------------------------------------------------------
+ * No counterpart in the reference.  FP32 FMA throughput of `device` in TFLOP/s, for the roofline of
+ * the FP32-issue-bound fused step: chains of plain FFMA and of packed FFMA2 (8 independent chains per
+ * thread, 8 blocks of 256 threads per SM, best of three timed launches; about 20 ms). */
+kami_status kami_fp32_peak(int32_t device, double* tflops_fma, double* tflops_fma2);
+
 /* Library version string. */
 const char* kami_vbd_version(void);
 

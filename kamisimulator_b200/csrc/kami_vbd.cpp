@@ -1589,6 +1589,15 @@ kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes,
 
 const char* kami_vbd_last_error_string(void) { return g_last_error.c_str(); }
 
+kami_status kami_fp32_peak(int32_t device, double* tflops_fma, double* tflops_fma2) {
+    if (!tflops_fma || !tflops_fma2) return fail(KAMI_ERR_INVALID_ARGUMENT, "null output");
+    KAMI_CUDA(cudaSetDevice(device), "cudaSetDevice");
+    int sms = 0;
+    KAMI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
+    KAMI_CUDA(measure_fp32_peak(sms, tflops_fma, tflops_fma2), "FP32 throughput probe");
+    return KAMI_OK;
+}
+
 const char* kami_vbd_version(void) { return "kami-vbd-b200 0.1 (sm_100a)"; }
 
 }  // extern "C"

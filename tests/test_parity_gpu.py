@@ -246,3 +246,13 @@ def test_nonfinite_strand_does_not_leak(form, tuning, schedule, pin_roots):
     assert not np.isfinite(xb[a:b]).all()
     clean.close()
     bad.close()
+
+
+def test_fp32_peak_probe():
+    """kami_fp32_peak: the FFMA / FFMA2 chain throughput that bench.py divides the fused step's FP32
+    rate by is a plausible B200 figure (nominal FP32: 74 TFLOP/s at 1965 MHz)."""
+    from kamisimulator_b200.vbd import fp32_peak
+
+    fma, fma2 = fp32_peak(0)
+    assert 30.0 < fma < 150.0, fma
+    assert 30.0 < fma2 < 300.0, fma2
