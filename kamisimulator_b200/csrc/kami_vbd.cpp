@@ -177,7 +177,8 @@ void release(kami_vbd_solver* h) {
         if (p) cudaFree(p);
     const CollParams& c = h->cp;
     void* cptrs[] = {(void*)c.vid, (void*)c.gid, c.cols,   c.ncols,  c.maxstep,  c.bmin,    c.bmax,
-                     c.cell,       c.count,      c.start,  c.cursor, c.sorted,   c.ext_bits, c.scan_tmp,
+                     c.cell,       c.count,      c.start,  c.cursor, c.srec,     c.sbmin,    c.sbmax,
+                     c.ext_bits,   c.scan_tmp,
                      h->d_snap,    h->d_hair_index, h->d_hair_stage};
     for (void* p : cptrs)
         if (p) cudaFree(p);
@@ -499,7 +500,9 @@ static kami_status setup_collisions(kami_vbd_solver* h, const kami_vbd_desc* d) 
     if (e == cudaSuccess) e = dalloc(&c.count, table);
     if (e == cudaSuccess) e = dalloc(&c.start, table);
     if (e == cudaSuccess) e = dalloc(&c.cursor, table);
-    if (e == cudaSuccess) e = dalloc(&c.sorted, S);
+    if (e == cudaSuccess) e = dalloc(&c.srec, S);
+    if (e == cudaSuccess) e = dalloc(&c.sbmin, S);
+    if (e == cudaSuccess) e = dalloc(&c.sbmax, S);
     if (e == cudaSuccess) e = dalloc(&c.ext_bits, 1);
     if (e == cudaSuccess) e = dalloc(&c.scan_tmp, coll_scan_tmp_size(table));
     if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_COLOUR2) e = dalloc(&h->d_snap, S);

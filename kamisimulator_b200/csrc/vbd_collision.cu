@@ -129,7 +129,11 @@ __global__ void coll_scatter_kernel(CollParams cp) {
     const uint32_t h = cp.cell[g];
     if (h == NO_CELL) return;
     const int32_t pos = atomicAdd(&cp.cursor[h], 1);
-    cp.sorted[pos] = (int32_t)g;
+    // the query's per-candidate values in bucket order: one contiguous read per candidate instead of
+    // a gather through the slot index
+    cp.srec[pos] = make_int4((int32_t)g, cp.vid[g], cp.gid[g], 0);
+    cp.sbmin[pos] = cp.bmin[g];
+    cp.sbmax[pos] = cp.bmax[g];
 }
 
 __global__ void coll_query_kernel(DeviceState st, CollParams cp) {
@@ -155,11 +159,12 @@ __global__ void coll_query_kernel(DeviceState st, CollParams cp) {
                                              (uint32_t)ci.z + (uint32_t)dz, mask);
                 const int32_t b = cp.start[h], e = b + cp.count[h];
                 for (int32_t k = b; k < e; k++) {
-                    const int32_t j = cp.sorted[k];
-                    if (j == g || cp.gid[j] != ga) continue;
-                    const int32_t vb = cp.vid[j];
+                    const int4 rec = cp.srec[k];
+                    const int32_t j = rec.x;
+                    if (j == g || rec.z != ga) continue;
+                    const int32_t vb = rec.y;
                     if (abs(vb - va) <= 2) continue;  // neighbouring segments (collision.cu:52)
-                    const float4 lob = cp.bmin[j], hib = cp.bmax[j];
+                    const float4 lob = cp.sbmin[k], hib = cp.sbmax[k];
                     if (lob.x > hia.x + slack || loa.x > hib.x + slack || lob.y > hia.y + slack ||
                         loa.y > hib.y + slack || lob.z > hia.z + slack || loa.z > hib.z + slack)
                         continue;

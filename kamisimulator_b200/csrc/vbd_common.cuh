@@ -141,9 +141,11 @@ struct CollParams {
     float4* bmax;        // [S] padded box: max xyz, 1 when the slot starts a segment
     uint32_t* cell;      // [S] hash bucket of the segment's box centre
     int32_t* count;      // [table] segments per bucket
-    int32_t* start;      // [table] first entry of each bucket in `sorted`
+    int32_t* start;      // [table] first entry of each bucket in the bucket-ordered arrays
     int32_t* cursor;     // [table] scatter cursor
-    int32_t* sorted;     // [S] segments grouped by bucket
+    int4* srec;          // [S] segments grouped by bucket: slot, boundary vertex index, groom
+    float4* sbmin;       // [S] bmin of the same entries (bucket order)
+    float4* sbmax;       // [S] bmax of the same entries (bucket order)
     unsigned* ext_bits;  // largest padded box extent (float bits): the cell size
     int32_t* scan_tmp;   // block sums of the bucket scan
     int table_bits;
