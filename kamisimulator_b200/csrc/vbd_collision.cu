@@ -434,62 +434,77 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
     dx_out[g] = make_float4(out.x, out.y, out.z, 0.f);
 }
 
-// One colour2 iteration of the sweep form with contacts, one tile per block and one thread per slot
-// (T = 32 C threads, T <= 512 so that the block's registers fit an SM): the even and odd position sweeps, then the even and odd orientation
-// sweeps, separated by __syncthreads, on the tile's positions, displacements and orientations in
-// shared memory.  Partners (other tiles) read the displacement the iteration started from in
-// `snap`, which the launch does not write, so the launch stands for the snapshot copy and the four
-// sweep launches (same operands and arithmetic).  Displacements go to dx_out, orientations are
-// updated in place.
-__global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, const float4* __restrict__ y4, float4* q,
-                                      const float4* __restrict__ snap, float4* __restrict__ dx_out,
-                                      const StepParams* __restrict__ spp, PhysParams pp, CollParams cp) {
+// One colour2 iteration of the sweep form with contacts, one tile per block (T = 32 C slots, T <= 512)
+// and one thread per slot pair: thread (r, lane) owns the slots of rows 2r and 2r + 1 of that lane,
+// one of each colour, so every thread works in every half-sweep.  The even and odd position sweeps,
+// then the even and odd orientation sweeps, run on the tile's positions, displacements and
+// orientations in shared memory, separated by __syncthreads.  Partners (other tiles) read the
+// displacement the iteration started from in `snap`, which the launch does not write, so the launch
+// stands for the snapshot copy and the four sweep launches (same operands and arithmetic).
+// Displacements go to dx_out, orientations are updated in place.
+__global__ void __launch_bounds__(256) coll_iteration_kernel(DeviceState st, const float4* __restrict__ y4, float4* q,
+                                                             const float4* __restrict__ snap,
+                                                             float4* __restrict__ dx_out,
+                                                             const StepParams* __restrict__ spp, PhysParams pp,
+                                                             CollParams cp) {
     extern __shared__ float4 coll_tile[];  // x | dx | q, T entries each
     const int C = cp.C;
     const int T = 32 * C;
     float4* sx = coll_tile;
     float4* sdx = sx + T;
     float4* sq = sdx + T;
-    const int p = threadIdx.x;  // storage offset in the tile: row p / 32, lane p % 32
+    const int lane = threadIdx.x & 31, row2 = (threadIdx.x >> 5) * 2;  // rows row2 (even) and row2 + 1 (odd)
     const int64_t base = (int64_t)blockIdx.x * T;
-    const int64_t g = base + p;
-    const float4 xm = st.xm[g], prm = st.prm[g];
-    sx[p] = xm;
-    sdx[p] = snap[g];
-    sq[p] = q[g];
-    const uint32_t fl = __float_as_uint(prm.w);
-    const int colour = (p >> 5) & 1;  // the row parity (C is even)
-    // in-tile neighbours (strands never cross tiles in the sweep form)
-    const int pn = (fl & F_HAS_NEXT) ? (int)(next_slot(g, C) - base) : p;
-    const int pq = (fl & F_HAS_PREV) ? (int)(prev_slot(g, C) - base) : p;
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const int p = (row2 + c) * 32 + lane;  // storage offset in the tile
+        sx[p] = st.xm[base + p];
+        sdx[p] = snap[base + p];
+        sq[p] = q[base + p];
+    }
     const float h = spp->h;
-    const bool moves = (fl & F_VALID) && xm.w != 0.f;
-    const float3 yv = moves ? xyz(y4[g]) : f3(0.f, 0.f, 0.f);
-    const float4 pp4 = (fl & F_HAS_PREV) ? st.prm[base + pq] : make_float4(1.f, 0.f, 0.f, 0.f);
     __syncthreads();
     for (int c = 0; c < 2; c++) {
-        if (colour == c && moves) {
-            const float3 out = coll_position(st, cp, snap, g, base + pq, fl, xm, prm, xyz(sdx[p]), yv, xyz(sx[pn]),
-                                             xyz(sdx[pn]), sq[p], xyz(sx[pq]), xyz(sdx[pq]), sq[pq], pp4, h, pp);
+        const int p = (row2 + c) * 32 + lane;
+        const int64_t g = base + p;
+        const float4 xm = sx[p], prm = st.prm[g];
+        const uint32_t fl = __float_as_uint(prm.w);
+        if ((fl & F_VALID) && xm.w != 0.f) {
+            // in-tile neighbours (strands never cross tiles in the sweep form)
+            const int pn = (fl & F_HAS_NEXT) ? (int)(next_slot(g, C) - base) : p;
+            const int pq = (fl & F_HAS_PREV) ? (int)(prev_slot(g, C) - base) : p;
+            const float4 pp4 = (fl & F_HAS_PREV) ? st.prm[base + pq] : make_float4(1.f, 0.f, 0.f, 0.f);
+            const float3 out = coll_position(st, cp, snap, g, base + pq, fl, xm, prm, xyz(sdx[p]), xyz(y4[g]),
+                                             xyz(sx[pn]), xyz(sdx[pn]), sq[p], xyz(sx[pq]), xyz(sdx[pq]), sq[pq], pp4,
+                                             h, pp);
             sdx[p] = make_float4(out.x, out.y, out.z, 0.f);
         }
         __syncthreads();
     }
-    const bool turns = (fl & F_HAS_NEXT) && !(fl & F_FIX_ORIENTATION);
     for (int c = 0; c < 2; c++) {
-        if (colour == c && turns) {
+        const int p = (row2 + c) * 32 + lane;
+        const int64_t g = base + p;
+        const float4 prm = st.prm[g];
+        const uint32_t fl = __float_as_uint(prm.w);
+        if ((fl & F_HAS_NEXT) && !(fl & F_FIX_ORIENTATION)) {
+            const int pn = (int)(next_slot(g, C) - base);
+            const int pq = (fl & F_HAS_PREV) ? (int)(prev_slot(g, C) - base) : p;
             const float4 unit = make_float4(0.f, 0.f, 0.f, 1.f);
             const float4 qp = (fl & F_HAS_PREV) ? sq[pq] : unit;
             const float4 qrp = (fl & F_HAS_PREV) ? st.qr[base + pq] : unit;
             const float4 qn = (fl & F_HAS_NEXT_ORIENTATION) ? sq[pn] : unit;
             const float m2k = -2.f * prm.y * (1.f / prm.x);
-            sq[p] = vbd_orientation(sq[p], fl, xyz(sx[pn]) - xyz(xm), xyz(sdx[p]), xyz(sdx[pn]), m2k, qp, qrp, qn,
+            sq[p] = vbd_orientation(sq[p], fl, xyz(sx[pn]) - xyz(sx[p]), xyz(sdx[p]), xyz(sdx[pn]), m2k, qp, qrp, qn,
                                     st.qr[g]);
         }
         __syncthreads();
     }
-    dx_out[g] = sdx[p];
-    q[g] = sq[p];
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const int p = (row2 + c) * 32 + lane;
+        dx_out[base + p] = sdx[p];
+        q[base + p] = sq[p];
+    }
 }
 
 inline unsigned blocks_of(int64_t n, int threads) { return (unsigned)((n + threads - 1) / threads); }
@@ -538,7 +553,8 @@ cudaError_t launch_coll_iteration(const DeviceState& st, const float4* y4, float
         return cudaErrorInvalidValue;
     if (st.num_tiles == 0) return cudaSuccess;
     const int T = 32 * cp.C;
-    coll_iteration_kernel<<<(unsigned)st.num_tiles, T, sizeof(float4) * 3 * T, s>>>(st, y4, q, snap, dx_out, d_sp, pp, cp);
+    coll_iteration_kernel<<<(unsigned)st.num_tiles, T / 2, sizeof(float4) * 3 * T, s>>>(st, y4, q, snap, dx_out, d_sp,
+                                                                                        pp, cp);
     return cudaGetLastError();
 }
 
