@@ -1594,10 +1594,14 @@ const char* kami_vbd_last_error_string(void) { return g_last_error.c_str(); }
 
 kami_status kami_fp32_peak(int32_t device, double* tflops_fma, double* tflops_fma2) {
     if (!tflops_fma || !tflops_fma2) return fail(KAMI_ERR_INVALID_ARGUMENT, "null output");
+    int prev = 0;
+    KAMI_CUDA(cudaGetDevice(&prev), "cudaGetDevice");
     KAMI_CUDA(cudaSetDevice(device), "cudaSetDevice");
     int sms = 0;
-    KAMI_CUDA(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device), "cudaDeviceGetAttribute");
-    KAMI_CUDA(measure_fp32_peak(sms, tflops_fma, tflops_fma2), "FP32 throughput probe");
+    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = measure_fp32_peak(sms, tflops_fma, tflops_fma2);
+    cudaSetDevice(prev);  // the caller's thread keeps its device
+    KAMI_CUDA(e, "FP32 throughput probe");
     return KAMI_OK;
 }
 
