@@ -136,41 +136,72 @@ __global__ void coll_scatter_kernel(CollParams cp) {
     cp.sbmax[pos] = cp.bmax[g];
 }
 
-__global__ void coll_query_kernel(DeviceState st, CollParams cp) {
-    const int64_t g = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (g >= cp.num_slots) return;
+// buildCollisionList's query for one segment per warp.  Lanes 0-26 take the 27 cells around the
+// segment's box centre; a lane whose bucket a lower lane already has drops it (every segment sits in
+// exactly one bucket, so this removes exactly the repeated candidates).  A warp prefix sum of the
+// bucket sizes numbers the candidates, and the lanes test them 32 at a time: groom, the
+// |i - j| <= 2 exemption (collision.cu:52), box overlap, then the distance test once per pair with
+// the lower boundary index first.  Accepted partners are compacted with a ballot into a shared list
+// of at most 16, then sorted by partner vertex index, so the list does not depend on the order in
+// which lanes found them.
+constexpr int kQueryWarps = 4;
+__global__ void __launch_bounds__(32 * kQueryWarps) coll_query_kernel(DeviceState st, CollParams cp) {
+    __shared__ int32_t s_beg[kQueryWarps][27], s_pre[kQueryWarps][28];
+    __shared__ int32_t s_lst[kQueryWarps][MAX_CONTACTS], s_key[kQueryWarps][MAX_CONTACTS];
+    const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
+    const int64_t g = (int64_t)blockIdx.x * kQueryWarps + w;
+    if (g >= cp.num_slots) return;  // uniform per warp
     int3 ci;
-    if (!box_cell(cp, g, ci)) {
-        cp.ncols[g] = 0;
+    if (!box_cell(cp, g, ci)) {  // uniform per warp (one segment)
+        if (lane == 0) cp.ncols[g] = 0;
         return;
     }
+    const uint32_t mask = (1u << cp.table_bits) - 1u;
+    uint32_t h = 0xffffffffu;
+    int32_t beg = 0, cnt = 0;
+    if (lane < 27) {
+        const int dxc = lane % 3 - 1, dy = (lane / 3) % 3 - 1, dz = lane / 9 - 1;
+        h = cell_hash((uint32_t)ci.x + (uint32_t)dxc, (uint32_t)ci.y + (uint32_t)dy, (uint32_t)ci.z + (uint32_t)dz, mask);
+        beg = cp.start[h];
+        cnt = cp.count[h];
+    }
+    for (int o = 0; o < 27; o++) {  // a bucket that a lower lane holds too is dropped
+        const uint32_t ho = __shfl_sync(0xffffffffu, h, o);
+        if (o < lane && ho == h) cnt = 0;
+    }
+    int32_t inc = cnt;  // inclusive prefix sum of the bucket sizes
+    for (int o = 1; o < 32; o <<= 1) {
+        const int32_t v = __shfl_up_sync(0xffffffffu, inc, o);
+        if (lane >= o) inc += v;
+    }
+    const int32_t total = __shfl_sync(0xffffffffu, inc, 31);
+    if (lane < 27) {
+        s_beg[w][lane] = beg;
+        s_pre[w][lane] = inc - cnt;
+    }
+    if (lane == 0) s_pre[w][27] = total;
+    __syncwarp();
+
     const float4 loa = cp.bmin[g], hia = cp.bmax[g];
     const int32_t va = cp.vid[g], ga = cp.gid[g];
     const float slack = 1e-3f * cell_size(cp);  // box overlap is a pre-filter: never reject a pair the distance test keeps
     const float3 xa0 = xyz(st.xm[g]), xa1 = xyz(st.xm[next_slot(g, cp.C)]);
-    const uint32_t mask = (1u << cp.table_bits) - 1u;
-    int32_t lst[MAX_CONTACTS], key[MAX_CONTACTS];
-    int n = 0;
-    bool over = false;
-    for (int dz = -1; dz <= 1; dz++)
-        for (int dy = -1; dy <= 1; dy++)
-            for (int dxc = -1; dxc <= 1; dxc++) {
-                const uint32_t h = cell_hash((uint32_t)ci.x + (uint32_t)dxc, (uint32_t)ci.y + (uint32_t)dy,
-                                             (uint32_t)ci.z + (uint32_t)dz, mask);
-                const int32_t b = cp.start[h], e = b + cp.count[h];
-                for (int32_t k = b; k < e; k++) {
-                    const int4 rec = cp.srec[k];
-                    const int32_t j = rec.x;
-                    if (j == g || rec.z != ga) continue;
-                    const int32_t vb = rec.y;
-                    if (abs(vb - va) <= 2) continue;  // neighbouring segments (collision.cu:52)
-                    const float4 lob = cp.sbmin[k], hib = cp.sbmax[k];
-                    if (lob.x > hia.x + slack || loa.x > hib.x + slack || lob.y > hia.y + slack ||
-                        loa.y > hib.y + slack || lob.z > hia.z + slack || loa.z > hib.z + slack)
-                        continue;
-                    bool dup = false;
-                    for (int m = 0; m < n && m < MAX_CONTACTS; m++) dup |= lst[m] == j;
-                    if (dup) continue;  // two of the 27 cells can share a bucket
+    int n = 0;  // accepted so far (uniform)
+    for (int32_t t0 = 0; t0 < total; t0 += 32) {
+        const int32_t t = t0 + lane;
+        bool hit = false;
+        int32_t j = -1, vb = 0;
+        if (t < total) {
+            int c = 0;
+            while (c < 26 && s_pre[w][c + 1] <= t) c++;
+            const int32_t k = s_beg[w][c] + (t - s_pre[w][c]);
+            const int4 rec = cp.srec[k];
+            j = rec.x;
+            vb = rec.y;
+            if (j != g && rec.z == ga && abs(vb - va) > 2) {
+                const float4 lob = cp.sbmin[k], hib = cp.sbmax[k];
+                if (!(lob.x > hia.x + slack || loa.x > hib.x + slack || lob.y > hia.y + slack ||
+                      loa.y > hib.y + slack || lob.z > hia.z + slack || loa.z > hib.z + slack)) {
                     const float3 xb0 = xyz(st.xm[j]), xb1 = xyz(st.xm[next_slot(j, cp.C)]);
                     const bool af = va < vb;
                     const float3 p0 = af ? xa0 : xb0, p1 = af ? xa1 : xb1, q0 = af ? xb0 : xa0, q1 = af ? xb1 : xa1;
@@ -183,32 +214,41 @@ __global__ void coll_query_kernel(DeviceState st, CollParams cp) {
                         r += af ? loa.w : lob.w;
                         r += af ? lob.w : loa.w;
                     }
-                    if (d2 < r * r) {
-                        if (n < MAX_CONTACTS) {
-                            lst[n] = j;
-                            key[n] = vb;
-                        } else {
-                            over = true;
-                        }
-                        n++;
-                    }
+                    hit = d2 < r * r;
                 }
             }
-    const int m = min(n, MAX_CONTACTS);
-    for (int i = 1; i < m; i++) {  // ascending partner vertex index
-        const int32_t kk = key[i], vv = lst[i];
-        int j = i - 1;
-        while (j >= 0 && key[j] > kk) {
-            key[j + 1] = key[j];
-            lst[j + 1] = lst[j];
-            j--;
         }
-        key[j + 1] = kk;
-        lst[j + 1] = vv;
+        const unsigned ballot = __ballot_sync(0xffffffffu, hit);
+        if (hit) {
+            const int slot = n + __popc(ballot & ((1u << lane) - 1u));
+            if (slot < MAX_CONTACTS) {
+                s_lst[w][slot] = j;
+                s_key[w][slot] = vb;
+            }
+        }
+        n += __popc(ballot);
     }
-    for (int i = 0; i < m; i++) cp.cols[(int64_t)i * cp.num_slots + g] = lst[i];
-    cp.ncols[g] = m;
-    if (over) atomicOr(st.status, STATUS_CONTACTS);
+    __syncwarp();
+    const int m = min(n, MAX_CONTACTS);
+    if (lane == 0) {
+        int32_t* lst = s_lst[w];
+        int32_t* key = s_key[w];
+        for (int i = 1; i < m; i++) {  // ascending partner vertex index
+            const int32_t kk = key[i], vv = lst[i];
+            int q = i - 1;
+            while (q >= 0 && key[q] > kk) {
+                key[q + 1] = key[q];
+                lst[q + 1] = lst[q];
+                q--;
+            }
+            key[q + 1] = kk;
+            lst[q + 1] = vv;
+        }
+        cp.ncols[g] = m;
+        if (n > MAX_CONTACTS) atomicOr(st.status, STATUS_CONTACTS);
+    }
+    __syncwarp();
+    if (lane < m) cp.cols[(int64_t)lane * cp.num_slots + g] = s_lst[w][lane];
 }
 
 // Exclusive scan of int32 counts, 4096 per block (1024 threads x 4): per-block scan + block sums.
@@ -535,7 +575,7 @@ cudaError_t launch_coll_detect(const DeviceState& st, const float4* dx4, const C
         return e;
     coll_scatter_kernel<<<blocks_of(S, 256), 256, 0, s>>>(cp);
     if ((e = cudaGetLastError()) != cudaSuccess) return e;
-    coll_query_kernel<<<blocks_of(S, 128), 128, 0, s>>>(st, cp);
+    coll_query_kernel<<<blocks_of(S, kQueryWarps), 32 * kQueryWarps, 0, s>>>(st, cp);
     return cudaGetLastError();
 }
 
