@@ -474,7 +474,7 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
     dx_out[g] = make_float4(out.x, out.y, out.z, 0.f);
 }
 
-// One colour2 iteration of the sweep form with contacts, one tile per block (T = 32 C slots, T <= 512)
+// One colour2 iteration of the sweep form with contacts, one tile per block (T = 32 C slots, T <= 1024)
 // and one thread per slot pair: thread (r, lane) owns the slots of rows 2r and 2r + 1 of that lane,
 // one of each colour, so every thread works in every half-sweep.  The even and odd position sweeps,
 // then the even and odd orientation sweeps, run on the tile's positions, displacements and
@@ -482,7 +482,7 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
 // displacement the iteration started from in `snap`, which the launch does not write, so the launch
 // stands for the snapshot copy and the four sweep launches (same operands and arithmetic).
 // Displacements go to dx_out, orientations are updated in place.
-__global__ void __launch_bounds__(256) coll_iteration_kernel(DeviceState st, const float4* __restrict__ y4, float4* q,
+__global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, const float4* __restrict__ y4, float4* q,
                                                              const float4* __restrict__ snap,
                                                              float4* __restrict__ dx_out,
                                                              const StepParams* __restrict__ spp, PhysParams pp,
@@ -584,7 +584,7 @@ cudaError_t launch_coll_steplimit(const DeviceState& st, const float4* dx4, cons
     return cudaGetLastError();
 }
 
-bool coll_iteration_supported(int C) { return C % 2 == 0 && C >= 2 && 32 * C <= 512; }
+bool coll_iteration_supported(int C) { return C % 2 == 0 && C >= 2 && 32 * C <= 1024; }
 
 cudaError_t launch_coll_iteration(const DeviceState& st, const float4* y4, float4* q, const float4* snap, float4* dx_out,
                                   const StepParams* d_sp, const PhysParams& pp, const CollParams& cp, cudaStream_t s) {

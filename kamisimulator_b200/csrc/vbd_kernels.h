@@ -45,7 +45,7 @@ cudaError_t launch_coll_detect(const DeviceState& st, const float4* dx4, const C
 cudaError_t launch_coll_steplimit(const DeviceState& st, const float4* dx4, const CollParams& cp, cudaStream_t s);
 // One colour2 iteration of the sweep form with contacts in one launch (one block per tile, one
 // thread per slot): reads the iteration's starting displacements from snap, writes dx_out, updates
-// q in place.  Tiles of up to 512 slots (coll_iteration_supported).
+// q in place.  Tiles of up to 1024 slots (coll_iteration_supported).
 bool coll_iteration_supported(int C);
 // FP32 FMA throughput (fp32_probe.cu): TFLOP/s of plain FFMA and of packed FFMA2 chains over
 // 8 blocks of 256 threads per SM, best of three timed launches on the current device.

@@ -83,6 +83,24 @@ def test_tangle_matches_the_oracle(schedule):
     assert np.abs(xf - x).max() > 1e-4  # the contacts changed the motion
 
 
+def test_long_strands_with_contacts_match_the_oracle():
+    """Strands of 600 vertices piling onto each other: sweep tiles of 640 slots, so one block of
+    320 threads per tile runs each iteration."""
+    g = synth.tangle(6, 600, seed=7, young=5e-5, layer=1e-4)
+    st = _settings("colour2")
+    s = helpers.gpu_solver(g, st, form="sweep")
+    assert 16 < s.slots_per_lane <= 32
+    s.close()
+    ex, et, x, _ = _lockstep(g, st, 12)
+    assert ex <= POS_TOL and et <= TWIST_TOL, (ex, et)
+    free = helpers.gpu_solver(g, _settings("colour2", hair_hair=False), form="sweep")
+    for _ in range(12):
+        free.step(1 / 120)
+    xf = free.get_positions_velocities()[0]
+    free.close()
+    assert np.abs(xf - x).max() > 1e-4  # the contacts changed the motion (5e-4 m in the oracle)
+
+
 def test_substeps_and_detection_period():
     """Two substeps per frame and detection on every second substep (the lists of the first
     substep carry over): per frame from shared states, then free running.  Free running, a contact
