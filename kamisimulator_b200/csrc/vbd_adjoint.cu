@@ -608,8 +608,9 @@ cudaError_t launch_adjoint_step(const DeviceState& st, const PhysParams& pp, con
             if (C == 2) {
                 adjoint_step_kernel<2, 2, true, 256><<<gblocks, 256, smem, s>>>(st, pp, sp, sdf, tp, ad);
             } else if (C == 4) {
-                static const cudaError_t attr = cudaFuncSetAttribute(
-                    adjoint_step_kernel<4, 1, true, 256>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+                // per launch: the attribute belongs to the current device, and a process may drive several
+                const cudaError_t attr = cudaFuncSetAttribute(adjoint_step_kernel<4, 1, true, 256>,
+                                                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
                 if (attr != cudaSuccess) return attr;
                 adjoint_step_kernel<4, 1, true, 256><<<gblocks, 256, smem, s>>>(st, pp, sp, sdf, tp, ad);
             } else {
