@@ -14,8 +14,9 @@ host buffers: every frame is one kami_vbd_step_host call, which uploads position
 pinned host memory (UploadHair), steps and reads them back (DownloadHair), overlapping the copies of
 one strand group with the step of another; `three_calls_value` is the same frame as
 kami_vbd_set_positions_velocities, kami_vbd_step, kami_vbd_get_positions_velocities in turn.  Extra
-`forms` report the plain per-groom sweep
-form and the batched form on 64 uneven grooms.  With N > 1 (torchrun) each rank steps its own groom
+`forms` report the sweep form, the batched form on 64 uneven grooms against the same grooms as one
+plain (fused, autotuned) handle each, and the other production forms; `trajectory` states the FP32
+GPU trajectory's distance to an FP64 replay of the same update over 100 frames.  With N > 1 (torchrun) each rank steps its own groom
 (weak scaling, no collective on the data path); times are maxima over ranks.
 
 --impl reference times the CPU restatement of the reference's update (oracle/, Jacobi schedule =
@@ -67,6 +68,21 @@ def config_dict(extra=None):
     if extra:
         c.update(extra)
     return c
+
+
+def fp32_probe(device=0):
+    """Measured FP32 FMA throughput of a GPU in TFLOP/s, (plain FFMA chains, packed FFMA2 chains), from
+    the bench-only probe library (kamisimulator_b200/csrc/fp32_probe.cu)."""
+    import ctypes
+
+    lib = ctypes.CDLL(os.path.join(ROOT, "kamisimulator_b200", "lib", "libkami_fp32_probe.so"))
+    lib.kami_fp32_peak.argtypes = [ctypes.c_int, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)]
+    lib.kami_fp32_peak.restype = ctypes.c_int
+    fma, fma2 = ctypes.c_double(), ctypes.c_double()
+    rc = lib.kami_fp32_peak(device, ctypes.byref(fma), ctypes.byref(fma2))
+    if rc != 0:
+        raise RuntimeError(f"kami_fp32_peak failed with cudaError {rc}")
+    return fma.value, fma2.value
 
 
 def hbm_peak():
@@ -245,7 +261,8 @@ def cpu_baseline_sample():
 
 
 def extra_forms(args, torch, stream, flush):
-    """Plain per-groom sweep form on the headline groom, and batched vs plain on 64 uneven grooms."""
+    """Plain per-groom sweep form on the headline groom, batched vs plain per-groom handles on 64 uneven
+    grooms, the adjoint, the SDF bake, hair-hair, long strands and the reference's default settings."""
     from kamisimulator_b200 import synth
     from kamisimulator_b200.vbd import Solver
 
@@ -276,31 +293,43 @@ def extra_forms(args, torch, stream, flush):
     torch.cuda.synchronize()
     ms_b = e0.elapsed_time(e1)
     b.close()
-    plain = [Solver(gg, form="sweep", **st) for gg in grooms]
-    for p in plain:
-        p.step(DT, stream=stream)
-    torch.cuda.synchronize()
-    npl = 3
-    e0.record(stream)
-    for _ in range(npl):
-        for p in plain:  # the CantileverTestSolver pattern: instances stepped one after another
-            p.step(DT, stream=stream)
-    e1.record(stream)
-    torch.cuda.synchronize()
-    ms_p = e0.elapsed_time(e1)
-    for p in plain:
-        p.close()
+
+    def per_groom(form, rounds):
+        """The grooms as one handle each (the CantileverTestSolver pattern: one Sim per instance,
+        stepped one after another, src/solvers/CantileverTestSolver.cpp:106-111)."""
+        hs = [Solver(gg, form=form, **st) for gg in grooms]
+        if form == "auto":  # the plain drop-in: fused, each handle autotuned on its own strands
+            for hh in hs:
+                hh.autotune(DT, trial_steps=4)
+        for hh in hs:
+            hh.step(DT, stream=stream)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        for _ in range(rounds):
+            for hh in hs:
+                hh.step(DT, stream=stream)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        for hh in hs:
+            hh.close()
+        return V * NUM_ITR * rounds / (ms / 1e3), ms / rounds
+
     vb = V * NUM_ITR * nb / (ms_b / 1e3)
-    vp = V * NUM_ITR * npl / (ms_p / 1e3)
+    vf, ms_f = per_groom("auto", 10)
+    vp, ms_p = per_groom("sweep", 3)
     out["batched_64_grooms"] = {"value": vb, "ms_per_step": ms_b / nb, "vertices": V,
                                 "tuning": {"slots_per_lane": best[0], "warps_per_block": best[1],
                                            "steps_per_launch": best[2], "register_cap": best[3]},
-                                "plain_per_groom_value": vp, "plain_ms_per_step": ms_p / npl,
-                                "batched_over_plain": vb / vp,
+                                "plain_per_groom_fused_value": vf, "plain_fused_ms_per_step": ms_f,
+                                "batched_over_plain_fused": vb / vf,
+                                "plain_per_groom_sweep_value": vp, "plain_sweep_ms_per_step": ms_p,
+                                "batched_over_plain_sweep": vb / vp,
                                 "what": "64 grooms (strands log-uniform [500, 20000], 16-128 vertices) in one "
                                         f"kami_vbd_batch_create handle, {nb} steps per kami_vbd_batch_step "
-                                        "(autotuned tile shape, CUDA graph) vs 64 "
-                                        "sweep-form handles stepped one after another"}
+                                        "(autotuned tile shape, CUDA graph), against 64 handles stepped one after "
+                                        "another with kami_vbd_step: the plain drop-in (form auto = fused, each "
+                                        "handle autotuned) and the sweep form"}
     out["adjoint_2k_x48"] = adjoint_timing(torch, stream)
     out["sdf_bake_128"] = sdf_bake_timing()
     try:
@@ -309,6 +338,53 @@ def extra_forms(args, torch, stream, flush):
         out["hair_hair_sweep"] = {"error": str(e)}
     out["long_strands_3k_x200"] = long_strand_timing(torch, stream, flush)
     out["reference_default_settings"] = default_settings_timing(torch, stream)
+    return out
+
+
+def trajectory_errors(frames=100, cut_strands=1000):
+    """The FP32 GPU trajectory against an FP64 replay of the same update (the FP64 oracle, colour2
+    schedule, same inputs) over `frames` frames, beside the FP32 oracle's: the cantilever of 64 rods
+    x 32 vertices (10 iterations, dt 1/60 s, 1 substep) and a cut of the headline groom's generator
+    (`cut_strands` x 64 vertices, 20 iterations, dt 1/120 s, the 128^3 head SDF).  Free-running: no
+    state is shared after frame 0.  Positions in m (max over vertices), twists in rad (max over
+    segments), each at the last frame and as the maximum over all frames."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.vbd import Solver
+    from oracle.oracle import OracleSim, twist_angles
+
+    cases = {
+        "cantilever_64x32": (synth.cantilever(), dict(num_itr=10, max_h=1 / 60, gravity=(0.0, 0.0, -9.81),
+                                                      radius=40e-6, density=1300.0, velocity_decay=0.05,
+                                                      damping=1e-6), 1 / 60),
+        f"groom_cut_{cut_strands}x64": (synth.groom(cut_strands, 64, seed=2), settings(), DT),
+    }
+    out = {}
+    for name, (g, st, dt) in cases.items():
+        o64 = OracleSim(g, dtype=np.float64, schedule="colour2", **st)
+        o32 = OracleSim(g, dtype=np.float32, schedule="colour2", **st)
+        s = Solver(g, form="auto", **st)
+        worst = {"gpu_vs_fp64_m": 0.0, "gpu_vs_fp64_rad": 0.0, "gpu_vs_fp32_oracle_m": 0.0,
+                 "gpu_vs_fp32_oracle_rad": 0.0, "fp32_oracle_vs_fp64_m": 0.0, "fp32_oracle_vs_fp64_rad": 0.0}
+        last = {}
+        for _ in range(frames):
+            s.step(dt)
+            o64.advance(dt)
+            o32.advance(dt)
+            x, _v = s.get_positions_velocities()
+            q = s.get_orientations()
+            last = {"gpu_vs_fp64_m": float(np.abs(x - o64.x).max()),
+                    "gpu_vs_fp64_rad": float(np.abs(twist_angles(o64.q, q)).max()),
+                    "gpu_vs_fp32_oracle_m": float(np.abs(x - o32.x).max()),
+                    "gpu_vs_fp32_oracle_rad": float(np.abs(twist_angles(o32.q, q)).max()),
+                    "fp32_oracle_vs_fp64_m": float(np.abs(o32.x - o64.x).max()),
+                    "fp32_oracle_vs_fp64_rad": float(np.abs(twist_angles(o64.q, o32.q.astype(np.float64))).max())}
+            worst = {k: max(worst[k], v) for k, v in last.items()}
+        travel = float(np.abs(o64.x - g.positions).max())
+        s.close()
+        out[name] = {"frames": frames, "vertices": g.num_vertices, "num_itr": st["num_itr"], "dt": dt,
+                     "last_frame": last, "max_over_frames": worst, "max_displacement_m": travel}
+    out["what"] = ("FP32 GPU step (kami_vbd_step, colour2) against the FP64 oracle replay of the same update, "
+                   "free-running over the frames, with the FP32 oracle's own FP64 gap beside it")
     return out
 
 
@@ -639,7 +715,7 @@ def run_ours(args):
         fp32_peak, fp32_source = FP32_PEAK_TFLOPS, "nominal FP32 (148 SMs x 128 FMA lanes x 2 x 1965 MHz)"
         probe = None
         try:
-            probe = vbd.fp32_peak(0)  # after the timed region: FFMA and FFMA2 chains on this GPU
+            probe = fp32_probe(0)  # after the timed region: FFMA and FFMA2 chains on this GPU
         except Exception as exc:  # the nominal figure stands in, and the line says so
             fp32_source += f" (probe failed: {exc})"
         if probe and max(probe) > 0:
@@ -669,6 +745,7 @@ def run_ours(args):
                 "fp32": fp32, "gpu_launches": args.steps, "clocks": clk.summary()}
     if world == 1 and rank == 0 and not args.skip_extra:
         line["forms"] = extra_forms(args, torch, stream, flush)
+        line["trajectory"] = trajectory_errors()
         line["cpu_baseline"] = cpu_baseline_sample()
     if world > 1:
         torch.distributed.barrier()
@@ -684,7 +761,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
-    ap.add_argument("--only", choices=["adjoint", "large", "hairhair", "bake", "long", "default"],
+    ap.add_argument("--only", choices=["adjoint", "large", "hairhair", "bake", "long", "default", "trajectory"],
                     help="run a single extra measurement")
     ap.add_argument("--tuning", help="fixed tile shape C,warps,steps_per_launch,register_cap instead of autotuning")
     args = ap.parse_args()
@@ -704,6 +781,8 @@ def main():
         print(json.dumps(hair_hair_timing(torch, torch.cuda.current_stream())), flush=True)
     elif args.only == "bake":
         print(json.dumps(sdf_bake_timing()), flush=True)
+    elif args.only == "trajectory":
+        print(json.dumps(trajectory_errors()), flush=True)
     elif args.only == "default":
         import torch
 

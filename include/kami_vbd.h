@@ -39,6 +39,10 @@ typedef enum kami_status {
     KAMI_ERR_IO = 10               /* a file could not be opened, read or written, or is not a USC .data file */
 } kami_status;
 
+/* Largest number of substeps (ceil(dt / max_h), Sim::advance, YarnBall/sim/step.cpp:38-62) one step
+ * call takes; a dt above it is rejected with KAMI_ERR_INVALID_ARGUMENT. */
+#define KAMI_MAX_SUBSTEPS 1000000
+
 /* Gauss-Seidel order of the position and orientation sweeps. */
 typedef enum kami_schedule {
     KAMI_SCHEDULE_COLOUR2 = 0, /* even then odd vertices, even then odd segments (by index within the strand) */
@@ -50,7 +54,9 @@ typedef enum kami_schedule {
 typedef enum kami_form {
     KAMI_FORM_AUTO = 0,  /* fused when every strand fits 8 warp tiles of 128 slots (1024 vertices) and
                             there is no hair-hair collision, else sweep */
-    KAMI_FORM_SWEEP = 1, /* one kernel per colour sweep, replayed from a CUDA graph (the plain per-groom form) */
+    KAMI_FORM_SWEEP = 1, /* one kernel per colour sweep, replayed from a CUDA graph: the reference's
+                            kernel-per-sweep structure (step.cpp:9-36), for hair-hair collision and
+                            strands over 1024 vertices */
     KAMI_FORM_FUSED = 2  /* one kernel per step: each warp owns a strand tile for all iterations; strands
                             longer than a tile run on across the warps of a group of 2-8 tiles */
 } kami_form;
@@ -380,11 +386,17 @@ kami_status kami_vbd_zero_rest_darboux_grad(kami_vbd_handle h);
  * It runs one KamiSimulator internal step like kami_vbd_step with the colour2 schedule and the sweep
  * kernels, but with no SDF pass and no finiteness check.  Scratch lives in a fixed __device__ array
  * for at most KAMI_NOALLOC_MAX_VERTICES vertices (12 MiB held by every device that loads the library
- * until exit); larger inputs are rejected with KAMI_ERR_UNSUPPORTED.  The first call on a device
- * resolves that array's address, so make it before any stream capture.  All calls share the scratch:
- * calls whose work overlaps on the GPU race and must be serialised by the caller.  Per-vertex
- * arrays hold what kami_vbd_create derives (inverse mass with pinned roots at 0, rest length,
- * stretch stiffness, orientations, stiffness-scaled rest Darboux quaternions). */
+ * until exit); larger inputs are rejected with KAMI_ERR_UNSUPPORTED.  Every call made outside a
+ * stream capture looks up that array's device address in the current context; a call made while
+ * its stream captures reuses the address of the last such call on the device, so make the first
+ * call on a device, and the first after a cudaDeviceReset, outside any capture.  All calls share
+ * the scratch: calls whose work overlaps on the GPU race and must be serialised by the caller.
+ * Per-vertex arrays hold what kami_vbd_create derives (inverse mass with pinned roots at 0, rest
+ * length, stretch stiffness, orientations, stiffness-scaled rest Darboux quaternions).  The strand
+ * offsets should satisfy strand_begin[0] == 0, strand_begin[num_strands] == num_vertices and be
+ * increasing; they stay on the device and are not checked, but each strand is clamped to the
+ * vertex range, so malformed offsets give wrong results, never an access out of bounds.  A dt
+ * that is not finite, or that needs more than KAMI_MAX_SUBSTEPS substeps of max_h, is rejected. */
 #define KAMI_NOALLOC_MAX_VERTICES 262144
 
 typedef struct kami_vbd_noalloc_args {
@@ -409,12 +421,6 @@ kami_status kami_vbd_step_noalloc(const kami_vbd_desc* settings, kami_vbd_noallo
 
 /* Description of the last error on the calling thread ("" if none). */
 const char* kami_vbd_last_error_string(void);
-
-/* ---- measurement -----------------------------------------------------------------------------------
- * No counterpart in the reference.  FP32 FMA throughput of `device` in TFLOP/s, for the roofline of
- * the FP32-issue-bound fused step: chains of plain FFMA and of packed FFMA2 (8 independent chains per
- * thread, 8 blocks of 256 threads per SM, best of three timed launches; about 20 ms). */
-kami_status kami_fp32_peak(int32_t device, double* tflops_fma, double* tflops_fma2);
 
 /* Library version string. */
 const char* kami_vbd_version(void);

@@ -1,4 +1,9 @@
-// fp32_probe.cu -- FP32 FMA throughput of this GPU (no counterpart in the reference).
+// fp32_probe.cu -- FP32 FMA throughput of this GPU (no counterpart in the reference).  A measurement
+// probe for bench.py, built into its own library (lib/libkami_fp32_probe.so), not the solver's:
+//
+//   extern "C" int kami_fp32_peak(int device, double* tflops_fma, double* tflops_fma2);
+//
+// returns 0 or the cudaError_t of the failing call, and restores the calling thread's device.
 //
 // The fused step is bound by FP32 instruction issue, so its roofline needs the FP32 peak, which the
 // HBM / tensor measurements do not give.  Each thread runs 8 independent FMA chains (a * x + b with
@@ -8,9 +13,6 @@
 // chains live.
 #include <cuda_runtime.h>
 
-#include "vbd_kernels.h"
-
-namespace kami {
 namespace {
 
 constexpr int kChains = 8;
@@ -44,8 +46,6 @@ __global__ void __launch_bounds__(256) fma2_probe_kernel(float* out, int iters, 
     if (s == -1.f) out[blockIdx.x * blockDim.x + threadIdx.x] = s;
 }
 
-}  // namespace
-
 cudaError_t measure_fp32_peak(int sm_count, double* tflops_fma, double* tflops_fma2) {
     const int threads = 256, blocks = sm_count * 8, iters = 1 << 15;
     float* out = nullptr;
@@ -78,4 +78,17 @@ cudaError_t measure_fp32_peak(int sm_count, double* tflops_fma, double* tflops_f
     return e;
 }
 
-}  // namespace kami
+}  // namespace
+
+extern "C" int kami_fp32_peak(int device, double* tflops_fma, double* tflops_fma2) {
+    if (!tflops_fma || !tflops_fma2) return (int)cudaErrorInvalidValue;
+    int prev = 0;
+    cudaError_t e = cudaGetDevice(&prev);
+    if (e != cudaSuccess) return (int)e;
+    if ((e = cudaSetDevice(device)) != cudaSuccess) return (int)e;
+    int sms = 0;
+    e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
+    if (e == cudaSuccess) e = measure_fp32_peak(sms, tflops_fma, tflops_fma2);
+    cudaSetDevice(prev);  // the caller's thread keeps its device
+    return (int)e;
+}

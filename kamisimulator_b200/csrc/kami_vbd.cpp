@@ -844,6 +844,15 @@ kami_status kami_vbd_set_body_transform(kami_vbd_handle h, const float rotation_
     return KAMI_OK;
 }
 
+// A step's dt: finite, and at most KAMI_MAX_SUBSTEPS substeps of max_h (ceil(dt / max_h) is bounded
+// before it is converted to int).  dt <= 0 passes: Sim::advance returns for it (step.cpp:38-39).
+static kami_status check_dt(const kami_vbd_solver* h, float dt) {
+    if (!std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
+    if (dt > 0.f && !(std::ceil(dt / h->max_h) <= (float)KAMI_MAX_SUBSTEPS))
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "dt / max_h needs more than %d substeps", KAMI_MAX_SUBSTEPS);
+    return KAMI_OK;
+}
+
 static StepParams advance_clock(kami_vbd_solver* h, float dt) {
     const int steps = std::max(1, (int)std::ceil(dt / h->max_h));
     h->last_h = h->h;
@@ -865,8 +874,8 @@ static StepParams advance_clock(kami_vbd_solver* h, float dt) {
 
 kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
     KAMI_TRY(valid_handle(h));
-    if (!(dt > 0.f)) return KAMI_OK;  // Sim::advance returns for h <= 0 (step.cpp:113)
-    if (!std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
+    KAMI_TRY(check_dt(h, dt));
+    if (!(dt > 0.f)) return KAMI_OK;  // Sim::advance returns for h <= 0 (step.cpp:38-39)
     const StepParams sp = advance_clock(h, dt);
     const int steps = sp.substeps;
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
@@ -985,7 +994,7 @@ kami_status kami_vbd_step_host(kami_vbd_handle h, float dt, const float* xyz, co
                                float* vxyz_out) {
     KAMI_TRY(valid_handle(h));
     if (!xyz || !vxyz || !xyz_out || !vxyz_out) return fail(KAMI_ERR_INVALID_ARGUMENT, "null position or velocity array");
-    if (!std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
+    KAMI_TRY(check_dt(h, dt));
     HostIO io{};
     const int64_t n = 3 * h->nv;
     bool direct = dt > 0.f && h->form == KAMI_FORM_FUSED && !h->hair_hair;
@@ -1131,7 +1140,8 @@ kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int3
 kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float* body_transforms, void* stream) {
     KAMI_TRY(valid_handle(h));
     if (n < 1) return fail(KAMI_ERR_INVALID_ARGUMENT, "n must be >= 1");
-    if (!(dt > 0.f) || !std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite and > 0");
+    KAMI_TRY(check_dt(h, dt));
+    if (!(dt > 0.f)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be > 0");
     if (h->form != KAMI_FORM_FUSED) {
         for (int j = 0; j < n; j++) {
             if (body_transforms) kami_vbd_set_body_transform(h, body_transforms + 7 * j, body_transforms + 7 * j + 4);
@@ -1337,7 +1347,8 @@ kami_status kami_vbd_set_tape_window(kami_vbd_handle h, int64_t tile_begin, int6
 kami_status kami_vbd_step_record(kami_vbd_handle h, float dt, void* stream) {
     KAMI_TRY(valid_handle(h));
     if (h->tape_capacity == 0) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
-    if (!(dt > 0.f) || !std::isfinite(dt)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite and > 0");
+    KAMI_TRY(check_dt(h, dt));
+    if (!(dt > 0.f)) return fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be > 0");
     const int substeps = std::max(1, (int)std::ceil(dt / h->max_h));
     if ((int)h->tape_steps.size() + substeps > h->tape_capacity)
         return fail(KAMI_ERR_STATE, "the tape holds %d substeps, %d are recorded and this step takes %d; run "
@@ -1591,19 +1602,6 @@ kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes,
 }
 
 const char* kami_vbd_last_error_string(void) { return g_last_error.c_str(); }
-
-kami_status kami_fp32_peak(int32_t device, double* tflops_fma, double* tflops_fma2) {
-    if (!tflops_fma || !tflops_fma2) return fail(KAMI_ERR_INVALID_ARGUMENT, "null output");
-    int prev = 0;
-    KAMI_CUDA(cudaGetDevice(&prev), "cudaGetDevice");
-    KAMI_CUDA(cudaSetDevice(device), "cudaSetDevice");
-    int sms = 0;
-    cudaError_t e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, device);
-    if (e == cudaSuccess) e = measure_fp32_peak(sms, tflops_fma, tflops_fma2);
-    cudaSetDevice(prev);  // the caller's thread keeps its device
-    KAMI_CUDA(e, "FP32 throughput probe");
-    return KAMI_OK;
-}
 
 const char* kami_vbd_version(void) { return "kami-vbd-b200 0.1 (sm_100a)"; }
 

@@ -15,11 +15,15 @@
 // Scratch: the inertial targets, the displacement iterate and the derived vertex flags live in
 // g_noalloc_scratch, a file-scope __device__ array sized for KAMI_NOALLOC_MAX_VERTICES vertices
 // (12 MiB), which every device that loads the library keeps until the process exits.  Host code
-// cannot use the symbol itself as a device address, so the first call on each device, with that
-// device current, resolves it once with cudaGetSymbolAddress; make that first call before any
-// stream capture.  All calls share the one array and it keeps the last call's contents; every
-// call writes each scratch entry before reading it, so nothing needs clearing.  Calls whose work
+// cannot use the symbol itself as a device address, so each call, with the caller's device
+// current, resolves it with cudaGetSymbolAddress (the set-up) unless its stream is capturing; make
+// the first call on each device, and the first after a cudaDeviceReset, outside any stream
+// capture.  All calls share the one array and it keeps the last call's contents; every call
+// writes each scratch entry before reading it, so nothing needs clearing.  Calls whose work
 // overlaps on the GPU (different streams, or concurrent host threads) race on the scratch.
+//
+// The strand offsets are device data, so the host cannot check them: the flags kernel clamps each
+// strand to the vertex range, and malformed offsets give wrong flags but no access out of bounds.
 #include <cuda_runtime.h>
 
 #include <algorithm>
@@ -77,8 +81,17 @@ __global__ void noalloc_flags_kernel(NoAllocArgs a) {
         if (a.sb[mid] <= i) lo = mid;
         else hi = mid - 1;
     }
-    const int64_t local = i - a.sb[lo];
-    const int64_t n = a.sb[lo + 1] - a.sb[lo];
+    // The offsets are the caller's and are not checked on the host (they live on the device), so
+    // the strand's range is clamped to [0, nv): no flag can then point a neighbour read past either
+    // end of the arrays, whatever the offsets hold.  A vertex outside every clamped range gets no
+    // flags and moves as a free particle.
+    const int64_t b = max((int64_t)a.sb[lo], (int64_t)0);
+    const int64_t n = min((int64_t)a.sb[lo + 1], a.nv) - b;
+    const int64_t local = i - b;
+    if (local < 0 || local >= n) {
+        a.scratch[2 * kMaxV + i] = make_float4(__uint_as_float(0u), 0.f, 0.f, 0.f);
+        return;
+    }
     uint32_t f = F_VALID;
     if (local == 0) f |= F_ROOT;
     if (local > 0) f |= F_HAS_PREV;
@@ -204,22 +217,36 @@ extern "C" kami_status kami_vbd_step_noalloc(const kami_vbd_desc* settings, kami
         return noalloc_fail(KAMI_ERR_UNSUPPORTED, "kami_vbd_step_noalloc runs the colour2 schedule only");
     if (settings->num_itr < 0 || !(settings->max_h > 0.f))
         return noalloc_fail(KAMI_ERR_INVALID_ARGUMENT, "num_itr must be >= 0 and max_h > 0");
-    if (!(dt > 0.f)) return KAMI_OK;  // Sim::advance returns for h <= 0
     if (!std::isfinite(dt)) return noalloc_fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");
+    if (!(dt > 0.f)) return KAMI_OK;  // Sim::advance returns for h <= 0
+    // Sim::advance's substep count (step.cpp:38-62), bounded before the conversion to int
+    const float ratio = std::ceil(dt / settings->max_h);
+    if (!(ratio <= (float)KAMI_MAX_SUBSTEPS))
+        return noalloc_fail(KAMI_ERR_INVALID_ARGUMENT, "dt / max_h needs more than KAMI_MAX_SUBSTEPS substeps");
 
     int dev = 0;
     cudaError_t e = cudaGetDevice(&dev);
     if (e != cudaSuccess) return noalloc_fail(KAMI_ERR_CUDA, "cudaGetDevice", e);
     if (dev < 0 || dev >= kMaxDevices) return noalloc_fail(KAMI_ERR_UNSUPPORTED, "device ordinal out of range");
+    cudaStream_t s = (cudaStream_t)stream;
+    // The symbol's device address belongs to the module loaded in the device's current context, and
+    // a cudaDeviceReset makes a new one, so it is looked up again on every call made outside a stream
+    // capture.  A call made while its stream captures takes the address of the last call made
+    // outside one on this device.
+    cudaStreamCaptureStatus capture = cudaStreamCaptureStatusNone;
+    e = cudaStreamIsCapturing(s, &capture);
+    if (e != cudaSuccess) return noalloc_fail(KAMI_ERR_CUDA, "cudaStreamIsCapturing", e);
     void* scratch = nullptr;
     {
         std::lock_guard<std::mutex> lock(g_scratch_mutex);
-        if (!g_scratch_ptr[dev]) {
-            e = cudaGetSymbolAddress(&g_scratch_ptr[dev], g_noalloc_scratch);
-            if (e != cudaSuccess) {
-                g_scratch_ptr[dev] = nullptr;
-                return noalloc_fail(KAMI_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch)", e);
-            }
+        if (capture == cudaStreamCaptureStatusNone) {
+            void* p = nullptr;
+            e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+            if (e != cudaSuccess) return noalloc_fail(KAMI_ERR_CUDA, "cudaGetSymbolAddress(g_noalloc_scratch)", e);
+            g_scratch_ptr[dev] = p;
+        } else if (!g_scratch_ptr[dev]) {
+            return noalloc_fail(KAMI_ERR_STATE,
+                                "the first kami_vbd_step_noalloc call on a device must come outside a stream capture");
         }
         scratch = g_scratch_ptr[dev];
     }
@@ -240,7 +267,7 @@ extern "C" kami_status kami_vbd_step_noalloc(const kami_vbd_desc* settings, kami
     pp.num_itr = settings->num_itr;
 
     // Sim::advance (step.cpp:38-62): clock = {h of the previous call, lastH, time}
-    const int steps = std::max(1, (int)std::ceil(dt / settings->max_h));
+    const int steps = std::max(1, (int)ratio);
     StepParams sp{};
     sp.last_h = a->clock[0];
     sp.h = dt / (float)steps;
@@ -260,7 +287,6 @@ extern "C" kami_status kami_vbd_step_noalloc(const kami_vbd_desc* settings, kami
     k.lr = a->rest_length;
     k.ks = a->stretch_stiffness;
     k.scratch = (float4*)scratch;
-    cudaStream_t s = (cudaStream_t)stream;
     const unsigned threads = 256, blocks = (unsigned)((k.nv + threads - 1) / threads);
     noalloc_flags_kernel<<<blocks, threads, 0, s>>>(k);
     for (int sub = 0; sub < steps; sub++) {

@@ -4,8 +4,8 @@
 //
 //  * sweep form: one kernel per phase (predict; per iteration: even-vertex, odd-vertex,
 //    even-segment, odd-segment sweeps; finish + SDF), each thread owning one slot and reading
-//    its neighbours from global memory.  This is the plain per-groom form; the host replays the
-//    whole step from a CUDA graph, as Sim::rebuildCUDAGraph does (YarnBall/sim/step.cpp:9-36).
+//    its neighbours from global memory: the reference's kernel-per-sweep structure.  The host
+//    replays the whole step from a CUDA graph, as Sim::rebuildCUDAGraph does (step.cpp:9-36).
 //
 //  * fused form: one kernel per step.  Each warp owns one tile (a strand, or several short
 //    strands, of up to 32*C vertices) in registers for every substep and iteration; neighbour

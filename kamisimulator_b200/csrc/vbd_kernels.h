@@ -47,9 +47,6 @@ cudaError_t launch_coll_steplimit(const DeviceState& st, const float4* dx4, cons
 // thread per slot): reads the iteration's starting displacements from snap, writes dx_out, updates
 // q in place.  Tiles of up to 1024 slots (coll_iteration_supported).
 bool coll_iteration_supported(int C);
-// FP32 FMA throughput (fp32_probe.cu): TFLOP/s of plain FFMA and of packed FFMA2 chains over
-// 8 blocks of 256 threads per SM, best of three timed launches on the current device.
-cudaError_t measure_fp32_peak(int sm_count, double* tflops_fma, double* tflops_fma2);
 cudaError_t launch_coll_iteration(const DeviceState& st, const float4* y4, float4* q, const float4* snap, float4* dx_out,
                                   const StepParams* d_sp, const PhysParams& pp, const CollParams& cp, cudaStream_t s);
 cudaError_t launch_sweep_position_coll(const DeviceState& st, const float4* y4, const float4* q, const float4* dx_in,

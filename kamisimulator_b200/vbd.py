@@ -39,7 +39,6 @@ EXPORTED = [
     "kami_vbd_batch_step", "kami_vbd_set_hair_layout", "kami_vbd_upload_hair", "kami_vbd_download_hair",
     "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake", "kami_vbd_sag_free",
     "kami_hair_subdivide", "kami_hair_resample", "kami_vbd_step_host", "kami_vbd_get_tiles_per_group",
-    "kami_fp32_peak",
 ]
 
 
@@ -143,7 +142,6 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_step": [vp, f32, vp],
         "kami_vbd_step_host": [vp, f32, vp, vp, vp, vp],
         "kami_vbd_get_tiles_per_group": [vp, ctypes.POINTER(i32)],
-        "kami_fp32_peak": [i32, ctypes.POINTER(ctypes.c_double), ctypes.POINTER(ctypes.c_double)],
         "kami_vbd_synchronize": [vp],
         "kami_vbd_state_size": [vp, ctypes.POINTER(ctypes.c_size_t)],
         "kami_vbd_get_state": [vp, vp, ctypes.c_size_t, i32],
@@ -530,14 +528,6 @@ class Solver:
 
 def version():
     return load_library().kami_vbd_version().decode()
-
-
-def fp32_peak(device=0):
-    """Measured FP32 FMA throughput of a GPU in TFLOP/s: (plain FFMA chains, packed FFMA2 chains)."""
-    lib = load_library()
-    fma, fma2 = ctypes.c_double(), ctypes.c_double()
-    _check(lib.kami_fp32_peak(device, ctypes.byref(fma), ctypes.byref(fma2)))
-    return fma.value, fma2.value
 
 
 def read_usc(path, max_verts=0):

@@ -1,4 +1,6 @@
 """Shared set-up for the tests: one settings dict drives both the CPU oracle and the GPU solver."""
+import ctypes
+
 import numpy as np
 
 from kamisimulator_b200 import synth
@@ -47,3 +49,23 @@ def random_velocities(groom, scale=0.3, seed=7):
     v = rng.normal(0.0, scale, (groom.num_vertices, 3)).astype(np.float32)
     v[groom.strand_begin[:-1]] = 0.0
     return v
+
+
+class NoAllocArgs(ctypes.Structure):
+    """kami_vbd_noalloc_args (include/kami_vbd.h)."""
+    _fields_ = [("num_vertices", ctypes.c_int64), ("num_strands", ctypes.c_int32),
+                ("strand_begin", ctypes.c_void_p), ("positions", ctypes.c_void_p), ("velocities", ctypes.c_void_p),
+                ("last_velocities", ctypes.c_void_p), ("orientations", ctypes.c_void_p),
+                ("rest_darboux", ctypes.c_void_p), ("inv_mass", ctypes.c_void_p), ("rest_length", ctypes.c_void_p),
+                ("stretch_stiffness", ctypes.c_void_p), ("clock", ctypes.c_float * 3)]
+
+
+def bind_noalloc():
+    """The library and its kami_vbd_step_noalloc entry point with argument types set."""
+    from kamisimulator_b200 import vbd
+
+    lib = vbd.load_library()
+    fn = lib.kami_vbd_step_noalloc
+    fn.argtypes = [ctypes.POINTER(vbd.Desc), ctypes.POINTER(NoAllocArgs), ctypes.c_float, ctypes.c_void_p]
+    fn.restype = ctypes.c_int
+    return lib, fn

@@ -167,3 +167,24 @@ def test_desc_defaults_for_hair_hair():
     assert d.barrier_thickness == pytest.approx(2 * 0.95 * 4e-5)  # StableCosseratRodsSolver.cpp:176-180
     assert d.k_collision == pytest.approx(1e-5) and d.k_friction == pytest.approx(5.0)
     assert d.friction_coeff == pytest.approx(0.1) and d.detection_scaler == pytest.approx(1.2)
+
+
+def test_noalloc_rejects_bad_dt_before_touching_a_device():
+    """A NaN or infinite dt, or one needing more than KAMI_MAX_SUBSTEPS substeps of max_h, is an
+    argument error found on the host; the (never dereferenced) array pointers need only be non-null."""
+    from tests.helpers import NoAllocArgs, bind_noalloc
+
+    lib, step_noalloc = bind_noalloc()
+    d = vbd.Desc()
+    lib.kami_vbd_desc_init(ctypes.byref(d))
+    d.schedule = 0
+    d.max_h = 1e-9
+    a = NoAllocArgs()
+    a.num_vertices, a.num_strands = 64, 2
+    for name in ("strand_begin", "positions", "velocities", "last_velocities", "orientations", "rest_darboux",
+                 "inv_mass", "rest_length", "stretch_stiffness"):
+        setattr(a, name, 256)
+    for dt in (float("nan"), float("inf"), -float("inf"), 1.0):  # 1 s / 1 ns = 1e9 substeps
+        assert step_noalloc(ctypes.byref(d), ctypes.byref(a), dt, None) == 1, dt
+        msg = lib.kami_vbd_last_error_string().decode()
+        assert "finite" in msg or "substeps" in msg, msg

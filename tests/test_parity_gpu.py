@@ -249,10 +249,11 @@ def test_nonfinite_strand_does_not_leak(form, tuning, schedule, pin_roots):
 
 
 def test_fp32_peak_probe():
-    """kami_fp32_peak: the FFMA / FFMA2 chain throughput that bench.py divides the fused step's FP32
-    rate by is a plausible B200 figure (nominal FP32: 74 TFLOP/s at 1965 MHz)."""
-    from kamisimulator_b200.vbd import fp32_peak
+    """kami_fp32_peak (the bench-only probe library): the FFMA / FFMA2 chain throughput that bench.py
+    divides the fused step's FP32 rate by is a plausible B200 figure (nominal FP32: 74 TFLOP/s at
+    1965 MHz)."""
+    import bench
 
-    fma, fma2 = fp32_peak(0)
+    fma, fma2 = bench.fp32_probe(0)
     assert 30.0 < fma < 150.0, fma
     assert 30.0 < fma2 < 300.0, fma2

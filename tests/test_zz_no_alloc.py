@@ -13,27 +13,9 @@ import numpy as np
 import pytest
 
 from tests import helpers
-from tests.helpers import POS_TOL, TWIST_TOL
+from tests.helpers import POS_TOL, TWIST_TOL, NoAllocArgs, bind_noalloc
 
 pytestmark = pytest.mark.gpu
-
-
-class NoAllocArgs(ctypes.Structure):
-    _fields_ = [("num_vertices", ctypes.c_int64), ("num_strands", ctypes.c_int32),
-                ("strand_begin", ctypes.c_void_p), ("positions", ctypes.c_void_p), ("velocities", ctypes.c_void_p),
-                ("last_velocities", ctypes.c_void_p), ("orientations", ctypes.c_void_p),
-                ("rest_darboux", ctypes.c_void_p), ("inv_mass", ctypes.c_void_p), ("rest_length", ctypes.c_void_p),
-                ("stretch_stiffness", ctypes.c_void_p), ("clock", ctypes.c_float * 3)]
-
-
-def _bind():
-    from kamisimulator_b200 import vbd
-
-    lib = vbd.load_library()
-    fn = lib.kami_vbd_step_noalloc
-    fn.argtypes = [ctypes.POINTER(vbd.Desc), ctypes.POINTER(NoAllocArgs), ctypes.c_float, ctypes.c_void_p]
-    fn.restype = ctypes.c_int
-    return lib, fn
 
 
 def test_noalloc_step_matches_handle_step_on_two_calls():
@@ -43,7 +25,7 @@ def test_noalloc_step_matches_handle_step_on_two_calls():
     from oracle import oracle as orc
     from oracle.oracle import twist_angles
 
-    lib, step_noalloc = _bind()
+    lib, step_noalloc = bind_noalloc()
     groom = helpers.soft_groom(200, (5, 61), seed=31)  # uneven strands: many start at an odd index
     v0 = helpers.random_velocities(groom, 0.2, seed=9)
     st = helpers.soft_settings(num_itr=6, max_h=1 / 120)  # two substeps per call
@@ -81,9 +63,12 @@ def test_noalloc_step_matches_handle_step_on_two_calls():
     torch.cuda.synchronize()
 
     for call in range(2):
+        free_before = torch.cuda.mem_get_info()[0]
         rc = step_noalloc(ctypes.byref(desc), ctypes.byref(args), dt, None)
         assert rc == 0, lib.kami_vbd_last_error_string().decode()
         torch.cuda.synchronize()
+        if call == 1:  # the first call may load the module; after it the device's free memory stays put
+            assert torch.cuda.mem_get_info()[0] == free_before
         handle.step(dt)
         xh, vh = handle.get_positions_velocities()
         qh = handle.get_orientations()
@@ -101,7 +86,7 @@ def test_noalloc_step_matches_handle_step_on_two_calls():
 def test_noalloc_rejects_more_vertices_than_its_scratch():
     from kamisimulator_b200 import vbd
 
-    lib, step_noalloc = _bind()
+    lib, step_noalloc = bind_noalloc()
     desc = vbd.Desc()
     lib.kami_vbd_desc_init(ctypes.byref(desc))
     args = NoAllocArgs()
@@ -110,3 +95,45 @@ def test_noalloc_rejects_more_vertices_than_its_scratch():
     rc = step_noalloc(ctypes.byref(desc), ctypes.byref(args), 1 / 60, None)
     assert rc == 6  # KAMI_ERR_UNSUPPORTED
     assert "262144" in lib.kami_vbd_last_error_string().decode()
+
+
+def test_noalloc_clamps_an_overlong_last_strand():
+    """strand_begin[num_strands] past num_vertices is clamped to the vertex range on the device: the
+    step equals the one with well-formed offsets, bit for bit, and reads nothing past the arrays."""
+    import torch
+
+    from kamisimulator_b200 import vbd
+    from oracle import oracle as orc
+
+    lib, step_noalloc = bind_noalloc()
+    groom = helpers.soft_groom(40, (5, 30), seed=5)
+    st = helpers.soft_settings(num_itr=4, max_h=1 / 60)
+    handle = helpers.gpu_solver(groom, st, form="sweep")
+    mat = orc.configure(groom, radius=st["radius"], density=st["density"], dtype=np.float32)
+    dev = torch.device("cuda")
+    t = lambda a: torch.tensor(np.ascontiguousarray(a), device=dev)  # noqa: E731
+    q0, qr = handle.get_orientations(), t(handle.get_rest_darboux())
+    handle.close()
+    im, lr, ks = t(mat["inv_mass"]), t(mat["l_rest"]), t(mat["k_stretch"])
+    desc = vbd.Desc()
+    lib.kami_vbd_desc_init(ctypes.byref(desc))
+    desc.gravity[:] = st["gravity"]
+    desc.num_itr, desc.max_h, desc.schedule, desc.wind_peak = st["num_itr"], st["max_h"], 0, 0.0
+    out = []
+    for extra in (0, 40):
+        sb = groom.strand_begin.astype(np.int32).copy()
+        sb[-1] += extra
+        bufs = dict(strand_begin=t(sb), positions=t(groom.positions.astype(np.float32)),
+                    velocities=t(helpers.random_velocities(groom, 0.2, seed=3)),
+                    last_velocities=torch.zeros((groom.num_vertices, 3), device=dev), orientations=t(q0),
+                    rest_darboux=qr, inv_mass=im, rest_length=lr, stretch_stiffness=ks)
+        args = NoAllocArgs()
+        args.num_vertices, args.num_strands = groom.num_vertices, groom.num_strands
+        for name, ten in bufs.items():
+            setattr(args, name, ten.data_ptr())
+        args.clock[:] = (np.float32(st["max_h"]), 0.0, 0.0)
+        assert step_noalloc(ctypes.byref(desc), ctypes.byref(args), 1 / 60, None) == 0
+        torch.cuda.synchronize()
+        out.append((bufs["positions"].cpu().numpy(), bufs["orientations"].cpu().numpy()))
+    assert np.array_equal(out[0][0], out[1][0]) and np.array_equal(out[0][1], out[1][1])
+    assert float(np.abs(out[0][0] - groom.positions).max()) > 1e-4
