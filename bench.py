@@ -331,6 +331,7 @@ def extra_forms(args, torch, stream, flush):
                                         "another with kami_vbd_step: the plain drop-in (form auto = fused, each "
                                         "handle autotuned) and the sweep form"}
     out["adjoint_2k_x48"] = adjoint_timing(torch, stream)
+    out["adjoint_fit"] = adjoint_fit(torch)
     out["sdf_bake_128"] = sdf_bake_timing()
     try:
         out["hair_hair_sweep"] = hair_hair_timing(torch, stream)
@@ -574,6 +575,53 @@ def large_adjoint(torch, s, counts, frames, tape_gb, k=10):
             "what": "d sum(c . x_239) / d per-strand stiffness over frames 210-239, head motion replayed"}
 
 
+def adjoint_fit(torch, iterations=60, frames=60, k=10, lr=0.1):
+    """Per-strand bend/twist stiffness fit on 2,000 strands x 48 vertices (20 iterations, dt 1/120 s,
+    head-sphere SDF): the target is the rollout at the true stiffness after `frames` frames, the
+    learnable scales start at truth x U[0.5, 2] (log-parameterised, Adam), the loss is the L2 distance
+    of the positions after the rollout, with a checkpoint every `k` frames.  Reports the loss curve
+    and how far the recovered scales are from 1 (the truth)."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.autograd import rollout_positions
+    from kamisimulator_b200.vbd import Solver
+
+    g = synth.groom(2000, 48, seed=4)
+    solver = Solver(g, form="fused", **settings())
+    unit = torch.tensor(solver.get_rest_darboux(), device="cuda")
+    strand_of = torch.tensor(np.repeat(np.arange(g.num_strands), np.diff(g.strand_begin)), device="cuda")
+    init = torch.tensor(solver.get_state(), device="cuda")
+    with torch.no_grad():
+        target = rollout_positions(torch.ones(g.num_strands, device="cuda"), solver, unit, strand_of, init, frames,
+                                   DT, k)
+    rng = np.random.default_rng(6)
+    start = rng.uniform(0.5, 2.0, g.num_strands)
+    logs = torch.tensor(np.log(start), dtype=torch.float32, device="cuda", requires_grad=True)
+    opt = torch.optim.Adam([logs], lr=lr)
+    losses = []
+    torch.cuda.synchronize()
+    t0 = time.perf_counter()
+    for _ in range(iterations):
+        opt.zero_grad()
+        x = rollout_positions(torch.exp(logs), solver, unit, strand_of, init, frames, DT, k)
+        loss = ((x - target) ** 2).sum()
+        loss.backward()
+        opt.step()
+        losses.append(loss.item())
+    torch.cuda.synchronize()
+    el = time.perf_counter() - t0
+    err = np.abs(np.exp(logs.detach().cpu().numpy()) - 1.0)
+    err0 = np.abs(start - 1.0)
+    solver.close()
+    return {"strands": g.num_strands, "verts_per_strand": 48, "frames": frames, "checkpoint_every": k,
+            "adam_iterations": iterations, "lr": lr, "seconds_per_iteration": el / iterations,
+            "loss_curve": [losses[i] for i in range(0, iterations, max(1, iterations // 12))] + [losses[-1]],
+            "loss_first": losses[0], "loss_last": losses[-1],
+            "scale_error_start": {"median": float(np.median(err0)), "p90": float(np.percentile(err0, 90))},
+            "scale_error_end": {"median": float(np.median(err)), "p90": float(np.percentile(err, 90))},
+            "what": "fit of per-strand stiffness scales (truth = 1) to the positions after a 60-frame rollout; "
+                    "|scale - 1| over the strands at the start and after the fit"}
+
+
 def adjoint_timing(torch, stream):
     """Device time per step of the forward step, the recorded forward and the adjoint (reverse) step
     on 2,000 strands x 48 vertices, plus one host-timed autograd round (60 steps, checkpoint 10)."""
@@ -587,6 +635,7 @@ def adjoint_timing(torch, stream):
     k = 10
     solver.tape_reserve(k, 0)
     init = solver.get_state()
+    solver_tape_gb = solver.tape_bytes_per_substep() * 60 / 1e9
 
     def timed(fn):
         solver.set_state(init)
@@ -614,20 +663,40 @@ def adjoint_timing(torch, stream):
     unit = torch.tensor(solver.get_rest_darboux(), device="cuda")
     strand_of = torch.tensor(np.repeat(np.arange(g.num_strands), np.diff(g.strand_begin)), device="cuda")
     init_d = torch.tensor(init, device="cuda")
-    scale = torch.ones(g.num_strands, device="cuda", requires_grad=True)
-    torch.cuda.synchronize()
-    t0 = time.perf_counter()
-    x = rollout_positions(scale, solver, unit, strand_of, init_d, 60, DT, k)
-    (x ** 2).sum().backward()
-    torch.cuda.synchronize()
-    round_s = time.perf_counter() - t0
+    frames = 60
+
+    def autograd_round(budget):
+        """Host time of the forward rollout and of its backward pass (60 frames, checkpoint every 10)."""
+        scale = torch.ones(g.num_strands, device="cuda", requires_grad=True)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        x = rollout_positions(scale, solver, unit, strand_of, init_d, frames, DT, k, tape_budget_bytes=budget)
+        loss = (x ** 2).sum()
+        torch.cuda.synchronize()
+        t1 = time.perf_counter()
+        loss.backward()
+        torch.cuda.synchronize()
+        return t1 - t0, time.perf_counter() - t1
+
+    autograd_round(0)  # warm-up
+    f_plain, b_recompute = autograd_round(0)
+    autograd_round(None)
+    f_tape, b_tape = autograd_round(None)
     solver.close()
     return {"forward_ms_per_step": fwd, "recorded_forward_ms_per_step": rec, "adjoint_ms_per_step": adj,
-            "adjoint_over_forward": adj / fwd, "backward_with_recompute_over_forward": (rec + adj) / fwd,
-            "autograd_round_s": round_s,
+            "adjoint_over_forward": adj / fwd, "recorded_forward_over_forward": rec / fwd,
+            "backward_with_recompute_over_forward": (rec + adj) / fwd,
+            "autograd": {"frames": frames, "checkpoint_every": k,
+                         "recompute_every_segment": {"forward_s": f_plain, "backward_s": b_recompute,
+                                                     "backward_over_forward": b_recompute / f_plain},
+                         "tape_recorded_in_forward": {"forward_s": f_tape, "backward_s": b_tape,
+                                                      "backward_over_forward": b_tape / f_plain,
+                                                      "forward_over_plain_forward": f_tape / f_plain,
+                                                      "tape_gb": solver_tape_gb}},
             "what": "2,000 strands x 48 vertices, 20 iterations, dt 1/120, sphere SDF; device time per step of "
-                    "kami_vbd_step, kami_vbd_step_record and kami_vbd_backward (10 recorded steps); "
-                    "autograd_round_s: host time of one 60-step rollout + backward with checkpoints every 10"}
+                    "kami_vbd_step, kami_vbd_step_record and kami_vbd_backward (10 recorded steps); autograd: host "
+                    "time of a 60-frame rollout and of its backward pass, every segment recomputed from its "
+                    "checkpoint (tape budget 0) or every segment recorded during the forward pass (default budget)"}
 
 
 def run_ours(args):
@@ -761,7 +830,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
-    ap.add_argument("--only", choices=["adjoint", "large", "hairhair", "bake", "long", "default", "trajectory"],
+    ap.add_argument("--only", choices=["adjoint", "fit", "large", "hairhair", "bake", "long", "default", "trajectory"],
                     help="run a single extra measurement")
     ap.add_argument("--tuning", help="fixed tile shape C,warps,steps_per_launch,register_cap instead of autotuning")
     args = ap.parse_args()
@@ -781,6 +850,10 @@ def main():
         print(json.dumps(hair_hair_timing(torch, torch.cuda.current_stream())), flush=True)
     elif args.only == "bake":
         print(json.dumps(sdf_bake_timing()), flush=True)
+    elif args.only == "fit":
+        import torch
+
+        print(json.dumps(adjoint_fit(torch)), flush=True)
     elif args.only == "trajectory":
         print(json.dumps(trajectory_errors()), flush=True)
     elif args.only == "default":

@@ -285,6 +285,7 @@ class Solver:
         _check(self.lib.kami_vbd_batch_count(h, ctypes.byref(ng)))
         self.num_grooms = ng.value
         self.max_h = float(np.float32(max_h))
+        self.num_itr = int(num_itr)
         del keep
 
     def substeps(self, dt):
@@ -486,6 +487,12 @@ class Solver:
     # -- differentiable stepping
     def tape_reserve(self, max_steps, max_tiles=0):
         _check(self.lib.kami_vbd_tape_reserve(self._h, max_steps, max_tiles))
+
+    def tape_bytes_per_substep(self, tiles=None):
+        """Device bytes one recorded substep of `tiles` warp tiles (all by default) takes on the tape:
+        (num_itr + 1) * 32 + 48 B per slot, as kami_vbd_tape_reserve allocates them."""
+        tiles = self.tile_count() if tiles is None else tiles
+        return ((self.num_itr + 1) * 32 + 48) * 32 * self.slots_per_lane * tiles
 
     def tile_count(self):
         n = ctypes.c_int64()

@@ -83,6 +83,46 @@ def test_stiffness_gradient_matches_fp64_autograd(sdf):
     solver.close()
 
 
+@pytest.mark.parametrize("budget", ["none", "one_segment", "all"])
+def test_tape_budget_modes_match_fp64_autograd(budget):
+    """The segments the tape budget holds are recorded in the forward pass, the others recomputed from
+    their checkpoints in the backward pass: no budget (every segment recomputed), one segment (7 frames
+    at k = 2: the last recorded, three recomputed) and the default (all recorded) give the FP64
+    gradient, with a moving body."""
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+
+    g, st, solver, unit, strand_of, init, v0 = _setup(num_strands=24, lengths=(6, 20), seed=17, sdf=True)
+    frames, k = 7, 2
+    body = np.array([list(synth.head_rotation(f / 60, 30.0, 2.0)) + [0.003 * f, -0.002 * f, 0.002 * f]
+                     for f in range(frames)], np.float32)
+    per_segment = solver.tape_bytes_per_substep() * solver.substeps(1 / 60) * k
+    tape = {"none": 0, "one_segment": per_segment, "all": None}[budget]
+    rng = np.random.default_rng(6)
+    scale0 = rng.uniform(0.7, 1.4, g.num_strands).astype(np.float32)
+    c = rng.normal(size=(g.num_vertices, 3))
+    scale = torch.tensor(scale0, device="cuda", requires_grad=True)
+    x = rollout_positions(scale, solver, unit, strand_of, init, frames, 1 / 60, checkpoint_every=k,
+                          body_transforms=body, tape_budget_bytes=tape)
+    (torch.tensor(c, dtype=torch.float32, device="cuda") * x).sum().backward()
+    _, g_ref, *_ = _torch_reference(g, st, v0, scale0, frames, c, body=body)
+    g_gpu = scale.grad.cpu().numpy()
+    assert _rel(g_gpu, g_ref) <= GRAD_TOL, (budget, _rel(g_gpu, g_ref))
+    # a second rollout on the same solver, and the backward of the first after it: the tape of the
+    # first is gone, so its backward recomputes every segment and still gives its own gradient
+    scale_a = torch.tensor(scale0, device="cuda", requires_grad=True)
+    xa = rollout_positions(scale_a, solver, unit, strand_of, init, frames, 1 / 60, checkpoint_every=k,
+                           body_transforms=body, tape_budget_bytes=tape)
+    scale_b = torch.tensor(scale0 * 1.3, device="cuda", requires_grad=True)
+    xb = rollout_positions(scale_b, solver, unit, strand_of, init, frames, 1 / 60, checkpoint_every=k,
+                           body_transforms=body, tape_budget_bytes=tape)
+    (torch.tensor(c, dtype=torch.float32, device="cuda") * xa).sum().backward()
+    assert _rel(scale_a.grad.cpu().numpy(), g_ref) <= GRAD_TOL, budget
+    del xb
+    solver.close()
+
+
 def test_gradient_with_a_moving_body_matches_fp64_autograd():
     """The head sphere yaws and slides into the strands frame by frame (kami_vbd_set_body_transform
     before every recorded step); the sliding head decides which vertices are projected."""
@@ -342,6 +382,43 @@ def test_checkpoint_interval_does_not_change_the_gradient():
     assert _rel(grads[0], grads[2]) <= 1e-5
     assert _rel(grads[1], grads[2]) <= 1e-5
     solver.close()
+
+
+def test_fit_gradient_at_the_initial_guess_matches_fp64_autograd():
+    """The stiffness-fit workload (2,000 strands x 48 vertices, 20 iterations, dt 1/120 s, head-sphere
+    SDF, target = the rollout at true stiffness after 60 frames, checkpoint every 10, scales starting at
+    truth x U[0.5, 2]) on a sample of 200 of its strands: the gradient of the L2 position loss at the
+    initial guess, against the FP64 autograd restatement.  Strands are independent and the loss is a sum
+    over vertices, so the sample's gradient is the full problem's on those strands."""
+    import torch
+
+    from kamisimulator_b200.autograd import rollout_positions
+
+    full = synth.groom(2000, 48, seed=4)
+    n, frames = 200, 60
+    sb = full.strand_begin[:n + 1]
+    g = type(full)(sb.copy(), full.positions[:sb[-1]].copy(), full.strand_young[:n].copy(), full.strand_dev[:n].copy())
+    st = dict(num_itr=20, max_h=1 / 120, gravity=(0.0, 0.0, -9.81), radius=40e-6,
+              sdf=synth.sphere_sdf(128, threshold=1e-3))
+    solver = helpers.gpu_solver(g, st, form="fused")
+    unit = torch.tensor(solver.get_rest_darboux(), device="cuda")
+    strand_of = torch.tensor(np.repeat(np.arange(g.num_strands), np.diff(g.strand_begin)), device="cuda")
+    init = torch.tensor(solver.get_state(), device="cuda")
+    with torch.no_grad():
+        target = rollout_positions(torch.ones(n, device="cuda"), solver, unit, strand_of, init, frames, 1 / 120, 10)
+    scale0 = np.random.default_rng(6).uniform(0.5, 2.0, 2000)[:n].astype(np.float32)
+    scale = torch.tensor(scale0, device="cuda", requires_grad=True)
+    x = rollout_positions(scale, solver, unit, strand_of, init, frames, 1 / 120, 10)
+    loss = ((x - target) ** 2).sum()
+    loss.backward()
+    g_gpu = scale.grad.cpu().numpy()
+    c = (2.0 * (x - target)).detach().cpu().numpy().astype(np.float64)  # d loss / d x at the initial guess
+    solver.close()
+    _, g_ref, *_ = _torch_reference(g, st, None, scale0, frames, c, dt=1 / 120)
+    print(f"\nfit gradient on 200 strands x 48, 60 frames: relative error {_rel(g_gpu, g_ref):.2e}, "
+          f"|g| {np.linalg.norm(g_ref):.3e}")
+    assert np.linalg.norm(g_ref) > 0
+    assert _rel(g_gpu, g_ref) <= GRAD_TOL, _rel(g_gpu, g_ref)
 
 
 def test_stiffness_fit_reduces_loss_on_the_2000_strand_workload():
