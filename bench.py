@@ -339,6 +339,9 @@ def extra_forms(args, torch, stream, flush):
         out["hair_hair_sweep"] = {"error": str(e)}
     out["long_strands_3k_x200"] = long_strand_timing(torch, stream, flush)
     out["reference_default_settings"] = default_settings_timing(torch, stream)
+    # the 80 M-vertex workload's kernels and body motion at a quarter of its size (bench.py --only large runs
+    # all 8 instances)
+    out["large_2x100k_x100"] = large_timing(torch, stream, frames=8, adjoint_frames=10, tape_gb=20.0, instances=2)
     return out
 
 
@@ -503,8 +506,8 @@ def hair_hair_timing(torch, stream, steps=50, h=4e-4):
     return res
 
 
-def large_timing(torch, stream, frames=24, adjoint_frames=30, tape_gb=60.0):
-    """8 instances x 100,000 strands x 100 vertices (80 M vertices), union-of-12-capsules SDF on 256^3,
+def large_timing(torch, stream, frames=24, adjoint_frames=30, tape_gb=60.0, instances=8):
+    """`instances` x 100,000 strands x 100 vertices (8 instances: 80 M vertices), union-of-12-capsules SDF on 256^3,
     head yawing +-30 deg at 1 Hz, 30 iterations, dt 1/120: kami_vbd_batch_step over `frames` frames with
     one body transform per frame (a sample of the 240-frame run).  Then the adjoint over the last
     `adjoint_frames` frames of the run (frames 210-239 of the head motion): a checkpointed rollout
@@ -515,7 +518,7 @@ def large_timing(torch, stream, frames=24, adjoint_frames=30, tape_gb=60.0):
 
     t0 = time.perf_counter()
     rng = np.random.default_rng(11)
-    inst = [synth.groom_strands(rng, np.full(100_000, 100)) for _ in range(8)]
+    inst = [synth.groom_strands(rng, np.full(100_000, 100)) for _ in range(instances)]
     sdf = synth.capsule_union_sdf(256, num_capsules=12, radius_range=(0.02, 0.08))
     gen_s = time.perf_counter() - t0
     st = dict(num_itr=30, max_h=DT, gravity=(0.0, 0.0, -9.81), radius=40e-6, density=1300.0, velocity_decay=0.05,
@@ -537,7 +540,8 @@ def large_timing(torch, stream, frames=24, adjoint_frames=30, tape_gb=60.0):
     torch.cuda.synchronize()
     ms = e0.elapsed_time(e1)
     s.synchronize()
-    out = {"value": V * 30 * frames / (ms / 1e3), "ms_per_step": ms / frames, "vertices": V, "frames_timed": frames,
+    out = {"value": V * 30 * frames / (ms / 1e3), "ms_per_step": ms / frames, "vertices": V, "instances": instances,
+           "frames_timed": frames,
            "tuning": dict(zip(("slots_per_lane", "warps_per_block", "steps_per_launch", "register_cap"), best)),
            "generate_s": gen_s, "create_s": create_s}
     out["adjoint"] = large_adjoint(torch, s, counts, adjoint_frames, tape_gb)
@@ -572,7 +576,8 @@ def large_adjoint(torch, s, counts, frames, tape_gb, k=10):
     return {"frames": frames, "checkpoint_every": k, "tiles": tiles, "tiles_per_window": chunk,
             "windows": -(-tiles // chunk), "tape_gb": chunk * per_tile / 1e9, "forward_s": t1 - t0,
             "backward_s": t2 - t1, "gradient_finite": finite,
-            "what": "d sum(c . x_239) / d per-strand stiffness over frames 210-239, head motion replayed"}
+            "what": f"d sum(c . x_239) / d per-strand stiffness over frames {first}-239, head motion replayed, every "
+                    "segment recomputed window by window"}
 
 
 def adjoint_fit(torch, iterations=60, frames=60, k=10, lr=0.1):

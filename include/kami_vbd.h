@@ -327,9 +327,20 @@ kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32
 kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int32_t* warps_per_block,
                                 int32_t* steps_per_launch, int32_t* register_cap);
 
+/* How the fused step's launches are scheduled (no counterpart in the reference).  0: one CTA per
+ * warps_per_block tiles (or per group of tiles), placed on the SMs by the hardware.
+ * KAMI_LAUNCH_PERSISTENT: as many CTAs as stay resident at once (or fewer, so that every CTA takes the
+ * same number of tiles), each looping over its tiles.  KAMI_LAUNCH_SDF_PREFETCH (with PERSISTENT): an
+ * iteration before each step's SDF pass, the grid cells the vertices will be projected in are
+ * prefetched into L2.  Results do not depend on the mode. */
+enum { KAMI_LAUNCH_PERSISTENT = 1, KAMI_LAUNCH_SDF_PREFETCH = 2 };
+kami_status kami_vbd_set_launch_mode(kami_vbd_handle h, int32_t mode);
+kami_status kami_vbd_get_launch_mode(kami_vbd_handle h, int32_t* mode);
+
 /* Times every tile shape on this handle's own strands (C in {min..4}, register cap {none, 120} for
  * C = 2, warps per CTA in {1,2,4,8}, steps per launch in {1,4,16}; trial_steps steps of dt each),
- * keeps the fastest and restores the simulation state and clock.
+ * keeps the fastest and restores the simulation state and clock; the fastest shape is then timed
+ * with each launch mode (kami_vbd_set_launch_mode) and keeps the fastest mode.
  * best = {C, warps, steps per launch, register cap}; best_rate in vertex-iters/s. */
 kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, int32_t best[4], double* best_rate);
 

@@ -93,6 +93,7 @@ struct kami_vbd_solver {
     // multi-step launches (kami_vbd_step_n) and tuning
     int steps_per_launch = 8;
     int reg_cap = 0;  // 0: fused kernel without a register cap; 120 / 168: the capped variants (C = 2 / 4); 2: packed
+    int launch_mode = 0;  // KAMI_LAUNCH_*: hardware-scheduled tile grid, or persistent resident CTAs
     StepParams* d_steps = nullptr;
     int d_steps_cap = 0;
     std::vector<StepParams> h_steps;
@@ -881,7 +882,7 @@ kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream) {
     kami_status st = on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
         if (h->form == KAMI_FORM_FUSED) {
             KAMI_CUDA(launch_fused_step(h->dstate(), h->pp, sp, h->sdf, h->layout.C, h->schedule == KAMI_SCHEDULE_JACOBI,
-                                        h->warps_per_block, s, nullptr, 1, h->reg_cap, h->layout.K),
+                                        h->warps_per_block, s, nullptr, 1, h->reg_cap, h->layout.K, h->launch_mode),
                       "fused step launch");
         } else {
             KAMI_TRY(build_sweep_graph(h, steps));
@@ -1137,6 +1138,26 @@ kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int3
     return KAMI_OK;
 }
 
+static_assert(KAMI_LAUNCH_PERSISTENT == LAUNCH_PERSISTENT && KAMI_LAUNCH_SDF_PREFETCH == LAUNCH_SDF_PREFETCH,
+              "the C ABI's launch mode bits are the launcher's");
+
+kami_status kami_vbd_set_launch_mode(kami_vbd_handle h, int32_t mode) {
+    KAMI_TRY(valid_handle(h));
+    if (mode & ~(KAMI_LAUNCH_PERSISTENT | KAMI_LAUNCH_SDF_PREFETCH))
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "launch mode bits are KAMI_LAUNCH_PERSISTENT | KAMI_LAUNCH_SDF_PREFETCH");
+    if ((mode & KAMI_LAUNCH_SDF_PREFETCH) && !(mode & KAMI_LAUNCH_PERSISTENT))
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "KAMI_LAUNCH_SDF_PREFETCH needs KAMI_LAUNCH_PERSISTENT");
+    if (mode != h->launch_mode) drop_graphs(h);
+    h->launch_mode = mode;
+    return KAMI_OK;
+}
+
+kami_status kami_vbd_get_launch_mode(kami_vbd_handle h, int32_t* mode) {
+    if (!h || !mode) return fail(KAMI_ERR_INVALID_ARGUMENT, "null handle or output");
+    *mode = h->launch_mode;
+    return KAMI_OK;
+}
+
 kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float* body_transforms, void* stream) {
     KAMI_TRY(valid_handle(h));
     if (n < 1) return fail(KAMI_ERR_INVALID_ARGUMENT, "n must be >= 1");
@@ -1174,7 +1195,7 @@ kami_status kami_vbd_step_n(kami_vbd_handle h, float dt, int32_t n, const float*
         for (int j0 = 0; j0 < n && err == cudaSuccess; j0 += F)
             err = launch_fused_step(h->dstate(), h->pp, h->h_steps[0], h->sdf, h->layout.C,
                                     h->schedule == KAMI_SCHEDULE_JACOBI, h->warps_per_block, h->stream, h->d_steps + j0,
-                                    std::min(F, n - j0), h->reg_cap, h->layout.K);
+                                    std::min(F, n - j0), h->reg_cap, h->layout.K, h->launch_mode);
         cudaGraph_t g = nullptr;
         cudaError_t e2 = cudaStreamEndCapture(h->stream, &g);
         if (err != cudaSuccess || e2 != cudaSuccess) {
@@ -1253,6 +1274,32 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
         }
     }
     if (st == KAMI_OK) st = kami_vbd_set_tuning(h, pick[0], pick[1], pick[2], pick[3]);
+    // the launch modes on the fastest shape (the packed variant has no persistent form)
+    int mode_best = 0;
+    const int modes[3] = {0, KAMI_LAUNCH_PERSISTENT, KAMI_LAUNCH_PERSISTENT | KAMI_LAUNCH_SDF_PREFETCH};
+    for (int mi = 0; mi < (pick[3] == 2 ? 1 : 3) && st == KAMI_OK; mi++) {
+        st = kami_vbd_set_launch_mode(h, modes[mi]);
+        if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
+        if (st == KAMI_OK) st = kami_vbd_step_n(h, dt, trial_steps, nullptr, nullptr);
+        if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
+        if (st != KAMI_OK) break;
+        cudaEventRecord(e0, h->stream);
+        st = kami_vbd_step_n(h, dt, trial_steps, nullptr, nullptr);
+        cudaEventRecord(e1, h->stream);
+        if (st != KAMI_OK) break;
+        if (cudaEventSynchronize(e1) != cudaSuccess) {
+            st = fail(KAMI_ERR_CUDA, "autotune timing");
+            break;
+        }
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, e0, e1);
+        const double rate = (double)h->nv * h->pp.num_itr * trial_steps / (ms * 1e-3);
+        if (mi == 0 || rate > rate_best) {
+            rate_best = rate;
+            mode_best = modes[mi];
+        }
+    }
+    if (st == KAMI_OK) st = kami_vbd_set_launch_mode(h, mode_best);
     if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
     if (e0) cudaEventDestroy(e0);
     if (e1) cudaEventDestroy(e1);

@@ -13,6 +13,9 @@
 //    update and the SDF projection run back to back, so HBM sees each vertex twice per step
 //    (one float4 load per array, one store per dynamic array).
 #include <algorithm>
+#include <map>
+#include <mutex>
+#include <tuple>
 
 #include "vbd_fused.cuh"
 #include "vbd_kernels.h"
@@ -270,9 +273,89 @@ cudaError_t launch_fused_frame(const DeviceState& st, const PhysParams& pp, cons
     return cudaErrorInvalidValue;
 }
 
+// Resident CTAs of `kernel` at `threads` threads on the current device (cached per device, kernel
+// and block size), times the SM count.
+static cudaError_t resident_ctas(const void* kernel, int threads, int64_t* out) {
+    static std::mutex mu;
+    static std::map<std::tuple<int, const void*, int>, int64_t> cache;
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(mu);
+    auto key = std::make_tuple(dev, kernel, threads);
+    auto it = cache.find(key);
+    if (it != cache.end()) {
+        *out = it->second;
+        return cudaSuccess;
+    }
+    int per_sm = 0, sms = 0;
+    if ((e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kernel, threads, 0)) != cudaSuccess) return e;
+    if ((e = cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev)) != cudaSuccess) return e;
+    *out = cache[key] = (int64_t)std::max(1, per_sm) * sms;
+    return cudaSuccess;
+}
+
+// The persistent grid for `units` units of work: as many CTAs as are resident at most, or fewer,
+// so that every CTA takes the same number of units (the last round is as full as the others).
+static cudaError_t persistent_grid(const void* kernel, int threads, int64_t units, unsigned* grid) {
+    int64_t resident = 0;
+    cudaError_t e = resident_ctas(kernel, threads, &resident);
+    if (e != cudaSuccess) return e;
+    const int64_t rounds = (units + resident - 1) / resident;
+    *grid = (unsigned)((units + rounds - 1) / rounds);
+    return cudaSuccess;
+}
+
+template <typename K>
+static cudaError_t launch_persistent(K kernel, int64_t units, int threads, cudaStream_t s, const DeviceState& st,
+                                     const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
+                                     const StepParams* d_steps, int nsteps) {
+    unsigned grid = 0;
+    cudaError_t e = persistent_grid((const void*)kernel, threads, units, &grid);
+    if (e != cudaSuccess) return e;
+    kernel<<<grid, threads, 0, s>>>(st, pp, sp, sdf, d_steps, nsteps);
+    return cudaGetLastError();
+}
+
+// The persistent form of launch_fused_step (LAUNCH_PERSISTENT).
+template <bool PF>
+static cudaError_t launch_fused_persistent(const DeviceState& st, const PhysParams& pp, const StepParams& sp,
+                                           const SdfParams& sdf, int C, bool jacobi, int warps_per_block,
+                                           cudaStream_t s, const StepParams* d_steps, int nsteps, int reg_cap,
+                                           int group) {
+    const int W = group > 1 ? group : warps_per_block;
+    const int64_t units = (st.num_tiles + W - 1) / W;
+    if (units == 0) return cudaSuccess;
+    const int threads = 32 * W;
+#define KAMI_PERSIST(KERNEL, CC)                                                                                 \
+    return jacobi ? launch_persistent(KERNEL<CC, true, PF>, units, threads, s, st, pp, sp, sdf, d_steps, nsteps) \
+                  : launch_persistent(KERNEL<CC, false, PF>, units, threads, s, st, pp, sp, sdf, d_steps, nsteps)
+    if (group > 1) {
+        if (group > 8 || st.num_tiles % group != 0) return cudaErrorInvalidValue;
+        if (C == 2 && reg_cap == 120) KAMI_PERSIST(fused_persistent_group_kernel_r120, 2);
+        if (C == 4 && reg_cap == 168) KAMI_PERSIST(fused_persistent_group_kernel_r168, 4);
+        if (C == 2) KAMI_PERSIST(fused_persistent_group_kernel, 2);
+        if (C == 4) KAMI_PERSIST(fused_persistent_group_kernel, 4);
+        return cudaErrorInvalidValue;
+    }
+    if (C == 2 && reg_cap == 120) KAMI_PERSIST(fused_persistent_kernel_r120, 2);
+    if (C == 4 && reg_cap == 168) KAMI_PERSIST(fused_persistent_kernel_r168, 4);
+    if (C == 2) KAMI_PERSIST(fused_persistent_kernel, 2);
+    if (C == 4) KAMI_PERSIST(fused_persistent_kernel, 4);
+#undef KAMI_PERSIST
+    return cudaErrorInvalidValue;
+}
+
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps,
-                              int nsteps, int reg_cap, int group) {
+                              int nsteps, int reg_cap, int group, int launch_mode) {
+    if ((launch_mode & LAUNCH_PERSISTENT) && !(reg_cap == 2 && C == 4 && !jacobi && group <= 1)) {
+        if (launch_mode & LAUNCH_SDF_PREFETCH)
+            return launch_fused_persistent<true>(st, pp, sp, sdf, C, jacobi, warps_per_block, s, d_steps, nsteps,
+                                                 reg_cap, group);
+        return launch_fused_persistent<false>(st, pp, sp, sdf, C, jacobi, warps_per_block, s, d_steps, nsteps, reg_cap,
+                                              group);
+    }
     if (group > 1) {
         if (group > 8 || st.num_tiles % group != 0) return cudaErrorInvalidValue;
         const unsigned gblocks = (unsigned)(st.num_tiles / group);

@@ -39,6 +39,7 @@ EXPORTED = [
     "kami_vbd_batch_step", "kami_vbd_set_hair_layout", "kami_vbd_upload_hair", "kami_vbd_download_hair",
     "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake", "kami_vbd_sag_free",
     "kami_hair_subdivide", "kami_hair_resample", "kami_vbd_step_host", "kami_vbd_get_tiles_per_group",
+    "kami_vbd_set_launch_mode", "kami_vbd_get_launch_mode",
 ]
 
 
@@ -149,6 +150,8 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_step_n": [vp, f32, i32, vp, vp],
         "kami_vbd_set_tuning": [vp, i32, i32, i32, i32],
         "kami_vbd_get_tuning": [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)],
+        "kami_vbd_set_launch_mode": [vp, i32],
+        "kami_vbd_get_launch_mode": [vp, ctypes.POINTER(i32)],
         "kami_vbd_autotune": [vp, f32, i32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)],
         "kami_vbd_tape_reserve": [vp, i32, i64],
         "kami_vbd_get_tile_count": [vp, ctypes.POINTER(i64)],
@@ -380,6 +383,16 @@ class Solver:
         _check(self.lib.kami_vbd_get_tuning(self._h, ctypes.byref(c), ctypes.byref(w), ctypes.byref(f),
                                             ctypes.byref(r)))
         return c.value, w.value, f.value, r.value
+
+    def set_launch_mode(self, mode):
+        """kami_vbd_set_launch_mode: 0 (hardware-scheduled tile grid), 1 (persistent), 3 (persistent with
+        the SDF cells prefetched into L2)."""
+        _check(self.lib.kami_vbd_set_launch_mode(self._h, int(mode)))
+
+    def get_launch_mode(self):
+        m = ctypes.c_int32()
+        _check(self.lib.kami_vbd_get_launch_mode(self._h, ctypes.byref(m)))
+        return m.value
 
     def autotune(self, dt, trial_steps=16):
         """Returns ((slots_per_lane, warps_per_block, steps_per_launch, register_cap), vertex-iters/s)."""

@@ -178,3 +178,34 @@ def test_four_slot_variants_match_the_plain_kernel_and_the_oracle(cap, schedule)
     finally:
         vbd.Solver.__init__ = orig
     assert ex <= helpers.POS_TOL and et <= helpers.TWIST_TOL, (ex, et)
+
+
+@pytest.mark.parametrize("case", ["c2_r120", "c4_r168", "c4_plain_steps4", "groups_of_2"])
+def test_launch_modes_give_the_same_steps(case):
+    """kami_vbd_set_launch_mode: the persistent grid (every CTA looping over an equal share of the
+    tiles) and its SDF-cell prefetch step each tile with the same arithmetic as the hardware-scheduled
+    grid, so positions and orientations agree bit for bit, for single tiles and groups of tiles."""
+    from kamisimulator_b200.vbd import Solver
+
+    lengths = (150, 250) if case == "groups_of_2" else (4, 60)
+    g = helpers.soft_groom(300, lengths, seed=41)
+    v = helpers.random_velocities(g, 0.2, seed=4)
+    st = helpers.soft_settings(max_h=1 / 120, num_itr=6, sdf=synth.sphere_sdf(64, threshold=2e-3))
+    tuning = {"c2_r120": (2, 4, 1, 120), "c4_r168": (4, 4, 1, 168), "c4_plain_steps4": (4, 2, 4, 1),
+              "groups_of_2": (4, 1, 2, 168)}[case]
+    out = []
+    for mode in (0, 1, 3):
+        s = Solver(g, form="fused", velocities=v, **st)
+        s.set_tuning(*tuning)
+        s.set_launch_mode(mode)
+        assert s.get_launch_mode() == mode
+        s.step_n(1 / 60, 5)
+        s.step(1 / 60)
+        x, vv = s.get_positions_velocities()
+        out.append((x, vv, s.get_orientations()))
+        if case == "groups_of_2":
+            assert s.tiles_per_group() == 2
+        s.close()
+    for x, vv, q in out[1:]:
+        assert np.array_equal(x, out[0][0]) and np.array_equal(vv, out[0][1]) and np.array_equal(q, out[0][2])
+    assert float(np.abs(out[0][0] - g.positions).max()) > 1e-3
