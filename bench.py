@@ -10,9 +10,11 @@ Metric: VBD vertex-iterations per second (vertices x iterations x steps / time),
 `value` times the fused step kernel with the state resident in HBM; the 95 MB working set fits
 the 126 MB L2, so a 256 MiB buffer is written between timed steps and only the step kernels are
 timed (CUDA events on the launching stream).  `e2e` is the same metric through the C ABI with
-host buffers: every frame is one kami_vbd_step_host call, which uploads positions/velocities from
-pinned host memory (UploadHair), steps and reads them back (DownloadHair), overlapping the copies of
-one strand group with the step of another; `three_calls_value` is the same frame as
+host buffers: every frame is one kami_vbd_step_hair call on the plugin's page-locked padded Hair
+arrays, which uploads positions/velocities (UploadHair), steps and writes them back (DownloadHair)
+from one kernel, overlapping the PCIe traffic of one tile with the step of another (the plugin's
+SolveNextStep + DownloadHair path); `packed_step_host_value` is kami_vbd_step_host on packed
+arrays, and `three_calls_value` is the same frame as
 kami_vbd_set_positions_velocities, kami_vbd_step, kami_vbd_get_positions_velocities in turn.  Extra
 `forms` report the sweep form, the batched form on 64 uneven grooms against the same grooms as one
 plain (fused, autotuned) handle each, and the other production forms; `trajectory` states the FP32
@@ -772,9 +774,17 @@ def run_ours(args):
         solver.step(DT, stream=stream)
         solver.get_positions_velocities(xh.numpy(), vh.numpy())
 
+    # the plugin's frame: its Hair (padded [strand][vertex] arrays, page-locked at Construct) uploaded,
+    # stepped and downloaded by one kami_vbd_step_hair call (UploadHair, SolveNextStep, DownloadHair)
+    solver.set_hair_layout(g.num_strands, 64)
+    hx = torch.empty((g.num_strands, 64, 3), dtype=torch.float32, pin_memory=True)
+    hv = torch.empty((g.num_strands, 64, 3), dtype=torch.float32, pin_memory=True)
+    solver.download_hair(hx, hv)
     for _ in range(3):
+        solver.step_hair(DT, hx, hv, hx, hv)
         solver.step_host(DT, xh, vh)
-    e2e_value = e2e_run(lambda: solver.step_host(DT, xh, vh))
+    e2e_value = e2e_run(lambda: solver.step_hair(DT, hx, hv, hx, hv))
+    e2e_packed = e2e_run(lambda: solver.step_host(DT, xh, vh))
     e2e_three_calls = e2e_run(three_calls)
     solver.close()
 
@@ -814,8 +824,10 @@ def run_ours(args):
                              "frac": achieved / peak, "traffic": traffic, "kernel": "fused_step_kernel (colour2, one step per launch)",
                              "bytes_per_launch": V * BYTES_PER_VERTEX_STEP, "peak_source": peak_kind},
                 "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": 24 * V, "d2h_bytes_per_step": 24 * V,
-                        "steps": e2e_steps, "call": "kami_vbd_step_host (pinned host buffers)",
-                        "three_calls_value": e2e_three_calls},
+                        "steps": e2e_steps,
+                        "call": "kami_vbd_step_hair on the plugin's page-locked padded Hair arrays (UploadHair + "
+                                "SolveNextStep + DownloadHair in one launch, the plugin's frame path)",
+                        "packed_step_host_value": e2e_packed, "three_calls_value": e2e_three_calls},
                 "fp32": fp32, "gpu_launches": args.steps, "clocks": clk.summary()}
     if world == 1 and rank == 0 and not args.skip_extra:
         line["forms"] = extra_forms(args, torch, stream, flush)

@@ -243,12 +243,32 @@ kami_status kami_vbd_sag_free(kami_vbd_handle h, int32_t iterations);
  * vertices are not in the solver, StableCosseratRodsSolver.cpp:134-136).  Then
  * kami_vbd_upload_hair / kami_vbd_download_hair replace UploadHair / DownloadHair
  * (StableCosseratRodsSolver.cpp:238-277) with one gather/scatter kernel over the padded arrays:
- * with device arrays nothing crosses PCIe; with host arrays each array is copied whole (download
- * copies it in and out, so the entries the solver does not own keep their values). */
+ * with device arrays nothing crosses PCIe; with host arrays inside page-locked allocations mapped
+ * into the device's address space (cudaHostAlloc, or kami_host_register) the kernel reads or writes
+ * the host arrays itself, only the entries the solver owns; with other host arrays each array is
+ * copied whole (download copies it in and out, so the entries the solver does not own keep their
+ * values). */
 kami_status kami_vbd_set_hair_layout(kami_vbd_handle h, int32_t hair_strands, int32_t max_verts,
                                      const int32_t* strand_refs);
 kami_status kami_vbd_upload_hair(kami_vbd_handle h, const float* xyz, const float* vxyz, int32_t memory);
 kami_status kami_vbd_download_hair(kami_vbd_handle h, float* xyz, float* vxyz, int32_t memory);
+
+/* One frame of the plugin over the padded Hair arrays of kami_vbd_set_hair_layout: UploadHair from
+ * hair_xyz_in / hair_vxyz_in (both NULL: the device state is current), SolveNextStep(dt) and
+ * DownloadHair to hair_xyz_out / hair_vxyz_out (both NULL: the results stay on the device); outputs
+ * may be the inputs.  StableCosseratRodsSolver.cpp:216-277 and KamiSimulator.cpp:380-390 in one call.
+ * With the fused form, no hair-hair collision and every given array inside one page-locked mapped
+ * allocation, it is one kernel launch that reads each tile's strands from the Hair, steps them and
+ * writes them back (the fused_frame kernel of kami_vbd_step_host); otherwise the three calls run in
+ * turn.  Blocks until the kernel has finished with the host arrays. */
+kami_status kami_vbd_step_hair(kami_vbd_handle h, float dt, const float* hair_xyz_in, const float* hair_vxyz_in,
+                               float* hair_xyz_out, float* hair_vxyz_out);
+
+/* Page-locks and maps an existing host range (cudaHostRegister, mapped and portable) so that the
+ * calls above take their one-launch paths on it, e.g. a Hair's arrays; kami_host_unregister undoes
+ * it.  The range must stay allocated while registered.  No counterpart in the reference. */
+kami_status kami_host_register(void* p, size_t bytes);
+kami_status kami_host_unregister(void* p);
 
 /* Body SDF grid baked from a closed, consistently wound triangle mesh on the GPU.  Replaces the
  * CPU bake of PNMesh::GenerateSDF + StoreSDFQueries (PNMesh.cpp:100-173; Discregrid in

@@ -75,6 +75,9 @@ struct kami_vbd_solver {
     int4* d_runs = nullptr;
     int32_t* d_run_begin = nullptr;
     int runs_C = 0;
+    // the same runs addressed in the padded Hair arrays (kami_vbd_set_hair_layout): .y is the padded
+    // entry of the run's first vertex; null when there is no Hair layout or it has 2^31 entries or more
+    int4* d_hair_runs = nullptr;
     int* d_status = nullptr;
     float4* d_sdf = nullptr;
     SdfParams sdf{};
@@ -113,6 +116,7 @@ struct kami_vbd_solver {
     // device-resident Hair: padded entry of each boundary vertex, and a staging copy of a padded
     // array for host transfers
     int64_t* d_hair_index = nullptr;
+    std::vector<int64_t> hair_index;  // host copy of d_hair_index
     float* d_hair_stage = nullptr;
     int64_t hair_entries = 0;  // Hair strands x max_verts
 
@@ -187,6 +191,7 @@ void release(kami_vbd_solver* h) {
     if (h->ev_b) cudaEventDestroy(h->ev_b);
     if (h->d_runs) cudaFree(h->d_runs);
     if (h->d_run_begin) cudaFree(h->d_run_begin);
+    if (h->d_hair_runs) cudaFree(h->d_hair_runs);
     if (h->stream) cudaStreamDestroy(h->stream);
     delete h;
 }
@@ -945,15 +950,30 @@ static kami_status build_host_runs(kami_vbd_solver* h) {
     std::vector<int32_t> next(begin.begin(), begin.end() - 1);
     std::vector<int4> runs(pieces.size());
     for (const Piece& pc : pieces) runs[next[pc.tile]++] = pc.run;
+    // with a Hair layout, the runs again with their first vertex's padded Hair entry (a strand's
+    // vertices are consecutive there too)
+    const bool hair = !h->hair_index.empty() && h->hair_entries < ((int64_t)1 << 31);
+    std::vector<int4> hruns;
+    if (hair) {
+        hruns = runs;
+        for (int4& r : hruns) r.y = (int32_t)h->hair_index[r.y];
+    }
     KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
     if (h->d_runs) cudaFree(h->d_runs);
     if (h->d_run_begin) cudaFree(h->d_run_begin);
+    if (h->d_hair_runs) cudaFree(h->d_hair_runs);
     h->d_runs = nullptr;
     h->d_run_begin = nullptr;
+    h->d_hair_runs = nullptr;
     h->runs_C = 0;
     KAMI_CUDA(dalloc(&h->d_runs, runs.size()), "strand runs");
     KAMI_CUDA(dalloc(&h->d_run_begin, begin.size()), "strand runs");
     KAMI_CUDA(cudaMemcpy(h->d_runs, runs.data(), sizeof(int4) * runs.size(), cudaMemcpyHostToDevice), "strand runs");
+    if (hair) {
+        KAMI_CUDA(dalloc(&h->d_hair_runs, hruns.size()), "Hair runs");
+        KAMI_CUDA(cudaMemcpy(h->d_hair_runs, hruns.data(), sizeof(int4) * hruns.size(), cudaMemcpyHostToDevice),
+                  "Hair runs");
+    }
     KAMI_CUDA(cudaMemcpy(h->d_run_begin, begin.data(), sizeof(int32_t) * begin.size(), cudaMemcpyHostToDevice),
               "strand runs");
     h->runs_C = C;
@@ -1022,6 +1042,57 @@ kami_status kami_vbd_step_host(kami_vbd_handle h, float dt, const float* xyz, co
     h->time += dt;
     h->counter += sp.substeps;
     return check_status_word(h);
+}
+
+kami_status kami_vbd_step_hair(kami_vbd_handle h, float dt, const float* hair_xyz_in, const float* hair_vxyz_in,
+                               float* hair_xyz_out, float* hair_vxyz_out) {
+    KAMI_TRY(valid_handle(h));
+    if (h->hair_index.empty()) return fail(KAMI_ERR_STATE, "call kami_vbd_set_hair_layout first");
+    if (!hair_xyz_in != !hair_vxyz_in || !hair_xyz_out != !hair_vxyz_out)
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "give both Hair input arrays or neither, and both outputs or neither");
+    KAMI_TRY(check_dt(h, dt));
+    const int64_t n = 3 * h->hair_entries;
+    HostIO io{};
+    bool direct = dt > 0.f && h->form == KAMI_FORM_FUSED && !h->hair_hair && h->hair_entries < ((int64_t)1 << 31);
+    if (direct && hair_xyz_in) {
+        io.x_in = mapped_range(hair_xyz_in, n);
+        io.v_in = mapped_range(hair_vxyz_in, n);
+        direct = io.x_in && io.v_in;
+    }
+    if (direct && hair_xyz_out) {
+        io.x_out = mapped_range(hair_xyz_out, n);
+        io.v_out = mapped_range(hair_vxyz_out, n);
+        direct = io.x_out && io.v_out;
+    }
+    if (!direct) {  // UploadHair, SolveNextStep, DownloadHair in turn
+        if (hair_xyz_in) KAMI_TRY(kami_vbd_upload_hair(h, hair_xyz_in, hair_vxyz_in, KAMI_MEMORY_HOST));
+        KAMI_TRY(kami_vbd_step(h, dt, nullptr));
+        if (hair_xyz_out) return kami_vbd_download_hair(h, hair_xyz_out, hair_vxyz_out, KAMI_MEMORY_HOST);
+        return kami_vbd_synchronize(h);
+    }
+    if (h->runs_C != h->layout.C) KAMI_TRY(build_host_runs(h));
+    if (!h->d_hair_runs) return fail(KAMI_ERR_STATE, "no Hair runs for this layout");
+    io.runs = h->d_hair_runs;
+    io.run_begin = h->d_run_begin;
+    const StepParams sp = advance_clock(h, dt);
+    KAMI_CUDA(launch_fused_frame(h->dstate(), h->pp, sp, h->sdf, io, h->layout.C, h->schedule == KAMI_SCHEDULE_JACOBI,
+                                 h->warps_per_block, h->stream, h->reg_cap, h->layout.K),
+              "fused Hair frame launch");
+    h->time += dt;
+    h->counter += sp.substeps;
+    return check_status_word(h);  // blocks: the host may touch the Hair arrays once this returns
+}
+
+kami_status kami_host_register(void* p, size_t bytes) {
+    if (!p || bytes == 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "null pointer or zero size");
+    KAMI_CUDA(cudaHostRegister(p, bytes, cudaHostRegisterMapped | cudaHostRegisterPortable), "cudaHostRegister");
+    return KAMI_OK;
+}
+
+kami_status kami_host_unregister(void* p) {
+    if (!p) return fail(KAMI_ERR_INVALID_ARGUMENT, "null pointer");
+    KAMI_CUDA(cudaHostUnregister(p), "cudaHostUnregister");
+    return KAMI_OK;
 }
 
 // Moves the live state to tiles of 32*C slots (gathered to boundary order and scattered back); the
@@ -1527,6 +1598,8 @@ kami_status kami_vbd_set_hair_layout(kami_vbd_handle h, int32_t hair_strands, in
     KAMI_CUDA(dalloc(&h->d_hair_index, h->nv), "Hair layout");
     KAMI_CUDA(cudaMemcpy(h->d_hair_index, index.data(), sizeof(int64_t) * h->nv, cudaMemcpyHostToDevice), "Hair layout");
     h->hair_entries = (int64_t)hair_strands * max_verts;
+    h->hair_index.swap(index);
+    h->runs_C = 0;  // the host-frame runs are rebuilt with the Hair's entries
     return KAMI_OK;
 }
 
@@ -1545,7 +1618,10 @@ kami_status kami_vbd_upload_hair(kami_vbd_handle h, const float* xyz, const floa
     for (int a = 0; a < 2; a++) {
         if (!srcs[a]) continue;
         const float* src = srcs[a];
-        if (memory == KAMI_MEMORY_HOST) {
+        const float* mapped = memory == KAMI_MEMORY_HOST ? mapped_range(src, 3 * h->hair_entries) : nullptr;
+        if (mapped) {  // page-locked and mapped: the scatter kernel reads the Hair over PCIe itself
+            src = mapped;
+        } else if (memory == KAMI_MEMORY_HOST) {
             KAMI_TRY(hair_stage(h));
             KAMI_CUDA(cudaMemcpyAsync(h->d_hair_stage, src, bytes, cudaMemcpyHostToDevice, h->stream), "Hair copy in");
             src = h->d_hair_stage;
@@ -1565,8 +1641,12 @@ kami_status kami_vbd_download_hair(kami_vbd_handle h, float* xyz, float* vxyz, i
     const size_t bytes = sizeof(float) * 3 * h->hair_entries;
     for (int a = 0; a < 2; a++) {
         if (!dsts[a]) continue;
-        if (memory == KAMI_MEMORY_DEVICE) {
-            KAMI_CUDA(launch_hair_out(srcs[a], dsts[a], h->d_slot_of, h->d_hair_index, h->nv, h->stream), "Hair gather");
+        float* mapped = memory == KAMI_MEMORY_HOST ? mapped_range(dsts[a], 3 * h->hair_entries) : nullptr;
+        if (memory == KAMI_MEMORY_DEVICE || mapped) {
+            // device memory, or page-locked and mapped: the gather kernel writes the owned entries in place
+            KAMI_CUDA(launch_hair_out(srcs[a], mapped ? mapped : dsts[a], h->d_slot_of, h->d_hair_index, h->nv,
+                                      h->stream),
+                      "Hair gather");
         } else {
             // the padded entries the solver does not own (skipped strands, padding) keep their values
             KAMI_TRY(hair_stage(h));

@@ -326,7 +326,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
     }
     float* const sx = stage;
     float* const sv = stage + 3 * 32 * C;
-    if constexpr (HOSTIO) {
+    if (HOSTIO && hio.x_in) {  // (no input buffers: the frame starts from the device state)
 #pragma unroll
         for (int k = 0; k < C; k++) {
             if (fl[k] & F_VALID) {  // padding slots keep their device values
@@ -629,7 +629,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
         st.vlast[g] = make_float4(vl[k].x, vl[k].y, vl[k].z, 0.f);
         st.q[g] = q[k];
     }
-    if constexpr (HOSTIO) {
+    if (HOSTIO && hio.x_out) {  // (no output buffers: the results stay on the device)
 #pragma unroll
         for (int k = 0; k < C; k++) {
             const int o = 3 * (lane * C + k);
@@ -682,7 +682,7 @@ __device__ __forceinline__ void fused_frame(DeviceState st, PhysParams pp, StepP
     const int64_t t = (int64_t)blockIdx.x * (blockDim.x >> 5) + w;
     if (t >= st.num_tiles) return;  // uniform per warp (per CTA for groups)
     float* const stage = kami_frame_stage + w * (6 * 32 * C);
-    const int r_end = hio.run_begin[t + 1];
+    const int r_end = hio.x_in ? hio.run_begin[t + 1] : 0;
     for (int r = hio.run_begin[t]; r < r_end; r++) {
         const int4 run = hio.runs[r];
         const float* gx = hio.x_in + 3LL * run.y;

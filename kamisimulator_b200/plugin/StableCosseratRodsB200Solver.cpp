@@ -22,7 +22,33 @@ std::string read_file(const std::string& path) {
 }  // namespace
 
 StableCosseratRodsB200Solver::~StableCosseratRodsB200Solver() {
+    try {
+        Flush();
+    } catch (...) {  // a destructor does not throw; the held-back step's error is dropped with the solver
+    }
+    ReleasePins();
     if (handle_) kami_vbd_destroy(handle_);
+}
+
+void StableCosseratRodsB200Solver::ReleasePins() {
+    if (pinned_) {
+        kami_host_unregister(hair_->positions.data());
+        kami_host_unregister(hair_->velocities.data());
+    }
+    pinned_ = false;
+}
+
+// Runs what UploadHair / SolveNextStep held back, without a download.
+void StableCosseratRodsB200Solver::Flush() {
+    const float* x = pending_upload_ ? hair_->positions.data() : nullptr;
+    const float* v = pending_upload_ ? hair_->velocities.data() : nullptr;
+    if (pending_step_) {
+        pending_step_ = pending_upload_ = false;
+        check(kami_vbd_step_hair(handle_, pending_dt_, x, v, nullptr, nullptr), "SolveNextStep");
+    } else if (pending_upload_) {
+        pending_upload_ = false;
+        check(kami_vbd_upload_hair(handle_, x, v, KAMI_MEMORY_HOST), "UploadHair");
+    }
 }
 
 void StableCosseratRodsB200Solver::check(kami_status st, const char* what) {
@@ -30,7 +56,9 @@ void StableCosseratRodsB200Solver::check(kami_status st, const char* what) {
 }
 
 void StableCosseratRodsB200Solver::SetBodyTransform(const float rotation_xyzw[4], const float translate[3]) {
-    if (handle_) check(kami_vbd_set_body_transform(handle_, rotation_xyzw, translate), "SetBodyTransform");
+    if (!handle_) return;
+    Flush();  // a held-back step runs with the transform it was given
+    check(kami_vbd_set_body_transform(handle_, rotation_xyzw, translate), "SetBodyTransform");
 }
 
 // StableCosseratRodsSolver::LoadSettingJsonContent + BuildYarnBallHair (StableCosseratRodsSolver.cpp:76-212).
@@ -180,6 +208,8 @@ void StableCosseratRodsB200Solver::Preprocess(const std::string& settingJsonPath
 }
 
 void StableCosseratRodsB200Solver::Construct(const std::string& settingJsonPath) {
+    if (handle_) Flush();
+    ReleasePins();  // Preprocess may reallocate the Hair's arrays
     Preprocess(settingJsonPath);
     kami_vbd_desc d = BuildDescriptor(settingJsonPath);
     if (d.num_strands == 0) throw std::runtime_error("the Hair has no strand with at least 4 vertices");
@@ -189,20 +219,47 @@ void StableCosseratRodsB200Solver::Construct(const std::string& settingJsonPath)
     // the Hair's padded arrays are read and written in place, through the strandRefs mapping
     check(kami_vbd_set_hair_layout(handle_, (int32_t)hair_->num_strands, (int32_t)hair_->max_verts, strand_refs_.data()),
           "Construct");
+    // page-locked Hair arrays let a frame read and write them from the kernel (kami_vbd_step_hair)
+    const size_t bytes = sizeof(float) * hair_->positions.size();
+    if (bytes > 0 && hair_->velocities.size() == hair_->positions.size()) {
+        const bool px = kami_host_register(hair_->positions.data(), bytes) == KAMI_OK;
+        const bool pv = px && kami_host_register(hair_->velocities.data(), bytes) == KAMI_OK;
+        if (px && !pv) kami_host_unregister(hair_->positions.data());
+        pinned_ = px && pv;  // otherwise the frames copy the arrays
+    }
 }
 
-void StableCosseratRodsB200Solver::SolveNextStep(float dt) { check(kami_vbd_step(handle_, dt, nullptr), "SolveNextStep"); }
+// Sim::advance + the SDF pass (StableCosseratRodsSolver.cpp:216-234).  Held back until the next
+// call, so that a DownloadHair right after it makes one kernel launch of the step and the download.
+void StableCosseratRodsB200Solver::SolveNextStep(float dt) {
+    if (!handle_) throw std::runtime_error("SolveNextStep before Construct");
+    if (pending_step_) Flush();
+    pending_step_ = true;
+    pending_dt_ = dt;
+}
 
-// Sim -> Hair (StableCosseratRodsSolver.cpp:258-277): one gather on the GPU into the padded arrays
+// Sim -> Hair (StableCosseratRodsSolver.cpp:258-277): with a held-back step, the step and the
+// download in one call; else one gather on the GPU into the padded arrays
 void StableCosseratRodsB200Solver::DownloadHair() {
+    if (pending_step_) {
+        const bool up = pending_upload_;
+        pending_step_ = pending_upload_ = false;
+        check(kami_vbd_step_hair(handle_, pending_dt_, up ? hair_->positions.data() : nullptr,
+                                 up ? hair_->velocities.data() : nullptr, hair_->positions.data(),
+                                 hair_->velocities.data()),
+              "SolveNextStep + DownloadHair");
+        return;
+    }
+    Flush();
     check(kami_vbd_download_hair(handle_, hair_->positions.data(), hair_->velocities.data(), KAMI_MEMORY_HOST),
           "DownloadHair");
 }
 
-// Hair -> Sim (StableCosseratRodsSolver.cpp:238-256)
+// Hair -> Sim (StableCosseratRodsSolver.cpp:238-256): held back until the next step or download
 void StableCosseratRodsB200Solver::UploadHair() {
-    check(kami_vbd_upload_hair(handle_, hair_->positions.data(), hair_->velocities.data(), KAMI_MEMORY_HOST),
-          "UploadHair");
+    if (!handle_) throw std::runtime_error("UploadHair before Construct");
+    Flush();
+    pending_upload_ = true;
 }
 
 std::string StableCosseratRodsB200Solver::GetInfoString() {

@@ -79,7 +79,11 @@ class StableCosseratRodsB200Solver : public Solver {
     void DownloadHair() override;
     std::string GetInfoString() override;
 
-    kami_vbd_handle handle() const { return handle_; }
+    // the C-ABI handle, for calls beyond the Solver interface (runs what is held back first)
+    kami_vbd_handle handle() {
+        if (handle_) Flush();
+        return handle_;
+    }
 
    private:
     kami_vbd_handle handle_ = nullptr;
@@ -92,6 +96,16 @@ class StableCosseratRodsB200Solver : public Solver {
     std::vector<int32_t> strand_begin_;
     std::vector<float> packed_pos_, packed_vel_;
     kami_vbd_sdf_desc sdf_desc_{};
+    // Frames over the Hair.  Construct page-locks the Hair's position and velocity arrays
+    // (kami_host_register); they must then not be reallocated until the solver is destroyed.  The
+    // last SolveNextStep before a DownloadHair, and an UploadHair before a SolveNextStep, are held
+    // back and run as one kami_vbd_step_hair call (upload, step and download in one launch); any
+    // other call runs what is held back first, so errors of a held-back step surface at that call.
+    bool pinned_ = false;
+    bool pending_upload_ = false, pending_step_ = false;
+    float pending_dt_ = 0.f;
+    void Flush();
+    void ReleasePins();
     void check(kami_status st, const char* what);
     // SubdivCoeff (DivideHair) and EnableResample / ResampleLen on the Hair, as Construct and
     // BuildYarnBallHair do them (StableCosseratRodsSolver.cpp:40, :141-163)

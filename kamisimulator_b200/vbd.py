@@ -39,7 +39,8 @@ EXPORTED = [
     "kami_vbd_batch_step", "kami_vbd_set_hair_layout", "kami_vbd_upload_hair", "kami_vbd_download_hair",
     "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake", "kami_vbd_sag_free",
     "kami_hair_subdivide", "kami_hair_resample", "kami_vbd_step_host", "kami_vbd_get_tiles_per_group",
-    "kami_vbd_set_launch_mode", "kami_vbd_get_launch_mode",
+    "kami_vbd_set_launch_mode", "kami_vbd_get_launch_mode", "kami_vbd_step_hair", "kami_host_register",
+    "kami_host_unregister",
 ]
 
 
@@ -151,6 +152,9 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_set_tuning": [vp, i32, i32, i32, i32],
         "kami_vbd_get_tuning": [vp, ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32), ctypes.POINTER(i32)],
         "kami_vbd_set_launch_mode": [vp, i32],
+        "kami_vbd_step_hair": [vp, f32, vp, vp, vp, vp],
+        "kami_host_register": [vp, ctypes.c_size_t],
+        "kami_host_unregister": [vp],
         "kami_vbd_get_launch_mode": [vp, ctypes.POINTER(i32)],
         "kami_vbd_autotune": [vp, f32, i32, ctypes.POINTER(i32), ctypes.POINTER(ctypes.c_double)],
         "kami_vbd_tape_reserve": [vp, i32, i64],
@@ -322,6 +326,12 @@ class Solver:
         px, mx = _ptr(x)
         pv, mv = _ptr(v)
         _check(self.lib.kami_vbd_upload_hair(self._h, px, pv, mx if x is not None else mv))
+
+    def step_hair(self, dt, x_in=None, v_in=None, x_out=None, v_out=None):
+        """kami_vbd_step_hair on padded Hair arrays (host float32, (hair_strands, max_verts, 3)):
+        upload (if x_in), step, download (if x_out), in one launch when the arrays are page-locked."""
+        p = [_ptr(a)[0] for a in (x_in, v_in, x_out, v_out)]
+        _check(self.lib.kami_vbd_step_hair(self._h, ctypes.c_float(dt), *p))
 
     def download_hair(self, x=None, v=None):
         """DownloadHair into padded arrays, in place (entries the solver does not own are kept)."""

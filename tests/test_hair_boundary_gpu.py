@@ -105,3 +105,59 @@ def test_usc_file_to_device_hair_round_trip(tmp_path):
     x = s.get_positions_velocities()[0]
     np.testing.assert_array_equal(np.concatenate([back[u, :c[u]] for u in refs]), x)
     s.close()
+
+
+def _pinned(a):
+    import torch
+
+    return torch.from_numpy(np.ascontiguousarray(a, np.float32)).pin_memory()
+
+
+@pytest.mark.parametrize("schedule", ["colour2", "jacobi"])
+def test_step_hair_frames_equal_upload_step_download(schedule):
+    """kami_vbd_step_hair on page-locked padded Hair arrays (one launch: the frame kernel reads each
+    tile's strands from the Hair, steps them and writes them back) against UploadHair, SolveNextStep,
+    DownloadHair as three calls on pageable arrays; the entries the solver does not own keep their
+    values.  Frames with input and output, with output only (the device state is current) and with
+    input only (the results stay on the device) all agree."""
+    import torch
+
+    padded, counts, g, refs = _hair()
+    st = dict(num_itr=6, max_h=1 / 120, gravity=(0.0, 0.0, -9.81), radius=40e-6, sdf=synth.sphere_sdf(64),
+              schedule=schedule)
+    a = helpers.gpu_solver(g, st, form="fused")
+    b = helpers.gpu_solver(g, st, form="fused")
+    for s in (a, b):
+        s.set_hair_layout(len(counts), MAXV, refs)
+    ha, va = padded.copy(), np.full_like(padded, -7.0)
+    hb, vb = _pinned(padded), _pinned(np.full_like(padded, -7.0))
+    a.download_hair(None, va)  # the solver's initial velocities into the owned entries
+    b.download_hair(None, vb)  # (page-locked: the gather kernel writes the host array itself)
+    np.testing.assert_array_equal(vb.numpy(), va)
+    rng = np.random.default_rng(2)
+    for f in range(6):
+        kick = (1e-3 * rng.standard_normal(va.shape)).astype(np.float32)
+        va += kick
+        vb += torch.from_numpy(kick)
+        a.upload_hair(ha, va)
+        a.step(1 / 60)
+        a.download_hair(ha, va)
+        if f % 3 == 0:
+            b.step_hair(1 / 60, hb, vb, hb, vb)
+        elif f % 3 == 1:
+            b.upload_hair(hb, vb)
+            b.step_hair(1 / 60, None, None, hb, vb)
+        else:
+            b.step_hair(1 / 60, hb, vb, None, None)
+            b.download_hair(hb, vb)
+        np.testing.assert_allclose(hb.numpy(), ha, rtol=0, atol=1e-6)
+        np.testing.assert_allclose(vb.numpy(), va, rtol=0, atol=2e-4)
+        hb.copy_(torch.from_numpy(ha))  # continue from the same state
+        vb.copy_(torch.from_numpy(va))
+    owned = np.zeros(padded.shape[:2], bool)
+    for u in refs:
+        owned[u, :counts[u]] = True
+    np.testing.assert_array_equal(hb.numpy()[~owned], padded[~owned])  # not the solver's: untouched
+    assert np.abs(ha[owned] - padded[owned]).max() > 1e-4
+    a.close()
+    b.close()
