@@ -327,15 +327,23 @@ __global__ void coll_steplimit_kernel(DeviceState st, const float4* __restrict__
 
 // ---- position sweep with contacts -----------------------------------------------------------------
 
-// One contact of segment (x0, x1) (displacements d0, d1) with the segment starting at slot o: the
-// IPC barrier and friction terms of cosserat.cu:177-226, for the segment's first vertex (own) or
-// its second vertex.
-__device__ __forceinline__ void contact_term(const DeviceState& st, const CollParams& cp, const float4* __restrict__ snap,
-                                             float3 x0, float3 x1, float3 d0, float3 d1, int64_t o, bool own,
-                                             float damp, float3& f, float H[6]) {
+// The partner segment of one contact: its end points and their displacements at the start of the
+// iteration.
+struct ContactOperands {
+    float3 b0, b1, db0, db1;
+};
+__device__ __forceinline__ ContactOperands load_contact(const DeviceState& st, const CollParams& cp,
+                                                       const float4* __restrict__ snap, int64_t o) {
     const int64_t on = next_slot(o, cp.C);
-    const float3 b0 = xyz(st.xm[o]), b1 = xyz(st.xm[on]);
-    const float3 db0 = xyz(snap[o]), db1 = xyz(snap[on]);
+    return ContactOperands{xyz(st.xm[o]), xyz(st.xm[on]), xyz(snap[o]), xyz(snap[on])};
+}
+
+// One contact of segment (x0, x1) (displacements d0, d1) with the partner segment c: the IPC barrier
+// and friction terms of cosserat.cu:177-226, for the segment's first vertex (own) or its second
+// vertex.
+__device__ __forceinline__ void contact_term(const CollParams& cp, const ContactOperands& c, float3 x0, float3 x1,
+                                             float3 d0, float3 d1, bool own, float damp, float3& f, float H[6]) {
+    const float3 b0 = c.b0, b1 = c.b1, db0 = c.db0, db1 = c.db1;
     const float2 uv = seg_closest(f3(0.f, 0.f, 0.f), (x1 - x0) + (d1 - d0), (b0 - x0) + (db0 - d0), (b1 - x0) + (db1 - d0));
     const float3 dpos = mixv(x0, x1, uv.x) - mixv(b0, b1, uv.y);
     const float3 ddpos = mixv(d0, d1, uv.x) - mixv(db0, db1, uv.y);
@@ -370,6 +378,23 @@ __device__ __forceinline__ void contact_term(const DeviceState& st, const CollPa
     }
 }
 
+// Every contact of the segment starting at slot g, in list order (the order of the sums is that of
+// one contact at a time).  The next contact's operands are loaded before the current one is
+// evaluated, so each gather overlaps the arithmetic of the contact before it.
+__device__ __forceinline__ void contact_terms(const DeviceState& st, const CollParams& cp, const float4* __restrict__ snap,
+                                              int64_t g, float3 x0, float3 x1, float3 d0, float3 d1, bool own,
+                                              float damp, float3& f, float H[6]) {
+    const int n = cp.ncols[g];
+    if (n <= 0) return;
+    ContactOperands cur = load_contact(st, cp, snap, cp.cols[g]);
+    for (int m = 0; m < n; m++) {
+        ContactOperands nxt = cur;
+        if (m + 1 < n) nxt = load_contact(st, cp, snap, cp.cols[(int64_t)(m + 1) * cp.num_slots + g]);
+        contact_term(cp, cur, x0, x1, d0, d1, own, damp, f, H);
+        cur = nxt;
+    }
+}
+
 // cosseratItr with contacts for one vertex (cosserat.cu:112-285): the full 3x3 block (hess3(m/h^2),
 // stretch, and each contact's IPC barrier and friction terms for the vertex's two segments), solved
 // with glm's adjugate inverse and clamped to the segments' step limit.  The in-strand operands are
@@ -400,9 +425,7 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
         H[1] += dd;
         H[2] += dd;
         step_limit = cp.maxstep[g];
-        const int n = cp.ncols[g];
-        for (int m = 0; m < n; m++)
-            contact_term(st, cp, snap, vi, xj, vi_dx, vj_dx, cp.cols[(int64_t)m * cp.num_slots + g], true, damp, f, H);
+        contact_terms(st, cp, snap, g, vi, xj, vi_dx, vj_dx, true, damp, f, H);
     }
     if (fl & F_HAS_PREV) {
         const float invl = 1.f / pp4.x;
@@ -412,9 +435,7 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
         float3 f2 = (-kk) * cc - (damp * dd) * vi_dx;
         dd *= 1.f + damp;
         float H2[6] = {dd, dd, dd, 0.f, 0.f, 0.f};
-        const int n = cp.ncols[gp];
-        for (int m = 0; m < n; m++)
-            contact_term(st, cp, snap, xp, vi, dp, vi_dx, cp.cols[(int64_t)m * cp.num_slots + gp], false, damp, f2, H2);
+        contact_terms(st, cp, snap, gp, xp, vi, dp, vi_dx, false, damp, f2, H2);
         step_limit = fminf(step_limit, cp.maxstep[gp]);
         f = f + f2;
 #pragma unroll

@@ -88,6 +88,17 @@ kami_vbd_desc StableCosseratRodsB200Solver::BuildDescriptor(const std::string& s
         auto it = j.find(k);
         if (it != j.end() && it->second.kind == JsonValue::Bool) dst = it->second.boolean;
     };
+    // What this solver does not build is refused rather than ignored: a YarnBall JSON scene
+    // (YBJsonPath, the reference's buildFromJSON route, StableCosseratRodsSolver.cpp:42-46: explicit
+    // pins, glued endpoints and their connection springs, jsonBuilder.cpp:83-85) and the SDF solver's
+    // strain limiting (UseStrainLimiting, SDFBodyCollisionSolver.cpp:37, :186).
+    auto yb = j.find("YBJsonPath");
+    if (yb != j.end() && yb->second.kind == JsonValue::String && !yb->second.text.empty() &&
+        std::ifstream(yb->second.text).good())
+        throw std::runtime_error("YBJsonPath: YarnBall JSON scenes (buildFromJSON, glued endpoints) are not supported");
+    auto sl = j.find("UseStrainLimiting");
+    if (sl != j.end() && sl->second.kind == JsonValue::Bool && sl->second.boolean)
+        throw std::runtime_error("UseStrainLimiting: the SDF pass's strain limiting is not supported");
     float num_itr = (float)d.num_itr, sag_free = 0.f;
     bool hair_hair = false;
     num("NumItr", num_itr);

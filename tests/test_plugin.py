@@ -70,6 +70,18 @@ def test_invalid_settings_are_rejected(tmp_path):
     r = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
                        capture_output=True, text=True)
     assert r.returncode == 1 and "Schedule" in r.stderr
+    # features of the reference this solver does not build are refused, not ignored
+    (tmp_path / "scene.json").write_text("{}")
+    for bad, word in (({"YBJsonPath": str(tmp_path / "scene.json")}, "YBJsonPath"),
+                      ({"UseStrainLimiting": True}, "UseStrainLimiting")):
+        (tmp_path / "s.json").write_text(json.dumps(bad))
+        r = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
+                           capture_output=True, text=True)
+        assert r.returncode == 1 and word in r.stderr, r.stderr
+    # a YBJsonPath that names no file falls back to the Hair, as in the reference (IsFileExist)
+    (tmp_path / "s.json").write_text(json.dumps({"YBJsonPath": str(tmp_path / "missing.json")}))
+    subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")], check=True,
+                   capture_output=True)
 
 
 def test_sag_free_setting(tmp_path):
