@@ -42,6 +42,41 @@ def test_max_over_ranks_and_weak_scaling_throughput():
     assert out[0][1] == pytest.approx(2 * 640000 * 20 * 100 / 0.020)
 
 
+def _plan_main(rank, world, port, out):
+    import torch
+    import torch.distributed as dist
+
+    import bench
+
+    os.environ.update(MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port), RANK=str(rank), WORLD_SIZE=str(world),
+                      LOCAL_RANK=str(rank))
+    dist.init_process_group("gloo", rank=rank, world_size=world)
+    try:
+        w, r, local = bench.dist_setup()
+        g = bench.rank_groom(r)
+        mine = torch.tensor([float(local), float(g.positions[:64].sum()), float(g.num_vertices)], dtype=torch.float64)
+        every = [torch.zeros_like(mine) for _ in range(world)]
+        dist.all_gather(every, mine)
+        out[rank] = [e.tolist() for e in every]
+    finally:
+        dist.destroy_process_group()
+
+
+def test_each_rank_binds_its_own_device_and_groom():
+    """bench.py's per-rank plan: rank r binds GPU LOCAL_RANK = r and steps a groom of its own (same
+    size, different strands), so N ranks run N independent replicas."""
+    world = 2
+    port = _free_port()
+    mgr = mp.Manager()
+    out = mgr.dict()
+    mp.spawn(_plan_main, args=(world, port, out), nprocs=world, join=True)
+    plans = out[0]
+    assert plans == out[1]
+    assert [p[0] for p in plans] == [0.0, 1.0]  # distinct devices
+    assert plans[0][1] != plans[1][1]  # distinct grooms
+    assert plans[0][2] == plans[1][2] == 640000.0  # of the same size (weak scaling)
+
+
 def test_reference_arm_runs_on_rank_zero_only(monkeypatch, capsys):
     import bench
 
