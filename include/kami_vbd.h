@@ -349,11 +349,9 @@ kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int3
 
 /* How the fused step's launches are scheduled (no counterpart in the reference).  0: one CTA per
  * warps_per_block tiles (or per group of tiles), placed on the SMs by the hardware.
- * KAMI_LAUNCH_PERSISTENT: as many CTAs as stay resident at once (or fewer, so that every CTA takes the
- * same number of tiles), each looping over its tiles.  KAMI_LAUNCH_SDF_PREFETCH (with PERSISTENT): an
- * iteration before each step's SDF pass, the grid cells the vertices will be projected in are
- * prefetched into L2.  Results do not depend on the mode. */
-enum { KAMI_LAUNCH_PERSISTENT = 1, KAMI_LAUNCH_SDF_PREFETCH = 2 };
+ * KAMI_LAUNCH_PERSISTENT: at most as many CTAs as stay resident at once, each looping over every
+ * gridDim-th unit of tiles.  The results agree to the last bits (the kernels are compiled apart). */
+enum { KAMI_LAUNCH_PERSISTENT = 1 };
 kami_status kami_vbd_set_launch_mode(kami_vbd_handle h, int32_t mode);
 kami_status kami_vbd_get_launch_mode(kami_vbd_handle h, int32_t* mode);
 

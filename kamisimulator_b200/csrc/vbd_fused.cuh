@@ -41,24 +41,6 @@ __device__ __forceinline__ float4 qmul_conj_fma(float4 l, float4 r) {
     return qmul_fma(l, make_float4(-r.x, -r.y, -r.z, r.w));
 }
 
-// L2 prefetch of the SDF cell around p (the lines of its 8 corners, vbd_sdf's nearest-node index):
-// a hint issued before the last substep's iterations, so the SDF pass's corner loads find the
-// lines in L2.
-__device__ __forceinline__ void sdf_prefetch_l2(float3 p, const SdfParams& sdf, const StepParams& st) {
-    const float4 invq = make_float4(-st.rot_x, -st.rot_y, -st.rot_z, st.rot_w);
-    const float3 lp = qrotate(invq, p - f3(st.tr_x, st.tr_y, st.tr_z)) - f3(sdf.min_x, sdf.min_y, sdf.min_z);
-    const int ix = __float2int_rn(lp.x * sdf.inv_x), iy = __float2int_rn(lp.y * sdf.inv_y),
-              iz = __float2int_rn(lp.z * sdf.inv_z);
-    if (ix < 0 || ix >= sdf.nx || iy < 0 || iy >= sdf.ny || iz < 0 || iz >= sdf.nz) return;
-    const int jy = min(iy + 1, sdf.ny - 1), jz = min(iz + 1, sdf.nz - 1);
-    const int64_t sy = sdf.nx, sz = (int64_t)sdf.nx * sdf.ny;
-    const float4* a = sdf.grid + ix;
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(a + iy * sy + iz * sz));
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(a + jy * sy + iz * sz));
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(a + iy * sy + jz * sz));
-    asm volatile("prefetch.global.L2 [%0];" ::"l"(a + jy * sy + jz * sz));
-}
-
 // One position update with folded coefficients (see the file comment).  Neighbour operands from
 // another strand (no segment in between: hn / hp false) are replaced by the vertex's own values
 // before they meet their zero coefficient, and vertices that do not move (upd false) keep dx, so a
@@ -261,11 +243,8 @@ struct GroupExchange {
 // tile position p = lane * C + k, and the step writes its results back to the host buffers
 // through the same area, as well as to the device state.
 // EXPLICIT_TILE steps tile `frame_tile` (the persistent kernels' tile loop) instead of the launch's own.
-// SDF_PREFETCH asks L2, before the iterations of each step's last substep, for the grid cells the
-// vertices will be projected in after them, from their predicted positions (a hint: the results do
-// not depend on it).
 template <int C, bool JACOBI, bool RECORD, bool PAIRED = false, bool HOSTIO = false, bool GROUPED = false,
-          bool EXPLICIT_TILE = false, bool SDF_PREFETCH = false>
+          bool EXPLICIT_TILE = false>
 __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                 TapeView tp, const StepParams* __restrict__ steps, int nsteps,
                                                 HostIO hio = HostIO{}, int64_t frame_tile = 0, float* stage = nullptr) {
@@ -406,10 +385,6 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                 Ve[k] = (-2.f * kk[k]) * e[k];
                 d3[k] = d3_of(q[k]);
             }
-        }
-        if (SDF_PREFETCH && s == sp.substeps - 1 && sdf.grid) {
-#pragma unroll
-            for (int k = 0; k < C; k++) sdf_prefetch_l2(x[k] + dx[k], sdf, sp);
         }
         float4 qP = shfl_up4(q[C - 1], 1);
         float3 d3P = shfl_up3(d3[C - 1], 1);  // the previous lane's d3_of(qP)
@@ -754,55 +729,54 @@ __global__ void __maxnreg__(120) fused_step_kernel_r120(DeviceState st, PhysPara
 }
 
 // ---- persistent form ----------------------------------------------------------------------------
-// A grid of CTAs that stay resident: CTA b's warp w steps tiles u * W + w for u = b, b + gridDim.x, ...
-// (W warps per CTA), or, for groups of K tiles (GROUPED, W = K), the groups b, b + gridDim.x, ...  The
-// host sizes the grid so that every CTA takes the same number of units (fused_persistent_grid), so
-// the SMs stay equally loaded to the end of the launch instead of running a partial last wave.
-template <int C, bool JACOBI, bool GROUPED, bool SDF_PREFETCH>
+// A grid of at most as many CTAs as stay resident: CTA b's warp w steps tiles u * W + w for
+// u = b, b + gridDim.x, ... (W warps per CTA), or, for groups of K tiles (GROUPED, W = K), the groups
+// b, b + gridDim.x, ...  With the grid at the resident count, the SMs' shares differ by one unit.
+template <int C, bool JACOBI, bool GROUPED>
 __device__ __forceinline__ void fused_persistent(DeviceState st, PhysParams pp, StepParams sp, SdfParams sdf,
                                                  const StepParams* __restrict__ steps, int nsteps) {
     // only the 32-bit unit index stays live across the step body (register pressure)
     for (int u = blockIdx.x; (int64_t)u * (blockDim.x >> 5) < st.num_tiles; u += gridDim.x) {
-        fused_step_body<C, JACOBI, false, false, false, GROUPED, true, SDF_PREFETCH>(
+        fused_step_body<C, JACOBI, false, false, false, GROUPED, true>(
             st, pp, sp, sdf, TapeView{}, steps, nsteps, HostIO{}, (int64_t)u * (blockDim.x >> 5) + (threadIdx.x >> 5));
         if (GROUPED) __syncthreads();  // the group exchange area is reused by the next group
     }
 }
-template <int C, bool JACOBI, bool SDF_PREFETCH>
+template <int C, bool JACOBI>
 __global__ void __launch_bounds__(256) fused_persistent_kernel(DeviceState st, PhysParams pp, StepParams sp,
                                                                SdfParams sdf, const StepParams* __restrict__ steps,
                                                                int nsteps) {
-    fused_persistent<C, JACOBI, false, SDF_PREFETCH>(st, pp, sp, sdf, steps, nsteps);
+    fused_persistent<C, JACOBI, false>(st, pp, sp, sdf, steps, nsteps);
 }
-template <int C, bool JACOBI, bool SDF_PREFETCH>
+template <int C, bool JACOBI>
 __global__ void __maxnreg__(120) fused_persistent_kernel_r120(DeviceState st, PhysParams pp, StepParams sp,
                                                               SdfParams sdf, const StepParams* __restrict__ steps,
                                                               int nsteps) {
-    fused_persistent<C, JACOBI, false, SDF_PREFETCH>(st, pp, sp, sdf, steps, nsteps);
+    fused_persistent<C, JACOBI, false>(st, pp, sp, sdf, steps, nsteps);
 }
-template <int C, bool JACOBI, bool SDF_PREFETCH>
+template <int C, bool JACOBI>
 __global__ void __maxnreg__(168) fused_persistent_kernel_r168(DeviceState st, PhysParams pp, StepParams sp,
                                                               SdfParams sdf, const StepParams* __restrict__ steps,
                                                               int nsteps) {
-    fused_persistent<C, JACOBI, false, SDF_PREFETCH>(st, pp, sp, sdf, steps, nsteps);
+    fused_persistent<C, JACOBI, false>(st, pp, sp, sdf, steps, nsteps);
 }
-template <int C, bool JACOBI, bool SDF_PREFETCH>
+template <int C, bool JACOBI>
 __global__ void __launch_bounds__(256) fused_persistent_group_kernel(DeviceState st, PhysParams pp, StepParams sp,
                                                                      SdfParams sdf, const StepParams* __restrict__ steps,
                                                                      int nsteps) {
-    fused_persistent<C, JACOBI, true, SDF_PREFETCH>(st, pp, sp, sdf, steps, nsteps);
+    fused_persistent<C, JACOBI, true>(st, pp, sp, sdf, steps, nsteps);
 }
-template <int C, bool JACOBI, bool SDF_PREFETCH>
+template <int C, bool JACOBI>
 __global__ void __maxnreg__(120) fused_persistent_group_kernel_r120(DeviceState st, PhysParams pp, StepParams sp,
                                                                     SdfParams sdf,
                                                                     const StepParams* __restrict__ steps, int nsteps) {
-    fused_persistent<C, JACOBI, true, SDF_PREFETCH>(st, pp, sp, sdf, steps, nsteps);
+    fused_persistent<C, JACOBI, true>(st, pp, sp, sdf, steps, nsteps);
 }
-template <int C, bool JACOBI, bool SDF_PREFETCH>
+template <int C, bool JACOBI>
 __global__ void __maxnreg__(168) fused_persistent_group_kernel_r168(DeviceState st, PhysParams pp, StepParams sp,
                                                                     SdfParams sdf,
                                                                     const StepParams* __restrict__ steps, int nsteps) {
-    fused_persistent<C, JACOBI, true, SDF_PREFETCH>(st, pp, sp, sdf, steps, nsteps);
+    fused_persistent<C, JACOBI, true>(st, pp, sp, sdf, steps, nsteps);
 }
 
 }  // namespace kami

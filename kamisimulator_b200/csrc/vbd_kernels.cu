@@ -295,14 +295,14 @@ static cudaError_t resident_ctas(const void* kernel, int threads, int64_t* out) 
     return cudaSuccess;
 }
 
-// The persistent grid for `units` units of work: as many CTAs as are resident at most, or fewer,
-// so that every CTA takes the same number of units (the last round is as full as the others).
+// The persistent grid for `units` units of work: the resident CTA count, or fewer when there are
+// fewer units.  (A smaller grid that gives every CTA the same number of units was measured slower:
+// the SMs then hold unequal numbers of CTAs, and the SM with the most sets the time.)
 static cudaError_t persistent_grid(const void* kernel, int threads, int64_t units, unsigned* grid) {
     int64_t resident = 0;
     cudaError_t e = resident_ctas(kernel, threads, &resident);
     if (e != cudaSuccess) return e;
-    const int64_t rounds = (units + resident - 1) / resident;
-    *grid = (unsigned)((units + rounds - 1) / rounds);
+    *grid = (unsigned)std::min<int64_t>(units, resident);
     return cudaSuccess;
 }
 
@@ -318,7 +318,6 @@ static cudaError_t launch_persistent(K kernel, int64_t units, int threads, cudaS
 }
 
 // The persistent form of launch_fused_step (LAUNCH_PERSISTENT).
-template <bool PF>
 static cudaError_t launch_fused_persistent(const DeviceState& st, const PhysParams& pp, const StepParams& sp,
                                            const SdfParams& sdf, int C, bool jacobi, int warps_per_block,
                                            cudaStream_t s, const StepParams* d_steps, int nsteps, int reg_cap,
@@ -328,8 +327,8 @@ static cudaError_t launch_fused_persistent(const DeviceState& st, const PhysPara
     if (units == 0) return cudaSuccess;
     const int threads = 32 * W;
 #define KAMI_PERSIST(KERNEL, CC)                                                                                 \
-    return jacobi ? launch_persistent(KERNEL<CC, true, PF>, units, threads, s, st, pp, sp, sdf, d_steps, nsteps) \
-                  : launch_persistent(KERNEL<CC, false, PF>, units, threads, s, st, pp, sp, sdf, d_steps, nsteps)
+    return jacobi ? launch_persistent(KERNEL<CC, true>, units, threads, s, st, pp, sp, sdf, d_steps, nsteps) \
+                  : launch_persistent(KERNEL<CC, false>, units, threads, s, st, pp, sp, sdf, d_steps, nsteps)
     if (group > 1) {
         if (group > 8 || st.num_tiles % group != 0) return cudaErrorInvalidValue;
         if (C == 2 && reg_cap == 120) KAMI_PERSIST(fused_persistent_group_kernel_r120, 2);
@@ -349,13 +348,8 @@ static cudaError_t launch_fused_persistent(const DeviceState& st, const PhysPara
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps,
                               int nsteps, int reg_cap, int group, int launch_mode) {
-    if ((launch_mode & LAUNCH_PERSISTENT) && !(reg_cap == 2 && C == 4 && !jacobi && group <= 1)) {
-        if (launch_mode & LAUNCH_SDF_PREFETCH)
-            return launch_fused_persistent<true>(st, pp, sp, sdf, C, jacobi, warps_per_block, s, d_steps, nsteps,
-                                                 reg_cap, group);
-        return launch_fused_persistent<false>(st, pp, sp, sdf, C, jacobi, warps_per_block, s, d_steps, nsteps, reg_cap,
-                                              group);
-    }
+    if ((launch_mode & LAUNCH_PERSISTENT) && !(reg_cap == 2 && C == 4 && !jacobi && group <= 1))
+        return launch_fused_persistent(st, pp, sp, sdf, C, jacobi, warps_per_block, s, d_steps, nsteps, reg_cap, group);
     if (group > 1) {
         if (group > 8 || st.num_tiles % group != 0) return cudaErrorInvalidValue;
         const unsigned gblocks = (unsigned)(st.num_tiles / group);

@@ -21,10 +21,9 @@ bool fused_supported(int C);
 // nsteps consecutive steps in one launch: parameters from d_steps[0..nsteps) (device), or sp when
 // d_steps is null (then nsteps must be 1).  group > 1: the layout's groups of `group` tiles, one CTA
 // of `group` warps each (warps_per_block and the packed variant do not apply).
-// launch_mode: 0 = one CTA per W tiles (or per group), scheduled by the hardware; bit 1 = persistent
-// (resident CTAs loop over the tiles, fused_persistent_kernel; the packed variant has no persistent
-// form); bit 2 = with the persistent form, prefetch each step's SDF cells into L2 an iteration early.
-enum : int { LAUNCH_PERSISTENT = 1, LAUNCH_SDF_PREFETCH = 2 };
+// launch_mode: 0 = one CTA per W tiles (or per group), scheduled by the hardware; LAUNCH_PERSISTENT =
+// resident CTAs loop over the tiles (fused_persistent_kernel; the packed variant has no persistent form).
+enum : int { LAUNCH_PERSISTENT = 1 };
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps = nullptr,
                               int nsteps = 1, int reg_cap = 0, int group = 1, int launch_mode = 0);

