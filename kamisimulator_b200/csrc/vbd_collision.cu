@@ -192,8 +192,12 @@ __global__ void __launch_bounds__(32 * kQueryWarps) coll_query_kernel(DeviceStat
         bool hit = false;
         int32_t j = -1, vb = 0;
         if (t < total) {
+            // the bucket of candidate t: the last c with s_pre[c] <= t (a binary search over the 27
+            // non-decreasing prefix sums; an empty bucket shares its start with the next one)
             int c = 0;
-            while (c < 26 && s_pre[w][c + 1] <= t) c++;
+#pragma unroll
+            for (int step = 16; step; step >>= 1)
+                if (c + step <= 26 && s_pre[w][c + step] <= t) c += step;
             const int32_t k = s_beg[w][c] + (t - s_pre[w][c]);
             const int4 rec = cp.srec[k];
             j = rec.x;
@@ -381,12 +385,12 @@ __device__ __forceinline__ void contact_term(const CollParams& cp, const Contact
 // Every contact of the segment starting at slot g, in list order (the order of the sums is that of
 // one contact at a time).  The next contact's operands are loaded before the current one is
 // evaluated, so each gather overlaps the arithmetic of the contact before it.
+// n: the segment's contact count; first: its first partner (cols[0][g]), read ahead by the caller.
 __device__ __forceinline__ void contact_terms(const DeviceState& st, const CollParams& cp, const float4* __restrict__ snap,
-                                              int64_t g, float3 x0, float3 x1, float3 d0, float3 d1, bool own,
-                                              float damp, float3& f, float H[6]) {
-    const int n = cp.ncols[g];
+                                              int64_t g, int n, int32_t first, float3 x0, float3 x1, float3 d0,
+                                              float3 d1, bool own, float damp, float3& f, float H[6]) {
     if (n <= 0) return;
-    ContactOperands cur = load_contact(st, cp, snap, cp.cols[g]);
+    ContactOperands cur = load_contact(st, cp, snap, first);
     for (int m = 0; m < n; m++) {
         ContactOperands nxt = cur;
         if (m + 1 < n) nxt = load_contact(st, cp, snap, cp.cols[(int64_t)(m + 1) * cp.num_slots + g]);
@@ -401,10 +405,23 @@ __device__ __forceinline__ void contact_terms(const DeviceState& st, const CollP
 // the current iterate: the next vertex (xj, dxj), this segment's orientation qg, the previous
 // vertex (xp, dp, its prm pp4) and its segment's orientation qgp; gn / gp are read only when the
 // flags say the neighbour exists.  Partners' dx come from `snap`.
+// The per-segment contact data (count, first partner, step limit) of the vertex's segment (g) and of
+// the previous one (gp) come from the caller, which can read them ahead of the sweep.
+struct SegContacts {
+    int n;
+    int32_t first;
+    float limit;
+};
+__device__ __forceinline__ SegContacts seg_contacts(const CollParams& cp, int64_t g) {
+    const int n = cp.ncols[g];
+    return SegContacts{n, n > 0 ? cp.cols[g] : 0, cp.maxstep[g]};
+}
+
 __device__ __forceinline__ float3 coll_position(const DeviceState& st, const CollParams& cp, const float4* snap,
                                                 int64_t g, int64_t gp, uint32_t fl, float4 xm, float4 prm, float3 vi_dx,
                                                 float3 yv, float3 xj, float3 vj_dx, float4 qg, float3 xp, float3 dp,
-                                                float4 qgp, float4 pp4, float h, const PhysParams& pp) {
+                                                float4 qgp, float4 pp4, SegContacts co, SegContacts cop, float h,
+                                                const PhysParams& pp) {
     const float damp = pp.damping / h;
     const float im = xm.w;
     const float3 vi = xyz(xm);
@@ -424,8 +441,8 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
         H[0] += dd;
         H[1] += dd;
         H[2] += dd;
-        step_limit = cp.maxstep[g];
-        contact_terms(st, cp, snap, g, vi, xj, vi_dx, vj_dx, true, damp, f, H);
+        step_limit = co.limit;
+        contact_terms(st, cp, snap, g, co.n, co.first, vi, xj, vi_dx, vj_dx, true, damp, f, H);
     }
     if (fl & F_HAS_PREV) {
         const float invl = 1.f / pp4.x;
@@ -435,8 +452,8 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
         float3 f2 = (-kk) * cc - (damp * dd) * vi_dx;
         dd *= 1.f + damp;
         float H2[6] = {dd, dd, dd, 0.f, 0.f, 0.f};
-        contact_terms(st, cp, snap, gp, xp, vi, dp, vi_dx, false, damp, f2, H2);
-        step_limit = fminf(step_limit, cp.maxstep[gp]);
+        contact_terms(st, cp, snap, gp, cop.n, cop.first, xp, vi, dp, vi_dx, false, damp, f2, H2);
+        step_limit = fminf(step_limit, cop.limit);
         f = f + f2;
 #pragma unroll
         for (int q = 0; q < 6; q++) H[q] += H2[q];
@@ -490,8 +507,10 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
         dp = xyz(dx_in[gp]);
         qgp = qcur[gp];
     }
+    const SegContacts co = (fl & F_HAS_NEXT) ? seg_contacts(cp, g) : SegContacts{0, 0, INFINITY};
+    const SegContacts cop = (fl & F_HAS_PREV) ? seg_contacts(cp, gp) : SegContacts{0, 0, INFINITY};
     const float3 out = coll_position(st, cp, snap, g, gp, fl, xm, prm, xyz(d4), xyz(y4[g]), xj, vj_dx,
-                                     (fl & F_HAS_NEXT) ? qcur[g] : unit, xp, dp, qgp, pp4, spp->h, pp);
+                                     (fl & F_HAS_NEXT) ? qcur[g] : unit, xp, dp, qgp, pp4, co, cop, spp->h, pp);
     dx_out[g] = make_float4(out.x, out.y, out.z, 0.f);
 }
 
@@ -502,42 +521,57 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
 // orientations in shared memory, separated by __syncthreads.  Partners (other tiles) read the
 // displacement the iteration started from in `snap`, which the launch does not write, so the launch
 // stands for the snapshot copy and the four sweep launches (same operands and arithmetic).
-// Displacements go to dx_out, orientations are updated in place.
+// Displacements go to dx_out, orientations are updated in place.  Everything a slot's updates read
+// that does not change in the launch (its parameters, rest Darboux, inertial target, contact count,
+// first partner and step limit) is read once at the start, so the sweeps' only global reads are the
+// partners' operands.
 __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, const float4* __restrict__ y4, float4* q,
                                                              const float4* __restrict__ snap,
                                                              float4* __restrict__ dx_out,
                                                              const StepParams* __restrict__ spp, PhysParams pp,
                                                              CollParams cp) {
-    extern __shared__ float4 coll_tile[];  // x | dx | q, T entries each
+    extern __shared__ float4 coll_tile[];  // x | dx | q | prm | qr, T entries each, then the contact data
     const int C = cp.C;
     const int T = 32 * C;
     float4* sx = coll_tile;
     float4* sdx = sx + T;
     float4* sq = sdx + T;
+    float4* sprm = sq + T;
+    float4* sqr = sprm + T;
+    SegContacts* sco = reinterpret_cast<SegContacts*>(sqr + T);
     const int lane = threadIdx.x & 31, row2 = (threadIdx.x >> 5) * 2;  // rows row2 (even) and row2 + 1 (odd)
     const int64_t base = (int64_t)blockIdx.x * T;
+    float3 yown[2];
 #pragma unroll
     for (int c = 0; c < 2; c++) {
         const int p = (row2 + c) * 32 + lane;  // storage offset in the tile
-        sx[p] = st.xm[base + p];
-        sdx[p] = snap[base + p];
-        sq[p] = q[base + p];
+        const int64_t g = base + p;
+        sx[p] = st.xm[g];
+        sdx[p] = snap[g];
+        sq[p] = q[g];
+        const float4 prm = st.prm[g];
+        sprm[p] = prm;
+        sqr[p] = st.qr[g];
+        sco[p] = (__float_as_uint(prm.w) & F_HAS_NEXT) ? seg_contacts(cp, g) : SegContacts{0, 0, INFINITY};
+        yown[c] = xyz(y4[g]);
     }
     const float h = spp->h;
     __syncthreads();
+#pragma unroll
     for (int c = 0; c < 2; c++) {
         const int p = (row2 + c) * 32 + lane;
         const int64_t g = base + p;
-        const float4 xm = sx[p], prm = st.prm[g];
+        const float4 xm = sx[p], prm = sprm[p];
         const uint32_t fl = __float_as_uint(prm.w);
         if ((fl & F_VALID) && xm.w != 0.f) {
             // in-tile neighbours (strands never cross tiles in the sweep form)
             const int pn = (fl & F_HAS_NEXT) ? (int)(next_slot(g, C) - base) : p;
             const int pq = (fl & F_HAS_PREV) ? (int)(prev_slot(g, C) - base) : p;
-            const float4 pp4 = (fl & F_HAS_PREV) ? st.prm[base + pq] : make_float4(1.f, 0.f, 0.f, 0.f);
-            const float3 out = coll_position(st, cp, snap, g, base + pq, fl, xm, prm, xyz(sdx[p]), xyz(y4[g]),
+            const float4 pp4 = (fl & F_HAS_PREV) ? sprm[pq] : make_float4(1.f, 0.f, 0.f, 0.f);
+            const SegContacts cop = (fl & F_HAS_PREV) ? sco[pq] : SegContacts{0, 0, INFINITY};
+            const float3 out = coll_position(st, cp, snap, g, base + pq, fl, xm, prm, xyz(sdx[p]), yown[c],
                                              xyz(sx[pn]), xyz(sdx[pn]), sq[p], xyz(sx[pq]), xyz(sdx[pq]), sq[pq], pp4,
-                                             h, pp);
+                                             sco[p], cop, h, pp);
             sdx[p] = make_float4(out.x, out.y, out.z, 0.f);
         }
         __syncthreads();
@@ -545,18 +579,18 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
     for (int c = 0; c < 2; c++) {
         const int p = (row2 + c) * 32 + lane;
         const int64_t g = base + p;
-        const float4 prm = st.prm[g];
+        const float4 prm = sprm[p];
         const uint32_t fl = __float_as_uint(prm.w);
         if ((fl & F_HAS_NEXT) && !(fl & F_FIX_ORIENTATION)) {
             const int pn = (int)(next_slot(g, C) - base);
             const int pq = (fl & F_HAS_PREV) ? (int)(prev_slot(g, C) - base) : p;
             const float4 unit = make_float4(0.f, 0.f, 0.f, 1.f);
             const float4 qp = (fl & F_HAS_PREV) ? sq[pq] : unit;
-            const float4 qrp = (fl & F_HAS_PREV) ? st.qr[base + pq] : unit;
+            const float4 qrp = (fl & F_HAS_PREV) ? sqr[pq] : unit;
             const float4 qn = (fl & F_HAS_NEXT_ORIENTATION) ? sq[pn] : unit;
             const float m2k = -2.f * prm.y * (1.f / prm.x);
             sq[p] = vbd_orientation(sq[p], fl, xyz(sx[pn]) - xyz(sx[p]), xyz(sdx[p]), xyz(sdx[pn]), m2k, qp, qrp, qn,
-                                    st.qr[g]);
+                                    sqr[p]);
         }
         __syncthreads();
     }
@@ -614,8 +648,12 @@ cudaError_t launch_coll_iteration(const DeviceState& st, const float4* y4, float
         return cudaErrorInvalidValue;
     if (st.num_tiles == 0) return cudaSuccess;
     const int T = 32 * cp.C;
-    coll_iteration_kernel<<<(unsigned)st.num_tiles, T / 2, sizeof(float4) * 3 * T, s>>>(st, y4, q, snap, dx_out, d_sp,
-                                                                                        pp, cp);
+    const size_t smem = (sizeof(float4) * 5 + sizeof(SegContacts)) * T;
+    if (smem > 48 * 1024) {  // the opt-in dynamic shared memory limit is set per device, so on every launch
+        cudaError_t e = cudaFuncSetAttribute(coll_iteration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    coll_iteration_kernel<<<(unsigned)st.num_tiles, T / 2, smem, s>>>(st, y4, q, snap, dx_out, d_sp, pp, cp);
     return cudaGetLastError();
 }
 
