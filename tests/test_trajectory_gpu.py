@@ -42,6 +42,7 @@ def test_cantilever_100_frames_against_the_fp32_and_fp64_oracles(form):
           f"GPU vs FP64 replay {worst64[0]:.2e} m / {worst64[1]:.2e} rad; tip height {o64.x[31, 2]:.3e} m")
     assert worst32[0] <= POS_TOL and worst32[1] <= TWIST_TOL, worst32
     # the rods bend under gravity (setYoung's millimetre units make them stiff: the tips sag 52 um),
-    # three orders of magnitude more than the error bound
-    assert float(-o64.x[31::32, 2].min()) > 100 * POS_TOL
+    # more than the position bar and a thousand times the error found
+    sag = float(-o64.x[31::32, 2].min())
+    assert sag > POS_TOL and sag > 1e3 * worst32[0]
     assert np.isfinite(worst64).all()
