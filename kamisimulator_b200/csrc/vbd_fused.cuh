@@ -591,7 +591,7 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
     }
 #pragma unroll
     for (int k = 0; k < C; k++) {
-        if (sdf.grid && (fl[k] & F_VALID) && !(fl[k] & F_ROOT)) vbd_sdf(x[k], v[k], sdf, sp);
+        if (sdf.grid) vbd_sdf_select(x[k], v[k], sdf, sp, (fl[k] & F_VALID) && !(fl[k] & F_ROOT));
         bad |= !finite3(x[k]) || !finite3(v[k]) || !finite4(q[k]);
     }
     }  // steps

@@ -435,21 +435,27 @@ def test_fit_gradient_at_the_initial_guess_matches_fp64_autograd():
     assert _rel(g_gpu, g_ref) <= GRAD_TOL, _rel(g_gpu, g_ref)
 
 
-def test_fit_gradient_over_60_frames_within_the_fp32_spread():
-    """The same at the fit's full 60 frames.  Over that horizon the gradient at the initial guess
-    depends on FP32 rounding: the FP32 run of the same autograd restatement lands tens of per cent
-    from the FP64 one (the strands the head touches carry most of the gradient, and the body pass's
-    branch and velocity fix make them rounding-sensitive).  The GPU gradient is held to 2x that FP32
-    spread (and to 1e-3 if the spread is smaller)."""
+def test_fit_gradient_over_60_frames_on_the_strands_fp32_resolves():
+    """The same at the fit's full 60 frames.  Over that horizon most of the gradient at the initial
+    guess depends on FP32 rounding: the FP32 run of the same autograd restatement lands about 90 %
+    (relative norm) from the FP64 one, because the strands the head touches carry most of the gradient
+    and the body pass's branch and velocity fix make them rounding-sensitive, while the untouched
+    strands' gradients are too small for FP32 to resolve.  The bar is therefore per strand: on every
+    strand where the FP32 restatement stays within 1e-4 of FP64 (a few dozen of the 200), the GPU
+    gradient is within 1e-3 of FP64; the rest is reported."""
     import torch
 
     g, st, scale0, c, g_gpu = _fit_gradient(60)
     _, g64, *_ = _torch_reference(g, st, None, scale0, 60, c, dt=1 / 120)
     _, g32, *_ = _torch_reference(g, st, None, scale0, 60, c, dt=1 / 120, dtype=torch.float32)
-    spread = _rel(g32, g64)
-    print(f"\nfit gradient, 200 strands x 48, 60 frames: GPU vs FP64 {_rel(g_gpu, g64):.2e}; FP32 restatement vs "
-          f"FP64 {spread:.2e}")
-    assert _rel(g_gpu, g64) <= max(GRAD_TOL, 2.0 * spread)
+    denom = np.maximum(np.abs(g64), 1e-300)
+    resolved = np.abs(g32 - g64) <= 1e-4 * denom
+    err = np.abs(g_gpu - g64) / denom
+    print(f"\nfit gradient, 200 strands x 48, 60 frames: {int(resolved.sum())} strands FP32 resolves (FP32 "
+          f"restatement within 1e-4), GPU worst there {err[resolved].max() if resolved.any() else 0.0:.2e}; "
+          f"relative norm over all strands: GPU {_rel(g_gpu, g64):.2e}, FP32 restatement {_rel(g32, g64):.2e}")
+    assert resolved.sum() >= 10
+    assert err[resolved].max() <= GRAD_TOL, np.sort(err[resolved])[-5:]
 
 
 def test_stiffness_fit_reduces_loss_on_the_2000_strand_workload():
