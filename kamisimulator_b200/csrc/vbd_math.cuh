@@ -173,60 +173,6 @@ __device__ __forceinline__ void vbd_sdf(float3& x, float3& v, const SdfParams& s
     }
 }
 
-// vbd_sdf without branches, for the fused kernels' epilogue: the same arithmetic on every slot, the
-// node indices clamped into the grid so that every corner load is in bounds, and the projection kept
-// only where vbd_sdf would apply it (active, inside the grid, phi < 0).  Where it applies, the result
-// is vbd_sdf's bit for bit.  With no branch between them, the corner loads of a lane's slots can be in
-// flight together.
-__device__ __forceinline__ void vbd_sdf_select(float3& x, float3& v, const SdfParams& sp, const StepParams& st,
-                                               bool active) {
-    float4 invq = make_float4(-st.rot_x, -st.rot_y, -st.rot_z, st.rot_w);
-    float3 lp = qrotate(invq, x - f3(st.tr_x, st.tr_y, st.tr_z)) - f3(sp.min_x, sp.min_y, sp.min_z);
-    int ix = (int)((double)(lp.x * sp.inv_x) + 0.5);
-    int iy = (int)((double)(lp.y * sp.inv_y) + 0.5);
-    int iz = (int)((double)(lp.z * sp.inv_z) + 0.5);
-    const bool inside = active && ix >= 0 && ix < sp.nx && iy >= 0 && iy < sp.ny && iz >= 0 && iz < sp.nz;
-    ix = min(max(ix, 0), sp.nx - 1);
-    iy = min(max(iy, 0), sp.ny - 1);
-    iz = min(max(iz, 0), sp.nz - 1);
-    const int jx = min(ix + 1, sp.nx - 1), jy = min(iy + 1, sp.ny - 1), jz = min(iz + 1, sp.nz - 1);
-    const bool ox = ix + 1 < sp.nx, oy = iy + 1 < sp.ny, oz = iz + 1 < sp.nz;
-    const int64_t sy = sp.nx, sz = (int64_t)sp.nx * sp.ny;
-    auto ld = [&](int cx, int cy, int cz, bool in) {
-        float4 c = __ldg(sp.grid + (cx + cy * sy + cz * sz));
-        if (!in) c.x = c.y = c.z = 0.f;
-        return c;
-    };
-    float4 c000 = ld(ix, iy, iz, true);
-    float4 c100 = ld(jx, iy, iz, ox);
-    float4 c010 = ld(ix, jy, iz, oy);
-    float4 c110 = ld(jx, jy, iz, ox && oy);
-    float4 c001 = ld(ix, iy, jz, oz);
-    float4 c101 = ld(jx, iy, jz, ox && oz);
-    float4 c011 = ld(ix, jy, jz, oy && oz);
-    float4 c111 = ld(jx, jy, jz, ox && oy && oz);
-    float ux = (float)((double)sp.inv_x * ((double)lp.x - ((double)ix - 0.5) * (double)sp.ds_x));
-    float uy = (float)((double)sp.inv_y * ((double)lp.y - ((double)iy - 0.5) * (double)sp.ds_y));
-    float uz = (float)((double)sp.inv_z * ((double)lp.z - ((double)iz - 0.5) * (double)sp.ds_z));
-    auto lerp4 = [](float4 a, float4 b, float t) {
-        return make_float4(a.x * (1.f - t) + b.x * t, a.y * (1.f - t) + b.y * t, a.z * (1.f - t) + b.z * t,
-                           a.w * (1.f - t) + b.w * t);
-    };
-    float4 c00 = lerp4(c000, c100, ux), c01 = lerp4(c001, c101, ux);
-    float4 c10 = lerp4(c010, c110, ux), c11 = lerp4(c011, c111, ux);
-    float4 c0 = lerp4(c00, c10, uy), c1 = lerp4(c01, c11, uy);
-    float4 r = lerp4(c0, c1, uz);
-    float3 n = f3(r.x, r.y, r.z) * rsqrtf(r.x * r.x + r.y * r.y + r.z * r.z);
-    float phi = r.w - sp.thresh;
-    const bool hit = inside && phi < 0.f;
-    const float3 xn = x - phi * n;
-    const float vl = sqrtf(dot3(v, v));
-    const float3 vn = v * (1.f / vl);
-    const float3 vfix = v - dot3(vn, n) * n;
-    v = (hit && vl >= 1e-6f) ? vfix : v;
-    x = hit ? xn : x;
-}
-
 __device__ __forceinline__ bool finite3(float3 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z); }
 __device__ __forceinline__ bool finite4(float4 a) { return isfinite(a.x) && isfinite(a.y) && isfinite(a.z) && isfinite(a.w); }
 
