@@ -349,11 +349,10 @@ kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int3
 
 /* How the fused step's launches are scheduled (no counterpart in the reference).  0: one CTA per
  * warps_per_block tiles (or per group of tiles), placed on the SMs by the hardware.
- * KAMI_LAUNCH_L2_PREFETCH: the same grid, each warp first asking L2 (bulk prefetch) for the state of
- * the tile that takes its place one wave later; same results.  KAMI_LAUNCH_PERSISTENT: at most as many
- * CTAs as stay resident at once, each looping over every gridDim-th unit of tiles; the results agree to
- * the last bits (the kernels are compiled apart). */
-enum { KAMI_LAUNCH_PERSISTENT = 1, KAMI_LAUNCH_L2_PREFETCH = 2 };
+ * KAMI_LAUNCH_PERSISTENT: at most as many CTAs as stay resident at once, each looping over every
+ * gridDim-th unit of tiles; the results agree to the last bits (the kernels are compiled apart).
+ * The autotuner times both and keeps the faster. */
+enum { KAMI_LAUNCH_PERSISTENT = 1 };
 kami_status kami_vbd_set_launch_mode(kami_vbd_handle h, int32_t mode);
 kami_status kami_vbd_get_launch_mode(kami_vbd_handle h, int32_t* mode);
 

@@ -1209,13 +1209,12 @@ kami_status kami_vbd_get_tuning(kami_vbd_handle h, int32_t* slots_per_lane, int3
     return KAMI_OK;
 }
 
-static_assert(KAMI_LAUNCH_PERSISTENT == LAUNCH_PERSISTENT && KAMI_LAUNCH_L2_PREFETCH == LAUNCH_L2_PREFETCH,
-              "the C ABI's launch modes are the launcher's");
+static_assert(KAMI_LAUNCH_PERSISTENT == LAUNCH_PERSISTENT, "the C ABI's launch mode is the launcher's");
 
 kami_status kami_vbd_set_launch_mode(kami_vbd_handle h, int32_t mode) {
     KAMI_TRY(valid_handle(h));
-    if (mode != 0 && mode != KAMI_LAUNCH_PERSISTENT && mode != KAMI_LAUNCH_L2_PREFETCH)
-        return fail(KAMI_ERR_INVALID_ARGUMENT, "the launch mode is 0, KAMI_LAUNCH_PERSISTENT or KAMI_LAUNCH_L2_PREFETCH");
+    if (mode != 0 && mode != KAMI_LAUNCH_PERSISTENT)
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "the launch mode is 0 or KAMI_LAUNCH_PERSISTENT");
     if (mode != h->launch_mode) drop_graphs(h);
     h->launch_mode = mode;
     return KAMI_OK;
@@ -1345,8 +1344,8 @@ kami_status kami_vbd_autotune(kami_vbd_handle h, float dt, int32_t trial_steps, 
     if (st == KAMI_OK) st = kami_vbd_set_tuning(h, pick[0], pick[1], pick[2], pick[3]);
     // the launch modes on the fastest shape (the packed variant has no persistent form)
     int mode_best = 0;
-    const int modes[3] = {0, KAMI_LAUNCH_L2_PREFETCH, KAMI_LAUNCH_PERSISTENT};
-    for (int mi = 0; mi < (pick[3] == 2 ? 2 : 3) && st == KAMI_OK; mi++) {
+    const int modes[2] = {0, KAMI_LAUNCH_PERSISTENT};
+    for (int mi = 0; mi < (pick[3] == 2 ? 1 : 2) && st == KAMI_OK; mi++) {
         st = kami_vbd_set_launch_mode(h, modes[mi]);
         if (st == KAMI_OK) st = kami_vbd_set_state(h, snap, bytes, KAMI_MEMORY_DEVICE);
         if (st == KAMI_OK) st = kami_vbd_step_n(h, dt, trial_steps, nullptr, nullptr);

@@ -75,9 +75,6 @@ struct DeviceState {
     const float4* prm; // lRest, kStretch, 0, flags (bit pattern)
     int64_t num_tiles;
     int* status;
-    // fused grid kernels: the warp stepping tile t asks L2 for the state of tile t + prefetch_tiles, the
-    // tile that takes a warp's place a wave later (0: no prefetch)
-    int64_t prefetch_tiles = 0;
 };
 
 // Iterates of recorded steps for the adjoint: for step s, iteration it (0 = after the predict) and

@@ -259,18 +259,6 @@ __device__ __forceinline__ void fused_step_body(DeviceState st, PhysParams pp, S
                              : (RECORD ? tp.tile_begin : 0) + (int64_t)blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (tile >= st.num_tiles) return;  // uniform per warp (per CTA for groups: num_tiles is a multiple of K)
     const int64_t base = tile * (32LL * C) + lane;
-    if (!HOSTIO && !RECORD && !EXPLICIT_TILE && st.prefetch_tiles > 0 && lane == 0) {
-        // the next wave's tile in this warp's place: its six state rows into L2 (bulk prefetch, a hint)
-        const int64_t nt = tile + st.prefetch_tiles;
-        if (nt < st.num_tiles) {
-            const int64_t o = nt * (32LL * C);
-            const unsigned bytes = 32u * C * sizeof(float4);
-            const float4* rows[6] = {st.xm + o, st.vel + o, st.vlast + o, st.q + o, st.qr + o, st.prm + o};
-#pragma unroll
-            for (int a = 0; a < 6; a++)
-                asm volatile("cp.async.bulk.prefetch.L2.global [%0], %1;" ::"l"(rows[a]), "r"(bytes) : "memory");
-        }
-    }
     // tile groups: neighbours across the warps of the CTA (see GroupExchange)
     const int gw = threadIdx.x >> 5, gK = blockDim.x >> 5;
     GroupExchange* gx = nullptr;

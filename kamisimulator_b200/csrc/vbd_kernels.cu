@@ -345,40 +345,11 @@ static cudaError_t launch_fused_persistent(const DeviceState& st, const PhysPara
     return cudaErrorInvalidValue;
 }
 
-// The grid kernel launch_fused_step runs for this shape (for the occupancy query).
-static const void* fused_kernel_for(int C, bool jacobi, int reg_cap, int group) {
-    if (group > 1) {
-        if (C == 2 && reg_cap == 120) return jacobi ? (const void*)fused_group_kernel_r120<2, true> : (const void*)fused_group_kernel_r120<2, false>;
-        if (C == 4 && reg_cap == 168) return jacobi ? (const void*)fused_group_kernel_r168<4, true> : (const void*)fused_group_kernel_r168<4, false>;
-        if (C == 2) return jacobi ? (const void*)fused_group_kernel<2, true> : (const void*)fused_group_kernel<2, false>;
-        if (C == 4) return jacobi ? (const void*)fused_group_kernel<4, true> : (const void*)fused_group_kernel<4, false>;
-        return nullptr;
-    }
-    if (reg_cap == 2 && C == 4 && !jacobi) return (const void*)fused_step_kernel_x2<4>;
-    if (reg_cap == 168 && C == 4) return jacobi ? (const void*)fused_step_kernel_r168<4, true> : (const void*)fused_step_kernel_r168<4, false>;
-    if (reg_cap == 120 && C == 2) return jacobi ? (const void*)fused_step_kernel_r120<2, true> : (const void*)fused_step_kernel_r120<2, false>;
-    if (C == 2) return jacobi ? (const void*)fused_step_kernel<2, true, false> : (const void*)fused_step_kernel<2, false, false>;
-    if (C == 4) return jacobi ? (const void*)fused_step_kernel<4, true, false> : (const void*)fused_step_kernel<4, false, false>;
-    return nullptr;
-}
-
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps,
                               int nsteps, int reg_cap, int group, int launch_mode) {
     if ((launch_mode & LAUNCH_PERSISTENT) && !(reg_cap == 2 && C == 4 && !jacobi && group <= 1))
         return launch_fused_persistent(st, pp, sp, sdf, C, jacobi, warps_per_block, s, d_steps, nsteps, reg_cap, group);
-    if (launch_mode & LAUNCH_L2_PREFETCH) {
-        // one wave ahead: the tiles the resident warps cover (the resident CTA count of the kernel the
-        // launch below picks, as the occupancy API gives it, times its warps)
-        DeviceState pst = st;
-        const int W = group > 1 ? group : warps_per_block;
-        const void* k = fused_kernel_for(C, jacobi, reg_cap, group);
-        int64_t resident = 0;
-        cudaError_t e = k ? resident_ctas(k, 32 * W, &resident) : cudaErrorInvalidValue;
-        if (e != cudaSuccess) return e;
-        pst.prefetch_tiles = resident * W;
-        return launch_fused_step(pst, pp, sp, sdf, C, jacobi, warps_per_block, s, d_steps, nsteps, reg_cap, group, 0);
-    }
     if (group > 1) {
         if (group > 8 || st.num_tiles % group != 0) return cudaErrorInvalidValue;
         const unsigned gblocks = (unsigned)(st.num_tiles / group);

@@ -22,9 +22,8 @@ bool fused_supported(int C);
 // d_steps is null (then nsteps must be 1).  group > 1: the layout's groups of `group` tiles, one CTA
 // of `group` warps each (warps_per_block and the packed variant do not apply).
 // launch_mode: 0 = one CTA per W tiles (or per group), scheduled by the hardware; LAUNCH_PERSISTENT =
-// resident CTAs loop over the tiles (fused_persistent_kernel; the packed variant has no persistent form);
-// LAUNCH_L2_PREFETCH (grid only) = each warp prefetches into L2 the state of the tile one wave ahead.
-enum : int { LAUNCH_PERSISTENT = 1, LAUNCH_L2_PREFETCH = 2 };
+// resident CTAs loop over the tiles (fused_persistent_kernel; the packed variant has no persistent form).
+enum : int { LAUNCH_PERSISTENT = 1 };
 cudaError_t launch_fused_step(const DeviceState& st, const PhysParams& pp, const StepParams& sp, const SdfParams& sdf,
                               int C, bool jacobi, int warps_per_block, cudaStream_t s, const StepParams* d_steps = nullptr,
                               int nsteps = 1, int reg_cap = 0, int group = 1, int launch_mode = 0);

@@ -395,8 +395,7 @@ class Solver:
         return c.value, w.value, f.value, r.value
 
     def set_launch_mode(self, mode):
-        """kami_vbd_set_launch_mode: 0 (hardware-scheduled tile grid), 1 (persistent resident CTAs) or 2 (the
-        grid, each warp prefetching into L2 the tile one wave ahead)."""
+        """kami_vbd_set_launch_mode: 0 (hardware-scheduled tile grid) or 1 (persistent resident CTAs)."""
         _check(self.lib.kami_vbd_set_launch_mode(self._h, int(mode)))
 
     def get_launch_mode(self):
