@@ -652,8 +652,8 @@ def adjoint_fit(torch, iterations=150, frames=60, k=10, lr=0.1, lr_end=0.005):
     with torch.no_grad():
         x2 = rollout_positions(torch.full((g.num_strands,), 2.0, device="cuda"), solver, unit, strand_of, init,
                                frames, DT, k)
-    moved = torch.zeros(g.num_strands, device="cuda").index_reduce_(
-        0, strand_of, (x2 - target).norm(dim=1), "amax", include_self=False).cpu().numpy()
+    moved = np.zeros(g.num_strands)
+    np.maximum.at(moved, strand_of.cpu().numpy(), (x2 - target).norm(dim=1).cpu().numpy())
     ident = moved > 1e-3
     solver.close()
     return {"strands": g.num_strands, "verts_per_strand": 48, "frames": frames, "checkpoint_every": k,
@@ -774,6 +774,7 @@ def run_ours(args):
         tuned = solver.get_tuning()
     else:
         tuned, _ = solver.autotune(DT, trial_steps=8)  # the library's autotuner; restores the state
+    launch_mode = solver.get_launch_mode()  # 0: hardware-scheduled tile grid, 1: persistent
     stream = torch.cuda.current_stream()
     flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):
@@ -862,7 +863,8 @@ def run_ours(args):
                 "vs_baseline": None, "dtype": "f32", "data": "synthetic",
                 "config": config_dict({"form": "fused", "per_gpu": "one 10,000 x 64 groom per GPU",
                                        "tuning": dict(zip(("slots_per_lane", "warps_per_block", "steps_per_launch",
-                                                           "register_cap"), tuned))}),
+                                                           "register_cap"), tuned)),
+                                       "launch_mode": launch_mode}),
                 "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s",
                              "frac": achieved / peak, "traffic": traffic, "kernel": "fused_step_kernel (colour2, one step per launch)",
                              "bytes_per_launch": V * BYTES_PER_VERTEX_STEP, "peak_source": peak_kind},
