@@ -33,7 +33,7 @@ import torch
 _rollout_ids = itertools.count(1)
 
 
-def _segments_recorded_in_forward(solver, frames, dt, k, tiles_per_chunk, budget):
+def _segments_recorded_in_forward(solver, frames, dt, k, tiles_per_chunk, budget, device):
     """Number of trailing segments whose tape fits the budget (0 with tile windows)."""
     tiles = solver.tile_count()
     if 0 < tiles_per_chunk < tiles:
@@ -41,7 +41,7 @@ def _segments_recorded_in_forward(solver, frames, dt, k, tiles_per_chunk, budget
     nseg = -(-frames // k)
     per_seg = solver.tape_bytes_per_substep() * solver.substeps(dt) * k
     if budget is None:
-        budget = torch.cuda.mem_get_info()[0] // 4
+        budget = torch.cuda.mem_get_info(device)[0] // 4
     return int(min(nseg, budget // per_seg)) if per_seg > 0 else 0
 
 
@@ -53,7 +53,8 @@ class StrandStiffnessRollout(torch.autograd.Function):
         init_state: flat CUDA float32 state (Solver.get_state_into layout).  Returns (V, 3) positions."""
         k = max(1, int(checkpoint_every))
         nseg = -(-frames // k)
-        m = _segments_recorded_in_forward(solver, frames, dt, k, int(tiles_per_chunk), tape_budget_bytes)
+        m = _segments_recorded_in_forward(solver, frames, dt, k, int(tiles_per_chunk), tape_budget_bytes,
+                                          init_state.device)
         first_recorded = nseg - m  # segments >= this one are recorded in the forward pass
         qr = (unit * scale[strand_of][:, None]).contiguous()
         torch.cuda.synchronize()
@@ -93,7 +94,7 @@ class StrandStiffnessRollout(torch.autograd.Function):
         avl = torch.zeros_like(av)
         aq = torch.zeros((nv, 4), dtype=torch.float32, device=dev)
         nseg = len(ctx.ckpts)
-        m = ctx.recorded if getattr(solver, "_tape_rollout", None) == ctx.rid else 0
+        m = ctx.recorded if solver._tape_rollout == ctx.rid else 0
         solver._tape_rollout = None  # this pass consumes the tape or reallocates it
         # the rest Darboux of this rollout (another rollout on the solver may have set its own since)
         solver.set_rest_darboux((unit * scale[strand_of][:, None]).contiguous())

@@ -222,6 +222,7 @@ class Solver:
         stepping all of them; velocities is then None or a list with one entry per groom)."""
         self.lib = load_library()
         self._h = None
+        self._tape_rollout = None  # the autograd rollout whose steps the tape holds (autograd.py)
         grooms = list(groom) if isinstance(groom, (list, tuple)) else [groom]
         if velocities is None or not isinstance(groom, (list, tuple)):
             velocities = [velocities] * len(grooms)
