@@ -106,6 +106,14 @@ def test_null_handle_calls_fail_cleanly():
     assert lib.kami_vbd_destroy(None) == 0
     n = ctypes.c_size_t()
     assert lib.kami_vbd_state_size(None, ctypes.byref(n)) == 1
+    assert lib.kami_vbd_set_launch_mode(None, 0) == 1
+    m = ctypes.c_int32()
+    assert lib.kami_vbd_get_launch_mode(None, ctypes.byref(m)) == 1
+    assert lib.kami_vbd_step_hair(None, ctypes.c_float(0.01), None, None, None, None) == 1
+    # host registration checks its arguments before any CUDA call
+    assert lib.kami_host_register(None, 64) == 1
+    assert lib.kami_host_register(ctypes.c_void_p(4096), 0) == 1
+    assert lib.kami_host_unregister(None) == 1
 
 
 def test_batch_rejects_grooms_with_different_solver_settings():

@@ -257,3 +257,28 @@ def test_fp32_peak_probe():
     fma, fma2 = bench.fp32_probe(0)
     assert 30.0 < fma < 150.0, fma
     assert 30.0 < fma2 < 300.0, fma2
+
+
+def test_stepping_calls_check_dt():
+    """Every stepping entry point rejects a dt that is not finite or that needs more than
+    KAMI_MAX_SUBSTEPS (10^6) substeps of max_h, before it converts the substep count to an integer;
+    dt <= 0 is a no-op for kami_vbd_step (Sim::advance returns for h <= 0)."""
+    from kamisimulator_b200.vbd import KamiError
+
+    g = synth.cantilever(4, 8)
+    st = dict(num_itr=4, max_h=1e-9, gravity=(0.0, 0.0, -9.81), radius=40e-6)
+    s = helpers.gpu_solver(g, st, form="fused")
+    x0, _ = s.get_positions_velocities()
+    s.set_hair_layout(g.num_strands, 8)
+    hx = np.zeros((g.num_strands, 8, 3), np.float32)
+    for dt in (float("nan"), float("inf"), 1.0):  # 1 s / 1 ns is 10^9 substeps
+        for call in (lambda: s.step(dt), lambda: s.step_n(dt, 2), lambda: s.step_host(dt, x0.copy(), x0.copy()),
+                     lambda: s.step_hair(dt, hx, hx, hx, hx)):
+            with pytest.raises(KamiError, match="INVALID_ARGUMENT"):
+                call()
+    s.step(-1.0)
+    s.step(0.0)
+    np.testing.assert_array_equal(s.get_positions_velocities()[0], x0)
+    with pytest.raises(KamiError, match="INVALID_ARGUMENT"):
+        s.set_launch_mode(7)
+    s.close()
