@@ -385,13 +385,32 @@ __device__ __forceinline__ void contact_term(const CollParams& cp, const Contact
 // Every contact of the segment starting at slot g, in list order (the order of the sums is that of
 // one contact at a time).  The next contact's operands are loaded before the current one is
 // evaluated, so each gather overlaps the arithmetic of the contact before it.
-// n: the segment's contact count; first: its first partner (cols[0][g]), read ahead by the caller.
+// The per-segment contact data (count, first partner, step limit) of the vertex's segment (g) and of
+// the previous one (gp) come from the caller, which can read them ahead of the sweep.
+struct SegContacts {
+    int n;
+    int32_t first;
+    float limit;
+    int cached;                  // how many of the n partners' operands `part` holds (the first ones)
+    const ContactOperands* part;  // shared memory (coll_iteration_kernel), or null
+};
+__device__ __forceinline__ SegContacts seg_contacts(const CollParams& cp, int64_t g) {
+    const int n = cp.ncols[g];
+    return SegContacts{n, n > 0 ? cp.cols[g] : 0, cp.maxstep[g], 0, nullptr};
+}
+__device__ __forceinline__ SegContacts no_contacts() { return SegContacts{0, 0, INFINITY, 0, nullptr}; }
+
+// The segment's contacts (count, first partner read ahead by the caller); the first `cached` of
+// them have their partner operands in shared memory already.
 __device__ __forceinline__ void contact_terms(const DeviceState& st, const CollParams& cp, const float4* __restrict__ snap,
-                                              int64_t g, int n, int32_t first, float3 x0, float3 x1, float3 d0,
+                                              int64_t g, const SegContacts& co, float3 x0, float3 x1, float3 d0,
                                               float3 d1, bool own, float damp, float3& f, float H[6]) {
-    if (n <= 0) return;
-    ContactOperands cur = load_contact(st, cp, snap, first);
-    for (int m = 0; m < n; m++) {
+    const int n = co.n;
+    for (int m = 0; m < co.cached; m++) contact_term(cp, co.part[m], x0, x1, d0, d1, own, damp, f, H);
+    if (co.cached >= n) return;
+    ContactOperands cur = load_contact(st, cp, snap, co.cached == 0 ? co.first
+                                                                     : cp.cols[(int64_t)co.cached * cp.num_slots + g]);
+    for (int m = co.cached; m < n; m++) {
         ContactOperands nxt = cur;
         if (m + 1 < n) nxt = load_contact(st, cp, snap, cp.cols[(int64_t)(m + 1) * cp.num_slots + g]);
         contact_term(cp, cur, x0, x1, d0, d1, own, damp, f, H);
@@ -405,18 +424,6 @@ __device__ __forceinline__ void contact_terms(const DeviceState& st, const CollP
 // the current iterate: the next vertex (xj, dxj), this segment's orientation qg, the previous
 // vertex (xp, dp, its prm pp4) and its segment's orientation qgp; gn / gp are read only when the
 // flags say the neighbour exists.  Partners' dx come from `snap`.
-// The per-segment contact data (count, first partner, step limit) of the vertex's segment (g) and of
-// the previous one (gp) come from the caller, which can read them ahead of the sweep.
-struct SegContacts {
-    int n;
-    int32_t first;
-    float limit;
-};
-__device__ __forceinline__ SegContacts seg_contacts(const CollParams& cp, int64_t g) {
-    const int n = cp.ncols[g];
-    return SegContacts{n, n > 0 ? cp.cols[g] : 0, cp.maxstep[g]};
-}
-
 __device__ __forceinline__ float3 coll_position(const DeviceState& st, const CollParams& cp, const float4* snap,
                                                 int64_t g, int64_t gp, uint32_t fl, float4 xm, float4 prm, float3 vi_dx,
                                                 float3 yv, float3 xj, float3 vj_dx, float4 qg, float3 xp, float3 dp,
@@ -442,7 +449,7 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
         H[1] += dd;
         H[2] += dd;
         step_limit = co.limit;
-        contact_terms(st, cp, snap, g, co.n, co.first, vi, xj, vi_dx, vj_dx, true, damp, f, H);
+        contact_terms(st, cp, snap, g, co, vi, xj, vi_dx, vj_dx, true, damp, f, H);
     }
     if (fl & F_HAS_PREV) {
         const float invl = 1.f / pp4.x;
@@ -452,7 +459,7 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
         float3 f2 = (-kk) * cc - (damp * dd) * vi_dx;
         dd *= 1.f + damp;
         float H2[6] = {dd, dd, dd, 0.f, 0.f, 0.f};
-        contact_terms(st, cp, snap, gp, cop.n, cop.first, xp, vi, dp, vi_dx, false, damp, f2, H2);
+        contact_terms(st, cp, snap, gp, cop, xp, vi, dp, vi_dx, false, damp, f2, H2);
         step_limit = fminf(step_limit, cop.limit);
         f = f + f2;
 #pragma unroll
@@ -507,11 +514,21 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
         dp = xyz(dx_in[gp]);
         qgp = qcur[gp];
     }
-    const SegContacts co = (fl & F_HAS_NEXT) ? seg_contacts(cp, g) : SegContacts{0, 0, INFINITY};
-    const SegContacts cop = (fl & F_HAS_PREV) ? seg_contacts(cp, gp) : SegContacts{0, 0, INFINITY};
+    const SegContacts co = (fl & F_HAS_NEXT) ? seg_contacts(cp, g) : no_contacts();
+    const SegContacts cop = (fl & F_HAS_PREV) ? seg_contacts(cp, gp) : no_contacts();
     const float3 out = coll_position(st, cp, snap, g, gp, fl, xm, prm, xyz(d4), xyz(y4[g]), xj, vj_dx,
                                      (fl & F_HAS_NEXT) ? qcur[g] : unit, xp, dp, qgp, pp4, co, cop, spp->h, pp);
     dx_out[g] = make_float4(out.x, out.y, out.z, 0.f);
+}
+
+// Contacts whose partner operands coll_iteration_kernel holds in shared memory, per tile of T slots
+// (2.5 per slot: at T = 64 the block's shared memory stays under 15 KB, so 14 blocks fit on an SM and
+// the 2,000 tiles of a 2,000-strand groom run in one wave; one per slot at T = 1024, which keeps the
+// block under the 227 KB limit).
+__host__ __device__ constexpr int coll_contact_cap(int T) { return T <= 512 ? T * 5 / 2 : T; }
+__host__ __device__ constexpr size_t coll_iteration_smem(int T) {
+    return (sizeof(float4) * 5 + sizeof(SegContacts)) * T + (sizeof(ContactOperands) + sizeof(int32_t)) * coll_contact_cap(T) +
+           sizeof(int32_t) * (T / 64);
 }
 
 // One colour2 iteration of the sweep form with contacts, one tile per block (T = 32 C slots, T <= 1024)
@@ -523,8 +540,14 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
 // stands for the snapshot copy and the four sweep launches (same operands and arithmetic).
 // Displacements go to dx_out, orientations are updated in place.  Everything a slot's updates read
 // that does not change in the launch (its parameters, rest Darboux, inertial target, contact count,
-// first partner and step limit) is read once at the start, so the sweeps' only global reads are the
-// partners' operands.
+// first partner and step limit) is read once at the start.  So are the partners' operands (the
+// partner segments' end points and their `snap` displacements, neither written in the launch): the
+// tile's contact lists are laid end to end in shared memory, first their partner indices, then the
+// operands gathered cooperatively (every thread a share of the tile's contacts, all loads
+// independent), up to coll_contact_cap(T) contacts per tile; a slot's contacts past the cap are read
+// from global memory in the sweep as before.  Each segment's list serves two vertices (its first as
+// `own`, its second as the previous segment), so the gather halves the partner reads and takes them
+// out of the sweeps' dependency chains.  The operands and the order of the sums are unchanged.
 __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, const float4* __restrict__ y4, float4* q,
                                                              const float4* __restrict__ snap,
                                                              float4* __restrict__ dx_out,
@@ -539,9 +562,14 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
     float4* sprm = sq + T;
     float4* sqr = sprm + T;
     SegContacts* sco = reinterpret_cast<SegContacts*>(sqr + T);
+    const int ncap = coll_contact_cap(T);
+    ContactOperands* spart = reinterpret_cast<ContactOperands*>(sco + T);
+    int32_t* spidx = reinterpret_cast<int32_t*>(spart + ncap);  // the partners' slots, then the warps' totals
+    int32_t* swarp = spidx + ncap;
     const int lane = threadIdx.x & 31, row2 = (threadIdx.x >> 5) * 2;  // rows row2 (even) and row2 + 1 (odd)
     const int64_t base = (int64_t)blockIdx.x * T;
     float3 yown[2];
+    SegContacts own[2];
 #pragma unroll
     for (int c = 0; c < 2; c++) {
         const int p = (row2 + c) * 32 + lane;  // storage offset in the tile
@@ -552,9 +580,39 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
         const float4 prm = st.prm[g];
         sprm[p] = prm;
         sqr[p] = st.qr[g];
-        sco[p] = (__float_as_uint(prm.w) & F_HAS_NEXT) ? seg_contacts(cp, g) : SegContacts{0, 0, INFINITY};
+        own[c] = (__float_as_uint(prm.w) & F_HAS_NEXT) ? seg_contacts(cp, g) : no_contacts();
         yown[c] = xyz(y4[g]);
     }
+    // the tile's contact lists end to end, in thread order (thread t: its even slot's list, then its
+    // odd slot's): an exclusive scan of the threads' contact counts, within each warp by shuffles and
+    // across the warps through swarp
+    const int cnt = own[0].n + own[1].n;
+    int incl = cnt;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        const int v = __shfl_up_sync(0xffffffffu, incl, d);
+        if (lane >= d) incl += v;
+    }
+    const int warp = threadIdx.x >> 5;
+    if (lane == 31) swarp[warp] = incl;
+    __syncthreads();
+    int first_off = incl - cnt;
+    for (int k = 0; k < warp; k++) first_off += swarp[k];
+    int total = 0;
+    for (int k = 0; k < (int)(blockDim.x >> 5); k++) total += swarp[k];
+    total = min(total, ncap);
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const int p = (row2 + c) * 32 + lane;
+        const int off = first_off + (c ? own[0].n : 0);
+        const int cached = max(0, min(own[c].n, ncap - off));
+        for (int m = 0; m < cached; m++) spidx[off + m] = cp.cols[(int64_t)m * cp.num_slots + base + p];
+        own[c].cached = cached;
+        own[c].part = spart + min(off, ncap);
+        sco[p] = own[c];
+    }
+    __syncthreads();
+    for (int k = threadIdx.x; k < total; k += blockDim.x) spart[k] = load_contact(st, cp, snap, spidx[k]);
     const float h = spp->h;
     __syncthreads();
 #pragma unroll
@@ -568,7 +626,7 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
             const int pn = (fl & F_HAS_NEXT) ? (int)(next_slot(g, C) - base) : p;
             const int pq = (fl & F_HAS_PREV) ? (int)(prev_slot(g, C) - base) : p;
             const float4 pp4 = (fl & F_HAS_PREV) ? sprm[pq] : make_float4(1.f, 0.f, 0.f, 0.f);
-            const SegContacts cop = (fl & F_HAS_PREV) ? sco[pq] : SegContacts{0, 0, INFINITY};
+            const SegContacts cop = (fl & F_HAS_PREV) ? sco[pq] : no_contacts();
             const float3 out = coll_position(st, cp, snap, g, base + pq, fl, xm, prm, xyz(sdx[p]), yown[c],
                                              xyz(sx[pn]), xyz(sdx[pn]), sq[p], xyz(sx[pq]), xyz(sdx[pq]), sq[pq], pp4,
                                              sco[p], cop, h, pp);
@@ -648,7 +706,7 @@ cudaError_t launch_coll_iteration(const DeviceState& st, const float4* y4, float
         return cudaErrorInvalidValue;
     if (st.num_tiles == 0) return cudaSuccess;
     const int T = 32 * cp.C;
-    const size_t smem = (sizeof(float4) * 5 + sizeof(SegContacts)) * T;
+    const size_t smem = coll_iteration_smem(T);
     if (smem > 48 * 1024) {  // the opt-in dynamic shared memory limit is set per device, so on every launch
         cudaError_t e = cudaFuncSetAttribute(coll_iteration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
