@@ -484,9 +484,10 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
     if (t >= num_threads) return;
     const int C = cp.C;
     const int rows = JACOBI ? C : C / 2;
-    const int64_t tile = t / (32LL * rows);
-    const int rem = (int)(t - tile * 32LL * rows);
-    const int r = rem >> 5, lane = rem & 31;
+    // thread t: tile t / 32 rows, row r, lane t mod 32 (a 32-bit division: t / 32 < 2^32)
+    const uint32_t trow = (uint32_t)((uint64_t)t >> 5);
+    const int64_t tile = trow / (uint32_t)rows;
+    const int r = (int)(trow - (uint32_t)tile * (uint32_t)rows), lane = (int)(t & 31);
     const int k = JACOBI ? r : 2 * r + colour;
     const int64_t g = tile * 32LL * C + (int64_t)k * 32 + lane;
     const float4 prm = st.prm[g];

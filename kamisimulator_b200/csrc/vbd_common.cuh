@@ -156,21 +156,24 @@ struct CollParams {
 // ---- tile slot neighbours ----------------------------------------------------------------------
 // Storage index of slot p+1 / p-1 of the strand slot stored at g (the caller knows it exists).  In
 // a group of tiles a strand runs on from lane 31's last slot of a tile into lane 0's first slot of
-// the next tile.
+// the next tile.  Slot g sits in row (g / 32) mod C of its tile, at lane g mod 32; the row index
+// needs only a 32-bit remainder (g / 32 < 2^32 for any slot count a device can hold), a mask when C
+// is a power of two, instead of a 64-bit division by the tile size.
+__host__ __device__ __forceinline__ int tile_row(int64_t g, int C) {
+    const uint32_t row = (uint32_t)((uint64_t)g >> 5);
+    return (int)((C & (C - 1)) == 0 ? row & (uint32_t)(C - 1) : row % (uint32_t)C);
+}
 __host__ __device__ __forceinline__ int64_t next_slot(int64_t g, int C) {
-    const int64_t T = 32LL * C;
-    const int64_t tile = g / T;
-    const int r = (int)(g - tile * T);
-    const int k = r >> 5, lane = r & 31;
-    return (k < C - 1) ? g + 32 : (lane < 31 ? tile * T + lane + 1 : (tile + 1) * T);
+    const int k = tile_row(g, C), lane = (int)(g & 31);
+    if (k < C - 1) return g + 32;
+    const int64_t tile_base = g - lane - 32LL * k;
+    return lane < 31 ? tile_base + lane + 1 : tile_base + 32LL * C;
 }
 __host__ __device__ __forceinline__ int64_t prev_slot(int64_t g, int C) {
-    const int64_t T = 32LL * C;
-    const int64_t tile = g / T;
-    const int r = (int)(g - tile * T);
-    const int k = r >> 5, lane = r & 31;
-    return (k > 0) ? g - 32
-                   : (lane > 0 ? tile * T + (int64_t)(C - 1) * 32 + lane - 1 : (tile - 1) * T + (int64_t)(C - 1) * 32 + 31);
+    const int k = tile_row(g, C), lane = (int)(g & 31);
+    if (k > 0) return g - 32;
+    const int64_t tile_base = g - lane;
+    return lane > 0 ? tile_base + 32LL * (C - 1) + lane - 1 : tile_base - 1;
 }
 
 // ---- small helpers ---------------------------------------------------------------------------

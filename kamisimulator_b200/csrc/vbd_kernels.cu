@@ -68,9 +68,10 @@ __global__ void sweep_position_kernel(DeviceState st, const float4* __restrict__
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= num_threads) return;
     int rows = JACOBI ? C : C / 2;
-    int64_t tile = t / (32LL * rows);
-    int rem = (int)(t - tile * 32LL * rows);
-    int r = rem >> 5, lane = rem & 31;
+    // thread t: tile t / 32 rows, row r, lane t mod 32 (a 32-bit division: t / 32 < 2^32)
+    const uint32_t trow = (uint32_t)((uint64_t)t >> 5);
+    int64_t tile = trow / (uint32_t)rows;
+    int r = (int)(trow - (uint32_t)tile * (uint32_t)rows), lane = (int)(t & 31);
     int k = JACOBI ? r : 2 * r + colour;
     int64_t g = tile * 32LL * C + (int64_t)k * 32 + lane;
     float4 prm = st.prm[g];
@@ -109,9 +110,10 @@ __global__ void sweep_orientation_kernel(DeviceState st, const float4* __restric
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= num_threads) return;
     int rows = JACOBI ? C : C / 2;
-    int64_t tile = t / (32LL * rows);
-    int rem = (int)(t - tile * 32LL * rows);
-    int r = rem >> 5, lane = rem & 31;
+    // thread t: tile t / 32 rows, row r, lane t mod 32 (a 32-bit division: t / 32 < 2^32)
+    const uint32_t trow = (uint32_t)((uint64_t)t >> 5);
+    int64_t tile = trow / (uint32_t)rows;
+    int r = (int)(trow - (uint32_t)tile * (uint32_t)rows), lane = (int)(t & 31);
     int k = JACOBI ? r : 2 * r + colour;
     int64_t g = tile * 32LL * C + (int64_t)k * 32 + lane;
     float4 prm = st.prm[g];
