@@ -319,6 +319,19 @@ kami_status kami_vbd_step(kami_vbd_handle h, float dt, void* stream);
  * (YBSimulator.cu:388-414). */
 kami_status kami_vbd_synchronize(kami_vbd_handle h);
 
+/* Strain limiting: SDFBodyCollisionSolver's StrainLimiting kernel (SDFCollisionSolver/
+ * cudaSDFCollision.cu:176-199), which the reference's SDF solver runs after its SDF pass when
+ * UseStrainLimiting is set (SDFBodyCollisionSolver.cpp:186).  For every strand, from the root to the
+ * tip, a segment whose length l differs from its rest length l0 by more than strain_error * l0 has
+ * its far vertex moved along the segment by (l - l0), towards the near vertex as already corrected.
+ * Positions only: velocities are left as they are.  l0 is the handle's rest length of the segment
+ * (the segment's initial length, as the SDF solver's restLengthsVec, SDFBodyCollisionSolver.cpp:
+ * 107-121).  Call it after kami_vbd_step, once per step, as the reference runs it once per
+ * SolveNextStep; the reference's StrainError defaults to 0.1 (SDFBodyCollisionSolver.h:26).
+ * strain_error must be finite and >= 0.  It has no adjoint: while the tape holds recorded steps it
+ * returns KAMI_ERR_STATE.  Stream-ordered like kami_vbd_step. */
+kami_status kami_vbd_strain_limit(kami_vbd_handle h, float strain_error, void* stream);
+
 /* Full dynamic state snapshot (positions, velocities, last velocities, orientations and the
  * h / lastH / time clock) for checkpoint/resume; the reference saves none of these. */
 kami_status kami_vbd_state_size(kami_vbd_handle h, size_t* bytes);

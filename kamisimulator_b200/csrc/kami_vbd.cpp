@@ -113,6 +113,11 @@ struct kami_vbd_solver {
     float4* d_snap = nullptr;
     std::vector<char> graph_detect;  // substeps of the cached sweep graph that run detection
 
+    // strain limiting (kami_vbd_strain_limit): root slot and vertex count of each strand, built on
+    // the first call for the current tile layout
+    int64_t* d_strand_root = nullptr;
+    int32_t* d_strand_len = nullptr;
+
     // device-resident Hair: padded entry of each boundary vertex, and a staging copy of a padded
     // array for host transfers
     int64_t* d_hair_index = nullptr;
@@ -184,7 +189,7 @@ void release(kami_vbd_solver* h) {
     void* cptrs[] = {(void*)c.vid, (void*)c.gid, c.cols,   c.ncols,  c.maxstep,  c.bmin,    c.bmax,
                      c.cell,       c.count,      c.start,  c.cursor, c.srec,     c.sbmin,    c.sbmax,
                      c.ext_bits,   c.scan_tmp,
-                     h->d_snap,    h->d_hair_index, h->d_hair_stage};
+                     h->d_snap,    h->d_hair_index, h->d_hair_stage, h->d_strand_root, h->d_strand_len};
     for (void* p : cptrs)
         if (p) cudaFree(p);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
@@ -1153,6 +1158,10 @@ static kami_status relayout(kami_vbd_solver* h, int C) {
     for (int i = 0; i < 4 && e == cudaSuccess; i++)
         if (had[i]) e = dalloc(scratch[i], S);
     h->layout = nl;
+    if (h->d_strand_root) cudaFree(h->d_strand_root);  // slots of the old layout
+    if (h->d_strand_len) cudaFree(h->d_strand_len);
+    h->d_strand_root = nullptr;
+    h->d_strand_len = nullptr;
     drop_graphs(h);
     if (e != cudaSuccess) return cuda_fail(e, "relayout scratch");
     return KAMI_OK;
@@ -1653,6 +1662,42 @@ kami_status kami_vbd_download_hair(kami_vbd_handle h, float* xyz, float* vxyz, i
         }
     }
     return check_status_word(h);
+}
+
+kami_status kami_vbd_strain_limit(kami_vbd_handle h, float strain_error, void* stream) {
+    KAMI_TRY(valid_handle(h));
+    if (!std::isfinite(strain_error) || strain_error < 0.f)
+        return fail(KAMI_ERR_INVALID_ARGUMENT, "strain_error must be finite and >= 0");
+    if (!h->tape_steps.empty())
+        return fail(KAMI_ERR_STATE, "the tape holds recorded steps; strain limiting has no adjoint, run kami_vbd_backward "
+                                    "first");
+    if (!h->d_strand_root) {
+        std::vector<int64_t> root(h->ns);
+        std::vector<int32_t> len(h->ns);
+        for (int32_t k = 0; k < h->ns; k++) {
+            root[k] = h->layout.slot_of[h->strand_begin[k]];
+            len[k] = h->strand_begin[k + 1] - h->strand_begin[k];
+        }
+        KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
+        cudaError_t e = dalloc(&h->d_strand_root, (size_t)h->ns);
+        if (e == cudaSuccess) e = dalloc(&h->d_strand_len, (size_t)h->ns);
+        if (e == cudaSuccess)
+            e = cudaMemcpy(h->d_strand_root, root.data(), sizeof(int64_t) * h->ns, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaMemcpy(h->d_strand_len, len.data(), sizeof(int32_t) * h->ns, cudaMemcpyHostToDevice);
+        if (e != cudaSuccess) {
+            if (h->d_strand_root) cudaFree(h->d_strand_root);
+            if (h->d_strand_len) cudaFree(h->d_strand_len);
+            h->d_strand_root = nullptr;
+            h->d_strand_len = nullptr;
+            return cuda_fail(e, "strain limiting strand table");
+        }
+    }
+    return on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
+        KAMI_CUDA(launch_strain_limit(h->d_xm, h->d_prm, h->d_strand_root, h->d_strand_len, h->ns, h->layout.C,
+                                      strain_error, s),
+                  "strain limiting launch");
+        return KAMI_OK;
+    });
 }
 
 kami_status kami_vbd_synchronize(kami_vbd_handle h) {

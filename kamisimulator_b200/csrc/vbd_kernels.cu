@@ -233,6 +233,51 @@ cudaError_t launch_sweep_finish(const DeviceState& st, const float4* dx4, const 
     return cudaGetLastError();
 }
 
+// SDFBodyCollisionSolver's StrainLimiting (SDFCollisionSolver/cudaSDFCollision.cu:176-199): one
+// thread per strand marches from the root to the tip; a segment whose length l differs from its rest
+// length l0 by more than strain_error * l0 has its far vertex moved along the segment by (l - l0),
+// towards the near vertex as already corrected (helper_math's length and normalize: sqrtf and rsqrtf
+// of the dot product).  The next vertex's position is loaded before the current segment is
+// corrected: loads do not depend on the corrections, so the march is one dependent chain of
+// arithmetic, not of memory latencies.
+__global__ void strain_limit_kernel(float4* xm, const float4* __restrict__ prm, const int64_t* __restrict__ root_slot,
+                                    const int32_t* __restrict__ strand_len, int32_t num_strands, int C,
+                                    float strain_error) {
+    const int32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= num_strands) return;
+    const int32_t n = strand_len[s];
+    int64_t g = root_slot[s];
+    float4 cur = xm[g];
+    int64_t gn = n > 1 ? next_slot(g, C) : g;
+    float4 nxt = xm[gn];
+    for (int32_t i = 0; i + 1 < n; i++) {
+        const float l0 = prm[g].x;
+        const int64_t gnn = i + 2 < n ? next_slot(gn, C) : gn;
+        const float4 after = xm[gnn];  // the vertex after next, loaded ahead
+        const float3 pc = xyz(cur), pn = xyz(nxt);
+        const float l = sqrtf(dot3(pn - pc, pn - pc));
+        if (fabsf(l - l0) > strain_error * l0) {
+            const float3 d = pc - pn;
+            const float3 dir = d * rsqrtf(dot3(d, d));
+            const float3 q = pn + (l - l0) * dir;
+            nxt = make_float4(q.x, q.y, q.z, nxt.w);
+            xm[gn] = nxt;
+        }
+        g = gn;
+        gn = gnn;
+        cur = nxt;
+        nxt = after;
+    }
+}
+
+cudaError_t launch_strain_limit(float4* xm, const float4* prm, const int64_t* root_slot, const int32_t* strand_len,
+                                int32_t num_strands, int C, float strain_error, cudaStream_t s) {
+    if (num_strands <= 0) return cudaSuccess;
+    strain_limit_kernel<<<blocks_for(num_strands, 128), 128, 0, s>>>(xm, prm, root_slot, strand_len, num_strands, C,
+                                                                   strain_error);
+    return cudaGetLastError();
+}
+
 bool fused_supported(int C) { return C == 2 || C == 4; }
 
 namespace {

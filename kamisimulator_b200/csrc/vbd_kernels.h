@@ -56,6 +56,10 @@ cudaError_t launch_sweep_position_coll(const DeviceState& st, const float4* y4, 
                                        float4* dx_out, const float4* snap, const StepParams* d_sp, const PhysParams& pp,
                                        const CollParams& cp, int colour, bool jacobi, cudaStream_t s);
 
+// Strain limiting after the step (strain_limit_kernel): root slot and vertex count of each strand.
+cudaError_t launch_strain_limit(float4* xm, const float4* prm, const int64_t* root_slot, const int32_t* strand_len,
+                                int32_t num_strands, int C, float strain_error, cudaStream_t s);
+
 // sag-free initialisation (sag_free.cu): `iterations` passes, one thread per strand; fs: a float per slot
 cudaError_t launch_sag_free(const DeviceState& st, float3 gravity, const int32_t* strand_begin, const int64_t* slot_of,
                             int32_t num_strands, float* fs, int iterations, cudaStream_t s);

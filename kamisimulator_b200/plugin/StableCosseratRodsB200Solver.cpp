@@ -38,13 +38,27 @@ void StableCosseratRodsB200Solver::ReleasePins() {
     pinned_ = false;
 }
 
+// A held-back step followed by the SDF solver's strain limiting (SDFBodyCollisionSolver::SolveNextStep,
+// SDFBodyCollisionSolver.cpp:182-187): upload, step and strain limiting as three calls.
+void StableCosseratRodsB200Solver::StepAndLimit(bool upload) {
+    if (upload)
+        check(kami_vbd_upload_hair(handle_, hair_->positions.data(), hair_->velocities.data(), KAMI_MEMORY_HOST),
+              "UploadHair");
+    check(kami_vbd_step(handle_, pending_dt_, nullptr), "SolveNextStep");
+    check(kami_vbd_strain_limit(handle_, strain_error_, nullptr), "SolveNextStep (strain limiting)");
+}
+
 // Runs what UploadHair / SolveNextStep held back, without a download.
 void StableCosseratRodsB200Solver::Flush() {
     const float* x = pending_upload_ ? hair_->positions.data() : nullptr;
     const float* v = pending_upload_ ? hair_->velocities.data() : nullptr;
     if (pending_step_) {
+        const bool up = pending_upload_;
         pending_step_ = pending_upload_ = false;
-        check(kami_vbd_step_hair(handle_, pending_dt_, x, v, nullptr, nullptr), "SolveNextStep");
+        if (limits_strain())
+            StepAndLimit(up);
+        else
+            check(kami_vbd_step_hair(handle_, pending_dt_, x, v, nullptr, nullptr), "SolveNextStep");
     } else if (pending_upload_) {
         pending_upload_ = false;
         check(kami_vbd_upload_hair(handle_, x, v, KAMI_MEMORY_HOST), "UploadHair");
@@ -90,15 +104,21 @@ kami_vbd_desc StableCosseratRodsB200Solver::BuildDescriptor(const std::string& s
     };
     // What this solver does not build is refused rather than ignored: a YarnBall JSON scene
     // (YBJsonPath, the reference's buildFromJSON route, StableCosseratRodsSolver.cpp:42-46: explicit
-    // pins, glued endpoints and their connection springs, jsonBuilder.cpp:83-85) and the SDF solver's
-    // strain limiting (UseStrainLimiting, SDFBodyCollisionSolver.cpp:37, :186).
+    // pins, glued endpoints and their connection springs, jsonBuilder.cpp:83-85).
     auto yb = j.find("YBJsonPath");
     if (yb != j.end() && yb->second.kind == JsonValue::String && !yb->second.text.empty() &&
         std::ifstream(yb->second.text).good())
         throw std::runtime_error("YBJsonPath: YarnBall JSON scenes (buildFromJSON, glued endpoints) are not supported");
-    auto sl = j.find("UseStrainLimiting");
-    if (sl != j.end() && sl->second.kind == JsonValue::Bool && sl->second.boolean)
-        throw std::runtime_error("UseStrainLimiting: the SDF pass's strain limiting is not supported");
+    // The SDF solver's strain limiting and its tolerance (SDFBodyCollisionSolver.cpp:36-37, defaults
+    // SDFBodyCollisionSolver.h:26-27), read from this settings file: the reference's SDF solver reads
+    // them from its own settings file, which StableCosseratRodsSolver never passes it (its enabling
+    // call, StableCosseratRodsSolver.cpp:60, is commented out).  Runs after each step when EnableSDF.
+    strain_limiting_ = false;
+    strain_error_ = 0.1f;
+    boolean("UseStrainLimiting", strain_limiting_);
+    num("StrainError", strain_error_);
+    if (!(strain_error_ >= 0.f) || !std::isfinite(strain_error_))
+        throw std::runtime_error("StrainError must be finite and >= 0");
     float num_itr = (float)d.num_itr, sag_free = 0.f;
     bool hair_hair = false;
     num("NumItr", num_itr);
@@ -252,7 +272,7 @@ void StableCosseratRodsB200Solver::SolveNextStep(float dt) {
 // Sim -> Hair (StableCosseratRodsSolver.cpp:258-277): with a held-back step, the step and the
 // download in one call; else one gather on the GPU into the padded arrays
 void StableCosseratRodsB200Solver::DownloadHair() {
-    if (pending_step_) {
+    if (pending_step_ && !limits_strain()) {
         const bool up = pending_upload_;
         pending_step_ = pending_upload_ = false;
         check(kami_vbd_step_hair(handle_, pending_dt_, up ? hair_->positions.data() : nullptr,

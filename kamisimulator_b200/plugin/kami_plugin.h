@@ -52,8 +52,9 @@ struct BodySDF {
 // (StableCosseratRodsSolver.h:41-112): NumItr, UseYoungsModule, YoungsModule,
 // StiffnessDeviationCoeff, StretchK, BendK, CurveRadius (the simulated radius is 0.05 x CurveRadius,
 // StableCosseratRodsSolver.cpp:177-179), Density, VelocityDecay, ExternalForceMultiplier, Wind*,
-// EnableSDF, EnableHairHairColl, SagFreeItr, SubdivCoeff, EnableResample, plus SDFThreshold
-// (SDFBodyCollisionSolver.h:25) and the extensions MaxTimeStep (the reference fixes 4e-4 s),
+// EnableSDF, EnableHairHairColl, SagFreeItr, SubdivCoeff, EnableResample, plus the SDF solver's
+// SDFThreshold, UseStrainLimiting and StrainError (SDFBodyCollisionSolver.h:25-27: strain limiting
+// after each step, when EnableSDF) and the extensions MaxTimeStep (the reference fixes 4e-4 s),
 // Gravity [x, y, z], Schedule ("colour2" | "jacobi") and Form ("auto" | "fused" | "sweep").
 // SagFreeItr runs that many passes of sag-free initialisation at Construct
 // (StableCosseratRodsSolver.cpp:208).  EnableHairHairColl turns on hair-hair collision with the reference solver's barrier
@@ -79,6 +80,10 @@ class StableCosseratRodsB200Solver : public Solver {
     void DownloadHair() override;
     std::string GetInfoString() override;
 
+    // the SDF solver's strain limiting as the settings set it (UseStrainLimiting, StrainError)
+    bool strain_limiting() const { return strain_limiting_; }
+    float strain_error() const { return strain_error_; }
+
     // the C-ABI handle, for calls beyond the Solver interface (runs what is held back first)
     kami_vbd_handle handle() {
         if (handle_) Flush();
@@ -91,6 +96,11 @@ class StableCosseratRodsB200Solver : public Solver {
     bool has_body_ = false;
     bool enable_sdf_ = true;
     float sdf_threshold_ = 0.015f;
+    bool strain_limiting_ = false;
+    float strain_error_ = 0.1f;
+    // strain limiting runs inside the SDF solver's step, so only with EnableSDF
+    bool limits_strain() const { return strain_limiting_ && enable_sdf_; }
+    void StepAndLimit(bool upload);
     std::string settings_dump_;
     std::vector<int> strand_refs_;      // Hair strand of each simulated strand
     std::vector<int32_t> strand_begin_;
@@ -99,8 +109,9 @@ class StableCosseratRodsB200Solver : public Solver {
     // Frames over the Hair.  Construct page-locks the Hair's position and velocity arrays
     // (kami_host_register); they must then not be reallocated until the solver is destroyed.  The
     // last SolveNextStep before a DownloadHair, and an UploadHair before a SolveNextStep, are held
-    // back and run as one kami_vbd_step_hair call (upload, step and download in one launch); any
-    // other call runs what is held back first, so errors of a held-back step surface at that call.
+    // back and run as one kami_vbd_step_hair call (upload, step and download in one launch), or, with
+    // strain limiting, as upload, step, strain limiting and download; any other call runs what is
+    // held back first, so errors of a held-back step surface at that call.
     bool pinned_ = false;
     bool pending_upload_ = false, pending_step_ = false;
     float pending_dt_ = 0.f;

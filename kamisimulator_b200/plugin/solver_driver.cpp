@@ -65,11 +65,12 @@ int main(int argc, char** argv) {
                         "\"num_itr\": %d, \"young\": %.9g, \"deviation\": %.9g, \"stiffness_mode\": %d, "
                         "\"velocity_decay\": %.9g, \"wind_peak\": %.9g, \"max_h\": %.9g, \"schedule\": %d, "
                         "\"form\": %d, \"gravity\": [%.9g, %.9g, %.9g], \"hair_hair\": %d, "
-                        "\"barrier_thickness\": %.9g, \"step_limit\": %d, \"sag_free_itr\": %d}\n",
+                        "\"barrier_thickness\": %.9g, \"step_limit\": %d, \"sag_free_itr\": %d, "
+                        "\"strain_limiting\": %d, \"strain_error\": %.9g}\n",
                         d.num_strands, d.strand_begin[d.num_strands], d.radius, d.density, d.num_itr, d.young,
                         d.deviation, d.stiffness_mode, d.velocity_decay, d.wind_peak, d.max_h, d.schedule, d.form,
                         d.gravity[0], d.gravity[1], d.gravity[2], d.hair_hair, d.barrier_thickness, d.step_limit,
-                        d.sag_free_itr);
+                        d.sag_free_itr, s.strain_limiting() ? 1 : 0, s.strain_error());
             return 0;
         }
         if (argc < 6) {

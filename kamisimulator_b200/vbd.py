@@ -40,7 +40,7 @@ EXPORTED = [
     "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake", "kami_vbd_sag_free",
     "kami_hair_subdivide", "kami_hair_resample", "kami_vbd_step_host", "kami_vbd_get_tiles_per_group",
     "kami_vbd_set_launch_mode", "kami_vbd_get_launch_mode", "kami_vbd_step_hair", "kami_host_register",
-    "kami_host_unregister",
+    "kami_host_unregister", "kami_vbd_strain_limit",
 ]
 
 
@@ -145,6 +145,7 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_step_host": [vp, f32, vp, vp, vp, vp],
         "kami_vbd_get_tiles_per_group": [vp, ctypes.POINTER(i32)],
         "kami_vbd_synchronize": [vp],
+        "kami_vbd_strain_limit": [vp, f32, vp],
         "kami_vbd_state_size": [vp, ctypes.POINTER(ctypes.c_size_t)],
         "kami_vbd_get_state": [vp, vp, ctypes.c_size_t, i32],
         "kami_vbd_set_state": [vp, vp, ctypes.c_size_t, i32],
@@ -414,6 +415,13 @@ class Solver:
 
     def synchronize(self):
         _check(self.lib.kami_vbd_synchronize(self._h))
+
+    def strain_limit(self, strain_error=0.1, stream=None):
+        """kami_vbd_strain_limit: the SDF solver's strain limiting (cudaSDFCollision.cu:176-199), run
+        after a step as SDFBodyCollisionSolver::SolveNextStep runs it after its SDF pass (default
+        StrainError 0.1, SDFBodyCollisionSolver.h:26)."""
+        s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
+        _check(self.lib.kami_vbd_strain_limit(self._h, ctypes.c_float(strain_error), s))
 
     def set_body_transform(self, rot, trans):
         r = (ctypes.c_float * 4)(*rot)

@@ -1306,4 +1306,30 @@ void oracle_flop_count(int64_t* position_ops, int64_t* orientation_ops) {
     *orientation_ops = Counted::ops;
 }
 
+// StrainLimiting (SDFCollisionSolver/cudaSDFCollision.cu:176-199), FP32, over packed strands
+// (x: 3 floats per vertex in strand order; l0: rest length of the segment starting at each vertex).
+// Per strand, from the root: l = length(x[i+1] - x[i]); if |l - l0| > strain_error * l0 then
+// x[i+1] += (l - l0) * normalize(x[i] - x[i+1]), with x[i] as already corrected.  helper_math's
+// length is sqrtf(dot) and normalize is v * rsqrtf(dot), whose host form is 1 / sqrtf
+// (extern/cuda_helpers/helper_math.h:66, :683, :694-697).
+void oracle_strain_limit_f32(int32_t num_strands, const int32_t* strand_begin, const float* l0, float strain_error,
+                             float* x) {
+    for (int32_t s = 0; s < num_strands; s++) {
+        for (int32_t i = strand_begin[s]; i + 1 < strand_begin[s + 1]; i++) {
+            float* a = x + 3 * (int64_t)i;
+            float* b = a + 3;
+            const float ux = b[0] - a[0], uy = b[1] - a[1], uz = b[2] - a[2];
+            const float l = std::sqrt(ux * ux + uy * uy + uz * uz);
+            if (std::fabs(l - l0[i]) > strain_error * l0[i]) {
+                const float dx = a[0] - b[0], dy = a[1] - b[1], dz = a[2] - b[2];
+                const float inv = 1.0f / std::sqrt(dx * dx + dy * dy + dz * dz);
+                const float k = l - l0[i];
+                b[0] += k * (dx * inv);
+                b[1] += k * (dy * inv);
+                b[2] += k * (dz * inv);
+            }
+        }
+    }
+}
+
 }  // extern "C"

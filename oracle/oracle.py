@@ -93,6 +93,9 @@ def load():
                                             ctypes.c_int64]
         lib.oracle_flop_count.restype = None
         lib.oracle_flop_count.argtypes = [ctypes.c_void_p, ctypes.c_void_p]
+        lib.oracle_strain_limit_f32.restype = None
+        lib.oracle_strain_limit_f32.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_float,
+                                                ctypes.c_void_p]
         lib.oracle_sdf_points_f64.restype = ctypes.c_int
         lib.oracle_sdf_points_f64.argtypes = [ctypes.c_int32, ctypes.c_void_p, ctypes.c_int32, ctypes.c_void_p,
                                               ctypes.c_int64, ctypes.c_void_p, ctypes.c_void_p]
@@ -206,6 +209,17 @@ class OracleSim:
         self.v_last[...] = st["v_last"]
         self.q[...] = st["q"]
         self.clock[...] = st["clock"]
+
+
+def strain_limit(x, strand_begin, rest_lengths, strain_error=0.1):
+    """The SDF solver's StrainLimiting (cudaSDFCollision.cu:176-199) on packed strands, FP32: returns
+    the corrected positions (rest_lengths[i]: rest length of the segment starting at vertex i)."""
+    lib = load()
+    out = np.ascontiguousarray(x, np.float32).copy()
+    sb = np.ascontiguousarray(strand_begin, np.int32)
+    l0 = np.ascontiguousarray(rest_lengths, np.float32)
+    lib.oracle_strain_limit_f32(len(sb) - 1, _p(sb), _p(l0), float(strain_error), _p(out))
+    return out
 
 
 def twist_angles(q_ref, q_new):

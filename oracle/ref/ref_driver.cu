@@ -202,6 +202,51 @@ int ref_download(void* h, float* x, float* v, float* q) {
     return 0;
 }
 
+// The SDF solver's StrainLimiting kernel (cudaSDFCollision.cu:176-199) over packed strands, set up
+// as SDFBodyCollisionSolver::InitAdditionalHairData does (SDFBodyCollisionSolver.cpp:100-121): every
+// particle's GlobalIdx and StrandLength, EdgeRestIdx.y naming its segment's rest length, and the
+// roots' indices.  l0[i]: rest length of the segment starting at vertex i.
+int ref_strain_limit(int32_t num_strands, const int32_t* strand_begin, const float* l0, float strain_error, float* x) {
+    const int64_t np = strand_begin[num_strands];
+    SDFSimulationParams p{};
+    p.NumStrands = (size_t)num_strands;
+    p.NumParticles = (size_t)np;
+    p.StrainError = strain_error;
+    p.UseStrainLimiting = true;
+    KamiCopySDFSimParamsToDevice(&p);
+    std::vector<ParticleForSDFColl> parts(np);
+    std::vector<int> roots(num_strands);
+    for (int32_t s = 0; s < num_strands; s++) {
+        roots[s] = strand_begin[s];
+        for (int32_t i = strand_begin[s]; i < strand_begin[s + 1]; i++) {
+            parts[i].Position = make_float3(x[3 * i], x[3 * i + 1], x[3 * i + 2]);
+            parts[i].StrandLength = strand_begin[s + 1] - strand_begin[s];
+            parts[i].LocalIdx = i - strand_begin[s];
+            parts[i].GlobalIdx = i;
+            parts[i].EdgeRestIdx.y = i;
+        }
+    }
+    SDFDeviceBuffers b{};
+    if (cudaMalloc(&b.Particles, sizeof(ParticleForSDFColl) * np) != cudaSuccess) return 1;
+    if (cudaMalloc(&b.restLenghts, sizeof(float) * np) != cudaSuccess) return 1;
+    if (cudaMalloc(&b.rootIdx, sizeof(int) * num_strands) != cudaSuccess) return 1;
+    cudaMemcpy(b.Particles, parts.data(), sizeof(ParticleForSDFColl) * np, cudaMemcpyHostToDevice);
+    cudaMemcpy(b.restLenghts, l0, sizeof(float) * np, cudaMemcpyHostToDevice);
+    cudaMemcpy(b.rootIdx, roots.data(), sizeof(int) * num_strands, cudaMemcpyHostToDevice);
+    KamiLaunchKernelStrainLimitingAfterSDFCollision(make_int2((num_strands + 127) / 128, 128), b);
+    cudaError_t e = cudaDeviceSynchronize();
+    cudaMemcpy(parts.data(), b.Particles, sizeof(ParticleForSDFColl) * np, cudaMemcpyDeviceToHost);
+    cudaFree(b.Particles);
+    cudaFree(b.restLenghts);
+    cudaFree(b.rootIdx);
+    for (int64_t i = 0; i < np; i++) {
+        x[3 * i] = parts[i].Position.x;
+        x[3 * i + 1] = parts[i].Position.y;
+        x[3 * i + 2] = parts[i].Position.z;
+    }
+    return e == cudaSuccess ? 0 : 1;
+}
+
 // One SDFHeadCollision pass over np particles, with the grid spacing SDFBodyCollisionSolver::InitParams
 // computes (SDFBodyCollisionSolver.cpp:142-159).  local_idx[i] == 0 marks strand roots.
 int ref_sdf_project(int64_t np, float* pos, float* vel, const int32_t* local_idx, const int32_t* dims, const float* gmin,

@@ -36,7 +36,8 @@ def load():
         lib.ref_step_hair_hair.restype = ctypes.c_int
         lib.ref_download.argtypes = [vp, vp, vp, vp]
         lib.ref_sdf_project.argtypes = [i64, vp, vp, vp, vp, vp, vp, f32, vp, vp, vp, vp]
-        for n in ("ref_material", "ref_set_state", "ref_advance", "ref_download", "ref_sdf_project"):
+        lib.ref_strain_limit.argtypes = [i32, vp, vp, f32, vp]
+        for n in ("ref_material", "ref_set_state", "ref_advance", "ref_download", "ref_sdf_project", "ref_strain_limit"):
             getattr(lib, n).restype = ctypes.c_int
         _lib = lib
     return _lib
@@ -123,6 +124,18 @@ def sdf_project(pos, vel, local_idx, sdf, rot=(0.0, 0.0, 0.0, 1.0), trans=(0.0, 
     if rc != 0:
         raise RuntimeError("ref_sdf_project failed")
     return p, v
+
+
+def strain_limit(x, strand_begin, rest_lengths, strain_error=0.1):
+    """One pass of the reference's StrainLimiting kernel (cudaSDFCollision.cu:176-199) on packed
+    strands; returns the corrected positions."""
+    lib = load()
+    out = np.ascontiguousarray(x, np.float32).copy()
+    sb = np.ascontiguousarray(strand_begin, np.int32)
+    l0 = np.ascontiguousarray(rest_lengths, np.float32)
+    if lib.ref_strain_limit(len(sb) - 1, _p(sb), _p(l0), float(strain_error), _p(out)) != 0:
+        raise RuntimeError("ref_strain_limit failed")
+    return out
 
 
 CPU_LIB_PATH = os.path.join(_HERE, "_ref", "libkami_ref_cpu.so")

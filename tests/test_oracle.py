@@ -333,3 +333,23 @@ def test_fp64_autograd_restatement_follows_the_fp64_oracle(wind):
     # the oracle rounds the wind's cosine argument to float, as the reference does
     np.testing.assert_allclose(state[0].numpy(), o.x, rtol=0, atol=1e-9)
     np.testing.assert_allclose(state[3].numpy(), o.q, rtol=0, atol=1e-8)
+
+
+def test_strain_limiting_restatement_on_a_hand_case():
+    """StrainLimiting (cudaSDFCollision.cu:176-199): from the root, a segment whose length is off its
+    rest length by more than StrainError x l0 gets its far vertex pulled along the segment to l0; the
+    next segment is then measured from the corrected vertex.  Segments inside the tolerance stay."""
+    x = np.array([[0, 0, 0], [0, 0, 1.5], [0, 0, 2.0], [0, 0, 3.05],
+                  [1, 0, 0], [1, 0, 0.5], [1, 0.6, 0.5]], np.float32)
+    sb = np.array([0, 4, 7], np.int32)
+    l0 = np.array([1, 1, 1, 0, 1, 0.5, 0], np.float32)
+    out = orc.strain_limit(x, sb, l0, 0.1)
+    # strand 0: 1.5 -> 1 (vertex 1 to z = 1); vertex 2 is then 1.0 from it (kept); 1.05 is within 10 % (kept)
+    np.testing.assert_allclose(out[:4], [[0, 0, 0], [0, 0, 1], [0, 0, 2], [0, 0, 3.05]], atol=1e-6)
+    # strand 1: 0.5 against 1 -> vertex 5 pushed out to z = 1; the 0.6 segment is then measured from there
+    assert abs(np.linalg.norm(out[5] - out[4]) - 1.0) < 1e-6
+    np.testing.assert_allclose(out[5], [1, 0, 1], atol=1e-6)
+    d6 = np.linalg.norm(out[6] - out[5])
+    assert abs(d6 - 0.5) < 1e-6  # |(1, 0.6, 0.5) - (1, 0, 1)| = 0.781 > 1.1 x 0.5: pulled to 0.5
+    # a tolerance that covers every strain changes nothing
+    np.testing.assert_array_equal(orc.strain_limit(x, sb, l0, 10.0), x)

@@ -73,7 +73,7 @@ def test_invalid_settings_are_rejected(tmp_path):
     # features of the reference this solver does not build are refused, not ignored
     (tmp_path / "scene.json").write_text("{}")
     for bad, word in (({"YBJsonPath": str(tmp_path / "scene.json")}, "YBJsonPath"),
-                      ({"UseStrainLimiting": True}, "UseStrainLimiting")):
+                      ({"UseStrainLimiting": True, "StrainError": -0.1}, "StrainError")):
         (tmp_path / "s.json").write_text(json.dumps(bad))
         r = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
                            capture_output=True, text=True)
@@ -82,6 +82,20 @@ def test_invalid_settings_are_rejected(tmp_path):
     (tmp_path / "s.json").write_text(json.dumps({"YBJsonPath": str(tmp_path / "missing.json")}))
     subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")], check=True,
                    capture_output=True)
+
+
+def test_strain_limiting_settings(tmp_path):
+    """The SDF solver's UseStrainLimiting and StrainError (SDFBodyCollisionSolver.cpp:36-37), off and
+    0.1 by default (SDFBodyCollisionSolver.h:26-27)."""
+    g = synth.cantilever(2, 8)
+    write_hair(tmp_path / "hair.bin", g)
+    for settings, on, err in (({}, 0, 0.1), ({"UseStrainLimiting": True}, 1, 0.1),
+                              ({"UseStrainLimiting": True, "StrainError": 0.05}, 1, 0.05)):
+        (tmp_path / "s.json").write_text(json.dumps(settings))
+        out = subprocess.run([DRIVER, "--dry-run", str(tmp_path / "s.json"), str(tmp_path / "hair.bin")],
+                             capture_output=True, text=True, check=True).stdout
+        d = json.loads(out)
+        assert d["strain_limiting"] == on and d["strain_error"] == pytest.approx(err)
 
 
 def test_sag_free_setting(tmp_path):
@@ -132,6 +146,39 @@ def test_plugin_steps_match_the_c_abi_and_the_oracle(tmp_path):
     np.testing.assert_allclose(packed, x, atol=1e-6)
     assert np.abs(packed - o.x).max() <= helpers.POS_TOL
     assert np.abs(packed - g.positions).max() > 1e-4  # the strands moved
+
+
+@pytest.mark.gpu
+def test_plugin_strain_limiting_after_each_step(tmp_path):
+    """UseStrainLimiting: every SolveNextStep is followed by the SDF solver's strain limiting, as
+    SDFBodyCollisionSolver::SolveNextStep runs it after its SDF pass (SDFBodyCollisionSolver.cpp:186);
+    the same as kami_vbd_step then kami_vbd_strain_limit through the C ABI."""
+    g = helpers.soft_groom(40, (6, 30), seed=12)
+    counts, mv = write_hair(tmp_path / "hair.bin", g, pad_to=40)
+    settings = {"NumItr": 6, "UseYoungsModule": True, "YoungsModule": 1e-4, "StiffnessDeviationCoeff": 0.5,
+                "CurveRadius": 40e-6 / 0.05, "Density": 1300, "VelocityDecay": 0.05, "WindPeak": 0,
+                "EnableSDF": True, "UseStrainLimiting": True, "StrainError": 0.002, "MaxTimeStep": 1 / 60,
+                "Gravity": [0.3, -0.4, -9.81], "SubdivCoeff": 1, "EnableResample": False}
+    (tmp_path / "s.json").write_text(json.dumps(settings))
+    steps = 5
+    subprocess.run([DRIVER, str(tmp_path / "s.json"), str(tmp_path / "hair.bin"), str(steps), str(1 / 60),
+                    str(tmp_path / "out.bin")], check=True, capture_output=True)
+    pos, _ = read_out(tmp_path / "out.bin", g.num_strands, mv)
+    packed = np.concatenate([pos[s, : counts[s]] for s in range(g.num_strands)])
+    st = dict(num_itr=6, max_h=1 / 60, gravity=(0.3, -0.4, -9.81), radius=40e-6, velocity_decay=0.05)
+    g.strand_young[:] = 1e-4
+    g.strand_dev[:] = 0.5
+    limited, free = helpers.gpu_solver(g, st), helpers.gpu_solver(g, st)
+    for _ in range(steps):
+        limited.step(1 / 60)
+        limited.strain_limit(0.002)
+        free.step(1 / 60)
+    x, _ = limited.get_positions_velocities()
+    xf, _ = free.get_positions_velocities()
+    limited.close()
+    free.close()
+    np.testing.assert_allclose(packed, x, atol=1e-6)
+    assert np.abs(x - xf).max() > 1e-5  # the limit changed the motion
 
 
 @pytest.mark.gpu
