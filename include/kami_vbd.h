@@ -143,6 +143,17 @@ typedef struct kami_vbd_desc {
      * BuildYarnBallHair does (StableCosseratRodsSolver.cpp:208; Sim::SagFree, YBSimulator.cu:480-674);
      * 0 = none.  kami_vbd_sag_free runs it on demand. */
     int32_t sag_free_itr;
+
+    /* Connection springs: Vertex::connectionIndex (YarnBall.h:56), the spring of stiffness 40 that
+     * cosseratItr adds to a vertex tied to another one (cosserat.cu:123-131), as YarnBall sets it for
+     * glued endpoints (jsonBuilder.cpp:165-185) and the two ends of a closed curve (reader.cpp:40-44).
+     * host, one entry per vertex: the vertex of the same groom it is tied to (both ways for a mutual
+     * tie), or -1; NULL = none.  The partner's displacement is read as it stood at the start of the
+     * iteration (colour2: a snapshot taken per iteration, as hair-hair partners are; jacobi: the
+     * previous iterate), where the reference reads it while other threads write it.  Handles with a
+     * tie run on the sweep form (form AUTO picks it; FUSED, hair_hair and a later change of the tile
+     * shape are KAMI_ERR_UNSUPPORTED). */
+    const int32_t* connection_index;
 } kami_vbd_desc;
 
 typedef struct kami_vbd_solver* kami_vbd_handle;
@@ -458,7 +469,8 @@ typedef struct kami_vbd_noalloc_args {
 } kami_vbd_noalloc_args;
 
 /* settings: scalar fields of a kami_vbd_desc (gravity, damping, velocity_decay, acceleration_ratio,
- * external_force_multiplier, wind, num_itr, max_h, schedule); geometry fields are ignored.
+ * external_force_multiplier, wind, num_itr, max_h, schedule); geometry fields are ignored, and a
+ * non-NULL connection_index is KAMI_ERR_UNSUPPORTED.
  * Asynchronous on `stream` (a cudaStream_t; NULL = legacy default stream); args->clock is updated. */
 kami_status kami_vbd_step_noalloc(const kami_vbd_desc* settings, kami_vbd_noalloc_args* args, float dt, void* stream);
 

@@ -113,6 +113,9 @@ struct kami_vbd_solver {
     float4* d_snap = nullptr;
     std::vector<char> graph_detect;  // substeps of the cached sweep graph that run detection
 
+    // connection springs: the slot each slot is tied to (-1: none), null when no vertex is tied
+    int64_t* d_conn = nullptr;
+
     // strain limiting (kami_vbd_strain_limit): root slot and vertex count of each strand, built on
     // the first call for the current tile layout
     int64_t* d_strand_root = nullptr;
@@ -163,6 +166,7 @@ struct kami_vbd_solver {
         s.vlast = d_vlast;
         s.q = d_q;
         s.qr = d_qr;
+        s.conn = d_conn;
         s.prm = d_prm;
         s.num_tiles = layout.num_tiles;
         s.status = d_status;
@@ -189,7 +193,7 @@ void release(kami_vbd_solver* h) {
     void* cptrs[] = {(void*)c.vid, (void*)c.gid, c.cols,   c.ncols,  c.maxstep,  c.bmin,    c.bmax,
                      c.cell,       c.count,      c.start,  c.cursor, c.srec,     c.sbmin,    c.sbmax,
                      c.ext_bits,   c.scan_tmp,
-                     h->d_snap,    h->d_hair_index, h->d_hair_stage, h->d_strand_root, h->d_strand_len};
+                     h->d_snap,    h->d_hair_index, h->d_hair_stage, h->d_strand_root, h->d_strand_len, h->d_conn};
     for (void* p : cptrs)
         if (p) cudaFree(p);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
@@ -305,7 +309,8 @@ kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
                     err = launch_sweep_position_coll(st, h->d_y, q_cur, dx_cur, dx_alt, dx_cur, h->d_step, h->pp, h->cp, 0,
                                                      true, s);
                 else
-                    err = launch_sweep_position(st, h->d_y, q_cur, dx_cur, dx_alt, h->d_step, h->pp, C, 0, true, s);
+                    err = launch_sweep_position(st, h->d_y, q_cur, dx_cur, dx_alt, h->d_step, h->pp, C, 0, true, s,
+                                                dx_cur);
                 std::swap(dx_cur, dx_alt);
                 if (err == cudaSuccess) err = launch_sweep_orientation(st, dx_cur, q_cur, q_alt, C, 0, true, s);
                 std::swap(q_cur, q_alt);
@@ -323,8 +328,11 @@ kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
                 for (int c = 0; c < 2 && err == cudaSuccess; c++)
                     err = launch_sweep_orientation(st, dx_cur, q_cur, q_cur, C, c, false, s);
             } else {
+                if (h->d_conn)  // the tied partners' dx at the start of the iteration
+                    err = cudaMemcpyAsync(h->d_snap, dx_cur, b4, cudaMemcpyDeviceToDevice, s);
                 for (int c = 0; c < 2 && err == cudaSuccess; c++)
-                    err = launch_sweep_position(st, h->d_y, q_cur, dx_cur, dx_cur, h->d_step, h->pp, C, c, false, s);
+                    err = launch_sweep_position(st, h->d_y, q_cur, dx_cur, dx_cur, h->d_step, h->pp, C, c, false, s,
+                                                h->d_snap);
                 for (int c = 0; c < 2 && err == cudaSuccess; c++)
                     err = launch_sweep_orientation(st, dx_cur, q_cur, q_cur, C, c, false, s);
             }
@@ -417,6 +425,21 @@ static kami_status validate_desc(const kami_vbd_desc* d) {
             if (!(s->grid_max[a] > s->grid_min[a])) return fail(KAMI_ERR_INVALID_ARGUMENT, "SDF grid_max must exceed grid_min");
     }
     if (d->sag_free_itr < 0) return fail(KAMI_ERR_INVALID_ARGUMENT, "sag_free_itr must be >= 0");
+    if (d->connection_index) {
+        const int32_t nv = d->strand_begin[d->num_strands];
+        bool tied = false;
+        for (int32_t i = 0; i < nv; i++) {
+            const int32_t c = d->connection_index[i];
+            if (c < -1 || c >= nv || c == i)
+                return fail(KAMI_ERR_INVALID_ARGUMENT,
+                            "connection_index[%d] = %d: must be -1 or another vertex of the groom (0..%d)", i, c, nv - 1);
+            tied |= c >= 0;
+        }
+        if (tied && d->hair_hair)
+            return fail(KAMI_ERR_UNSUPPORTED, "connection springs together with hair-hair collision are not supported");
+        if (tied && d->form == KAMI_FORM_FUSED)
+            return fail(KAMI_ERR_UNSUPPORTED, "connection springs run on the sweep form (a tie may join two tiles)");
+    }
     if (d->hair_hair) {
         if (!(d->barrier_thickness > 0.f)) return fail(KAMI_ERR_INVALID_ARGUMENT, "barrier_thickness must be > 0");
         if (!(d->detection_scaler > 1.f))  // Sim::uploadMeta, YBSimulator.cu:326
@@ -562,9 +585,18 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
     positions.reserve(3 * total_vertices);
     velocities.reserve(3 * total_vertices);
     Material m;
+    std::vector<int32_t> ties;  // boundary vertex each vertex is tied to, or -1 (empty: no tie)
     for (int32_t g = 0; g < n; g++) {
         const kami_vbd_desc* e = &descs[g];
         const int32_t base = h->strand_begin.back();
+        if (e->connection_index) {
+            const int32_t nvg = e->strand_begin[e->num_strands];
+            for (int32_t i = 0; i < nvg; i++)
+                if (e->connection_index[i] >= 0) {
+                    if (ties.empty()) ties.assign(total_vertices, -1);
+                    ties[base + i] = base + e->connection_index[i];
+                }
+        }
         for (int32_t s = 1; s <= e->num_strands; s++) h->strand_begin.push_back(base + e->strand_begin[s]);
         h->groom_strand_begin.push_back(h->groom_strand_begin.back() + e->num_strands);
         const int32_t nvg = e->strand_begin[e->num_strands];
@@ -615,13 +647,14 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
     // the fused form runs strands longer than a tile of 4 slots per lane on groups of up to 8 tiles
     int K = 1;
     if (!fused_supported(C) && d->slots_per_lane == 0 && tiles_per_group_for(h->strand_begin.data(), h->ns, 4) > 0) {
-        if (d->form != KAMI_FORM_SWEEP && !d->hair_hair) {
+        if (d->form != KAMI_FORM_SWEEP && !d->hair_hair && ties.empty()) {
             C = 4;
             K = tiles_per_group_for(h->strand_begin.data(), h->ns, 4);
         }
     }
     int form = d->form;
-    if (form == KAMI_FORM_AUTO) form = (fused_supported(C) && !d->hair_hair) ? KAMI_FORM_FUSED : KAMI_FORM_SWEEP;
+    if (form == KAMI_FORM_AUTO)
+        form = (fused_supported(C) && !d->hair_hair && ties.empty()) ? KAMI_FORM_FUSED : KAMI_FORM_SWEEP;
     if (d->hair_hair) {
         // Sim::uploadMeta (YBSimulator.cu:328-332): contacts must fit between a segment's ends
         float min_seg = FLT_MAX;
@@ -714,6 +747,14 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
     if (e == cudaSuccess) e = cudaMemcpy(h->d_qr, qr.data(), b4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(h->d_prm, prm.data(), b4, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemset(h->d_status, 0, sizeof(int));
+    if (e == cudaSuccess && !ties.empty()) {  // connection springs, by slot; colour2 snapshots the partners' dx
+        std::vector<int64_t> conn(S, -1);
+        for (int64_t i = 0; i < h->nv; i++)
+            if (ties[i] >= 0) conn[h->layout.slot_of[i]] = h->layout.slot_of[ties[i]];
+        e = dalloc(&h->d_conn, S);
+        if (e == cudaSuccess) e = cudaMemcpy(h->d_conn, conn.data(), sizeof(int64_t) * S, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_COLOUR2) e = dalloc(&h->d_snap, S);
+    }
     if (e != cudaSuccess) return bail(cuda_fail(e, "uploading solver state"));
 
     if (d->sdf) {
@@ -1172,6 +1213,8 @@ kami_status kami_vbd_set_tuning(kami_vbd_handle h, int32_t slots_per_lane, int32
     KAMI_TRY(valid_handle(h));
     if (slots_per_lane != 0 && h->hair_hair && slots_per_lane != h->layout.C)
         return fail(KAMI_ERR_UNSUPPORTED, "the tile shape of a handle with hair-hair collision is fixed at creation");
+    if (slots_per_lane != 0 && h->d_conn && slots_per_lane != h->layout.C)
+        return fail(KAMI_ERR_UNSUPPORTED, "the tile shape of a handle with connection springs is fixed at creation");
     if (slots_per_lane != 0) {
         const int cmin = slots_per_lane_for(h->strand_begin.data(), h->ns);
         if (h->form == KAMI_FORM_FUSED) {  // longer strands take groups of tiles

@@ -215,6 +215,8 @@ extern "C" kami_status kami_vbd_step_noalloc(const kami_vbd_desc* settings, kami
         return noalloc_fail(KAMI_ERR_INVALID_ARGUMENT, "a device array pointer is null");
     if (settings->schedule != KAMI_SCHEDULE_COLOUR2)
         return noalloc_fail(KAMI_ERR_UNSUPPORTED, "kami_vbd_step_noalloc runs the colour2 schedule only");
+    if (settings->connection_index)
+        return noalloc_fail(KAMI_ERR_UNSUPPORTED, "kami_vbd_step_noalloc has no connection springs");
     if (settings->num_itr < 0 || !(settings->max_h > 0.f))
         return noalloc_fail(KAMI_ERR_INVALID_ARGUMENT, "num_itr must be >= 0 and max_h > 0");
     if (!std::isfinite(dt)) return noalloc_fail(KAMI_ERR_INVALID_ARGUMENT, "dt must be finite");

@@ -75,6 +75,7 @@ struct DeviceState {
     const float4* prm; // lRest, kStretch, 0, flags (bit pattern)
     int64_t num_tiles;
     int* status;
+    const int64_t* conn = nullptr;  // slot each slot is tied to by a connection spring, or -1 (sweep form)
 };
 
 // Iterates of recorded steps for the adjoint: for step s, iteration it (0 = after the predict) and

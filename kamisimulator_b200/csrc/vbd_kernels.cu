@@ -61,10 +61,13 @@ __device__ __forceinline__ SegData seg_data(const DeviceState& st, const float4*
 
 // Position sweep.  COLOUR2: threads cover the rows of one colour (k = 2r + colour), read and
 // write dx in place.  JACOBI: threads cover every row, read dx_in and write dx_out.
+// Tied vertices (st.conn): the connection spring of cosseratItr (cosserat.cu:123-131), stiffness 40,
+// to the partner's position at the start of the step (positions do not move within it) and the
+// partner's dx in conn_dx, the iteration's starting values.
 template <bool JACOBI>
 __global__ void sweep_position_kernel(DeviceState st, const float4* __restrict__ y4, const float4* __restrict__ qcur,
                                       const float4* dx_in, float4* dx_out, const StepParams* __restrict__ spp,
-                                      PhysParams pp, int C, int colour, int64_t num_threads) {
+                                      PhysParams pp, int C, int colour, int64_t num_threads, const float4* conn_dx) {
     int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= num_threads) return;
     int rows = JACOBI ? C : C / 2;
@@ -97,9 +100,20 @@ __global__ void sweep_position_kernel(DeviceState st, const float4* __restrict__
         sp = seg_data(st, qcur, gp, g, st.prm[gp]);
         dxp = xyz(dx_in[gp]);
     }
-    BlockConst bc = vbd_block_const(xm.w, fl, sn.dd, sp.dd, h, damp);
-    float3 nd = vbd_position(dx, xyz(y4[g]), fl, bc, sn.e, sn.invl, sn.kk, sn.dd, sn.d3, dxn, sp.e, sp.invl, sp.kk,
-                             sp.dd, sp.d3, dxp, damp, pp.accel_ratio);
+    const int64_t tie = st.conn ? st.conn[g] : -1;
+    float3 nd;
+    if (tie >= 0) {
+        constexpr float k_tie = 4e1f;  // cosserat.cu:125
+        const BlockConst bc = vbd_block_const_tied(xm.w, fl, sn.dd, sp.dd, h, damp, k_tie);
+        const float3 f0 = bc.a * (xyz(y4[g]) - dx) -
+                          k_tie * ((xyz(xm) - xyz(st.xm[tie])) + (dx - xyz(conn_dx[tie])) + damp * dx);
+        nd = vbd_position_from(f0, dx, fl, bc, sn.e, sn.invl, sn.kk, sn.dd, sn.d3, dxn, sp.e, sp.invl, sp.kk, sp.dd,
+                               sp.d3, dxp, damp, pp.accel_ratio);
+    } else {
+        const BlockConst bc = vbd_block_const(xm.w, fl, sn.dd, sp.dd, h, damp);
+        nd = vbd_position(dx, xyz(y4[g]), fl, bc, sn.e, sn.invl, sn.kk, sn.dd, sn.d3, dxn, sp.e, sp.invl, sp.kk, sp.dd,
+                          sp.d3, dxp, damp, pp.accel_ratio);
+    }
     dx_out[g] = make_float4(nd.x, nd.y, nd.z, 0.f);
 }
 
@@ -208,12 +222,15 @@ cudaError_t launch_sweep_predict(const DeviceState& st, float4* y4, float4* dx4,
 
 cudaError_t launch_sweep_position(const DeviceState& st, const float4* y4, const float4* q, const float4* dx_in,
                                   float4* dx_out, const StepParams* d_sp, const PhysParams& pp, int C, int colour,
-                                  bool jacobi, cudaStream_t s) {
+                                  bool jacobi, cudaStream_t s, const float4* conn_dx) {
+    if (st.conn && !conn_dx) return cudaErrorInvalidValue;
     int64_t n = st.num_tiles * 32LL * (jacobi ? C : C / 2);
     if (jacobi)
-        sweep_position_kernel<true><<<blocks_for(n, 256), 256, 0, s>>>(st, y4, q, dx_in, dx_out, d_sp, pp, C, colour, n);
+        sweep_position_kernel<true><<<blocks_for(n, 256), 256, 0, s>>>(st, y4, q, dx_in, dx_out, d_sp, pp, C, colour, n,
+                                                                       conn_dx);
     else
-        sweep_position_kernel<false><<<blocks_for(n, 256), 256, 0, s>>>(st, y4, q, dx_in, dx_out, d_sp, pp, C, colour, n);
+        sweep_position_kernel<false><<<blocks_for(n, 256), 256, 0, s>>>(st, y4, q, dx_in, dx_out, d_sp, pp, C, colour,
+                                                                        n, conn_dx);
     return cudaGetLastError();
 }
 

@@ -9,9 +9,10 @@ namespace kami {
 
 cudaError_t launch_sweep_predict(const DeviceState& st, float4* y4, float4* dx4, const StepParams* d_sp,
                                  const PhysParams& pp, int64_t num_slots, cudaStream_t s);
+// conn_dx: the partners' dx for tied vertices (st.conn), the iteration's starting values
 cudaError_t launch_sweep_position(const DeviceState& st, const float4* y4, const float4* q, const float4* dx_in,
                                   float4* dx_out, const StepParams* d_sp, const PhysParams& pp, int C, int colour,
-                                  bool jacobi, cudaStream_t s);
+                                  bool jacobi, cudaStream_t s, const float4* conn_dx = nullptr);
 cudaError_t launch_sweep_orientation(const DeviceState& st, const float4* dx4, const float4* q_in, float4* q_out, int C,
                                      int colour, bool jacobi, cudaStream_t s);
 cudaError_t launch_sweep_finish(const DeviceState& st, const float4* dx4, const StepParams* d_sp, const PhysParams& pp,

@@ -65,16 +65,31 @@ __device__ __forceinline__ BlockConst vbd_block_const(float inv_mass, uint32_t f
     return b;
 }
 
+// vbd_block_const for a vertex tied by a connection spring of stiffness k_tie: k_tie (1 + damp) on
+// the diagonal, added before the segments' terms as cosseratItr adds it (cosserat.cu:130).
+__device__ __forceinline__ BlockConst vbd_block_const_tied(float inv_mass, uint32_t fl, float dd_next, float dd_prev,
+                                                           float h, float damp, float k_tie) {
+    BlockConst b;
+    b.a = 1.f / (inv_mass * h * h);
+    float s = k_tie * (1.f + damp);
+    if (fl & F_HAS_NEXT) s += dd_next * (1.f + damp);
+    if (fl & F_HAS_PREV) s += dd_prev * (1.f + damp);
+    b.inv_s = 1.f / s;
+    b.inv_s3a = 1.f / (s + 3.f * b.a);
+    return b;
+}
+
 // Position block solve of one vertex: cosseratItr, YarnBall/sim/cosserat.cu:112-161 and
 // :254-285, without the hair-hair collision terms (:163-227) and with the step limit at
 // infinity (recomputeStepLimitKernel<false,*>, collision.cu:95-131).
 //   segment i   (next): e_n = x_{i+1} - x_i, 1/l, k = kStretch/l, d = k/l, d3 = q_i e_x q_i*
 //   segment i-1 (prev): the same for the previous segment.
-__device__ __forceinline__ float3 vbd_position(float3 dx, float3 y, uint32_t fl, BlockConst bc, float3 e_n, float invl_n,
-                                               float kk_n, float dd_n, float3 d3_n, float3 dx_next, float3 e_p,
-                                               float invl_p, float kk_p, float dd_p, float3 d3_p, float3 dx_prev,
-                                               float damp, float accel) {
-    float3 f = bc.a * (y - dx);
+// vbd_position_from starts from the force f: the inertial force bc.a (y - dx), to which a tied
+// vertex has added its connection spring's force.
+__device__ __forceinline__ float3 vbd_position_from(float3 f, float3 dx, uint32_t fl, BlockConst bc, float3 e_n,
+                                                    float invl_n, float kk_n, float dd_n, float3 d3_n, float3 dx_next,
+                                                    float3 e_p, float invl_p, float kk_p, float dd_p, float3 d3_p,
+                                                    float3 dx_prev, float damp, float accel) {
     if (fl & F_HAS_NEXT) {
         float3 c = (e_n + (dx_next - dx)) * invl_n - d3_n;
         f = f + (kk_n * c - (damp * dd_n) * dx);
@@ -87,6 +102,13 @@ __device__ __forceinline__ float3 vbd_position(float3 dx, float3 y, uint32_t fl,
     float mb = m * bc.inv_s3a;
     float3 delta = f3((f.x - m) * bc.inv_s + mb, (f.y - m) * bc.inv_s + mb, (f.z - m) * bc.inv_s + mb);
     return dx + accel * delta;
+}
+__device__ __forceinline__ float3 vbd_position(float3 dx, float3 y, uint32_t fl, BlockConst bc, float3 e_n, float invl_n,
+                                               float kk_n, float dd_n, float3 d3_n, float3 dx_next, float3 e_p,
+                                               float invl_p, float kk_p, float dd_p, float3 d3_p, float3 dx_prev,
+                                               float damp, float accel) {
+    return vbd_position_from(bc.a * (y - dx), dx, fl, bc, e_n, invl_n, kk_n, dd_n, d3_n, dx_next, e_p, invl_p, kk_p,
+                             dd_p, d3_p, dx_prev, damp, accel);
 }
 
 // Closed-form segment orientation: quaternionLambdaItr, YarnBall/sim/cosserat.cu:290-337

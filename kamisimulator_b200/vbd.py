@@ -99,6 +99,7 @@ class Desc(ctypes.Structure):
         ("step_limit", ctypes.c_int32),
         ("velocity_radius", ctypes.c_int32),
         ("sag_free_itr", ctypes.c_int32),
+        ("connection_index", ctypes.c_void_p),
     ]
 
 
@@ -218,15 +219,19 @@ class Solver:
                  velocities=None, device=-1, slots_per_lane=0, warps_per_block=0, hair_hair=False,
                  barrier_thickness=None, k_collision=None, k_friction=None, friction_coeff=None,
                  detection_scaler=None, detection_period=None, step_limit=None, velocity_radius=None,
-                 sag_free_itr=0):
+                 sag_free_itr=0, connection_index=None):
         """groom: one groom (kami_vbd_create) or a list of grooms (kami_vbd_batch_create, one handle
-        stepping all of them; velocities is then None or a list with one entry per groom)."""
+        stepping all of them; velocities and connection_index are then None or lists with one entry
+        per groom).  connection_index: per vertex, the vertex of the same groom it is tied to by a
+        connection spring (Vertex::connectionIndex), or -1."""
         self.lib = load_library()
         self._h = None
         self._tape_rollout = None  # the autograd rollout whose steps the tape holds (autograd.py)
         grooms = list(groom) if isinstance(groom, (list, tuple)) else [groom]
         if velocities is None or not isinstance(groom, (list, tuple)):
             velocities = [velocities] * len(grooms)
+        if connection_index is None or not isinstance(groom, (list, tuple)):
+            connection_index = [connection_index] * len(grooms)
         keep = []
         sdf_ptr = None
         if sdf is not None:
@@ -242,7 +247,7 @@ class Solver:
             keep += [phi, grad, sd_]
             sdf_ptr = ctypes.pointer(sd_)
         descs = (Desc * len(grooms))()
-        for d, g, v in zip(descs, grooms, velocities):
+        for d, g, v, ci in zip(descs, grooms, velocities, connection_index):
             sb = np.ascontiguousarray(g.strand_begin, np.int32)
             pos = _f32(g.positions)
             vel = None if v is None else _f32(v)
@@ -275,6 +280,12 @@ class Solver:
             d.sdf = sdf_ptr
             d.hair_hair = int(bool(hair_hair))
             d.sag_free_itr = int(sag_free_itr)
+            if ci is not None:
+                ci = np.ascontiguousarray(ci, np.int32)
+                if ci.shape != (g.num_vertices,):
+                    raise ValueError("connection_index needs one entry per vertex")
+                keep.append(ci)
+                d.connection_index = ci.ctypes.data
             for name, val in (("barrier_thickness", barrier_thickness), ("k_collision", k_collision),
                               ("k_friction", k_friction), ("friction_coeff", friction_coeff),
                               ("detection_scaler", detection_scaler), ("detection_period", detection_period),

@@ -26,6 +26,9 @@
 //   schedule 0 "colour2": Gauss-Seidel over a 2-colouring by local index parity
 //                         within each strand: even vertices, odd vertices, then
 //                         even segments, odd segments.
+// Vertices in another vertex's update that other threads may be writing -- hair-hair
+// partners and connection-spring partners -- are read as they stood at the start of the
+// iteration (a snapshot) under both schedules.
 #include <cmath>
 #include <cstdint>
 #include <cstring>
@@ -232,6 +235,8 @@ typedef struct oracle_params {
     int32_t detection_period; // detectionPeriod
     int32_t step_limit;       // useStepSizeLimit
     int32_t velocity_radius;  // useVelocityRadius
+    // Vertex::connectionIndex (YarnBall.h:56): per vertex the vertex it is tied to, or -1; null = none
+    const int32_t* connection;
 } oracle_params;
 
 }  // extern "C"
@@ -558,6 +563,17 @@ V3<T> positionUpdate(const StepCtx<T>& c, const T* dxr, int64_t i, T h) {
     T inert = T(1) / (c.im[i] * h * h);
     for (int k = 0; k < 6; k++) H[k] = inert;  // hess3(float) fills all six entries (SymMat.h:16-18)
     V3<T> f = (T(1) / (h * h * c.im[i])) * (ld3(c.y.data(), i) - vi_dx);
+    if (c.p->connection && c.p->connection[i] >= 0) {
+        // the connection spring (cosserat.cu:123-131) to the partner's position at the start of the
+        // step (x does not move within it) and its dx at the start of the iteration (the snapshot)
+        const int64_t j = c.p->connection[i];
+        const T stiffness = T(4e1);
+        f = f - stiffness * ((ld3(c.x, i) - ld3(c.x, j)) + (vi_dx - ld3(c.snap.data(), j)) + damping * vi_dx);
+        const T d = stiffness * (1 + damping);
+        H[0] += d;
+        H[1] += d;
+        H[2] += d;
+    }
     T stepLimit = std::numeric_limits<T>::infinity();
     if (c.fl[i] & HAS_NEXT) {  // segment i, as thread i computes it (:141-161)
         V3<T> xi = ld3(c.x, i), xj = ld3(c.x, i + 1), vj_dx = ld3(dxr, i + 1);
@@ -758,7 +774,7 @@ int advanceT(const oracle_params* p, int64_t nv, int32_t ns, const int32_t* sb, 
             recomputeStepLimit(c);
         }
         for (int it = 0; it < p->num_itr; it++) {
-            if (p->hair_hair) c.snap = c.dx;  // partner dx of this iteration (both schedules)
+            if (p->hair_hair || p->connection) c.snap = c.dx;  // partner dx of this iteration (both schedules)
             if (p->schedule == 1) {
 #pragma omp parallel for schedule(static)
                 for (int64_t i = 0; i < nv; i++) st3(c.dxNew.data(), i, positionUpdate(c, c.dx.data(), i, h));

@@ -60,6 +60,7 @@ class OracleParams(ctypes.Structure):
         ("detection_period", ctypes.c_int32),
         ("step_limit", ctypes.c_int32),
         ("velocity_radius", ctypes.c_int32),
+        ("connection", ctypes.c_void_p),
     ]
 
 
@@ -136,9 +137,11 @@ class OracleSim:
                  schedule="colour2", sdf=None, body_rot=(0.0, 0.0, 0.0, 1.0), body_trans=(0.0, 0.0, 0.0),
                  stiffness_mode=0, k_stretch=3e3, k_bend=6e-4, pin_roots=True, dtype=np.float32, num_threads=0,
                  velocities=None, hair_hair=False, barrier_thickness=7.6e-5, k_collision=1e-5, k_friction=5.0,
-                 friction_coeff=0.1, detection_scaler=1.2, detection_period=1, step_limit=None, velocity_radius=True):
+                 friction_coeff=0.1, detection_scaler=1.2, detection_period=1, step_limit=None, velocity_radius=True,
+                 connection_index=None):
         """hair_hair: the hair-hair collision path (EnableHairHairColl); step_limit defaults to it, as
-        StableCosseratRodsSolver sets useStepSizeLimit = EnableHairHairColl (.cpp:184)."""
+        StableCosseratRodsSolver sets useStepSizeLimit = EnableHairHairColl (.cpp:184).
+        connection_index: per vertex the vertex it is tied to by a connection spring, or -1."""
         self.dtype = dtype
         self.lib = load()
         self.groom = groom
@@ -183,6 +186,10 @@ class OracleSim:
         p.friction_coeff, p.detection_scaler, p.detection_period = friction_coeff, detection_scaler, detection_period
         p.step_limit = int(bool(hair_hair if step_limit is None else step_limit))
         p.velocity_radius = int(bool(velocity_radius))
+        self._conn_keep = None
+        if connection_index is not None:
+            self._conn_keep = np.ascontiguousarray(connection_index, np.int32)
+            p.connection = self._conn_keep.ctypes.data
         self.params = p
 
     def set_body_transform(self, rot, trans):

@@ -102,6 +102,15 @@ int ref_material(void* h, float* inv_mass, float* l_rest, float* k_stretch, uint
     return 0;
 }
 
+// Sets every vertex's connectionIndex (YarnBall.h:56; -1: none), as glueEndpoints and the closed-curve
+// reader set it (jsonBuilder.cpp:165-185, reader.cpp:40-44), and uploads the vertices.
+int ref_set_connections(void* h, const int32_t* conn) {
+    auto& sim = ((Holder*)h)->sim;
+    for (int i = 0; i < sim->meta.numVerts; i++) sim->verts[i].connectionIndex = conn[i];
+    sim->upload();
+    return cudaDeviceSynchronize() == cudaSuccess ? 0 : 1;
+}
+
 // Overwrites positions, velocities, last velocities, orientations and the clock.
 int ref_set_state(void* h, const float* x, const float* v, const float* vlast, const float* q, const float* clock) {
     auto& sim = ((Holder*)h)->sim;

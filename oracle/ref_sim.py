@@ -37,7 +37,9 @@ def load():
         lib.ref_download.argtypes = [vp, vp, vp, vp]
         lib.ref_sdf_project.argtypes = [i64, vp, vp, vp, vp, vp, vp, f32, vp, vp, vp, vp]
         lib.ref_strain_limit.argtypes = [i32, vp, vp, f32, vp]
-        for n in ("ref_material", "ref_set_state", "ref_advance", "ref_download", "ref_sdf_project", "ref_strain_limit"):
+        lib.ref_set_connections.argtypes = [vp, vp]
+        for n in ("ref_material", "ref_set_state", "ref_advance", "ref_download", "ref_sdf_project", "ref_strain_limit",
+                  "ref_set_connections"):
             getattr(lib, n).restype = ctypes.c_int
         _lib = lib
     return _lib
@@ -97,6 +99,12 @@ class RefSim:
     def advance(self, dt):
         if self.lib.ref_advance(self.h, dt) != 0:
             raise RuntimeError("ref_advance failed")
+
+    def set_connections(self, connection_index):
+        """Vertex::connectionIndex of every vertex (-1: none)."""
+        c = np.ascontiguousarray(connection_index, np.int32)
+        if self.lib.ref_set_connections(self.h, _p(c)) != 0:
+            raise RuntimeError("ref_set_connections failed")
 
     def download(self):
         x = np.zeros((self.nv, 3), np.float32)
