@@ -165,10 +165,8 @@ __global__ void __launch_bounds__(32 * kQueryWarps) coll_query_kernel(DeviceStat
         beg = cp.start[h];
         cnt = cp.count[h];
     }
-    for (int o = 0; o < 27; o++) {  // a bucket that a lower lane holds too is dropped
-        const uint32_t ho = __shfl_sync(0xffffffffu, h, o);
-        if (o < lane && ho == h) cnt = 0;
-    }
+    // a bucket that a lower lane holds too is dropped: the lanes holding the same bucket, by one match
+    if (__match_any_sync(0xffffffffu, h) & ((1u << lane) - 1u)) cnt = 0;
     int32_t inc = cnt;  // inclusive prefix sum of the bucket sizes
     for (int o = 1; o < 32; o <<= 1) {
         const int32_t v = __shfl_up_sync(0xffffffffu, inc, o);
