@@ -150,9 +150,10 @@ typedef struct kami_vbd_desc {
      * host, one entry per vertex: the vertex of the same groom it is tied to (both ways for a mutual
      * tie), or -1; NULL = none.  The partner's displacement is read as it stood at the start of the
      * iteration (colour2: a snapshot taken per iteration, as hair-hair partners are; jacobi: the
-     * previous iterate), where the reference reads it while other threads write it.  Handles with a
-     * tie run on the sweep form (form AUTO picks it; FUSED, hair_hair and a later change of the tile
-     * shape are KAMI_ERR_UNSUPPORTED). */
+     * previous iterate), where the reference reads it while other threads write it.  With hair-hair
+     * collision, a pair of segments joined by a tie is not a contact (collision.cu:47-48; tested
+     * from either segment).  Handles with a tie run on the sweep form (form AUTO picks it; FUSED and
+     * a later change of the tile shape are KAMI_ERR_UNSUPPORTED). */
     const int32_t* connection_index;
 } kami_vbd_desc;
 

@@ -435,8 +435,6 @@ static kami_status validate_desc(const kami_vbd_desc* d) {
                             "connection_index[%d] = %d: must be -1 or another vertex of the groom (0..%d)", i, c, nv - 1);
             tied |= c >= 0;
         }
-        if (tied && d->hair_hair)
-            return fail(KAMI_ERR_UNSUPPORTED, "connection springs together with hair-hair collision are not supported");
         if (tied && d->form == KAMI_FORM_FUSED)
             return fail(KAMI_ERR_UNSUPPORTED, "connection springs run on the sweep form (a tie may join two tiles)");
     }
@@ -539,7 +537,7 @@ static kami_status setup_collisions(kami_vbd_solver* h, const kami_vbd_desc* d) 
     if (e == cudaSuccess) e = dalloc(&c.sbmax, S);
     if (e == cudaSuccess) e = dalloc(&c.ext_bits, 1);
     if (e == cudaSuccess) e = dalloc(&c.scan_tmp, coll_scan_tmp_size(table));
-    if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_COLOUR2) e = dalloc(&h->d_snap, S);
+    if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_COLOUR2 && !h->d_snap) e = dalloc(&h->d_snap, S);
     if (e != cudaSuccess) return cuda_fail(e, "allocating hair-hair collision arrays");
     e = cudaMemcpy(dvid, vid.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice);
     if (e == cudaSuccess) e = cudaMemcpy(dgid, gid.data(), sizeof(int32_t) * S, cudaMemcpyHostToDevice);

@@ -183,7 +183,8 @@ __global__ void __launch_bounds__(32 * kQueryWarps) coll_query_kernel(DeviceStat
     const float4 loa = cp.bmin[g], hia = cp.bmax[g];
     const int32_t va = cp.vid[g], ga = cp.gid[g];
     const float slack = 1e-3f * cell_size(cp);  // box overlap is a pre-filter: never reject a pair the distance test keeps
-    const float3 xa0 = xyz(st.xm[g]), xa1 = xyz(st.xm[next_slot(g, cp.C)]);
+    const int64_t ga1 = next_slot(g, cp.C);
+    const float3 xa0 = xyz(st.xm[g]), xa1 = xyz(st.xm[ga1]);
     int n = 0;  // accepted so far (uniform)
     for (int32_t t0 = 0; t0 < total; t0 += 32) {
         const int32_t t = t0 + lane;
@@ -200,7 +201,14 @@ __global__ void __launch_bounds__(32 * kQueryWarps) coll_query_kernel(DeviceStat
             const int4 rec = cp.srec[k];
             j = rec.x;
             vb = rec.y;
-            if (j != g && rec.z == ga && abs(vb - va) > 2) {
+            bool glued = false;
+            if (st.conn && j != g) {  // glued pairs are exempt (collision.cu:47-48), tested from either segment
+                const int64_t ja = next_slot(j, cp.C), ta0 = st.conn[g], ta1 = st.conn[ga1], tb0 = st.conn[j],
+                              tb1 = st.conn[ja];
+                glued = ta0 == j || ta1 == j || ta0 == ja || ta1 == ja || tb0 == g || tb1 == g || tb0 == ga1 ||
+                        tb1 == ga1;
+            }
+            if (j != g && rec.z == ga && abs(vb - va) > 2 && !glued) {
                 const float4 lob = cp.sbmin[k], hib = cp.sbmax[k];
                 if (!(lob.x > hia.x + slack || loa.x > hib.x + slack || lob.y > hia.y + slack ||
                       loa.y > hib.y + slack || lob.z > hia.z + slack || loa.z > hib.z + slack)) {
@@ -435,6 +443,17 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
 #pragma unroll
     for (int n = 0; n < 6; n++) H[n] = inert;  // hess3(float) fills all six entries (SymMat.h:16-18)
     float3 f = (1.f / (h * h * im)) * (yv - vi_dx);
+    if (st.conn) {
+        const int64_t t = st.conn[g];
+        if (t >= 0) {  // connection spring (cosserat.cu:123-131), the partner's dx from `snap`
+            constexpr float k_tie = 4e1f;
+            f = f - k_tie * ((vi - xyz(st.xm[t])) + (vi_dx - xyz(__ldcg(snap + t))) + damp * vi_dx);
+            const float d = k_tie * (1.f + damp);
+            H[0] += d;
+            H[1] += d;
+            H[2] += d;
+        }
+    }
     float step_limit = INFINITY;
     if (fl & F_HAS_NEXT) {
         const float invl = 1.f / prm.x;

@@ -413,6 +413,12 @@ int detectCollisions(StepCtx<T>& c) {
         for (int64_t j = 0; j < nv; j++) {
             if (j == i || !(c.fl[j] & HAS_NEXT) || std::llabs(j - i) <= 2) continue;
             const int64_t a = std::min(i, j), b = std::max(i, j);
+            if (p->connection) {  // glued pairs are exempt (collision.cu:47-48), tested from either segment
+                const int32_t* t = p->connection;
+                if (t[a] == b || t[a + 1] == b || t[a] == b + 1 || t[a + 1] == b + 1 || t[b] == a || t[b + 1] == a ||
+                    t[b] == a + 1 || t[b + 1] == a + 1)
+                    continue;
+            }
             V3<T> a0 = ld3(c.x, a);
             V3<T> A1 = ld3(c.x, a + 1) - a0, B0 = ld3(c.x, b) - a0, B1 = ld3(c.x, b + 1) - a0;
             T u, w;

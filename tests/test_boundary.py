@@ -200,8 +200,8 @@ def test_noalloc_rejects_bad_dt_before_touching_a_device():
 
 
 def test_connection_indices_are_checked_before_any_device_work():
-    """connection_index entries must be -1 or another vertex of the groom; a tie cannot be combined
-    with hair-hair collision or the fused form (1 = KAMI_ERR_INVALID_ARGUMENT, 6 = KAMI_ERR_UNSUPPORTED)."""
+    """connection_index entries must be -1 or another vertex of the groom; a tie cannot run on the
+    fused form (1 = KAMI_ERR_INVALID_ARGUMENT, 6 = KAMI_ERR_UNSUPPORTED)."""
     g = synth.cantilever(2, 8)
     keep = []
     for bad in (8 * 2, -2):
@@ -221,11 +221,8 @@ def test_connection_indices_are_checked_before_any_device_work():
     conn = np.full(g.num_vertices, -1, np.int32)
     conn[7], conn[15] = 15, 7
     keep.append(conn)
-    for field, value in (("hair_hair", 1), ("form", 2)):
-        d = _desc(g, keep)
-        d.connection_index = conn.ctypes.data
-        setattr(d, field, value)
-        if field == "hair_hair":
-            d.barrier_thickness = 1e-6
-        rc, msg = _create(d)
-        assert rc == 6 and "connection" in msg, msg
+    d = _desc(g, keep)
+    d.connection_index = conn.ctypes.data
+    d.form = 2  # KAMI_FORM_FUSED
+    rc, msg = _create(d)
+    assert rc == 6 and "connection" in msg, msg

@@ -118,3 +118,82 @@ def test_connection_springs_take_the_sweep_form_and_are_refused_elsewhere():
         plain.tape_reserve(1)
     finally:
         plain.close()
+
+
+def _tied_drape():
+    """The soft strand falling onto the stiff one, the two middle vertices tied to each other: the
+    spring pulls the crossing together, and the segments around the tie are exempt from contact
+    (collision.cu:47-48) while the rest of the drape still lands on the bar."""
+    g = synth.bar_and_drape(verts=16, gap=6e-5, bar_young=3e-5, drape_young=3e-5)
+    conn = np.full(g.num_vertices, -1, np.int32)
+    conn[8], conn[16 + 8] = 16 + 8, 8
+    v0 = np.zeros((g.num_vertices, 3), np.float32)
+    v0[16:, 2] = -0.02
+    return g, conn, v0
+
+
+@pytest.mark.parametrize("schedule", ["colour2", "jacobi"])
+def test_connection_springs_with_hair_hair_contacts_match_the_oracle(schedule):
+    g, conn, v0 = _tied_drape()
+    st = dict(num_itr=10, max_h=1 / 120, gravity=(0.0, 0.0, -2.0), radius=2e-6, schedule=schedule, hair_hair=True,
+              barrier_thickness=7.6e-5)
+    o = helpers.oracle_sim(g, dict(st, connection_index=conn), np.float32, v0)
+    untied = helpers.oracle_sim(g, st, np.float32, v0)
+    s = helpers.gpu_solver(g, dict(st, connection_index=conn), form="sweep", velocities=v0)
+    worst_x = worst_t = effect = 0.0
+    try:
+        for f in range(8):
+            if f > 0:
+                s.set_state(_state_from(o))
+                untied.load_state(o.state())
+            o.advance(1 / 120)
+            untied.advance(1 / 120)
+            s.step(1 / 120)
+            x, _ = s.get_positions_velocities()
+            worst_x = max(worst_x, float(np.abs(x - o.x).max()))
+            worst_t = max(worst_t, float(np.abs(orc.twist_angles(o.q, s.get_orientations())).max()))
+            effect = max(effect, float(np.abs(untied.x - o.x).max()))
+    finally:
+        s.close()
+    assert effect > 1e-5  # the tie changes the motion
+    assert worst_x <= POS_TOL and worst_t <= TWIST_TOL, (worst_x, worst_t)
+
+
+@pytest.mark.skipif(not ref_sim.available(), reason="oracle/_ref not built (needs the reference sources)")
+def test_connection_springs_with_hair_hair_contacts_match_the_reference_kernels():
+    """The reference's own hair-hair kernels (its detection with the glued-pair exemption, the
+    contact terms and the connection spring of cosseratItr) with the same connectionIndex, against
+    this solver's Jacobi sweep form, per step from the oracle's state."""
+    g, conn, v0 = _tied_drape()
+    st = dict(num_itr=10, max_h=1 / 120, gravity=(0.0, 0.0, -2.0), radius=2e-6, schedule="jacobi", hair_hair=True,
+              barrier_thickness=7.6e-5)
+    o = helpers.oracle_sim(g, dict(st, connection_index=conn), np.float32, v0)
+    s = helpers.gpu_solver(g, dict(st, connection_index=conn), form="sweep")
+    refs = [ref_sim.RefSim(g, young=3e-5, radius=2e-6, num_itr=10, max_h=1 / 120, gravity=(0.0, 0.0, -2.0))
+            for _ in range(2)]
+    worst = dict(oracle=0.0, ours=0.0, spread=0.0, twist=0.0)
+    try:
+        for r in refs:
+            r.set_connections(conn)
+        for _ in range(6):
+            state = (o.x.copy(), o.v.copy(), o.v_last.copy(), o.q.copy(), o.clock.copy())
+            outs = []
+            for r in refs:
+                r.set_state(*state[:4], state[4][:3])
+                assert r.step_hair_hair(1 / 120, 7.6e-5) == 0
+                outs.append(r.download())
+            s.set_state(_state_from(o))
+            o.advance(1 / 120)
+            s.step(1 / 120)
+            (x0, _, q0), (x1, _, _) = outs
+            xs, _ = s.get_positions_velocities()
+            worst["spread"] = max(worst["spread"], float(np.abs(x0 - x1).max()))
+            worst["oracle"] = max(worst["oracle"], float(np.abs(o.x - x0).max()))
+            worst["ours"] = max(worst["ours"], float(np.abs(xs - x0).max()))
+            worst["twist"] = max(worst["twist"], float(np.abs(orc.twist_angles(q0, s.get_orientations())).max()))
+    finally:
+        for r in refs:
+            r.close()
+        s.close()
+    print("tied hair-hair reference pin", worst)
+    assert worst["oracle"] <= POS_TOL and worst["ours"] <= POS_TOL and worst["twist"] <= TWIST_TOL, worst
