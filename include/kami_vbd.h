@@ -341,7 +341,9 @@ kami_status kami_vbd_synchronize(kami_vbd_handle h);
  * 107-121).  Call it after kami_vbd_step, once per step, as the reference runs it once per
  * SolveNextStep; the reference's StrainError defaults to 0.1 (SDFBodyCollisionSolver.h:26).
  * strain_error must be finite and >= 0.  It has no adjoint: while the tape holds recorded steps it
- * returns KAMI_ERR_STATE.  Stream-ordered like kami_vbd_step. */
+ * returns KAMI_ERR_STATE.  Stream-ordered like kami_vbd_step.  The first call after creation or a
+ * change of the tile shape builds a table of 12 bytes per strand on the device (a synchronising
+ * allocation); later calls allocate nothing. */
 kami_status kami_vbd_strain_limit(kami_vbd_handle h, float strain_error, void* stream);
 
 /* Full dynamic state snapshot (positions, velocities, last velocities, orientations and the
