@@ -327,6 +327,11 @@ kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
                                                      c, false, s);
                 for (int c = 0; c < 2 && err == cudaSuccess; c++)
                     err = launch_sweep_orientation(st, dx_cur, q_cur, q_cur, C, c, false, s);
+            } else if (h->layout.K == 1 && sweep_iteration_supported(C) && h->d_snap) {
+                // the whole iteration in one launch, from dx_cur into the other of d_dx and d_snap
+                float4* other = dx_cur == h->d_dx ? h->d_snap : h->d_dx;
+                err = launch_sweep_iteration(st, h->d_y, q_cur, dx_cur, other, h->d_step, h->pp, C, s);
+                dx_cur = other;
             } else {
                 if (h->d_conn)  // the tied partners' dx at the start of the iteration
                     err = cudaMemcpyAsync(h->d_snap, dx_cur, b4, cudaMemcpyDeviceToDevice, s);
@@ -734,6 +739,8 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
         if (e == cudaSuccess) e = dalloc(&h->d_step, 1);
         if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_JACOBI) e = dalloc(&h->d_dx2, S);
         if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_JACOBI) e = dalloc(&h->d_q2, S);
+        // colour2: the other dx buffer of the one-launch iterations (and the partners' snapshot)
+        if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_COLOUR2) e = dalloc(&h->d_snap, S);
     }
     if (e != cudaSuccess) return bail(cuda_fail(e, "allocating solver state"));
     const size_t b4 = sizeof(float4) * S;
@@ -751,7 +758,6 @@ static kami_status create_impl(const kami_vbd_desc* descs, int32_t n, kami_vbd_h
             if (ties[i] >= 0) conn[h->layout.slot_of[i]] = h->layout.slot_of[ties[i]];
         e = dalloc(&h->d_conn, S);
         if (e == cudaSuccess) e = cudaMemcpy(h->d_conn, conn.data(), sizeof(int64_t) * S, cudaMemcpyHostToDevice);
-        if (e == cudaSuccess && h->schedule == KAMI_SCHEDULE_COLOUR2) e = dalloc(&h->d_snap, S);
     }
     if (e != cudaSuccess) return bail(cuda_fail(e, "uploading solver state"));
 
