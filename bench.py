@@ -285,7 +285,9 @@ def extra_forms(args, torch, stream, flush):
     n = max(20, args.steps // 20)
     ms = time_steps(s, n, stream, flush)
     out["plain_sweep"] = {"value": g.num_vertices * NUM_ITR * n / (ms / 1e3), "ms_per_step": ms / n,
-                          "what": "same groom, one kernel per colour sweep (4 per iteration) replayed from a CUDA graph"}
+                          "what": "same groom, the sweep form (the reference's sweep order: even and odd vertices, "
+                                  "then even and odd segments per iteration, one launch per iteration over tiles "
+                                  "in shared memory) replayed from a CUDA graph"}
     s.close()
 
     grooms = synth.batched_grooms(64)
