@@ -304,7 +304,12 @@ kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
         float4* q_cur = h->d_q;
         float4* q_alt = h->d_q2;
         for (int it = 0; it < h->pp.num_itr && err == cudaSuccess; it++) {
-            if (jac) {
+            if (jac && !h->hair_hair && h->layout.K == 1 && sweep_iteration_supported(C)) {
+                // the whole iteration in one launch: dx_cur -> dx_alt, q_cur -> q_alt
+                err = launch_sweep_iteration(st, h->d_y, q_cur, q_alt, dx_cur, dx_alt, h->d_step, h->pp, C, true, s);
+                std::swap(dx_cur, dx_alt);
+                std::swap(q_cur, q_alt);
+            } else if (jac) {
                 if (h->hair_hair)
                     err = launch_sweep_position_coll(st, h->d_y, q_cur, dx_cur, dx_alt, dx_cur, h->d_step, h->pp, h->cp, 0,
                                                      true, s);
@@ -330,7 +335,7 @@ kami_status build_sweep_graph(kami_vbd_solver* h, int substeps) {
             } else if (h->layout.K == 1 && sweep_iteration_supported(C) && h->d_snap) {
                 // the whole iteration in one launch, from dx_cur into the other of d_dx and d_snap
                 float4* other = dx_cur == h->d_dx ? h->d_snap : h->d_dx;
-                err = launch_sweep_iteration(st, h->d_y, q_cur, dx_cur, other, h->d_step, h->pp, C, s);
+                err = launch_sweep_iteration(st, h->d_y, q_cur, q_cur, dx_cur, other, h->d_step, h->pp, C, false, s);
                 dx_cur = other;
             } else {
                 if (h->d_conn)  // the tied partners' dx at the start of the iteration

@@ -265,20 +265,149 @@ __global__ void __launch_bounds__(512) sweep_iteration_kernel(DeviceState st, co
     }
 }
 
+// One Jacobi iteration of the sweep form in one launch, as sweep_iteration_kernel does colour2: every
+// position from the previous iterate, then every orientation from the new displacements and the
+// previous orientations (double-buffered in shared memory), as the two Jacobi launches
+// (sweep_position_kernel<true>, sweep_orientation_kernel<true>) do.  Tied partners' dx come from
+// dx_in, the previous iterate.  dx goes to dx_out, q to q_out.
+__global__ void __launch_bounds__(512) sweep_iteration_jacobi_kernel(DeviceState st, const float4* __restrict__ y4,
+                                                                     const float4* __restrict__ q_in,
+                                                                     float4* __restrict__ q_out,
+                                                                     const float4* __restrict__ dx_in,
+                                                                     float4* __restrict__ dx_out,
+                                                                     const StepParams* __restrict__ spp, PhysParams pp,
+                                                                     int C) {
+    extern __shared__ float4 sweep_tile[];  // x | dx | q | prm | qr | new dx | new q, T entries each
+    const int T = 32 * C;
+    float4* sx = sweep_tile;
+    float4* sdx = sx + T;
+    float4* sq = sdx + T;
+    float4* sprm = sq + T;
+    float4* sqr = sprm + T;
+    float4* sdx2 = sqr + T;
+    float4* sq2 = sdx2 + T;
+    const int lane = threadIdx.x & 31, row2 = (threadIdx.x >> 5) * 2;
+    const int64_t base = (int64_t)blockIdx.x * T;
+    float3 yown[2];
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const int p = (row2 + c) * 32 + lane;
+        const int64_t g = base + p;
+        sx[p] = st.xm[g];
+        sdx[p] = dx_in[g];
+        sq[p] = q_in[g];
+        sprm[p] = st.prm[g];
+        sqr[p] = st.qr[g];
+        yown[c] = xyz(y4[g]);
+    }
+    const float h = spp->h;
+    const float damp = pp.damping / h;
+    __syncthreads();
+    // (the updates are written out as in sweep_iteration_kernel, so that they compile to the same
+    // arithmetic as the per-sweep kernels)
+#pragma unroll
+    for (int c = 0; c < 2; c++) {  // every position from the previous iterate
+        const int p = (row2 + c) * 32 + lane;
+        const int64_t g = base + p;
+        const float4 prm = sprm[p], xm = sx[p];
+        const uint32_t fl = __float_as_uint(prm.w);
+        if ((fl & F_VALID) && xm.w != 0.f) {
+            const float3 dx = xyz(sdx[p]);
+            SegData sn{}, sp{};
+            float3 dxn = f3(0.f, 0.f, 0.f), dxp = f3(0.f, 0.f, 0.f);
+            if (fl & F_HAS_NEXT) {  // seg_data of the segment at g, from the tile
+                const int pn = (int)(next_slot(g, C) - base);
+                sn.e = xyz(sx[pn]) - xyz(xm);
+                sn.invl = 1.f / prm.x;
+                sn.kk = prm.y * sn.invl;
+                sn.dd = sn.kk * sn.invl;
+                sn.d3 = d3_of(sq[p]);
+                dxn = xyz(sdx[pn]);
+            }
+            if (fl & F_HAS_PREV) {
+                const int pq = (int)(prev_slot(g, C) - base);
+                const float4 pp4 = sprm[pq];
+                sp.e = xyz(xm) - xyz(sx[pq]);
+                sp.invl = 1.f / pp4.x;
+                sp.kk = pp4.y * sp.invl;
+                sp.dd = sp.kk * sp.invl;
+                sp.d3 = d3_of(sq[pq]);
+                dxp = xyz(sdx[pq]);
+            }
+            const int64_t tie = st.conn ? st.conn[g] : -1;
+            float3 nd;
+            if (tie >= 0) {  // as sweep_position_kernel: the partner's dx at the start of the iteration
+                constexpr float k_tie = 4e1f;  // cosserat.cu:125
+                const BlockConst bc = vbd_block_const_tied(xm.w, fl, sn.dd, sp.dd, h, damp, k_tie);
+                const float3 f0 = bc.a * (yown[c] - dx) -
+                                  k_tie * ((xyz(xm) - xyz(st.xm[tie])) + (dx - xyz(dx_in[tie])) + damp * dx);
+                nd = vbd_position_from(f0, dx, fl, bc, sn.e, sn.invl, sn.kk, sn.dd, sn.d3, dxn, sp.e, sp.invl, sp.kk,
+                                       sp.dd, sp.d3, dxp, damp, pp.accel_ratio);
+            } else {
+                const BlockConst bc = vbd_block_const(xm.w, fl, sn.dd, sp.dd, h, damp);
+                nd = vbd_position(dx, yown[c], fl, bc, sn.e, sn.invl, sn.kk, sn.dd, sn.d3, dxn, sp.e, sp.invl, sp.kk,
+                                  sp.dd, sp.d3, dxp, damp, pp.accel_ratio);
+            }
+            sdx2[p] = make_float4(nd.x, nd.y, nd.z, 0.f);
+        } else {
+            sdx2[p] = sdx[p];
+        }
+    }
+    __syncthreads();
+#pragma unroll
+    for (int c = 0; c < 2; c++) {  // every orientation from the new dx and the previous q
+        const int p = (row2 + c) * 32 + lane;
+        const int64_t g = base + p;
+        const float4 prm = sprm[p];
+        const uint32_t fl = __float_as_uint(prm.w);
+        if ((fl & F_HAS_NEXT) && !(fl & F_FIX_ORIENTATION)) {
+            const int pn = (int)(next_slot(g, C) - base);
+            const float4 unit = make_float4(0.f, 0.f, 0.f, 1.f);
+            float4 qp = unit, qrp = unit, qn = unit;
+            if (fl & F_HAS_PREV) {
+                const int pq = (int)(prev_slot(g, C) - base);
+                qp = sq[pq];
+                qrp = sqr[pq];
+            }
+            if (fl & F_HAS_NEXT_ORIENTATION) qn = sq[pn];
+            const float m2k = -2.f * prm.y * (1.f / prm.x);
+            sq2[p] = vbd_orientation(sq[p], fl, xyz(sx[pn]) - xyz(sx[p]), xyz(sdx2[p]), xyz(sdx2[pn]), m2k, qp, qrp, qn,
+                                     sqr[p]);
+        } else {
+            sq2[p] = sq[p];
+        }
+    }
+#pragma unroll
+    for (int c = 0; c < 2; c++) {
+        const int p = (row2 + c) * 32 + lane;
+        dx_out[base + p] = sdx2[p];
+        q_out[base + p] = sq2[p];
+    }
+}
+
 bool sweep_iteration_supported(int C) { return C % 2 == 0 && C >= 2 && 32 * C <= 1024; }
 
-cudaError_t launch_sweep_iteration(const DeviceState& st, const float4* y4, float4* q, const float4* dx_in,
-                                   float4* dx_out, const StepParams* d_sp, const PhysParams& pp, int C, cudaStream_t s) {
-    if (!sweep_iteration_supported(C) || !y4 || !q || !dx_in || !dx_out || dx_in == dx_out || !d_sp)
+cudaError_t launch_sweep_iteration(const DeviceState& st, const float4* y4, const float4* q_in, float4* q_out,
+                                   const float4* dx_in, float4* dx_out, const StepParams* d_sp, const PhysParams& pp,
+                                   int C, bool jacobi, cudaStream_t s) {
+    if (!sweep_iteration_supported(C) || !y4 || !q_in || !q_out || !dx_in || !dx_out || dx_in == dx_out || !d_sp)
         return cudaErrorInvalidValue;
+    if (jacobi == (q_in == q_out)) return cudaErrorInvalidValue;  // colour2 in place, jacobi into another buffer
     if (st.num_tiles == 0) return cudaSuccess;
     const int T = 32 * C;
-    const size_t smem = sizeof(float4) * 5 * T;
+    const size_t smem = sizeof(float4) * (jacobi ? 7 : 5) * T;
     if (smem > 48 * 1024) {  // the opt-in limit is set per device, so on every launch
-        cudaError_t e = cudaFuncSetAttribute(sweep_iteration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e = jacobi ? cudaFuncSetAttribute(sweep_iteration_jacobi_kernel,
+                                                      cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem)
+                               : cudaFuncSetAttribute(sweep_iteration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                                      (int)smem);
         if (e != cudaSuccess) return e;
     }
-    sweep_iteration_kernel<<<(unsigned)st.num_tiles, T / 2, smem, s>>>(st, y4, q, dx_in, dx_out, d_sp, pp, C);
+    if (jacobi)
+        sweep_iteration_jacobi_kernel<<<(unsigned)st.num_tiles, T / 2, smem, s>>>(st, y4, q_in, q_out, dx_in, dx_out,
+                                                                                  d_sp, pp, C);
+    else
+        sweep_iteration_kernel<<<(unsigned)st.num_tiles, T / 2, smem, s>>>(st, y4, q_out, dx_in, dx_out, d_sp, pp, C);
     return cudaGetLastError();
 }
 

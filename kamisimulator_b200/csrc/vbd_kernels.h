@@ -13,11 +13,13 @@ cudaError_t launch_sweep_predict(const DeviceState& st, float4* y4, float4* dx4,
 cudaError_t launch_sweep_position(const DeviceState& st, const float4* y4, const float4* q, const float4* dx_in,
                                   float4* dx_out, const StepParams* d_sp, const PhysParams& pp, int C, int colour,
                                   bool jacobi, cudaStream_t s, const float4* conn_dx = nullptr);
-// One colour2 iteration (both position sweeps, both orientation sweeps) in one launch, one block per
-// tile of up to 1024 slots: reads dx_in, writes dx_out, q in place (sweep_iteration_supported).
+// One iteration (colour2: both position sweeps, both orientation sweeps; jacobi: the position and
+// the orientation sweep) in one launch, one block per tile of up to 1024 slots: reads dx_in, writes
+// dx_out; q in place for colour2 (q_in == q_out), into q_out for jacobi (sweep_iteration_supported).
 bool sweep_iteration_supported(int C);
-cudaError_t launch_sweep_iteration(const DeviceState& st, const float4* y4, float4* q, const float4* dx_in,
-                                   float4* dx_out, const StepParams* d_sp, const PhysParams& pp, int C, cudaStream_t s);
+cudaError_t launch_sweep_iteration(const DeviceState& st, const float4* y4, const float4* q_in, float4* q_out,
+                                   const float4* dx_in, float4* dx_out, const StepParams* d_sp, const PhysParams& pp,
+                                   int C, bool jacobi, cudaStream_t s);
 cudaError_t launch_sweep_orientation(const DeviceState& st, const float4* dx4, const float4* q_in, float4* q_out, int C,
                                      int colour, bool jacobi, cudaStream_t s);
 cudaError_t launch_sweep_finish(const DeviceState& st, const float4* dx4, const StepParams* d_sp, const PhysParams& pp,

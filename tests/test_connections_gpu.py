@@ -197,3 +197,30 @@ def test_connection_springs_with_hair_hair_contacts_match_the_reference_kernels(
         s.close()
     print("tied hair-hair reference pin", worst)
     assert worst["oracle"] <= POS_TOL and worst["ours"] <= POS_TOL and worst["twist"] <= TWIST_TOL, worst
+
+
+def test_ties_in_a_batch_handle_are_per_groom():
+    """connection_index holds each groom's own vertex indices: two tied grooms in one batch handle step
+    as they do in two handles of their own, bit for bit."""
+    from kamisimulator_b200.vbd import Solver
+
+    g0, c0 = _scene()
+    g1 = synth.cantilever(3, 12, young=3.0)
+    c1 = np.full(g1.num_vertices, -1, np.int32)
+    c1[11], c1[23] = 23, 11  # the tips of the first two rods
+    st = dict(num_itr=12, max_h=1 / 120, gravity=(0.0, 0.0, -9.81), radius=40e-6)
+    b = Solver([g0, g1], connection_index=[c0, c1], **st)
+    s0 = Solver(g0, connection_index=c0, **st)
+    s1 = Solver(g1, connection_index=c1, **st)
+    try:
+        for _ in range(5):
+            b.step(1 / 120)
+            s0.step(1 / 120)
+            s1.step(1 / 120)
+        xb = b.get_positions_velocities()[0]
+        x0 = s0.get_positions_velocities()[0]
+        x1 = s1.get_positions_velocities()[0]
+    finally:
+        for s in (b, s0, s1):
+            s.close()
+    np.testing.assert_array_equal(xb, np.concatenate([x0, x1]))

@@ -1,7 +1,7 @@
-"""The sweep form's colour2 iteration in one launch (sweep_iteration_kernel, tiles of up to 1024
-slots) against the four launches per iteration (sweep_position_kernel and sweep_orientation_kernel,
-which tiles over 1024 slots keep): the same operands and arithmetic, so the same state bit for bit,
-with and without connection springs."""
+"""The sweep form's iteration in one launch (sweep_iteration_kernel, tiles of up to 1024 slots)
+against the per-sweep launches (sweep_position_kernel and sweep_orientation_kernel: four per
+colour2 iteration, two per Jacobi iteration, which tiles over 1024 slots keep): the same operands
+and arithmetic, so the same state bit for bit, with and without connection springs."""
 import numpy as np
 import pytest
 
@@ -11,10 +11,11 @@ from tests import helpers
 pytestmark = pytest.mark.gpu
 
 
+@pytest.mark.parametrize("schedule", ["colour2", "jacobi"])
 @pytest.mark.parametrize("tied", [False, True])
-def test_one_launch_iteration_equals_the_four_sweep_launches(tied):
+def test_one_launch_iteration_equals_the_sweep_launches(tied, schedule):
     g = helpers.soft_groom(200, (8, 60), seed=17)
-    st = helpers.soft_settings(sdf=synth.sphere_sdf(64, threshold=2e-3), num_itr=8, max_h=1 / 120)
+    st = helpers.soft_settings(sdf=synth.sphere_sdf(64, threshold=2e-3), num_itr=8, max_h=1 / 120, schedule=schedule)
     if tied:  # every strand's tip tied to the next strand's tip, both ways
         conn = np.full(g.num_vertices, -1, np.int32)
         tips = np.asarray(g.strand_begin[1:]) - 1
@@ -22,7 +23,7 @@ def test_one_launch_iteration_equals_the_four_sweep_launches(tied):
             conn[a], conn[b] = b, a
         st["connection_index"] = conn
     one = helpers.gpu_solver(g, dict(st, slots_per_lane=2), form="sweep")    # 64-slot tiles: one launch
-    four = helpers.gpu_solver(g, dict(st, slots_per_lane=34), form="sweep")  # 1088-slot tiles: four launches
+    four = helpers.gpu_solver(g, dict(st, slots_per_lane=34), form="sweep")  # 1088-slot tiles: per-sweep launches
     try:
         assert (one.slots_per_lane, four.slots_per_lane) == (2, 34)
         for _ in range(6):
