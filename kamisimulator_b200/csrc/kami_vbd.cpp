@@ -120,6 +120,8 @@ struct kami_vbd_solver {
     // the first call for the current tile layout
     int64_t* d_strand_root = nullptr;
     int32_t* d_strand_len = nullptr;
+    int32_t* d_strand_cta = nullptr;  // staged form: first strand (in root order) of each CTA's slot range
+    int32_t strain_ctas = 0, strain_slots_per_cta = 0;  // 0 CTAs: one thread per strand over global memory
 
     // device-resident Hair: padded entry of each boundary vertex, and a staging copy of a padded
     // array for host transfers
@@ -193,7 +195,8 @@ void release(kami_vbd_solver* h) {
     void* cptrs[] = {(void*)c.vid, (void*)c.gid, c.cols,   c.ncols,  c.maxstep,  c.bmin,    c.bmax,
                      c.cell,       c.count,      c.start,  c.cursor, c.srec,     c.sbmin,    c.sbmax,
                      c.ext_bits,   c.scan_tmp,
-                     h->d_snap,    h->d_hair_index, h->d_hair_stage, h->d_strand_root, h->d_strand_len, h->d_conn};
+                     h->d_snap,    h->d_hair_index, h->d_hair_stage, h->d_strand_root, h->d_strand_len, h->d_conn,
+                     h->d_strand_cta};
     for (void* p : cptrs)
         if (p) cudaFree(p);
     if (h->ev_a) cudaEventDestroy(h->ev_a);
@@ -1210,8 +1213,10 @@ static kami_status relayout(kami_vbd_solver* h, int C) {
     h->layout = nl;
     if (h->d_strand_root) cudaFree(h->d_strand_root);  // slots of the old layout
     if (h->d_strand_len) cudaFree(h->d_strand_len);
+    if (h->d_strand_cta) cudaFree(h->d_strand_cta);
     h->d_strand_root = nullptr;
     h->d_strand_len = nullptr;
+    h->d_strand_cta = nullptr;
     drop_graphs(h);
     if (e != cudaSuccess) return cuda_fail(e, "relayout scratch");
     return KAMI_OK;
@@ -1724,30 +1729,64 @@ kami_status kami_vbd_strain_limit(kami_vbd_handle h, float strain_error, void* s
         return fail(KAMI_ERR_STATE, "the tape holds recorded steps; strain limiting has no adjoint, run kami_vbd_backward "
                                     "first");
     if (!h->d_strand_root) {
+        // strands in the order of their root slots; the staged form gives each CTA a slot range of whole
+        // tile groups (at least 2,048 slots) and the strands rooted in it
+        std::vector<int32_t> order(h->ns);
+        for (int32_t k = 0; k < h->ns; k++) order[k] = k;
+        std::sort(order.begin(), order.end(), [&](int32_t a, int32_t b) {
+            return h->layout.slot_of[h->strand_begin[a]] < h->layout.slot_of[h->strand_begin[b]];
+        });
         std::vector<int64_t> root(h->ns);
         std::vector<int32_t> len(h->ns);
         for (int32_t k = 0; k < h->ns; k++) {
-            root[k] = h->layout.slot_of[h->strand_begin[k]];
-            len[k] = h->strand_begin[k + 1] - h->strand_begin[k];
+            root[k] = h->layout.slot_of[h->strand_begin[order[k]]];
+            len[k] = h->strand_begin[order[k] + 1] - h->strand_begin[order[k]];
+        }
+        const int64_t unit = 32LL * h->layout.C * std::max(1, h->layout.K);  // slots of a tile group
+        int64_t per_cta = unit * std::max<int64_t>(1, 2048 / unit);
+        std::vector<int32_t> cta;
+        if (per_cta <= kStrainStagedMaxSlots) {
+            const int64_t n_cta = (h->layout.num_slots + per_cta - 1) / per_cta;
+            cta.assign(n_cta + 1, 0);
+            int32_t k = 0;
+            for (int64_t c = 0; c <= n_cta; c++) {
+                while (k < h->ns && root[k] < c * per_cta) k++;
+                cta[c] = k;
+            }
+        } else {
+            per_cta = 0;
         }
         KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");
         cudaError_t e = dalloc(&h->d_strand_root, (size_t)h->ns);
         if (e == cudaSuccess) e = dalloc(&h->d_strand_len, (size_t)h->ns);
+        if (e == cudaSuccess && !cta.empty()) e = dalloc(&h->d_strand_cta, cta.size());
         if (e == cudaSuccess)
             e = cudaMemcpy(h->d_strand_root, root.data(), sizeof(int64_t) * h->ns, cudaMemcpyHostToDevice);
         if (e == cudaSuccess) e = cudaMemcpy(h->d_strand_len, len.data(), sizeof(int32_t) * h->ns, cudaMemcpyHostToDevice);
+        if (e == cudaSuccess && !cta.empty())
+            e = cudaMemcpy(h->d_strand_cta, cta.data(), sizeof(int32_t) * cta.size(), cudaMemcpyHostToDevice);
         if (e != cudaSuccess) {
             if (h->d_strand_root) cudaFree(h->d_strand_root);
             if (h->d_strand_len) cudaFree(h->d_strand_len);
+            if (h->d_strand_cta) cudaFree(h->d_strand_cta);
             h->d_strand_root = nullptr;
             h->d_strand_len = nullptr;
+            h->d_strand_cta = nullptr;
             return cuda_fail(e, "strain limiting strand table");
         }
+        h->strain_ctas = cta.empty() ? 0 : (int32_t)(cta.size() - 1);
+        h->strain_slots_per_cta = (int32_t)per_cta;
     }
     return on_stream(h, stream, [&](cudaStream_t s) -> kami_status {
-        KAMI_CUDA(launch_strain_limit(h->d_xm, h->d_prm, h->d_strand_root, h->d_strand_len, h->ns, h->layout.C,
-                                      strain_error, s),
-                  "strain limiting launch");
+        if (h->strain_ctas > 0)
+            KAMI_CUDA(launch_strain_limit_staged(h->d_xm, h->d_prm, h->d_strand_root, h->d_strand_len, h->d_strand_cta,
+                                                 h->strain_ctas, h->layout.num_slots, h->strain_slots_per_cta,
+                                                 h->layout.C, strain_error, s),
+                      "strain limiting launch");
+        else
+            KAMI_CUDA(launch_strain_limit(h->d_xm, h->d_prm, h->d_strand_root, h->d_strand_len, h->ns, h->layout.C,
+                                          strain_error, s),
+                      "strain limiting launch");
         return KAMI_OK;
     });
 }

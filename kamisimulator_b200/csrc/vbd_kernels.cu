@@ -547,6 +547,65 @@ __global__ void strain_limit_kernel(float4* xm, const float4* __restrict__ prm, 
     }
 }
 
+// The same march with the state staged in shared memory: CTA b owns slots [b S, (b + 1) S) of whole
+// tile groups (so every strand rooted there lies inside), loads their positions and rest lengths
+// with coalesced loads, marches the strands rooted there (cta_begin[b] .. cta_begin[b + 1] in
+// root_slot, ascending) in shared memory, one thread per strand, and writes the positions back.
+__global__ void __launch_bounds__(128) strain_limit_staged_kernel(float4* xm, const float4* __restrict__ prm,
+                                                                 const int64_t* __restrict__ root_slot,
+                                                                 const int32_t* __restrict__ strand_len,
+                                                                 const int32_t* __restrict__ cta_begin,
+                                                                 int64_t num_slots, int slots_per_cta, int C,
+                                                                 float strain_error) {
+    extern __shared__ float4 staged[];  // positions, then rest lengths
+    float* sl0 = reinterpret_cast<float*>(staged + slots_per_cta);
+    const int64_t s0 = (int64_t)blockIdx.x * slots_per_cta;  // a multiple of the tile size
+    const int n_here = (int)min((int64_t)slots_per_cta, num_slots - s0);
+    for (int i = threadIdx.x; i < n_here; i += blockDim.x) {
+        staged[i] = xm[s0 + i];
+        sl0[i] = prm[s0 + i].x;
+    }
+    __syncthreads();
+    for (int32_t k = cta_begin[blockIdx.x] + (int32_t)threadIdx.x; k < cta_begin[blockIdx.x + 1]; k += blockDim.x) {
+        const int32_t n = strand_len[k];
+        int64_t g = root_slot[k] - s0;  // local slots keep the tile arithmetic (s0 is tile-aligned)
+        float3 cur = xyz(staged[g]);
+        for (int32_t i = 0; i + 1 < n; i++) {
+            const int64_t gn = next_slot(g, C);
+            const float4 nx = staged[gn];
+            const float l0 = sl0[g];
+            const float3 pn = xyz(nx);
+            const float l = sqrtf(dot3(pn - cur, pn - cur));
+            if (fabsf(l - l0) > strain_error * l0) {
+                const float3 d = cur - pn;
+                const float3 dir = d * rsqrtf(dot3(d, d));
+                cur = pn + (l - l0) * dir;
+                staged[gn] = make_float4(cur.x, cur.y, cur.z, nx.w);
+            } else {
+                cur = pn;
+            }
+            g = gn;
+        }
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < n_here; i += blockDim.x) xm[s0 + i] = staged[i];
+}
+
+cudaError_t launch_strain_limit_staged(float4* xm, const float4* prm, const int64_t* root_slot,
+                                       const int32_t* strand_len, const int32_t* cta_begin, int32_t num_ctas,
+                                       int64_t num_slots, int slots_per_cta, int C, float strain_error, cudaStream_t s) {
+    if (num_ctas <= 0) return cudaSuccess;
+    const size_t smem = (sizeof(float4) + sizeof(float)) * (size_t)slots_per_cta;
+    if (smem > 48 * 1024) {  // the opt-in limit is set per device, so on every launch
+        cudaError_t e =
+            cudaFuncSetAttribute(strain_limit_staged_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        if (e != cudaSuccess) return e;
+    }
+    strain_limit_staged_kernel<<<(unsigned)num_ctas, 128, smem, s>>>(xm, prm, root_slot, strand_len, cta_begin,
+                                                                    num_slots, slots_per_cta, C, strain_error);
+    return cudaGetLastError();
+}
+
 cudaError_t launch_strain_limit(float4* xm, const float4* prm, const int64_t* root_slot, const int32_t* strand_len,
                                 int32_t num_strands, int C, float strain_error, cudaStream_t s) {
     if (num_strands <= 0) return cudaSuccess;

@@ -67,6 +67,13 @@ cudaError_t launch_sweep_position_coll(const DeviceState& st, const float4* y4, 
 // Strain limiting after the step (strain_limit_kernel): root slot and vertex count of each strand.
 cudaError_t launch_strain_limit(float4* xm, const float4* prm, const int64_t* root_slot, const int32_t* strand_len,
                                 int32_t num_strands, int C, float strain_error, cudaStream_t s);
+// The same with the state staged in shared memory (strain_limit_staged_kernel): slots_per_cta is a
+// multiple of the tile group (tiles_per_group x 32 C slots), root_slot ascending, cta_begin[num_ctas
+// + 1] the first strand of each CTA's slot range.
+constexpr int kStrainStagedMaxSlots = 11000;  // 20 B of shared memory per slot
+cudaError_t launch_strain_limit_staged(float4* xm, const float4* prm, const int64_t* root_slot,
+                                       const int32_t* strand_len, const int32_t* cta_begin, int32_t num_ctas,
+                                       int64_t num_slots, int slots_per_cta, int C, float strain_error, cudaStream_t s);
 
 // sag-free initialisation (sag_free.cu): `iterations` passes, one thread per strand; fs: a float per slot
 cudaError_t launch_sag_free(const DeviceState& st, float3 gravity, const int32_t* strand_begin, const int64_t* slot_of,
