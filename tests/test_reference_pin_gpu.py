@@ -178,3 +178,51 @@ def test_reference_gpu_speed_on_the_groom():
         s.close()
     print("reference GPU speed", out)
     assert out["ours_fused_jacobi_ms_per_step"] < ref_ms
+
+
+def test_batched_form_against_the_reference_per_groom_sims():
+    """The batched form against the reference's own plain per-groom GPU form: the 64 uneven grooms of
+    the batched workload (26.4 M vertices), each as one YarnBall::Sim built from the reference's
+    source and stepped in turn (CantileverTestSolver's pattern, CantileverTestSolver.cpp:106-111),
+    against one kami_vbd_batch_step handle over all of them.  Same settings on both sides: Jacobi, 20
+    iterations, one substep of 1/120 s, no SDF (the reference's Sim has no SDF pass).  Prints the
+    rates; the batched form must be at least 5x the reference's per-groom Sims."""
+    import time
+
+    from kamisimulator_b200.vbd import Solver
+
+    grooms = synth.batched_grooms(seed=3)
+    for g in grooms:
+        g.strand_young[:] = 2.0
+    nv = sum(g.num_vertices for g in grooms)
+    refs = [ref_sim.RefSim(g, young=2.0, num_itr=20, max_h=1 / 120) for g in grooms]
+    try:
+        for r in refs:
+            r.advance(1 / 120)
+        frames = 3
+        t0 = time.perf_counter()
+        for _ in range(frames):
+            for r in refs:
+                r.advance(1 / 120)  # returns after the reference's own stream synchronisation
+        ref_ms = (time.perf_counter() - t0) * 1e3 / frames
+    finally:
+        for r in refs:
+            r.close()
+    st = dict(num_itr=20, max_h=1 / 120, gravity=(0.0, 0.0, -9.81), radius=40e-6, schedule="jacobi")
+    b = Solver(grooms, **st)
+    try:
+        b.autotune(1 / 120, trial_steps=4)
+        b.batch_step(1 / 120, 4)
+        b.synchronize()
+        n = 24
+        t0 = time.perf_counter()
+        b.batch_step(1 / 120, n)
+        b.synchronize()
+        ours_ms = (time.perf_counter() - t0) * 1e3 / n
+    finally:
+        b.close()
+    out = {"vertices": nv, "reference_per_groom_ms_per_frame": ref_ms, "batched_ms_per_frame": ours_ms,
+           "reference_vertex_iters_per_s": nv * 20 / (ref_ms * 1e-3),
+           "batched_vertex_iters_per_s": nv * 20 / (ours_ms * 1e-3), "ratio": ref_ms / ours_ms}
+    print("batched vs the reference's per-groom Sims", out)
+    assert out["ratio"] >= 5.0, out
