@@ -271,8 +271,9 @@ def cpu_baseline_sample():
 
 
 def extra_forms(args, torch, stream, flush):
-    """Plain per-groom sweep form on the headline groom, batched vs plain per-groom handles on 64 uneven
-    grooms, the adjoint, the SDF bake, hair-hair, long strands and the reference's default settings."""
+    """Plain per-groom sweep form and strain limiting on the headline groom, batched vs plain per-groom
+    handles on 64 uneven grooms, the adjoint, the SDF bake, hair-hair, long strands and the reference's
+    default settings."""
     from kamisimulator_b200 import synth
     from kamisimulator_b200.vbd import Solver
 
@@ -288,6 +289,29 @@ def extra_forms(args, torch, stream, flush):
                           "what": "same groom, the sweep form (the reference's sweep order: even and odd vertices, "
                                   "then even and odd segments per iteration, one launch per iteration over tiles "
                                   "in shared memory) replayed from a CUDA graph"}
+    s.close()
+
+    # the SDF solver's strain limiting after each step of the plain fused handle (kami_vbd_strain_limit)
+    s = Solver(g, form="fused", **st)
+    s.set_tuning(2, 4, 1, 120)
+    for _ in range(3):
+        s.step(DT, stream=stream)
+        s.strain_limit(0.1, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    nl = 100
+    e0.record(stream)
+    for _ in range(nl):
+        s.strain_limit(0.1, stream=stream)
+    e1.record(stream)
+    for _ in range(nl):
+        s.step(DT, stream=stream)
+        s.strain_limit(0.1, stream=stream)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    out["strain_limit"] = {"ms_per_call": e0.elapsed_time(e1) / nl, "step_and_limit_ms": e1.elapsed_time(e2) / nl,
+                           "what": "same groom, StrainLimiting (StrainError 0.1) after each fused step, CUDA events "
+                                   "over 100 calls (L2 not flushed)"}
     s.close()
 
     grooms = synth.batched_grooms(64)
