@@ -141,3 +141,29 @@ def test_strain_limit_arguments_and_the_tape():
             s.strain_limit(0.1)
     finally:
         s.close()
+
+
+def test_strain_limit_on_a_batch_handle_matches_each_groom_on_its_own():
+    """A batch handle limits every groom's strands: the same positions, bit for bit, as each groom's
+    own handle (the walk's arithmetic does not depend on where a strand sits in the tiles)."""
+    from kamisimulator_b200.vbd import Solver
+
+    g0 = helpers.soft_groom(120, (6, 64), seed=31)
+    g1 = synth.groom(80, 40, seed=5)
+    x0, x1 = _strained(g0, 1), _strained(g1, 2)
+    st = dict(num_itr=2, max_h=1 / 120)
+    b = Solver([g0, g1], **st)
+    s0, s1 = Solver(g0, **st), Solver(g1, **st)
+    try:
+        b.set_positions_velocities(np.concatenate([x0, x1]), np.zeros((g0.num_vertices + g1.num_vertices, 3), np.float32))
+        s0.set_positions_velocities(x0, np.zeros_like(x0))
+        s1.set_positions_velocities(x1, np.zeros_like(x1))
+        for s in (b, s0, s1):
+            s.strain_limit(0.1)
+        xb = b.get_positions_velocities()[0]
+        want = np.concatenate([s0.get_positions_velocities()[0], s1.get_positions_velocities()[0]])
+    finally:
+        for s in (b, s0, s1):
+            s.close()
+    assert np.abs(want - np.concatenate([x0, x1])).max() > 1e-4
+    np.testing.assert_array_equal(xb, want)
