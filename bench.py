@@ -291,28 +291,7 @@ def extra_forms(args, torch, stream, flush):
                                   "in shared memory) replayed from a CUDA graph"}
     s.close()
 
-    # the SDF solver's strain limiting after each step of the plain fused handle (kami_vbd_strain_limit)
-    s = Solver(g, form="fused", **st)
-    s.set_tuning(2, 4, 1, 120)
-    for _ in range(3):
-        s.step(DT, stream=stream)
-        s.strain_limit(0.1, stream=stream)
-    torch.cuda.synchronize()
-    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
-    nl = 100
-    e0.record(stream)
-    for _ in range(nl):
-        s.strain_limit(0.1, stream=stream)
-    e1.record(stream)
-    for _ in range(nl):
-        s.step(DT, stream=stream)
-        s.strain_limit(0.1, stream=stream)
-    e2.record(stream)
-    torch.cuda.synchronize()
-    out["strain_limit"] = {"ms_per_call": e0.elapsed_time(e1) / nl, "step_and_limit_ms": e1.elapsed_time(e2) / nl,
-                           "what": "same groom, StrainLimiting (StrainError 0.1) after each fused step, CUDA events "
-                                   "over 100 calls (L2 not flushed)"}
-    s.close()
+    out["strain_limit"] = strain_limit_timing(torch, stream)
 
     grooms = synth.batched_grooms(64)
     V = sum(gg.num_vertices for gg in grooms)
@@ -528,6 +507,35 @@ def sdf_bake_timing():
     return {"seconds": gpu_s, "node_triangle_tests_per_s": pairs / gpu_s,
             "cpu_oracle_node_triangle_tests_per_s": 8 ** 3 * T.shape[0] / cpu_s, "cpu_threads": orc.load().oracle_num_threads(),
             "what": "128^3 nodes x 20,480 triangles, exact signed distance + gradients, whole kami_sdf_bake call"}
+
+
+def strain_limit_timing(torch, stream, calls=100):
+    """The SDF solver's strain limiting (kami_vbd_strain_limit, StrainError 0.1) after each fused step of
+    the headline groom: CUDA events around `calls` limits alone, then `calls` steps each followed by a
+    limit (L2 not flushed)."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.vbd import Solver
+
+    s = Solver(synth.groom(), form="fused", **settings())
+    s.set_tuning(2, 4, 1, 120)
+    for _ in range(3):
+        s.step(DT, stream=stream)
+        s.strain_limit(0.1, stream=stream)
+    torch.cuda.synchronize()
+    e0, e1, e2 = (torch.cuda.Event(enable_timing=True) for _ in range(3))
+    e0.record(stream)
+    for _ in range(calls):
+        s.strain_limit(0.1, stream=stream)
+    e1.record(stream)
+    for _ in range(calls):
+        s.step(DT, stream=stream)
+        s.strain_limit(0.1, stream=stream)
+    e2.record(stream)
+    torch.cuda.synchronize()
+    s.close()
+    return {"ms_per_call": e0.elapsed_time(e1) / calls, "step_and_limit_ms": e1.elapsed_time(e2) / calls,
+            "what": "10,000 x 64 groom, StrainLimiting (StrainError 0.1) after each fused step, CUDA events over "
+                    f"{calls} calls (L2 not flushed)"}
 
 
 def hair_hair_timing(torch, stream, steps=50, h=4e-4):
@@ -918,7 +926,8 @@ def main():
     ap.add_argument("--warmup", type=int, default=10)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
-    ap.add_argument("--only", choices=["adjoint", "fit", "large", "hairhair", "bake", "long", "default", "trajectory"],
+    ap.add_argument("--only", choices=["adjoint", "fit", "large", "hairhair", "bake", "long", "default", "trajectory",
+                                       "strain"],
                     help="run a single extra measurement")
     ap.add_argument("--tuning", help="fixed tile shape C,warps,steps_per_launch,register_cap instead of autotuning")
     args = ap.parse_args()
@@ -932,6 +941,10 @@ def main():
         import torch
 
         print(json.dumps(large_timing(torch, torch.cuda.current_stream())), flush=True)
+    elif args.only == "strain":
+        import torch
+
+        print(json.dumps(strain_limit_timing(torch, torch.cuda.current_stream())), flush=True)
     elif args.only == "hairhair":
         import torch
 
