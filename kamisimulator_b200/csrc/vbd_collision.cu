@@ -98,8 +98,7 @@ __global__ void coll_box_kernel(DeviceState st, const float4* __restrict__ dx4, 
     if ((threadIdx.x & 31) == 0 && ext > 0.f) atomicMax(cp.ext_bits, __float_as_uint(ext));
 }
 
-__device__ __forceinline__ bool box_cell(const CollParams& cp, int64_t g, int3& ci) {
-    const float4 lo = cp.bmin[g], hi = cp.bmax[g];
+__device__ __forceinline__ bool box_cell_of(const CollParams& cp, float4 lo, float4 hi, int3& ci) {
     if (hi.w == 0.f) return false;
     const float3 c = f3(0.5f * (lo.x + hi.x), 0.5f * (lo.y + hi.y), 0.5f * (lo.z + hi.z));
     const float cs = cell_size(cp);
@@ -107,6 +106,9 @@ __device__ __forceinline__ bool box_cell(const CollParams& cp, int64_t g, int3& 
     const float inv = 1.f / cs;
     ci = make_int3(__float2int_rd(c.x * inv), __float2int_rd(c.y * inv), __float2int_rd(c.z * inv));
     return true;
+}
+__device__ __forceinline__ bool box_cell(const CollParams& cp, int64_t g, int3& ci) {
+    return box_cell_of(cp, cp.bmin[g], cp.bmax[g], ci);
 }
 
 __global__ void coll_hash_kernel(CollParams cp) {
@@ -145,17 +147,24 @@ __global__ void coll_scatter_kernel(CollParams cp) {
 // of at most 16, then sorted by partner vertex index, so the list does not depend on the order in
 // which lanes found them.
 constexpr int kQueryWarps = 4;
-__global__ void __launch_bounds__(32 * kQueryWarps) coll_query_kernel(DeviceState st, CollParams cp) {
+__global__ void __launch_bounds__(32 * kQueryWarps, 9) coll_query_kernel(DeviceState st, CollParams cp) {
     __shared__ int32_t s_beg[kQueryWarps][27], s_pre[kQueryWarps][28];
     __shared__ int32_t s_lst[kQueryWarps][MAX_CONTACTS], s_key[kQueryWarps][MAX_CONTACTS];
     const int lane = threadIdx.x & 31, w = threadIdx.x >> 5;
     const int64_t g = (int64_t)blockIdx.x * kQueryWarps + w;
     if (g >= cp.num_slots) return;  // uniform per warp
+    // the segment's own operands are loaded before the bucket look-ups, so that they are in flight
+    // beside them instead of after them
+    const float4 loa = cp.bmin[g], hia = cp.bmax[g];
+    const int32_t va = cp.vid[g], ga = cp.gid[g];
     int3 ci;
-    if (!box_cell(cp, g, ci)) {  // uniform per warp (one segment)
+    if (!box_cell_of(cp, loa, hia, ci)) {  // uniform per warp (one segment)
         if (lane == 0) cp.ncols[g] = 0;
         return;
     }
+    // a segment with a box has a next vertex in its tile, so ga1 is in bounds
+    const int64_t ga1 = next_slot(g, cp.C);
+    const float3 xa0 = xyz(st.xm[g]), xa1 = xyz(st.xm[ga1]);
     const uint32_t mask = (1u << cp.table_bits) - 1u;
     uint32_t h = 0xffffffffu;
     int32_t beg = 0, cnt = 0;
@@ -180,11 +189,7 @@ __global__ void __launch_bounds__(32 * kQueryWarps) coll_query_kernel(DeviceStat
     if (lane == 0) s_pre[w][27] = total;
     __syncwarp();
 
-    const float4 loa = cp.bmin[g], hia = cp.bmax[g];
-    const int32_t va = cp.vid[g], ga = cp.gid[g];
     const float slack = 1e-3f * cell_size(cp);  // box overlap is a pre-filter: never reject a pair the distance test keeps
-    const int64_t ga1 = next_slot(g, cp.C);
-    const float3 xa0 = xyz(st.xm[g]), xa1 = xyz(st.xm[ga1]);
     int n = 0;  // accepted so far (uniform)
     for (int32_t t0 = 0; t0 < total; t0 += 32) {
         const int32_t t = t0 + lane;
@@ -198,7 +203,10 @@ __global__ void __launch_bounds__(32 * kQueryWarps) coll_query_kernel(DeviceStat
             for (int step = 16; step; step >>= 1)
                 if (c + step <= 26 && s_pre[w][c + step] <= t) c += step;
             const int32_t k = s_beg[w][c] + (t - s_pre[w][c]);
+            // the candidate's record and box in one round of loads (the box is read whether or not the
+            // record's tests pass)
             const int4 rec = cp.srec[k];
+            const float4 lob = cp.sbmin[k], hib = cp.sbmax[k];
             j = rec.x;
             vb = rec.y;
             bool glued = false;
@@ -208,10 +216,10 @@ __global__ void __launch_bounds__(32 * kQueryWarps) coll_query_kernel(DeviceStat
                 glued = ta0 == j || ta1 == j || ta0 == ja || ta1 == ja || tb0 == g || tb1 == g || tb0 == ga1 ||
                         tb1 == ga1;
             }
-            if (j != g && rec.z == ga && abs(vb - va) > 2 && !glued) {
-                const float4 lob = cp.sbmin[k], hib = cp.sbmax[k];
-                if (!(lob.x > hia.x + slack || loa.x > hib.x + slack || lob.y > hia.y + slack ||
-                      loa.y > hib.y + slack || lob.z > hia.z + slack || loa.z > hib.z + slack)) {
+            const bool apart = (lob.x > hia.x + slack) | (loa.x > hib.x + slack) | (lob.y > hia.y + slack) |
+                               (loa.y > hib.y + slack) | (lob.z > hia.z + slack) | (loa.z > hib.z + slack);
+            if ((j != g) & (rec.z == ga) & (abs(vb - va) > 2) & !glued & !apart) {
+                {
                     const float3 xb0 = xyz(st.xm[j]), xb1 = xyz(st.xm[next_slot(j, cp.C)]);
                     const bool af = va < vb;
                     const float3 p0 = af ? xa0 : xb0, p1 = af ? xa1 : xb1, q0 = af ? xb0 : xa0, q1 = af ? xb1 : xa1;
