@@ -270,33 +270,23 @@ def cpu_baseline_sample():
                       f"(oracle/kami_oracle.cpp, OpenMP)"}
 
 
-def extra_forms(args, torch, stream, flush):
-    """Plain per-groom sweep form and strain limiting on the headline groom, batched vs plain per-groom
-    handles on 64 uneven grooms, the adjoint, the SDF bake, hair-hair, long strands and the reference's
-    default settings."""
+def batched_timing(torch, stream, flush, num_grooms=64, per_groom_handles=True, tuning=None):
+    """kami_vbd_batch_step over `num_grooms` uneven grooms (strands log-uniform [500, 20000], 16-128
+    vertices) in one handle, against the same grooms as one plain drop-in handle each (form auto =
+    fused, each autotuned) and as sweep-form handles, stepped one after another.  `tuning` fixes the
+    batch's tile shape instead of autotuning it (profiling runs)."""
     from kamisimulator_b200 import synth
     from kamisimulator_b200.vbd import Solver
 
-    out = {}
-    g = synth.groom()
     st = settings()
-    s = Solver(g, form="sweep", **st)
-    for _ in range(3):
-        s.step(DT, stream=stream)
-    n = max(20, args.steps // 20)
-    ms = time_steps(s, n, stream, flush)
-    out["plain_sweep"] = {"value": g.num_vertices * NUM_ITR * n / (ms / 1e3), "ms_per_step": ms / n,
-                          "what": "same groom, the sweep form (the reference's sweep order: even and odd vertices, "
-                                  "then even and odd segments per iteration, one launch per iteration over tiles "
-                                  "in shared memory) replayed from a CUDA graph"}
-    s.close()
-
-    out["strain_limit"] = strain_limit_timing(torch, stream)
-
-    grooms = synth.batched_grooms(64)
+    grooms = synth.batched_grooms(num_grooms)
     V = sum(gg.num_vertices for gg in grooms)
     b = Solver(grooms, form="fused", **st)  # kami_vbd_batch_create
-    best, tuned_rate = b.autotune(DT, trial_steps=8)
+    if tuning:
+        b.set_tuning(*tuning)
+        best = b.get_tuning()
+    else:
+        best, _ = b.autotune(DT, trial_steps=8)
     nb = 24
     b.batch_step(DT, nb, stream=stream)  # warm-up: captures the graph for n = nb
     torch.cuda.synchronize()
@@ -331,20 +321,47 @@ def extra_forms(args, torch, stream, flush):
         return V * NUM_ITR * rounds / (ms / 1e3), ms / rounds
 
     vb = V * NUM_ITR * nb / (ms_b / 1e3)
-    vf, ms_f = per_groom("auto", 10)
-    vp, ms_p = per_groom("sweep", 3)
-    out["batched_64_grooms"] = {"value": vb, "ms_per_step": ms_b / nb, "vertices": V,
-                                "tuning": {"slots_per_lane": best[0], "warps_per_block": best[1],
-                                           "steps_per_launch": best[2], "register_cap": best[3]},
-                                "plain_per_groom_fused_value": vf, "plain_fused_ms_per_step": ms_f,
-                                "batched_over_plain_fused": vb / vf,
-                                "plain_per_groom_sweep_value": vp, "plain_sweep_ms_per_step": ms_p,
-                                "batched_over_plain_sweep": vb / vp,
-                                "what": "64 grooms (strands log-uniform [500, 20000], 16-128 vertices) in one "
-                                        f"kami_vbd_batch_create handle, {nb} steps per kami_vbd_batch_step "
-                                        "(autotuned tile shape, CUDA graph), against 64 handles stepped one after "
-                                        "another with kami_vbd_step: the plain drop-in (form auto = fused, each "
-                                        "handle autotuned) and the sweep form"}
+    res = {"value": vb, "ms_per_step": ms_b / nb, "vertices": V, "grooms": num_grooms,
+           "tuning": {"slots_per_lane": best[0], "warps_per_block": best[1], "steps_per_launch": best[2],
+                      "register_cap": best[3]},
+           "what": f"{num_grooms} grooms (strands log-uniform [500, 20000], 16-128 vertices) in one "
+                   f"kami_vbd_batch_create handle, {nb} steps per kami_vbd_batch_step "
+                   f"({'fixed' if tuning else 'autotuned'} tile shape, CUDA graph), against {num_grooms} handles "
+                   "stepped one after another with kami_vbd_step: the plain drop-in (form auto = fused, each "
+                   "handle autotuned) and the sweep form"}
+    if per_groom_handles:
+        vf, ms_f = per_groom("auto", 10)
+        vp, ms_p = per_groom("sweep", 3)
+        res.update({"plain_per_groom_fused_value": vf, "plain_fused_ms_per_step": ms_f,
+                    "batched_over_plain_fused": vb / vf, "plain_per_groom_sweep_value": vp,
+                    "plain_sweep_ms_per_step": ms_p, "batched_over_plain_sweep": vb / vp})
+    return res
+
+
+def extra_forms(args, torch, stream, flush):
+    """Plain per-groom sweep form and strain limiting on the headline groom, batched vs plain per-groom
+    handles on 64 uneven grooms, the adjoint, the SDF bake, hair-hair, long strands and the reference's
+    default settings."""
+    from kamisimulator_b200 import synth
+    from kamisimulator_b200.vbd import Solver
+
+    out = {}
+    g = synth.groom()
+    st = settings()
+    s = Solver(g, form="sweep", **st)
+    for _ in range(3):
+        s.step(DT, stream=stream)
+    n = max(20, args.steps // 20)
+    ms = time_steps(s, n, stream, flush)
+    out["plain_sweep"] = {"value": g.num_vertices * NUM_ITR * n / (ms / 1e3), "ms_per_step": ms / n,
+                          "what": "same groom, the sweep form (the reference's sweep order: even and odd vertices, "
+                                  "then even and odd segments per iteration, one launch per iteration over tiles "
+                                  "in shared memory) replayed from a CUDA graph"}
+    s.close()
+
+    out["strain_limit"] = strain_limit_timing(torch, stream)
+
+    out["batched_64_grooms"] = batched_timing(torch, stream, flush)
     out["adjoint_2k_x48"] = adjoint_timing(torch, stream)
     out["adjoint_fit"] = adjoint_fit(torch)
     out["sdf_bake_128"] = sdf_bake_timing()
@@ -494,12 +511,17 @@ def sdf_bake_timing():
     from kamisimulator_b200 import synth, vbd
     from oracle import oracle as orc
 
+    import torch
+
     V, T = synth.icosphere(5, radius=0.09)
     lo, hi = (-0.15,) * 3, (0.15,) * 3
     vbd.bake_sdf(V, T, (16, 16, 16), lo, hi)  # warm-up (context, module)
-    t0 = time.perf_counter()
-    vbd.bake_sdf(V, T, (128, 128, 128), lo, hi)
-    gpu_s = time.perf_counter() - t0
+    torch.cuda.synchronize()  # nothing of the legs before it runs inside the timed calls
+    gpu_s = float("inf")
+    for _ in range(3):  # best of three whole calls (host allocations and page faults vary between calls)
+        t0 = time.perf_counter()
+        vbd.bake_sdf(V, T, (128, 128, 128), lo, hi)
+        gpu_s = min(gpu_s, time.perf_counter() - t0)
     t0 = time.perf_counter()
     orc.sdf_bake(V, T, (8, 8, 8), lo, hi)
     cpu_s = time.perf_counter() - t0
@@ -830,8 +852,9 @@ def run_ours(args):
     ms_step = max_ms / args.steps
 
     # end to end through the C ABI with pinned host buffers: one kami_vbd_step_host call per frame
-    # (upload, step, download, pipelined over strand groups), and for comparison the same frame as
-    # three calls (kami_vbd_set_positions_velocities, kami_vbd_step, kami_vbd_get_positions_velocities)
+    # (one kernel reads the host arrays, steps the tiles and writes the host arrays back), and for
+    # comparison the same frame as three calls (kami_vbd_set_positions_velocities, kami_vbd_step,
+    # kami_vbd_get_positions_velocities)
     xh = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
     vh = torch.empty((V, 3), dtype=torch.float32, pin_memory=True)
     solver.get_positions_velocities(xh.numpy(), vh.numpy())
@@ -927,8 +950,11 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--skip-extra", action="store_true", help="only the headline timing (profiling runs)")
     ap.add_argument("--only", choices=["adjoint", "fit", "large", "hairhair", "bake", "long", "default", "trajectory",
-                                       "strain"],
+                                       "strain", "batched"],
                     help="run a single extra measurement")
+    ap.add_argument("--grooms", type=int, default=64,
+                    help="--only batched: the number of grooms (a smaller batch of the same generator for profiling "
+                         "runs skips the per-groom handles)")
     ap.add_argument("--tuning", help="fixed tile shape C,warps,steps_per_launch,register_cap instead of autotuning")
     args = ap.parse_args()
     if args.warmup < 3:
@@ -941,6 +967,13 @@ def main():
         import torch
 
         print(json.dumps(large_timing(torch, torch.cuda.current_stream())), flush=True)
+    elif args.only == "batched":
+        import torch
+
+        flush = torch.empty(256 << 20, dtype=torch.uint8, device="cuda")
+        tuning = [int(t) for t in args.tuning.split(",")] if args.tuning else None
+        print(json.dumps(batched_timing(torch, torch.cuda.current_stream(), flush, args.grooms,
+                                        per_groom_handles=args.grooms == 64, tuning=tuning)), flush=True)
     elif args.only == "strain":
         import torch
 

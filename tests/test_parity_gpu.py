@@ -75,11 +75,13 @@ def test_soft_uneven_strands_jacobi(form):
 
 
 @pytest.mark.parametrize("form", ["fused", "sweep"])
-def test_groom_cut_with_head_sdf_per_step(form):
-    """A 400-strand cut of the 10,000 x 64 groom with the 128^3 head sphere, 20 iterations."""
+@pytest.mark.parametrize("schedule", ["colour2", "jacobi"])
+def test_groom_cut_with_head_sdf_per_step(form, schedule):
+    """A 400-strand cut of the 10,000 x 64 groom with the 128^3 head sphere, 20 iterations, under the
+    production schedule (colour2) and the reference kernels' own order (jacobi)."""
     g = synth.groom(400, 64, seed=2)
     sdf = synth.sphere_sdf(128)
-    st = dict(num_itr=20, max_h=1 / 120, gravity=(0.0, 0.0, -9.81), radius=40e-6, sdf=sdf)
+    st = dict(num_itr=20, max_h=1 / 120, gravity=(0.0, 0.0, -9.81), radius=40e-6, sdf=sdf, schedule=schedule)
     ex, et = _lockstep(g, st, form, 6, 1 / 120, reseed_each_frame=True)
     assert ex <= POS_TOL and et <= TWIST_TOL, (ex, et)
 
