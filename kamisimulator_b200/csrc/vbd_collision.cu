@@ -358,9 +358,22 @@ __device__ __forceinline__ ContactOperands load_contact(const DeviceState& st, c
 
 // One contact of segment (x0, x1) (displacements d0, d1) with the partner segment c: the IPC barrier
 // and friction terms of cosserat.cu:177-226, for the segment's first vertex (own) or its second
-// vertex.
-__device__ __forceinline__ void contact_term(const CollParams& cp, const ContactOperands& c, float3 x0, float3 x1,
-                                             float3 d0, float3 d1, bool own, float damp, float3& f, float H[6]) {
+// vertex.  contact_eval computes everything that does not depend on the running sums (f, H);
+// contact_apply adds the result to them in the reference's order: the barrier's force and Hessian,
+// then friction's.  A pair that does not touch (d > 1), or has no tangential slip, carries zero
+// coefficients, and contact_term skips its application.
+struct ContactOut {
+    float3 nrm, u;            // contact normal; tangential relative displacement
+    float cf, sH, cfr, sfr;  // force along nrm, Hessian weight of nrm nrm^T; friction force along u, its Hessian weight
+    bool touch;
+};
+__device__ __forceinline__ ContactOut contact_eval(const CollParams& cp, const ContactOperands& c, float3 x0, float3 x1,
+                                                  float3 d0, float3 d1, bool own, float damp) {
+    ContactOut o;
+    o.nrm = f3(0.f, 0.f, 0.f);
+    o.u = f3(0.f, 0.f, 0.f);
+    o.cf = o.sH = o.cfr = o.sfr = 0.f;
+    o.touch = false;
     const float3 b0 = c.b0, b1 = c.b1, db0 = c.db0, db1 = c.db1;
     const float2 uv = seg_closest(f3(0.f, 0.f, 0.f), (x1 - x0) + (d1 - d0), (b0 - x0) + (db0 - d0), (b1 - x0) + (db1 - d0));
     const float3 dpos = mixv(x0, x1, uv.x) - mixv(b0, b1, uv.y);
@@ -371,29 +384,45 @@ __device__ __forceinline__ void contact_term(const CollParams& cp, const Contact
     const float wt = own ? 1.f - uv.x : uv.x;
     d = d - cp.radius2;
     d *= cp.invb;
-    if (d > 1.f) return;  // not touching
+    if (d > 1.f) return o;  // not touching
     d = fmaxf(d, 1e-3f);
     const float invd = 1.f / d;
     const float logd = logf(d);
     float dH = (-3.f + (2.f + invd) * invd - 2.f * logd) * cp.kcol * cp.invb;
     const float ff = -(1.f - d) * (d - 1.f + 2.f * d * logd) * invd * cp.kcol;
     const float3 mydx = own ? d0 : d1;
-    f = f + (ff * wt - damp * dH * wt * wt * dot3(nrm, mydx)) * nrm;
+    o.touch = true;
+    o.nrm = nrm;
+    o.cf = ff * wt - damp * dH * wt * wt * dot3(nrm, mydx);
     dH *= 1.f + damp;
-    float op[6] = {nrm.x * nrm.x, nrm.y * nrm.y, nrm.z * nrm.z, nrm.x * nrm.y, nrm.x * nrm.z, nrm.y * nrm.z};
-#pragma unroll
-    for (int k = 0; k < 6; k++) H[k] += op[k] * (dH * wt * wt);
+    o.sH = dH * wt * wt;
     const float3 u = ddpos - dot3(nrm, ddpos) * nrm;
     const float ul = sqrtf(len2(u));
     if (ul > 0.f) {
         const float f1 = fminf(cp.kfric, cp.mu * ff / ul);
-        op[0] -= 1.f;
-        op[1] -= 1.f;
-        op[2] -= 1.f;
-        f = f - (f1 * wt) * u;
-#pragma unroll
-        for (int k = 0; k < 6; k++) H[k] -= op[k] * (wt * wt * f1);
+        o.u = u;
+        o.cfr = f1 * wt;
+        o.sfr = wt * wt * f1;
     }
+    return o;
+}
+__device__ __forceinline__ void contact_apply(const ContactOut& o, float3& f, float H[6]) {
+    const float3 nrm = o.nrm;
+    f = f + o.cf * nrm;
+    float op[6] = {nrm.x * nrm.x, nrm.y * nrm.y, nrm.z * nrm.z, nrm.x * nrm.y, nrm.x * nrm.z, nrm.y * nrm.z};
+#pragma unroll
+    for (int k = 0; k < 6; k++) H[k] += op[k] * o.sH;
+    op[0] -= 1.f;
+    op[1] -= 1.f;
+    op[2] -= 1.f;
+    f = f - o.cfr * o.u;
+#pragma unroll
+    for (int k = 0; k < 6; k++) H[k] -= op[k] * o.sfr;
+}
+__device__ __forceinline__ void contact_term(const CollParams& cp, const ContactOperands& c, float3 x0, float3 x1,
+                                             float3 d0, float3 d1, bool own, float damp, float3& f, float H[6]) {
+    const ContactOut o = contact_eval(cp, c, x0, x1, d0, d1, own, damp);
+    if (o.touch) contact_apply(o, f, H);
 }
 
 // Every contact of the segment starting at slot g, in list order (the order of the sums is that of
@@ -414,13 +443,14 @@ __device__ __forceinline__ SegContacts seg_contacts(const CollParams& cp, int64_
 }
 __device__ __forceinline__ SegContacts no_contacts() { return SegContacts{0, 0, INFINITY, 0, nullptr}; }
 
-// The segment's contacts (count, first partner read ahead by the caller); the first `cached` of
-// them have their partner operands in shared memory already.
-__device__ __forceinline__ void contact_terms(const DeviceState& st, const CollParams& cp, const float4* __restrict__ snap,
-                                              int64_t g, const SegContacts& co, float3 x0, float3 x1, float3 d0,
-                                              float3 d1, bool own, float damp, float3& f, float H[6]) {
+// The segment's contacts past the first `cached` (whose partner operands the caller holds in shared
+// memory), read from global memory: the next contact's operands are loaded before the current one is
+// evaluated, so each gather overlaps the arithmetic of the contact before it.
+__device__ __forceinline__ void contact_terms_global(const DeviceState& st, const CollParams& cp,
+                                                     const float4* __restrict__ snap, int64_t g, const SegContacts& co,
+                                                     float3 x0, float3 x1, float3 d0, float3 d1, bool own, float damp,
+                                                     float3& f, float H[6]) {
     const int n = co.n;
-    for (int m = 0; m < co.cached; m++) contact_term(cp, co.part[m], x0, x1, d0, d1, own, damp, f, H);
     if (co.cached >= n) return;
     ContactOperands cur = load_contact(st, cp, snap, co.cached == 0 ? co.first
                                                                      : cp.cols[(int64_t)co.cached * cp.num_slots + g]);
@@ -432,25 +462,36 @@ __device__ __forceinline__ void contact_terms(const DeviceState& st, const CollP
     }
 }
 
-// cosseratItr with contacts for one vertex (cosserat.cu:112-285): the full 3x3 block (hess3(m/h^2),
-// stretch, and each contact's IPC barrier and friction terms for the vertex's two segments), solved
-// with glm's adjugate inverse and clamped to the segments' step limit.  The in-strand operands are
-// the current iterate: the next vertex (xj, dxj), this segment's orientation qg, the previous
-// vertex (xp, dp, its prm pp4) and its segment's orientation qgp; gn / gp are read only when the
-// flags say the neighbour exists.  Partners' dx come from `snap`.
-__device__ __forceinline__ float3 coll_position(const DeviceState& st, const CollParams& cp, const float4* snap,
-                                                int64_t g, int64_t gp, uint32_t fl, float4 xm, float4 prm, float3 vi_dx,
-                                                float3 yv, float3 xj, float3 vj_dx, float4 qg, float3 xp, float3 dp,
-                                                float4 qgp, float4 pp4, SegContacts co, SegContacts cop, float h,
-                                                const PhysParams& pp) {
+// The segment's contacts (count, first partner read ahead by the caller); the first `cached` of
+// them have their partner operands in shared memory already.
+__device__ __forceinline__ void contact_terms(const DeviceState& st, const CollParams& cp, const float4* __restrict__ snap,
+                                              int64_t g, const SegContacts& co, float3 x0, float3 x1, float3 d0,
+                                              float3 d1, bool own, float damp, float3& f, float H[6]) {
+    for (int m = 0; m < co.cached; m++) contact_term(cp, co.part[m], x0, x1, d0, d1, own, damp, f, H);
+    contact_terms_global(st, cp, snap, g, co, x0, x1, d0, d1, own, damp, f, H);
+}
+
+// cosseratItr with contacts for one vertex (cosserat.cu:112-285), in three parts:
+//  * coll_terms_next: hess3(m/h^2) and the inertial force, the connection spring, and the stretch of
+//    the vertex's own segment (to the next vertex xj, dxj, orientation qg); the step limit of that
+//    segment;
+//  * coll_terms_prev: the stretch of the previous segment (vertex xp, dp, its prm pp4, orientation
+//    qgp), into separate sums;
+//  * coll_solve: the two sums added, the full 3x3 block solved with glm's adjugate inverse, and the
+//    update clamped to the segments' step limit.
+// Each segment's contacts (IPC barrier and friction, both ends) are added to its sums between the
+// parts; coll_position does it for one vertex, the one-warp tiles of coll_iteration_kernel for the
+// whole tile at once.
+__device__ __forceinline__ void coll_terms_next(const DeviceState& st, const float4* snap, int64_t g, uint32_t fl,
+                                                float4 xm, float4 prm, float3 vi_dx, float3 yv, float3 xj, float3 vj_dx,
+                                                float4 qg, float h, const PhysParams& pp, float3& f, float H[6]) {
     const float damp = pp.damping / h;
     const float im = xm.w;
     const float3 vi = xyz(xm);
-    float H[6];
     const float inert = 1.f / (im * h * h);
 #pragma unroll
     for (int n = 0; n < 6; n++) H[n] = inert;  // hess3(float) fills all six entries (SymMat.h:16-18)
-    float3 f = (1.f / (h * h * im)) * (yv - vi_dx);
+    f = (1.f / (h * h * im)) * (yv - vi_dx);
     if (st.conn) {
         const int64_t t = st.conn[g];
         if (t >= 0) {  // connection spring (cosserat.cu:123-131), the partner's dx from `snap`
@@ -462,7 +503,6 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
             H[2] += d;
         }
     }
-    float step_limit = INFINITY;
     if (fl & F_HAS_NEXT) {
         const float invl = 1.f / prm.x;
         const float3 cc = ((xj - vi) + (vj_dx - vi_dx)) * invl - d3_of(qg);
@@ -473,19 +513,26 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
         H[0] += dd;
         H[1] += dd;
         H[2] += dd;
-        step_limit = co.limit;
-        contact_terms(st, cp, snap, g, co, vi, xj, vi_dx, vj_dx, true, damp, f, H);
     }
-    if (fl & F_HAS_PREV) {
-        const float invl = 1.f / pp4.x;
-        const float3 cc = ((vi - xp) + (vi_dx - dp)) * invl - d3_of(qgp);
-        const float kk = pp4.y * invl;
-        float dd = kk * invl;
-        float3 f2 = (-kk) * cc - (damp * dd) * vi_dx;
-        dd *= 1.f + damp;
-        float H2[6] = {dd, dd, dd, 0.f, 0.f, 0.f};
-        contact_terms(st, cp, snap, gp, cop, xp, vi, dp, vi_dx, false, damp, f2, H2);
-        step_limit = fminf(step_limit, cop.limit);
+}
+__device__ __forceinline__ void coll_terms_prev(float3 vi, float3 vi_dx, float3 xp, float3 dp, float4 qgp, float4 pp4,
+                                                float damp, float3& f2, float H2[6]) {
+    const float invl = 1.f / pp4.x;
+    const float3 cc = ((vi - xp) + (vi_dx - dp)) * invl - d3_of(qgp);
+    const float kk = pp4.y * invl;
+    float dd = kk * invl;
+    f2 = (-kk) * cc - (damp * dd) * vi_dx;
+    dd *= 1.f + damp;
+    H2[0] = dd;
+    H2[1] = dd;
+    H2[2] = dd;
+    H2[3] = 0.f;
+    H2[4] = 0.f;
+    H2[5] = 0.f;
+}
+__device__ __forceinline__ float3 coll_solve(float3 vi_dx, float3 f, float H[6], bool has_prev, float3 f2,
+                                             const float H2[6], float step_limit, const PhysParams& pp) {
+    if (has_prev) {
         f = f + f2;
 #pragma unroll
         for (int q = 0; q < 6; q++) H[q] += H2[q];
@@ -495,6 +542,36 @@ __device__ __forceinline__ float3 coll_position(const DeviceState& st, const Col
     const float l = sqrtf(len2(out));
     if (l > step_limit && l > 0.f) out = out * (step_limit / l);
     return out;
+}
+
+// cosseratItr with contacts for one vertex: the three parts with each segment's contacts, in list order
+// (the order of the sums is that of one contact at a time).  The in-strand operands are the current
+// iterate: the next vertex (xj, dxj), this segment's orientation qg, the previous vertex (xp, dp, its
+// prm pp4) and its segment's orientation qgp; gn / gp are read only when the flags say the neighbour
+// exists.  Partners' dx come from `snap`.
+__device__ __forceinline__ float3 coll_position(const DeviceState& st, const CollParams& cp, const float4* snap,
+                                                int64_t g, int64_t gp, uint32_t fl, float4 xm, float4 prm, float3 vi_dx,
+                                                float3 yv, float3 xj, float3 vj_dx, float4 qg, float3 xp, float3 dp,
+                                                float4 qgp, float4 pp4, SegContacts co, SegContacts cop, float h,
+                                                const PhysParams& pp) {
+    const float damp = pp.damping / h;
+    const float3 vi = xyz(xm);
+    float3 f;
+    float H[6];
+    coll_terms_next(st, snap, g, fl, xm, prm, vi_dx, yv, xj, vj_dx, qg, h, pp, f, H);
+    float step_limit = INFINITY;
+    if (fl & F_HAS_NEXT) {
+        step_limit = co.limit;
+        contact_terms(st, cp, snap, g, co, vi, xj, vi_dx, vj_dx, true, damp, f, H);
+    }
+    float3 f2 = f3(0.f, 0.f, 0.f);
+    float H2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    if (fl & F_HAS_PREV) {
+        coll_terms_prev(vi, vi_dx, xp, dp, qgp, pp4, damp, f2, H2);
+        contact_terms(st, cp, snap, gp, cop, xp, vi, dp, vi_dx, false, damp, f2, H2);
+        step_limit = fminf(step_limit, cop.limit);
+    }
+    return coll_solve(vi_dx, f, H, (fl & F_HAS_PREV) != 0, f2, H2, step_limit, pp);
 }
 
 // The position sweep of the sweep form with hair-hair contacts (one thread per slot of one colour,
@@ -553,8 +630,23 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
 // block under the 227 KB limit).
 __host__ __device__ constexpr int coll_contact_cap(int T) { return T <= 512 ? T * 5 / 2 : T; }
 __host__ __device__ constexpr size_t coll_iteration_smem(int T) {
-    return (sizeof(float4) * 5 + sizeof(SegContacts)) * T + (sizeof(ContactOperands) + sizeof(int32_t)) * coll_contact_cap(T) +
-           sizeof(int32_t) * (T / 64);
+    return (sizeof(float4) * 5 + sizeof(SegContacts)) * T +
+           (sizeof(ContactOperands) + sizeof(int32_t) + sizeof(int16_t)) * coll_contact_cap(T) + sizeof(int32_t) * (T / 64);
+}
+
+// A contact's evaluation passed from the lane that computed it to the lane whose sums take it.
+__device__ __forceinline__ ContactOut shfl_contact(const ContactOut& o, int src) {
+    ContactOut r;
+    r.nrm = f3(__shfl_sync(0xffffffffu, o.nrm.x, src), __shfl_sync(0xffffffffu, o.nrm.y, src),
+               __shfl_sync(0xffffffffu, o.nrm.z, src));
+    r.u = f3(__shfl_sync(0xffffffffu, o.u.x, src), __shfl_sync(0xffffffffu, o.u.y, src),
+             __shfl_sync(0xffffffffu, o.u.z, src));
+    r.cf = __shfl_sync(0xffffffffu, o.cf, src);
+    r.sH = __shfl_sync(0xffffffffu, o.sH, src);
+    r.cfr = __shfl_sync(0xffffffffu, o.cfr, src);
+    r.sfr = __shfl_sync(0xffffffffu, o.sfr, src);
+    r.touch = __shfl_sync(0xffffffffu, (int)o.touch, src) != 0;
+    return r;
 }
 
 // One colour2 iteration of the sweep form with contacts, one tile per block (T = 32 C slots, T <= 1024)
@@ -574,6 +666,17 @@ __host__ __device__ constexpr size_t coll_iteration_smem(int T) {
 // from global memory in the sweep as before.  Each segment's list serves two vertices (its first as
 // `own`, its second as the previous segment), so the gather halves the partner reads and takes them
 // out of the sweeps' dependency chains.  The operands and the order of the sums are unchanged.
+//
+// ONE_WARP (tiles of 64 slots, one warp per block): a position half-sweep evaluates the tile's cached
+// contacts 32 at a time, one per lane, each from its segment's end point of the half-sweep's colour
+// (the first end point as `own`, the second as the previous segment), and every vertex then adds its
+// own segment's and its previous segment's evaluations to its two sums in list order, taking them from
+// the evaluating lanes by shuffles.  The operands, the arithmetic and the order of each sum are those
+// of coll_position; what changes is that a vertex with many contacts no longer evaluates them one
+// after another while the other lanes of its warp wait.  The tiles of a groom run in one wave when
+// they fit, so the iteration takes as long as its slowest tile, which is the one with the most
+// contacts on one vertex.
+template <bool ONE_WARP>
 __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, const float4* __restrict__ y4, float4* q,
                                                              const float4* __restrict__ snap,
                                                              float4* __restrict__ dx_out,
@@ -592,6 +695,7 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
     ContactOperands* spart = reinterpret_cast<ContactOperands*>(sco + T);
     int32_t* spidx = reinterpret_cast<int32_t*>(spart + ncap);  // the partners' slots, then the warps' totals
     int32_t* swarp = spidx + ncap;
+    int16_t* sown = reinterpret_cast<int16_t*>(swarp + T / 64);  // each cached contact's segment (its first slot)
     const int lane = threadIdx.x & 31, row2 = (threadIdx.x >> 5) * 2;  // rows row2 (even) and row2 + 1 (odd)
     const int64_t base = (int64_t)blockIdx.x * T;
     float3 yown[2];
@@ -632,7 +736,10 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
         const int p = (row2 + c) * 32 + lane;
         const int off = first_off + (c ? own[0].n : 0);
         const int cached = max(0, min(own[c].n, ncap - off));
-        for (int m = 0; m < cached; m++) spidx[off + m] = cp.cols[(int64_t)m * cp.num_slots + base + p];
+        for (int m = 0; m < cached; m++) {
+            spidx[off + m] = cp.cols[(int64_t)m * cp.num_slots + base + p];
+            sown[off + m] = (int16_t)p;
+        }
         own[c].cached = cached;
         own[c].part = spart + min(off, ncap);
         sco[p] = own[c];
@@ -641,6 +748,68 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
     for (int k = threadIdx.x; k < total; k += blockDim.x) spart[k] = load_contact(st, cp, snap, spidx[k]);
     const float h = spp->h;
     __syncthreads();
+    if constexpr (ONE_WARP) {
+        const float damp = pp.damping / h;
+#pragma unroll 1
+        for (int c = 0; c < 2; c++) {
+            const int p = c * 32 + lane;  // rows 0 (even) and 1 (odd): the row is the colour
+            const int64_t g = base + p;
+            const float4 xm = sx[p], prm = sprm[p];
+            const uint32_t fl = __float_as_uint(prm.w);
+            const bool act = (fl & F_VALID) && xm.w != 0.f;
+            const bool hn = act && (fl & F_HAS_NEXT), hp = act && (fl & F_HAS_PREV);
+            const int pn = hn ? (int)(next_slot(g, C) - base) : p;
+            const int pq = hp ? (int)(prev_slot(g, C) - base) : p;
+            const float3 vi = xyz(xm), vi_dx = xyz(sdx[p]), xj = xyz(sx[pn]), vj_dx = xyz(sdx[pn]);
+            const float3 xp = xyz(sx[pq]), dp = xyz(sdx[pq]);
+            const SegContacts co = sco[p];
+            const SegContacts cop = hp ? sco[pq] : no_contacts();
+            float3 f = f3(0.f, 0.f, 0.f), f2 = f3(0.f, 0.f, 0.f);
+            float H[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f}, H2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+            float step_limit = INFINITY;
+            if (act) {
+                coll_terms_next(st, snap, g, fl, xm, prm, vi_dx, c ? yown[1] : yown[0], xj, vj_dx, sq[p], h, pp, f, H);
+                if (hn) step_limit = co.limit;
+                if (hp) coll_terms_prev(vi, vi_dx, xp, dp, sq[pq], sprm[pq], damp, f2, H2);
+            }
+            // this vertex's cached entries: [a0, a0 + n0) of its own segment, [a1, a1 + n1) of the previous one
+            const int a0 = hn ? (int)(co.part - spart) : 0, n0 = hn ? co.cached : 0;
+            const int a1 = hp ? (int)(cop.part - spart) : 0, n1 = hp ? cop.cached : 0;
+            for (int r0 = 0; r0 < total; r0 += 32) {  // (total is uniform)
+                ContactOut o;
+                o.touch = false;
+                o.nrm = o.u = f3(0.f, 0.f, 0.f);
+                o.cf = o.sH = o.cfr = o.sfr = 0.f;
+                const int e = r0 + lane;
+                if (e < total) {
+                    const int s0 = sown[e];  // the contact's segment: its end points s0 and s1
+                    const int s1 = (int)(next_slot(base + s0, C) - base);
+                    o = contact_eval(cp, spart[e], xyz(sx[s0]), xyz(sx[s1]), xyz(sdx[s0]), xyz(sdx[s1]), (s0 >> 5) == c,
+                                     damp);
+                }
+                const int lo0 = max(a0, r0), k0 = max(0, min(a0 + n0, r0 + 32) - lo0);
+                const int lo1 = max(a1, r0), k1 = max(0, min(a1 + n1, r0 + 32) - lo1);
+                const int kmax = __reduce_max_sync(0xffffffffu, max(k0, k1));
+                for (int j = 0; j < kmax; j++) {
+                    const ContactOut e0 = shfl_contact(o, (lo0 + j - r0) & 31);
+                    const ContactOut e1 = shfl_contact(o, (lo1 + j - r0) & 31);
+                    if (j < k0 && e0.touch) contact_apply(e0, f, H);
+                    if (j < k1 && e1.touch) contact_apply(e1, f2, H2);
+                }
+            }
+            if (act) {
+                // contacts past the tile's cap, from global memory, after the cached ones
+                if (hn) contact_terms_global(st, cp, snap, g, co, vi, xj, vi_dx, vj_dx, true, damp, f, H);
+                if (hp) {
+                    contact_terms_global(st, cp, snap, base + pq, cop, xp, vi, dp, vi_dx, false, damp, f2, H2);
+                    step_limit = fminf(step_limit, cop.limit);
+                }
+                const float3 out = coll_solve(vi_dx, f, H, hp, f2, H2, step_limit, pp);
+                sdx[p] = make_float4(out.x, out.y, out.z, 0.f);
+            }
+            __syncwarp();
+        }
+    } else {
 #pragma unroll
     for (int c = 0; c < 2; c++) {
         const int p = (row2 + c) * 32 + lane;
@@ -659,6 +828,7 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
             sdx[p] = make_float4(out.x, out.y, out.z, 0.f);
         }
         __syncthreads();
+    }
     }
     for (int c = 0; c < 2; c++) {
         const int p = (row2 + c) * 32 + lane;
@@ -733,11 +903,16 @@ cudaError_t launch_coll_iteration(const DeviceState& st, const float4* y4, float
     if (st.num_tiles == 0) return cudaSuccess;
     const int T = 32 * cp.C;
     const size_t smem = coll_iteration_smem(T);
+    if (cp.C == 2) {  // one warp per tile
+        coll_iteration_kernel<true><<<(unsigned)st.num_tiles, T / 2, smem, s>>>(st, y4, q, snap, dx_out, d_sp, pp, cp);
+        return cudaGetLastError();
+    }
     if (smem > 48 * 1024) {  // the opt-in dynamic shared memory limit is set per device, so on every launch
-        cudaError_t e = cudaFuncSetAttribute(coll_iteration_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaError_t e =
+            cudaFuncSetAttribute(coll_iteration_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
     }
-    coll_iteration_kernel<<<(unsigned)st.num_tiles, T / 2, smem, s>>>(st, y4, q, snap, dx_out, d_sp, pp, cp);
+    coll_iteration_kernel<false><<<(unsigned)st.num_tiles, T / 2, smem, s>>>(st, y4, q, snap, dx_out, d_sp, pp, cp);
     return cudaGetLastError();
 }
 
