@@ -416,6 +416,15 @@ kami_status kami_vbd_get_tiles_per_group(kami_vbd_handle h, int32_t* tiles_per_g
  * kami_vbd_backward; the adjoint of vertices outside the window passes through unchanged. */
 kami_status kami_vbd_set_tape_window(kami_vbd_handle h, int64_t tile_begin, int64_t tile_end);
 
+/* kami_vbd_set_state for the strands of the tape window only (no counterpart in the reference): from
+ * a whole-groom state buffer (kami_vbd_get_state layout) in device memory, restores the state of the
+ * strands whose tiles lie in the window, and the step clock; the other strands keep their state.
+ * Restoring a checkpoint window by window then moves 1/n of the state per window instead of all of
+ * it.  With host memory, or a window that covers the whole groom, it is kami_vbd_set_state.  When the
+ * window is smaller than the groom and the adjoints are in device memory, kami_vbd_backward likewise
+ * reads and writes only the window's entries of the adjoint arrays. */
+kami_status kami_vbd_restore_tape_window(kami_vbd_handle h, const void* src, size_t bytes, int32_t memory);
+
 /* kami_vbd_step that also records its iterates.  A step of ceil(dt / max_h) substeps takes as many
  * of the tape's max_steps entries (one per substep; KAMI_ERR_STATE when they do not fit). */
 kami_status kami_vbd_step_record(kami_vbd_handle h, float dt, void* stream);

@@ -19,7 +19,8 @@ every segment from the checkpoints instead.
 
 With ``tiles_per_chunk`` the backward pass works on one window of warp tiles at a time (strands are
 independent; the window is rounded up to whole groups of tiles when strands run across several), so
-the tape memory is bounded by the window; every segment is then recomputed.  ``body_transforms``
+the tape memory is bounded by the window; every segment is then recomputed, and each window restores
+its checkpoints and moves its adjoints for its own strands only.  ``body_transforms``
 ((frames, 7): rotation x y z w, translation per frame) moves the body SDF frame by frame, in the
 forward pass and in the recorded steps alike.  The solver must use the fused form with the colour2
 schedule (wind is allowed); a frame of several substeps (dt > max_h) is recorded substep by substep.
@@ -126,7 +127,7 @@ class StrandStiffnessRollout(torch.autograd.Function):
 
 
 def _recompute_segment(ctx, solver, seg):
-    solver.set_state_from(ctx.ckpts[seg])
+    solver.restore_tape_window_from(ctx.ckpts[seg])  # the window's strands (all of them without a window)
     n = min(ctx.k, ctx.frames - seg * ctx.k)
     for j in range(n):
         _move_body(solver, ctx.body, seg * ctx.k + j)

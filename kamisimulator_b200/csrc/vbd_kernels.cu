@@ -439,18 +439,22 @@ __global__ void sweep_finish_kernel(DeviceState st, const float4* __restrict__ d
 // ==========================================================================================
 // boundary gather / scatter (API vertex order <-> tile slots)
 // ==========================================================================================
+// With a vertex list (tape windows), entry i stands for vertex list[i]; without one, for vertex i.
+__device__ __forceinline__ int64_t listed(const int64_t* __restrict__ list, int64_t i) { return list ? list[i] : i; }
 __global__ void scatter3_kernel(const float* __restrict__ src, float4* __restrict__ dst,
-                                const int64_t* __restrict__ slot_of, int64_t nv) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nv) return;
+                                const int64_t* __restrict__ slot_of, int64_t nv, const int64_t* __restrict__ list) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nv) return;
+    const int64_t i = listed(list, t);
     float4* d = dst + slot_of[i];
     float4 o = *d;
     *d = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], o.w);
 }
 __global__ void gather3_kernel(const float4* __restrict__ src, float* __restrict__ dst,
-                               const int64_t* __restrict__ slot_of, int64_t nv) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= nv) return;
+                               const int64_t* __restrict__ slot_of, int64_t nv, const int64_t* __restrict__ list) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= nv) return;
+    const int64_t i = listed(list, t);
     float4 a = src[slot_of[i]];
     dst[3 * i] = a.x;
     dst[3 * i + 1] = a.y;
@@ -458,15 +462,35 @@ __global__ void gather3_kernel(const float4* __restrict__ src, float* __restrict
 }
 __global__ void scatter4_kernel(const float4* __restrict__ src, float4* __restrict__ dst,
                                 const int64_t* __restrict__ slot_of, int64_t nv) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nv) return;
     dst[slot_of[i]] = src[i];
 }
+// the listed vertices' 4-vectors from a caller's boundary array, read as floats (its 4-vectors need
+// not start on 16-byte boundaries, e.g. the orientations inside a state buffer)
+__global__ void scatter4_list_kernel(const float* __restrict__ src, float4* __restrict__ dst,
+                                     const int64_t* __restrict__ slot_of, int64_t n, const int64_t* __restrict__ list) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int64_t i = list[t];
+    dst[slot_of[i]] = make_float4(src[4 * i], src[4 * i + 1], src[4 * i + 2], src[4 * i + 3]);
+}
 __global__ void gather4_kernel(const float4* __restrict__ src, float4* __restrict__ dst,
                                const int64_t* __restrict__ slot_of, int64_t nv) {
-    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nv) return;
     dst[i] = src[slot_of[i]];
+}
+__global__ void gather4_list_kernel(const float4* __restrict__ src, float* __restrict__ dst,
+                                    const int64_t* __restrict__ slot_of, int64_t n, const int64_t* __restrict__ list) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int64_t i = list[t];
+    const float4 a = src[slot_of[i]];
+    dst[4 * i] = a.x;
+    dst[4 * i + 1] = a.y;
+    dst[4 * i + 2] = a.z;
+    dst[4 * i + 3] = a.w;
 }
 
 // ==========================================================================================
@@ -829,14 +853,16 @@ cudaError_t launch_hair_out(const float4* src, float* dst, const int64_t* slot_o
     return cudaGetLastError();
 }
 
-cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
+cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s,
+                            const int64_t* list) {
     if (nv == 0) return cudaSuccess;
-    scatter3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
+    scatter3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv, list);
     return cudaGetLastError();
 }
-cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
+cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s,
+                           const int64_t* list) {
     if (nv == 0) return cudaSuccess;
-    gather3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
+    gather3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv, list);
     return cudaGetLastError();
 }
 cudaError_t launch_scatter4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
@@ -847,6 +873,18 @@ cudaError_t launch_scatter4(const float4* src, float4* dst, const int64_t* slot_
 cudaError_t launch_gather4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
     if (nv == 0) return cudaSuccess;
     gather4_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
+    return cudaGetLastError();
+}
+cudaError_t launch_scatter4_list(const float* src, float4* dst, const int64_t* slot_of, const int64_t* list, int64_t n,
+                                 cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    scatter4_list_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, dst, slot_of, n, list);
+    return cudaGetLastError();
+}
+cudaError_t launch_gather4_list(const float4* src, float* dst, const int64_t* slot_of, const int64_t* list, int64_t n,
+                                cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    gather4_list_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, dst, slot_of, n, list);
     return cudaGetLastError();
 }
 

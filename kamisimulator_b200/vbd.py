@@ -40,7 +40,7 @@ EXPORTED = [
     "kami_usc_info", "kami_usc_read", "kami_usc_write", "kami_sdf_bake", "kami_vbd_sag_free",
     "kami_hair_subdivide", "kami_hair_resample", "kami_vbd_step_host", "kami_vbd_get_tiles_per_group",
     "kami_vbd_set_launch_mode", "kami_vbd_get_launch_mode", "kami_vbd_step_hair", "kami_host_register",
-    "kami_host_unregister", "kami_vbd_strain_limit",
+    "kami_host_unregister", "kami_vbd_strain_limit", "kami_vbd_restore_tape_window",
 ]
 
 
@@ -162,6 +162,7 @@ def load_library(path: str = LIB_PATH):
         "kami_vbd_tape_reserve": [vp, i32, i64],
         "kami_vbd_get_tile_count": [vp, ctypes.POINTER(i64)],
         "kami_vbd_set_tape_window": [vp, i64, i64],
+        "kami_vbd_restore_tape_window": [vp, vp, ctypes.c_size_t, i32],
         "kami_vbd_step_record": [vp, f32, vp],
         "kami_vbd_backward": [vp, vp, vp, vp, vp, i32, vp],
         "kami_vbd_get_rest_darboux_grad": [vp, vp, i32],
@@ -549,6 +550,13 @@ class Solver:
 
     def set_tape_window(self, tile_begin, tile_end):
         _check(self.lib.kami_vbd_set_tape_window(self._h, tile_begin, tile_end))
+
+    def restore_tape_window_from(self, buf):
+        """set_state_from for the strands of the tape window only (and the step clock): a whole-groom
+        state buffer, of which only the window's strands are read when it is a CUDA tensor."""
+        p, m = _ptr(buf)
+        nbytes = buf.numel() * buf.element_size() if hasattr(buf, "numel") else buf.nbytes
+        _check(self.lib.kami_vbd_restore_tape_window(self._h, p, nbytes, m))
 
     def step_record(self, dt, stream=None):
         s = None if stream is None else ctypes.c_void_p(stream if isinstance(stream, int) else stream.cuda_stream)
