@@ -422,7 +422,8 @@ kami_status kami_vbd_set_tape_window(kami_vbd_handle h, int64_t tile_begin, int6
  * Restoring a checkpoint window by window then moves 1/n of the state per window instead of all of
  * it.  With host memory, or a window that covers the whole groom, it is kami_vbd_set_state.  When the
  * window is smaller than the groom and the adjoints are in device memory, kami_vbd_backward likewise
- * reads and writes only the window's entries of the adjoint arrays. */
+ * reads and writes only the window's entries of the adjoint arrays.  The first such call on a layout
+ * allocates a slot -> vertex map of 8 B per slot. */
 kami_status kami_vbd_restore_tape_window(kami_vbd_handle h, const void* src, size_t bytes, int32_t memory);
 
 /* kami_vbd_step that also records its iterates.  A step of ceil(dt / max_h) substeps takes as many

@@ -134,11 +134,10 @@ struct kami_vbd_solver {
     int tape_capacity = 0;
     int64_t tape_tiles = 0;               // tiles the tape holds per step
     int64_t win_begin = 0, win_end = 0;   // tile window that recording and the adjoint cover
-    // the boundary vertices of the window's strands (built when a window smaller than the groom is
+    // the boundary vertex of every slot, -1 for padding (built when a window smaller than the groom is
     // first used, for the layout it was built on)
-    int64_t* d_win_list = nullptr;
-    int64_t win_list_cap = 0, win_list_count = 0, win_list_begin = -1, win_list_end = -1;
-    int win_list_C = 0, win_list_K = 0;
+    int64_t* d_vert_of = nullptr;
+    int vert_of_C = 0, vert_of_K = 0;
     struct TapeStep {
         StepParams sp;  // one substep (sp.substeps == 1) of a recorded advance
         bool sdf;       // the advance's last substep, which ends with the body pass
@@ -193,7 +192,7 @@ void release(kami_vbd_solver* h) {
     void* ptrs[] = {h->d_slot_of, h->d_xm, h->d_vel, h->d_vlast, h->d_q,     h->d_qr,    h->d_prm,
                     h->d_y,       h->d_dx, h->d_dx2, h->d_q2,    h->d_step,  h->d_stage, h->d_status,
                     h->d_sdf,     h->d_tdx, h->d_tq, h->d_tx,    h->d_tv,    h->d_tvl,   h->d_gx,
-                    h->d_gv,      h->d_gvl, h->d_gq, h->d_gqr,   h->d_win_list};
+                    h->d_gv,      h->d_gvl, h->d_gq, h->d_gqr,   h->d_vert_of};
     for (void* p : ptrs)
         if (p) cudaFree(p);
     const CollParams& c = h->cp;
@@ -1515,42 +1514,24 @@ kami_status kami_vbd_get_tiles_per_group(kami_vbd_handle h, int32_t* tiles_per_g
     return KAMI_OK;
 }
 
-// The window's vertices for the scatters and gathers of kami_vbd_backward and
-// kami_vbd_restore_tape_window: null (every vertex) when the window covers the whole groom.  A
-// strand lies in the window when its first vertex's tile does (windows are whole groups of tiles,
-// and a strand never leaves its group).
-static kami_status window_list(kami_vbd_solver* h, const int64_t** list, int64_t* count) {
-    *list = nullptr;
-    *count = h->nv;
+// The tape window's slots [s0, s0 + n) and the slot -> vertex map for the scatters and gathers of
+// kami_vbd_backward and kami_vbd_restore_tape_window; *vert_of stays null when the window covers the
+// whole groom.
+static kami_status window_slots(kami_vbd_solver* h, const int64_t** vert_of, int64_t* s0, int64_t* n) {
+    *vert_of = nullptr;
     if (h->win_begin == 0 && h->win_end >= h->layout.num_tiles) return KAMI_OK;
-    if (h->win_list_begin != h->win_begin || h->win_list_end != h->win_end || h->win_list_C != h->layout.C ||
-        h->win_list_K != h->layout.K) {
-        const int64_t T = 32LL * h->layout.C;
-        std::vector<int64_t> verts;
-        for (int32_t k = 0; k < h->ns; k++) {
-            const int64_t v0 = h->strand_begin[k], v1 = h->strand_begin[k + 1];
-            const int64_t tile = h->layout.slot_of[v0] / T;
-            if (tile >= h->win_begin && tile < h->win_end)
-                for (int64_t v = v0; v < v1; v++) verts.push_back(v);
-        }
-        if ((int64_t)verts.size() > h->win_list_cap) {
-            if (h->d_win_list) cudaFree(h->d_win_list);
-            h->d_win_list = nullptr;
-            h->win_list_cap = 0;
-            KAMI_CUDA(dalloc(&h->d_win_list, verts.size()), "allocating the window's vertex list");
-            h->win_list_cap = (int64_t)verts.size();
-        }
-        if (!verts.empty())
-            KAMI_CUDA(cudaMemcpy(h->d_win_list, verts.data(), sizeof(int64_t) * verts.size(), cudaMemcpyHostToDevice),
-                      "window vertex list");
-        h->win_list_count = (int64_t)verts.size();
-        h->win_list_begin = h->win_begin;
-        h->win_list_end = h->win_end;
-        h->win_list_C = h->layout.C;
-        h->win_list_K = h->layout.K;
+    if (!h->d_vert_of || h->vert_of_C != h->layout.C || h->vert_of_K != h->layout.K) {
+        if (h->d_vert_of) cudaFree(h->d_vert_of);
+        h->d_vert_of = nullptr;
+        KAMI_CUDA(dalloc(&h->d_vert_of, (size_t)h->layout.num_slots), "allocating the slot -> vertex map");
+        KAMI_CUDA(launch_vert_of(h->d_slot_of, h->d_vert_of, h->nv, h->layout.num_slots, h->stream), "slot -> vertex map");
+        h->vert_of_C = h->layout.C;
+        h->vert_of_K = h->layout.K;
     }
-    *list = h->d_win_list;
-    *count = h->win_list_count;
+    const int64_t T = 32LL * h->layout.C;
+    *vert_of = h->d_vert_of;
+    *s0 = h->win_begin * T;
+    *n = (h->win_end - h->win_begin) * T;
     return KAMI_OK;
 }
 
@@ -1620,17 +1601,15 @@ kami_status kami_vbd_backward(kami_vbd_handle h, float* adj_x, float* adj_v, flo
     // entries: the slots of its tiles are reset and its vertices scattered straight from the caller's
     // arrays and gathered back into them (the other entries of those arrays are left as they are,
     // which is what the whole-groom copies would write back too).
-    const int64_t* wl = nullptr;
-    int64_t wn = h->nv;
-    if (memory == KAMI_MEMORY_DEVICE) KAMI_TRY(window_list(h, &wl, &wn));
-    if (wl) {
-        const int64_t T = 32LL * h->layout.C, s0 = h->win_begin * T, ns = (h->win_end - h->win_begin) * T;
+    const int64_t* wv = nullptr;
+    int64_t ws0 = 0, wn = 0;
+    if (memory == KAMI_MEMORY_DEVICE) KAMI_TRY(window_slots(h, &wv, &ws0, &wn));
+    if (wv) {
         for (int a = 0; a < 3; a++) {
-            KAMI_CUDA(cudaMemsetAsync(adj3[a] + s0, 0, sizeof(float4) * ns, h->stream), "adjoint reset");
-            KAMI_CUDA(launch_scatter3(ins3[a], adj3[a], h->d_slot_of, wn, h->stream, wl), "scatter adjoint");
+            KAMI_CUDA(cudaMemsetAsync(adj3[a] + ws0, 0, sizeof(float4) * wn, h->stream), "adjoint reset");
+            KAMI_CUDA(launch_scatter_slots(ins3[a], adj3[a], wv, ws0, wn, 3, h->stream), "scatter adjoint");
         }
-        KAMI_CUDA(cudaMemsetAsync(h->d_gq + s0, 0, sizeof(float4) * ns, h->stream), "adjoint reset");
-        KAMI_CUDA(launch_scatter4_list(adj_q, h->d_gq, h->d_slot_of, wl, wn, h->stream), "scatter adjoint");
+        KAMI_CUDA(launch_scatter_slots(adj_q, h->d_gq, wv, ws0, wn, 4, h->stream), "scatter adjoint");
     } else {
         for (int a = 0; a < 3; a++) {
             KAMI_CUDA(cudaMemsetAsync(adj3[a], 0, sizeof(float4) * S, h->stream), "adjoint reset");
@@ -1654,10 +1633,10 @@ kami_status kami_vbd_backward(kami_vbd_handle h, float* adj_x, float* adj_v, flo
     });
     if (st != KAMI_OK) return st;
     h->tape_steps.clear();
-    if (wl) {
+    if (wv) {
         for (int a = 0; a < 3; a++)
-            KAMI_CUDA(launch_gather3(adj3[a], ins3[a], h->d_slot_of, wn, h->stream, wl), "gather adjoint");
-        KAMI_CUDA(launch_gather4_list(h->d_gq, adj_q, h->d_slot_of, wl, wn, h->stream), "gather adjoint");
+            KAMI_CUDA(launch_gather_slots(adj3[a], ins3[a], wv, ws0, wn, 3, h->stream), "gather adjoint");
+        KAMI_CUDA(launch_gather_slots(h->d_gq, adj_q, wv, ws0, wn, 4, h->stream), "gather adjoint");
     } else {
         for (int a = 0; a < 3; a++) {
             KAMI_CUDA(launch_gather3(adj3[a], h->d_stage, h->d_slot_of, h->nv, h->stream), "gather adjoint");
@@ -1931,10 +1910,10 @@ kami_status kami_vbd_set_state(kami_vbd_handle h, const void* src, size_t bytes,
 kami_status kami_vbd_restore_tape_window(kami_vbd_handle h, const void* src, size_t bytes, int32_t memory) {
     KAMI_TRY(valid_handle(h));
     if (h->tape_capacity == 0) return fail(KAMI_ERR_STATE, "call kami_vbd_tape_reserve first");
-    const int64_t* wl = nullptr;
-    int64_t wn = h->nv;
-    if (memory == KAMI_MEMORY_DEVICE) KAMI_TRY(window_list(h, &wl, &wn));
-    if (!wl) return kami_vbd_set_state(h, src, bytes, memory);  // the whole groom, or host memory
+    const int64_t* wv = nullptr;
+    int64_t ws0 = 0, wn = 0;
+    if (memory == KAMI_MEMORY_DEVICE) KAMI_TRY(window_slots(h, &wv, &ws0, &wn));
+    if (!wv) return kami_vbd_set_state(h, src, bytes, memory);  // the whole groom, or host memory
     size_t need = 0;
     kami_vbd_state_size(h, &need);
     if (!src || bytes < need) return fail(KAMI_ERR_INVALID_ARGUMENT, "state buffer must hold %zu bytes", need);
@@ -1942,8 +1921,8 @@ kami_status kami_vbd_restore_tape_window(kami_vbd_handle h, const void* src, siz
     const int64_t nv = h->nv;
     float4* dsts[3] = {h->d_xm, h->d_vel, h->d_vlast};
     for (int a = 0; a < 3; a++)
-        KAMI_CUDA(launch_scatter3(f + 3 * nv * a, dsts[a], h->d_slot_of, wn, h->stream, wl), "scatter state");
-    KAMI_CUDA(launch_scatter4_list(f + 9 * nv, h->d_q, h->d_slot_of, wl, wn, h->stream), "scatter state");
+        KAMI_CUDA(launch_scatter_slots(f + 3 * nv * a, dsts[a], wv, ws0, wn, 3, h->stream), "scatter state");
+    KAMI_CUDA(launch_scatter_slots(f + 9 * nv, h->d_q, wv, ws0, wn, 4, h->stream), "scatter state");
     float clk[4];
     KAMI_CUDA(cudaMemcpyAsync(clk, f + 13 * nv, sizeof(clk), cudaMemcpyDeviceToHost, h->stream), "state clock");
     KAMI_CUDA(cudaStreamSynchronize(h->stream), "cudaStreamSynchronize");

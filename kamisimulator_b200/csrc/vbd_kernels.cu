@@ -439,22 +439,18 @@ __global__ void sweep_finish_kernel(DeviceState st, const float4* __restrict__ d
 // ==========================================================================================
 // boundary gather / scatter (API vertex order <-> tile slots)
 // ==========================================================================================
-// With a vertex list (tape windows), entry i stands for vertex list[i]; without one, for vertex i.
-__device__ __forceinline__ int64_t listed(const int64_t* __restrict__ list, int64_t i) { return list ? list[i] : i; }
 __global__ void scatter3_kernel(const float* __restrict__ src, float4* __restrict__ dst,
-                                const int64_t* __restrict__ slot_of, int64_t nv, const int64_t* __restrict__ list) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nv) return;
-    const int64_t i = listed(list, t);
+                                const int64_t* __restrict__ slot_of, int64_t nv) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
     float4* d = dst + slot_of[i];
     float4 o = *d;
     *d = make_float4(src[3 * i], src[3 * i + 1], src[3 * i + 2], o.w);
 }
 __global__ void gather3_kernel(const float4* __restrict__ src, float* __restrict__ dst,
-                               const int64_t* __restrict__ slot_of, int64_t nv, const int64_t* __restrict__ list) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= nv) return;
-    const int64_t i = listed(list, t);
+                               const int64_t* __restrict__ slot_of, int64_t nv) {
+    int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= nv) return;
     float4 a = src[slot_of[i]];
     dst[3 * i] = a.x;
     dst[3 * i + 1] = a.y;
@@ -466,31 +462,42 @@ __global__ void scatter4_kernel(const float4* __restrict__ src, float4* __restri
     if (i >= nv) return;
     dst[slot_of[i]] = src[i];
 }
-// the listed vertices' 4-vectors from a caller's boundary array, read as floats (its 4-vectors need
-// not start on 16-byte boundaries, e.g. the orientations inside a state buffer)
-__global__ void scatter4_list_kernel(const float* __restrict__ src, float4* __restrict__ dst,
-                                     const int64_t* __restrict__ slot_of, int64_t n, const int64_t* __restrict__ list) {
-    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
-    if (t >= n) return;
-    const int64_t i = list[t];
-    dst[slot_of[i]] = make_float4(src[4 * i], src[4 * i + 1], src[4 * i + 2], src[4 * i + 3]);
-}
 __global__ void gather4_kernel(const float4* __restrict__ src, float4* __restrict__ dst,
                                const int64_t* __restrict__ slot_of, int64_t nv) {
     const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= nv) return;
     dst[i] = src[slot_of[i]];
 }
-__global__ void gather4_list_kernel(const float4* __restrict__ src, float* __restrict__ dst,
-                                    const int64_t* __restrict__ slot_of, int64_t n, const int64_t* __restrict__ list) {
+// Tape windows: the slots [s0, s0 + n) of a window and the boundary vertices they hold (vert_of: the
+// vertex of each slot, -1 for padding).  Slot side in tile order, boundary side read and written as
+// floats (its 4-vectors need not start on 16-byte boundaries, e.g. the orientations inside a state
+// buffer).  `comps` is 3 (the slot's .w is kept) or 4.
+__global__ void vert_of_kernel(const int64_t* __restrict__ slot_of, int64_t* __restrict__ vert_of, int64_t nv) {
+    const int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < nv) vert_of[slot_of[i]] = i;
+}
+__global__ void scatter_slots_kernel(const float* __restrict__ src, float4* __restrict__ dst,
+                                     const int64_t* __restrict__ vert_of, int64_t s0, int64_t n, int comps) {
     const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
     if (t >= n) return;
-    const int64_t i = list[t];
-    const float4 a = src[slot_of[i]];
-    dst[4 * i] = a.x;
-    dst[4 * i + 1] = a.y;
-    dst[4 * i + 2] = a.z;
-    dst[4 * i + 3] = a.w;
+    const int64_t s = s0 + t, v = vert_of[s];
+    if (v < 0) return;
+    if (comps == 3)
+        dst[s] = make_float4(src[3 * v], src[3 * v + 1], src[3 * v + 2], dst[s].w);
+    else
+        dst[s] = make_float4(src[4 * v], src[4 * v + 1], src[4 * v + 2], src[4 * v + 3]);
+}
+__global__ void gather_slots_kernel(const float4* __restrict__ src, float* __restrict__ dst,
+                                    const int64_t* __restrict__ vert_of, int64_t s0, int64_t n, int comps) {
+    const int64_t t = (int64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    if (t >= n) return;
+    const int64_t s = s0 + t, v = vert_of[s];
+    if (v < 0) return;
+    const float4 a = src[s];
+    dst[comps * v] = a.x;
+    dst[comps * v + 1] = a.y;
+    dst[comps * v + 2] = a.z;
+    if (comps == 4) dst[4 * v + 3] = a.w;
 }
 
 // ==========================================================================================
@@ -853,16 +860,14 @@ cudaError_t launch_hair_out(const float4* src, float* dst, const int64_t* slot_o
     return cudaGetLastError();
 }
 
-cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s,
-                            const int64_t* list) {
+cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
     if (nv == 0) return cudaSuccess;
-    scatter3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv, list);
+    scatter3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
     return cudaGetLastError();
 }
-cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s,
-                           const int64_t* list) {
+cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
     if (nv == 0) return cudaSuccess;
-    gather3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv, list);
+    gather3_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
     return cudaGetLastError();
 }
 cudaError_t launch_scatter4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s) {
@@ -875,16 +880,22 @@ cudaError_t launch_gather4(const float4* src, float4* dst, const int64_t* slot_o
     gather4_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(src, dst, slot_of, nv);
     return cudaGetLastError();
 }
-cudaError_t launch_scatter4_list(const float* src, float4* dst, const int64_t* slot_of, const int64_t* list, int64_t n,
-                                 cudaStream_t s) {
-    if (n == 0) return cudaSuccess;
-    scatter4_list_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, dst, slot_of, n, list);
+cudaError_t launch_vert_of(const int64_t* slot_of, int64_t* vert_of, int64_t nv, int64_t num_slots, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(vert_of, 0xff, sizeof(int64_t) * num_slots, s);  // -1: padding
+    if (e != cudaSuccess || nv == 0) return e;
+    vert_of_kernel<<<blocks_for(nv, 256), 256, 0, s>>>(slot_of, vert_of, nv);
     return cudaGetLastError();
 }
-cudaError_t launch_gather4_list(const float4* src, float* dst, const int64_t* slot_of, const int64_t* list, int64_t n,
+cudaError_t launch_scatter_slots(const float* src, float4* dst, const int64_t* vert_of, int64_t s0, int64_t n, int comps,
+                                 cudaStream_t s) {
+    if (n == 0) return cudaSuccess;
+    scatter_slots_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, dst, vert_of, s0, n, comps);
+    return cudaGetLastError();
+}
+cudaError_t launch_gather_slots(const float4* src, float* dst, const int64_t* vert_of, int64_t s0, int64_t n, int comps,
                                 cudaStream_t s) {
     if (n == 0) return cudaSuccess;
-    gather4_list_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, dst, slot_of, n, list);
+    gather_slots_kernel<<<blocks_for(n, 256), 256, 0, s>>>(src, dst, vert_of, s0, n, comps);
     return cudaGetLastError();
 }
 

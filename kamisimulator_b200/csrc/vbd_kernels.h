@@ -85,19 +85,18 @@ cudaError_t launch_hair_in(const float* src, float4* dst, const int64_t* slot_of
 cudaError_t launch_hair_out(const float4* src, float* dst, const int64_t* slot_of, const int64_t* hair_index, int64_t nv,
                             cudaStream_t s);
 
-// boundary order <-> tile slots for vertices 0 .. nv-1, or, with a list, for vertices list[0 .. nv-1]
-// (the strands of a tape window); src / dst in boundary order are indexed by the vertex either way.
-// The 3-vector forms read and write the boundary side as floats.
-cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s,
-                            const int64_t* list = nullptr);
-cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s,
-                           const int64_t* list = nullptr);
+cudaError_t launch_scatter3(const float* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
+cudaError_t launch_gather3(const float4* src, float* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
 cudaError_t launch_scatter4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
 cudaError_t launch_gather4(const float4* src, float4* dst, const int64_t* slot_of, int64_t nv, cudaStream_t s);
-// 4-vectors of the listed vertices from / to a caller's boundary array of floats (any 4-byte alignment)
-cudaError_t launch_scatter4_list(const float* src, float4* dst, const int64_t* slot_of, const int64_t* list, int64_t n,
+
+// Tape windows: vert_of (num_slots entries) = the boundary vertex of every slot, -1 for padding; and
+// slots [s0, s0 + n) <-> their vertices in a caller's boundary array of `comps` (3 or 4) floats per
+// vertex, any 4-byte alignment (a 3-component scatter keeps the slot's .w).
+cudaError_t launch_vert_of(const int64_t* slot_of, int64_t* vert_of, int64_t nv, int64_t num_slots, cudaStream_t s);
+cudaError_t launch_scatter_slots(const float* src, float4* dst, const int64_t* vert_of, int64_t s0, int64_t n, int comps,
                                  cudaStream_t s);
-cudaError_t launch_gather4_list(const float4* src, float* dst, const int64_t* slot_of, const int64_t* list, int64_t n,
+cudaError_t launch_gather_slots(const float4* src, float* dst, const int64_t* vert_of, int64_t s0, int64_t n, int comps,
                                 cudaStream_t s);
 
 }  // namespace kami

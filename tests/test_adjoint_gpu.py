@@ -332,6 +332,38 @@ def test_tile_windows_do_not_change_the_gradient():
     solver.close()
 
 
+def test_restore_tape_window_restores_the_window_only():
+    """kami_vbd_restore_tape_window from a device state buffer rewrites the strands of the tape window
+    and the clock and leaves every other strand as it is; from host memory it is kami_vbd_set_state."""
+    import torch
+
+    g, st, solver, unit, strand_of, init, _ = _setup(num_strands=40, lengths=(5, 31), sdf=True)
+    nv, sb = g.num_vertices, g.strand_begin
+    assert nv % 4 != 0  # the orientations inside the state buffer are not 16-byte aligned
+    tiles = solver.tile_count()
+    solver.tape_reserve(1, 3)
+    solver.set_tape_window(tiles - 3, tiles)
+    a = solver.get_state()
+    for _ in range(2):
+        solver.step(1 / 60)
+    b = solver.get_state()
+    solver.restore_tape_window_from(torch.tensor(a, device="cuda"))
+    c = solver.get_state()
+    np.testing.assert_array_equal(c[13 * nv:], a[13 * nv:])  # the clock
+    restored = 0
+    for k in range(g.num_strands):
+        parts = [np.s_[3 * sb[k]:3 * sb[k + 1]], np.s_[3 * (nv + sb[k]):3 * (nv + sb[k + 1])],
+                 np.s_[3 * (2 * nv + sb[k]):3 * (2 * nv + sb[k + 1])], np.s_[9 * nv + 4 * sb[k]:9 * nv + 4 * sb[k + 1]]]
+        same_a = all(np.array_equal(c[p], a[p]) for p in parts)
+        same_b = all(np.array_equal(c[p], b[p]) for p in parts)
+        assert same_a != same_b, k  # every strand is either restored or left alone, whole
+        restored += same_a
+    assert 0 < restored < g.num_strands
+    solver.restore_tape_window_from(a)  # host memory: the whole state
+    np.testing.assert_array_equal(solver.get_state(), a)
+    solver.close()
+
+
 @pytest.mark.parametrize("lengths,group", [((150, 250), 2), ((300, 500), 4), ((600, 900), 8)])
 def test_grouped_tiles_gradient_matches_fp64_autograd(lengths, group):
     """Strands of 150-900 vertices run across groups of 2, 4 and 8 tiles: the recorded step and the
