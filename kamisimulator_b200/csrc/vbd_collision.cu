@@ -700,6 +700,7 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
     const int64_t base = (int64_t)blockIdx.x * T;
     float3 yown[2];
     SegContacts own[2];
+    int32_t second[2];  // each slot's second partner (read ahead, like the first)
 #pragma unroll
     for (int c = 0; c < 2; c++) {
         const int p = (row2 + c) * 32 + lane;  // storage offset in the tile
@@ -710,7 +711,15 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
         const float4 prm = st.prm[g];
         sprm[p] = prm;
         sqr[p] = st.qr[g];
-        own[c] = (__float_as_uint(prm.w) & F_HAS_NEXT) ? seg_contacts(cp, g) : no_contacts();
+        // the segment's contact count, first two partners and step limit, read together with the slot's
+        // state instead of after its flags and count (the arrays have an entry for every slot, and the
+        // query leaves no contacts on a slot without a segment)
+        const int n = cp.ncols[g];
+        const int32_t c0 = cp.cols[g], c1 = cp.cols[cp.num_slots + g];
+        const float lim = cp.maxstep[g];
+        const bool seg = __float_as_uint(prm.w) & F_HAS_NEXT;
+        own[c] = seg ? SegContacts{n, n > 0 ? c0 : 0, lim, 0, nullptr} : no_contacts();
+        second[c] = c1;
         yown[c] = xyz(y4[g]);
     }
     // the tile's contact lists end to end, in thread order (thread t: its even slot's list, then its
@@ -737,7 +746,7 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
         const int off = first_off + (c ? own[0].n : 0);
         const int cached = max(0, min(own[c].n, ncap - off));
         for (int m = 0; m < cached; m++) {
-            spidx[off + m] = cp.cols[(int64_t)m * cp.num_slots + base + p];
+            spidx[off + m] = m == 0 ? own[c].first : m == 1 ? second[c] : cp.cols[(int64_t)m * cp.num_slots + base + p];
             sown[off + m] = (int16_t)p;
         }
         own[c].cached = cached;
