@@ -629,9 +629,17 @@ __global__ void sweep_position_coll_kernel(DeviceState st, const float4* __restr
 // the 2,000 tiles of a 2,000-strand groom run in one wave; one per slot at T = 1024, which keeps the
 // block under the 227 KB limit).
 __host__ __device__ constexpr int coll_contact_cap(int T) { return T <= 512 ? T * 5 / 2 : T; }
+// Shared memory of coll_iteration_kernel: x | dx | q | prm | qr (T float4 each), the slots' contact
+// data (T SegContacts), the cached contacts' operands, partner slots and segments (coll_contact_cap(T)
+// each), the warps' totals; then, for tiles of several warps, the cached contacts' evaluations
+// (coll_contact_cap(T) ContactOut from coll_out_offset(T), 16-byte aligned).
+__host__ __device__ constexpr size_t coll_out_offset(int T) {
+    return ((sizeof(float4) * 5 + sizeof(SegContacts)) * T +
+            (sizeof(ContactOperands) + sizeof(int32_t) + sizeof(int16_t)) * coll_contact_cap(T) +
+            sizeof(int32_t) * (T / 64) + 15) / 16 * 16;
+}
 __host__ __device__ constexpr size_t coll_iteration_smem(int T) {
-    return (sizeof(float4) * 5 + sizeof(SegContacts)) * T +
-           (sizeof(ContactOperands) + sizeof(int32_t) + sizeof(int16_t)) * coll_contact_cap(T) + sizeof(int32_t) * (T / 64);
+    return T == 64 ? coll_out_offset(T) : coll_out_offset(T) + sizeof(ContactOut) * coll_contact_cap(T);
 }
 
 // A contact's evaluation passed from the lane that computed it to the lane whose sums take it.
@@ -819,25 +827,56 @@ __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, con
             __syncwarp();
         }
     } else {
-#pragma unroll
-    for (int c = 0; c < 2; c++) {
-        const int p = (row2 + c) * 32 + lane;
-        const int64_t g = base + p;
-        const float4 xm = sx[p], prm = sprm[p];
-        const uint32_t fl = __float_as_uint(prm.w);
-        if ((fl & F_VALID) && xm.w != 0.f) {
-            // in-tile neighbours (strands never cross tiles in the sweep form)
-            const int pn = (fl & F_HAS_NEXT) ? (int)(next_slot(g, C) - base) : p;
-            const int pq = (fl & F_HAS_PREV) ? (int)(prev_slot(g, C) - base) : p;
-            const float4 pp4 = (fl & F_HAS_PREV) ? sprm[pq] : make_float4(1.f, 0.f, 0.f, 0.f);
-            const SegContacts cop = (fl & F_HAS_PREV) ? sco[pq] : no_contacts();
-            const float3 out = coll_position(st, cp, snap, g, base + pq, fl, xm, prm, xyz(sdx[p]), yown[c],
-                                             xyz(sx[pn]), xyz(sdx[pn]), sq[p], xyz(sx[pq]), xyz(sdx[pq]), sq[pq], pp4,
-                                             sco[p], cop, h, pp);
-            sdx[p] = make_float4(out.x, out.y, out.z, 0.f);
+        // several warps per tile: the evaluations go through shared memory (after the owner array)
+        ContactOut* sout = reinterpret_cast<ContactOut*>(coll_out_offset(T) + reinterpret_cast<char*>(coll_tile));
+        const float damp = pp.damping / h;
+#pragma unroll 1
+        for (int c = 0; c < 2; c++) {
+            // the tile's cached contacts, each from its segment's end point of colour c
+            for (int e = threadIdx.x; e < total; e += blockDim.x) {
+                const int s0 = sown[e];
+                const int s1 = (int)(next_slot(base + s0, C) - base);
+                sout[e] = contact_eval(cp, spart[e], xyz(sx[s0]), xyz(sx[s1]), xyz(sdx[s0]), xyz(sdx[s1]),
+                                       ((s0 >> 5) & 1) == c, damp);
+            }
+            __syncthreads();
+            const int p = (row2 + c) * 32 + lane;
+            const int64_t g = base + p;
+            const float4 xm = sx[p], prm = sprm[p];
+            const uint32_t fl = __float_as_uint(prm.w);
+            if ((fl & F_VALID) && xm.w != 0.f) {
+                // in-tile neighbours (strands never cross tiles in the sweep form)
+                const bool hn = fl & F_HAS_NEXT, hp = fl & F_HAS_PREV;
+                const int pn = hn ? (int)(next_slot(g, C) - base) : p;
+                const int pq = hp ? (int)(prev_slot(g, C) - base) : p;
+                const float3 vi = xyz(xm), vi_dx = xyz(sdx[p]), xj = xyz(sx[pn]), vj_dx = xyz(sdx[pn]);
+                const float3 xp = xyz(sx[pq]), dp = xyz(sdx[pq]);
+                const SegContacts co = sco[p];
+                const SegContacts cop = hp ? sco[pq] : no_contacts();
+                float3 f, f2 = f3(0.f, 0.f, 0.f);
+                float H[6], H2[6] = {0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+                coll_terms_next(st, snap, g, fl, xm, prm, vi_dx, c ? yown[1] : yown[0], xj, vj_dx, sq[p], h, pp, f, H);
+                float step_limit = INFINITY;
+                if (hn) {
+                    step_limit = co.limit;
+                    const ContactOut* ev = sout + (co.part - spart);
+                    for (int m = 0; m < co.cached; m++)
+                        if (ev[m].touch) contact_apply(ev[m], f, H);
+                    contact_terms_global(st, cp, snap, g, co, vi, xj, vi_dx, vj_dx, true, damp, f, H);
+                }
+                if (hp) {
+                    coll_terms_prev(vi, vi_dx, xp, dp, sq[pq], sprm[pq], damp, f2, H2);
+                    const ContactOut* ev = sout + (cop.part - spart);
+                    for (int m = 0; m < cop.cached; m++)
+                        if (ev[m].touch) contact_apply(ev[m], f2, H2);
+                    contact_terms_global(st, cp, snap, base + pq, cop, xp, vi, dp, vi_dx, false, damp, f2, H2);
+                    step_limit = fminf(step_limit, cop.limit);
+                }
+                const float3 out = coll_solve(vi_dx, f, H, hp, f2, H2, step_limit, pp);
+                sdx[p] = make_float4(out.x, out.y, out.z, 0.f);
+            }
+            __syncthreads();
         }
-        __syncthreads();
-    }
     }
     for (int c = 0; c < 2; c++) {
         const int p = (row2 + c) * 32 + lane;
