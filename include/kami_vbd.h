@@ -31,7 +31,7 @@ typedef enum kami_status {
     KAMI_ERR_OUT_OF_MEMORY = 3,    /* device or pinned-host allocation failed */
     KAMI_ERR_NONFINITE = 4,        /* the device status word saw a NaN/Inf position, velocity or orientation */
     KAMI_ERR_GEOMETRY = 5,         /* zero-length or dangling segment (Sim::configure, YBSimulator.cu:185-197) */
-    KAMI_ERR_UNSUPPORTED = 6,      /* request outside what this build supports (e.g. strand longer than a tile) */
+    KAMI_ERR_UNSUPPORTED = 6,      /* request outside what this library supports (e.g. strand longer than a tile) */
     KAMI_ERR_TIMEOUT = 7,          /* a bounded device wait gave up */
     KAMI_ERR_STATE = 8,            /* call made in the wrong order (e.g. backward without a recorded forward) */
     KAMI_ERR_CONTACTS = 9,         /* a segment had more than 16 hair-hair contacts (MAX_COLLISIONS_PER_SEGMENT,
