@@ -683,7 +683,8 @@ __device__ __forceinline__ ContactOut shfl_contact(const ContactOut& o, int src)
 // of coll_position; what changes is that a vertex with many contacts no longer evaluates them one
 // after another while the other lanes of its warp wait.  The tiles of a groom run in one wave when
 // they fit, so the iteration takes as long as its slowest tile, which is the one with the most
-// contacts on one vertex.
+// contacts on one vertex.  Tiles of several warps (!ONE_WARP) do the same with the block's threads
+// over the tile's cached contacts and the evaluations in shared memory (coll_out_offset).
 template <bool ONE_WARP>
 __global__ void __launch_bounds__(512) coll_iteration_kernel(DeviceState st, const float4* __restrict__ y4, float4* q,
                                                              const float4* __restrict__ snap,
