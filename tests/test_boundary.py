@@ -111,6 +111,8 @@ def test_null_handle_calls_fail_cleanly():
     assert lib.kami_vbd_get_launch_mode(None, ctypes.byref(m)) == 1
     assert lib.kami_vbd_step_hair(None, ctypes.c_float(0.01), None, None, None, None) == 1
     assert lib.kami_vbd_strain_limit(None, ctypes.c_float(0.1), None) == 1
+    assert lib.kami_vbd_set_tape_window(None, 0, 1) == 1
+    assert lib.kami_vbd_restore_tape_window(None, None, 0, vbd.MEM_DEVICE) == 1
     # host registration checks its arguments before any CUDA call
     assert lib.kami_host_register(None, 64) == 1
     assert lib.kami_host_register(ctypes.c_void_p(4096), 0) == 1
